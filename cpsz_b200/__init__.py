@@ -1,0 +1,326 @@
+"""cpsz_b200 -- B200-native (sm_100a) cpSZ critical-point-preserving compressor.
+
+Python mirror of the reference's public operator interface for the offline path
+(bzhan166/cpSZ):
+
+=============================================  =====================================================
+reference (C++)                                here
+=============================================  =====================================================
+``sz_compress_cp_preserve_2d_offline<float>``  :func:`sz_compress_cp_preserve_2d_offline`
+``sz_decompress_cp_preserve_2d_offline``       :func:`sz_decompress_cp_preserve_2d_offline`
+``sz_compress_cp_preserve_3d_offline_log``     :func:`sz_compress_cp_preserve_3d_offline_log`
+``sz_decompress_cp_preserve_3d_online_log``    :func:`sz_decompress_cp_preserve_3d_online_log`
+``sz_lossless_compress/decompress`` (ZSTD)     :func:`sz_lossless_compress` / :func:`sz_lossless_decompress`
+=============================================  =====================================================
+
+Everything runs through ``libcpsz_b200.so`` (C ABI, ``include/cpsz_b200.h``):
+hand-written CUDA kernels for sm_100a driven by C++ host code.  There is no CPU
+fallback; without the library or a GPU every call raises :class:`CpszError`.
+Fields are numpy arrays (host) or CUDA tensors/arrays exposing
+``__cuda_array_interface__`` (device, used in place).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "_lib", "libcpsz_b200.so")
+
+CPSZ_OK = 0
+ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "out of memory", 4: "malformed blob", 5: "device wait timed out",
+          6: "unsupported input", 7: "no CUDA device"}
+
+
+class CpszError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{ERRORS.get(code, code)}] {msg}")
+        self.code = code
+
+
+_lib = None
+_lock = threading.Lock()
+_sz = C.c_size_t
+_vp = C.c_void_p
+
+
+def _declare(L):
+    L.cpsz_b200_last_error.restype = C.c_char_p
+    L.cpsz_b200_version.restype = C.c_int
+    L.cpsz_b200_ctx_create.argtypes = [C.c_int, C.POINTER(_vp)]
+    L.cpsz_b200_ctx_destroy.argtypes = [_vp]
+    L.cpsz_b200_ctx_kernel_launches.argtypes = [_vp, C.POINTER(C.c_uint64)]
+    L.cpsz_b200_ctx_stream.argtypes = [_vp, C.POINTER(_vp)]
+    L.cpsz_b200_compress_2d_offline_f32.argtypes = [_vp, _vp, _vp, _sz, _sz, C.c_double, C.POINTER(_vp), C.POINTER(_sz)]
+    L.cpsz_b200_compress_2d_offline_f32_into.argtypes = [_vp, _vp, _vp, _sz, _sz, C.c_double, _vp, _sz, C.POINTER(_sz)]
+    L.cpsz_b200_decompress_2d_offline_f32.argtypes = [_vp, C.c_char_p, _sz, _sz, _sz, _vp, _vp]
+    L.cpsz_b200_compress_2d_stages.argtypes = [_vp, _vp, _vp, _sz, _sz, C.c_double, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.cpsz_b200_blob_size_2d.argtypes = [C.c_char_p]
+    L.cpsz_b200_blob_size_2d.restype = _sz
+    L.cpsz_b200_generate_field_2d.argtypes = [C.c_uint64, _sz, _sz, C.c_int, C.c_double, C.c_double, _vp, _vp]
+    L.cpsz_b200_generate_field_3d.argtypes = [C.c_uint64, _sz, _sz, _sz, C.c_int, C.c_double, C.c_double, _vp, _vp, _vp]
+    L.cpsz_b200_batch_layout.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp]
+    L.cpsz_b200_zstd_compress.argtypes = [C.c_char_p, _sz, C.c_int, C.POINTER(_vp), C.POINTER(_sz)]
+    L.cpsz_b200_zstd_decompress.argtypes = [C.c_char_p, _sz, _vp, _sz]
+    for name in ("cpsz_b200_compress_3d_offline_log_f32", "cpsz_b200_decompress_3d_online_log_f32",
+                 "cpsz_b200_cp_check_2d", "cpsz_b200_cp_check_3d"):
+        if hasattr(L, name):
+            getattr(L, name).restype = C.c_int
+    if hasattr(L, "cpsz_b200_compress_3d_offline_log_f32"):
+        L.cpsz_b200_compress_3d_offline_log_f32.argtypes = [_vp, _vp, _vp, _vp, _sz, _sz, _sz, C.c_double,
+                                                            C.POINTER(_vp), C.POINTER(_sz)]
+        L.cpsz_b200_decompress_3d_online_log_f32.argtypes = [_vp, C.c_char_p, _sz, _sz, _sz, _sz, _vp, _vp, _vp]
+    if hasattr(L, "cpsz_b200_cp_check_2d"):
+        L.cpsz_b200_cp_check_2d.argtypes = [_vp, _vp, _vp, _vp, _vp, _sz, _sz, _vp, C.POINTER(C.c_uint64)]
+        L.cpsz_b200_cp_check_3d.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _sz, _sz, _vp,
+                                            C.POINTER(C.c_uint64)]
+
+
+def lib():
+    """The loaded native library (built in-tree on first use if absent)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                from . import build as _b
+                _b.build()
+            L = C.CDLL(LIB_PATH)
+            _declare(L)
+            _lib = L
+    return _lib
+
+
+def _check(rc: int):
+    if rc != CPSZ_OK:
+        raise CpszError(rc, lib().cpsz_b200_last_error().decode(errors="replace"))
+
+
+class Context:
+    """A device workspace + stream (``cpsz_b200_ctx``)."""
+
+    def __init__(self, device: int = 0):
+        h = _vp()
+        _check(lib().cpsz_b200_ctx_create(device, C.byref(h)))
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            lib().cpsz_b200_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def kernel_launches(self) -> int:
+        v = C.c_uint64()
+        _check(lib().cpsz_b200_ctx_kernel_launches(self.handle, C.byref(v)))
+        return v.value
+
+    @property
+    def stream(self) -> int:
+        v = _vp()
+        _check(lib().cpsz_b200_ctx_stream(self.handle, C.byref(v)))
+        return v.value or 0
+
+
+def _h(ctx):
+    return ctx.handle if ctx is not None else None
+
+
+def _ptr(a, dtype=np.float32):
+    """(pointer, keepalive, shape) of a host numpy array or a device array."""
+    if hasattr(a, "__cuda_array_interface__"):
+        cai = a.__cuda_array_interface__
+        if np.dtype(cai["typestr"]) != np.dtype(dtype):
+            raise TypeError(f"expected {np.dtype(dtype)} device array")
+        if cai.get("strides") not in (None,):
+            exp = []
+            s = np.dtype(dtype).itemsize
+            for d in reversed(cai["shape"]):
+                exp.insert(0, s)
+                s *= d
+            if tuple(cai["strides"]) != tuple(exp):
+                raise TypeError("device array must be C-contiguous")
+        return cai["data"][0], a, tuple(cai["shape"])
+    arr = np.ascontiguousarray(a, dtype=dtype)
+    return arr.ctypes.data, arr, arr.shape
+
+
+# ---- 2D ---------------------------------------------------------------------------
+
+def sz_compress_cp_preserve_2d_offline(U, V, r1: int | None = None, r2: int | None = None, max_pwr_eb: float = 0.1,
+                                       ctx: Context | None = None) -> bytes:
+    """GPU ``sz_compress_cp_preserve_2d_offline<float>``: returns the blob (bytes)."""
+    pu, ku, su = _ptr(U)
+    pv, kv, sv = _ptr(V)
+    if r1 is None:
+        r1, r2 = su
+    if su != sv or int(np.prod(su)) != r1 * r2:
+        raise ValueError("U and V must both hold r1*r2 floats")
+    out = _vp()
+    n = _sz()
+    _check(lib().cpsz_b200_compress_2d_offline_f32(_h(ctx), pu, pv, r1, r2, float(max_pwr_eb), C.byref(out),
+                                                   C.byref(n)))
+    try:
+        return C.string_at(out, n.value)
+    finally:
+        C.CDLL(None).free(out)
+
+
+def compress_2d_into(U, V, r1, r2, max_pwr_eb, out, ctx: Context | None = None) -> int:
+    """Compress into caller memory ``out`` (host numpy uint8 or device uint8 array); returns the blob size."""
+    pu, ku, _ = _ptr(U)
+    pv, kv, _ = _ptr(V)
+    po, ko, so = _ptr(out, np.uint8)
+    n = _sz()
+    _check(lib().cpsz_b200_compress_2d_offline_f32_into(_h(ctx), pu, pv, r1, r2, float(max_pwr_eb), po,
+                                                        int(np.prod(so)), C.byref(n)))
+    return n.value
+
+
+def sz_decompress_cp_preserve_2d_offline(blob: bytes, r1: int, r2: int, U=None, V=None,
+                                         ctx: Context | None = None):
+    """GPU ``sz_decompress_cp_preserve_2d_offline<float>``: returns (U, V).
+
+    U, V may be given as preallocated host or device float32 arrays of r1*r2."""
+    if U is None:
+        U = np.empty((r1, r2), np.float32)
+    if V is None:
+        V = np.empty((r1, r2), np.float32)
+    pu, ku, _ = _ptr(U)
+    pv, kv, _ = _ptr(V)
+    if ku is not U or kv is not V:
+        raise TypeError("output arrays must be C-contiguous float32")
+    _check(lib().cpsz_b200_decompress_2d_offline_f32(_h(ctx), blob, len(blob), r1, r2, pu, pv))
+    return U, V
+
+
+def compress_2d_stages(U, V, max_pwr_eb: float, ctx: Context | None = None) -> dict:
+    """Intermediate streams of the 2D compressor (ids, block-order codes, reconstruction)."""
+    U = np.ascontiguousarray(U, np.float32)
+    V = np.ascontiguousarray(V, np.float32)
+    r1, r2 = U.shape
+    n = r1 * r2
+    ids = np.empty(2 * n, np.int32)
+    cu = np.empty(n, np.int32)
+    cv = np.empty(n, np.int32)
+    ru = np.empty((r1, r2), np.float32)
+    rv = np.empty((r1, r2), np.float32)
+    nu = (C.c_size_t * 2)()
+    _check(lib().cpsz_b200_compress_2d_stages(_h(ctx), U.ctypes.data, V.ctypes.data, r1, r2, float(max_pwr_eb),
+                                              ids.ctypes.data, cu.ctypes.data, cv.ctypes.data, ru.ctypes.data,
+                                              rv.ctypes.data, C.addressof(nu)))
+    return {"ids": ids, "codes_u": cu, "codes_v": cv, "recon_u": ru, "recon_v": rv, "n_unpred": (nu[0], nu[1])}
+
+
+def blob_size_2d(blob: bytes) -> int:
+    return lib().cpsz_b200_blob_size_2d(blob)
+
+
+# ---- 3D ---------------------------------------------------------------------------
+
+def sz_compress_cp_preserve_3d_offline_log(U, V, W, r1=None, r2=None, r3=None, max_pwr_eb: float = 0.1,
+                                           ctx: Context | None = None) -> bytes:
+    """GPU ``sz_compress_cp_preserve_3d_offline_log<float>``: returns the blob (bytes)."""
+    pu, ku, su = _ptr(U)
+    pv, kv, sv = _ptr(V)
+    pw, kw, sw = _ptr(W)
+    if r1 is None:
+        r1, r2, r3 = su
+    if not (su == sv == sw) or int(np.prod(su)) != r1 * r2 * r3:
+        raise ValueError("U, V, W must each hold r1*r2*r3 floats")
+    out = _vp()
+    n = _sz()
+    _check(lib().cpsz_b200_compress_3d_offline_log_f32(_h(ctx), pu, pv, pw, r1, r2, r3, float(max_pwr_eb),
+                                                       C.byref(out), C.byref(n)))
+    try:
+        return C.string_at(out, n.value)
+    finally:
+        C.CDLL(None).free(out)
+
+
+def sz_decompress_cp_preserve_3d_online_log(blob: bytes, r1: int, r2: int, r3: int, U=None, V=None, W=None,
+                                            ctx: Context | None = None):
+    """GPU ``sz_decompress_cp_preserve_3d_online_log<float>``: returns (U, V, W)."""
+    outs = []
+    for a in (U, V, W):
+        outs.append(np.empty((r1, r2, r3), np.float32) if a is None else a)
+    ptrs = [_ptr(a)[0] for a in outs]
+    _check(lib().cpsz_b200_decompress_3d_online_log_f32(_h(ctx), blob, len(blob), r1, r2, r3, *ptrs))
+    return tuple(outs)
+
+
+# ---- exact critical-point check ------------------------------------------------------
+
+CP_TYPES_2D = ("NONE", "SINGULAR", "ATTRACTING", "REPELLING", "SADDLE", "ATTRACTING_FOCUS", "REPELLING_FOCUS",
+               "CENTER")
+
+
+def cp_check_2d(Ua, Va, Ub=None, Vb=None, cells: bool = False, ctx: Context | None = None):
+    """Exact per-cell CP classification of (Ua, Va), compared with (Ub, Vb) if given.
+
+    Returns dict(cps_a, cps_b, lost_or_spurious, type_changed[, cells])."""
+    pa = [_ptr(a) for a in (Ua, Va)]
+    r1, r2 = pa[0][2]
+    pb = [_ptr(b) for b in (Ub, Vb)] if Ub is not None else None
+    ncell = 2 * (r1 - 1) * (r2 - 1) if r1 > 1 and r2 > 1 else 0
+    out = np.zeros(max(ncell, 1), np.uint8) if cells else None
+    counts = (C.c_uint64 * 4)()
+    _check(lib().cpsz_b200_cp_check_2d(_h(ctx), pa[0][0], pa[1][0], pb[0][0] if pb else None,
+                                       pb[1][0] if pb else None, r1, r2, out.ctypes.data if cells else None, counts))
+    res = {"cps_a": counts[0], "cps_b": counts[1], "lost_or_spurious": counts[2], "type_changed": counts[3]}
+    if cells:
+        res["cells"] = out[:ncell]
+    return res
+
+
+def cp_check_3d(Ua, Va, Wa, Ub=None, Vb=None, Wb=None, cells: bool = False, ctx: Context | None = None):
+    pa = [_ptr(a) for a in (Ua, Va, Wa)]
+    r1, r2, r3 = pa[0][2]
+    pb = [_ptr(b) for b in (Ub, Vb, Wb)] if Ub is not None else None
+    ncell = 6 * (r1 - 1) * (r2 - 1) * (r3 - 1) if min(r1, r2, r3) > 1 else 0
+    out = np.zeros(max(ncell, 1), np.uint8) if cells else None
+    counts = (C.c_uint64 * 4)()
+    _check(lib().cpsz_b200_cp_check_3d(_h(ctx), pa[0][0], pa[1][0], pa[2][0], pb[0][0] if pb else None,
+                                       pb[1][0] if pb else None, pb[2][0] if pb else None, r1, r2, r3,
+                                       out.ctypes.data if cells else None, counts))
+    res = {"cps_a": counts[0], "cps_b": counts[1], "lost_or_spurious": counts[2], "type_changed": counts[3]}
+    if cells:
+        res["cells"] = out[:ncell]
+    return res
+
+
+# ---- lossless stage (host ZSTD, as the reference) -------------------------------------
+
+def sz_lossless_compress(data: bytes, level: int = 3) -> bytes:
+    out = _vp()
+    n = _sz()
+    _check(lib().cpsz_b200_zstd_compress(data, len(data), level, C.byref(out), C.byref(n)))
+    try:
+        return C.string_at(out, n.value)
+    finally:
+        C.CDLL(None).free(out)
+
+
+def sz_lossless_decompress(data: bytes, target_size: int) -> bytes:
+    buf = C.create_string_buffer(target_size)
+    _check(lib().cpsz_b200_zstd_decompress(data, len(data), C.addressof(buf), target_size))
+    return buf.raw
+
+
+from . import workloads  # noqa: E402  (synthetic generators; needs lib())
+
+__all__ = [
+    "Context", "CpszError", "lib", "sz_compress_cp_preserve_2d_offline", "sz_decompress_cp_preserve_2d_offline",
+    "sz_compress_cp_preserve_3d_offline_log", "sz_decompress_cp_preserve_3d_online_log", "compress_2d_into",
+    "compress_2d_stages", "cp_check_2d", "cp_check_3d", "sz_lossless_compress", "sz_lossless_decompress",
+    "workloads",
+]

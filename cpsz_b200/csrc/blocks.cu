@@ -1,0 +1,262 @@
+// blocks.cu -- 12x12 block-order plumbing of the 2D field blobs, and a
+// generic device-wide exclusive scan.
+//
+// The reference emits quantization codes and unpredictable values in 12x12
+// block order (blocks row-major, rows inside a block, src/sz_compress_3d.cpp:
+// 126-193).  A "segment" is one row of one block (up to 12 points, contiguous
+// in block order); segments are numbered in block order:
+//   ord = bi*12*nby + bj*h + li,   h = rows of block-row bi (12, or the remainder),
+// and element (i, j) sits at block-order position
+//   bi*12*r2 + bj*12*h + li*w + lj,   w = columns of block bj.
+#include <algorithm>
+
+#include "kernels.h"
+
+namespace cpsz {
+
+namespace {
+
+constexpr int BS = 12;
+constexpr int NT = 256;
+
+struct Seg {
+  int i, j0, w;
+  long long pos;  // block-order position of the segment's first element
+};
+
+__device__ __forceinline__ Seg seg_of(long long ord, int r1, int r2, int nby) {
+  long long per_brow = (long long)BS * nby;
+  int bi = (int)(ord / per_brow);
+  int rem = (int)(ord - (long long)bi * per_brow);
+  int h = min(BS, r1 - bi * BS);
+  int bj = rem / h, li = rem - bj * h;
+  int w = min(BS, r2 - bj * BS);
+  Seg s;
+  s.i = bi * BS + li;
+  s.j0 = bj * BS;
+  s.w = w;
+  s.pos = (long long)bi * BS * r2 + (long long)bj * BS * h + (long long)li * w;
+  return s;
+}
+
+__global__ void __launch_bounds__(NT) r2b_kernel(const uint16_t* __restrict__ raster, long long pitch, int r1, int r2,
+                                                 int nby, long long nseg, uint16_t* __restrict__ blocks) {
+  long long ord = (long long)blockIdx.x * NT + threadIdx.x;
+  if (ord >= nseg) return;
+  Seg s = seg_of(ord, r1, r2, nby);
+  const uint16_t* src = raster + (long long)s.i * pitch + s.j0;
+  for (int k = 0; k < s.w; k++) blocks[s.pos + k] = src[k];
+}
+
+__global__ void __launch_bounds__(NT) b2r_kernel(const uint16_t* __restrict__ blocks, int r1, int r2, int nby,
+                                                 long long nseg, uint16_t* __restrict__ raster, long long pitch) {
+  long long ord = (long long)blockIdx.x * NT + threadIdx.x;
+  if (ord >= nseg) return;
+  Seg s = seg_of(ord, r1, r2, nby);
+  uint16_t* dst = raster + (long long)s.i * pitch + s.j0;
+  for (int k = 0; k < s.w; k++) dst[k] = blocks[s.pos + k];
+}
+
+__global__ void __launch_bounds__(NT) seg_count_kernel(const uint16_t* __restrict__ raster, long long pitch, int r1,
+                                                       int r2, int nby, long long nseg, unsigned int* __restrict__ cnt) {
+  long long ord = (long long)blockIdx.x * NT + threadIdx.x;
+  if (ord >= nseg) return;
+  Seg s = seg_of(ord, r1, r2, nby);
+  const uint16_t* src = raster + (long long)s.i * pitch + s.j0;
+  unsigned int c = 0;
+  for (int k = 0; k < s.w; k++) c += (src[k] == 0);
+  cnt[ord] = c;
+}
+
+__global__ void __launch_bounds__(NT) gather_kernel(const uint16_t* __restrict__ raster, long long pitch,
+                                                    const float* __restrict__ x, long long x_pitch, int r1, int r2,
+                                                    int nby, long long nseg, const unsigned int* __restrict__ off,
+                                                    float* __restrict__ unpred) {
+  long long ord = (long long)blockIdx.x * NT + threadIdx.x;
+  if (ord >= nseg) return;
+  Seg s = seg_of(ord, r1, r2, nby);
+  const uint16_t* src = raster + (long long)s.i * pitch + s.j0;
+  const float* xs = x + (long long)s.i * x_pitch + s.j0;
+  unsigned int o = off[ord];
+  for (int k = 0; k < s.w; k++)
+    if (src[k] == 0) unpred[o++] = xs[k];
+}
+
+__global__ void __launch_bounds__(NT) scatter_kernel(const uint16_t* __restrict__ raster, long long pitch,
+                                                     const float* __restrict__ unpred, unsigned long long n_unpred,
+                                                     int r1, int r2, int nby, long long nseg,
+                                                     const unsigned int* __restrict__ off, float* __restrict__ x,
+                                                     long long x_pitch, int* flag) {
+  long long ord = (long long)blockIdx.x * NT + threadIdx.x;
+  if (ord >= nseg) return;
+  Seg s = seg_of(ord, r1, r2, nby);
+  const uint16_t* src = raster + (long long)s.i * pitch + s.j0;
+  float* xs = x + (long long)s.i * x_pitch + s.j0;
+  unsigned long long o = off[ord];
+  for (int k = 0; k < s.w; k++)
+    if (src[k] == 0) {
+      if (o < n_unpred) xs[k] = unpred[o];
+      else atomicOr(flag, FLAG_RAW_RANGE);
+      o++;
+    }
+}
+
+// ---- generic exclusive scan (u32) ---------------------------------------------------
+constexpr int SCAN_NT = 1024;
+constexpr int SCAN_PER = 8;
+constexpr int SCAN_CHUNK = SCAN_NT * SCAN_PER;
+
+__device__ __forceinline__ unsigned int block_exclusive_scan(unsigned int v, unsigned int* warp_tot,
+                                                             unsigned int* total) {
+  unsigned int x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) >= o) x += y;
+  }
+  if ((threadIdx.x & 31) == 31) warp_tot[threadIdx.x >> 5] = x;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    unsigned int w = (threadIdx.x < blockDim.x / 32) ? warp_tot[threadIdx.x] : 0u;
+    for (int o = 1; o < 32; o <<= 1) {
+      unsigned int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (threadIdx.x >= o) w += y;
+    }
+    warp_tot[threadIdx.x] = w;
+  }
+  __syncthreads();
+  unsigned int pre = (threadIdx.x >= 32 ? warp_tot[(threadIdx.x >> 5) - 1] : 0u) + x - v;
+  if (total) *total = warp_tot[blockDim.x / 32 - 1];
+  __syncthreads();
+  return pre;
+}
+
+__global__ void __launch_bounds__(SCAN_NT) scan_reduce_kernel(const unsigned int* __restrict__ in, size_t n,
+                                                              unsigned int* __restrict__ part) {
+  __shared__ unsigned int warp_tot[32];
+  size_t base = (size_t)blockIdx.x * SCAN_CHUNK;
+  unsigned int s = 0;
+  for (int k = 0; k < SCAN_PER; k++) {
+    size_t i = base + (size_t)k * SCAN_NT + threadIdx.x;
+    if (i < n) s += in[i];
+  }
+  unsigned int total;
+  block_exclusive_scan(s, warp_tot, &total);
+  if (threadIdx.x == 0) part[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(SCAN_NT) scan_partials_kernel(unsigned int* __restrict__ part, size_t np) {
+  __shared__ unsigned int warp_tot[32];
+  __shared__ unsigned int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (size_t base = 0; base < np; base += SCAN_NT) {
+    size_t i = base + threadIdx.x;
+    unsigned int v = i < np ? part[i] : 0u;
+    unsigned int total;
+    unsigned int pre = block_exclusive_scan(v, warp_tot, &total);
+    if (i < np) part[i] = carry + pre;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[np] = carry;
+}
+
+__global__ void __launch_bounds__(SCAN_NT) scan_down_kernel(const unsigned int* __restrict__ in, size_t n,
+                                                            const unsigned int* __restrict__ part,
+                                                            unsigned int* __restrict__ out) {
+  __shared__ unsigned int warp_tot[32];
+  size_t base = (size_t)blockIdx.x * SCAN_CHUNK + (size_t)threadIdx.x * SCAN_PER;
+  unsigned int v[SCAN_PER];
+  unsigned int s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_PER; k++) {
+    size_t i = base + k;
+    v[k] = i < n ? in[i] : 0u;
+    s += v[k];
+  }
+  unsigned int pre = block_exclusive_scan(s, warp_tot, nullptr) + part[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < SCAN_PER; k++) {
+    size_t i = base + k;
+    if (i < n) out[i] = pre;
+    pre += v[k];
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = part[gridDim.x];
+}
+
+inline long long nseg_of(int r1, int r2) { return (long long)r1 * ((r2 - 1) / BS + 1); }
+inline unsigned grid_of(long long n) { return (unsigned)((n + NT - 1) / NT); }
+
+}  // namespace
+
+size_t scan_u32_tmp_bytes(size_t n) { return ((n + SCAN_CHUNK - 1) / SCAN_CHUNK + 2) * sizeof(unsigned int) + 256; }
+
+int launch_scan_u32(cpsz_b200_ctx* ctx, const unsigned int* in, unsigned int* out, size_t n, void* tmp) {
+  size_t nb = (n + SCAN_CHUNK - 1) / SCAN_CHUNK;
+  if (nb == 0) {
+    cudaMemsetAsync(out, 0, sizeof(unsigned int), ctx->stream);
+    return CPSZ_OK;
+  }
+  unsigned int* part = (unsigned int*)tmp;
+  scan_reduce_kernel<<<(unsigned)nb, SCAN_NT, 0, ctx->stream>>>(in, n, part);
+  scan_partials_kernel<<<1, SCAN_NT, 0, ctx->stream>>>(part, nb);
+  scan_down_kernel<<<(unsigned)nb, SCAN_NT, 0, ctx->stream>>>(in, n, part, out);
+  count_launch(ctx, 3);
+  return check_launch("scan_u32");
+}
+
+int launch_raster_to_blocks_u16(cpsz_b200_ctx* ctx, const uint16_t* raster, long long pitch, int r1, int r2,
+                                uint16_t* blocks, unsigned long long* hist) {
+  long long nseg = nseg_of(r1, r2);
+  int nby = (r2 - 1) / BS + 1;
+  r2b_kernel<<<grid_of(nseg), NT, 0, ctx->stream>>>(raster, pitch, r1, r2, nby, nseg, blocks);
+  count_launch(ctx);
+  CPSZ_TRY(check_launch("r2b_kernel"));
+  if (hist) return launch_hist_u16(ctx, blocks, (size_t)r1 * r2, hist);
+  return CPSZ_OK;
+}
+
+int launch_blocks_to_raster_u16(cpsz_b200_ctx* ctx, const uint16_t* blocks, int r1, int r2, uint16_t* raster,
+                                long long pitch) {
+  long long nseg = nseg_of(r1, r2);
+  int nby = (r2 - 1) / BS + 1;
+  b2r_kernel<<<grid_of(nseg), NT, 0, ctx->stream>>>(blocks, r1, r2, nby, nseg, raster, pitch);
+  count_launch(ctx);
+  return check_launch("b2r_kernel");
+}
+
+size_t segment_scan_tmp_bytes(int r1, int r2) { return scan_u32_tmp_bytes((size_t)nseg_of(r1, r2)); }
+
+int launch_segment_scan(cpsz_b200_ctx* ctx, const uint16_t* codes_raster, long long pitch, int r1, int r2,
+                        unsigned int* seg_count, unsigned int* seg_off, void* scan_tmp) {
+  long long nseg = nseg_of(r1, r2);
+  int nby = (r2 - 1) / BS + 1;
+  seg_count_kernel<<<grid_of(nseg), NT, 0, ctx->stream>>>(codes_raster, pitch, r1, r2, nby, nseg, seg_count);
+  count_launch(ctx);
+  CPSZ_TRY(check_launch("seg_count_kernel"));
+  return launch_scan_u32(ctx, seg_count, seg_off, (size_t)nseg, scan_tmp);
+}
+
+int launch_gather_unpred(cpsz_b200_ctx* ctx, const uint16_t* codes_raster, long long pitch, const float* x,
+                         long long x_pitch, int r1, int r2, const unsigned int* seg_off, float* unpred) {
+  long long nseg = nseg_of(r1, r2);
+  int nby = (r2 - 1) / BS + 1;
+  gather_kernel<<<grid_of(nseg), NT, 0, ctx->stream>>>(codes_raster, pitch, x, x_pitch, r1, r2, nby, nseg, seg_off,
+                                                       unpred);
+  count_launch(ctx);
+  return check_launch("gather_kernel");
+}
+
+int launch_scatter_unpred(cpsz_b200_ctx* ctx, const uint16_t* codes_raster, long long pitch, const float* unpred,
+                          unsigned long long n_unpred, int r1, int r2, const unsigned int* seg_off, float* x_raster,
+                          long long x_pitch) {
+  long long nseg = nseg_of(r1, r2);
+  int nby = (r2 - 1) / BS + 1;
+  scatter_kernel<<<grid_of(nseg), NT, 0, ctx->stream>>>(codes_raster, pitch, unpred, n_unpred, r1, r2, nby, nseg,
+                                                        seg_off, x_raster, x_pitch, ctx->d_flag);
+  count_launch(ctx);
+  return check_launch("scatter_kernel");
+}
+
+}  // namespace cpsz

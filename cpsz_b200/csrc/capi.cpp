@@ -1,0 +1,271 @@
+// capi.cpp -- the extern "C" layer of libcpsz_b200.so and the C++ drop-ins
+// that keep the reference's template signatures.
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "cpsz_b200.h"
+#include "cpsz_b200.hpp"
+#include "pipeline.h"
+
+// system libzstd.so.1 (linked directly; the image has no zstd.h)
+extern "C" {
+size_t ZSTD_compress(void* dst, size_t dstCapacity, const void* src, size_t srcSize, int compressionLevel);
+size_t ZSTD_decompress(void* dst, size_t dstCapacity, const void* src, size_t compressedSize);
+size_t ZSTD_compressBound(size_t srcSize);
+unsigned ZSTD_isError(size_t code);
+const char* ZSTD_getErrorName(size_t code);
+}
+
+namespace cpsz {
+
+int copy_out(cpsz_b200_ctx* ctx, void* dst, const void* d_src, size_t n) {
+  if (!n) return CPSZ_OK;
+  cudaMemcpyKind k = is_device_ptr(dst) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  CPSZ_CUDA_TRY(cudaMemcpyAsync(dst, d_src, n, k, ctx->stream));
+  return CPSZ_OK;
+}
+
+int copy_in(cpsz_b200_ctx* ctx, void* d_dst, const void* src, size_t n) {
+  if (!n) return CPSZ_OK;
+  cudaMemcpyKind k = is_device_ptr(src) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  CPSZ_CUDA_TRY(cudaMemcpyAsync(d_dst, src, n, k, ctx->stream));
+  return CPSZ_OK;
+}
+
+}  // namespace cpsz
+
+using namespace cpsz;
+
+#define RESOLVE(ctx)            \
+  int _rc = CPSZ_OK;            \
+  ctx = resolve_ctx(ctx, &_rc); \
+  if (!ctx) return _rc;         \
+  clear_error();
+
+extern "C" {
+
+int cpsz_b200_compress_2d_offline_f32(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2,
+                                      double max_pwr_eb, unsigned char** blob, size_t* blob_size) {
+  if (!blob || !blob_size) return set_error(CPSZ_ERR_INVALID, "null output pointer");
+  *blob = nullptr;
+  *blob_size = 0;
+  RESOLVE(ctx);
+  Blob2D b;
+  CPSZ_TRY(compress_2d(ctx, U, V, r1, r2, max_pwr_eb, &b, nullptr));
+  unsigned char* h = (unsigned char*)malloc(b.size ? b.size : 1);
+  if (!h) return set_error(CPSZ_ERR_NOMEM, "host blob of %zu bytes", b.size);
+  CPSZ_TRY(pinned_reserve(ctx, b.size));
+  cudaError_t e = cudaMemcpyAsync(ctx->pinned, b.d_blob, b.size, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    free(h);
+    return set_error(CPSZ_ERR_CUDA, "blob download: %s", cudaGetErrorString(e));
+  }
+  memcpy(h, ctx->pinned, b.size);
+  *blob = h;
+  *blob_size = b.size;
+  return CPSZ_OK;
+}
+
+int cpsz_b200_compress_2d_offline_f32_into(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2,
+                                           double max_pwr_eb, unsigned char* out, size_t out_cap, size_t* blob_size) {
+  if (!out || !blob_size) return set_error(CPSZ_ERR_INVALID, "null output pointer");
+  RESOLVE(ctx);
+  Blob2D b;
+  CPSZ_TRY(compress_2d(ctx, U, V, r1, r2, max_pwr_eb, &b, nullptr));
+  *blob_size = b.size;
+  if (b.size > out_cap) return set_error(CPSZ_ERR_INVALID, "output capacity %zu < blob size %zu", out_cap, b.size);
+  CPSZ_TRY(copy_out(ctx, out, b.d_blob, b.size));
+  CPSZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return CPSZ_OK;
+}
+
+int cpsz_b200_decompress_2d_offline_f32(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_size, size_t r1,
+                                        size_t r2, float* U, float* V) {
+  RESOLVE(ctx);
+  CPSZ_TRY(decompress_2d(ctx, blob, blob_size, r1, r2, U, V));
+  CPSZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return CPSZ_OK;
+}
+
+int cpsz_b200_compress_2d_stages(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2,
+                                 double max_pwr_eb, int32_t* ids, int32_t* codes_u, int32_t* codes_v, float* recon_u,
+                                 float* recon_v, size_t* n_unpred) {
+  RESOLVE(ctx);
+  const size_t N = r1 * r2;
+  if (N == 0) return set_error(CPSZ_ERR_INVALID, "empty field");
+  // taps are separate device buffers so the product path's arena layout is untouched
+  uint8_t* d_ids = nullptr;
+  uint16_t* d_codes = nullptr;
+  float* d_recon = nullptr;
+  CPSZ_CUDA_TRY(cudaMalloc((void**)&d_ids, 2 * N + 16));
+  CPSZ_CUDA_TRY(cudaMalloc((void**)&d_codes, 4 * N + 16));
+  CPSZ_CUDA_TRY(cudaMalloc((void**)&d_recon, 8 * N + 16));
+  StageTap tap;
+  tap.ids = d_ids;
+  tap.codes_blocks[0] = d_codes;
+  tap.codes_blocks[1] = d_codes + N;
+  tap.recon[0] = d_recon;
+  tap.recon[1] = d_recon + N;
+  Blob2D b;
+  int rc = compress_2d(ctx, U, V, r1, r2, max_pwr_eb, &b, &tap);
+  if (rc == CPSZ_OK) {
+    std::vector<uint8_t> hid(2 * N);
+    std::vector<uint16_t> hc(2 * N);
+    std::vector<float> hr(2 * N);
+    cudaError_t e = cudaMemcpyAsync(hid.data(), d_ids, 2 * N, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hc.data(), d_codes, 4 * N, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hr.data(), d_recon, 8 * N, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+      rc = set_error(CPSZ_ERR_CUDA, "stage download: %s", cudaGetErrorString(e));
+    } else {
+      if (ids)
+        for (size_t i = 0; i < 2 * N; i++) ids[i] = (hid[i] == ID_ZERO) ? 0 : (int32_t)hid[i];
+      if (codes_u)
+        for (size_t i = 0; i < N; i++) codes_u[i] = hc[i];
+      if (codes_v)
+        for (size_t i = 0; i < N; i++) codes_v[i] = hc[N + i];
+      if (recon_u) memcpy(recon_u, hr.data(), 4 * N);
+      if (recon_v) memcpy(recon_v, hr.data() + N, 4 * N);
+      if (n_unpred) {
+        n_unpred[0] = b.n_unpred[0];
+        n_unpred[1] = b.n_unpred[1];
+      }
+    }
+  }
+  cudaFree(d_ids);
+  cudaFree(d_codes);
+  cudaFree(d_recon);
+  return rc;
+}
+
+int cpsz_b200_debug_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2, double max_pwr_eb,
+                         double* eb_out, uint8_t* id_codes) {
+  RESOLVE(ctx);
+  const size_t N = r1 * r2;
+  const QuantTable& qt = quant_table_2d();
+  float *dU = nullptr, *dV = nullptr;
+  double *deb = nullptr, *dtab = nullptr;
+  uint8_t* dids = nullptr;
+  unsigned long long* dh = nullptr;
+  CPSZ_CUDA_TRY(cudaMalloc((void**)&dU, 4 * N));
+  CPSZ_CUDA_TRY(cudaMalloc((void**)&dV, 4 * N));
+  CPSZ_CUDA_TRY(cudaMalloc((void**)&deb, 8 * N));
+  CPSZ_CUDA_TRY(cudaMalloc((void**)&dids, 2 * N));
+  CPSZ_CUDA_TRY(cudaMalloc((void**)&dtab, QUANT_TAB_MAX * 8));
+  CPSZ_CUDA_TRY(cudaMalloc((void**)&dh, 256 * 8));
+  cudaMemcpy(dU, U, 4 * N, cudaMemcpyHostToDevice);
+  cudaMemcpy(dV, V, 4 * N, cudaMemcpyHostToDevice);
+  cudaMemcpy(dtab, qt.t, QUANT_TAB_MAX * 8, cudaMemcpyHostToDevice);
+  cudaMemset(dh, 0, 256 * 8);
+  int rc = launch_eb2d(ctx, dU, dV, (int)r1, (int)r2, max_pwr_eb, dtab, qt.n, dids, dids + N, dh, deb);
+  cudaStreamSynchronize(ctx->stream);
+  if (rc == CPSZ_OK) {
+    if (eb_out) cudaMemcpy(eb_out, deb, 8 * N, cudaMemcpyDeviceToHost);
+    if (id_codes) cudaMemcpy(id_codes, dids, 2 * N, cudaMemcpyDeviceToHost);
+  }
+  cudaFree(dU);
+  cudaFree(dV);
+  cudaFree(deb);
+  cudaFree(dids);
+  cudaFree(dtab);
+  cudaFree(dh);
+  return rc;
+}
+
+int cpsz_b200_debug_quant_table(int which, double* t, int* n) {
+  const QuantTable& q = which == 3 ? quant_table_3d() : quant_table_2d();
+  if (t) memcpy(t, q.t, sizeof(q.t));
+  if (n) *n = q.n;
+  return CPSZ_OK;
+}
+
+size_t cpsz_b200_blob_size_2d(const unsigned char* blob) {
+  if (!blob) return 0;
+  unsigned long long s[3];
+  memcpy(s, blob + 12, 24);
+  return 36 + (size_t)s[0] + (size_t)s[1] + (size_t)s[2];
+}
+
+int cpsz_b200_zstd_compress(const unsigned char* data, size_t n, int level, unsigned char** out, size_t* out_size) {
+  if (!out || !out_size || (!data && n)) return set_error(CPSZ_ERR_INVALID, "null pointer");
+  size_t cap = ZSTD_compressBound(n);
+  unsigned char* o = (unsigned char*)malloc(cap ? cap : 1);
+  if (!o) return set_error(CPSZ_ERR_NOMEM, "zstd output");
+  size_t r = ZSTD_compress(o, cap, data, n, level);
+  if (ZSTD_isError(r)) {
+    free(o);
+    return set_error(CPSZ_ERR_INVALID, "ZSTD_compress: %s", ZSTD_getErrorName(r));
+  }
+  *out = o;
+  *out_size = r;
+  return CPSZ_OK;
+}
+
+int cpsz_b200_zstd_decompress(const unsigned char* data, size_t n, unsigned char* out, size_t out_size) {
+  size_t r = ZSTD_decompress(out, out_size, data, n);
+  if (ZSTD_isError(r)) return set_error(CPSZ_ERR_FORMAT, "ZSTD_decompress: %s", ZSTD_getErrorName(r));
+  if (r != out_size) return set_error(CPSZ_ERR_FORMAT, "ZSTD_decompress: %zu bytes, expected %zu", r, out_size);
+  return CPSZ_OK;
+}
+
+}  // extern "C"
+
+// ---- C++ drop-ins with the reference's template signatures ---------------------
+
+template <typename T>
+unsigned char* sz_compress_cp_preserve_2d_offline(const T* U, const T* V, size_t r1, size_t r2,
+                                                  size_t& compressed_size, bool transpose, double max_pwr_eb) {
+  (void)transpose;  // ignored by the reference as well
+  compressed_size = 0;
+  if (sizeof(T) != sizeof(float)) {
+    set_error(CPSZ_ERR_UNSUPPORTED, "only float fields are supported on the GPU path");
+    return nullptr;
+  }
+  unsigned char* blob = nullptr;
+  size_t size = 0;
+  if (cpsz_b200_compress_2d_offline_f32(nullptr, (const float*)U, (const float*)V, r1, r2, max_pwr_eb, &blob, &size) !=
+      CPSZ_OK)
+    return nullptr;
+  compressed_size = size;
+  return blob;
+}
+
+template <typename T>
+void sz_decompress_cp_preserve_2d_offline(const unsigned char* compressed, size_t r1, size_t r2, T*& U, T*& V) {
+  if (U) free(U);
+  if (V) free(V);
+  U = nullptr;
+  V = nullptr;
+  if (sizeof(T) != sizeof(float)) {
+    set_error(CPSZ_ERR_UNSUPPORTED, "only float fields are supported on the GPU path");
+    return;
+  }
+  size_t n = r1 * r2;
+  T* u = (T*)malloc(n * sizeof(T));
+  T* v = (T*)malloc(n * sizeof(T));
+  if (!u || !v) {
+    free(u);
+    free(v);
+    set_error(CPSZ_ERR_NOMEM, "output fields");
+    return;
+  }
+  // The reference reads the blob without a length; the sections it names bound it.
+  size_t blob_size = cpsz_b200_blob_size_2d(compressed);
+  if (cpsz_b200_decompress_2d_offline_f32(nullptr, compressed, blob_size, r1, r2, (float*)u, (float*)v) != CPSZ_OK) {
+    free(u);
+    free(v);
+    return;
+  }
+  U = u;
+  V = v;
+}
+
+template unsigned char* sz_compress_cp_preserve_2d_offline<float>(const float*, const float*, size_t, size_t, size_t&,
+                                                                  bool, double);
+template unsigned char* sz_compress_cp_preserve_2d_offline<double>(const double*, const double*, size_t, size_t,
+                                                                   size_t&, bool, double);
+template void sz_decompress_cp_preserve_2d_offline<float>(const unsigned char*, size_t, size_t, float*&, float*&);
+template void sz_decompress_cp_preserve_2d_offline<double>(const unsigned char*, size_t, size_t, double*&, double*&);

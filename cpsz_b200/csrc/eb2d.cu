@@ -1,0 +1,134 @@
+// eb2d.cu -- 2D offline error-bound derivation fused with its exponential
+// quantization and the id histogram.
+//
+// One CTA owns a TY x TX tile of vertices.  It stages the (TY+2) x (TX+2)
+// vertex halo of U and V in shared memory (coalesced row loads), evaluates
+// both triangles of every one of the (TY+1) x (TX+1) cells that touch the tile
+// once (FP64, bit-exact to src/sz_compress_cp_preserve_2d.cpp:125-172), keeps
+// the per-triangle bounds in shared memory, and then reduces the six incident
+// triangles of each vertex in the reference's traversal order (:195-218).
+// The vertex bound is quantized for U and V against host-computed thresholds
+// (base 4, thr = 2^-52; include/sz_cp_preserve_utils.hpp:14-22, applied at
+// src/sz_compress_cp_preserve_2d.cpp:226-244) and written as one byte per
+// component: the id, or 255 when the bound is <= thr (precision 0, Huffman
+// symbol 0).  A shared-memory histogram of the Huffman symbols is folded into
+// a global one.
+#include "eb_math.cuh"
+#include "kernels.h"
+
+namespace cpsz {
+
+namespace {
+constexpr int TX = 32;
+constexpr int TY = 16;
+constexpr int NT = 256;
+constexpr int CX = TX + 1;  // cells per tile row
+constexpr int CY = TY + 1;
+}  // namespace
+
+__global__ void __launch_bounds__(NT) eb2d_kernel(const float* __restrict__ U, const float* __restrict__ V, int r1,
+                                                  int r2, double max_pwr_eb, const double* __restrict__ thr_tab,
+                                                  int thr_n, uint8_t* __restrict__ ids_u, uint8_t* __restrict__ ids_v,
+                                                  unsigned long long* __restrict__ hist, int* __restrict__ flag,
+                                                  double* __restrict__ eb_out) {
+  __shared__ float su[TY + 2][TX + 3];
+  __shared__ float sv[TY + 2][TX + 3];
+  __shared__ double tri[2][CY][CX];
+  __shared__ double tab[QUANT_TAB_MAX];
+  __shared__ unsigned int shist[256];
+
+  const int tid = threadIdx.x;
+  const int i0 = blockIdx.y * TY, j0 = blockIdx.x * TX;
+  for (int k = tid; k < 256; k += NT) shist[k] = 0;
+  for (int k = tid; k < thr_n; k += NT) tab[k] = thr_tab[k];
+  // vertex halo: rows i0-1 .. i0+TY, cols j0-1 .. j0+TX
+  for (int k = tid; k < (TY + 2) * (TX + 2); k += NT) {
+    int a = k / (TX + 2), b = k % (TX + 2);
+    int gi = i0 - 1 + a, gj = j0 - 1 + b;
+    float u = 0.f, v = 0.f;
+    if (gi >= 0 && gi < r1 && gj >= 0 && gj < r2) {
+      size_t g = (size_t)gi * r2 + gj;
+      u = U[g];
+      v = V[g];
+    }
+    su[a][b] = u;
+    sv[a][b] = v;
+  }
+  __syncthreads();
+  // cells (ci, cj) = (i0-1+a, j0-1+b), a in [0, CY), b in [0, CX)
+  for (int k = tid; k < CY * CX; k += NT) {
+    int a = k / CX, b = k % CX;
+    int ci = i0 - 1 + a, cj = j0 - 1 + b;
+    double e0 = 0, e1 = 0;
+    if (ci >= 0 && ci < r1 - 1 && cj >= 0 && cj < r2 - 1) {
+      // upper: offsets {0, r2, r2+1} -> (a,b), (a+1,b), (a+1,b+1)
+      e0 = dev::tri_eb(su[a][b], su[a + 1][b], su[a + 1][b + 1], sv[a][b], sv[a + 1][b], sv[a + 1][b + 1], 0);
+      // lower: offsets {0, 1, r2+1} -> (a,b), (a,b+1), (a+1,b+1)
+      e1 = dev::tri_eb(su[a][b], su[a][b + 1], su[a + 1][b + 1], sv[a][b], sv[a][b + 1], sv[a + 1][b + 1], 1);
+    }
+    tri[0][a][b] = e0;
+    tri[1][a][b] = e1;
+  }
+  __syncthreads();
+  const double thr = tab[0];
+  for (int k = tid; k < TY * TX; k += NT) {
+    int a = k / TX, b = k % TX;
+    int gi = i0 + a, gj = j0 + b;
+    if (gi >= r1 || gj >= r2) continue;
+    // vertex (gi, gj) is local (a+1, b+1); cell (gi-1+x, gj-1+y) is tri[.][a+x][b+y]
+    double eb = max_pwr_eb;
+    bool up = gi >= 1, left = gj >= 1, down = gi < r1 - 1, right = gj < r2 - 1;
+    if (up && left) {
+      eb = dev::minf_d(eb, tri[0][a][b]);
+      eb = dev::minf_d(eb, tri[1][a][b]);
+    }
+    if (up && right) eb = dev::minf_d(eb, tri[0][a][b + 1]);
+    if (down && left) eb = dev::minf_d(eb, tri[1][a + 1][b]);
+    if (down && right) {
+      eb = dev::minf_d(eb, tri[0][a + 1][b + 1]);
+      eb = dev::minf_d(eb, tri[1][a + 1][b + 1]);
+    }
+    float uu = su[a + 1][b + 1], vv = sv[a + 1][b + 1];
+    uint8_t code[2];
+    int sym[2];
+    double ev[2] = {(double)fabsf(uu) * eb, (double)fabsf(vv) * eb};
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+      double e = ev[c];
+      if (e <= thr) {
+        code[c] = ID_ZERO;
+        sym[c] = 0;
+      } else {
+        int ex = (int)((__double_as_longlong(e) >> 52) & 0x7ff) - 1023;
+        int id = dev::count_thresholds(tab, thr_n, e, (ex + 52) >> 1);
+        if (id >= ID_ZERO) {
+          atomicOr(flag, FLAG_ID_OVERFLOW);
+          id = ID_ZERO - 1;
+        }
+        code[c] = (uint8_t)id;
+        sym[c] = id;
+      }
+    }
+    size_t g = (size_t)gi * r2 + gj;
+    if (eb_out) eb_out[g] = eb;
+    ids_u[g] = code[0];
+    ids_v[g] = code[1];
+    atomicAdd(&shist[sym[0]], 1u);
+    atomicAdd(&shist[sym[1]], 1u);
+  }
+  __syncthreads();
+  for (int k = tid; k < 256; k += NT)
+    if (shist[k]) atomicAdd(&hist[k], (unsigned long long)shist[k]);
+}
+
+int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, double max_pwr_eb,
+                const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
+                double* eb_out) {
+  dim3 grid((r2 + TX - 1) / TX, (r1 + TY - 1) / TY);
+  eb2d_kernel<<<grid, NT, 0, ctx->stream>>>(U, V, r1, r2, max_pwr_eb, d_thr_tab, thr_n, ids_u, ids_v, hist,
+                                            ctx->d_flag, eb_out);
+  count_launch(ctx);
+  return check_launch("eb2d_kernel");
+}
+
+}  // namespace cpsz

@@ -1,0 +1,246 @@
+// eb_math.cuh -- per-simplex critical-point-preserving error bounds, device side.
+//
+// These functions reproduce the reference's CPU arithmetic bit for bit; the
+// translation unit that includes them is compiled with -fmad=false so that no
+// product is fused into a following sum.  Operand types follow the reference
+// exactly: float*float products stay float and are widened to double, sums
+// run left to right in the declared type, sqrt and division are IEEE
+// round-to-nearest (CUDA's default for double, and for float without
+// -use_fast_math).  MINF(a,b) = (a<b)?a:b and MAX(a,b) = (a>b)?a:b keep their
+// NaN behaviour.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace cpsz {
+namespace dev {
+
+__device__ __forceinline__ double minf_d(double a, double b) { return (a < b) ? a : b; }
+__device__ __forceinline__ double max_d(double a, double b) { return (a > b) ? a : b; }
+
+// accumulate(): include/sz_cp_preserve_utils.hpp:194-198
+__device__ __forceinline__ void acc(double v, double& p, double& n) {
+  if (v >= 0) p += v;
+  else n += -v;
+}
+
+// max_eb_to_keep_sign, degree 1 / 2: include/sz_cp_preserve_utils.hpp:61-92
+__device__ __forceinline__ double keep_sign1(double P, double N) {
+  if ((N == 0) || (P == 0)) return 1;
+  return fabs(P - N) / (P + N);
+}
+__device__ __forceinline__ double keep_sign2(double positive, double negative) {
+  if ((negative == 0) || (positive == 0)) return 1;
+  double P = sqrt(positive), N = sqrt(negative);
+  return fabs(P - N) / (P + N);
+}
+
+// max_eb_to_keep_sign_2d_offline_2 / _4 (T = double):
+// src/sz_compress_cp_preserve_2d.cpp:31-49
+__device__ __forceinline__ double off2(double a, double b) {
+  double p = 0, n = 0;
+  acc(a, p, n);
+  acc(b, p, n);
+  return keep_sign2(p, n);
+}
+__device__ __forceinline__ double off4(double a, double b, double c, double d) {
+  double p = 0, n = 0;
+  acc(a, p, n);
+  acc(b, p, n);
+  acc(c, p, n);
+  acc(d, p, n);
+  return keep_sign2(p, n);
+}
+
+// max_eb_to_keep_sign_det2x2<float>: src/sz_compress_cp_preserve_2d.cpp:18-29
+__device__ __forceinline__ double keep_sign_det2x2(float u0, float u1, float u2, float v0, float v1, float v2) {
+  double p = 0, n = 0;
+  acc((double)(u0 * v1), p, n);
+  acc((double)(-u0 * v2), p, n);
+  acc((double)(u1 * v2), p, n);
+  acc((double)(-u1 * v0), p, n);
+  acc((double)(u2 * v0), p, n);
+  acc((double)(-u2 * v1), p, n);
+  return keep_sign2(p, n);
+}
+
+// max_eb_to_keep_sign_eigen_delta_2<float>: src/sz_compress_cp_preserve_2d.cpp:79-123.
+// The triangle coordinates are compile-time constants of the two triangle
+// kinds; the adjugate entries c[] are passed precomputed (float, exactly as
+// get_adjugate_matrix_for_position produces them, including signed zeros).
+__device__ __noinline__ double keep_sign_eigen(float u0, float u1, float u2, float v0, float v1, float v2, float c0,
+                                               float c1, float c2, float c3) {
+  double eb;
+  {
+    double p = 0, n = 0;
+    acc((double)(c0 * u0), p, n);
+    acc((double)(c1 * u1), p, n);
+    acc((double)(-(c0 + c1) * u2), p, n);
+    acc((double)(c2 * v0), p, n);
+    acc((double)(c3 * v1), p, n);
+    acc((double)(-(c2 + c3) * v2), p, n);
+    eb = keep_sign1(p, n);
+    eb = minf_d(eb, keep_sign_det2x2(u0, u1, u2, v0, v1, v2));
+  }
+  float m = c1 * c2 - c0 * c3;
+  float C = (-m) * (u0 * v1 - u0 * v2 + u1 * v2 - u1 * v0 + u2 * v0 - u2 * v1);
+  if (C == 0) return 0;
+  if (C < 0) return eb;
+  float co[6];
+  co[0] = c0 * u0;
+  co[1] = c1 * u1;
+  co[2] = -(c1 + c0) * u2;
+  co[3] = c2 * v0;
+  co[4] = c3 * v1;
+  co[5] = -(c3 + c2) * v2;
+  double p = 0, n = 0;
+#pragma unroll
+  for (int i = 0; i < 6; i++)
+#pragma unroll
+    for (int j = 0; j < 6; j++) acc((double)(co[i] * co[j]), p, n);
+  acc((double)(-4 * m * u1 * v0), p, n);
+  acc((double)(4 * m * u2 * v0), p, n);
+  acc((double)(4 * m * u0 * v1), p, n);
+  acc((double)(-4 * m * u2 * v1), p, n);
+  acc((double)(-4 * m * u0 * v2), p, n);
+  acc((double)(4 * m * u1 * v2), p, n);
+  return minf_d(eb, keep_sign2(p, n));
+}
+
+// Adjugate of the triangle coordinate matrix (get_adjugate_matrix_for_position,
+// src/sz_compress_cp_preserve_2d.cpp:55-63) for the reversed coordinates the
+// offline loop passes (:204-206), evaluated in float.
+__device__ __forceinline__ void adjugate(float x0, float x1, float x2, float y0, float y1, float y2, float c[4]) {
+  float det = (x0 - x2) * (y1 - y2) - (x1 - x2) * (y0 - y2);
+  c[0] = (y1 - y2) / det;
+  c[1] = -(y0 - y2) / det;
+  c[2] = -(x1 - x2) / det;
+  c[3] = (x0 - x2) / det;
+}
+
+// max_eb_to_keep_position_and_type<float>: src/sz_compress_cp_preserve_2d.cpp:125-172.
+// kind 0 = "upper" triangle X = {{0,0},{1,0},{1,1}}, kind 1 = "lower"
+// X = {{0,0},{0,1},{1,1}}, passed as x = X[.][1], y = X[.][0].
+__device__ __forceinline__ double tri_eb(float u0, float u1, float u2, float v0, float v1, float v2, int kind) {
+  double u0v1 = (double)(u0 * v1);
+  double u1v0 = (double)(u1 * v0);
+  double u0v2 = (double)(u0 * v2);
+  double u2v0 = (double)(u2 * v0);
+  double u1v2 = (double)(u1 * v2);
+  double u2v1 = (double)(u2 * v1);
+  double det = u0v1 - u1v0 + u1v2 - u2v1 + u2v0 - u0v2;
+  double eb = 0;
+  if (det != 0) {
+    bool f1 = (det / (u2v0 - u0v2) >= 1);
+    bool f2 = (det / (u1v2 - u2v1) >= 1);
+    bool f3 = (det / (u0v1 - u1v0) >= 1);
+    if (f1 && f2 && f3) {
+      double eb1 = minf_d(off2(u2v0, -u0v2), off4(u0v1, -u1v0, u1v2, -u2v1));
+      double eb2 = minf_d(off2(u1v2, -u2v1), off4(u0v1, -u1v0, u2v0, -u0v2));
+      double eb3 = minf_d(off2(u0v1, -u1v0), off4(u1v2, -u2v1, u2v0, -u0v2));
+      float c[4];
+      if (kind == 0) adjugate(0.f, 0.f, 1.f, 0.f, 1.f, 1.f, c);
+      else adjugate(0.f, 1.f, 1.f, 0.f, 0.f, 1.f, c);
+      double eb4 = minf_d(eb3, keep_sign_eigen(u0, u1, u2, v0, v1, v2, c[0], c[1], c[2], c[3]));
+      eb = minf_d(eb1, eb2);
+      eb = minf_d(eb, eb4);
+    } else {
+      eb = 0;
+      if (!f1) eb = max_d(eb, minf_d(off2(u2v0, -u0v2), off4(u0v1, -u1v0, u1v2, -u2v1)));
+      if (!f2) eb = max_d(eb, minf_d(off2(u1v2, -u2v1), off4(u0v1, -u1v0, u2v0, -u0v2)));
+      if (!f3) eb = max_d(eb, minf_d(off2(u0v1, -u1v0), off4(u1v2, -u2v1, u2v0, -u0v2)));
+    }
+  }
+  return eb;
+}
+
+// ---- 3D (src/sz_compress_cp_preserve_3d.cpp:266-358) --------------------------
+
+// acbrt1: include/sz_cp_preserve_utils.hpp:173-184 (the reference's own
+// bit-level initial guess and two float Newton steps).
+__device__ __forceinline__ float acbrt1(float x0) {
+  int ix = __float_as_int(x0);
+  ix = ix / 4 + ix / 16;
+  ix = ix + ix / 16;
+  ix = ix + ix / 256;
+  ix = 0x2a5137a0 + ix;
+  float x = __int_as_float(ix);
+  x = 0.33333333f * (2.0f * x + x0 / (x * x));
+  x = 0.33333333f * (2.0f * x + x0 / (x * x));
+  return x;
+}
+
+__device__ __forceinline__ float keep_sign_3d(float positive, float negative) {
+  if (positive == 0 && negative == 0) return 0;
+  float P = acbrt1(positive), N = acbrt1(negative);
+  return fabsf(P - N) / (P + N);
+}
+
+__device__ __forceinline__ int sgnf(float v) { return (0.0f < v) - (v < 0.0f); }
+__device__ __forceinline__ bool same_direction(float a, float b, float c, float d) {
+  int s = sgnf(a);
+  if (s == 0) return false;
+  return (s == sgnf(b)) && (s == sgnf(c)) && (s == sgnf(d));
+}
+
+__device__ __forceinline__ float maxf_(float a, float b) { return (a > b) ? a : b; }
+__device__ __forceinline__ float minf_(float a, float b) { return (a < b) ? a : b; }
+
+__device__ __noinline__ double tet_eb(float u0, float u1, float u2, float u3, float v0, float v1, float v2, float v3,
+                                      float w0, float w1, float w2, float w3) {
+  double u3v1w2 = u3 * v1 * w2, u3v2w1 = u3 * v2 * w1, u3v2w0 = u3 * v2 * w0, u3v0w2 = u3 * v0 * w2,
+         u3v0w1 = u3 * v0 * w1, u3v1w0 = u3 * v1 * w0;
+  double u1v3w2 = u1 * v3 * w2, u2v3w1 = u2 * v3 * w1, u2v3w0 = u2 * v3 * w0, u0v3w2 = u0 * v3 * w2,
+         u0v3w1 = u0 * v3 * w1, u1v3w0 = u1 * v3 * w0;
+  double u1v2w3 = u1 * v2 * w3, u2v1w3 = u2 * v1 * w3, u0v2w3 = u0 * v2 * w3, u2v0w3 = u2 * v0 * w3,
+         u0v1w3 = u0 * v1 * w3, u1v0w3 = u1 * v0 * w3;
+  double u0v1w2 = u0 * v1 * w2, u0v2w1 = u0 * v2 * w1, u1v2w0 = u1 * v2 * w0, u1v0w2 = u1 * v0 * w2,
+         u2v0w1 = u2 * v0 * w1, u2v1w0 = u2 * v1 * w0;
+  double u3_0 = -u3v1w2 + u3v2w1, u3_1 = -u3v2w0 + u3v0w2, u3_2 = -u3v0w1 + u3v1w0;
+  double v3_0 = u1v3w2 - u2v3w1, v3_1 = u2v3w0 - u0v3w2, v3_2 = u0v3w1 - u1v3w0;
+  double w3_0 = -u1v2w3 + u2v1w3, w3_1 = u0v2w3 - u2v0w3, w3_2 = -u0v1w3 + u1v0w3;
+  double c_4 = u0v1w2 - u0v2w1 + u1v2w0 - u1v0w2 + u2v0w1 - u2v1w0;
+  double M0 = u3_0 + v3_0 + w3_0;
+  double M1 = u3_1 + v3_1 + w3_1;
+  double M2 = u3_2 + v3_2 + w3_2;
+  double M3 = c_4;
+  double M = M0 + M1 + M2 + M3;
+  if (M == 0) return 0;
+  bool flag0 = (M0 == 0) || (M / M0 > 1);
+  bool flag1 = (M1 == 0) || (M / M1 > 1);
+  bool flag2 = (M2 == 0) || (M / M2 > 1);
+  bool flag3 = (M3 == 0) || (M / M3 > 1);
+  if (flag0 && flag1 && flag2 && flag3) {
+    if (same_direction(u0, u1, u2, u3) || same_direction(v0, v1, v2, v3) || same_direction(w0, w1, w2, w3)) return 1;
+    return 0;
+  }
+  float eb = 0;
+  double pm0 = 0, nm0 = 0, pm1 = 0, nm1 = 0, pm2 = 0, nm2 = 0, pm3 = 0, nm3 = 0;
+  acc(-u3v1w2, pm0, nm0); acc(u3v2w1, pm0, nm0); acc(u1v3w2, pm0, nm0);
+  acc(-u2v3w1, pm0, nm0); acc(-u1v2w3, pm0, nm0); acc(u2v1w3, pm0, nm0);
+  acc(-u3v2w0, pm1, nm1); acc(u3v0w2, pm1, nm1); acc(u2v3w0, pm1, nm1);
+  acc(-u0v3w2, pm1, nm1); acc(u0v2w3, pm1, nm1); acc(-u2v0w3, pm1, nm1);
+  acc(-u3v0w1, pm2, nm2); acc(u3v1w0, pm2, nm2); acc(u0v3w1, pm2, nm2);
+  acc(-u1v3w0, pm2, nm2); acc(-u0v1w3, pm2, nm2); acc(u1v0w3, pm2, nm2);
+  acc(u0v1w2, pm3, nm3); acc(-u0v2w1, pm3, nm3); acc(u1v2w0, pm3, nm3);
+  acc(-u1v0w2, pm3, nm3); acc(u2v0w1, pm3, nm3); acc(-u2v1w0, pm3, nm3);
+  float p_m0 = (float)pm0, p_m1 = (float)pm1, p_m2 = (float)pm2, p_m3 = (float)pm3;
+  float n_m0 = (float)nm0, n_m1 = (float)nm1, n_m2 = (float)nm2, n_m3 = (float)nm3;
+  if (!flag0) eb = maxf_(eb, minf_(keep_sign_3d(p_m0, n_m0), keep_sign_3d(p_m1 + p_m2 + p_m3, n_m1 + n_m2 + n_m3)));
+  if (!flag1) eb = maxf_(eb, minf_(keep_sign_3d(p_m1, n_m1), keep_sign_3d(p_m0 + p_m2 + p_m3, n_m0 + n_m2 + n_m3)));
+  if (!flag2) eb = maxf_(eb, minf_(keep_sign_3d(p_m2, n_m2), keep_sign_3d(p_m0 + p_m1 + p_m3, n_m0 + n_m1 + n_m3)));
+  if (!flag3) eb = maxf_(eb, minf_(keep_sign_3d(p_m3, n_m3), keep_sign_3d(p_m0 + p_m1 + p_m2, n_m0 + n_m1 + n_m2)));
+  return eb;
+}
+
+// Quantized-id lookup against host-computed thresholds t[1..n): the id is the
+// number of thresholds <= e.  `guess` starts near the answer; the loops fix it.
+__device__ __forceinline__ int count_thresholds(const double* t, int n, double e, int guess) {
+  int g = guess < 0 ? 0 : (guess > n - 1 ? n - 1 : guess);
+  while (g + 1 < n && e >= t[g + 1]) g++;
+  while (g > 0 && e < t[g]) g--;
+  return g;
+}
+
+}  // namespace dev
+}  // namespace cpsz

@@ -1,0 +1,410 @@
+// huffman.cu -- GPU side of the SZ-1.x Huffman codec used by the reference
+// (src/sz_huffman.cpp): symbol histograms, the MSB-first bit packer and a
+// self-synchronising parallel decoder.
+//
+// Encoder.  The reference's packer (encode, src/sz_huffman.cpp:217-320) emits
+// the MSB-first concatenation of the codes, zero padded to a byte.  Here a CTA
+// owns 4096 consecutive symbols: pass 1 sums code lengths per CTA, a scan gives
+// every CTA its starting bit, pass 2 re-reads the symbols, scans the lengths
+// inside the CTA, ORs the codes into a shared-memory word buffer aligned to
+// the global 32-bit word grid, and stores it with plain coalesced stores except
+// for the two edge words, which are shared with the neighbouring CTAs and use
+// atomicOr.  Words are stored byte-swapped so memory holds the big-endian byte
+// stream the reference writes.
+//
+// Decoder.  The reference stream has no chunk index, so decoding uses
+// self-synchronisation (after Weissenberger & Schmidt, ICPP 2018): the stream
+// is cut into S-bit subsequences, each thread first decodes its subsequence
+// from its nominal start (finding the codeword boundary at which it leaves),
+// then subsequences whose assumed start differs from their predecessor's exit
+// are re-decoded from that exit until nothing changes (prefix codes
+// resynchronise within a few codewords, so this settles in one or two
+// rounds), then counts are scanned and every thread decodes again, writing its
+// symbols.  Lookup is a 2^12-entry first-level table with a bit-serial tree
+// walk for longer codes.
+#include "kernels.h"
+
+namespace cpsz {
+
+namespace {
+
+constexpr int ENC_NT = 256;
+constexpr int ENC_PER_THREAD = 16;
+constexpr int ENC_PER_CTA = ENC_NT * ENC_PER_THREAD;
+
+__device__ __forceinline__ uint32_t bswap32(uint32_t x) { return __byte_perm(x, 0, 0x0123); }
+
+template <class Sym>
+__device__ __forceinline__ int sym_at(const Sym* s, size_t i, bool map_id_zero) {
+  int v = (int)s[i];
+  if (map_id_zero && v == ID_ZERO) v = 0;
+  return v;
+}
+
+template <class Sym>
+__global__ void __launch_bounds__(ENC_NT) enc_count_kernel(const Sym* __restrict__ sym, size_t n, bool map_id_zero,
+                                                           const uint8_t* __restrict__ len,
+                                                           unsigned long long* __restrict__ cta_bits) {
+  __shared__ unsigned int red[ENC_NT / 32];
+  size_t base = (size_t)blockIdx.x * ENC_PER_CTA;
+  unsigned int bits = 0;
+#pragma unroll 4
+  for (int k = 0; k < ENC_PER_THREAD; k++) {
+    size_t i = base + (size_t)k * ENC_NT + threadIdx.x;
+    if (i < n) bits += len[sym_at(sym, i, map_id_zero)];
+  }
+  for (int o = 16; o; o >>= 1) bits += __shfl_xor_sync(0xffffffffu, bits, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = bits;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0;
+    for (int w = 0; w < ENC_NT / 32; w++) t += red[w];
+    cta_bits[blockIdx.x] = t;
+  }
+}
+
+// Exclusive scan of the per-CTA bit counts (single CTA, sequential over chunks).
+__global__ void __launch_bounds__(1024) scan_u64_kernel(const unsigned long long* __restrict__ in,
+                                                        unsigned long long* __restrict__ out, size_t n) {
+  __shared__ unsigned long long warp_tot[32];
+  __shared__ unsigned long long carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (size_t base = 0; base < n; base += 1024) {
+    size_t i = base + threadIdx.x;
+    unsigned long long v = i < n ? in[i] : 0ull;
+    unsigned long long x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+      if ((threadIdx.x & 31) >= o) x += y;
+    }
+    if ((threadIdx.x & 31) == 31) warp_tot[threadIdx.x >> 5] = x;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      unsigned long long w = warp_tot[threadIdx.x];
+      for (int o = 1; o < 32; o <<= 1) {
+        unsigned long long y = __shfl_up_sync(0xffffffffu, w, o);
+        if (threadIdx.x >= o) w += y;
+      }
+      warp_tot[threadIdx.x] = w;
+    }
+    __syncthreads();
+    unsigned long long pre = carry + (threadIdx.x >= 32 ? warp_tot[(threadIdx.x >> 5) - 1] : 0ull) + x - v;
+    if (i < n) out[i] = pre;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry = pre + v;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[n] = carry;
+}
+
+template <class Sym>
+__global__ void __launch_bounds__(ENC_NT) enc_write_kernel(const Sym* __restrict__ sym, size_t n, bool map_id_zero,
+                                                           const unsigned long long* __restrict__ code,
+                                                           const uint8_t* __restrict__ len,
+                                                           const unsigned long long* __restrict__ cta_off,
+                                                           uint32_t* __restrict__ out, int max_len) {
+  extern __shared__ uint32_t sbuf[];
+  __shared__ unsigned int warp_tot[ENC_NT / 32];
+  const size_t base = (size_t)blockIdx.x * ENC_PER_CTA;
+  const unsigned long long start = cta_off[blockIdx.x];
+  const unsigned long long end = cta_off[blockIdx.x + 1];
+  if (start == end) return;
+  const int shift = (int)(start & 31);
+  const int nwords = (int)(((end - 1) >> 5) - (start >> 5) + 1);
+  for (int k = threadIdx.x; k < nwords; k += ENC_NT) sbuf[k] = 0;
+  // thread t owns symbols base + t*16 .. +15 (contiguous run for in-order packing)
+  const size_t my = base + (size_t)threadIdx.x * ENC_PER_THREAD;
+  int s_loc[ENC_PER_THREAD];
+  unsigned int bits = 0;
+#pragma unroll
+  for (int k = 0; k < ENC_PER_THREAD; k++) {
+    size_t i = my + k;
+    s_loc[k] = (i < n) ? sym_at(sym, i, map_id_zero) : -1;
+    if (s_loc[k] >= 0) bits += len[s_loc[k]];
+  }
+  unsigned int x = bits;
+  for (int o = 1; o < 32; o <<= 1) {
+    unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) >= o) x += y;
+  }
+  if ((threadIdx.x & 31) == 31) warp_tot[threadIdx.x >> 5] = x;
+  __syncthreads();
+  unsigned int pre = x - bits;
+  for (int w = 0; w < (int)(threadIdx.x >> 5); w++) pre += warp_tot[w];
+  unsigned int pos = (unsigned int)shift + pre;  // bit position inside sbuf
+#pragma unroll
+  for (int k = 0; k < ENC_PER_THREAD; k++) {
+    if (s_loc[k] < 0) break;
+    int l = len[s_loc[k]];
+    unsigned long long c = code[s_loc[k]];
+    while (l > 0) {
+      int wi = pos >> 5, off = pos & 31;
+      int room = 32 - off;
+      int take = l < room ? l : room;
+      uint32_t part = (uint32_t)((c >> (l - take)) & ((take == 32) ? 0xffffffffull : ((1ull << take) - 1)));
+      atomicOr(&sbuf[wi], part << (room - take));
+      pos += take;
+      l -= take;
+    }
+  }
+  __syncthreads();
+  const size_t w0 = start >> 5;
+  for (int k = threadIdx.x; k < nwords; k += ENC_NT) {
+    uint32_t v = bswap32(sbuf[k]);
+    if (k == 0 || k == nwords - 1) atomicOr(&out[w0 + k], v);
+    else out[w0 + k] = v;
+  }
+  (void)max_len;
+}
+
+template <class Sym>
+int encode_impl(cpsz_b200_ctx* ctx, const Sym* sym, size_t n, bool map_id_zero, HuffEncTable tab, uint32_t* out,
+                unsigned long long* d_total_bits, void* tmp) {
+  if (n == 0) return CPSZ_OK;
+  size_t nb = (n + ENC_PER_CTA - 1) / ENC_PER_CTA;
+  unsigned long long* cta_bits = (unsigned long long*)tmp;
+  unsigned long long* cta_off = cta_bits + align_up(nb, 32);
+  enc_count_kernel<Sym><<<(unsigned)nb, ENC_NT, 0, ctx->stream>>>(sym, n, map_id_zero, tab.len, cta_bits);
+  scan_u64_kernel<<<1, 1024, 0, ctx->stream>>>(cta_bits, cta_off, nb);
+  int max_len = 64;
+  size_t smem = ((size_t)ENC_PER_CTA * max_len) / 32 * 4 + 16;
+  // worst case is 32 KB of words for 64-bit codes
+  enc_write_kernel<Sym><<<(unsigned)nb, ENC_NT, smem, ctx->stream>>>(sym, n, map_id_zero, tab.code, tab.len,
+                                                                       cta_off, out, max_len);
+  if (d_total_bits)
+    cudaMemcpyAsync(d_total_bits, cta_off + nb, sizeof(unsigned long long), cudaMemcpyDeviceToDevice, ctx->stream);
+  count_launch(ctx, 3);
+  return check_launch("huffman encode");
+}
+
+// ---- histogram -------------------------------------------------------------------
+constexpr int HIST_NT = 512;
+constexpr int HIST_LO = 32768 - 4096;  // shared window of the code histogram
+constexpr int HIST_W = 8192;
+
+__global__ void __launch_bounds__(HIST_NT) hist_u16_kernel(const uint16_t* __restrict__ s, size_t n,
+                                                           unsigned long long* __restrict__ hist) {
+  __shared__ unsigned int sh[HIST_W + 1];  // window + symbol 0
+  for (int k = threadIdx.x; k <= HIST_W; k += HIST_NT) sh[k] = 0;
+  __syncthreads();
+  size_t stride = (size_t)gridDim.x * HIST_NT;
+  for (size_t i = (size_t)blockIdx.x * HIST_NT + threadIdx.x; i < n; i += stride) {
+    int v = s[i];
+    int w = v - HIST_LO;
+    if (v == 0) atomicAdd(&sh[HIST_W], 1u);
+    else if ((unsigned)w < (unsigned)HIST_W) atomicAdd(&sh[w], 1u);
+    else atomicAdd(&hist[v], 1ull);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < HIST_W; k += HIST_NT)
+    if (sh[k]) atomicAdd(&hist[HIST_LO + k], (unsigned long long)sh[k]);
+  if (threadIdx.x == 0 && sh[HIST_W]) atomicAdd(&hist[0], (unsigned long long)sh[HIST_W]);
+}
+
+// ---- decoder ---------------------------------------------------------------------
+constexpr int DEC_S = 1024;  // bits per subsequence
+constexpr int DEC_NT = 256;
+
+struct BitReader {
+  const uint32_t* w;  // big-endian words
+  __device__ __forceinline__ uint32_t peek32(unsigned long long pos) const {
+    size_t wi = pos >> 5;
+    uint32_t a = bswap32(__ldg(w + wi)), b = bswap32(__ldg(w + wi + 1));
+    return __funnelshift_l(b, a, (unsigned)(pos & 31));
+  }
+};
+
+// Decodes one symbol at `pos`; returns its length in bits (0 on a corrupt walk).
+__device__ __forceinline__ int decode_one(const BitReader& br, const uint32_t* lut, const HuffDecTable& T,
+                                          unsigned long long pos, uint32_t* sym) {
+  uint32_t p = br.peek32(pos);
+  uint32_t e = lut[p >> (32 - HUFF_LUT_BITS)];
+  if (!(e & 0x80)) {
+    *sym = e >> 8;
+    return (int)(e & 0x7f);
+  }
+  uint32_t node = e >> 8;
+  int l = HUFF_LUT_BITS;
+  while (l < 64) {
+    uint32_t bit = (br.peek32(pos + l) >> 31) & 1u;
+    node = T.child[2 * node + bit];
+    l++;
+    if (node == 0 || node >= (uint32_t)T.node_count) return 0;
+    if (T.leaf[node]) {
+      *sym = T.sym[node];
+      return l;
+    }
+  }
+  return 0;
+}
+
+__device__ __forceinline__ void load_lut(uint32_t* slut, const uint32_t* lut) {
+  for (int k = threadIdx.x; k < (1 << HUFF_LUT_BITS); k += blockDim.x) slut[k] = lut[k];
+  __syncthreads();
+}
+
+// Phase 1/2: decode subsequence t from start[t] (or nominal) to its limit, or
+// from the predecessor's exit when `resync` and that differs.
+__global__ void __launch_bounds__(DEC_NT) dec_scan_kernel(BitReader br, HuffDecTable T, unsigned long long nbits,
+                                                          int nsub, unsigned long long* __restrict__ start,
+                                                          unsigned long long* __restrict__ end,
+                                                          unsigned int* __restrict__ cnt, int resync,
+                                                          int* __restrict__ changed, int* flag) {
+  __shared__ uint32_t slut[1 << HUFF_LUT_BITS];
+  load_lut(slut, T.lut);
+  int t = blockIdx.x * DEC_NT + threadIdx.x;
+  if (t >= nsub) return;
+  unsigned long long s;
+  if (!resync) {
+    s = (unsigned long long)t * DEC_S;
+    start[t] = s;
+  } else {
+    if (t == 0) return;
+    s = end[t - 1];
+    if (s == start[t]) return;
+    start[t] = s;
+    *changed = 1;
+  }
+  unsigned long long lim = (unsigned long long)(t + 1) * DEC_S;
+  if (lim > nbits) lim = nbits;
+  unsigned long long pos = s;
+  unsigned int c = 0;
+  while (pos < lim) {
+    uint32_t sym;
+    int l = decode_one(br, slut, T, pos, &sym);
+    if (l == 0) {
+      // an unsynchronised start may run into invalid paths only on a corrupt stream
+      if (resync || t == 0) atomicOr(flag, FLAG_HUFF_CORRUPT);
+      pos = lim;
+      break;
+    }
+    pos += l;
+    c++;
+  }
+  end[t] = pos;
+  cnt[t] = c;
+}
+
+template <class Out>
+__global__ void __launch_bounds__(DEC_NT) dec_write_kernel(BitReader br, HuffDecTable T, unsigned long long nbits,
+                                                           int nsub, const unsigned long long* __restrict__ start,
+                                                           const unsigned long long* __restrict__ off,
+                                                           size_t n, Out* __restrict__ out) {
+  __shared__ uint32_t slut[1 << HUFF_LUT_BITS];
+  load_lut(slut, T.lut);
+  int t = blockIdx.x * DEC_NT + threadIdx.x;
+  if (t >= nsub) return;
+  unsigned long long lim = (unsigned long long)(t + 1) * DEC_S;
+  if (lim > nbits) lim = nbits;
+  unsigned long long pos = start[t];
+  unsigned long long o = off[t];
+  while (pos < lim && o < n) {
+    uint32_t sym;
+    int l = decode_one(br, slut, T, pos, &sym);
+    if (l == 0) break;
+    out[o++] = (Out)sym;
+    pos += l;
+  }
+}
+
+__global__ void fill_kernel_u8(uint8_t* out, size_t n, uint8_t v) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) out[i] = v;
+}
+__global__ void fill_kernel_u16(uint16_t* out, size_t n, uint16_t v) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) out[i] = v;
+}
+
+__global__ void u32_to_u64_kernel(const unsigned int* in, unsigned long long* out, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = in[i];
+}
+
+__global__ void check_total_kernel(const unsigned long long* off, int nsub, size_t n, int* flag) {
+  if (off[nsub] < n) atomicOr(flag, FLAG_HUFF_CORRUPT);
+}
+
+}  // namespace
+
+size_t huff_encode_tmp_bytes(size_t n) {
+  size_t nb = (n + ENC_PER_CTA - 1) / ENC_PER_CTA;
+  return (align_up(nb, 32) + nb + 1 + 32) * sizeof(unsigned long long);
+}
+
+int launch_huff_encode_u8(cpsz_b200_ctx* ctx, const uint8_t* sym, size_t n, bool map_id_zero, HuffEncTable tab,
+                          uint32_t* out_words, unsigned long long* d_total_bits, void* tmp) {
+  return encode_impl<uint8_t>(ctx, sym, n, map_id_zero, tab, out_words, d_total_bits, tmp);
+}
+
+int launch_huff_encode_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, HuffEncTable tab, uint32_t* out_words,
+                           unsigned long long* d_total_bits, void* tmp) {
+  return encode_impl<uint16_t>(ctx, sym, n, false, tab, out_words, d_total_bits, tmp);
+}
+
+int launch_hist_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, unsigned long long* hist) {
+  if (n == 0) return CPSZ_OK;
+  int grid = ctx->num_sms * 2;
+  size_t need = (n + HIST_NT - 1) / HIST_NT;
+  if ((size_t)grid > need) grid = (int)need;
+  hist_u16_kernel<<<grid, HIST_NT, 0, ctx->stream>>>(sym, n, hist);
+  count_launch(ctx);
+  return check_launch("hist_u16_kernel");
+}
+
+size_t huff_decode_tmp_bytes(size_t nbits) {
+  size_t nsub = (nbits + DEC_S - 1) / DEC_S + 1;
+  return align_up(nsub + 1, 32) * 8 * 3 + align_up(nsub + 1, 32) * 4 * 2 + 4096;
+}
+
+int launch_huff_decode(cpsz_b200_ctx* ctx, const uint8_t* bytes, size_t nbytes, size_t n, HuffDecTable tab, void* out,
+                       int out_bytes_per_sym, void* tmp) {
+  if (n == 0) return CPSZ_OK;
+  if (tab.root_is_leaf) {
+    unsigned grid = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 8);
+    if (out_bytes_per_sym == 1) fill_kernel_u8<<<grid, 256, 0, ctx->stream>>>((uint8_t*)out, n, (uint8_t)tab.root_sym);
+    else fill_kernel_u16<<<grid, 256, 0, ctx->stream>>>((uint16_t*)out, n, (uint16_t)tab.root_sym);
+    count_launch(ctx);
+    return check_launch("huffman fill");
+  }
+  unsigned long long nbits = (unsigned long long)nbytes * 8;
+  int nsub = (int)((nbits + DEC_S - 1) / DEC_S);
+  if (nsub == 0) return set_error(CPSZ_ERR_FORMAT, "empty Huffman stream for %zu symbols", n);
+  char* p = (char*)tmp;
+  size_t a = align_up((size_t)nsub + 1, 32);
+  unsigned long long* start = (unsigned long long*)p;
+  p += a * 8;
+  unsigned long long* end = (unsigned long long*)p;
+  p += a * 8;
+  unsigned long long* off = (unsigned long long*)p;
+  p += a * 8;
+  unsigned int* cnt = (unsigned int*)p;
+  p += a * 4;
+  int* changed = (int*)p;
+  BitReader br{(const uint32_t*)bytes};
+  unsigned grid = (unsigned)((nsub + DEC_NT - 1) / DEC_NT);
+  dec_scan_kernel<<<grid, DEC_NT, 0, ctx->stream>>>(br, tab, nbits, nsub, start, end, cnt, 0, changed, ctx->d_flag);
+  count_launch(ctx);
+  // resynchronisation rounds; each round fixes at least one more subsequence,
+  // in practice the first round already converges.
+  int* h_changed = (int*)ctx->pinned;
+  for (int round = 0; round < nsub; round++) {
+    cudaMemsetAsync(changed, 0, sizeof(int), ctx->stream);
+    dec_scan_kernel<<<grid, DEC_NT, 0, ctx->stream>>>(br, tab, nbits, nsub, start, end, cnt, 1, changed, ctx->d_flag);
+    count_launch(ctx);
+    cudaMemcpyAsync(h_changed, changed, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    CPSZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    if (!*h_changed) break;
+  }
+  unsigned long long* cnt64 = end;  // reuse: exits no longer needed after the final round
+  u32_to_u64_kernel<<<(nsub + 255) / 256, 256, 0, ctx->stream>>>(cnt, cnt64, nsub);
+  scan_u64_kernel<<<1, 1024, 0, ctx->stream>>>(cnt64, off, (size_t)nsub);
+  check_total_kernel<<<1, 1, 0, ctx->stream>>>(off, nsub, n, ctx->d_flag);
+  if (out_bytes_per_sym == 1)
+    dec_write_kernel<uint8_t><<<grid, DEC_NT, 0, ctx->stream>>>(br, tab, nbits, nsub, start, off, n, (uint8_t*)out);
+  else
+    dec_write_kernel<uint16_t><<<grid, DEC_NT, 0, ctx->stream>>>(br, tab, nbits, nsub, start, off, n, (uint16_t*)out);
+  count_launch(ctx, 4);
+  return check_launch("huffman decode");
+}
+
+}  // namespace cpsz

@@ -1,0 +1,111 @@
+// kernels.h -- launch wrappers of the device kernels (all on ctx->stream).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "runtime.h"
+
+namespace cpsz {
+
+constexpr int QUANT_TAB_MAX = QuantTable::kMax;
+// Byte code of a vertex whose quantized bound is zero (precision 0, Huffman symbol 0).
+constexpr uint8_t ID_ZERO = 255;
+
+// Device error flag bits (ctx->d_flag[0]).
+constexpr int FLAG_ID_OVERFLOW = 1;   // an error-bound id does not fit in a byte
+constexpr int FLAG_TIMEOUT = 2;       // a bounded inter-CTA wait gave up
+constexpr int FLAG_HUFF_CORRUPT = 4;  // a Huffman stream does not decode to the expected symbols
+constexpr int FLAG_RAW_RANGE = 8;     // an unpredictable-value index fell outside the stored list
+
+// ---- 2D error bounds ---------------------------------------------------------
+int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, double max_pwr_eb,
+                const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
+                double* eb_out = nullptr);
+
+// ---- 2D Lorenzo wavefront ------------------------------------------------------
+// One field of the wavefront.  Raster arrays carry their own row pitch (elements).
+struct WaveField {
+  const float* x;      // compress: original values; decompress: raw values scattered to raster
+  const uint8_t* ids;  // per-vertex id byte (compress: id or ID_ZERO; decompress: Huffman symbol)
+  uint16_t* codes;     // quantization codes, raster (compress: out, decompress: in)
+  float* out;          // compress: reconstruction (optional); decompress: decoded field
+  float* gbnd;         // last row of every 256-row group: ngroups * r2 floats
+  int* gprog;          // columns published per group (zeroed before launch)
+  long long x_pitch, id_pitch, code_pitch, out_pitch;
+  int r1, r2;
+};
+struct WaveItem {
+  int field;
+  int group;
+};
+constexpr int WAVE_WARPS = 8;
+constexpr int WAVE_GROUP_ROWS = WAVE_WARPS * 32;
+// Items must be ordered so that (field, g-1) precedes (field, g).
+int launch_wave2d(cpsz_b200_ctx* ctx, bool decompress, const WaveField* d_fields, const WaveItem* d_items,
+                  int n_items, int* d_queue, int max_ctas);
+
+// ---- block-order plumbing (12 x 12 blocks) ---------------------------------------
+// Raster (pitched) -> 12x12-block order, and back.  Histogram of the block-order
+// symbols (65536 bins) fused into the forward permutation.
+int launch_raster_to_blocks_u16(cpsz_b200_ctx* ctx, const uint16_t* raster, long long pitch, int r1, int r2,
+                                uint16_t* blocks, unsigned long long* hist);
+int launch_blocks_to_raster_u16(cpsz_b200_ctx* ctx, const uint16_t* blocks, int r1, int r2, uint16_t* raster,
+                                long long pitch);
+// Zero-code counts per row segment (one 12-wide block row) in block order,
+// exclusive-scanned into seg_off (size r1*nby+1; seg_off[r1*nby] = total).
+int launch_segment_scan(cpsz_b200_ctx* ctx, const uint16_t* codes_raster, long long pitch, int r1, int r2,
+                        unsigned int* seg_count, unsigned int* seg_off, void* scan_tmp);
+size_t segment_scan_tmp_bytes(int r1, int r2);
+// Compress: gather x at zero-code positions into block order (unpred list).
+int launch_gather_unpred(cpsz_b200_ctx* ctx, const uint16_t* codes_raster, long long pitch, const float* x,
+                         long long x_pitch, int r1, int r2, const unsigned int* seg_off, float* unpred);
+// Decompress: scatter the unpred list to raster positions of zero codes.
+int launch_scatter_unpred(cpsz_b200_ctx* ctx, const uint16_t* codes_raster, long long pitch, const float* unpred,
+                          unsigned long long n_unpred, int r1, int r2, const unsigned int* seg_off, float* x_raster,
+                          long long x_pitch);
+
+// ---- Huffman -------------------------------------------------------------------
+// Codebook for the encoder: per symbol, code right-aligned (bit len-1 = first bit).
+struct HuffEncTable {
+  const unsigned long long* code;
+  const uint8_t* len;
+  int nsym;
+};
+// Symbols: u8 (map 255 -> 0 when map_id_zero) or u16.  Output: MSB-first bit
+// stream, zero padded, written as bytes at out (device, zero-initialised for
+// ceil(bits/8) bytes rounded up to 4).
+size_t huff_encode_tmp_bytes(size_t n);
+int launch_huff_encode_u8(cpsz_b200_ctx* ctx, const uint8_t* sym, size_t n, bool map_id_zero, HuffEncTable tab,
+                          uint32_t* out_words, unsigned long long* d_total_bits, void* tmp);
+int launch_huff_encode_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, HuffEncTable tab,
+                           uint32_t* out_words, unsigned long long* d_total_bits, void* tmp);
+// Histograms (global, 64-bit bins).
+int launch_hist_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, unsigned long long* hist);
+
+// Decoder table: first-level lookup of HUFF_LUT_BITS bits; entries
+//   leaf:  (sym << 8) | len            (len in 1..HUFF_LUT_BITS)
+//   inner: 0x80 | (node << 8)          (walk the tree from `node` bit by bit)
+// Tree arrays: child[2*node + bit] (node index; leaves have t = 1 and sym in C).
+constexpr int HUFF_LUT_BITS = 12;
+struct HuffDecTable {
+  const uint32_t* lut;       // 1 << HUFF_LUT_BITS entries
+  const uint32_t* child;     // 2 * node_count
+  const uint32_t* sym;       // node_count (leaf symbol)
+  const uint8_t* leaf;       // node_count
+  int node_count;
+  int root_is_leaf;          // single-symbol stream (no bits)
+  uint32_t root_sym;
+};
+size_t huff_decode_tmp_bytes(size_t nbits);
+// Decodes exactly n symbols from a bit stream of nbits bits (words: big-endian
+// byte order, padded with >= 8 zero bytes).  Output u8 or u16.
+int launch_huff_decode(cpsz_b200_ctx* ctx, const uint8_t* bytes, size_t nbytes, size_t n, HuffDecTable tab,
+                       void* out, int out_bytes_per_sym, void* tmp);
+
+// ---- generic scans ----------------------------------------------------------------
+size_t scan_u32_tmp_bytes(size_t n);
+// Exclusive scan of n u32 values into out (n+1 entries, out[n] = total).
+int launch_scan_u32(cpsz_b200_ctx* ctx, const unsigned int* in, unsigned int* out, size_t n, void* tmp);
+
+}  // namespace cpsz

@@ -1,0 +1,41 @@
+// pipeline.h -- host orchestration entry points shared by the C ABI layer.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include "kernels.h"
+#include "runtime.h"
+
+namespace cpsz {
+
+// Result of a compression call: the blob lives in the context's arena until
+// the next call on the same context.
+struct Blob2D {
+  uint8_t* d_blob = nullptr;
+  size_t size = 0;
+  size_t n_unpred[2] = {0, 0};
+};
+
+// Optional device-side copies of intermediate stages (parity tests).
+struct StageTap {
+  uint8_t* ids = nullptr;                    // 2N id bytes (ID_ZERO = precision 0)
+  uint16_t* codes_blocks[2] = {nullptr, nullptr};
+  float* unpred[2] = {nullptr, nullptr};
+  float* recon[2] = {nullptr, nullptr};      // compressor-side reconstruction (raster)
+};
+
+int build_wave_items(int nfields, const int* r1s, std::vector<WaveItem>& items);
+
+int compress_2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2, double max_pwr_eb,
+                Blob2D* out, const StageTap* tap);
+int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_size, size_t r1, size_t r2, float* U,
+                  float* V);
+
+// Copies n bytes from device memory to `dst`, which may be host or device memory.
+int copy_out(cpsz_b200_ctx* ctx, void* dst, const void* d_src, size_t n);
+// Copies n bytes from `src` (host or device) into device memory `d_dst`.
+int copy_in(cpsz_b200_ctx* ctx, void* d_dst, const void* src, size_t n);
+
+}  // namespace cpsz

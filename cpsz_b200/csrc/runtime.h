@@ -1,0 +1,109 @@
+// runtime.h -- host-side runtime of libcpsz_b200: error reporting, per-call
+// device arena, pinned staging, launch accounting, and the host-computed
+// quantization tables shared by the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "cpsz_b200.h"
+
+namespace cpsz {
+
+// ---- errors ---------------------------------------------------------------
+int set_error(int code, const char* fmt, ...);
+void clear_error();
+
+struct Status {
+  int code = CPSZ_OK;
+  bool ok() const { return code == CPSZ_OK; }
+};
+
+#define CPSZ_CUDA_TRY(expr)                                                                         \
+  do {                                                                                              \
+    cudaError_t _e = (expr);                                                                        \
+    if (_e != cudaSuccess)                                                                          \
+      return ::cpsz::set_error(CPSZ_ERR_CUDA, "%s failed: %s (%s:%d)", #expr, cudaGetErrorString(_e), \
+                               __FILE__, __LINE__);                                                 \
+  } while (0)
+
+#define CPSZ_TRY(expr)           \
+  do {                           \
+    int _rc = (expr);            \
+    if (_rc != CPSZ_OK) return _rc; \
+  } while (0)
+
+// ---- quantization tables (computed on the host with glibc's log2) ----------
+// The reference quantizes an error bound e with
+//   id = (int)(log2(e / thr) / log2(base)),   e <= thr -> id 0 (precision 0)
+// (include/sz_cp_preserve_utils.hpp:14-22).  Because glibc's log2 is not
+// CUDA's, the kernels never call log2: for every id k >= 1 the host finds
+// the smallest double e with id(e) >= k by bisection over the ordered bit
+// patterns, calling the host log2 itself, and the kernels count thresholds.
+struct QuantTable {
+  static constexpr int kMax = 256;
+  double thr = 0;       // quantization threshold
+  int base = 0;         // 4 (2D) or 2 (3D)
+  int n = 0;            // thresholds t[1..n) valid; t[0] = thr (id >= 0 region starts above thr)
+  double t[kMax] = {};  // t[k] = smallest e with id(e) >= k
+};
+// 2D: base 4, thr = DBL_EPSILON, applied to e = |U| * eb.
+const QuantTable& quant_table_2d();
+// 3D: id of abs_eb = log2(1 + required_eb) with base 2, thr = FLT_EPSILON;
+// thresholds are over required_eb directly (log2(1+x) folded in).
+const QuantTable& quant_table_3d();
+
+// ---- context ----------------------------------------------------------------
+struct Arena {
+  char* base = nullptr;
+  size_t cap = 0;
+  size_t used = 0;
+};
+
+}  // namespace cpsz
+
+struct cpsz_b200_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t aux = nullptr;  // second stream for overlapping independent stages
+  cudaEvent_t ev[8] = {};
+  cpsz::Arena arena;
+  void* pinned = nullptr;
+  size_t pinned_cap = 0;
+  uint64_t launches = 0;
+  int num_sms = 0;
+  int* d_flag = nullptr;  // device error / timeout flag (persistent)
+  // optional per-stage timing of the last call (CUDA events on `stream`)
+  bool timing = false;
+  static constexpr int kMaxMarks = 24;
+  cudaEvent_t tev[kMaxMarks] = {};
+  const char* tname[kMaxMarks] = {};
+  int nmarks = 0;
+};
+
+namespace cpsz {
+
+cpsz_b200_ctx* resolve_ctx(cpsz_b200_ctx* ctx, int* rc);
+// Ensures the arena holds at least `bytes` and resets it for a new call.
+int arena_reserve(cpsz_b200_ctx* ctx, size_t bytes);
+// Bump allocation (256-byte aligned) from the reserved arena.
+void* arena_alloc(cpsz_b200_ctx* ctx, size_t bytes);
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+int pinned_reserve(cpsz_b200_ctx* ctx, size_t bytes);
+
+// Pointer kind: true if `p` is device (or managed) memory usable by kernels.
+bool is_device_ptr(const void* p);
+
+inline void count_launch(cpsz_b200_ctx* ctx, int n = 1) { ctx->launches += (uint64_t)n; }
+// Stage marks: when timing is on, records an event named `name` on the stream;
+// stage i spans marks i..i+1.  reset_marks() starts a new call.
+void reset_marks(cpsz_b200_ctx* ctx);
+void mark(cpsz_b200_ctx* ctx, const char* name);
+int check_launch(const char* what);
+
+}  // namespace cpsz

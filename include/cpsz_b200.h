@@ -1,0 +1,155 @@
+/* cpsz_b200.h -- C ABI of the B200-native cpSZ hot path (libcpsz_b200.so).
+ *
+ * Plain pointers and sizes only.  Every entry point returns a status code
+ * (CPSZ_OK = 0); cpsz_b200_last_error() gives the text of the calling thread's
+ * last failure.  Pointers documented as "host or device" may be either: the
+ * library inspects them with the CUDA runtime and copies host data in/out
+ * inside the call.  All GPU work runs on one device (the context's) on one
+ * stream per context; a context is not safe for concurrent use from several
+ * threads, distinct contexts are.  Passing ctx = NULL uses a per-thread default
+ * context on the current device.
+ *
+ * Blob formats are byte-for-byte those of the reference cpSZ (bzhan166/cpSZ):
+ * a blob written here decodes with the reference's decoders and vice versa.
+ * The 3 padding bytes of the reference's meanInfo<float> record (written
+ * uninitialised by the reference) are written as zero.
+ */
+#ifndef CPSZ_B200_H
+#define CPSZ_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  CPSZ_OK = 0,
+  CPSZ_ERR_INVALID = 1,     /* bad argument (null pointer, zero/oversized dimension, ...) */
+  CPSZ_ERR_CUDA = 2,        /* CUDA runtime / launch failure */
+  CPSZ_ERR_NOMEM = 3,       /* host or device allocation failed */
+  CPSZ_ERR_FORMAT = 4,      /* malformed or truncated blob */
+  CPSZ_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up */
+  CPSZ_ERR_UNSUPPORTED = 6, /* input outside what the format can represent */
+  CPSZ_ERR_NO_DEVICE = 7    /* no CUDA device visible */
+};
+
+typedef struct cpsz_b200_ctx cpsz_b200_ctx;
+
+/* Text of this thread's last error ("" if none). */
+const char* cpsz_b200_last_error(void);
+/* Library version (major*10000 + minor*100 + patch). */
+int cpsz_b200_version(void);
+
+/* Context: device workspace (grow-only arena), one CUDA stream, pinned staging. */
+int cpsz_b200_ctx_create(int device, cpsz_b200_ctx** ctx);
+int cpsz_b200_ctx_destroy(cpsz_b200_ctx* ctx);
+/* Number of kernels this context has launched so far (for launch accounting). */
+int cpsz_b200_ctx_kernel_launches(cpsz_b200_ctx* ctx, uint64_t* count);
+/* Stream of the context as an opaque handle (a cudaStream_t). */
+int cpsz_b200_ctx_stream(cpsz_b200_ctx* ctx, void** stream);
+/* Per-stage timing: when on, each call records CUDA events on the context's
+ * stream at its stage boundaries; cpsz_b200_ctx_stage_times() returns the
+ * last call's stages (name of the stage starting at each mark, duration in ms). */
+int cpsz_b200_ctx_set_timing(cpsz_b200_ctx* ctx, int on);
+int cpsz_b200_ctx_stage_times(cpsz_b200_ctx* ctx, int max_stages, const char** names, float* ms, int* n_stages);
+
+/* ---- 2D offline CP-preserving compression -------------------------------
+ * Replaces sz_compress_cp_preserve_2d_offline<float>
+ * (reference include/sz_compress_cp_preserve_2d.hpp:10,
+ *  src/sz_compress_cp_preserve_2d.cpp:175-274).
+ * U, V: r1 x r2 row-major float (host or device).  On success *blob is a
+ * malloc'd host buffer (caller free()s it) of *blob_size bytes. */
+int cpsz_b200_compress_2d_offline_f32(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2,
+                                      double max_pwr_eb, unsigned char** blob, size_t* blob_size);
+
+/* Same, writing the blob into caller memory out (host or device) of capacity
+ * out_cap; *blob_size receives the size (CPSZ_ERR_INVALID if out_cap is too
+ * small, with *blob_size set to the size needed). */
+int cpsz_b200_compress_2d_offline_f32_into(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2,
+                                           double max_pwr_eb, unsigned char* out, size_t out_cap, size_t* blob_size);
+
+/* Replaces sz_decompress_cp_preserve_2d_offline<float>
+ * (reference include/sz_decompress_cp_preserve_2d.hpp:11,
+ *  src/sz_decompress_cp_preserve_2d.cpp:8-52).
+ * blob: host memory of blob_size bytes.  U, V: caller-allocated r1*r2 floats
+ * (host or device). */
+int cpsz_b200_decompress_2d_offline_f32(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_size, size_t r1,
+                                        size_t r2, float* U, float* V);
+
+/* ---- 3D offline (log) CP-preserving compression -------------------------
+ * Replaces sz_compress_cp_preserve_3d_offline_log<float>
+ * (reference include/sz_compress_cp_preserve_3d.hpp:8,
+ *  src/sz_compress_cp_preserve_3d.cpp:360-581). */
+int cpsz_b200_compress_3d_offline_log_f32(cpsz_b200_ctx* ctx, const float* U, const float* V, const float* W,
+                                          size_t r1, size_t r2, size_t r3, double max_pwr_eb, unsigned char** blob,
+                                          size_t* blob_size);
+/* Replaces sz_decompress_cp_preserve_3d_online_log<float>
+ * (reference include/sz_decompress_cp_preserve_3d.hpp:11,
+ *  src/sz_decompress_cp_preserve_3d.cpp:7-110). */
+int cpsz_b200_decompress_3d_online_log_f32(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_size,
+                                           size_t r1, size_t r2, size_t r3, float* U, float* V, float* W);
+
+/* ---- stage-level entry point (parity tests, profiling) --------------------
+ * Runs the 2D offline compressor and copies out its intermediate streams
+ * (each output optional, host memory):
+ *   ids[2N]      the per-vertex quantized error-bound ids the reference
+ *                Huffman-codes (U ids then V ids; src/sz_compress_cp_preserve_2d.cpp:177-244)
+ *   codes_u/v[N] Lorenzo quantization codes in 12x12 block order
+ *                (include/sz_compress_block_processing.hpp:106-139)
+ *   recon_u/v[N] the compressor-side reconstruction (raster)
+ *   n_unpred[2]  unpredictable-value counts of U and V. */
+int cpsz_b200_compress_2d_stages(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2,
+                                 double max_pwr_eb, int32_t* ids, int32_t* codes_u, int32_t* codes_v, float* recon_u,
+                                 float* recon_v, size_t* n_unpred);
+
+/* Size of a 2D offline blob from its header (the reference's decoder takes
+ * no length; this lets a caller without one bound the read). */
+size_t cpsz_b200_blob_size_2d(const unsigned char* blob);
+
+/* ---- diagnostics (no reference counterpart) ---------------------------------
+ * The 2D bound kernel alone: per-vertex bound before quantization (eb_out, N
+ * doubles) and id bytes (id_codes, 2N; 255 = precision 0).  Host buffers. */
+int cpsz_b200_debug_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2,
+                         double max_pwr_eb, double* eb_out, uint8_t* id_codes);
+/* Host-computed quantization thresholds (which = 2 or 3): t[k] is the smallest
+ * bound with id >= k under the host libm's log2 (256 doubles). */
+int cpsz_b200_debug_quant_table(int which, double* t, int* n);
+
+/* ---- exact critical-point checker -----------------------------------------
+ * Per-cell CP classification with exact predicates (float products compared
+ * exactly, expansion arithmetic for Jacobian signs, Simulation of Simplicity
+ * on vertex index for ties).  Cell ids follow the reference's evaluation tool
+ * (test/cp_extraction_2d.cpp:117-147): cell 2*(i*(r2-1)+j)+k, k=0 triangle
+ * {(i,j),(i+1,j),(i+1,j+1)}, k=1 {(i,j),(i,j+1),(i+1,j+1)}.  Types as
+ * test/cp_extraction_2d.cpp:34-40 plus 1: 0 = no CP, 1+t for t in
+ * {SINGULAR, ATTRACTING, REPELLING, SADDLE, ATTRACTING_FOCUS, REPELLING_FOCUS,
+ * CENTER}.  cells_out (optional, host or device): 2*(r1-1)*(r2-1) bytes.
+ * counts[0..3] = {CPs in a, CPs in b, lost+spurious, type changed} when b != NULL. */
+int cpsz_b200_cp_check_2d(cpsz_b200_ctx* ctx, const float* Ua, const float* Va, const float* Ub, const float* Vb,
+                          size_t r1, size_t r2, uint8_t* cells_out, uint64_t counts[4]);
+/* 3D: 6 tets per cube (test/cp_extraction_3d.cpp:39-77 ordering), cell id
+ * 6*(cube index)+t; types 1+t for t in test/cp_extraction_3d.cpp:30-38. */
+int cpsz_b200_cp_check_3d(cpsz_b200_ctx* ctx, const float* Ua, const float* Va, const float* Wa, const float* Ub,
+                          const float* Vb, const float* Wb, size_t r1, size_t r2, size_t r3, uint8_t* cells_out,
+                          uint64_t counts[4]);
+
+/* ---- synthetic workloads (host) -------------------------------------------
+ * Seeded Gaussian-windowed linear-flow fields (no reference counterpart: the
+ * reference's dataset is not distributed).  Outputs are host arrays. */
+int cpsz_b200_generate_field_2d(uint64_t seed, size_t r1, size_t r2, int n_flows, double sigma, double noise_std,
+                                float* U, float* V);
+int cpsz_b200_generate_field_3d(uint64_t seed, size_t r1, size_t r2, size_t r3, int n_flows, double sigma,
+                                double noise_std, float* U, float* V, float* W);
+int cpsz_b200_batch_layout(uint64_t base_seed, int n_fields, int lo, int hi, size_t* r1, size_t* r2, uint64_t* seeds,
+                           double* ebs);
+
+/* ---- host lossless stage (ZSTD level 3, as src/sz_lossless.cpp:11-26) ---- */
+int cpsz_b200_zstd_compress(const unsigned char* data, size_t n, int level, unsigned char** out, size_t* out_size);
+int cpsz_b200_zstd_decompress(const unsigned char* data, size_t n, unsigned char* out, size_t out_size);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CPSZ_B200_H */

@@ -1,0 +1,102 @@
+"""2D offline path on the GPU vs the oracle: blob bytes, decoded fields and the
+intermediate streams, bit-exact (integer/byte data compared exactly, floats by bit pattern)."""
+import numpy as np
+import pytest
+
+import cpsz_b200
+from cpsz_b200 import workloads as W
+from tests._util import assert_bits_equal, assert_blob_equal_2d, golden_cases
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("path", golden_cases("2d_"), ids=lambda p: p.split("/")[-1])
+def test_gpu_matches_reference_fixture(ctx, path):
+    g = np.load(path)
+    U, V, eb = g["U"], g["V"], float(g["eb"])
+    blob = cpsz_b200.sz_compress_cp_preserve_2d_offline(U, V, max_pwr_eb=eb, ctx=ctx)
+    assert_blob_equal_2d(blob, g["blob"].tobytes())
+    du, dv = cpsz_b200.sz_decompress_cp_preserve_2d_offline(g["blob"].tobytes(), *U.shape, ctx=ctx)
+    assert_bits_equal(du, g["dU"])
+    assert_bits_equal(dv, g["dV"])
+
+
+SHAPES = [(1, 1), (1, 2), (2, 1), (2, 2), (1, 300), (300, 1), (3, 4097), (4097, 3), (13, 17), (255, 257),
+          (256, 256), (257, 255), (511, 33), (600, 700)]
+
+
+@pytest.mark.parametrize("r1,r2", SHAPES)
+@pytest.mark.parametrize("eb", [0.1, 0.01])
+def test_gpu_blob_equals_oracle(ctx, oracle, r1, r2, eb):
+    U, V = W.cfg0_like(r1 * 7919 + r2, r1, r2)
+    a = cpsz_b200.sz_compress_cp_preserve_2d_offline(U, V, max_pwr_eb=eb, ctx=ctx)
+    b = oracle.compress_2d(U, V, eb)
+    assert_blob_equal_2d(a, b)
+    du, dv = cpsz_b200.sz_decompress_cp_preserve_2d_offline(a, r1, r2, ctx=ctx)
+    ou, ov = oracle.decompress_2d(b, r1, r2)
+    assert_bits_equal(du, ou)
+    assert_bits_equal(dv, ov)
+
+
+def test_gpu_stages_equal_oracle(ctx, oracle):
+    r1, r2, eb = 345, 678, 0.1
+    U, V = W.cfg0_like(42, r1, r2)
+    st = cpsz_b200.compress_2d_stages(U, V, eb, ctx=ctx)
+    e = oracle.eb_2d(U, V, eb)
+    ids, eu, ev = oracle.quantize_eb_2d(U, V, e)
+    assert np.array_equal(st["ids"], ids)
+    for data, prec, key, rkey in ((U, eu, "codes_u", "recon_u"), (V, ev, "codes_v", "recon_v")):
+        t, up, rec = oracle.lorenzo_2d(data, prec.reshape(data.shape))
+        assert np.array_equal(st[key], t)
+        assert_bits_equal(st[rkey], rec)
+
+
+def test_gpu_cfg0_full_size(ctx, oracle):
+    U, V = W.cfg0(0)
+    a = cpsz_b200.sz_compress_cp_preserve_2d_offline(U, V, max_pwr_eb=0.1, ctx=ctx)
+    b = oracle.compress_2d(U, V, 0.1)
+    assert_blob_equal_2d(a, b)
+    du, dv = cpsz_b200.sz_decompress_cp_preserve_2d_offline(a, *U.shape, ctx=ctx)
+    ou, ov = oracle.decompress_2d(b, *U.shape)
+    assert_bits_equal(du, ou)
+    assert_bits_equal(dv, ov)
+
+
+def test_gpu_device_resident_inputs(ctx, oracle):
+    torch = pytest.importorskip("torch")
+    U, V = W.cfg0_like(7, 500, 400)
+    dU = torch.from_numpy(U).cuda()
+    dV = torch.from_numpy(V).cuda()
+    a = cpsz_b200.sz_compress_cp_preserve_2d_offline(dU, dV, max_pwr_eb=0.1, ctx=ctx)
+    assert_blob_equal_2d(a, oracle.compress_2d(U, V, 0.1))
+    oU = torch.empty_like(dU)
+    oV = torch.empty_like(dV)
+    cpsz_b200.sz_decompress_cp_preserve_2d_offline(a, 500, 400, oU, oV, ctx=ctx)
+    torch.cuda.synchronize()
+    ou, ov = oracle.decompress_2d(a, 500, 400)
+    assert_bits_equal(oU.cpu().numpy(), ou)
+    assert_bits_equal(oV.cpu().numpy(), ov)
+
+
+def test_gpu_constant_and_zero_fields(ctx, oracle):
+    for U in (np.zeros((40, 50), np.float32), np.full((40, 50), 0.5, np.float32)):
+        V = U.copy()
+        a = cpsz_b200.sz_compress_cp_preserve_2d_offline(U, V, max_pwr_eb=0.1, ctx=ctx)
+        assert_blob_equal_2d(a, oracle.compress_2d(U, V, 0.1))
+        du, dv = cpsz_b200.sz_decompress_cp_preserve_2d_offline(a, 40, 50, ctx=ctx)
+        ou, ov = oracle.decompress_2d(a, 40, 50)
+        assert_bits_equal(du, ou)
+
+
+def test_gpu_rejects_corrupt_blobs(ctx):
+    U, V = W.cfg0_like(9, 64, 64)
+    blob = bytearray(cpsz_b200.sz_compress_cp_preserve_2d_offline(U, V, max_pwr_eb=0.1, ctx=ctx))
+    with pytest.raises(cpsz_b200.CpszError):
+        cpsz_b200.sz_decompress_cp_preserve_2d_offline(bytes(blob[: len(blob) // 2]), 64, 64, ctx=ctx)
+    bad = bytearray(blob)
+    bad[12:20] = (10 ** 12).to_bytes(8, "little")  # absurd id-section size
+    with pytest.raises(cpsz_b200.CpszError):
+        cpsz_b200.sz_decompress_cp_preserve_2d_offline(bytes(bad), 64, 64, ctx=ctx)
+    # the context is still usable afterwards
+    du, dv = cpsz_b200.sz_decompress_cp_preserve_2d_offline(bytes(blob), 64, 64, ctx=ctx)
+    assert np.isfinite(du).all()

@@ -1,0 +1,43 @@
+"""The restated oracle against the reference's own sources (oracle/_ref),
+run live on seeded generator fields (skipped where the reference build is absent)."""
+import numpy as np
+import pytest
+
+from cpsz_b200 import workloads as W
+from oracle import ref_2d_in_bounds, ref_3d_in_bounds
+from tests._util import assert_bits_equal, assert_blob_equal_2d
+
+
+@pytest.mark.parametrize("r1,r2,eb,seed", [(200, 300, 0.1, 6), (517, 611, 0.1, 7), (300, 257, 0.01, 8),
+                                           (64, 1000, 0.05, 9), (1000, 40, 0.1, 10)])
+def test_2d_blob_and_decode_identical(oracle, reference, r1, r2, eb, seed):
+    U, V = W.cfg0_like(seed, r1, r2)
+    a = oracle.compress_2d(U, V, eb)
+    if not ref_2d_in_bounds(a, r1, r2):
+        pytest.skip("workload exceeds the reference's fixed scratch buffers")
+    b = reference.compress_2d(U, V, eb)
+    assert_blob_equal_2d(a, b)
+    da = oracle.decompress_2d(a, r1, r2)
+    db = reference.decompress_2d(b, r1, r2)
+    for x, y in zip(da, db):
+        assert_bits_equal(x, y)
+
+
+@pytest.mark.parametrize("shape,eb,seed", [((48, 48, 48), 0.05, 4), ((40, 33, 50), 0.01, 5), ((30, 60, 45), 0.1, 6)])
+def test_3d_blob_and_decode_identical(oracle, reference, shape, eb, seed):
+    U, V, Wf = W.field_3d(seed, *shape, max(1, int(np.prod(shape)) // 4000), 6.0)
+    a = oracle.compress_3d(U, V, Wf, eb)
+    if not ref_3d_in_bounds(a, *shape):
+        pytest.skip("workload exceeds the reference's fixed scratch buffer")
+    b = reference.compress_3d(U, V, Wf, eb)
+    assert a == b
+    for x, y in zip(oracle.decompress_3d(a, *shape), reference.decompress_3d(b, *shape)):
+        assert_bits_equal(x, y)
+
+
+def test_zstd_stage_matches(reference):
+    import cpsz_b200
+
+    U, V = W.cfg0_like(3, 256, 256)
+    data = U.tobytes() + V.tobytes()
+    assert cpsz_b200.sz_lossless_compress(data, 3) == reference.zstd_compress(data)
