@@ -48,13 +48,27 @@ __global__ void __launch_bounds__(NT) r2b_kernel(const uint16_t* __restrict__ ra
   for (int k = 0; k < s.w; k++) blocks[s.pos + k] = src[k];
 }
 
+// Decompression side of a point: the addend 2(code - 32768) * p that the
+// wavefront adds to its prediction (p = 4^id * 2^-52, 0 for id 0;
+// src/sz_decompress_cp_preserve_2d.cpp:30-34, include/sz_decompression_utils.hpp:65-73),
+// or a raw flag for code 0 (the raw value is scattered in afterwards).
 __global__ void __launch_bounds__(NT) b2r_kernel(const uint16_t* __restrict__ blocks, int r1, int r2, int nby,
-                                                 long long nseg, uint16_t* __restrict__ raster, long long pitch) {
+                                                 long long nseg, uint16_t* __restrict__ raster, long long pitch,
+                                                 const uint8_t* __restrict__ ids, float2* __restrict__ pair) {
   long long ord = (long long)blockIdx.x * NT + threadIdx.x;
   if (ord >= nseg) return;
   Seg s = seg_of(ord, r1, r2, nby);
   uint16_t* dst = raster + (long long)s.i * pitch + s.j0;
   for (int k = 0; k < s.w; k++) dst[k] = blocks[s.pos + k];
+  if (pair) {
+    const long long base = (long long)s.i * r2 + s.j0;
+    for (int k = 0; k < s.w; k++) {
+      const int code = blocks[s.pos + k];
+      const int id = ids[base + k];
+      const float p = id ? __int_as_float((2 * id - 52 + 127) << 23) : 0.f;
+      pair[base + k] = make_float2((float)(2 * (code - 32768)) * p, __int_as_float(code == 0 ? 1 : 0));
+    }
+  }
 }
 
 __global__ void __launch_bounds__(NT) seg_count_kernel(const uint16_t* __restrict__ raster, long long pitch, int r1,
@@ -85,17 +99,17 @@ __global__ void __launch_bounds__(NT) gather_kernel(const uint16_t* __restrict__
 __global__ void __launch_bounds__(NT) scatter_kernel(const uint16_t* __restrict__ raster, long long pitch,
                                                      const float* __restrict__ unpred, unsigned long long n_unpred,
                                                      int r1, int r2, int nby, long long nseg,
-                                                     const unsigned int* __restrict__ off, float* __restrict__ x,
-                                                     long long x_pitch, int* flag) {
+                                                     const unsigned int* __restrict__ off,
+                                                     float2* __restrict__ pairs, int* flag) {
   long long ord = (long long)blockIdx.x * NT + threadIdx.x;
   if (ord >= nseg) return;
   Seg s = seg_of(ord, r1, r2, nby);
   const uint16_t* src = raster + (long long)s.i * pitch + s.j0;
-  float* xs = x + (long long)s.i * x_pitch + s.j0;
+  float2* xs = pairs + (long long)s.i * r2 + s.j0;
   unsigned long long o = off[ord];
   for (int k = 0; k < s.w; k++)
     if (src[k] == 0) {
-      if (o < n_unpred) xs[k] = unpred[o];
+      if (o < n_unpred) xs[k].x = unpred[o];
       else atomicOr(flag, FLAG_RAW_RANGE);
       o++;
     }
@@ -218,10 +232,10 @@ int launch_raster_to_blocks_u16(cpsz_b200_ctx* ctx, const uint16_t* raster, long
 }
 
 int launch_blocks_to_raster_u16(cpsz_b200_ctx* ctx, const uint16_t* blocks, int r1, int r2, uint16_t* raster,
-                                long long pitch) {
+                                long long pitch, const uint8_t* ids, float2* pair) {
   long long nseg = nseg_of(r1, r2);
   int nby = (r2 - 1) / BS + 1;
-  b2r_kernel<<<grid_of(nseg), NT, 0, ctx->stream>>>(blocks, r1, r2, nby, nseg, raster, pitch);
+  b2r_kernel<<<grid_of(nseg), NT, 0, ctx->stream>>>(blocks, r1, r2, nby, nseg, raster, pitch, ids, pair);
   count_launch(ctx);
   return check_launch("b2r_kernel");
 }
@@ -249,12 +263,11 @@ int launch_gather_unpred(cpsz_b200_ctx* ctx, const uint16_t* codes_raster, long 
 }
 
 int launch_scatter_unpred(cpsz_b200_ctx* ctx, const uint16_t* codes_raster, long long pitch, const float* unpred,
-                          unsigned long long n_unpred, int r1, int r2, const unsigned int* seg_off, float* x_raster,
-                          long long x_pitch) {
+                          unsigned long long n_unpred, int r1, int r2, const unsigned int* seg_off, float2* pairs) {
   long long nseg = nseg_of(r1, r2);
   int nby = (r2 - 1) / BS + 1;
   scatter_kernel<<<grid_of(nseg), NT, 0, ctx->stream>>>(codes_raster, pitch, unpred, n_unpred, r1, r2, nby, nseg,
-                                                        seg_off, x_raster, x_pitch, ctx->d_flag);
+                                                        seg_off, pairs, ctx->d_flag);
   count_launch(ctx);
   return check_launch("scatter_kernel");
 }

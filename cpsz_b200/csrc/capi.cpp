@@ -160,7 +160,7 @@ int cpsz_b200_debug_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, siz
   cudaMemcpy(dV, V, 4 * N, cudaMemcpyHostToDevice);
   cudaMemcpy(dtab, qt.t, QUANT_TAB_MAX * 8, cudaMemcpyHostToDevice);
   cudaMemset(dh, 0, 256 * 8);
-  int rc = launch_eb2d(ctx, dU, dV, (int)r1, (int)r2, max_pwr_eb, dtab, qt.n, dids, dids + N, dh, deb);
+  int rc = launch_eb2d(ctx, dU, dV, (int)r1, (int)r2, max_pwr_eb, dtab, qt.n, dids, dids + N, dh, nullptr, nullptr, deb);
   cudaStreamSynchronize(ctx->stream);
   if (rc == CPSZ_OK) {
     if (eb_out) cudaMemcpy(eb_out, deb, 8 * N, cudaMemcpyDeviceToHost);
@@ -173,6 +173,26 @@ int cpsz_b200_debug_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, siz
   cudaFree(dtab);
   cudaFree(dh);
   return rc;
+}
+
+int cpsz_b200_debug_wave_trace(cpsz_b200_ctx* ctx, size_t len, long long* out) {
+  RESOLVE(ctx);
+  if (out) {
+    if (!ctx->d_wave_trace) return set_error(CPSZ_ERR_INVALID, "wave trace not enabled");
+    size_t n = len < ctx->wave_trace_len ? len : ctx->wave_trace_len;
+    CPSZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    CPSZ_CUDA_TRY(cudaMemcpy(out, ctx->d_wave_trace, n * 8, cudaMemcpyDeviceToHost));
+    return CPSZ_OK;
+  }
+  if (ctx->d_wave_trace) cudaFree(ctx->d_wave_trace);
+  ctx->d_wave_trace = nullptr;
+  ctx->wave_trace_len = 0;
+  if (len) {
+    CPSZ_CUDA_TRY(cudaMalloc((void**)&ctx->d_wave_trace, len * 8));
+    CPSZ_CUDA_TRY(cudaMemset(ctx->d_wave_trace, 0, len * 8));
+    ctx->wave_trace_len = len;
+  }
+  return CPSZ_OK;
 }
 
 int cpsz_b200_debug_quant_table(int which, double* t, int* n) {

@@ -30,6 +30,7 @@ __global__ void __launch_bounds__(NT) eb2d_kernel(const float* __restrict__ U, c
                                                   int r2, double max_pwr_eb, const double* __restrict__ thr_tab,
                                                   int thr_n, uint8_t* __restrict__ ids_u, uint8_t* __restrict__ ids_v,
                                                   unsigned long long* __restrict__ hist, int* __restrict__ flag,
+                                                  float2* __restrict__ pair_u, float2* __restrict__ pair_v,
                                                   double* __restrict__ eb_out) {
   __shared__ float su[TY + 2][TX + 3];
   __shared__ float sv[TY + 2][TX + 3];
@@ -101,9 +102,9 @@ __global__ void __launch_bounds__(NT) eb2d_kernel(const float* __restrict__ U, c
       } else {
         int ex = (int)((__double_as_longlong(e) >> 52) & 0x7ff) - 1023;
         int id = dev::count_thresholds(tab, thr_n, e, (ex + 52) >> 1);
-        if (id >= ID_ZERO) {
+        if (id > ID_MAX_2D) {
           atomicOr(flag, FLAG_ID_OVERFLOW);
-          id = ID_ZERO - 1;
+          id = ID_MAX_2D;
         }
         code[c] = (uint8_t)id;
         sym[c] = id;
@@ -113,6 +114,13 @@ __global__ void __launch_bounds__(NT) eb2d_kernel(const float* __restrict__ U, c
     if (eb_out) eb_out[g] = eb;
     ids_u[g] = code[0];
     ids_v[g] = code[1];
+    if (pair_u) {
+      // the wavefront's input: value and 1/precision = 2^(52 - 2 id) (NaN for precision 0)
+      pair_u[g] = make_float2(uu, code[0] == ID_ZERO ? __int_as_float(0x7FC00000)
+                                                     : __int_as_float((127 + 52 - 2 * (int)code[0]) << 23));
+      pair_v[g] = make_float2(vv, code[1] == ID_ZERO ? __int_as_float(0x7FC00000)
+                                                     : __int_as_float((127 + 52 - 2 * (int)code[1]) << 23));
+    }
     atomicAdd(&shist[sym[0]], 1u);
     atomicAdd(&shist[sym[1]], 1u);
   }
@@ -123,10 +131,10 @@ __global__ void __launch_bounds__(NT) eb2d_kernel(const float* __restrict__ U, c
 
 int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, double max_pwr_eb,
                 const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
-                double* eb_out) {
+                float2* pair_u, float2* pair_v, double* eb_out) {
   dim3 grid((r2 + TX - 1) / TX, (r1 + TY - 1) / TY);
   eb2d_kernel<<<grid, NT, 0, ctx->stream>>>(U, V, r1, r2, max_pwr_eb, d_thr_tab, thr_n, ids_u, ids_v, hist,
-                                            ctx->d_flag, eb_out);
+                                            ctx->d_flag, pair_u, pair_v, eb_out);
   count_launch(ctx);
   return check_launch("eb2d_kernel");
 }

@@ -11,6 +11,9 @@ namespace cpsz {
 constexpr int QUANT_TAB_MAX = QuantTable::kMax;
 // Byte code of a vertex whose quantized bound is zero (precision 0, Huffman symbol 0).
 constexpr uint8_t ID_ZERO = 255;
+// Largest supported 2D id: precision 4^id * 2^-52 and its inverse stay normal
+// floats (id 88 is a bound of 2^124, far beyond any relative bound <= 1).
+constexpr int ID_MAX_2D = 88;
 
 // Device error flag bits (ctx->d_flag[0]).
 constexpr int FLAG_ID_OVERFLOW = 1;   // an error-bound id does not fit in a byte
@@ -21,19 +24,24 @@ constexpr int FLAG_RAW_RANGE = 8;     // an unpredictable-value index fell outsi
 // ---- 2D error bounds ---------------------------------------------------------
 int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, double max_pwr_eb,
                 const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
-                double* eb_out = nullptr);
+                float2* pair_u, float2* pair_v, double* eb_out = nullptr);
 
 // ---- 2D Lorenzo wavefront ------------------------------------------------------
 // One field of the wavefront.  Raster arrays carry their own row pitch (elements).
 struct WaveField {
-  const float* x;      // compress: original values; decompress: raw values scattered to raster
-  const uint8_t* ids;  // per-vertex id byte (compress: id or ID_ZERO; decompress: Huffman symbol)
-  uint16_t* codes;     // quantization codes, raster (compress: out, decompress: in)
-  float* out;          // compress: reconstruction (optional); decompress: decoded field
-  float* gbnd;         // last row of every 256-row group: ngroups * r2 floats
-  int* gprog;          // columns published per group (zeroed before launch)
-  long long x_pitch, id_pitch, code_pitch, out_pitch;
+  // per-point input pair: compress (value, bits of 1/precision; NaN for
+  // precision 0), decompress (addend 2(code-32768)*p or the raw value, raw flag)
+  const float2* pair;
+  uint16_t* codes;     // compress: quantization codes out (raster)
+  float* out;          // compress: reconstruction (optional tap); decompress: decoded field
+  // last row of every 256-row group, ngroups * r2 tagged words
+  // ((column + 1) << 32 | float bits); zeroed before every launch
+  unsigned long long* gbnd;
+  long long pair_pitch, code_pitch, out_pitch;
   int r1, r2;
+  // optional diagnostics: per (group, warp) 4 counters {start clock, end clock,
+  // spins waiting for the row above, spins waiting for ring credit}
+  long long* trace;
 };
 struct WaveItem {
   int field;
@@ -50,8 +58,11 @@ int launch_wave2d(cpsz_b200_ctx* ctx, bool decompress, const WaveField* d_fields
 // symbols (65536 bins) fused into the forward permutation.
 int launch_raster_to_blocks_u16(cpsz_b200_ctx* ctx, const uint16_t* raster, long long pitch, int r1, int r2,
                                 uint16_t* blocks, unsigned long long* hist);
+// With pair != NULL also writes, per raster point (pitch r2), the
+// decompression pair (addend 2(code - 32768) * 4^id * 2^-52 (0 for id 0),
+// raw flag bits = (code == 0)).
 int launch_blocks_to_raster_u16(cpsz_b200_ctx* ctx, const uint16_t* blocks, int r1, int r2, uint16_t* raster,
-                                long long pitch);
+                                long long pitch, const uint8_t* ids = nullptr, float2* pair = nullptr);
 // Zero-code counts per row segment (one 12-wide block row) in block order,
 // exclusive-scanned into seg_off (size r1*nby+1; seg_off[r1*nby] = total).
 int launch_segment_scan(cpsz_b200_ctx* ctx, const uint16_t* codes_raster, long long pitch, int r1, int r2,
@@ -60,10 +71,10 @@ size_t segment_scan_tmp_bytes(int r1, int r2);
 // Compress: gather x at zero-code positions into block order (unpred list).
 int launch_gather_unpred(cpsz_b200_ctx* ctx, const uint16_t* codes_raster, long long pitch, const float* x,
                          long long x_pitch, int r1, int r2, const unsigned int* seg_off, float* unpred);
-// Decompress: scatter the unpred list to raster positions of zero codes.
+// Decompress: scatter the unpred list into the .x of the raster pairs (pitch
+// r2) at zero-code positions.
 int launch_scatter_unpred(cpsz_b200_ctx* ctx, const uint16_t* codes_raster, long long pitch, const float* unpred,
-                          unsigned long long n_unpred, int r1, int r2, const unsigned int* seg_off, float* x_raster,
-                          long long x_pitch);
+                          unsigned long long n_unpred, int r1, int r2, const unsigned int* seg_off, float2* pairs);
 
 // ---- Huffman -------------------------------------------------------------------
 // Codebook for the encoder: per symbol, code right-aligned (bit len-1 = first bit).

@@ -41,10 +41,10 @@ struct DevBuf {
   uint8_t* ids;  // 2N: U ids then V ids
   unsigned long long* hist_ids;
   uint16_t* craster[2];
+  float2* pairs[2];  // per-point (value, 1/precision) pairs read by the wavefront
   uint16_t* cblocks[2];
   unsigned long long* hist_codes[2];
-  float* gbnd;
-  int* gprog;
+  unsigned long long* gbnd;
   int* queue;
   WaveField* fields;
   WaveItem* items;
@@ -112,10 +112,11 @@ int compress_2d(cpsz_b200_ctx* ctx, const float* U_in, const float* V_in, size_t
   add(2 * N);                         // ids
   add(256 * 8);                       // hist ids
   add(4 * N);                         // codes raster
+  add(16 * N);                        // wavefront input pairs
   add(4 * N);                         // codes blocks
   add(2 * 65536 * 8);                 // hist codes
-  add(2 * (size_t)ngroups * r2 * 4);  // boundary rows
-  add(2 * (size_t)ngroups * 4 + 64);  // progress + queue
+  add(2 * (size_t)ngroups * r2 * 8);  // boundary rows (tagged words)
+  add(64);                            // work-queue counter
   add(2 * sizeof(WaveField) + 2 * (size_t)ngroups * sizeof(WaveItem));
   add(2 * 2 * (nseg + 1) * 4);
   add(2 * segment_scan_tmp_bytes(r1, r2));
@@ -152,12 +153,12 @@ int compress_2d(cpsz_b200_ctx* ctx, const float* U_in, const float* V_in, size_t
   d.hist_ids = (unsigned long long*)A(256 * 8);
   for (int f = 0; f < 2; f++) {
     d.craster[f] = (uint16_t*)A(2 * N);
+    d.pairs[f] = (float2*)A(8 * N);
     d.cblocks[f] = (uint16_t*)A(2 * N);
     d.hist_codes[f] = (unsigned long long*)A(65536 * 8);
   }
-  d.gbnd = (float*)A(2 * (size_t)ngroups * r2 * 4);
-  d.gprog = (int*)A(2 * (size_t)ngroups * 4 + 64);
-  d.queue = d.gprog + 2 * ngroups;
+  d.gbnd = (unsigned long long*)A(2 * (size_t)ngroups * r2 * 8);
+  d.queue = (int*)A(64);
   d.fields = (WaveField*)A(2 * sizeof(WaveField));
   d.items = (WaveItem*)A(2 * (size_t)ngroups * sizeof(WaveItem));
   for (int f = 0; f < 2; f++) {
@@ -190,7 +191,8 @@ int compress_2d(cpsz_b200_ctx* ctx, const float* U_in, const float* V_in, size_t
   CPSZ_CUDA_TRY(cudaMemsetAsync(d.hist_ids, 0, 256 * 8, st));
   CPSZ_CUDA_TRY(cudaMemcpyAsync(d.thr_tab, qt.t, QUANT_TAB_MAX * 8, cudaMemcpyHostToDevice, st));
   mark(ctx, "eb2d");
-  CPSZ_TRY(launch_eb2d(ctx, d.U, d.V, r1, r2, max_pwr_eb, d.thr_tab, qt.n, d.ids, d.ids + N, d.hist_ids));
+  CPSZ_TRY(launch_eb2d(ctx, d.U, d.V, r1, r2, max_pwr_eb, d.thr_tab, qt.n, d.ids, d.ids + N, d.hist_ids,
+                       d.pairs[0], d.pairs[1]));
   mark(ctx, "eb2d_end");
   unsigned long long* h_hist_ids = (unsigned long long*)ctx->pinned;
   CPSZ_CUDA_TRY(cudaMemcpyAsync(h_hist_ids, d.hist_ids, 256 * 8, cudaMemcpyDeviceToHost, st));
@@ -201,14 +203,14 @@ int compress_2d(cpsz_b200_ctx* ctx, const float* U_in, const float* V_in, size_t
   std::vector<WaveField> hf(2);
   for (int f = 0; f < 2; f++) {
     WaveField& F = hf[f];
-    F.x = f ? d.V : d.U;
-    F.ids = d.ids + (size_t)f * N;
+    F.pair = d.pairs[f];
     F.codes = d.craster[f];
+    F.trace = (ctx->d_wave_trace && ctx->wave_trace_len >= 2 * (size_t)ngroups * WAVE_WARPS * 4)
+                  ? ctx->d_wave_trace + (size_t)f * ngroups * WAVE_WARPS * 4
+                  : nullptr;
     F.out = tap ? tap->recon[f] : nullptr;
     F.gbnd = d.gbnd + (size_t)f * ngroups * r2;
-    F.gprog = d.gprog + f * ngroups;
-    F.x_pitch = r2;
-    F.id_pitch = r2;
+    F.pair_pitch = r2;
     F.code_pitch = r2;
     F.out_pitch = r2;
     F.r1 = r1;
@@ -219,7 +221,8 @@ int compress_2d(cpsz_b200_ctx* ctx, const float* U_in, const float* V_in, size_t
   int n_items = build_wave_items(2, r1v, items);
   CPSZ_CUDA_TRY(cudaMemcpyAsync(d.fields, hf.data(), 2 * sizeof(WaveField), cudaMemcpyHostToDevice, st));
   CPSZ_CUDA_TRY(cudaMemcpyAsync(d.items, items.data(), n_items * sizeof(WaveItem), cudaMemcpyHostToDevice, st));
-  CPSZ_CUDA_TRY(cudaMemsetAsync(d.gprog, 0, 2 * (size_t)ngroups * 4 + 64, st));
+  CPSZ_CUDA_TRY(cudaMemsetAsync(d.gbnd, 0, 2 * (size_t)ngroups * r2 * 8, st));
+  CPSZ_CUDA_TRY(cudaMemsetAsync(d.queue, 0, 64, st));
   mark(ctx, "wave2d_compress");
   CPSZ_TRY(launch_wave2d(ctx, false, d.fields, d.items, n_items, d.queue, 0));
   mark(ctx, "blocks+hist+unpred");
@@ -438,7 +441,8 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
   if (!huff_parse(blob + BLOB_HDR, eb_size, 2047, &hid)) return CPSZ_ERR_FORMAT;
   if (hid.section_bytes > eb_size) return set_error(CPSZ_ERR_FORMAT, "id section overruns");
   for (uint32_t s : hid.sym)
-    if (s >= 255) return set_error(CPSZ_ERR_UNSUPPORTED, "error-bound id %u beyond the 8-bit id stream", s);
+    if (s > (uint32_t)ID_MAX_2D)
+      return set_error(CPSZ_ERR_UNSUPPORTED, "error-bound id %u beyond the supported range (<= %d)", s, ID_MAX_2D);
   FieldView fv[2];
   CPSZ_TRY(parse_field(blob, BLOB_HDR + eb_size, u_size, N, nblocks, &fv[0]));
   CPSZ_TRY(parse_field(blob, BLOB_HDR + eb_size + u_size, v_size, N, nblocks, &fv[1]));
@@ -457,12 +461,13 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
   }
   add(4 * N);  // codes blocks
   add(4 * N);  // codes raster
+  add(8 * N);  // (pairs: the raw raster below holds 16 N)
   add(8 * N);  // raw raster
   add(2 * 4 * N);  // unpred lists
   add(2 * 2 * (nseg + 1) * 4);
   add(2 * segment_scan_tmp_bytes(r1, r2));
-  add(2 * (size_t)ngroups * r2 * 4);
-  add(2 * (size_t)ngroups * 4 + 64);
+  add(2 * (size_t)ngroups * r2 * 8);
+  add(64);
   add(2 * sizeof(WaveField) + 2 * (size_t)ngroups * sizeof(WaveItem));
   CPSZ_TRY(arena_reserve(ctx, bytes));
   CPSZ_TRY(pinned_reserve(ctx, 4096));
@@ -495,14 +500,14 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
   }
   uint16_t* cblocks[2];
   uint16_t* craster[2];
-  float* raw[2];
+  float2* raw[2];  // (addend, raw flag) per point; .x holds the raw value where the code is 0
   float* unpred[2];
   unsigned int *seg_cnt[2], *seg_off[2];
   void* scan_tmp[2];
   for (int f = 0; f < 2; f++) {
     cblocks[f] = (uint16_t*)A(2 * N);
     craster[f] = (uint16_t*)A(2 * N);
-    raw[f] = (float*)A(4 * N);
+    raw[f] = (float2*)A(8 * N);
     unpred[f] = (float*)A(4 * fv[f].n_unpred + 4);
     seg_cnt[f] = (unsigned int*)A((nseg + 1) * 4);
     seg_off[f] = (unsigned int*)A((nseg + 1) * 4);
@@ -510,9 +515,8 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
     if (fv[f].n_unpred)
       CPSZ_CUDA_TRY(cudaMemcpyAsync(unpred[f], blob + fv[f].unpred_off, 4 * fv[f].n_unpred, cudaMemcpyHostToDevice, st));
   }
-  float* gbnd = (float*)A(2 * (size_t)ngroups * r2 * 4);
-  int* gprog = (int*)A(2 * (size_t)ngroups * 4 + 64);
-  int* queue = gprog + 2 * ngroups;
+  unsigned long long* gbnd = (unsigned long long*)A(2 * (size_t)ngroups * r2 * 8);
+  int* queue = (int*)A(64);
   WaveField* dfields = (WaveField*)A(2 * sizeof(WaveField));
   WaveItem* ditems = (WaveItem*)A(2 * (size_t)ngroups * sizeof(WaveItem));
   if (!ditems) return set_error(CPSZ_ERR_NOMEM, "workspace layout overflow");
@@ -528,23 +532,21 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
   mark(ctx, "raster+scatter");
   unsigned int* h_cnt = (unsigned int*)ctx->pinned + 16;
   for (int f = 0; f < 2; f++) {
-    CPSZ_TRY(launch_blocks_to_raster_u16(ctx, cblocks[f], r1, r2, craster[f], r2));
+    CPSZ_TRY(launch_blocks_to_raster_u16(ctx, cblocks[f], r1, r2, craster[f], r2, ids + (size_t)f * N, raw[f]));
     CPSZ_TRY(launch_segment_scan(ctx, craster[f], r2, r1, r2, seg_cnt[f], seg_off[f], scan_tmp[f]));
-    CPSZ_TRY(launch_scatter_unpred(ctx, craster[f], r2, unpred[f], fv[f].n_unpred, r1, r2, seg_off[f], raw[f], r2));
+    CPSZ_TRY(launch_scatter_unpred(ctx, craster[f], r2, unpred[f], fv[f].n_unpred, r1, r2, seg_off[f], raw[f]));
     CPSZ_CUDA_TRY(cudaMemcpyAsync(h_cnt + f, seg_off[f] + nseg, 4, cudaMemcpyDeviceToHost, st));
   }
   // ---- wavefront ----
   WaveField hf[2];
   for (int f = 0; f < 2; f++) {
     WaveField& F = hf[f];
-    F.x = raw[f];
-    F.ids = ids + (size_t)f * N;
-    F.codes = craster[f];
+    F.pair = raw[f];
+    F.codes = nullptr;
+    F.trace = nullptr;
     F.out = f ? dV : dU;
     F.gbnd = gbnd + (size_t)f * ngroups * r2;
-    F.gprog = gprog + f * ngroups;
-    F.x_pitch = r2;
-    F.id_pitch = r2;
+    F.pair_pitch = r2;
     F.code_pitch = r2;
     F.out_pitch = r2;
     F.r1 = r1;
@@ -555,7 +557,8 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
   int n_items = build_wave_items(2, r1v, items);
   CPSZ_CUDA_TRY(cudaMemcpyAsync(dfields, hf, sizeof(hf), cudaMemcpyHostToDevice, st));
   CPSZ_CUDA_TRY(cudaMemcpyAsync(ditems, items.data(), n_items * sizeof(WaveItem), cudaMemcpyHostToDevice, st));
-  CPSZ_CUDA_TRY(cudaMemsetAsync(gprog, 0, 2 * (size_t)ngroups * 4 + 64, st));
+  CPSZ_CUDA_TRY(cudaMemsetAsync(gbnd, 0, 2 * (size_t)ngroups * r2 * 8, st));
+  CPSZ_CUDA_TRY(cudaMemsetAsync(queue, 0, 64, st));
   mark(ctx, "wave2d_decompress");
   CPSZ_TRY(launch_wave2d(ctx, true, dfields, ditems, n_items, queue, 0));
   mark(ctx, "d2h");

@@ -84,6 +84,9 @@ struct cpsz_b200_ctx {
   cudaEvent_t tev[kMaxMarks] = {};
   const char* tname[kMaxMarks] = {};
   int nmarks = 0;
+  // optional wavefront trace (diagnostics): 4 counters per (field, group, warp)
+  long long* d_wave_trace = nullptr;
+  size_t wave_trace_len = 0;
 };
 
 namespace cpsz {

@@ -6,31 +6,53 @@
 // traversal of src/sz_compress_3d.cpp:126-193 with its rolling (bs+1)x(d2+1)
 // buffer is exactly the raster recurrence with zero padding), so the field is
 // a serial recurrence whose critical path is r1 + r2 points.  Bit-exactness
-// rules out any reformulation; the parallel schedule is a skewed wavefront:
+// rules out any reformulation; the parallel schedule is a skewed wavefront,
+// and the design goal is the fewest issued instructions per step, because a
+// warp issues in order and its step time is its instruction stream:
 //
 //  * a warp owns 32 consecutive rows (lane = row) and at step s lane l
 //    processes column s - l; the value above comes from lane l-1's result of
 //    the previous step through one __shfl_up_sync, the value up-left is the
 //    value above of the previous step, the value to the left is the lane's own
 //    previous result;
-//  * a CTA owns a 256-row group (8 warps); warp w's lane 0 reads the row above
-//    from warp w-1's lane 31 through a shared-memory ring with credit-based
-//    flow control;
+//  * inputs are one 8-byte pair per point (compress: value and the bits of
+//    1/precision, NaN for precision 0; decompress: the precomputed addend or
+//    the raw value, and a raw flag), staged per 32-step window k as a
+//    "parallelogram" tile -- row l holds columns [32k - l, 32k - l + 32),
+//    exactly what lane l touches during steps [32k, 32k + 32) -- filled with
+//    coalesced 8-byte cp.async row copies one window ahead (double buffered)
+//    and drained with coalesced row stores one window behind.  A 33-element
+//    row pitch makes the per-step accesses tile[l][t] bank-conflict free.
+//    Points outside the field are staged as pairs that reconstruct to 0, so a
+//    step has no bounds branches;
+//  * a CTA owns a 256-row group (8 warps).  Warp w takes the row above from
+//    warp w-1 through a shared-memory ring of tagged words, 8 columns at a
+//    time (one warp-uniform tag test per 8 steps); lane 31 stores one tagged
+//    word per step.  The CTA's first warp takes the previous group's last row
+//    from global memory, a whole 32-column window at a time, validated once
+//    per window and loaded coalesced one window ahead;
 //  * CTAs are persistent and pull (field, group) items from a device work
 //    queue (atomic counter).  An item's predecessor (same field, previous
-//    group) was dequeued earlier by a running CTA, so every wait ends; warp 0
-//    reads that group's last row from global memory after an acquire load of
-//    its progress counter, which the producer advances with release stores.
-//    Every wait is bounded; on expiry the kernel sets FLAG_TIMEOUT and
-//    finishes without waiting.
+//    group) was dequeued earlier by a running CTA, so every wait ends.
 //
-// Per point (compress, include/sz_compression_utils.hpp:52-65):
-//   diff = (float)(x - pred); y = |diff| / p (exact: p is a power of two)
-//   y < 65535  <=>  |diff|/p + 1 < 65536 (the reference's capacity test)
-//   q = (trunc(y) + 1) >> 1 == (int)((|diff|/p + 1) / 2), signed by diff > 0
-//   dec = (float)((double)pred + (double)(2q) * p); kept iff |dec - x| <= p
-// and per point (decompress, include/sz_decompression_utils.hpp:65-73):
-//   code 0 -> raw value, else (float)((double)pred + (double)(2(code-32768)) * p).
+// Tagged words are 64-bit (column + 1) << 32 | float bits, written and read as
+// single aligned 64-bit accesses, so a reader that sees the expected tag holds
+// that column's value and no memory fence is needed.  Every wait is bounded;
+// on expiry the kernel sets FLAG_TIMEOUT and stops waiting.
+//
+// Arithmetic (bit-identical to include/sz_compression_utils.hpp:52-65 and
+// include/sz_decompression_utils.hpp:65-73).  The precision is p = 2^ex, so
+//   y = |x - pred| / p = |x - pred| * (1/p) is exact in float, and the
+//   reference's capacity test |diff|/p + 1 < 65536 is y < 65535 (y + 1 is
+//   exact in double below 2^16);
+//   (int)((|diff|/p + 1) / 2) = (trunc(y) + 1) >> 1;
+//   the reference's (float)((double)pred + (double)(2q) * p) equals the float
+//   sum pred + 2q*p: 2q*p is exact in float (|2q| < 2^17), and whenever the
+//   exact sum does not fit a double one addend lies below 2^-5 ulp of the
+//   other, where rounding through double and rounding once agree;
+//   |dec - x| <= p compares a float against a power of two.
+// Decompression adds the precomputed 2(code - 32768) * p (0 when id = 0) or
+// takes the stored raw value.
 #include "kernels.h"
 
 namespace cpsz {
@@ -39,222 +61,266 @@ namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int RING = 128;
+constexpr int TP = 33;         // tile row pitch (elements)
+constexpr int TILE = 32 * TP;  // elements per tile
 constexpr long long SPIN_LIMIT = 1ll << 22;
 
-__device__ __forceinline__ int ld_acquire(const int* p) {
-  int v;
-  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
+// exact float of an integer |n| < 2^22 without the conversion unit
+__device__ __forceinline__ float small_int_to_float(int n) {
+  return __int_as_float(0x4B400000 + n) - 12582912.0f;
 }
-__device__ __forceinline__ void st_release(int* p, int v) {
-  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ unsigned long long tagged(int c, float v) {
+  return ((unsigned long long)(unsigned)(c + 1) << 32) | (unsigned long long)__float_as_uint(v);
 }
-__device__ __forceinline__ double pow2d(int e) { return __longlong_as_double((long long)(e + 1023) << 52); }
-__device__ __forceinline__ float pow2f(int e) { return __int_as_float((e + 127) << 23); }
+__device__ __forceinline__ bool tag_is(unsigned long long w, int c) { return (unsigned)(w >> 32) == (unsigned)(c + 1); }
+__device__ __forceinline__ float tag_val(unsigned long long w) { return __uint_as_float((unsigned)w); }
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ long long globaltimer_ns() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+struct WarpTiles {
+  float2 in[2][TILE];
+  uint32_t out[2][TILE];
+};
 
 struct Shared {
-  float ring[WAVE_WARPS][RING];
-  volatile int prod[WAVE_WARPS];
-  volatile int cons[WAVE_WARPS];
+  unsigned long long ring[WAVE_WARPS][RING];
+  volatile int cons[WAVE_WARPS];  // ring columns its consumer has finished with
   int item;
 };
 
-template <bool DECOMP>
-struct Lane {
-  // one element of work prefetched into registers
-  float x;
-  uint8_t id;
-  uint16_t code;
-};
+constexpr size_t kDynSmem = sizeof(WarpTiles) * WAVE_WARPS;
 
 template <bool DECOMP>
-__device__ __forceinline__ void load8(const WaveField& F, bool rowok, long long rowc, int s0, int lane,
-                                      Lane<DECOMP> (&b)[8]) {
-  const float* xr = F.x + rowc * F.x_pitch;
-  const uint8_t* ir = F.ids + rowc * F.id_pitch;
-  const uint16_t* cr = F.codes + rowc * F.code_pitch;
-#pragma unroll
-  for (int k = 0; k < 8; k++) {
-    int c = s0 + k - lane;
-    bool v = rowok && c >= 0 && c < F.r2;
-    b[k].x = v ? xr[c] : 0.f;
-    b[k].id = v ? ir[c] : (uint8_t)0;
-    if (DECOMP) b[k].code = v ? cr[c] : (uint16_t)0;
-  }
-  // pull the row's next lines into L1 well ahead of use
-  int cp = s0 + 64 - lane;
-  if (rowok && cp >= 0 && cp < F.r2) {
-    asm volatile("prefetch.global.L1 [%0];" ::"l"(xr + cp));
-    if (DECOMP) asm volatile("prefetch.global.L1 [%0];" ::"l"(cr + cp));
-  }
-}
-
-template <bool DECOMP>
-__device__ __forceinline__ void run_strip(const WaveField& F, int group, int warp, int lane, Shared& sh, int* flag) {
+__device__ __forceinline__ void run_strip(const WaveField& F, int group, int warp, int lane, Shared& sh,
+                                          WarpTiles& T, int* flag) {
   const int r1 = F.r1, r2 = F.r2;
   const int row0 = group * WAVE_GROUP_ROWS + warp * 32;
-  const int row = row0 + lane;
-  const bool rowok = row < r1;
-  const long long rowc = rowok ? row : 0;
-  // who produces for whom
+  const int nrows = min(32, r1 - row0);
   const bool has_above = row0 > 0;
   const bool above_global = has_above && warp == 0;
+  const bool above_ring = has_above && !above_global;
   const bool has_below = row0 + 32 < r1;
   const bool below_global = has_below && warp == WAVE_WARPS - 1;
-  const float* gb_in = above_global ? F.gbnd + (size_t)(group - 1) * r2 : nullptr;
-  const int* gp_in = above_global ? F.gprog + (group - 1) : nullptr;
-  float* gb_out = F.gbnd + (size_t)group * r2;
-  int* gp_out = F.gprog + group;
-  float* orow = F.out ? F.out + rowc * F.out_pitch : nullptr;
-  uint16_t* crow = F.codes + rowc * F.code_pitch;
+  const bool below_ring = has_below && !below_global;
+  const unsigned long long* gb_in = above_global ? F.gbnd + (size_t)(group - 1) * r2 : nullptr;
+  unsigned long long* gb_out = F.gbnd + (size_t)group * r2;
+  // staged pair of a point outside the field: reconstructs to 0
+  const float2 pad = DECOMP ? make_float2(0.f, __int_as_float(1)) : make_float2(0.f, __int_as_float(0x7FC00000));
 
-  int avail = 0;       // lane 0: columns of the row above known to be available
-  int credit = RING;   // lane 31: columns it may run ahead of its consumer
+  int credit = RING;  // ring columns this warp may write before re-reading its consumer's progress
   bool aborted = false;
+  long long spin_above = 0, spin_credit = 0;
+  const long long t_start = F.trace ? globaltimer_ns() : 0;
   float outPrev = 0.f, upPrev = 0.f;
-  const int nsteps = r2 + 31;
+  const int nwin = (r2 + 31 + 31) / 32;  // windows that contain any step
+  const float2* rows_in = F.pair + (long long)row0 * F.pair_pitch;
 
-  auto step = [&](int s, const Lane<DECOMP>& e) {
-    const int c = s - lane;
-    float above = __shfl_up_sync(FULL, outPrev, 1);
-    if (lane == 0) {
-      above = 0.f;
-      if (has_above && c >= 0 && c < r2) {
-        if (c >= avail && !aborted) {
-          long long spins = 0;
-          if (above_global) {
-            int v = ld_acquire(gp_in);
-            while (v <= c) {
-              if (++spins > SPIN_LIMIT) { atomicOr(flag, FLAG_TIMEOUT); aborted = true; break; }
-              __nanosleep(64);
-              v = ld_acquire(gp_in);
-            }
-            avail = v;
-          } else {
-            int v = sh.prod[warp - 1];
-            while (v <= c) {
-              if (++spins > SPIN_LIMIT) { atomicOr(flag, FLAG_TIMEOUT); aborted = true; break; }
-              v = sh.prod[warp - 1];
-            }
-            avail = v;
-          }
-        }
-        if (!aborted) {
-          if (above_global) above = __ldcg(gb_in + c);
-          else {
-            above = sh.ring[warp - 1][c & (RING - 1)];
-            if ((c & 15) == 15 || c == r2 - 1) sh.cons[warp] = c + 1;
-          }
-        }
+  // stage window k: row l, columns [32k - l, 32k - l + 32); lane t takes column t
+  auto fill = [&](int k, int buf) {
+    const float2* rp = rows_in;
+    int c = 32 * k + lane;
+    float2* d = &T.in[buf][lane];
+#pragma unroll 4
+    for (int l = 0; l < 32; l++, c--, d += TP, rp += F.pair_pitch) {
+      if (l < nrows && (unsigned)c < (unsigned)r2) cp_async8(d, rp + c);
+      else *d = pad;
+    }
+    cp_commit();
+  };
+  // write window k's outputs: row l, columns [32k - l, 32k - l + 32)
+  auto drain = [&](int k, int buf) {
+    int c = 32 * k + lane;
+    const uint32_t* s = &T.out[buf][lane];
+    long long r = row0;
+    for (int l = 0; l < nrows; l++, c--, s += TP, r++) {
+      if ((unsigned)c < (unsigned)r2) {
+        const uint32_t v = *s;
+        if (DECOMP) F.out[r * F.out_pitch + c] = __uint_as_float(v);
+        else F.codes[r * F.code_pitch + c] = (uint16_t)v;
       }
     }
-    const float U = above, UL = upPrev;
-    float out = 0.f;
-    if (rowok && c >= 0 && c < r2) {
-      const float pred = (outPrev + U) - UL;
-      if (DECOMP) {
-        if (e.code == 0) {
-          out = e.x;
-        } else {
-          const double p = (e.id == 0) ? 0.0 : pow2d(2 * (int)e.id - 52);
-          out = (float)((double)pred + (double)(2 * ((int)e.code - 32768)) * p);
-        }
-        orow[c] = out;
-      } else {
-        int code = 0;
-        out = e.x;
-        if (e.id != ID_ZERO) {
-          const int ex = 2 * (int)e.id - 52;  // precision = 2^ex
-          const float diff = e.x - pred;
-          // |diff| * 2^-ex is exact in float for ex in [-52, 126); beyond
-          // that range the double path is used.
-          bool small;
-          int qa;
-          if (ex < 100) {
-            const float y = fabsf(diff) * pow2f(-ex);
-            small = y < 65535.0f;
-            qa = small ? (((int)y + 1) >> 1) : 0;
-          } else {
-            const double qd = fabs((double)diff) * pow2d(-ex) + 1.0;
-            small = qd < 65536.0;
-            qa = small ? (int)(qd * 0.5) : 0;
-          }
-          if (small) {
-            const int q = (diff > 0) ? qa : -qa;
-            const double p = pow2d(ex);
-            const float dec = (float)((double)pred + (double)(2 * q) * p);
-            if ((double)fabsf(dec - e.x) <= p) {
-              out = dec;
-              code = q + 32768;
-            }
-          }
-        }
-        crow[c] = (uint16_t)code;
-        if (orow) orow[c] = out;
-      }
-      // lane 31 hands the row down
-      if (lane == 31) {
-        if (below_global) {
-          gb_out[c] = out;
-          if ((c & 7) == 7 || c == r2 - 1) {
-            __threadfence();
-            st_release(gp_out, c + 1);
-          }
-        } else if (has_below && !aborted) {
-          if (credit <= c) {
-            long long spins = 0;
-            int v = sh.cons[warp + 1];
-            while (v + RING <= c) {
-              if (++spins > SPIN_LIMIT) { atomicOr(flag, FLAG_TIMEOUT); aborted = true; break; }
-              v = sh.cons[warp + 1];
-            }
-            credit = v + RING;
-          }
-          sh.ring[warp][c & (RING - 1)] = out;
-          __threadfence_block();
-          sh.prod[warp] = c + 1;
-        }
-      }
-    }
-    upPrev = U;
-    outPrev = out;
+  };
+  auto ring_word = [&](int c) -> unsigned long long {
+    return *(volatile unsigned long long*)&sh.ring[warp - 1][c & (RING - 1)];
+  };
+  // coalesced prefetch of the previous group's last row, one window ahead
+  unsigned long long gcur = 0, gnext = 0;
+  auto gload = [&](int k) -> unsigned long long {
+    const int c = 32 * k + lane;
+    return (c < r2) ? __ldcg(gb_in + c) : 0ull;
   };
 
-  Lane<DECOMP> A[8], B[8];
-  load8<DECOMP>(F, rowok, rowc, 0, lane, A);
-  for (int s0 = 0; s0 < nsteps; s0 += 16) {
-    load8<DECOMP>(F, rowok, rowc, s0 + 8, lane, B);
+  fill(0, 0);
+  if (above_global) gnext = gload(0);
+  for (int k = 0; k < nwin; k++) {
+    const int buf = k & 1;
+    cp_wait_all();
+    __syncwarp();
+    if (k + 1 < nwin) fill(k + 1, buf ^ 1);
+    if (k >= 1) drain(k - 1, buf ^ 1);
+    if (above_global) {
+      // the whole window of the row above must be present: one poll per window
+      gcur = gnext;
+      const int cl = 32 * k + lane;
+      bool ok = cl >= r2 || tag_is(gcur, cl);
+      long long spins = 0;
+      while (!__all_sync(FULL, ok) && !aborted) {
+        if (++spins > SPIN_LIMIT) {
+          if (lane == 0) atomicOr(flag, FLAG_TIMEOUT);
+          aborted = true;
+          break;
+        }
+        __nanosleep(100);
+        if (!ok) {
+          gcur = __ldcg(gb_in + cl);
+          ok = tag_is(gcur, cl);
+        }
+      }
+      spin_above += spins;
+      gnext = gload(k + 1);
+    }
+    __syncwarp();
+    const float2* tin = &T.in[buf][lane * TP];
+    uint32_t* to = &T.out[buf][lane * TP];
+#pragma unroll 1
+    for (int tb = 0; tb < 32; tb += 8) {
+      const int cb = 32 * k + tb;  // lane 0's column at the block's first step
+      // ---- the row above, 8 columns (all lanes hold lane 0's values) ----
+      float ab[8];
+      if (above_global) {
 #pragma unroll
-    for (int k = 0; k < 8; k++)
-      if (s0 + k < nsteps) step(s0 + k, A[k]);
-    load8<DECOMP>(F, rowok, rowc, s0 + 16, lane, A);
+        for (int j = 0; j < 8; j++) ab[j] = tag_val(__shfl_sync(FULL, gcur, tb + j));
+      } else if (above_ring) {
+        unsigned long long wv[8];
+        bool ok = true;
 #pragma unroll
-    for (int k = 0; k < 8; k++)
-      if (s0 + 8 + k < nsteps) step(s0 + 8 + k, B[k]);
+        for (int j = 0; j < 8; j++) {
+          wv[j] = ring_word(cb + j);
+          ok &= (cb + j >= r2) | tag_is(wv[j], cb + j);
+        }
+        if (!ok && !aborted) {  // warp-uniform: all lanes read the same words
+          long long spins = 0;
+          do {
+            if (++spins > SPIN_LIMIT) {
+              if (lane == 0) atomicOr(flag, FLAG_TIMEOUT);
+              aborted = true;
+              break;
+            }
+            ok = true;
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+              wv[j] = ring_word(cb + j);
+              ok &= (cb + j >= r2) | tag_is(wv[j], cb + j);
+            }
+          } while (!ok);
+          spin_above += spins;
+        }
+#pragma unroll
+        for (int j = 0; j < 8; j++) ab[j] = tag_val(wv[j]);
+        if (lane == 0) sh.cons[warp] = cb;  // columns below cb have been consumed
+      } else {
+#pragma unroll
+        for (int j = 0; j < 8; j++) ab[j] = 0.f;
+      }
+      // ---- ring credit for the 8 columns lane 31 writes in this block ----
+      if (below_ring) {
+        const int cmax = cb - 24;
+        if (cmax >= credit && !aborted) {
+          long long spins = 0;
+          int v = sh.cons[warp + 1];
+          while (v + RING <= cmax) {
+            if (++spins > SPIN_LIMIT) {
+              if (lane == 0) atomicOr(flag, FLAG_TIMEOUT);
+              aborted = true;
+              break;
+            }
+            v = sh.cons[warp + 1];
+          }
+          spin_credit += spins;
+          credit = v + RING;
+        }
+      }
+      // ---- 8 steps ----
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        const int t = tb + j;
+        const float shfl = __shfl_up_sync(FULL, outPrev, 1);
+        const float U = (lane == 0) ? (aborted ? 0.f : ab[j]) : shfl;
+        const float pred = (outPrev + U) - upPrev;
+        const float2 e = tin[t];
+        float out;
+        if (DECOMP) {
+          out = (__float_as_int(e.y) != 0) ? e.x : pred + e.x;
+          to[t] = __float_as_uint(out);
+        } else {
+          const float x = e.x, inv = e.y;  // inv = 1/p (NaN for precision 0)
+          const float p = __int_as_float(0x7F000000 - __float_as_int(inv));
+          const float diff = x - pred;
+          const float y = fabsf(diff) * inv;
+          const int qa = ((int)fminf(y, 65536.0f) + 1) >> 1;
+          const int q = (diff > 0.f) ? qa : -qa;
+          const float dec = pred + small_int_to_float(2 * q) * p;
+          const bool ok = (y < 65535.0f) & (fabsf(dec - x) <= p);
+          out = ok ? dec : x;
+          to[t] = ok ? (uint32_t)(q + 32768) : 0u;
+          if (F.out) {  // optional reconstruction tap (tests)
+            const int c = cb + j - lane;
+            if (lane < nrows && (unsigned)c < (unsigned)r2) F.out[(long long)(row0 + lane) * F.out_pitch + c] = out;
+          }
+        }
+        // lane 31 hands its row down (column cb + j - 31)
+        const int c31 = cb + j - 31;
+        if (lane == 31 && (unsigned)c31 < (unsigned)r2) {
+          if (below_ring) *(volatile unsigned long long*)&sh.ring[warp][c31 & (RING - 1)] = tagged(c31, out);
+          else if (below_global) __stcg(gb_out + c31, tagged(c31, out));
+        }
+        upPrev = U;
+        outPrev = out;
+      }
+    }
   }
-  // a producer that aborted still releases its consumers
-  if (lane == 31 && below_global && aborted) st_release(gp_out, r2);
-  if (lane == 31 && has_below && !below_global) sh.prod[warp] = r2;
+  cp_wait_all();
+  __syncwarp();
+  drain(nwin - 1, (nwin - 1) & 1);
+  if (lane == 0 && above_ring) sh.cons[warp] = r2 + RING;
+  if (F.trace && lane == 0) {
+    long long* tr = F.trace + ((long long)group * WAVE_WARPS + warp) * 4;
+    tr[0] = t_start;
+    tr[1] = globaltimer_ns();
+    tr[2] = spin_above;
+    tr[3] = spin_credit;
+  }
 }
 
 template <bool DECOMP>
-__global__ void __launch_bounds__(WAVE_WARPS * 32) wave2d_kernel(const WaveField* __restrict__ fields,
-                                                                 const WaveItem* __restrict__ items, int n_items,
-                                                                 int* queue, int* flag) {
+__global__ void __launch_bounds__(WAVE_WARPS * 32, 1) wave2d_kernel(const WaveField* __restrict__ fields,
+                                                                    const WaveItem* __restrict__ items, int n_items,
+                                                                    int* queue, int* flag) {
   __shared__ Shared sh;
+  extern __shared__ __align__(16) unsigned char dyn[];
+  WarpTiles* tiles = reinterpret_cast<WarpTiles*>(dyn);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (;;) {
     if (threadIdx.x == 0) sh.item = atomicAdd(queue, 1);
-    if (threadIdx.x < WAVE_WARPS) {
-      sh.prod[threadIdx.x] = 0;
-      sh.cons[threadIdx.x] = 0;
-    }
+    for (int k = threadIdx.x; k < WAVE_WARPS * RING; k += blockDim.x) (&sh.ring[0][0])[k] = 0ull;
+    if (threadIdx.x < WAVE_WARPS) sh.cons[threadIdx.x] = 0;
     __syncthreads();
     const int it = sh.item;
     if (it >= n_items) break;
     const WaveItem item = items[it];
     const WaveField F = fields[item.field];
-    if (item.group * WAVE_GROUP_ROWS + warp * 32 < F.r1) run_strip<DECOMP>(F, item.group, warp, lane, sh, flag);
+    if (item.group * WAVE_GROUP_ROWS + warp * 32 < F.r1)
+      run_strip<DECOMP>(F, item.group, warp, lane, sh, tiles[warp], flag);
     __syncthreads();
   }
 }
@@ -263,20 +329,31 @@ __global__ void __launch_bounds__(WAVE_WARPS * 32) wave2d_kernel(const WaveField
 
 int launch_wave2d(cpsz_b200_ctx* ctx, bool decompress, const WaveField* d_fields, const WaveItem* d_items,
                   int n_items, int* d_queue, int max_ctas) {
+  static bool attr_set[2] = {false, false};
+  if (!attr_set[decompress]) {
+    cudaError_t e = decompress ? cudaFuncSetAttribute(wave2d_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                      (int)kDynSmem)
+                               : cudaFuncSetAttribute(wave2d_kernel<false>,
+                                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDynSmem);
+    if (e != cudaSuccess) return set_error(CPSZ_ERR_CUDA, "wave2d smem attribute: %s", cudaGetErrorString(e));
+    attr_set[decompress] = true;
+  }
   int per_sm = 0;
   if (decompress)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wave2d_kernel<true>, WAVE_WARPS * 32, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wave2d_kernel<true>, WAVE_WARPS * 32, kDynSmem);
   else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wave2d_kernel<false>, WAVE_WARPS * 32, 0);
-  if (per_sm < 1) per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wave2d_kernel<false>, WAVE_WARPS * 32, kDynSmem);
+  if (per_sm < 1) return set_error(CPSZ_ERR_CUDA, "wave2d kernel does not fit on an SM");
   int grid = ctx->num_sms * per_sm;
   if (max_ctas > 0 && grid > max_ctas) grid = max_ctas;
   if (grid > n_items) grid = n_items;
   if (grid < 1) return CPSZ_OK;
   if (decompress)
-    wave2d_kernel<true><<<grid, WAVE_WARPS * 32, 0, ctx->stream>>>(d_fields, d_items, n_items, d_queue, ctx->d_flag);
+    wave2d_kernel<true><<<grid, WAVE_WARPS * 32, kDynSmem, ctx->stream>>>(d_fields, d_items, n_items, d_queue,
+                                                                          ctx->d_flag);
   else
-    wave2d_kernel<false><<<grid, WAVE_WARPS * 32, 0, ctx->stream>>>(d_fields, d_items, n_items, d_queue, ctx->d_flag);
+    wave2d_kernel<false><<<grid, WAVE_WARPS * 32, kDynSmem, ctx->stream>>>(d_fields, d_items, n_items, d_queue,
+                                                                           ctx->d_flag);
   count_launch(ctx);
   return check_launch("wave2d_kernel");
 }

@@ -113,6 +113,12 @@ size_t cpsz_b200_blob_size_2d(const unsigned char* blob);
  * doubles) and id bytes (id_codes, 2N; 255 = precision 0).  Host buffers. */
 int cpsz_b200_debug_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2,
                          double max_pwr_eb, double* eb_out, uint8_t* id_codes);
+/* Wavefront trace: with out == NULL, (re)allocates a device trace of len
+ * counters (len = 0 disables it); compressions on this context then record,
+ * per (field, 256-row group, warp), {start ns, end ns, spins waiting for the
+ * row above, spins waiting for ring credit}.  With out != NULL, copies len
+ * counters out. */
+int cpsz_b200_debug_wave_trace(cpsz_b200_ctx* ctx, size_t len, long long* out);
 /* Host-computed quantization thresholds (which = 2 or 3): t[k] is the smallest
  * bound with id >= k under the host libm's log2 (256 doubles). */
 int cpsz_b200_debug_quant_table(int which, double* t, int* n);
