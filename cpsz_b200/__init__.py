@@ -63,6 +63,8 @@ def _declare(L):
     L.cpsz_b200_generate_field_2d.argtypes = [C.c_uint64, _sz, _sz, C.c_int, C.c_double, C.c_double, _vp, _vp]
     L.cpsz_b200_generate_field_3d.argtypes = [C.c_uint64, _sz, _sz, _sz, C.c_int, C.c_double, C.c_double, _vp, _vp, _vp]
     L.cpsz_b200_batch_layout.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp]
+    L.cpsz_b200_huffman_codebook.argtypes = [_vp, _sz, _sz, _vp, _vp, _vp, C.POINTER(_sz)]
+    L.cpsz_b200_huffman_encode_u16.argtypes = [_vp, _vp, _sz, _vp, _vp, _vp, _sz, C.POINTER(C.c_uint64)]
     L.cpsz_b200_zstd_compress.argtypes = [C.c_char_p, _sz, C.c_int, C.POINTER(_vp), C.POINTER(_sz)]
     L.cpsz_b200_zstd_decompress.argtypes = [C.c_char_p, _sz, _vp, _sz]
     for name in ("cpsz_b200_compress_3d_offline_log_f32", "cpsz_b200_decompress_3d_online_log_f32",
@@ -139,8 +141,10 @@ def _ptr(a, dtype=np.float32):
     """(pointer, keepalive, shape) of a host numpy array or a device array."""
     if hasattr(a, "__cuda_array_interface__"):
         cai = a.__cuda_array_interface__
-        if np.dtype(cai["typestr"]) != np.dtype(dtype):
-            raise TypeError(f"expected {np.dtype(dtype)} device array")
+        got, want = np.dtype(cai["typestr"]), np.dtype(dtype)
+        same_int = got.kind in "iu" and want.kind in "iu" and got.itemsize == want.itemsize
+        if got != want and not same_int:
+            raise TypeError(f"expected {want} device array, got {got}")
         if cai.get("strides") not in (None,):
             exp = []
             s = np.dtype(dtype).itemsize
@@ -296,6 +300,34 @@ def cp_check_3d(Ua, Va, Wa, Ub=None, Vb=None, Wb=None, cells: bool = False, ctx:
     if cells:
         res["cells"] = out[:ncell]
     return res
+
+
+# ---- Huffman stage ----------------------------------------------------------------------
+
+def huffman_codebook(hist, state_num: int):
+    """(code[u64], len[u8], tree_section bytes) of the reference's tree for a histogram."""
+    hist = np.ascontiguousarray(hist, np.uint64)
+    bins = hist.size
+    code = np.zeros(bins, np.uint64)
+    ln = np.zeros(bins, np.uint8)
+    size = _sz(0)
+    _check(lib().cpsz_b200_huffman_codebook(hist.ctypes.data, bins, state_num, None, None, None, C.byref(size)))
+    tree = np.zeros(size.value, np.uint8)
+    _check(lib().cpsz_b200_huffman_codebook(hist.ctypes.data, bins, state_num, code.ctypes.data, ln.ctypes.data,
+                                            tree.ctypes.data, C.byref(size)))
+    return code, ln, tree.tobytes()
+
+
+def huffman_encode_u16(sym, code, ln, out, ctx: Context | None = None) -> int:
+    """GPU bit packing of device uint16 symbols with a device codebook into device `out`; returns the bit count."""
+    ps, ks, ss = _ptr(sym, np.uint16)
+    pc, kc, _ = _ptr(code, np.uint64)
+    pl, kl, _ = _ptr(ln, np.uint8)
+    po, ko, so = _ptr(out, np.uint8)
+    bits = C.c_uint64()
+    _check(lib().cpsz_b200_huffman_encode_u16(_h(ctx), ps, int(np.prod(ss)), pc, pl, po, int(np.prod(so)),
+                                              C.byref(bits)))
+    return bits.value
 
 
 # ---- lossless stage (host ZSTD, as the reference) -------------------------------------

@@ -6,6 +6,7 @@
 
 #include "cpsz_b200.h"
 #include "cpsz_b200.hpp"
+#include "huffman_host.h"
 #include "pipeline.h"
 
 // system libzstd.so.1 (linked directly; the image has no zstd.h)
@@ -199,6 +200,48 @@ int cpsz_b200_debug_quant_table(int which, double* t, int* n) {
   const QuantTable& q = which == 3 ? quant_table_3d() : quant_table_2d();
   if (t) memcpy(t, q.t, sizeof(q.t));
   if (n) *n = q.n;
+  return CPSZ_OK;
+}
+
+int cpsz_b200_huffman_codebook(const uint64_t* hist, size_t bins, size_t state_num, uint64_t* code, uint8_t* len,
+                               unsigned char* tree_bytes, size_t* tree_size) {
+  clear_error();
+  if (!hist || !bins || !tree_size) return set_error(CPSZ_ERR_INVALID, "null histogram or tree_size");
+  HuffCodebook cb;
+  if (!huff_build((const unsigned long long*)hist, bins, state_num, &cb)) return CPSZ_ERR_INVALID;
+  if (code) memcpy(code, cb.code.data(), bins * 8);
+  if (len) memcpy(len, cb.len.data(), bins);
+  if (tree_bytes) {
+    if (*tree_size < cb.tree_bytes.size())
+      return set_error(CPSZ_ERR_INVALID, "tree buffer of %zu bytes < %zu", *tree_size, cb.tree_bytes.size());
+    memcpy(tree_bytes, cb.tree_bytes.data(), cb.tree_bytes.size());
+  }
+  *tree_size = cb.tree_bytes.size();
+  return CPSZ_OK;
+}
+
+int cpsz_b200_huffman_encode_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, const uint64_t* code,
+                                 const uint8_t* len, unsigned char* out, size_t out_cap, uint64_t* total_bits) {
+  if (!sym || !code || !len || !out || !total_bits) return set_error(CPSZ_ERR_INVALID, "null pointer argument");
+  if (((uintptr_t)out & 3) != 0) return set_error(CPSZ_ERR_INVALID, "output must be 4-byte aligned");
+  RESOLVE(ctx);
+  CPSZ_TRY(arena_reserve(ctx, huff_encode_tmp_bytes(n) + 1024));
+  CPSZ_TRY(pinned_reserve(ctx, 4096));
+  void* tmp = arena_alloc(ctx, huff_encode_tmp_bytes(n));
+  unsigned long long* d_total = (unsigned long long*)arena_alloc(ctx, 64);
+  CPSZ_CUDA_TRY(cudaMemsetAsync(out, 0, out_cap, ctx->stream));
+  CPSZ_CUDA_TRY(cudaMemsetAsync(d_total, 0, 8, ctx->stream));
+  CPSZ_CUDA_TRY(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+  CPSZ_TRY(launch_huff_encode_u16(ctx, sym, n, HuffEncTable{(const unsigned long long*)code, len, 65536},
+                                  (uint32_t*)out, out_cap, d_total, tmp));
+  unsigned long long* h = (unsigned long long*)ctx->pinned;
+  CPSZ_CUDA_TRY(cudaMemcpyAsync(h, d_total, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CPSZ_CUDA_TRY(cudaMemcpyAsync(h + 1, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CPSZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  *total_bits = h[0];
+  if ((*total_bits + 7) / 8 > out_cap || (*(int*)(h + 1) & FLAG_OUT_CAPACITY))
+    return set_error(CPSZ_ERR_INVALID, "output capacity %zu < %llu bytes", out_cap,
+                     (unsigned long long)((*total_bits + 7) / 8));
   return CPSZ_OK;
 }
 

@@ -103,7 +103,8 @@ __global__ void __launch_bounds__(ENC_NT) enc_write_kernel(const Sym* __restrict
                                                            const unsigned long long* __restrict__ code,
                                                            const uint8_t* __restrict__ len,
                                                            const unsigned long long* __restrict__ cta_off,
-                                                           uint32_t* __restrict__ out, int max_len) {
+                                                           uint32_t* __restrict__ out, size_t cap_words,
+                                                           int* __restrict__ flag) {
   extern __shared__ uint32_t sbuf[];
   __shared__ unsigned int warp_tot[ENC_NT / 32];
   const size_t base = (size_t)blockIdx.x * ENC_PER_CTA;
@@ -151,27 +152,29 @@ __global__ void __launch_bounds__(ENC_NT) enc_write_kernel(const Sym* __restrict
   __syncthreads();
   const size_t w0 = start >> 5;
   for (int k = threadIdx.x; k < nwords; k += ENC_NT) {
+    if (w0 + k >= cap_words) {
+      atomicOr(flag, FLAG_OUT_CAPACITY);
+      break;
+    }
     uint32_t v = bswap32(sbuf[k]);
     if (k == 0 || k == nwords - 1) atomicOr(&out[w0 + k], v);
     else out[w0 + k] = v;
   }
-  (void)max_len;
 }
 
 template <class Sym>
 int encode_impl(cpsz_b200_ctx* ctx, const Sym* sym, size_t n, bool map_id_zero, HuffEncTable tab, uint32_t* out,
-                unsigned long long* d_total_bits, void* tmp) {
+                size_t out_cap_bytes, unsigned long long* d_total_bits, void* tmp) {
   if (n == 0) return CPSZ_OK;
   size_t nb = (n + ENC_PER_CTA - 1) / ENC_PER_CTA;
   unsigned long long* cta_bits = (unsigned long long*)tmp;
   unsigned long long* cta_off = cta_bits + align_up(nb, 32);
   enc_count_kernel<Sym><<<(unsigned)nb, ENC_NT, 0, ctx->stream>>>(sym, n, map_id_zero, tab.len, cta_bits);
   scan_u64_kernel<<<1, 1024, 0, ctx->stream>>>(cta_bits, cta_off, nb);
-  int max_len = 64;
-  size_t smem = ((size_t)ENC_PER_CTA * max_len) / 32 * 4 + 16;
-  // worst case is 32 KB of words for 64-bit codes
+  // shared word buffer for the worst case of 64-bit codes (32 KB)
+  size_t smem = ((size_t)ENC_PER_CTA * 64) / 32 * 4 + 16;
   enc_write_kernel<Sym><<<(unsigned)nb, ENC_NT, smem, ctx->stream>>>(sym, n, map_id_zero, tab.code, tab.len,
-                                                                       cta_off, out, max_len);
+                                                                       cta_off, out, out_cap_bytes / 4, ctx->d_flag);
   if (d_total_bits)
     cudaMemcpyAsync(d_total_bits, cta_off + nb, sizeof(unsigned long long), cudaMemcpyDeviceToDevice, ctx->stream);
   count_launch(ctx, 3);
@@ -332,13 +335,13 @@ size_t huff_encode_tmp_bytes(size_t n) {
 }
 
 int launch_huff_encode_u8(cpsz_b200_ctx* ctx, const uint8_t* sym, size_t n, bool map_id_zero, HuffEncTable tab,
-                          uint32_t* out_words, unsigned long long* d_total_bits, void* tmp) {
-  return encode_impl<uint8_t>(ctx, sym, n, map_id_zero, tab, out_words, d_total_bits, tmp);
+                          uint32_t* out_words, size_t out_cap_bytes, unsigned long long* d_total_bits, void* tmp) {
+  return encode_impl<uint8_t>(ctx, sym, n, map_id_zero, tab, out_words, out_cap_bytes, d_total_bits, tmp);
 }
 
 int launch_huff_encode_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, HuffEncTable tab, uint32_t* out_words,
-                           unsigned long long* d_total_bits, void* tmp) {
-  return encode_impl<uint16_t>(ctx, sym, n, false, tab, out_words, d_total_bits, tmp);
+                           size_t out_cap_bytes, unsigned long long* d_total_bits, void* tmp) {
+  return encode_impl<uint16_t>(ctx, sym, n, false, tab, out_words, out_cap_bytes, d_total_bits, tmp);
 }
 
 int launch_hist_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, unsigned long long* hist) {

@@ -20,6 +20,7 @@ constexpr int FLAG_ID_OVERFLOW = 1;   // an error-bound id does not fit in a byt
 constexpr int FLAG_TIMEOUT = 2;       // a bounded inter-CTA wait gave up
 constexpr int FLAG_HUFF_CORRUPT = 4;  // a Huffman stream does not decode to the expected symbols
 constexpr int FLAG_RAW_RANGE = 8;     // an unpredictable-value index fell outside the stored list
+constexpr int FLAG_OUT_CAPACITY = 16; // an output stream did not fit its buffer
 
 // ---- 2D error bounds ---------------------------------------------------------
 int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, double max_pwr_eb,
@@ -87,10 +88,11 @@ struct HuffEncTable {
 // stream, zero padded, written as bytes at out (device, zero-initialised for
 // ceil(bits/8) bytes rounded up to 4).
 size_t huff_encode_tmp_bytes(size_t n);
+// Words at or beyond out_cap_bytes / 4 are not written (FLAG_OUT_CAPACITY is raised).
 int launch_huff_encode_u8(cpsz_b200_ctx* ctx, const uint8_t* sym, size_t n, bool map_id_zero, HuffEncTable tab,
-                          uint32_t* out_words, unsigned long long* d_total_bits, void* tmp);
+                          uint32_t* out_words, size_t out_cap_bytes, unsigned long long* d_total_bits, void* tmp);
 int launch_huff_encode_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, HuffEncTable tab,
-                           uint32_t* out_words, unsigned long long* d_total_bits, void* tmp);
+                           uint32_t* out_words, size_t out_cap_bytes, unsigned long long* d_total_bits, void* tmp);
 // Histograms (global, 64-bit bins).
 int launch_hist_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, unsigned long long* hist);
 

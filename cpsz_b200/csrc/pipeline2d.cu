@@ -74,6 +74,7 @@ int flag_error(int flag) {
     return set_error(CPSZ_ERR_UNSUPPORTED, "an error-bound id does not fit the 8-bit id stream (max_pwr_eb too large)");
   if (flag & FLAG_HUFF_CORRUPT) return set_error(CPSZ_ERR_FORMAT, "Huffman stream does not decode");
   if (flag & FLAG_RAW_RANGE) return set_error(CPSZ_ERR_FORMAT, "unpredictable-value list shorter than its codes");
+  if (flag & FLAG_OUT_CAPACITY) return set_error(CPSZ_ERR_INVALID, "an output stream exceeded its buffer");
   return CPSZ_OK;
 }
 
@@ -267,10 +268,10 @@ int compress_2d(cpsz_b200_ctx* ctx, const float* U_in, const float* V_in, size_t
     CPSZ_CUDA_TRY(cudaMemsetAsync(d.bits[k], 0, align_up(bits_bytes[k], 4) + 8, st));
   }
   CPSZ_TRY(launch_huff_encode_u8(ctx, d.ids, 2 * N, true, HuffEncTable{d.enc_code[0], d.enc_len[0], 256}, d.bits[0],
-                                 nullptr, d.enc_tmp[0]));
+                                 ids_bits_cap, nullptr, d.enc_tmp[0]));
   for (int f = 0; f < 2; f++)
     CPSZ_TRY(launch_huff_encode_u16(ctx, d.cblocks[f], N, HuffEncTable{d.enc_code[1 + f], d.enc_len[1 + f], 65536},
-                                    d.bits[1 + f], nullptr, d.enc_tmp[1 + f]));
+                                    d.bits[1 + f], codes_bits_cap, nullptr, d.enc_tmp[1 + f]));
 
   mark(ctx, "blob_assembly");
   // ---- stage 5: blob assembly in device memory ----

@@ -104,6 +104,23 @@ int cpsz_b200_compress_2d_stages(cpsz_b200_ctx* ctx, const float* U, const float
                                  double max_pwr_eb, int32_t* ids, int32_t* codes_u, int32_t* codes_v, float* recon_u,
                                  float* recon_v, size_t* n_unpred);
 
+/* ---- SZ-1.x Huffman stage -------------------------------------------------
+ * Codebook of the reference's Huffman tree for a histogram over `bins`
+ * symbols (Huffman_encode_tree_and_data's tree, reference
+ * src/sz_compression_utils.cpp:62-82, src/sz_huffman.cpp:195-215): per symbol
+ * the right-aligned code and its length (0 = absent), and the serialized tree
+ * section (node_count, tree_size, tree bytes) the blob stores before the bits.
+ * Host memory; tree_bytes may be NULL to query *tree_size. */
+int cpsz_b200_huffman_codebook(const uint64_t* hist, size_t bins, size_t state_num, uint64_t* code, uint8_t* len,
+                               unsigned char* tree_bytes, size_t* tree_size);
+/* GPU bit packing of n 16-bit symbols with that codebook (the reference's
+ * encode(), src/sz_huffman.cpp:217-320): writes the MSB-first stream, zero
+ * padded, as bytes at `out` (device, out_cap bytes, 4-byte aligned) and the
+ * stream's bit count to *total_bits (host).  sym, code, len: device memory.
+ * Scratch comes from the context's workspace. */
+int cpsz_b200_huffman_encode_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, const uint64_t* code,
+                                 const uint8_t* len, unsigned char* out, size_t out_cap, uint64_t* total_bits);
+
 /* Size of a 2D offline blob from its header (the reference's decoder takes
  * no length; this lets a caller without one bound the read). */
 size_t cpsz_b200_blob_size_2d(const unsigned char* blob);

@@ -1,0 +1,46 @@
+"""The Huffman stage alone: codebook (host) and GPU bit packing vs the oracle."""
+import numpy as np
+import pytest
+
+import cpsz_b200
+
+pytestmark = pytest.mark.gpu
+
+
+def _streams():
+    rng = np.random.default_rng(3)
+    yield rng.integers(32768 - 40, 32768 + 40, 100_000).astype(np.int32)
+    # a skewed stream with many distinct symbols and long codes
+    yield (32768 + np.round(rng.standard_cauchy(300_000) * 20)).clip(1, 65535).astype(np.int32)
+    yield np.full(5000, 32768, np.int32)  # single symbol: empty bit stream
+    yield rng.integers(0, 65536, 70_000).astype(np.int32)
+
+
+@pytest.mark.parametrize("k", range(4))
+def test_gpu_huffman_matches_oracle(ctx, oracle, k):
+    torch = pytest.importorskip("torch")
+    sym = list(_streams())[k]
+    hist = np.bincount(sym, minlength=65536).astype(np.uint64)
+    code, ln, tree = cpsz_b200.huffman_codebook(hist, 131072)
+    ref = oracle.huffman_encode(131072, sym)
+    assert ref[: len(tree)] == tree
+    nbytes = int.from_bytes(ref[len(tree): len(tree) + 8], "little")
+    d_sym = torch.from_numpy(sym.astype(np.uint16)).cuda()
+    d_code = torch.from_numpy(code.view(np.int64)).cuda()
+    d_len = torch.from_numpy(ln).cuda()
+    out = torch.zeros(nbytes + 64, dtype=torch.uint8, device="cuda")
+    bits = cpsz_b200.huffman_encode_u16(d_sym, d_code, d_len, out, ctx=ctx)
+    assert (bits + 7) // 8 == nbytes
+    assert out[:nbytes].cpu().numpy().tobytes() == ref[len(tree) + 8:]
+
+
+def test_gpu_huffman_rejects_small_output(ctx):
+    torch = pytest.importorskip("torch")
+    sym = np.random.default_rng(1).integers(100, 5000, 50_000).astype(np.int32)
+    hist = np.bincount(sym, minlength=65536).astype(np.uint64)
+    code, ln, tree = cpsz_b200.huffman_codebook(hist, 131072)
+    out = torch.zeros(64, dtype=torch.uint8, device="cuda")
+    with pytest.raises(cpsz_b200.CpszError):
+        cpsz_b200.huffman_encode_u16(torch.from_numpy(sym.astype(np.uint16)).cuda(),
+                                     torch.from_numpy(code.view(np.int64)).cuda(), torch.from_numpy(ln).cuda(), out,
+                                     ctx=ctx)
