@@ -65,6 +65,7 @@ def _declare(L):
     L.cpsz_b200_batch_layout.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp]
     L.cpsz_b200_huffman_codebook.argtypes = [_vp, _sz, _sz, _vp, _vp, _vp, C.POINTER(_sz)]
     L.cpsz_b200_huffman_encode_u16.argtypes = [_vp, _vp, _sz, _vp, _vp, _vp, _sz, C.POINTER(C.c_uint64)]
+    L.cpsz_b200_huffman_encode_u16_noalloc.argtypes = [_vp, _sz, _vp, _vp, _vp, _sz, _vp, _vp]
     L.cpsz_b200_zstd_compress.argtypes = [C.c_char_p, _sz, C.c_int, C.POINTER(_vp), C.POINTER(_sz)]
     L.cpsz_b200_zstd_decompress.argtypes = [C.c_char_p, _sz, _vp, _sz]
     for name in ("cpsz_b200_compress_3d_offline_log_f32", "cpsz_b200_decompress_3d_online_log_f32",
@@ -328,6 +329,18 @@ def huffman_encode_u16(sym, code, ln, out, ctx: Context | None = None) -> int:
     _check(lib().cpsz_b200_huffman_encode_u16(_h(ctx), ps, int(np.prod(ss)), pc, pl, po, int(np.prod(so)),
                                               C.byref(bits)))
     return bits.value
+
+
+def huffman_encode_u16_noalloc(sym, code, ln, out, total_bits, stream: int = 0) -> None:
+    """The allocation-free variant: all arguments are device arrays (total_bits: one uint64);
+    enqueued on `stream` (a cudaStream_t value) without waiting."""
+    ps, ks, ss = _ptr(sym, np.uint16)
+    pc, kc, _ = _ptr(code, np.uint64)
+    pl, kl, _ = _ptr(ln, np.uint8)
+    po, ko, so = _ptr(out, np.uint8)
+    pt, kt, _ = _ptr(total_bits, np.uint64)
+    _check(lib().cpsz_b200_huffman_encode_u16_noalloc(ps, int(np.prod(ss)), pc, pl, po, int(np.prod(so)), pt,
+                                                      stream or None))
 
 
 # ---- lossless stage (host ZSTD, as the reference) -------------------------------------

@@ -22,6 +22,8 @@
 // rounds), then counts are scanned and every thread decodes again, writing its
 // symbols.  Lookup is a 2^12-entry first-level table with a bit-serial tree
 // walk for longer codes.
+#include <mutex>
+
 #include "kernels.h"
 
 namespace cpsz {
@@ -410,4 +412,82 @@ int launch_huff_decode(cpsz_b200_ctx* ctx, const uint8_t* bytes, size_t nbytes, 
   return check_launch("huffman decode");
 }
 
+// ---- Huffman packing without any allocation ---------------------------------------------
+//
+// Some callers cannot allocate device memory at the point where they encode:
+// an in-situ analysis hook running inside a simulation that reserved all GPU
+// memory for its own pool at start-up, a plugin that is only handed
+// preallocated buffers by its host framework, or a real-time loop where a
+// cudaMalloc (which may synchronise the device) is not allowed.  For them
+// this entry point packs a symbol stream with the same kernels as
+// cpsz_b200_huffman_encode_u16 but takes its scratch -- the per-CTA bit
+// counts and their scan -- from a fixed array in this file instead of a
+// context workspace.  The array (about 260 KB) lives on every GPU that loads
+// the library until the process exits, and it bounds the stream length.
+
+constexpr size_t kNoAllocMaxSymbols = size_t(1) << 26;  // 67,108,864 symbols per call
+constexpr size_t kNoAllocMaxCtas = kNoAllocMaxSymbols / ENC_PER_CTA;
+constexpr size_t kNoAllocCounts = kNoAllocMaxCtas + 32;  // per-CTA bit counts (+ padding)
+// layout: [counts: kNoAllocCounts][offsets: kNoAllocMaxCtas + 1][flag word]
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocCounts + kNoAllocMaxCtas + 1 + 1];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+unsigned long long* g_noalloc_addr[64] = {};  // device address of the array, per device
+
+// Resolves the array's device address on the current device (once per device).
+int noalloc_scratch(unsigned long long** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return set_error(CPSZ_ERR_NO_DEVICE, "no CUDA device: %s", cudaGetErrorString(e));
+  if (dev < 0 || dev >= 64) return set_error(CPSZ_ERR_INVALID, "device %d out of range", dev);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      return set_error(CPSZ_ERR_CUDA, "cudaGetSymbolAddress of the no-alloc scratch: %s", cudaGetErrorString(e));
+    g_noalloc_addr[dev] = (unsigned long long*)p;
+  }
+  *out = g_noalloc_addr[dev];
+  return CPSZ_OK;
+}
+
+}  // namespace
+
 }  // namespace cpsz
+
+extern "C" int cpsz_b200_huffman_encode_u16_noalloc(const uint16_t* sym, size_t n, const uint64_t* code,
+                                                    const uint8_t* len, unsigned char* out, size_t out_cap,
+                                                    uint64_t* total_bits, void* stream) {
+  using namespace cpsz;
+  clear_error();
+  if (!sym || !code || !len || !out || !total_bits) return set_error(CPSZ_ERR_INVALID, "null pointer argument");
+  if (((uintptr_t)out & 3) != 0) return set_error(CPSZ_ERR_INVALID, "output must be 4-byte aligned");
+  if (n > kNoAllocMaxSymbols)
+    return set_error(CPSZ_ERR_INVALID, "%zu symbols exceed the no-alloc maximum of %zu symbols per call", n,
+                     kNoAllocMaxSymbols);
+  unsigned long long* scratch = nullptr;
+  CPSZ_TRY(noalloc_scratch(&scratch));
+  cudaStream_t st = (cudaStream_t)stream;
+  unsigned long long* cta_bits = scratch;
+  unsigned long long* cta_off = scratch + kNoAllocCounts;
+  int* flag = (int*)(cta_off + kNoAllocMaxCtas + 1);
+  // the packer ORs the edge words of every CTA: the output starts at zero
+  CPSZ_CUDA_TRY(cudaMemsetAsync(out, 0, out_cap, st));
+  CPSZ_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(unsigned long long), st));
+  if (n == 0) {
+    CPSZ_CUDA_TRY(cudaMemsetAsync(total_bits, 0, sizeof(uint64_t), st));
+    return CPSZ_OK;
+  }
+  const size_t nb = (n + ENC_PER_CTA - 1) / ENC_PER_CTA;
+  enc_count_kernel<uint16_t><<<(unsigned)nb, ENC_NT, 0, st>>>(sym, n, false, len, cta_bits);
+  scan_u64_kernel<<<1, 1024, 0, st>>>(cta_bits, cta_off, nb);
+  const size_t smem = ((size_t)ENC_PER_CTA * 64) / 32 * 4 + 16;
+  enc_write_kernel<uint16_t><<<(unsigned)nb, ENC_NT, smem, st>>>(sym, n, false,
+                                                                 (const unsigned long long*)code, len, cta_off,
+                                                                 (uint32_t*)out, out_cap / 4, flag);
+  CPSZ_CUDA_TRY(cudaMemcpyAsync(total_bits, cta_off + nb, sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
+  return check_launch("huffman no-alloc encode");
+}

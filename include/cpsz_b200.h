@@ -120,6 +120,27 @@ int cpsz_b200_huffman_codebook(const uint64_t* hist, size_t bins, size_t state_n
  * Scratch comes from the context's workspace. */
 int cpsz_b200_huffman_encode_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, const uint64_t* code,
                                  const uint8_t* len, unsigned char* out, size_t out_cap, uint64_t* total_bits);
+/* The same packing for callers that cannot allocate device memory where they
+ * encode -- an in-situ hook inside a simulation that reserved the GPU's memory
+ * for its own pool, a plugin handed only preallocated buffers, a loop where a
+ * possibly synchronising cudaMalloc is not allowed.  This entry point has no
+ * counterpart in the reference.  It calls no allocator: its scratch (per-CTA
+ * bit counts and their scan) is a fixed ~260 KB array inside the library that
+ * every GPU loading it keeps until process exit, which limits n to 67,108,864
+ * symbols per call (larger n is rejected with CPSZ_ERR_INVALID).
+ * All pointers are device memory: sym (n symbols), code/len (codebook from
+ * cpsz_b200_huffman_codebook), out (out_cap bytes, 4-byte aligned, zeroed by
+ * the call), total_bits (one uint64, receives the bit count).  The work is
+ * enqueued on `stream` (a cudaStream_t; NULL = legacy default stream) and the
+ * call returns without waiting; a stream longer than out_cap is cut off at the
+ * capacity, which the caller detects as (*total_bits + 7) / 8 > out_cap.
+ * The first call on a device looks up the scratch array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  All calls on a device share the one array, so
+ * calls whose GPU work overlaps (concurrent streams, threads) race and must be
+ * serialised by the caller. */
+int cpsz_b200_huffman_encode_u16_noalloc(const uint16_t* sym, size_t n, const uint64_t* code, const uint8_t* len,
+                                         unsigned char* out, size_t out_cap, uint64_t* total_bits, void* stream);
 
 /* Size of a 2D offline blob from its header (the reference's decoder takes
  * no length; this lets a caller without one bound the read). */
