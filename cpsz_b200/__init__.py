@@ -72,10 +72,16 @@ def _declare(L):
                  "cpsz_b200_cp_check_2d", "cpsz_b200_cp_check_3d"):
         if hasattr(L, name):
             getattr(L, name).restype = C.c_int
-    if hasattr(L, "cpsz_b200_compress_3d_offline_log_f32"):
-        L.cpsz_b200_compress_3d_offline_log_f32.argtypes = [_vp, _vp, _vp, _vp, _sz, _sz, _sz, C.c_double,
-                                                            C.POINTER(_vp), C.POINTER(_sz)]
-        L.cpsz_b200_decompress_3d_online_log_f32.argtypes = [_vp, C.c_char_p, _sz, _sz, _sz, _sz, _vp, _vp, _vp]
+    L.cpsz_b200_compress_3d_offline_log_f32.argtypes = [_vp, _vp, _vp, _vp, _sz, _sz, _sz, C.c_double,
+                                                        C.POINTER(_vp), C.POINTER(_sz)]
+    L.cpsz_b200_compress_3d_offline_log_f32_into.argtypes = [_vp, _vp, _vp, _vp, _sz, _sz, _sz, C.c_double, _vp, _sz,
+                                                             C.POINTER(_sz)]
+    L.cpsz_b200_decompress_3d_online_log_f32.argtypes = [_vp, C.c_char_p, _sz, _sz, _sz, _sz, _vp, _vp, _vp]
+    L.cpsz_b200_blob_size_3d.argtypes = [C.c_char_p, _sz, _sz, _sz]
+    L.cpsz_b200_blob_size_3d.restype = _sz
+    L.cpsz_b200_libm_tables_prepare.argtypes = [C.c_char_p]
+    L.cpsz_b200_debug_eb3d.argtypes = [_vp, _vp, _vp, _vp, _sz, _sz, _sz, C.c_double, _vp, _vp]
+    L.cpsz_b200_debug_libm.argtypes = [_vp, C.c_int, _vp, _sz, _vp]
     if hasattr(L, "cpsz_b200_cp_check_2d"):
         L.cpsz_b200_cp_check_2d.argtypes = [_vp, _vp, _vp, _vp, _vp, _sz, _sz, _vp, C.POINTER(C.c_uint64)]
         L.cpsz_b200_cp_check_3d.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _sz, _sz, _vp,
@@ -261,6 +267,47 @@ def sz_decompress_cp_preserve_3d_online_log(blob: bytes, r1: int, r2: int, r3: i
     ptrs = [_ptr(a)[0] for a in outs]
     _check(lib().cpsz_b200_decompress_3d_online_log_f32(_h(ctx), blob, len(blob), r1, r2, r3, *ptrs))
     return tuple(outs)
+
+
+def compress_3d_into(U, V, W, r1, r2, r3, max_pwr_eb, out, ctx: Context | None = None) -> int:
+    """3D compression into a caller buffer (numpy uint8 or device array); returns the blob size."""
+    pu, _, _ = _ptr(U)
+    pv, _, _ = _ptr(V)
+    pw, _, _ = _ptr(W)
+    po, _, so = _ptr(out, np.uint8)
+    n = _sz()
+    _check(lib().cpsz_b200_compress_3d_offline_log_f32_into(_h(ctx), pu, pv, pw, r1, r2, r3, float(max_pwr_eb), po,
+                                                            int(np.prod(so)), C.byref(n)))
+    return n.value
+
+
+def blob_size_3d(blob: bytes, r1: int, r2: int, r3: int) -> int:
+    return lib().cpsz_b200_blob_size_3d(blob, r1, r2, r3)
+
+
+def libm_tables_prepare(path: str | None = None) -> None:
+    """Builds (or loads) the host log2f / exp2f tables the 3D kernels use."""
+    _check(lib().cpsz_b200_libm_tables_prepare(path.encode() if path else None))
+
+
+def debug_eb3d(U, V, W, max_pwr_eb: float, ctx: Context | None = None):
+    """Per-vertex 3D bound (float64) and id bytes (255 = bound not positive) from the GPU kernel."""
+    U, V, W = (np.ascontiguousarray(a, np.float32) for a in (U, V, W))
+    r1, r2, r3 = U.shape
+    eb = np.empty(U.shape, np.float64)
+    ids = np.empty(U.shape, np.uint8)
+    _check(lib().cpsz_b200_debug_eb3d(_h(ctx), U.ctypes.data, V.ctypes.data, W.ctypes.data, r1, r2, r3,
+                                      float(max_pwr_eb), eb.ctypes.data, ids.ctypes.data))
+    return eb, ids
+
+
+def debug_libm(which: str, x, ctx: Context | None = None):
+    """The GPU's reproduction of the host library's log2f ('log2f') or exp2f ('exp2f')."""
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.empty_like(x)
+    _check(lib().cpsz_b200_debug_libm(_h(ctx), {"log2f": 0, "exp2f": 1}[which], x.ctypes.data, x.size,
+                                      out.ctypes.data))
+    return out
 
 
 # ---- exact critical-point check ------------------------------------------------------

@@ -86,5 +86,21 @@ def build(verbose: bool = False, extra: list[str] | None = None) -> str:
     return LIB
 
 
+def prepare_tables(verbose: bool = False) -> str:
+    """Generates the host log2f / exp2f tables beside the library (skipped when
+    a cache for this C library version exists); runs in a child process so the
+    build process does not keep the library loaded."""
+    code = ("import ctypes,sys; L=ctypes.CDLL(sys.argv[1]); L.cpsz_b200_libm_tables_prepare.argtypes=[ctypes.c_char_p];"
+            "sys.exit(L.cpsz_b200_libm_tables_prepare(None))")
+    r = subprocess.run([sys.executable, "-c", code, LIB], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"libm table generation failed ({r.returncode}): {r.stderr}")
+    path = os.path.join(LIBDIR, "libm_f32_tables.bin")
+    if verbose:
+        print("tables", path)
+    return path
+
+
 if __name__ == "__main__":
     build(verbose=True)
+    prepare_tables(verbose=True)

@@ -245,6 +245,125 @@ int cpsz_b200_huffman_encode_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t
   return CPSZ_OK;
 }
 
+// ---- 3D ----------------------------------------------------------------------------
+
+int cpsz_b200_compress_3d_offline_log_f32(cpsz_b200_ctx* ctx, const float* U, const float* V, const float* W,
+                                          size_t r1, size_t r2, size_t r3, double max_pwr_eb, unsigned char** blob,
+                                          size_t* blob_size) {
+  if (!blob || !blob_size) return set_error(CPSZ_ERR_INVALID, "null output pointer");
+  *blob = nullptr;
+  *blob_size = 0;
+  RESOLVE(ctx);
+  Blob3D b;
+  CPSZ_TRY(compress_3d(ctx, U, V, W, r1, r2, r3, max_pwr_eb, &b));
+  unsigned char* h = (unsigned char*)malloc(b.size ? b.size : 1);
+  if (!h) return set_error(CPSZ_ERR_NOMEM, "host blob of %zu bytes", b.size);
+  int rc = pinned_reserve(ctx, b.size);
+  if (rc != CPSZ_OK) {
+    free(h);
+    return rc;
+  }
+  cudaError_t e = cudaMemcpyAsync(ctx->pinned, b.d_blob, b.size, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    free(h);
+    return set_error(CPSZ_ERR_CUDA, "blob download: %s", cudaGetErrorString(e));
+  }
+  memcpy(h, ctx->pinned, b.size);
+  *blob = h;
+  *blob_size = b.size;
+  return CPSZ_OK;
+}
+
+int cpsz_b200_compress_3d_offline_log_f32_into(cpsz_b200_ctx* ctx, const float* U, const float* V, const float* W,
+                                               size_t r1, size_t r2, size_t r3, double max_pwr_eb, unsigned char* out,
+                                               size_t out_cap, size_t* blob_size) {
+  if (!out || !blob_size) return set_error(CPSZ_ERR_INVALID, "null output pointer");
+  RESOLVE(ctx);
+  Blob3D b;
+  CPSZ_TRY(compress_3d(ctx, U, V, W, r1, r2, r3, max_pwr_eb, &b));
+  *blob_size = b.size;
+  if (b.size > out_cap) return set_error(CPSZ_ERR_INVALID, "output capacity %zu < blob size %zu", out_cap, b.size);
+  CPSZ_TRY(copy_out(ctx, out, b.d_blob, b.size));
+  CPSZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return CPSZ_OK;
+}
+
+int cpsz_b200_decompress_3d_online_log_f32(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_size,
+                                           size_t r1, size_t r2, size_t r3, float* U, float* V, float* W) {
+  RESOLVE(ctx);
+  CPSZ_TRY(decompress_3d(ctx, blob, blob_size, r1, r2, r3, U, V, W));
+  CPSZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return CPSZ_OK;
+}
+
+size_t cpsz_b200_blob_size_3d(const unsigned char* blob, size_t r1, size_t r2, size_t r3) {
+  if (!blob || !r1 || !r2 || !r3) return 0;
+  const size_t N = r1 * r2 * r3, smap = (N - 1) / 8 + 1;
+  size_t at = 8 + 3 * smap;
+  unsigned long long n_unpred;
+  memcpy(&n_unpred, blob + at, 8);
+  at += 8 + 4 * n_unpred + 8;
+  for (int k = 0; k < 2; k++) {
+    if (k == 1) at += 8;
+    unsigned int tree_size;
+    unsigned long long nbytes;
+    memcpy(&tree_size, blob + at + 8, 4);
+    memcpy(&nbytes, blob + at + 12 + tree_size, 8);
+    at += 12 + (size_t)tree_size + 8 + nbytes;
+  }
+  return at;
+}
+
+int cpsz_b200_debug_eb3d(cpsz_b200_ctx* ctx, const float* U, const float* V, const float* W, size_t r1, size_t r2,
+                         size_t r3, double max_pwr_eb, double* eb_out, uint8_t* id_codes) {
+  RESOLVE(ctx);
+  const size_t N = r1 * r2 * r3;
+  if (!N) return set_error(CPSZ_ERR_INVALID, "empty field");
+  const QuantTable& qt = quant_table_3d();
+  float* dF = nullptr;
+  double *deb = nullptr, *dtab = nullptr;
+  uint8_t* dids = nullptr;
+  CPSZ_CUDA_TRY(cudaMalloc((void**)&dF, 12 * N));
+  CPSZ_CUDA_TRY(cudaMalloc((void**)&deb, 8 * N));
+  CPSZ_CUDA_TRY(cudaMalloc((void**)&dids, N));
+  CPSZ_CUDA_TRY(cudaMalloc((void**)&dtab, QUANT_TAB_MAX * 8));
+  cudaMemcpy(dF, U, 4 * N, cudaMemcpyHostToDevice);
+  cudaMemcpy(dF + N, V, 4 * N, cudaMemcpyHostToDevice);
+  cudaMemcpy(dF + 2 * N, W, 4 * N, cudaMemcpyHostToDevice);
+  cudaMemcpy(dtab, qt.t, QUANT_TAB_MAX * 8, cudaMemcpyHostToDevice);
+  cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream);
+  int rc = launch_eb3d(ctx, dF, dF + N, dF + 2 * N, (int)r1, (int)r2, (int)r3, max_pwr_eb, dtab, qt.n, dids, deb);
+  cudaStreamSynchronize(ctx->stream);
+  if (rc == CPSZ_OK) {
+    if (eb_out) cudaMemcpy(eb_out, deb, 8 * N, cudaMemcpyDeviceToHost);
+    if (id_codes) cudaMemcpy(id_codes, dids, N, cudaMemcpyDeviceToHost);
+  }
+  cudaFree(dF);
+  cudaFree(deb);
+  cudaFree(dids);
+  cudaFree(dtab);
+  return rc;
+}
+
+int cpsz_b200_debug_libm(cpsz_b200_ctx* ctx, int which, const float* in, size_t n, float* out) {
+  RESOLVE(ctx);
+  if (!in || !out || (which != 0 && which != 1)) return set_error(CPSZ_ERR_INVALID, "invalid argument");
+  if (!n) return CPSZ_OK;
+  LibmTables lt;
+  CPSZ_TRY(libm_tables_device(ctx, &lt));
+  float *di = nullptr, *dout = nullptr;
+  CPSZ_CUDA_TRY(cudaMalloc((void**)&di, 4 * n));
+  CPSZ_CUDA_TRY(cudaMalloc((void**)&dout, 4 * n));
+  cudaMemcpy(di, in, 4 * n, cudaMemcpyHostToDevice);
+  int rc = launch_libm_eval(ctx, which, di, n, lt, dout);
+  cudaStreamSynchronize(ctx->stream);
+  if (rc == CPSZ_OK) cudaMemcpy(out, dout, 4 * n, cudaMemcpyDeviceToHost);
+  cudaFree(di);
+  cudaFree(dout);
+  return rc;
+}
+
 size_t cpsz_b200_blob_size_2d(const unsigned char* blob) {
   if (!blob) return 0;
   unsigned long long s[3];
@@ -332,3 +451,67 @@ template unsigned char* sz_compress_cp_preserve_2d_offline<double>(const double*
                                                                    size_t&, bool, double);
 template void sz_decompress_cp_preserve_2d_offline<float>(const unsigned char*, size_t, size_t, float*&, float*&);
 template void sz_decompress_cp_preserve_2d_offline<double>(const unsigned char*, size_t, size_t, double*&, double*&);
+
+template <typename T>
+unsigned char* sz_compress_cp_preserve_3d_offline_log(const T* U, const T* V, const T* W, size_t r1, size_t r2,
+                                                      size_t r3, size_t& compressed_size, bool transpose,
+                                                      double max_pwr_eb) {
+  (void)transpose;  // ignored by the reference as well
+  compressed_size = 0;
+  if (sizeof(T) != sizeof(float)) {
+    set_error(CPSZ_ERR_UNSUPPORTED, "only float fields are supported on the GPU path");
+    return nullptr;
+  }
+  unsigned char* blob = nullptr;
+  size_t size = 0;
+  if (cpsz_b200_compress_3d_offline_log_f32(nullptr, (const float*)U, (const float*)V, (const float*)W, r1, r2, r3,
+                                            max_pwr_eb, &blob, &size) != CPSZ_OK)
+    return nullptr;
+  compressed_size = size;
+  return blob;
+}
+
+template <typename T>
+void sz_decompress_cp_preserve_3d_online_log(const unsigned char* compressed, size_t r1, size_t r2, size_t r3, T*& U,
+                                             T*& V, T*& W) {
+  if (U) free(U);
+  if (V) free(V);
+  if (W) free(W);
+  U = V = W = nullptr;
+  if (sizeof(T) != sizeof(float)) {
+    set_error(CPSZ_ERR_UNSUPPORTED, "only float fields are supported on the GPU path");
+    return;
+  }
+  const size_t n = r1 * r2 * r3;
+  T* u = (T*)malloc(n * sizeof(T));
+  T* v = (T*)malloc(n * sizeof(T));
+  T* w = (T*)malloc(n * sizeof(T));
+  if (!u || !v || !w) {
+    free(u);
+    free(v);
+    free(w);
+    set_error(CPSZ_ERR_NOMEM, "output fields");
+    return;
+  }
+  // The reference reads the blob without a length; the sections it names bound it.
+  const size_t blob_size = cpsz_b200_blob_size_3d(compressed, r1, r2, r3);
+  if (cpsz_b200_decompress_3d_online_log_f32(nullptr, compressed, blob_size, r1, r2, r3, (float*)u, (float*)v,
+                                             (float*)w) != CPSZ_OK) {
+    free(u);
+    free(v);
+    free(w);
+    return;
+  }
+  U = u;
+  V = v;
+  W = w;
+}
+
+template unsigned char* sz_compress_cp_preserve_3d_offline_log<float>(const float*, const float*, const float*, size_t,
+                                                                      size_t, size_t, size_t&, bool, double);
+template unsigned char* sz_compress_cp_preserve_3d_offline_log<double>(const double*, const double*, const double*,
+                                                                       size_t, size_t, size_t, size_t&, bool, double);
+template void sz_decompress_cp_preserve_3d_online_log<float>(const unsigned char*, size_t, size_t, size_t, float*&,
+                                                             float*&, float*&);
+template void sz_decompress_cp_preserve_3d_online_log<double>(const unsigned char*, size_t, size_t, size_t, double*&,
+                                                              double*&, double*&);

@@ -68,7 +68,7 @@ __device__ __forceinline__ double keep_sign_det2x2(float u0, float u1, float u2,
 // The triangle coordinates are compile-time constants of the two triangle
 // kinds; the adjugate entries c[] are passed precomputed (float, exactly as
 // get_adjugate_matrix_for_position produces them, including signed zeros).
-__device__ __noinline__ double keep_sign_eigen(float u0, float u1, float u2, float v0, float v1, float v2, float c0,
+static __device__ __noinline__ double keep_sign_eigen(float u0, float u1, float u2, float v0, float v1, float v2, float c0,
                                                float c1, float c2, float c3) {
   double eb;
   {
@@ -186,7 +186,7 @@ __device__ __forceinline__ bool same_direction(float a, float b, float c, float 
 __device__ __forceinline__ float maxf_(float a, float b) { return (a > b) ? a : b; }
 __device__ __forceinline__ float minf_(float a, float b) { return (a < b) ? a : b; }
 
-__device__ __noinline__ double tet_eb(float u0, float u1, float u2, float u3, float v0, float v1, float v2, float v3,
+static __device__ __noinline__ double tet_eb(float u0, float u1, float u2, float u3, float v0, float v1, float v2, float v3,
                                       float w0, float w1, float w2, float w3) {
   double u3v1w2 = u3 * v1 * w2, u3v2w1 = u3 * v2 * w1, u3v2w0 = u3 * v2 * w0, u3v0w2 = u3 * v0 * w2,
          u3v0w1 = u3 * v0 * w1, u3v1w0 = u3 * v1 * w0;

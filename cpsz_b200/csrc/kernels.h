@@ -4,6 +4,7 @@
 #include <cstddef>
 #include <cstdint>
 
+#include "libm.h"
 #include "runtime.h"
 
 namespace cpsz {
@@ -115,6 +116,42 @@ size_t huff_decode_tmp_bytes(size_t nbits);
 // byte order, padded with >= 8 zero bytes).  Output u8 or u16.
 int launch_huff_decode(cpsz_b200_ctx* ctx, const uint8_t* bytes, size_t nbytes, size_t n, HuffDecTable tab,
                        void* out, int out_bytes_per_sym, void* tmp);
+
+// ---- 3D offline (log) path ----------------------------------------------------------
+// Id written for predictable-bound points that still end unpredictable
+// (id_max = (int)log2(1/FLT_EPSILON) + 1, src/sz_compress_cp_preserve_3d.cpp:436).
+constexpr int ID_RAW_3D = 24;
+// Per-vertex bound (24 tets, reference order) -> id byte (ID_ZERO when the
+// bound is not positive; ids >= ID_RAW_3D raise FLAG_ID_OVERFLOW).  eb_out
+// (optional) receives the bound before quantization.
+int launch_eb3d(cpsz_b200_ctx* ctx, const float* U, const float* V, const float* W, int r1, int r2, int r3,
+                double max_pwr_eb, const double* d_thr, int thr_n, uint8_t* id_q, double* eb_out = nullptr);
+// Log transform: pairs[i] = (log2f|U|, log2f|V|, log2f|W| (-100 for 0), 1/precision
+// or NaN); sign bitmaps (bit 7-(i%8) of byte i/8 = value > 0) as 3 arrays of
+// sign_words 32-bit words.
+int launch_log3d(cpsz_b200_ctx* ctx, const float* U, const float* V, const float* W, const uint8_t* id_q, size_t n,
+                 const LibmFn& L, float4* pairs, uint32_t* signs, size_t sign_words);
+// Host-library log2f (which 0) / exp2f (which 1) of n device floats.
+int launch_libm_eval(cpsz_b200_ctx* ctx, int which, const float* in, size_t n, const LibmTables& L, float* out);
+// Raster compaction in chunks: chunk_count() chunks; counts of predicted
+// points per chunk (compress: codes.x != 0; decompress: id not 0 / ID_RAW_3D).
+size_t chunk_count(size_t n);
+int launch_chunk_count_3d(cpsz_b200_ctx* ctx, bool compress, const void* src, size_t n, unsigned* cnt);
+// Compress: codes_out (3 per predicted point), unpred (U,V,W per other point),
+// ids rewritten in place to the reference's final ids, id histogram.
+int launch_compact3d(cpsz_b200_ctx* ctx, const ushort4* codes, uint8_t* ids, const float* U, const float* V,
+                     const float* W, size_t n, const unsigned* chunk_off, uint16_t* codes_out, float* unpred,
+                     unsigned long long* hist_ids);
+// Decompress: pairs = (3 addends, 0) for predicted points, (3 raw values, raw
+// flag) for the others.  Short streams raise FLAG_RAW_RANGE.
+int launch_prep3d(cpsz_b200_ctx* ctx, const uint8_t* ids, size_t n, const unsigned* chunk_off, const uint16_t* codes,
+                  size_t n_codes, const float* unpred, size_t n_unpred, float4* pairs);
+// Lorenzo recursion, one launch per anti-diagonal plane.  Compress: in =
+// log3d pairs, codes out (0,0,0 for unpredictable points).  Decompress: in =
+// prep3d pairs, decoded U, V, W out.  rec: reconstructed log values (scratch).
+int launch_wave3d_planes(cpsz_b200_ctx* ctx, bool decompress, const float4* in, float4* rec, ushort4* codes,
+                         const uint8_t* signs, size_t sign_bytes, const LibmTables* L, float* U, float* V, float* W,
+                         int r1, int r2, int r3);
 
 // ---- generic scans ----------------------------------------------------------------
 size_t scan_u32_tmp_bytes(size_t n);

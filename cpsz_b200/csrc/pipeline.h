@@ -33,6 +33,17 @@ int compress_2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, s
 int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_size, size_t r1, size_t r2, float* U,
                   float* V);
 
+struct Blob3D {
+  uint8_t* d_blob = nullptr;
+  size_t size = 0;
+  size_t n_unpred = 0;  // floats (3 per unpredictable point)
+  size_t n_codes = 0;   // codes (3 per predicted point)
+};
+int compress_3d(cpsz_b200_ctx* ctx, const float* U, const float* V, const float* W, size_t r1, size_t r2, size_t r3,
+                double max_pwr_eb, Blob3D* out);
+int decompress_3d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_size, size_t r1, size_t r2, size_t r3,
+                  float* U, float* V, float* W);
+
 // Copies n bytes from device memory to `dst`, which may be host or device memory.
 int copy_out(cpsz_b200_ctx* ctx, void* dst, const void* d_src, size_t n);
 // Copies n bytes from `src` (host or device) into device memory `d_dst`.

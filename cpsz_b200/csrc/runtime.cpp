@@ -1,6 +1,8 @@
 // runtime.cpp -- errors, contexts, arenas and host-computed quantization tables.
 #include "runtime.h"
 
+#include "libm.h"
+
 #include <cfloat>
 #include <cmath>
 #include <cstdio>
@@ -265,6 +267,8 @@ int cpsz_b200_ctx_destroy(cpsz_b200_ctx* c) {
   if (c->arena.base) cudaFree(c->arena.base);
   if (c->pinned) cudaFreeHost(c->pinned);
   if (c->d_flag) cudaFree(c->d_flag);
+  if (c->libm_mem) cudaFree(c->libm_mem);
+  delete (cpsz::LibmTables*)c->libm_view;
   for (auto& ev : c->ev)
     if (ev) cudaEventDestroy(ev);
   for (auto& ev : c->tev)

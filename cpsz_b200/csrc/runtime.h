@@ -87,6 +87,9 @@ struct cpsz_b200_ctx {
   // optional wavefront trace (diagnostics): 4 counters per (field, group, warp)
   long long* d_wave_trace = nullptr;
   size_t wave_trace_len = 0;
+  // device copy of the host log2f / exp2f tables (libm.h), uploaded on first use
+  void* libm_mem = nullptr;
+  void* libm_view = nullptr;  // cpsz::LibmTables*
 };
 
 namespace cpsz {

@@ -90,6 +90,19 @@ int cpsz_b200_compress_3d_offline_log_f32(cpsz_b200_ctx* ctx, const float* U, co
  *  src/sz_decompress_cp_preserve_3d.cpp:7-110). */
 int cpsz_b200_decompress_3d_online_log_f32(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_size,
                                            size_t r1, size_t r2, size_t r3, float* U, float* V, float* W);
+/* The 3D compressor writing into a caller buffer `out` (host or device) of
+ * out_cap bytes; *blob_size receives the blob size (also when it does not fit). */
+int cpsz_b200_compress_3d_offline_log_f32_into(cpsz_b200_ctx* ctx, const float* U, const float* V, const float* W,
+                                               size_t r1, size_t r2, size_t r3, double max_pwr_eb, unsigned char* out,
+                                               size_t out_cap, size_t* blob_size);
+/* Size of a 3D blob from its own section headers (the reference's decoder
+ * takes no length). */
+size_t cpsz_b200_blob_size_3d(const unsigned char* blob, size_t r1, size_t r2, size_t r3);
+/* The 3D path reproduces the host C library's log2f / exp2f bit for bit from
+ * tables built by scanning every float input once (about a minute on 8 cores)
+ * and cached in a file (path; NULL = beside the shared library).  Called by the
+ * build; the first 3D call does the same when the cache is missing. */
+int cpsz_b200_libm_tables_prepare(const char* path);
 
 /* ---- stage-level entry point (parity tests, profiling) --------------------
  * Runs the 2D offline compressor and copies out its intermediate streams
@@ -151,6 +164,12 @@ size_t cpsz_b200_blob_size_2d(const unsigned char* blob);
  * doubles) and id bytes (id_codes, 2N; 255 = precision 0).  Host buffers. */
 int cpsz_b200_debug_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2,
                          double max_pwr_eb, double* eb_out, uint8_t* id_codes);
+/* The 3D bound kernel alone: per-vertex bound (N doubles) and id bytes (N;
+ * 255 = bound not positive).  Host buffers. */
+int cpsz_b200_debug_eb3d(cpsz_b200_ctx* ctx, const float* U, const float* V, const float* W, size_t r1, size_t r2,
+                         size_t r3, double max_pwr_eb, double* eb_out, uint8_t* id_codes);
+/* The GPU's host-library log2f (which 0) or exp2f (which 1) of n host floats. */
+int cpsz_b200_debug_libm(cpsz_b200_ctx* ctx, int which, const float* in, size_t n, float* out);
 /* Wavefront trace: with out == NULL, (re)allocates a device trace of len
  * counters (len = 0 disables it); compressions on this context then record,
  * per (field, 256-row group, warp), {start ns, end ns, spins waiting for the

@@ -77,6 +77,8 @@ class Oracle:
         L.cpo_compress_3d_offline_log.restype = C.c_void_p
         L.cpo_decompress_3d_online_log.argtypes = [C.c_char_p, _sz, _sz, _sz, _sz, _f32p, _f32p, _f32p]
         L.cpo_free.argtypes = [C.c_void_p]
+        L.cpo_log2f_array.argtypes = [_f32p, _sz, _f32p]
+        L.cpo_exp2f_array.argtypes = [_f32p, _sz, _f32p]
 
     # -- 2D --
     def eb_2d(self, U, V, eb):
@@ -155,6 +157,14 @@ class Oracle:
         if rc:
             raise ValueError(f"oracle: malformed 3D blob (code {rc})")
         return tuple(out)
+
+    def host_libm(self, which: str, x):
+        """The host C library's log2f ('log2f') or exp2f ('exp2f') of a float array."""
+        x = np.ascontiguousarray(x, np.float32).ravel()
+        out = np.empty_like(x)
+        fn = self.lib.cpo_log2f_array if which == "log2f" else self.lib.cpo_exp2f_array
+        fn(x, x.size, out)
+        return out
 
 
 class Reference:

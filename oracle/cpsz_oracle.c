@@ -445,3 +445,15 @@ int cpo_decompress_2d_offline(const unsigned char* blob, size_t blob_size, size_
 }
 
 void cpo_free(void* p) { free(p); }
+
+/* The host C library's single-precision log2f / exp2f over arrays: the
+ * functions the reference's 3D path calls (include/sz_cp_preserve_utils.hpp:
+ * 201-216, src/sz_decompress_cp_preserve_3d.cpp:95-104), exposed so the GPU's
+ * reproduction can be checked element by element. */
+void cpo_log2f_array(const float* in, size_t n, float* out) {
+  for (size_t i = 0; i < n; i++) out[i] = log2f(in[i]);
+}
+
+void cpo_exp2f_array(const float* in, size_t n, float* out) {
+  for (size_t i = 0; i < n; i++) out[i] = exp2f(in[i]);
+}

@@ -78,6 +78,11 @@ unsigned char* cpo_compress_3d_offline_log(const float* U, const float* V, const
 int cpo_decompress_3d_online_log(const unsigned char* blob, size_t blob_size, size_t r1, size_t r2, size_t r3,
                                  float* U, float* V, float* W);
 
+/* The host C library's log2f / exp2f element-wise (what the reference's 3D
+ * path calls). */
+void cpo_log2f_array(const float* in, size_t n, float* out);
+void cpo_exp2f_array(const float* in, size_t n, float* out);
+
 void cpo_free(void* p);
 
 #ifdef __cplusplus
