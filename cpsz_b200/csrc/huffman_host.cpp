@@ -21,95 +21,71 @@ namespace cpsz {
 
 namespace {
 
-struct Node {
-  unsigned long long freq;
-  int left, right;
-  uint32_t c;
-  bool leaf;
-};
-
+// The heap stores freq << 20 | node in one word (the comparisons look at the
+// frequency only): the reference's exact insertion / removal semantics with
+// one 8-byte load per visited slot.
 class Heap {
  public:
-  Heap(std::vector<Node>& pool, size_t cap) : pool_(pool), q_(cap + 2, -1) {}
-  void insert(int n) {
+  // `storage` keeps its capacity across calls (fresh pages cost a fault each)
+  Heap(std::vector<unsigned long long>& storage, size_t cap) : q_(storage) {
+    if (q_.size() < cap + 2) q_.resize(cap + 2);
+  }
+  void insert(unsigned long long f, int n) {
+    const unsigned long long e = (f << kShift) | (unsigned long long)n;
     int i = end_++, j;
     while ((j = i >> 1)) {
-      if (pool_[q_[j]].freq <= pool_[n].freq) break;
+      if ((q_[j] >> kShift) <= f) break;
       q_[i] = q_[j];
       i = j;
     }
-    q_[i] = n;
+    q_[i] = e;
   }
-  int remove() {
+  // Removes the top entry and returns its key (freq << kShift | node).
+  unsigned long long remove_key() {
     int i = 1, l;
-    int n = q_[1];
+    const unsigned long long n = q_[1];
     end_--;
+    const unsigned long long* q = q_.data();
+    const int lim = (int)q_.size() - 8;
     while ((l = i << 1) < end_) {
-      if (l + 1 < end_ && pool_[q_[l + 1]].freq < pool_[q_[l]].freq) l++;
-      q_[i] = q_[l];
+      // the 8 great-grandchildren share one cache line: fetch it two levels early
+      if (4 * l < lim) __builtin_prefetch(q + 4 * l);
+      // branch-free child choice (the comparison is data-dependent and
+      // mispredicts half the time)
+      l += (int)((l + 1 < end_) & ((q[l + 1] >> kShift) < (q[l] >> kShift)));
+      q_[i] = q[l];
       i = l;
     }
     q_[i] = q_[end_];
     return n;
   }
   int size() const { return end_ - 1; }
-  int top() const { return q_[1]; }
+  int top() const { return (int)(q_[1] & kMask); }
+  static constexpr int kShift = 20;
+  static constexpr unsigned long long kMask = (1ull << kShift) - 1;
 
  private:
-  std::vector<Node>& pool_;
-  std::vector<int> q_;
+  std::vector<unsigned long long>& q_;
   int end_ = 1;
 };
+
+// Per-thread scratch reused by every build on the thread.
+struct Scratch {
+  std::vector<uint32_t> leaf_sym, L, R, C;
+  std::vector<uint8_t> T;
+  std::vector<int> kids;
+  std::vector<unsigned long long> heap;
+};
+Scratch& scratch() {
+  static thread_local Scratch s;
+  return s;
+}
 
 size_t tree_size_for(size_t nodes) {
   if (nodes <= 256) return 1 + 3 * nodes + 4 * nodes;
   if (nodes <= 65536) return 1 + 4 * nodes + nodes + 4 * nodes;
   return 1 + 12 * nodes + nodes;
 }
-
-struct Walker {
-  const std::vector<Node>& pool;
-  const unsigned long long* hist;
-  HuffCodebook* out;
-  std::vector<uint32_t> L, R, C;
-  std::vector<uint8_t> T;
-  uint32_t n_inode = 0;
-  bool too_long = false;
-
-  void codes(int n, int depth, unsigned long long bits) {
-    const Node& nd = pool[n];
-    if (nd.leaf) {
-      if (depth > 64) {
-        too_long = true;
-        return;
-      }
-      out->code[nd.c] = bits;
-      out->len[nd.c] = (uint8_t)depth;
-      if (depth > out->max_len) out->max_len = depth;
-      out->total_bits += hist[nd.c] * (unsigned long long)depth;
-      return;
-    }
-    if (depth >= 64) {
-      too_long = true;
-      return;
-    }
-    codes(nd.left, depth + 1, bits << 1);
-    codes(nd.right, depth + 1, (bits << 1) | 1ull);
-  }
-  void pad(int n, uint32_t i) {
-    const Node& nd = pool[n];
-    C[i] = nd.c;
-    T[i] = nd.leaf ? 1 : 0;
-    if (nd.left >= 0) {
-      L[i] = ++n_inode;
-      pad(nd.left, n_inode);
-    }
-    if (nd.right >= 0) {
-      R[i] = ++n_inode;
-      pad(nd.right, n_inode);
-    }
-  }
-};
 
 template <class T>
 void put(std::vector<uint8_t>& v, size_t& at, T x) {
@@ -120,26 +96,33 @@ void put(std::vector<uint8_t>& v, size_t& at, T x) {
 }  // namespace
 
 bool huff_build(const unsigned long long* hist, size_t bins, size_t state_num, HuffCodebook* out) {
-  size_t distinct = 0;
+  // Leaves are nodes 0..distinct-1 in symbol order (the reference inserts them
+  // that way); merged nodes follow.  Node data lives in two small arrays so
+  // the merge loop and the walk stay cache-resident.
+  Scratch& sc = scratch();
+  std::vector<uint32_t>& leaf_sym = sc.leaf_sym;
+  leaf_sym.clear();
   for (size_t s = 0; s < bins; s++)
-    if (hist[s]) distinct++;
+    if (hist[s]) leaf_sym.push_back((uint32_t)s);
+  const size_t distinct = leaf_sym.size();
   if (distinct == 0) {
     set_error(CPSZ_ERR_INVALID, "Huffman: empty histogram");
     return false;
   }
-  std::vector<Node> pool;
-  pool.reserve(2 * distinct);
-  Heap heap(pool, 2 * distinct);
-  for (size_t s = 0; s < bins; s++) {
-    if (!hist[s]) continue;
-    pool.push_back(Node{hist[s], -1, -1, (uint32_t)s, true});
-    heap.insert((int)pool.size() - 1);
-  }
+  std::vector<int>& kids = sc.kids;  // (left, right) of merged node distinct + m
+  if (kids.size() < 2 * distinct) kids.resize(2 * distinct);
+  Heap heap(sc.heap, 2 * distinct);
+  for (size_t d = 0; d < distinct; d++) heap.insert(hist[leaf_sym[d]], (int)d);
+  int next_node = (int)distinct;
   while (heap.size() > 1) {
-    int first = heap.remove();
-    int second = heap.remove();
-    pool.push_back(Node{pool[second].freq + pool[first].freq, second, first, 0u, false});
-    heap.insert((int)pool.size() - 1);
+    // new_node(0, 0, qremove(), qremove()): the first removal becomes the
+    // right child
+    const unsigned long long first = heap.remove_key();
+    const unsigned long long second = heap.remove_key();
+    const int m = next_node - (int)distinct;
+    kids[2 * m] = (int)(second & Heap::kMask);
+    kids[2 * m + 1] = (int)(first & Heap::kMask);
+    heap.insert((second >> Heap::kShift) + (first >> Heap::kShift), next_node++);
   }
   const int root = heap.top();
   out->code.assign(bins, 0);
@@ -147,26 +130,59 @@ bool huff_build(const unsigned long long* hist, size_t bins, size_t state_num, H
   out->distinct = distinct;
   out->max_len = 0;
   out->total_bits = 0;
-  Walker w{pool, hist, out, {}, {}, {}, {}};
-  w.codes(root, 0, 0);
-  if (w.too_long) {
-    set_error(CPSZ_ERR_UNSUPPORTED, "Huffman code longer than 64 bits");
-    return false;
-  }
   size_t node_count = 0;
   for (size_t s = 0; s < state_num && s < bins; s++)
     if (hist[s]) node_count++;
   node_count = node_count * 2 - 1;
-  const size_t nn = pool.size();
+  const size_t nn = (size_t)next_node;
   if (node_count != nn) {
     set_error(CPSZ_ERR_UNSUPPORTED, "Huffman: symbols beyond state_num");
     return false;
   }
-  w.L.assign(nn, 0);
-  w.R.assign(nn, 0);
-  w.C.assign(nn, 0);
-  w.T.assign(nn, 0);
-  w.pad(root, 0);
+  // One pre-order walk: codes (left 0 / right 1, build_code) and the
+  // serialization's node numbering (pad_tree_*: a node's number is its
+  // pre-order position; L/R hold the children's numbers).
+  std::vector<uint32_t>&L = sc.L, &R = sc.R, &C = sc.C;
+  std::vector<uint8_t>& T = sc.T;
+  L.assign(nn, 0);
+  R.assign(nn, 0);
+  C.assign(nn, 0);
+  T.assign(nn, 0);
+  struct Frame {
+    int node, parent, side, depth;
+    unsigned long long bits;
+  };
+  std::vector<Frame> st;
+  st.reserve(160);
+  st.push_back(Frame{root, -1, 0, 0, 0ull});
+  uint32_t next = 0;
+  while (!st.empty()) {
+    const Frame f = st.back();
+    st.pop_back();
+    const uint32_t i = next++;
+    if (f.parent >= 0) (f.side ? R : L)[f.parent] = i;
+    if (f.node < (int)distinct) {
+      const uint32_t c = leaf_sym[f.node];
+      C[i] = c;
+      T[i] = 1;
+      if (f.depth > 64) {
+        set_error(CPSZ_ERR_UNSUPPORTED, "Huffman code longer than 64 bits");
+        return false;
+      }
+      out->code[c] = f.bits;
+      out->len[c] = (uint8_t)f.depth;
+      if (f.depth > out->max_len) out->max_len = f.depth;
+      out->total_bits += hist[c] * (unsigned long long)f.depth;
+      continue;
+    }
+    if (f.depth >= 64) {
+      set_error(CPSZ_ERR_UNSUPPORTED, "Huffman code longer than 64 bits");
+      return false;
+    }
+    const int m = f.node - (int)distinct;
+    st.push_back(Frame{kids[2 * m + 1], (int)i, 1, f.depth + 1, (f.bits << 1) | 1ull});
+    st.push_back(Frame{kids[2 * m], (int)i, 0, f.depth + 1, f.bits << 1});
+  }
   const size_t tsz = tree_size_for(node_count);
   out->tree_bytes.assign(8 + 4 + tsz, 0);
   size_t at = 0;
@@ -175,15 +191,15 @@ bool huff_build(const unsigned long long* hist, size_t bins, size_t state_num, H
   put<uint8_t>(out->tree_bytes, at, 0);  // sysEndianType
   const int wdt = node_count <= 256 ? 1 : (node_count <= 65536 ? 2 : 4);
   for (int side = 0; side < 2; side++) {
-    const std::vector<uint32_t>& A = side ? w.R : w.L;
+    const std::vector<uint32_t>& A = side ? R : L;
     for (size_t i = 0; i < node_count; i++) {
       if (wdt == 1) put<uint8_t>(out->tree_bytes, at, (uint8_t)A[i]);
       else if (wdt == 2) put<uint16_t>(out->tree_bytes, at, (uint16_t)A[i]);
       else put<uint32_t>(out->tree_bytes, at, A[i]);
     }
   }
-  for (size_t i = 0; i < node_count; i++) put<uint32_t>(out->tree_bytes, at, w.C[i]);
-  for (size_t i = 0; i < node_count; i++) put<uint8_t>(out->tree_bytes, at, w.T[i]);
+  for (size_t i = 0; i < node_count; i++) put<uint32_t>(out->tree_bytes, at, C[i]);
+  for (size_t i = 0; i < node_count; i++) put<uint8_t>(out->tree_bytes, at, T[i]);
   return true;
 }
 
