@@ -186,6 +186,19 @@ __device__ __forceinline__ bool same_direction(float a, float b, float c, float 
 __device__ __forceinline__ float maxf_(float a, float b) { return (a > b) ? a : b; }
 __device__ __forceinline__ float minf_(float a, float b) { return (a < b) ? a : b; }
 
+// (M / Mi > 1) of the reference for nonzero doubles M, Mi, decided exactly
+// without a division: the rounded quotient exceeds 1 iff the exact one
+// exceeds 1 + 2^-53 (1 + 2^-53 itself rounds to the even neighbour 1).
+__device__ __forceinline__ bool quotient_above_one(double M, double Mi) {
+  if (!isfinite(M) || !isfinite(Mi)) return M / Mi > 1;
+  if ((M < 0) != (Mi < 0)) return false;
+  const double a = fabs(M), b = fabs(Mi);
+  if (a > 2.0 * b) return true;
+  if (a < b) return false;
+  // b <= a <= 2b: a - b is exact (Sterbenz), and so is the scaling by 2^53
+  return (a - b) * 9007199254740992.0 > b;
+}
+
 static __device__ __noinline__ double tet_eb(float u0, float u1, float u2, float u3, float v0, float v1, float v2, float v3,
                                       float w0, float w1, float w2, float w3) {
   double u3v1w2 = u3 * v1 * w2, u3v2w1 = u3 * v2 * w1, u3v2w0 = u3 * v2 * w0, u3v0w2 = u3 * v0 * w2,
@@ -206,10 +219,10 @@ static __device__ __noinline__ double tet_eb(float u0, float u1, float u2, float
   double M3 = c_4;
   double M = M0 + M1 + M2 + M3;
   if (M == 0) return 0;
-  bool flag0 = (M0 == 0) || (M / M0 > 1);
-  bool flag1 = (M1 == 0) || (M / M1 > 1);
-  bool flag2 = (M2 == 0) || (M / M2 > 1);
-  bool flag3 = (M3 == 0) || (M / M3 > 1);
+  bool flag0 = (M0 == 0) || quotient_above_one(M, M0);
+  bool flag1 = (M1 == 0) || quotient_above_one(M, M1);
+  bool flag2 = (M2 == 0) || quotient_above_one(M, M2);
+  bool flag3 = (M3 == 0) || quotient_above_one(M, M3);
   if (flag0 && flag1 && flag2 && flag3) {
     if (same_direction(u0, u1, u2, u3) || same_direction(v0, v1, v2, v3) || same_direction(w0, w1, w2, w3)) return 1;
     return 0;
@@ -226,10 +239,39 @@ static __device__ __noinline__ double tet_eb(float u0, float u1, float u2, float
   acc(-u1v0w2, pm3, nm3); acc(u2v0w1, pm3, nm3); acc(-u2v1w0, pm3, nm3);
   float p_m0 = (float)pm0, p_m1 = (float)pm1, p_m2 = (float)pm2, p_m3 = (float)pm3;
   float n_m0 = (float)nm0, n_m1 = (float)nm1, n_m2 = (float)nm2, n_m3 = (float)nm3;
-  if (!flag0) eb = maxf_(eb, minf_(keep_sign_3d(p_m0, n_m0), keep_sign_3d(p_m1 + p_m2 + p_m3, n_m1 + n_m2 + n_m3)));
-  if (!flag1) eb = maxf_(eb, minf_(keep_sign_3d(p_m1, n_m1), keep_sign_3d(p_m0 + p_m2 + p_m3, n_m0 + n_m2 + n_m3)));
-  if (!flag2) eb = maxf_(eb, minf_(keep_sign_3d(p_m2, n_m2), keep_sign_3d(p_m0 + p_m1 + p_m3, n_m0 + n_m1 + n_m3)));
-  if (!flag3) eb = maxf_(eb, minf_(keep_sign_3d(p_m3, n_m3), keep_sign_3d(p_m0 + p_m1 + p_m2, n_m0 + n_m1 + n_m2)));
+  // the "other three minors" sums, in the reference's left-to-right order
+  const float sp0 = p_m1 + p_m2 + p_m3, sn0 = n_m1 + n_m2 + n_m3;
+  const float sp1 = p_m0 + p_m2 + p_m3, sn1 = n_m0 + n_m2 + n_m3;
+  const float sp2 = p_m0 + p_m1 + p_m3, sn2 = n_m0 + n_m1 + n_m3;
+  const float sp3 = p_m0 + p_m1 + p_m2, sn3 = n_m0 + n_m1 + n_m2;
+  if (isfinite(sp0) && isfinite(sp1) && isfinite(sp2) && isfinite(sp3) && isfinite(sn0) && isfinite(sn1) &&
+      isfinite(sn2) && isfinite(sn3)) {
+    // Every magnitude is finite (each appears in three of the sums), so every
+    // keep_sign_3d value is a finite non-negative float and MAX/MINF are plain
+    // max/min: a flag whose first bound cannot raise eb leaves it unchanged,
+    // and its second bound need not be evaluated.
+    if (!flag0) {
+      const float e1 = keep_sign_3d(p_m0, n_m0);
+      if (e1 > eb) eb = maxf_(eb, minf_(e1, keep_sign_3d(sp0, sn0)));
+    }
+    if (!flag1) {
+      const float e1 = keep_sign_3d(p_m1, n_m1);
+      if (e1 > eb) eb = maxf_(eb, minf_(e1, keep_sign_3d(sp1, sn1)));
+    }
+    if (!flag2) {
+      const float e1 = keep_sign_3d(p_m2, n_m2);
+      if (e1 > eb) eb = maxf_(eb, minf_(e1, keep_sign_3d(sp2, sn2)));
+    }
+    if (!flag3) {
+      const float e1 = keep_sign_3d(p_m3, n_m3);
+      if (e1 > eb) eb = maxf_(eb, minf_(e1, keep_sign_3d(sp3, sn3)));
+    }
+    return eb;
+  }
+  if (!flag0) eb = maxf_(eb, minf_(keep_sign_3d(p_m0, n_m0), keep_sign_3d(sp0, sn0)));
+  if (!flag1) eb = maxf_(eb, minf_(keep_sign_3d(p_m1, n_m1), keep_sign_3d(sp1, sn1)));
+  if (!flag2) eb = maxf_(eb, minf_(keep_sign_3d(p_m2, n_m2), keep_sign_3d(sp2, sn2)));
+  if (!flag3) eb = maxf_(eb, minf_(keep_sign_3d(p_m3, n_m3), keep_sign_3d(sp3, sn3)));
   return eb;
 }
 

@@ -34,7 +34,7 @@ __constant__ int8_t c_tet[6][3][3] = {{{0, 0, 1}, {0, 1, 1}, {1, 1, 1}}, {{0, 1,
 
 __device__ __forceinline__ double min_ref(double s, double cur) { return (s < cur) ? s : cur; }
 
-__global__ void __launch_bounds__(EB_NT) eb3d_kernel(const float* __restrict__ U, const float* __restrict__ V,
+__global__ void __launch_bounds__(EB_NT, 3) eb3d_kernel(const float* __restrict__ U, const float* __restrict__ V,
                                                      const float* __restrict__ W, int r1, int r2, int r3,
                                                      int i_chunk, double max_pwr_eb, const double* __restrict__ thr,
                                                      int thr_n, uint8_t* __restrict__ id_q,

@@ -35,13 +35,20 @@ def assert_blob_equal_2d(a: bytes, b: bytes):
     assert bad.size == 0, f"{bad.size} bytes differ, first at {bad[:8].tolist()}"
 
 
-def assert_bits_equal(a, b):
+def assert_bits_equal(a, b, nan_equal: bool = False):
+    """Bit-pattern equality of two arrays.  nan_equal: any NaN matches any NaN
+    (for intermediate bounds, where only NaN-ness reaches the output: x86 and
+    the GPU encode the NaN of an invalid operation differently)."""
     a = np.ascontiguousarray(a)
     b = np.ascontiguousarray(b)
     assert a.shape == b.shape and a.dtype == b.dtype
-    va = a.view(np.uint32) if a.dtype == np.float32 else a
-    vb = b.view(np.uint32) if b.dtype == np.float32 else b
-    bad = np.nonzero(va.ravel() != vb.ravel())[0]
+    views = {np.dtype(np.float32): np.uint32, np.dtype(np.float64): np.uint64}
+    va = a.view(views[a.dtype]) if a.dtype in views else a
+    vb = b.view(views[b.dtype]) if b.dtype in views else b
+    diff = va.ravel() != vb.ravel()
+    if nan_equal and a.dtype in views:
+        diff &= ~(np.isnan(a.ravel()) & np.isnan(b.ravel()))
+    bad = np.nonzero(diff)[0]
     assert bad.size == 0, f"{bad.size} of {a.size} values differ, first at {bad[:8].tolist()}"
 
 

@@ -142,3 +142,22 @@ def test_gpu_3d_rejects_bad_input(ctx):
     F = [np.ones((1, 6, 6), np.float32) for _ in range(3)]
     with pytest.raises(cpsz_b200.CpszError):
         cpsz_b200.sz_compress_cp_preserve_3d_offline_log(*F, max_pwr_eb=5.0, ctx=ctx)
+
+
+def test_gpu_eb3d_nonfinite_and_overflow(ctx, oracle):
+    """Triple products that overflow float, and NaN / inf inputs: the bound
+    kernel's division-free and pruned paths fall back exactly."""
+    rng = np.random.default_rng(8)
+    shape = (9, 10, 11)
+    U, V, Wf = (rng.normal(size=shape).astype(np.float32) for _ in range(3))
+    U[2:4] *= 3e13  # products beyond FLT_MAX
+    V[:, 5] *= 1e30
+    Wf[5, 5, 5] = np.nan
+    U[7, 1, 2] = np.inf
+    for eb in (0.1, 0.9):
+        e, ids = cpsz_b200.debug_eb3d(U, V, Wf, eb, ctx=ctx)
+        ref = oracle.eb_3d(U, V, Wf, eb)
+        assert np.isnan(ref).any()
+        assert_bits_equal(e, ref, nan_equal=True)
+        assert np.array_equal(ids == 255, ~(ref > 0))
+    _check_roundtrip(ctx, oracle, U, V, Wf, 0.1)
