@@ -364,6 +364,92 @@ int cpsz_b200_debug_libm(cpsz_b200_ctx* ctx, int which, const float* in, size_t 
   return rc;
 }
 
+// ---- exact critical-point checker ----------------------------------------------------
+
+namespace {
+
+// Device copies of up to six fields (host inputs are uploaded; device ones used in place).
+struct CpInputs {
+  const float* d[6] = {};
+  std::vector<void*> owned;
+  ~CpInputs() {
+    for (void* p : owned) cudaFree(p);
+  }
+  int stage(cpsz_b200_ctx* ctx, const float* const* in, int k, size_t n) {
+    for (int f = 0; f < k; f++) {
+      if (!in[f]) continue;
+      if (is_device_ptr(in[f])) {
+        d[f] = in[f];
+        continue;
+      }
+      void* p = nullptr;
+      CPSZ_CUDA_TRY(cudaMalloc(&p, 4 * n));
+      owned.push_back(p);
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(p, in[f], 4 * n, cudaMemcpyHostToDevice, ctx->stream));
+      d[f] = (const float*)p;
+    }
+    return CPSZ_OK;
+  }
+};
+
+int cp_check_run(cpsz_b200_ctx* ctx, int dims, const float* const* in, const size_t* r, uint8_t* cells_out,
+                 uint64_t counts[4]) {
+  const size_t n = r[0] * r[1] * (dims == 3 ? r[2] : 1);
+  if (!n) return set_error(CPSZ_ERR_INVALID, "empty field");
+  for (int k = 0; k < dims; k++)
+    if (r[k] > (1u << 30)) return set_error(CPSZ_ERR_UNSUPPORTED, "dimension %zu too large", r[k]);
+  const int nf = dims;  // fields per set
+  for (int f = 0; f < nf; f++)
+    if (!in[f]) return set_error(CPSZ_ERR_INVALID, "null field a");
+  const bool with_b = in[nf] != nullptr;
+  for (int f = 0; f < nf; f++)
+    if (with_b != (in[nf + f] != nullptr)) return set_error(CPSZ_ERR_INVALID, "field b given partially");
+  size_t ncell = 1;
+  for (int k = 0; k < dims; k++) ncell *= (r[k] > 1 ? r[k] - 1 : 0);
+  ncell *= (dims == 3 ? 6 : 2);
+  CpInputs ci;
+  CPSZ_TRY(ci.stage(ctx, in, 2 * nf, n));
+  CPSZ_TRY(arena_reserve(ctx, ncell + 4096));
+  CPSZ_TRY(pinned_reserve(ctx, 4096));
+  unsigned long long* d_counts = (unsigned long long*)arena_alloc(ctx, 64);
+  uint8_t* d_cells = nullptr;
+  const bool cells_dev = cells_out && is_device_ptr(cells_out);
+  if (cells_out) d_cells = cells_dev ? cells_out : (uint8_t*)arena_alloc(ctx, ncell + 16);
+  CPSZ_CUDA_TRY(cudaMemsetAsync(d_counts, 0, 64, ctx->stream));
+  if (dims == 2)
+    CPSZ_TRY(launch_cp_check_2d(ctx, ci.d[0], ci.d[1], ci.d[2], ci.d[3], (int)r[0], (int)r[1], d_cells, d_counts));
+  else
+    CPSZ_TRY(launch_cp_check_3d(ctx, ci.d[0], ci.d[1], ci.d[2], ci.d[3], ci.d[4], ci.d[5], (int)r[0], (int)r[1],
+                                (int)r[2], d_cells, d_counts));
+  if (cells_out && !cells_dev && ncell)
+    CPSZ_CUDA_TRY(cudaMemcpyAsync(cells_out, d_cells, ncell, cudaMemcpyDeviceToHost, ctx->stream));
+  unsigned long long* h = (unsigned long long*)ctx->pinned;
+  CPSZ_CUDA_TRY(cudaMemcpyAsync(h, d_counts, 32, cudaMemcpyDeviceToHost, ctx->stream));
+  CPSZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  if (counts)
+    for (int k = 0; k < 4; k++) counts[k] = h[k];
+  return CPSZ_OK;
+}
+
+}  // namespace
+
+int cpsz_b200_cp_check_2d(cpsz_b200_ctx* ctx, const float* Ua, const float* Va, const float* Ub, const float* Vb,
+                          size_t r1, size_t r2, uint8_t* cells_out, uint64_t counts[4]) {
+  RESOLVE(ctx);
+  const float* in[4] = {Ua, Va, Ub, Vb};
+  const size_t r[2] = {r1, r2};
+  return cp_check_run(ctx, 2, in, r, cells_out, counts);
+}
+
+int cpsz_b200_cp_check_3d(cpsz_b200_ctx* ctx, const float* Ua, const float* Va, const float* Wa, const float* Ub,
+                          const float* Vb, const float* Wb, size_t r1, size_t r2, size_t r3, uint8_t* cells_out,
+                          uint64_t counts[4]) {
+  RESOLVE(ctx);
+  const float* in[6] = {Ua, Va, Wa, Ub, Vb, Wb};
+  const size_t r[3] = {r1, r2, r3};
+  return cp_check_run(ctx, 3, in, r, cells_out, counts);
+}
+
 size_t cpsz_b200_blob_size_2d(const unsigned char* blob) {
   if (!blob) return 0;
   unsigned long long s[3];

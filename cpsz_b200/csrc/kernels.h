@@ -153,6 +153,16 @@ int launch_wave3d_planes(cpsz_b200_ctx* ctx, bool decompress, const float4* in, 
                          const uint8_t* signs, size_t sign_bytes, const LibmTables* L, float* U, float* V, float* W,
                          int r1, int r2, int r3);
 
+// ---- exact critical-point checker -----------------------------------------------------
+// Per-cell CP codes of field a (0 none, 1 + type) into `cells` (optional,
+// device) and counts[0..3] += {CPs in a, CPs in b, cells with a CP in exactly
+// one field, cells whose CP type differs}; b may be null.
+int launch_cp_check_2d(cpsz_b200_ctx* ctx, const float* Ua, const float* Va, const float* Ub, const float* Vb, int r1,
+                       int r2, uint8_t* cells, unsigned long long* counts);
+int launch_cp_check_3d(cpsz_b200_ctx* ctx, const float* Ua, const float* Va, const float* Wa, const float* Ub,
+                       const float* Vb, const float* Wb, int r1, int r2, int r3, uint8_t* cells,
+                       unsigned long long* counts);
+
 // ---- generic scans ----------------------------------------------------------------
 size_t scan_u32_tmp_bytes(size_t n);
 // Exclusive scan of n u32 values into out (n+1 entries, out[n] = total).
