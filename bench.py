@@ -50,6 +50,8 @@ WORKLOADS = {
     "3d_384x384x384_eb0.05": ("3d", (384, 384, 384), 0.05, "cfg2"),
     # profiling-size case of the 3D kernels (cfg2 generator at 256^3, 201 MB > L2)
     "3d_256x256x256_eb0.05": ("3d", (256, 256, 256), 0.05, "cfg2"),
+    # 256 fields, sides uniform in [128, 4096], eb in {0.01, 0.05, 0.1}, one flow per 40x40 cells
+    "batch_256x2d_cfg3": ("batch", None, None, "cfg3"),
 }
 DEFAULT = "2d_8192x8192_eb0.1"
 
@@ -177,10 +179,19 @@ def run_reference(args, rank, world):
 
     if rank != 0:
         return None
-    fields, eb = make_fields(args.workload)
     kind = WORKLOADS[args.workload][0]
     use_ref = os.path.exists(oracle.REF_SO)
-    tiles = reference_samples(args.workload, fields, eb)
+    if kind == "batch":
+        # whole fields of the batch (the smaller ones), each with its own bound
+        bf, bebs = make_batch()
+        order = sorted(range(len(bf)), key=lambda k: bf[k][0].size)
+        tiles = [bf[k] for k in order if bf[k][0].size <= 1_500_000]
+        tile_ebs = [bebs[k] for k in order if bf[k][0].size <= 1_500_000]
+        kind = "2d"
+    else:
+        fields, eb = make_fields(args.workload)
+        tiles = reference_samples(args.workload, fields, eb)
+        tile_ebs = [eb] * len(tiles)
     cores = os.cpu_count() or 1
     tmp = tempfile.mkdtemp(prefix="cpsz_ref_")
     paths = []
@@ -195,7 +206,7 @@ def run_reference(args, rank, world):
     times = []
     total_bytes = 0
     with ctxm.Pool(cores) as pool:
-        jobs = [(kind, p, eb, use_ref) for p in paths[:cores]]
+        jobs = [(kind, p, tile_ebs[k], use_ref) for k, p in enumerate(paths[:cores])]
         for step in range(args.warmup + args.steps):
             t0 = time.perf_counter()
             res = pool.map(_ref_worker, jobs)
@@ -205,8 +216,9 @@ def run_reference(args, rank, world):
                 total_bytes = sum(np.load(p, mmap_mode="r").nbytes for job in jobs for p in job[1])
     per_step = statistics.mean(times)
     gbs = total_bytes / per_step / 1e9
-    sample = (f"{len(jobs)} independent {'1024x1024' if kind == '2d' else '96^3'} tiles of the workload, "
-              f"one per process, compressed concurrently per step")
+    what = ("whole fields of the batch (up to 1.5M points each)" if WORKLOADS[args.workload][0] == "batch"
+            else f"{'1024x1024' if kind == '2d' else '96^3'} tiles of the workload")
+    sample = f"{len(jobs)} independent {what}, one per process, compressed concurrently per step"
     line = {
         "impl": "reference", "metric": "compress_GBps", "value": round(gbs, 4), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(per_step * 1e3, 3),
@@ -351,6 +363,85 @@ def run_product(args, rank, world, device):
     }
 
 
+def make_batch(seed_offset: int = 0):
+    from cpsz_b200 import workloads as W
+
+    lay = W.batch_layout(3 + 1000 * seed_offset, 256, 128, 4096)
+    fields = [W.cfg3_field(r1, r2, sd) for r1, r2, sd, _ in lay]
+    return fields, [eb for *_, eb in lay]
+
+
+def run_batch(args, rank, world, device):
+    """The batched workload: every step compresses all 256 fields with one
+    batched call (fields resident in HBM, blobs written to HBM); the same
+    fields through one single-field call each, and end to end from host
+    memory, are reported beside it."""
+    import torch
+
+    import cpsz_b200
+
+    fields, ebs = make_batch(rank)
+    raw = sum(U.nbytes + V.nbytes for U, V in fields)
+    ctx = cpsz_b200.Context(device)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=device)
+    dev = [(torch.from_numpy(U).to(f"cuda:{device}"), torch.from_numpy(V).to(f"cuda:{device}")) for U, V in fields]
+    out = torch.empty(raw + (256 << 20), dtype=torch.uint8, device=f"cuda:{device}")
+    clk = Clocks(device).__enter__()
+    for _ in range(args.warmup):
+        offsets = cpsz_b200.compress_2d_batch(dev, ebs, out=out, ctx=ctx)
+    torch.cuda.synchronize(device)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    launches0 = ctx.kernel_launches
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    try:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            offsets = cpsz_b200.compress_2d_batch(dev, ebs, out=out, ctx=ctx)
+        ev1.record(stream)
+        torch.cuda.synchronize(device)
+    finally:
+        clk.__exit__(None, None, None)
+    launches = (ctx.kernel_launches - launches0) // max(args.steps, 1)
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([ms], device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    blob_bytes = int(offsets[-1])
+    # one single-field call per field, same device-resident fields
+    ev0.record(stream)
+    for (u, v), eb in zip(dev, ebs):
+        cpsz_b200.compress_2d_into(u, v, u.shape[0], u.shape[1], eb, out, ctx=ctx)
+    ev1.record(stream)
+    torch.cuda.synchronize(device)
+    per_field_ms = ev0.elapsed_time(ev1)
+    # end to end: host fields in, blobs into pinned host memory
+    h_out = torch.empty(raw + (256 << 20), dtype=torch.uint8).pin_memory().numpy()
+    cpsz_b200.compress_2d_batch(fields, ebs, out=h_out, ctx=ctx)
+    t0 = time.perf_counter()
+    cpsz_b200.compress_2d_batch(fields, ebs, out=h_out, ctx=ctx)
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+    return {
+        "metric": "compress_GBps", "value": round(raw * world / (ms / 1e3) / 1e9, 3), "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
+        "config": {"workload": args.workload, "fields": len(fields), "points": int(raw // 8),
+                   "inputs_exceed_l2": True, "parallelism": f"replicas{world}",
+                   "value_io": "fields resident in HBM, blobs written to HBM"},
+        "ratio_pre_zstd": round(raw / blob_bytes, 4),
+        "per_field_calls_GBps": round(raw / (per_field_ms / 1e3) / 1e9, 3),
+        "e2e": {"value": round(raw / (e2e_ms / 1e3) / 1e9, 3), "unit": "GB/s", "h2d_bytes_per_step": raw,
+                "d2h_bytes_per_step": blob_bytes, "host_input": "pageable numpy arrays"},
+        "cpu_baseline": None, "clocks": clk.summary(), "gpu_launches": launches,
+    }
+
+
 def stage_times(ctx):
     import ctypes as C
 
@@ -393,6 +484,16 @@ def main():
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if WORKLOADS[args.workload][0] == "batch":
+        line = run_batch(args, rank, world, local)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(line))
+        return
     r = run_product(args, rank, world, local)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

@@ -72,6 +72,7 @@ def _declare(L):
                  "cpsz_b200_cp_check_2d", "cpsz_b200_cp_check_3d"):
         if hasattr(L, name):
             getattr(L, name).restype = C.c_int
+    L.cpsz_b200_compress_2d_batch_f32.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp]
     L.cpsz_b200_compress_3d_offline_log_f32.argtypes = [_vp, _vp, _vp, _vp, _sz, _sz, _sz, C.c_double,
                                                         C.POINTER(_vp), C.POINTER(_sz)]
     L.cpsz_b200_compress_3d_offline_log_f32_into.argtypes = [_vp, _vp, _vp, _vp, _sz, _sz, _sz, C.c_double, _vp, _sz,
@@ -195,6 +196,40 @@ def compress_2d_into(U, V, r1, r2, max_pwr_eb, out, ctx: Context | None = None) 
     _check(lib().cpsz_b200_compress_2d_offline_f32_into(_h(ctx), pu, pv, r1, r2, float(max_pwr_eb), po,
                                                         int(np.prod(so)), C.byref(n)))
     return n.value
+
+
+def compress_2d_batch(fields, ebs, out=None, ctx: Context | None = None):
+    """Batched 2D compression of [(U, V), ...] with per-field bounds.
+
+    With out=None returns the list of blobs (bytes); with `out` (host numpy
+    uint8 or device uint8 array) writes them back to back and returns the
+    offsets array (n + 1 entries)."""
+    n = len(fields)
+    ptrs_u = (_vp * max(n, 1))()
+    ptrs_v = (_vp * max(n, 1))()
+    r1 = np.zeros(max(n, 1), np.uint64)
+    r2 = np.zeros(max(n, 1), np.uint64)
+    keep = []
+    for k, (U, V) in enumerate(fields):
+        pu, _, su = _ptr(U)
+        pv, _, sv = _ptr(V)
+        if su != sv or len(su) != 2:
+            raise ValueError("each field is a pair of equal 2D arrays")
+        ptrs_u[k], ptrs_v[k] = pu, pv
+        r1[k], r2[k] = su
+        keep.append((U, V))
+    ebs = np.ascontiguousarray(np.broadcast_to(np.asarray(ebs, np.float64), (n,)))
+    ret_bytes = out is None
+    if out is None:
+        cap = sum(int(a.size) * 8 for a, _ in fields) * 2 + n * (4 << 20) + (1 << 20)
+        out = np.empty(cap, np.uint8)
+    po, _, so = _ptr(out, np.uint8)
+    offsets = np.zeros(n + 1, np.uint64)
+    _check(lib().cpsz_b200_compress_2d_batch_f32(_h(ctx), n, ptrs_u, ptrs_v, r1.ctypes.data, r2.ctypes.data,
+                                                 ebs.ctypes.data, po, int(np.prod(so)), offsets.ctypes.data))
+    if ret_bytes:
+        return [out[int(offsets[k]):int(offsets[k + 1])].tobytes() for k in range(n)]
+    return offsets
 
 
 def sz_decompress_cp_preserve_2d_offline(blob: bytes, r1: int, r2: int, U=None, V=None,

@@ -245,6 +245,15 @@ int cpsz_b200_huffman_encode_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t
   return CPSZ_OK;
 }
 
+int cpsz_b200_compress_2d_batch_f32(cpsz_b200_ctx* ctx, int n_fields, const float* const* U, const float* const* V,
+                                    const size_t* r1, const size_t* r2, const double* max_pwr_eb, unsigned char* out,
+                                    size_t out_cap, size_t* offsets) {
+  RESOLVE(ctx);
+  CPSZ_TRY(compress_2d_batch(ctx, n_fields, U, V, r1, r2, max_pwr_eb, out, out_cap, offsets));
+  CPSZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return CPSZ_OK;
+}
+
 // ---- 3D ----------------------------------------------------------------------------
 
 int cpsz_b200_compress_3d_offline_log_f32(cpsz_b200_ctx* ctx, const float* U, const float* V, const float* W,

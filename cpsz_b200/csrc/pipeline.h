@@ -32,6 +32,9 @@ int compress_2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, s
                 Blob2D* out, const StageTap* tap);
 int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_size, size_t r1, size_t r2, float* U,
                   float* V);
+// n fields; blobs back to back into `out` (host or device), offsets[0..n].
+int compress_2d_batch(cpsz_b200_ctx* ctx, int n, const float* const* U, const float* const* V, const size_t* r1,
+                      const size_t* r2, const double* ebs, unsigned char* out, size_t out_cap, size_t* offsets);
 
 struct Blob3D {
   uint8_t* d_blob = nullptr;

@@ -8,6 +8,12 @@
 //   -> blob assembled in device memory -> one copy to the caller.
 // The id tree is built on the host while the wavefront runs.
 //
+// Batches (compress_2d_batch) run in passes of up to 32 fields: every stage
+// is issued for all fields of the pass, the wavefront is one persistent
+// launch over all of them (its work queue interleaves the fields' row
+// groups), and the host builds the pass's Huffman trees on all host threads.
+// A single-field call is a pass of one field.
+//
 // Decompress (sz_decompress_cp_preserve_2d_offline<float>,
 // src/sz_decompress_cp_preserve_2d.cpp:8-52): host header/tree parsing ->
 // GPU Huffman decode of ids and codes -> raster permutation, unpredictable
@@ -18,8 +24,11 @@
 //   | HUF(ids, 2048 states, 2N) | FIELD(U) | FIELD(V)
 //   FIELD = int 12 | char 0 | int 32768 | meanInfo<float>{false,0} (8 B) | size_t 0
 //         | size_t n_unpred | float[n_unpred] | ceil(nblocks/8) zero bytes | HUF(codes, 131072 states, N)
+#include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "huffman_host.h"
@@ -33,9 +42,15 @@ namespace {
 constexpr int BS = 12;
 constexpr size_t FIELD_HDR = 4 + 1 + 4 + 8 + 8 + 8;  // up to and including n_unpred
 constexpr size_t BLOB_HDR = 4 + 8 + 8 + 8 + 8;
+// pinned staging per field: id histogram, two code histograms, unpredictable counts
+constexpr size_t JOB_PINNED = (256 + 2 * 65536) * 8 + 64;
+constexpr size_t PINNED_BASE = 4096;  // the flag word and scalars live below
+// sub-batch limits: fields per pass (pinned staging) and points per pass (workspace)
+constexpr int BATCH_MAX_FIELDS = 32;
+constexpr size_t BATCH_MAX_POINTS = (size_t)1 << 27;
 
 struct DevBuf {
-  // arena sub-allocations of one compress call
+  // arena sub-allocations of one field
   float* U;
   float* V;
   uint8_t* ids;  // 2N: U ids then V ids
@@ -45,20 +60,35 @@ struct DevBuf {
   uint16_t* cblocks[2];
   unsigned long long* hist_codes[2];
   unsigned long long* gbnd;
-  int* queue;
-  WaveField* fields;
-  WaveItem* items;
   unsigned int* seg_cnt[2];
   unsigned int* seg_off[2];
   void* scan_tmp[2];
   float* unpred[2];
-  double* thr_tab;
   unsigned long long* enc_code[3];
   uint8_t* enc_len[3];
   void* enc_tmp[3];
   uint32_t* bits[3];
-  unsigned long long* bits_total;
   uint8_t* blob;
+};
+
+// One field of a compression pass (a pass holds one or more fields).
+struct Job2D {
+  const float* U_in = nullptr;
+  const float* V_in = nullptr;
+  int r1 = 0, r2 = 0, ngroups = 0;
+  size_t N = 0, nseg = 0, nblocks = 0;
+  double eb = 0;
+  bool dev_in = false;
+  size_t ids_bits_cap = 0, codes_bits_cap = 0, blob_cap = 0;
+  DevBuf d{};
+  unsigned long long* h_hist_ids = nullptr;    // pinned
+  unsigned long long* h_hist_codes = nullptr;  // pinned, 2 x 65536
+  unsigned int* h_nunpred = nullptr;           // pinned, 2
+  HuffCodebook cb[3];
+  bool tree_ok[3] = {false, false, false};
+  size_t n_unpred[2] = {0, 0};
+  size_t sec_bytes[3] = {0, 0, 0}, bits_bytes[3] = {0, 0, 0};
+  size_t size = 0;  // blob bytes
 };
 
 int read_flag(cpsz_b200_ctx* ctx, int* out) {
@@ -78,6 +108,366 @@ int flag_error(int flag) {
   return CPSZ_OK;
 }
 
+// Runs f(0..n-1) on up to hardware_concurrency host threads.
+template <class Fn>
+void parallel_for(int n, Fn f) {
+  unsigned nt = std::thread::hardware_concurrency();
+  if (nt < 1) nt = 1;
+  if ((int)nt > n) nt = (unsigned)n;
+  if (nt <= 1) {
+    for (int i = 0; i < n; i++) f(i);
+    return;
+  }
+  std::atomic<int> next{0};
+  std::vector<std::thread> th;
+  for (unsigned t = 0; t < nt; t++)
+    th.emplace_back([&] {
+      for (int i = next++; i < n; i = next++) f(i);
+    });
+  for (auto& t : th) t.join();
+}
+
+int job_init(Job2D& j, const float* U, const float* V, size_t r1s, size_t r2s, double eb) {
+  if (!U || !V) return set_error(CPSZ_ERR_INVALID, "null input field");
+  if (r1s == 0 || r2s == 0) return set_error(CPSZ_ERR_INVALID, "empty field (%zu x %zu)", r1s, r2s);
+  if (r1s > (1u << 30) || r2s > (1u << 30) || r1s * r2s > (size_t)INT32_MAX)
+    return set_error(CPSZ_ERR_UNSUPPORTED, "field of %zu x %zu points exceeds 2^31 points", r1s, r2s);
+  if (eb != eb) return set_error(CPSZ_ERR_INVALID, "max_pwr_eb is NaN");
+  j.U_in = U;
+  j.V_in = V;
+  j.r1 = (int)r1s;
+  j.r2 = (int)r2s;
+  j.N = r1s * r2s;
+  j.eb = eb;
+  j.ngroups = (j.r1 + WAVE_GROUP_ROWS - 1) / WAVE_GROUP_ROWS;
+  const int nby = (j.r2 - 1) / BS + 1, nbx = (j.r1 - 1) / BS + 1;
+  j.nseg = (size_t)j.r1 * nby;
+  j.nblocks = (size_t)nbx * nby;
+  j.dev_in = is_device_ptr(U) && is_device_ptr(V);
+  // bit streams: Huffman averages < log2(distinct) + 1 bits per symbol
+  j.ids_bits_cap = (2 * j.N * 9 + 7) / 8 + 64;
+  j.codes_bits_cap = (j.N * 17 + 7) / 8 + 64;
+  j.blob_cap = BLOB_HDR + 2 * FIELD_HDR + 8 * j.N + 2 * ((j.nblocks + 7) / 8) + 3 * (12 + 1 + 13 * 131072 + 8) +
+               j.ids_bits_cap + 2 * j.codes_bits_cap + 64;
+  return CPSZ_OK;
+}
+
+// Workspace of one field (each piece padded as the arena pads it).
+size_t job_bytes(const Job2D& j) {
+  size_t bytes = 0;
+  auto add = [&](size_t b) { bytes += align_up(b, 256) + 256; };
+  const size_t N = j.N;
+  if (!j.dev_in) add(8 * N);
+  add(2 * N);                           // ids
+  add(256 * 8);                         // hist ids
+  add(4 * N);                           // codes raster
+  add(16 * N);                          // wavefront input pairs
+  add(4 * N);                           // codes blocks
+  add(2 * 65536 * 8);                   // hist codes
+  add(2 * (size_t)j.ngroups * j.r2 * 8);  // boundary rows (tagged words)
+  add(2 * 2 * (j.nseg + 1) * 4);
+  add(2 * segment_scan_tmp_bytes(j.r1, j.r2));
+  add(2 * 4 * N);  // unpred
+  add(256 * 9);
+  add(2 * 65536 * 9);
+  add(huff_encode_tmp_bytes(2 * N));
+  add(2 * huff_encode_tmp_bytes(N));
+  add(j.ids_bits_cap);
+  add(2 * j.codes_bits_cap);
+  add(j.blob_cap);
+  return bytes;
+}
+
+int job_alloc(cpsz_b200_ctx* ctx, Job2D& j) {
+  auto A = [&](size_t b) { return arena_alloc(ctx, b); };
+  DevBuf& d = j.d;
+  const size_t N = j.N;
+  if (j.dev_in) {
+    d.U = const_cast<float*>(j.U_in);
+    d.V = const_cast<float*>(j.V_in);
+  } else {
+    d.U = (float*)A(4 * N);
+    d.V = (float*)A(4 * N);
+  }
+  d.ids = (uint8_t*)A(2 * N);
+  d.hist_ids = (unsigned long long*)A(256 * 8);
+  for (int f = 0; f < 2; f++) {
+    d.craster[f] = (uint16_t*)A(2 * N);
+    d.pairs[f] = (float2*)A(8 * N);
+    d.cblocks[f] = (uint16_t*)A(2 * N);
+    d.hist_codes[f] = (unsigned long long*)A(65536 * 8);
+  }
+  d.gbnd = (unsigned long long*)A(2 * (size_t)j.ngroups * j.r2 * 8);
+  for (int f = 0; f < 2; f++) {
+    d.seg_cnt[f] = (unsigned int*)A((j.nseg + 1) * 4);
+    d.seg_off[f] = (unsigned int*)A((j.nseg + 1) * 4);
+    d.scan_tmp[f] = A(segment_scan_tmp_bytes(j.r1, j.r2));
+    d.unpred[f] = (float*)A(4 * N);
+  }
+  d.enc_code[0] = (unsigned long long*)A(256 * 8);
+  d.enc_len[0] = (uint8_t*)A(256);
+  for (int f = 1; f < 3; f++) {
+    d.enc_code[f] = (unsigned long long*)A(65536 * 8);
+    d.enc_len[f] = (uint8_t*)A(65536);
+  }
+  d.enc_tmp[0] = A(huff_encode_tmp_bytes(2 * N));
+  d.enc_tmp[1] = A(huff_encode_tmp_bytes(N));
+  d.enc_tmp[2] = A(huff_encode_tmp_bytes(N));
+  d.bits[0] = (uint32_t*)A(j.ids_bits_cap);
+  d.bits[1] = (uint32_t*)A(j.codes_bits_cap);
+  d.bits[2] = (uint32_t*)A(j.codes_bits_cap);
+  d.blob = (uint8_t*)A(j.blob_cap);
+  if (!d.blob) return set_error(CPSZ_ERR_NOMEM, "workspace layout overflow");
+  return CPSZ_OK;
+}
+
+// Blob assembly of one field in device memory (header, id tree, two field
+// blobs); the small host-made pieces go up in one copy and are scattered
+// with device-to-device copies.
+int job_assemble(cpsz_b200_ctx* ctx, Job2D& j) {
+  cudaStream_t st = ctx->stream;
+  const size_t ind_bytes = (j.nblocks + 7) / 8;
+  size_t field_size[2];
+  for (int f = 0; f < 2; f++) field_size[f] = FIELD_HDR + 4 * j.n_unpred[f] + ind_bytes + j.sec_bytes[1 + f];
+  const size_t total = BLOB_HDR + j.sec_bytes[0] + field_size[0] + field_size[1];
+  if (total > j.blob_cap) return set_error(CPSZ_ERR_UNSUPPORTED, "blob larger than its bound");
+  std::vector<uint8_t> small;
+  struct Piece {
+    size_t dst, src, n;
+  };
+  std::vector<Piece> pieces;
+  auto stage = [&](size_t dst, const void* p, size_t n) {
+    pieces.push_back(Piece{dst, small.size(), n});
+    small.insert(small.end(), (const uint8_t*)p, (const uint8_t*)p + n);
+  };
+  {
+    uint8_t hdr[BLOB_HDR];
+    const int base = 4;
+    const double thr = DBL_EPSILON;
+    memcpy(hdr, &base, 4);
+    memcpy(hdr + 4, &thr, 8);
+    memcpy(hdr + 12, &j.sec_bytes[0], 8);
+    memcpy(hdr + 20, &field_size[0], 8);
+    memcpy(hdr + 28, &field_size[1], 8);
+    stage(0, hdr, BLOB_HDR);
+  }
+  size_t at = BLOB_HDR;
+  size_t bit_dst[3], unpred_dst[2];
+  auto stage_huff = [&](int k) {
+    stage(at, j.cb[k].tree_bytes.data(), j.cb[k].tree_bytes.size());
+    at += j.cb[k].tree_bytes.size();
+    unsigned long long nb = j.bits_bytes[k];
+    stage(at, &nb, 8);
+    at += 8;
+    bit_dst[k] = at;
+    at += j.bits_bytes[k];
+  };
+  stage_huff(0);
+  std::vector<uint8_t> zeros(ind_bytes, 0);
+  for (int f = 0; f < 2; f++) {
+    uint8_t fh[FIELD_HDR];
+    memset(fh, 0, sizeof(fh));
+    const int bs = BS, radius = 32768;
+    memcpy(fh, &bs, 4);
+    memcpy(fh + 5, &radius, 4);
+    // meanInfo<float>{false, 0}: 8 zero bytes; reg_count = 0
+    unsigned long long nu = j.n_unpred[f];
+    memcpy(fh + 5 + 4 + 8 + 8, &nu, 8);
+    stage(at, fh, FIELD_HDR);
+    at += FIELD_HDR;
+    unpred_dst[f] = at;
+    at += 4 * j.n_unpred[f];
+    stage(at, zeros.data(), ind_bytes);
+    at += ind_bytes;
+    stage_huff(1 + f);
+  }
+  if (at != total) return set_error(CPSZ_ERR_INVALID, "internal: blob layout mismatch (%zu != %zu)", at, total);
+  uint8_t* blob = j.d.blob;
+  uint8_t* d_small = blob + align_up(total, 256);
+  if (align_up(total, 256) + small.size() > j.blob_cap) {
+    for (const Piece& p : pieces)
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(blob + p.dst, small.data() + p.src, p.n, cudaMemcpyHostToDevice, st));
+  } else {
+    // pageable source: the runtime stages it before returning, so `small` may go
+    CPSZ_CUDA_TRY(cudaMemcpyAsync(d_small, small.data(), small.size(), cudaMemcpyHostToDevice, st));
+    for (const Piece& p : pieces)
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(blob + p.dst, d_small + p.src, p.n, cudaMemcpyDeviceToDevice, st));
+  }
+  for (int k = 0; k < 3; k++)
+    if (j.bits_bytes[k])
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(blob + bit_dst[k], j.d.bits[k], j.bits_bytes[k], cudaMemcpyDeviceToDevice, st));
+  for (int f = 0; f < 2; f++)
+    if (j.n_unpred[f])
+      CPSZ_CUDA_TRY(
+          cudaMemcpyAsync(blob + unpred_dst[f], j.d.unpred[f], 4 * j.n_unpred[f], cudaMemcpyDeviceToDevice, st));
+  j.size = total;
+  return CPSZ_OK;
+}
+
+// One compression pass over `jobs` (workspace reserved by the caller).
+int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) {
+  cudaStream_t st = ctx->stream;
+  const int nj = (int)jobs.size();
+  const QuantTable& qt = quant_table_2d();
+  // pass-wide device pieces
+  double* thr_tab = (double*)arena_alloc(ctx, QUANT_TAB_MAX * 8);
+  int* queue = (int*)arena_alloc(ctx, 64);
+  WaveField* d_fields = (WaveField*)arena_alloc(ctx, 2 * nj * sizeof(WaveField));
+  int total_groups = 0;
+  for (const Job2D& j : jobs) total_groups += j.ngroups;
+  WaveItem* d_items = (WaveItem*)arena_alloc(ctx, 2 * (size_t)total_groups * sizeof(WaveItem));
+  if (!d_items) return set_error(CPSZ_ERR_NOMEM, "workspace layout overflow");
+  for (Job2D& j : jobs) CPSZ_TRY(job_alloc(ctx, j));
+  for (int k = 0; k < nj; k++) {
+    uint8_t* base = (uint8_t*)ctx->pinned + PINNED_BASE + (size_t)k * JOB_PINNED;
+    jobs[k].h_hist_ids = (unsigned long long*)base;
+    jobs[k].h_hist_codes = jobs[k].h_hist_ids + 256;
+    jobs[k].h_nunpred = (unsigned int*)(jobs[k].h_hist_codes + 2 * 65536);
+  }
+
+  // ---- stage 1: inputs and error bounds ----
+  reset_marks(ctx);
+  mark(ctx, "h2d+setup");
+  CPSZ_CUDA_TRY(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), st));
+  CPSZ_CUDA_TRY(cudaMemcpyAsync(thr_tab, qt.t, QUANT_TAB_MAX * 8, cudaMemcpyHostToDevice, st));
+  for (Job2D& j : jobs) {
+    if (!j.dev_in) {
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.U, j.U_in, 4 * j.N, cudaMemcpyHostToDevice, st));
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.V, j.V_in, 4 * j.N, cudaMemcpyHostToDevice, st));
+    }
+    CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.hist_ids, 0, 256 * 8, st));
+  }
+  mark(ctx, "eb2d");
+  for (Job2D& j : jobs) {
+    CPSZ_TRY(launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N, j.d.hist_ids,
+                         j.d.pairs[0], j.d.pairs[1]));
+    CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_hist_ids, j.d.hist_ids, 256 * 8, cudaMemcpyDeviceToHost, st));
+  }
+  mark(ctx, "eb2d_end");
+  CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[0], st));
+  if (tap && tap->ids)
+    CPSZ_CUDA_TRY(cudaMemcpyAsync(tap->ids, jobs[0].d.ids, 2 * jobs[0].N, cudaMemcpyDeviceToDevice, st));
+
+  // ---- stage 2: one persistent wavefront over every field of the pass ----
+  std::vector<WaveField> hf(2 * nj);
+  std::vector<int> r1v(2 * nj);
+  for (int k = 0; k < nj; k++) {
+    Job2D& j = jobs[k];
+    CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.gbnd, 0, 2 * (size_t)j.ngroups * j.r2 * 8, st));
+    for (int f = 0; f < 2; f++) {
+      WaveField& F = hf[2 * k + f];
+      F.pair = j.d.pairs[f];
+      F.codes = j.d.craster[f];
+      F.trace = (nj == 1 && ctx->d_wave_trace && ctx->wave_trace_len >= 2 * (size_t)j.ngroups * WAVE_WARPS * 4)
+                    ? ctx->d_wave_trace + (size_t)f * j.ngroups * WAVE_WARPS * 4
+                    : nullptr;
+      F.out = tap ? tap->recon[f] : nullptr;
+      F.gbnd = j.d.gbnd + (size_t)f * j.ngroups * j.r2;
+      F.pair_pitch = j.r2;
+      F.code_pitch = j.r2;
+      F.out_pitch = j.r2;
+      F.r1 = j.r1;
+      F.r2 = j.r2;
+      r1v[2 * k + f] = j.r1;
+    }
+  }
+  std::vector<WaveItem> items;
+  const int n_items = build_wave_items(2 * nj, r1v.data(), items);
+  CPSZ_CUDA_TRY(cudaMemcpyAsync(d_fields, hf.data(), hf.size() * sizeof(WaveField), cudaMemcpyHostToDevice, st));
+  CPSZ_CUDA_TRY(cudaMemcpyAsync(d_items, items.data(), n_items * sizeof(WaveItem), cudaMemcpyHostToDevice, st));
+  CPSZ_CUDA_TRY(cudaMemsetAsync(queue, 0, 64, st));
+  mark(ctx, "wave2d_compress");
+  CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, 0));
+  mark(ctx, "blocks+hist+unpred");
+
+  // ---- stage 3: block order, histograms, unpredictables ----
+  for (Job2D& j : jobs)
+    for (int f = 0; f < 2; f++) {
+      CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.hist_codes[f], 0, 65536 * 8, st));
+      CPSZ_TRY(launch_raster_to_blocks_u16(ctx, j.d.craster[f], j.r2, j.r1, j.r2, j.d.cblocks[f], j.d.hist_codes[f]));
+      CPSZ_TRY(launch_segment_scan(ctx, j.d.craster[f], j.r2, j.r1, j.r2, j.d.seg_cnt[f], j.d.seg_off[f],
+                                   j.d.scan_tmp[f]));
+      CPSZ_TRY(launch_gather_unpred(ctx, j.d.craster[f], j.r2, f ? j.d.V : j.d.U, j.r2, j.r1, j.r2, j.d.seg_off[f],
+                                    j.d.unpred[f]));
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_hist_codes + (size_t)f * 65536, j.d.hist_codes[f], 65536 * 8,
+                                    cudaMemcpyDeviceToHost, st));
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_nunpred + f, j.d.seg_off[f] + j.nseg, 4, cudaMemcpyDeviceToHost, st));
+    }
+  mark(ctx, "host_trees");
+  CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[1], st));
+
+  // host: id trees while the GPU runs the wavefront, then the code trees
+  CPSZ_CUDA_TRY(cudaEventSynchronize(ctx->ev[0]));
+  parallel_for(nj, [&](int k) { jobs[k].tree_ok[0] = huff_build(jobs[k].h_hist_ids, 256, 2048, &jobs[k].cb[0]); });
+  CPSZ_CUDA_TRY(cudaEventSynchronize(ctx->ev[1]));
+  int flag = 0;
+  CPSZ_TRY(read_flag(ctx, &flag));
+  if (flag) return flag_error(flag);
+  parallel_for(2 * nj, [&](int q) {
+    Job2D& j = jobs[q / 2];
+    const int f = q % 2;
+    j.tree_ok[1 + f] = huff_build(j.h_hist_codes + (size_t)f * 65536, 65536, 131072, &j.cb[1 + f]);
+  });
+  for (Job2D& j : jobs) {
+    for (int k = 0; k < 3; k++)
+      if (!j.tree_ok[k]) return set_error(CPSZ_ERR_UNSUPPORTED, "Huffman tree construction failed (code longer than 64 bits)");
+    j.n_unpred[0] = j.h_nunpred[0];
+    j.n_unpred[1] = j.h_nunpred[1];
+  }
+
+  // ---- stage 4: bit packing ----
+  mark(ctx, "huffman_encode");
+  for (Job2D& j : jobs) {
+    for (int k = 0; k < 3; k++) {
+      j.sec_bytes[k] = huff_section_bytes(j.cb[k]);
+      j.bits_bytes[k] = (j.cb[k].total_bits + 7) / 8;
+    }
+    if (j.bits_bytes[0] + 8 > j.ids_bits_cap || j.bits_bytes[1] + 8 > j.codes_bits_cap ||
+        j.bits_bytes[2] + 8 > j.codes_bits_cap)
+      return set_error(CPSZ_ERR_UNSUPPORTED, "Huffman stream larger than its bound");
+    for (int k = 0; k < 3; k++) {
+      const size_t bins = k ? 65536 : 256;
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.enc_code[k], j.cb[k].code.data(), bins * 8, cudaMemcpyHostToDevice, st));
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.enc_len[k], j.cb[k].len.data(), bins, cudaMemcpyHostToDevice, st));
+      CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.bits[k], 0, align_up(j.bits_bytes[k], 4) + 8, st));
+    }
+    CPSZ_TRY(launch_huff_encode_u8(ctx, j.d.ids, 2 * j.N, true, HuffEncTable{j.d.enc_code[0], j.d.enc_len[0], 256},
+                                   j.d.bits[0], j.ids_bits_cap, nullptr, j.d.enc_tmp[0]));
+    for (int f = 0; f < 2; f++)
+      CPSZ_TRY(launch_huff_encode_u16(ctx, j.d.cblocks[f], j.N,
+                                      HuffEncTable{j.d.enc_code[1 + f], j.d.enc_len[1 + f], 65536}, j.d.bits[1 + f],
+                                      j.codes_bits_cap, nullptr, j.d.enc_tmp[1 + f]));
+  }
+
+  // ---- stage 5: blob assembly in device memory ----
+  mark(ctx, "blob_assembly");
+  for (Job2D& j : jobs) CPSZ_TRY(job_assemble(ctx, j));
+  mark(ctx, "end");
+  if (tap) {
+    Job2D& j = jobs[0];
+    for (int f = 0; f < 2; f++) {
+      if (tap->codes_blocks[f])
+        CPSZ_CUDA_TRY(cudaMemcpyAsync(tap->codes_blocks[f], j.d.cblocks[f], 2 * j.N, cudaMemcpyDeviceToDevice, st));
+      if (tap->unpred[f] && j.n_unpred[f])
+        CPSZ_CUDA_TRY(
+            cudaMemcpyAsync(tap->unpred[f], j.d.unpred[f], 4 * j.n_unpred[f], cudaMemcpyDeviceToDevice, st));
+    }
+  }
+  return CPSZ_OK;
+}
+
+size_t pass_bytes(const std::vector<Job2D>& jobs) {
+  size_t bytes = 0;
+  int total_groups = 0;
+  for (const Job2D& j : jobs) {
+    bytes += job_bytes(j);
+    total_groups += j.ngroups;
+  }
+  bytes += align_up(QUANT_TAB_MAX * 8, 256) + 256 + 512 + align_up(2 * jobs.size() * sizeof(WaveField), 256) + 256 +
+           align_up(2 * (size_t)total_groups * sizeof(WaveItem), 256) + 256;
+  return bytes;
+}
+
 }  // namespace
 
 int build_wave_items(int nfields, const int* r1s, std::vector<WaveItem>& items) {
@@ -92,285 +482,55 @@ int build_wave_items(int nfields, const int* r1s, std::vector<WaveItem>& items) 
 
 int compress_2d(cpsz_b200_ctx* ctx, const float* U_in, const float* V_in, size_t r1s, size_t r2s, double max_pwr_eb,
                 Blob2D* out, const StageTap* tap) {
-  if (!U_in || !V_in) return set_error(CPSZ_ERR_INVALID, "null input field");
-  if (r1s == 0 || r2s == 0) return set_error(CPSZ_ERR_INVALID, "empty field (%zu x %zu)", r1s, r2s);
-  if (r1s > (1u << 30) || r2s > (1u << 30) || r1s * r2s > (size_t)INT32_MAX)
-    return set_error(CPSZ_ERR_UNSUPPORTED, "field of %zu x %zu points exceeds 2^31 points", r1s, r2s);
-  if (max_pwr_eb != max_pwr_eb) return set_error(CPSZ_ERR_INVALID, "max_pwr_eb is NaN");
-  const int r1 = (int)r1s, r2 = (int)r2s;
-  const size_t N = r1s * r2s;
-  const int ngroups = (r1 + WAVE_GROUP_ROWS - 1) / WAVE_GROUP_ROWS;
-  const int nby = (r2 - 1) / BS + 1, nbx = (r1 - 1) / BS + 1;
-  const size_t nseg = (size_t)r1 * nby;
-  const size_t nblocks = (size_t)nbx * nby;
-  const bool dev_in = is_device_ptr(U_in) && is_device_ptr(V_in);
-  const QuantTable& qt = quant_table_2d();
+  std::vector<Job2D> jobs(1);
+  CPSZ_TRY(job_init(jobs[0], U_in, V_in, r1s, r2s, max_pwr_eb));
+  CPSZ_TRY(arena_reserve(ctx, pass_bytes(jobs)));
+  CPSZ_TRY(pinned_reserve(ctx, PINNED_BASE + JOB_PINNED));
+  CPSZ_TRY(run_pass(ctx, jobs, tap));
+  out->d_blob = jobs[0].d.blob;
+  out->size = jobs[0].size;
+  out->n_unpred[0] = jobs[0].n_unpred[0];
+  out->n_unpred[1] = jobs[0].n_unpred[1];
+  return CPSZ_OK;
+}
 
-  // ---- workspace ----
-  size_t bytes = 0;
-  auto add = [&](size_t b) { bytes += align_up(b, 256) + 256; };
-  if (!dev_in) add(8 * N);
-  add(2 * N);                         // ids
-  add(256 * 8);                       // hist ids
-  add(4 * N);                         // codes raster
-  add(16 * N);                        // wavefront input pairs
-  add(4 * N);                         // codes blocks
-  add(2 * 65536 * 8);                 // hist codes
-  add(2 * (size_t)ngroups * r2 * 8);  // boundary rows (tagged words)
-  add(64);                            // work-queue counter
-  add(2 * sizeof(WaveField) + 2 * (size_t)ngroups * sizeof(WaveItem));
-  add(2 * 2 * (nseg + 1) * 4);
-  add(2 * segment_scan_tmp_bytes(r1, r2));
-  add(2 * 4 * N);  // unpred
-  add(QUANT_TAB_MAX * 8);
-  add(256 * 9);
-  add(2 * 65536 * 9);
-  add(huff_encode_tmp_bytes(2 * N));
-  add(2 * huff_encode_tmp_bytes(N));
-  // bit streams: Huffman averages < log2(distinct) + 1 bits per symbol
-  const size_t ids_bits_cap = (2 * N * 9 + 7) / 8 + 64;
-  const size_t codes_bits_cap = (N * 17 + 7) / 8 + 64;
-  add(ids_bits_cap);
-  add(2 * codes_bits_cap);
-  add(64);
-  const size_t blob_cap = BLOB_HDR + 2 * FIELD_HDR + 8 * N + 2 * ((nblocks + 7) / 8) + 3 * (12 + 1 + 13 * 131072 + 8) +
-                          ids_bits_cap + 2 * codes_bits_cap + 64;
-  add(blob_cap);
-  CPSZ_TRY(arena_reserve(ctx, bytes));
-  CPSZ_TRY(pinned_reserve(ctx, 2 * 65536 * 8 + 256 * 8 + 4096));
-  DevBuf d{};
-  auto A = [&](size_t b) { return arena_alloc(ctx, b); };
-  cudaStream_t st = ctx->stream;
-  if (dev_in) {
-    d.U = const_cast<float*>(U_in);
-    d.V = const_cast<float*>(V_in);
-  } else {
-    d.U = (float*)A(4 * N);
-    d.V = (float*)A(4 * N);
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(d.U, U_in, 4 * N, cudaMemcpyHostToDevice, st));
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(d.V, V_in, 4 * N, cudaMemcpyHostToDevice, st));
-  }
-  d.ids = (uint8_t*)A(2 * N);
-  d.hist_ids = (unsigned long long*)A(256 * 8);
-  for (int f = 0; f < 2; f++) {
-    d.craster[f] = (uint16_t*)A(2 * N);
-    d.pairs[f] = (float2*)A(8 * N);
-    d.cblocks[f] = (uint16_t*)A(2 * N);
-    d.hist_codes[f] = (unsigned long long*)A(65536 * 8);
-  }
-  d.gbnd = (unsigned long long*)A(2 * (size_t)ngroups * r2 * 8);
-  d.queue = (int*)A(64);
-  d.fields = (WaveField*)A(2 * sizeof(WaveField));
-  d.items = (WaveItem*)A(2 * (size_t)ngroups * sizeof(WaveItem));
-  for (int f = 0; f < 2; f++) {
-    d.seg_cnt[f] = (unsigned int*)A((nseg + 1) * 4);
-    d.seg_off[f] = (unsigned int*)A((nseg + 1) * 4);
-    d.scan_tmp[f] = A(segment_scan_tmp_bytes(r1, r2));
-    d.unpred[f] = (float*)A(4 * N);
-  }
-  d.thr_tab = (double*)A(QUANT_TAB_MAX * 8);
-  d.enc_code[0] = (unsigned long long*)A(256 * 8);
-  d.enc_len[0] = (uint8_t*)A(256);
-  for (int f = 1; f < 3; f++) {
-    d.enc_code[f] = (unsigned long long*)A(65536 * 8);
-    d.enc_len[f] = (uint8_t*)A(65536);
-  }
-  d.enc_tmp[0] = A(huff_encode_tmp_bytes(2 * N));
-  d.enc_tmp[1] = A(huff_encode_tmp_bytes(N));
-  d.enc_tmp[2] = A(huff_encode_tmp_bytes(N));
-  d.bits[0] = (uint32_t*)A(ids_bits_cap);
-  d.bits[1] = (uint32_t*)A(codes_bits_cap);
-  d.bits[2] = (uint32_t*)A(codes_bits_cap);
-  d.bits_total = (unsigned long long*)A(64);
-  d.blob = (uint8_t*)A(blob_cap);
-  if (!d.blob) return set_error(CPSZ_ERR_NOMEM, "workspace layout overflow");
-
-  // ---- stage 1: error bounds ----
-  reset_marks(ctx);
-  mark(ctx, "h2d+setup");
-  CPSZ_CUDA_TRY(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), st));
-  CPSZ_CUDA_TRY(cudaMemsetAsync(d.hist_ids, 0, 256 * 8, st));
-  CPSZ_CUDA_TRY(cudaMemcpyAsync(d.thr_tab, qt.t, QUANT_TAB_MAX * 8, cudaMemcpyHostToDevice, st));
-  mark(ctx, "eb2d");
-  CPSZ_TRY(launch_eb2d(ctx, d.U, d.V, r1, r2, max_pwr_eb, d.thr_tab, qt.n, d.ids, d.ids + N, d.hist_ids,
-                       d.pairs[0], d.pairs[1]));
-  mark(ctx, "eb2d_end");
-  unsigned long long* h_hist_ids = (unsigned long long*)ctx->pinned;
-  CPSZ_CUDA_TRY(cudaMemcpyAsync(h_hist_ids, d.hist_ids, 256 * 8, cudaMemcpyDeviceToHost, st));
-  CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[0], st));
-  if (tap && tap->ids) CPSZ_CUDA_TRY(cudaMemcpyAsync(tap->ids, d.ids, 2 * N, cudaMemcpyDeviceToDevice, st));
-
-  // ---- stage 2: Lorenzo wavefront of U and V ----
-  std::vector<WaveField> hf(2);
-  for (int f = 0; f < 2; f++) {
-    WaveField& F = hf[f];
-    F.pair = d.pairs[f];
-    F.codes = d.craster[f];
-    F.trace = (ctx->d_wave_trace && ctx->wave_trace_len >= 2 * (size_t)ngroups * WAVE_WARPS * 4)
-                  ? ctx->d_wave_trace + (size_t)f * ngroups * WAVE_WARPS * 4
-                  : nullptr;
-    F.out = tap ? tap->recon[f] : nullptr;
-    F.gbnd = d.gbnd + (size_t)f * ngroups * r2;
-    F.pair_pitch = r2;
-    F.code_pitch = r2;
-    F.out_pitch = r2;
-    F.r1 = r1;
-    F.r2 = r2;
-  }
-  int r1v[2] = {r1, r1};
-  std::vector<WaveItem> items;
-  int n_items = build_wave_items(2, r1v, items);
-  CPSZ_CUDA_TRY(cudaMemcpyAsync(d.fields, hf.data(), 2 * sizeof(WaveField), cudaMemcpyHostToDevice, st));
-  CPSZ_CUDA_TRY(cudaMemcpyAsync(d.items, items.data(), n_items * sizeof(WaveItem), cudaMemcpyHostToDevice, st));
-  CPSZ_CUDA_TRY(cudaMemsetAsync(d.gbnd, 0, 2 * (size_t)ngroups * r2 * 8, st));
-  CPSZ_CUDA_TRY(cudaMemsetAsync(d.queue, 0, 64, st));
-  mark(ctx, "wave2d_compress");
-  CPSZ_TRY(launch_wave2d(ctx, false, d.fields, d.items, n_items, d.queue, 0));
-  mark(ctx, "blocks+hist+unpred");
-
-  // ---- stage 3: block order, histograms, unpredictables ----
-  unsigned long long* h_hist_codes = h_hist_ids + 256;
-  unsigned int* h_nunpred = (unsigned int*)(h_hist_codes + 2 * 65536);
-  for (int f = 0; f < 2; f++) {
-    CPSZ_CUDA_TRY(cudaMemsetAsync(d.hist_codes[f], 0, 65536 * 8, st));
-    CPSZ_TRY(launch_raster_to_blocks_u16(ctx, d.craster[f], r2, r1, r2, d.cblocks[f], d.hist_codes[f]));
-    CPSZ_TRY(launch_segment_scan(ctx, d.craster[f], r2, r1, r2, d.seg_cnt[f], d.seg_off[f], d.scan_tmp[f]));
-    CPSZ_TRY(launch_gather_unpred(ctx, d.craster[f], r2, f ? d.V : d.U, r2, r1, r2, d.seg_off[f], d.unpred[f]));
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(h_hist_codes + (size_t)f * 65536, d.hist_codes[f], 65536 * 8,
-                                  cudaMemcpyDeviceToHost, st));
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(h_nunpred + f, d.seg_off[f] + nseg, 4, cudaMemcpyDeviceToHost, st));
-  }
-  mark(ctx, "host_trees");
-  CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[1], st));
-
-  // host: id tree while the GPU runs the wavefront
-  CPSZ_CUDA_TRY(cudaEventSynchronize(ctx->ev[0]));
-  HuffCodebook cb[3];
-  if (!huff_build(h_hist_ids, 256, 2048, &cb[0])) return CPSZ_ERR_INVALID;
-  CPSZ_CUDA_TRY(cudaEventSynchronize(ctx->ev[1]));
-  int flag = 0;
-  CPSZ_TRY(read_flag(ctx, &flag));
-  if (flag) return flag_error(flag);
-  for (int f = 0; f < 2; f++)
-    if (!huff_build(h_hist_codes + (size_t)f * 65536, 65536, 131072, &cb[1 + f])) return CPSZ_ERR_INVALID;
-  const size_t n_unpred[2] = {h_nunpred[0], h_nunpred[1]};
-
-  // ---- stage 4: bit packing ----
-  const size_t sec_bytes[3] = {huff_section_bytes(cb[0]), huff_section_bytes(cb[1]), huff_section_bytes(cb[2])};
-  const size_t bits_bytes[3] = {(cb[0].total_bits + 7) / 8, (cb[1].total_bits + 7) / 8, (cb[2].total_bits + 7) / 8};
-  if (bits_bytes[0] + 8 > ids_bits_cap || bits_bytes[1] + 8 > codes_bits_cap || bits_bytes[2] + 8 > codes_bits_cap)
-    return set_error(CPSZ_ERR_UNSUPPORTED, "Huffman stream larger than its bound");
-  mark(ctx, "huffman_encode");
-  for (int k = 0; k < 3; k++) {
-    const size_t bins = k ? 65536 : 256;
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(d.enc_code[k], cb[k].code.data(), bins * 8, cudaMemcpyHostToDevice, st));
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(d.enc_len[k], cb[k].len.data(), bins, cudaMemcpyHostToDevice, st));
-    CPSZ_CUDA_TRY(cudaMemsetAsync(d.bits[k], 0, align_up(bits_bytes[k], 4) + 8, st));
-  }
-  CPSZ_TRY(launch_huff_encode_u8(ctx, d.ids, 2 * N, true, HuffEncTable{d.enc_code[0], d.enc_len[0], 256}, d.bits[0],
-                                 ids_bits_cap, nullptr, d.enc_tmp[0]));
-  for (int f = 0; f < 2; f++)
-    CPSZ_TRY(launch_huff_encode_u16(ctx, d.cblocks[f], N, HuffEncTable{d.enc_code[1 + f], d.enc_len[1 + f], 65536},
-                                    d.bits[1 + f], codes_bits_cap, nullptr, d.enc_tmp[1 + f]));
-
-  mark(ctx, "blob_assembly");
-  // ---- stage 5: blob assembly in device memory ----
-  const size_t ind_bytes = (nblocks + 7) / 8;
-  size_t field_size[2];
-  for (int f = 0; f < 2; f++) field_size[f] = FIELD_HDR + 4 * n_unpred[f] + ind_bytes + sec_bytes[1 + f];
-  const size_t total = BLOB_HDR + sec_bytes[0] + field_size[0] + field_size[1];
-  if (total > blob_cap) return set_error(CPSZ_ERR_UNSUPPORTED, "blob larger than its bound");
-  std::vector<uint8_t> hdr(BLOB_HDR + 2 * (FIELD_HDR + 12 + 131072 * 13 + 8), 0);
-  // header
-  {
-    size_t at = 0;
-    auto put = [&](const void* p, size_t n) {
-      memcpy(hdr.data() + at, p, n);
-      at += n;
-    };
-    const int base = 4;
-    const double thr = DBL_EPSILON;
-    put(&base, 4);
-    put(&thr, 8);
-    put(&sec_bytes[0], 8);
-    put(&field_size[0], 8);
-    put(&field_size[1], 8);
-  }
-  // host staging of all small pieces: blob header, id tree + size, field headers, code trees + sizes
-  std::vector<uint8_t> small;
-  struct Piece { size_t dst, src, n; };
-  std::vector<Piece> pieces;
-  auto stage = [&](size_t dst, const void* p, size_t n) {
-    pieces.push_back(Piece{dst, small.size(), n});
-    small.insert(small.end(), (const uint8_t*)p, (const uint8_t*)p + n);
-  };
+int compress_2d_batch(cpsz_b200_ctx* ctx, int n, const float* const* U, const float* const* V, const size_t* r1,
+                      const size_t* r2, const double* ebs, unsigned char* out, size_t out_cap, size_t* offsets) {
+  if (n < 0 || (n > 0 && (!U || !V || !r1 || !r2 || !ebs))) return set_error(CPSZ_ERR_INVALID, "null batch argument");
+  if (!out || !offsets) return set_error(CPSZ_ERR_INVALID, "null output");
+  const bool dev_out = is_device_ptr(out);
   size_t at = 0;
-  stage(at, hdr.data(), BLOB_HDR);
-  at += BLOB_HDR;
-  size_t bit_dst[3], unpred_dst[2];
-  auto stage_huff = [&](int k) {
-    stage(at, cb[k].tree_bytes.data(), cb[k].tree_bytes.size());
-    at += cb[k].tree_bytes.size();
-    unsigned long long nb = bits_bytes[k];
-    stage(at, &nb, 8);
-    at += 8;
-    bit_dst[k] = at;
-    at += bits_bytes[k];
-  };
-  stage_huff(0);
-  for (int f = 0; f < 2; f++) {
-    uint8_t fh[FIELD_HDR];
-    memset(fh, 0, sizeof(fh));
-    const int bs = BS, radius = 32768;
-    memcpy(fh, &bs, 4);
-    fh[4] = 0;
-    memcpy(fh + 5, &radius, 4);
-    // meanInfo<float>{false, 0}: 8 zero bytes; reg_count = 0
-    unsigned long long nu = n_unpred[f];
-    memcpy(fh + 5 + 4 + 8 + 8, &nu, 8);
-    stage(at, fh, FIELD_HDR);
-    at += FIELD_HDR;
-    unpred_dst[f] = at;
-    at += 4 * n_unpred[f];
-    std::vector<uint8_t> zeros(ind_bytes, 0);
-    stage(at, zeros.data(), ind_bytes);
-    at += ind_bytes;
-    stage_huff(1 + f);
-  }
-  if (at != total) return set_error(CPSZ_ERR_INVALID, "internal: blob layout mismatch (%zu != %zu)", at, total);
-  // upload the staged small pieces once, then scatter them with D2D copies
-  uint8_t* d_small = d.blob + align_up(total, 256);
-  if (align_up(total, 256) + small.size() > blob_cap) {
-    // fall back: the small pieces go straight from host
-    for (const Piece& p : pieces)
-      CPSZ_CUDA_TRY(cudaMemcpyAsync(d.blob + p.dst, small.data() + p.src, p.n, cudaMemcpyHostToDevice, st));
-  } else {
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(d_small, small.data(), small.size(), cudaMemcpyHostToDevice, st));
-    for (const Piece& p : pieces)
-      CPSZ_CUDA_TRY(cudaMemcpyAsync(d.blob + p.dst, d_small + p.src, p.n, cudaMemcpyDeviceToDevice, st));
-  }
-  for (int k = 0; k < 3; k++)
-    if (bits_bytes[k])
-      CPSZ_CUDA_TRY(cudaMemcpyAsync(d.blob + bit_dst[k], d.bits[k], bits_bytes[k], cudaMemcpyDeviceToDevice, st));
-  for (int f = 0; f < 2; f++)
-    if (n_unpred[f])
-      CPSZ_CUDA_TRY(
-          cudaMemcpyAsync(d.blob + unpred_dst[f], d.unpred[f], 4 * n_unpred[f], cudaMemcpyDeviceToDevice, st));
-  mark(ctx, "end");
-  out->d_blob = d.blob;
-  out->size = total;
-  out->n_unpred[0] = n_unpred[0];
-  out->n_unpred[1] = n_unpred[1];
-  if (tap) {
-    for (int f = 0; f < 2; f++) {
-      if (tap->codes_blocks[f])
-        CPSZ_CUDA_TRY(cudaMemcpyAsync(tap->codes_blocks[f], d.cblocks[f], 2 * N, cudaMemcpyDeviceToDevice, st));
-      if (tap->unpred[f] && n_unpred[f])
-        CPSZ_CUDA_TRY(cudaMemcpyAsync(tap->unpred[f], d.unpred[f], 4 * n_unpred[f], cudaMemcpyDeviceToDevice, st));
+  int k0 = 0;
+  offsets[0] = 0;
+  while (k0 < n) {
+    // greedy pass: up to BATCH_MAX_FIELDS fields and BATCH_MAX_POINTS points (a larger field goes alone)
+    std::vector<Job2D> jobs;
+    size_t pts = 0;
+    int k = k0;
+    while (k < n && (int)jobs.size() < BATCH_MAX_FIELDS) {
+      Job2D j;
+      CPSZ_TRY(job_init(j, U[k], V[k], r1[k], r2[k], ebs[k]));
+      if (!jobs.empty() && pts + j.N > BATCH_MAX_POINTS) break;
+      pts += j.N;
+      jobs.push_back(std::move(j));
+      k++;
     }
+    CPSZ_TRY(arena_reserve(ctx, pass_bytes(jobs)));
+    CPSZ_TRY(pinned_reserve(ctx, PINNED_BASE + jobs.size() * JOB_PINNED));
+    CPSZ_TRY(run_pass(ctx, jobs, nullptr));
+    for (size_t q = 0; q < jobs.size(); q++) {
+      const Job2D& j = jobs[q];
+      if (at + j.size > out_cap)
+        return set_error(CPSZ_ERR_INVALID, "output capacity %zu < %zu bytes of blobs", out_cap, at + j.size);
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(out + at, j.d.blob, j.size,
+                                    dev_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
+      at += j.size;
+      offsets[k0 + q + 1] = at;
+    }
+    // the next pass reuses the workspace
+    CPSZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    k0 = k;
   }
-  // `small` must outlive the async H2D from pageable memory: pageable copies
-  // are staged synchronously by the runtime before cudaMemcpyAsync returns.
   return CPSZ_OK;
 }
 

@@ -78,6 +78,19 @@ int cpsz_b200_compress_2d_offline_f32_into(cpsz_b200_ctx* ctx, const float* U, c
 int cpsz_b200_decompress_2d_offline_f32(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_size, size_t r1,
                                         size_t r2, float* U, float* V);
 
+/* ---- batched 2D compression (many independent fields) ----------------------
+ * Compresses n_fields fields in passes of up to 32 fields: every kernel stage
+ * runs for all fields of a pass, the Lorenzo wavefront is one persistent
+ * launch over all of them, and the Huffman trees are built on all host threads.
+ * U[k], V[k]: host or device pointers of r1[k] x r2[k] floats; max_pwr_eb[k]
+ * per field.  Blobs are written back to back into `out` (host or device,
+ * out_cap bytes): blob k spans [offsets[k], offsets[k+1]), offsets has
+ * n_fields + 1 entries.  Each blob is byte-identical to
+ * cpsz_b200_compress_2d_offline_f32 of that field alone. */
+int cpsz_b200_compress_2d_batch_f32(cpsz_b200_ctx* ctx, int n_fields, const float* const* U, const float* const* V,
+                                    const size_t* r1, const size_t* r2, const double* max_pwr_eb, unsigned char* out,
+                                    size_t out_cap, size_t* offsets);
+
 /* ---- 3D offline (log) CP-preserving compression -------------------------
  * Replaces sz_compress_cp_preserve_3d_offline_log<float>
  * (reference include/sz_compress_cp_preserve_3d.hpp:8,
