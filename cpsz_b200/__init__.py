@@ -83,6 +83,7 @@ def _declare(L):
     L.cpsz_b200_libm_tables_prepare.argtypes = [C.c_char_p]
     L.cpsz_b200_debug_eb3d.argtypes = [_vp, _vp, _vp, _vp, _sz, _sz, _sz, C.c_double, _vp, _vp]
     L.cpsz_b200_debug_libm.argtypes = [_vp, C.c_int, _vp, _sz, _vp]
+    L.cpsz_b200_debug_umma_gemm.argtypes = [_vp, _vp, _vp, _vp]
     if hasattr(L, "cpsz_b200_cp_check_2d"):
         L.cpsz_b200_cp_check_2d.argtypes = [_vp, _vp, _vp, _vp, _vp, _sz, _sz, _vp, C.POINTER(C.c_uint64)]
         L.cpsz_b200_cp_check_3d.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _sz, _sz, _vp,
@@ -343,6 +344,26 @@ def debug_libm(which: str, x, ctx: Context | None = None):
     _check(lib().cpsz_b200_debug_libm(_h(ctx), {"log2f": 0, "exp2f": 1}[which], x.ctypes.data, x.size,
                                       out.ctypes.data))
     return out
+
+
+def to_bf16_bits(x) -> np.ndarray:
+    """float32 -> bfloat16 bit patterns (round to nearest even)."""
+    b = np.ascontiguousarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    return ((b + 0x7FFF + ((b >> 16) & 1)) >> 16).astype(np.uint16)
+
+
+def bf16_bits_to_f32(b) -> np.ndarray:
+    return (np.asarray(b, np.uint32) << 16).view(np.float32)
+
+
+def debug_umma_gemm(A_bits, B_bits, ctx: Context | None = None):
+    """128x128 fp32 D = A B^T from bf16 bit arrays, on the tensor cores (tcgen05)."""
+    A = np.ascontiguousarray(A_bits, np.uint16)
+    B = np.ascontiguousarray(B_bits, np.uint16)
+    assert A.shape == (128, 128) and B.shape == (128, 128)
+    D = np.zeros((128, 128), np.float32)
+    _check(lib().cpsz_b200_debug_umma_gemm(_h(ctx), A.ctypes.data, B.ctypes.data, D.ctypes.data))
+    return D
 
 
 # ---- exact critical-point check ------------------------------------------------------

@@ -355,6 +355,35 @@ int cpsz_b200_debug_eb3d(cpsz_b200_ctx* ctx, const float* U, const float* V, con
   return rc;
 }
 
+int cpsz_b200_debug_umma_gemm(cpsz_b200_ctx* ctx, const uint16_t* A, const uint16_t* B, float* D) {
+  RESOLVE(ctx);
+  if (!A || !B || !D) return set_error(CPSZ_ERR_INVALID, "null pointer");
+  void *dA = nullptr, *dB = nullptr;
+  float* dD = nullptr;
+  CPSZ_CUDA_TRY(cudaMalloc(&dA, 128 * 128 * 2));
+  CPSZ_CUDA_TRY(cudaMalloc(&dB, 128 * 128 * 2));
+  CPSZ_CUDA_TRY(cudaMalloc((void**)&dD, 128 * 128 * 4));
+  cudaMemcpy(dA, A, 128 * 128 * 2, cudaMemcpyHostToDevice);
+  cudaMemcpy(dB, B, 128 * 128 * 2, cudaMemcpyHostToDevice);
+  cudaMemset(dD, 0, 128 * 128 * 4);
+  cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream);
+  int rc = launch_umma_selftest(ctx, dA, dB, dD);
+  int flag = 0;
+  if (rc == CPSZ_OK) {
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) rc = set_error(CPSZ_ERR_CUDA, "tensor-core self-test: %s", cudaGetErrorString(e));
+  }
+  if (rc == CPSZ_OK) {
+    cudaMemcpy(D, dD, 128 * 128 * 4, cudaMemcpyDeviceToHost);
+    cudaMemcpy(&flag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost);
+    if (flag) rc = set_error(CPSZ_ERR_TIMEOUT, "tensor-core self-test: MMA completion wait gave up");
+  }
+  cudaFree(dA);
+  cudaFree(dB);
+  cudaFree(dD);
+  return rc;
+}
+
 int cpsz_b200_debug_libm(cpsz_b200_ctx* ctx, int which, const float* in, size_t n, float* out) {
   RESOLVE(ctx);
   if (!in || !out || (which != 0 && which != 1)) return set_error(CPSZ_ERR_INVALID, "invalid argument");

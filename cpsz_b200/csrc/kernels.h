@@ -163,6 +163,11 @@ int launch_cp_check_3d(cpsz_b200_ctx* ctx, const float* Ua, const float* Va, con
                        const float* Vb, const float* Wb, int r1, int r2, int r3, uint8_t* cells,
                        unsigned long long* counts);
 
+// ---- learned-bound MLP (tcgen05) ------------------------------------------------------
+// D (128 x 128 fp32, row-major) = A (128 x 128 bf16) * B (128 x 128 bf16)^T on
+// one CTA through shared memory and TMEM (device pointers).
+int launch_umma_selftest(cpsz_b200_ctx* ctx, const void* A, const void* B, float* D);
+
 // ---- generic scans ----------------------------------------------------------------
 size_t scan_u32_tmp_bytes(size_t n);
 // Exclusive scan of n u32 values into out (n+1 entries, out[n] = total).

@@ -181,6 +181,9 @@ int cpsz_b200_debug_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, siz
  * 255 = bound not positive).  Host buffers. */
 int cpsz_b200_debug_eb3d(cpsz_b200_ctx* ctx, const float* U, const float* V, const float* W, size_t r1, size_t r2,
                          size_t r3, double max_pwr_eb, double* eb_out, uint8_t* id_codes);
+/* Tensor-core self-check: D (128x128 fp32) = A (128x128 bf16 bits) * B^T
+ * (128x128 bf16 bits), row-major host arrays, through tcgen05 / TMEM. */
+int cpsz_b200_debug_umma_gemm(cpsz_b200_ctx* ctx, const uint16_t* A, const uint16_t* B, float* D);
 /* The GPU's host-library log2f (which 0) or exp2f (which 1) of n host floats. */
 int cpsz_b200_debug_libm(cpsz_b200_ctx* ctx, int which, const float* in, size_t n, float* out);
 /* Wavefront trace: with out == NULL, (re)allocates a device trace of len
