@@ -84,6 +84,17 @@ def _declare(L):
     L.cpsz_b200_debug_eb3d.argtypes = [_vp, _vp, _vp, _vp, _sz, _sz, _sz, C.c_double, _vp, _vp]
     L.cpsz_b200_debug_libm.argtypes = [_vp, C.c_int, _vp, _sz, _vp]
     L.cpsz_b200_debug_umma_gemm.argtypes = [_vp, _vp, _vp, _vp]
+    L.cpsz_b200_mlp_param_count.restype = _sz
+    L.cpsz_b200_mlp_create.argtypes = [_vp, C.c_uint64, C.POINTER(_vp)]
+    L.cpsz_b200_mlp_destroy.argtypes = [_vp]
+    L.cpsz_b200_mlp_get_params.argtypes = [_vp, _vp]
+    L.cpsz_b200_mlp_set_params.argtypes = [_vp, _vp]
+    L.cpsz_b200_mlp_forward.argtypes = [_vp, _vp, _sz, _vp]
+    L.cpsz_b200_mlp_train_step.argtypes = [_vp, _vp, _vp, _sz, C.c_float, _vp, _vp]
+    L.cpsz_b200_mlp_features_2d.argtypes = [_vp, _vp, _vp, _sz, _sz, _vp, _vp, _sz, _vp]
+    L.cpsz_b200_learned_labels_2d.argtypes = [_vp, _vp, _vp, _sz, _sz, _vp, _vp, _sz, C.c_int, _vp]
+    L.cpsz_b200_compress_2d_learned_f32.argtypes = [_vp, _vp, _vp, _vp, _sz, _sz, C.c_double, _vp, _vp, _sz,
+                                                    C.POINTER(_sz), _vp]
     if hasattr(L, "cpsz_b200_cp_check_2d"):
         L.cpsz_b200_cp_check_2d.argtypes = [_vp, _vp, _vp, _vp, _vp, _sz, _sz, _vp, C.POINTER(C.c_uint64)]
         L.cpsz_b200_cp_check_3d.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _sz, _sz, _vp,
@@ -335,6 +346,109 @@ def debug_eb3d(U, V, W, max_pwr_eb: float, ctx: Context | None = None):
     _check(lib().cpsz_b200_debug_eb3d(_h(ctx), U.ctypes.data, V.ctypes.data, W.ctypes.data, r1, r2, r3,
                                       float(max_pwr_eb), eb.ctypes.data, ids.ctypes.data))
     return eb, ids
+
+
+# ---- learned error bounds ----------------------------------------------------------------
+
+class Mlp:
+    """The learned bound proposer (99 -> 128 -> 128 -> 1 MLP on the tensor cores)."""
+
+    def __init__(self, ctx: Context, seed: int = 0, params=None):
+        self.ctx = ctx
+        h = _vp()
+        _check(lib().cpsz_b200_mlp_create(ctx.handle, seed, C.byref(h)))
+        self.handle = h
+        if params is not None:
+            self.set_params(params)
+
+    @staticmethod
+    def param_count() -> int:
+        return int(lib().cpsz_b200_mlp_param_count())
+
+    def params(self) -> np.ndarray:
+        out = np.empty(self.param_count(), np.float32)
+        _check(lib().cpsz_b200_mlp_get_params(self.handle, out.ctypes.data))
+        return out
+
+    def set_params(self, p) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.param_count()
+        _check(lib().cpsz_b200_mlp_set_params(self.handle, p.ctypes.data))
+
+    def forward(self, X_bits) -> np.ndarray:
+        X = np.ascontiguousarray(X_bits, np.uint16)
+        y = np.empty(X.shape[0], np.float32)
+        _check(lib().cpsz_b200_mlp_forward(self.handle, X.ctypes.data, X.shape[0], y.ctypes.data))
+        return y
+
+    def train_step(self, X_bits, t, lr: float, grads: bool = False):
+        """(mean squared error, gradients or None); Adam step when lr > 0."""
+        X = np.ascontiguousarray(X_bits, np.uint16)
+        t = np.ascontiguousarray(t, np.float32)
+        g = np.empty(self.param_count(), np.float32) if grads else None
+        loss = C.c_float()
+        _check(lib().cpsz_b200_mlp_train_step(self.handle, X.ctypes.data, t.ctypes.data, X.shape[0], float(lr),
+                                               g.ctypes.data if grads else None, C.byref(loss)))
+        return loss.value, g
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().cpsz_b200_mlp_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def mlp_features_2d(U, V, eb_analytic, idx, ctx: Context | None = None) -> np.ndarray:
+    U = np.ascontiguousarray(U, np.float32)
+    V = np.ascontiguousarray(V, np.float32)
+    eb = np.ascontiguousarray(eb_analytic, np.float64)
+    idx = np.ascontiguousarray(idx, np.int32)
+    X = np.empty((idx.size, 128), np.uint16)
+    _check(lib().cpsz_b200_mlp_features_2d(_h(ctx), U.ctypes.data, V.ctypes.data, U.shape[0], U.shape[1],
+                                           eb.ctypes.data, idx.ctypes.data, idx.size, X.ctypes.data))
+    return X
+
+
+def learned_labels_2d(U, V, eb_analytic, idx, steps: int = 16, ctx: Context | None = None) -> np.ndarray:
+    U = np.ascontiguousarray(U, np.float32)
+    V = np.ascontiguousarray(V, np.float32)
+    eb = np.ascontiguousarray(eb_analytic, np.float64)
+    idx = np.ascontiguousarray(idx, np.int32)
+    t = np.empty(idx.size, np.float32)
+    _check(lib().cpsz_b200_learned_labels_2d(_h(ctx), U.ctypes.data, V.ctypes.data, U.shape[0], U.shape[1],
+                                             eb.ctypes.data, idx.ctypes.data, idx.size, steps, t.ctypes.data))
+    return t
+
+
+def compress_2d_learned(U, V, max_pwr_eb: float = 0.1, mlp: Mlp | None = None, log2_mult=None, out=None,
+                        ctx: Context | None = None):
+    """2D offline blob with learned bounds; returns (blob bytes or size, stats dict)."""
+    pu, _, su = _ptr(U)
+    pv, _, sv = _ptr(V)
+    r1, r2 = su
+    pm = None
+    keep = None
+    if log2_mult is not None:
+        pm, keep, _ = _ptr(log2_mult)
+    ret_bytes = out is None
+    if out is None:
+        out = np.empty(int(np.prod(su)) * 8 + (8 << 20), np.uint8)
+    po, _, so = _ptr(out, np.uint8)
+    n = _sz()
+    stats = np.zeros(4, np.uint64)
+    _check(lib().cpsz_b200_compress_2d_learned_f32(_h(ctx), mlp.handle if mlp else None, pu, pv, r1, r2,
+                                                   float(max_pwr_eb), pm, po, int(np.prod(so)), C.byref(n),
+                                                   stats.ctypes.data))
+    st = {"passes": int(stats[0]), "reverted": int(stats[1]), "fell_back": int(stats[2]), "kept": int(stats[3])}
+    del keep
+    if ret_bytes:
+        return out[:n.value].tobytes(), st
+    return n.value, st
 
 
 def debug_libm(which: str, x, ctx: Context | None = None):

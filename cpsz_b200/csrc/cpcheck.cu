@@ -436,6 +436,59 @@ __global__ void __launch_bounds__(128) cp3d_kernel(const float* __restrict__ Ua,
   flush(tl, counts);
 }
 
+// ---- labels for the learned bound proposer ---------------------------------------
+// For a vertex with analytic bound e_a: the largest t in [0, tmax] (bisection,
+// `steps` halvings) such that moving the vertex alone to any corner of the box
+// (u +- |u| e, v +- |v| e), e = e_a 2^t, leaves the CP codes of its six
+// incident triangles unchanged.
+__global__ void labels2d_kernel(const float* __restrict__ U, const float* __restrict__ V, int r1, int r2,
+                                const double* __restrict__ eb_a, const int* __restrict__ idx, int n, int steps,
+                                float tmax, float* __restrict__ out) {
+  // incident triangles: cell offset (di, dj), kind, position of the vertex
+  const int inc[6][4] = {{0, 0, 0, 0}, {0, 0, 1, 0}, {-1, 0, 0, 1}, {-1, -1, 0, 2}, {-1, -1, 1, 2}, {0, -1, 1, 1}};
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const int v = idx[s];
+    const int i = v / r2, j = v - (v / r2) * r2;
+    float tu[6][3], tv[6][3];
+    int kind[6], pos[6], orig[6], nt = 0;
+    for (int q = 0; q < 6; q++) {
+      const int ci = i + inc[q][0], cj = j + inc[q][1], k = inc[q][2];
+      if (ci < 0 || cj < 0 || ci > r1 - 2 || cj > r2 - 2) continue;
+      const int pi[3] = {ci, ci + (k == 0), ci + 1};
+      const int pj[3] = {cj, cj + (k == 1), cj + 1};
+      for (int p = 0; p < 3; p++) {
+        tu[nt][p] = U[(size_t)pi[p] * r2 + pj[p]];
+        tv[nt][p] = V[(size_t)pi[p] * r2 + pj[p]];
+      }
+      kind[nt] = k;
+      pos[nt] = inc[q][3];
+      orig[nt] = tri_cp(tu[nt], tv[nt], k);
+      nt++;
+    }
+    const float u0 = U[v], v0 = V[v];
+    const double e0 = eb_a[v];
+    float lo = 0.f, hi = tmax;
+    for (int it = 0; it < steps; it++) {
+      const float mid = 0.5f * (lo + hi);
+      const double e = e0 * exp2((double)mid);
+      bool pass = e == e;
+      for (int c = 0; c < 4 && pass; c++) {
+        const float cu = (float)((double)u0 + ((c & 1) ? 1.0 : -1.0) * fabs((double)u0) * e);
+        const float cv = (float)((double)v0 + ((c & 2) ? 1.0 : -1.0) * fabs((double)v0) * e);
+        for (int q = 0; q < nt && pass; q++) {
+          float a[3] = {tu[q][0], tu[q][1], tu[q][2]}, b[3] = {tv[q][0], tv[q][1], tv[q][2]};
+          a[pos[q]] = cu;
+          b[pos[q]] = cv;
+          pass = tri_cp(a, b, kind[q]) == orig[q];
+        }
+      }
+      if (pass) lo = mid;
+      else hi = mid;
+    }
+    out[s] = lo;
+  }
+}
+
 }  // namespace
 
 int launch_cp_check_2d(cpsz_b200_ctx* ctx, const float* Ua, const float* Va, const float* Ub, const float* Vb, int r1,
@@ -447,6 +500,16 @@ int launch_cp_check_2d(cpsz_b200_ctx* ctx, const float* Ua, const float* Va, con
   cp2d_kernel<<<(int)g, 256, 0, ctx->stream>>>(Ua, Va, Ub, Vb, r1, r2, cells, counts);
   count_launch(ctx);
   return check_launch("cp2d_kernel");
+}
+
+int launch_labels_2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, const double* eb_a,
+                     const int* idx, int n, int steps, float tmax, float* out) {
+  if (n <= 0) return CPSZ_OK;
+  int g = (n + 127) / 128;
+  if (g > ctx->num_sms * 8) g = ctx->num_sms * 8;
+  labels2d_kernel<<<g, 128, 0, ctx->stream>>>(U, V, r1, r2, eb_a, idx, n, steps, tmax, out);
+  count_launch(ctx);
+  return check_launch("labels2d_kernel");
 }
 
 int launch_cp_check_3d(cpsz_b200_ctx* ctx, const float* Ua, const float* Va, const float* Wa, const float* Ub,

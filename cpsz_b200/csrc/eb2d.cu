@@ -140,3 +140,74 @@ int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int 
 }
 
 }  // namespace cpsz
+
+namespace cpsz {
+
+namespace {
+
+// Quantization of given per-vertex bounds (the learned-bound path): the same
+// id arithmetic, symbols and wavefront pairs as eb2d_kernel, with the bound
+// read from eb_in instead of derived from the triangles.
+__global__ void __launch_bounds__(256) quant2d_kernel(const float* __restrict__ U, const float* __restrict__ V,
+                                                      size_t n, const double* __restrict__ eb_in,
+                                                      const double* __restrict__ thr_tab, int thr_n,
+                                                      uint8_t* __restrict__ ids_u, uint8_t* __restrict__ ids_v,
+                                                      unsigned long long* __restrict__ hist, int* __restrict__ flag,
+                                                      float2* __restrict__ pair_u, float2* __restrict__ pair_v) {
+  __shared__ double tab[QUANT_TAB_MAX];
+  __shared__ unsigned int shist[256];
+  for (int k = threadIdx.x; k < 256; k += blockDim.x) shist[k] = 0;
+  for (int k = threadIdx.x; k < thr_n; k += blockDim.x) tab[k] = thr_tab[k];
+  __syncthreads();
+  const double thr = tab[0];
+  for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (size_t)gridDim.x * blockDim.x) {
+    const double eb = eb_in[g];
+    const float uu = U[g], vv = V[g];
+    uint8_t code[2];
+    int sym[2];
+    const double ev[2] = {(double)fabsf(uu) * eb, (double)fabsf(vv) * eb};
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+      const double e = ev[c];
+      if (e <= thr) {
+        code[c] = ID_ZERO;
+        sym[c] = 0;
+      } else {
+        int ex = (int)((__double_as_longlong(e) >> 52) & 0x7ff) - 1023;
+        int id = dev::count_thresholds(tab, thr_n, e, (ex + 52) >> 1);
+        if (id > ID_MAX_2D) {
+          atomicOr(flag, FLAG_ID_OVERFLOW);
+          id = ID_MAX_2D;
+        }
+        code[c] = (uint8_t)id;
+        sym[c] = id;
+      }
+    }
+    ids_u[g] = code[0];
+    ids_v[g] = code[1];
+    pair_u[g] = make_float2(uu, code[0] == ID_ZERO ? __int_as_float(0x7FC00000)
+                                                   : __int_as_float((127 + 52 - 2 * (int)code[0]) << 23));
+    pair_v[g] = make_float2(vv, code[1] == ID_ZERO ? __int_as_float(0x7FC00000)
+                                                   : __int_as_float((127 + 52 - 2 * (int)code[1]) << 23));
+    atomicAdd(&shist[sym[0]], 1u);
+    atomicAdd(&shist[sym[1]], 1u);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < 256; k += blockDim.x)
+    if (shist[k]) atomicAdd(&hist[k], (unsigned long long)shist[k]);
+}
+
+}  // namespace
+
+int launch_quant2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t n, const double* eb_in,
+                   const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
+                   float2* pair_u, float2* pair_v) {
+  size_t g = (n + 255) / 256;
+  if (g > (size_t)ctx->num_sms * 8) g = (size_t)ctx->num_sms * 8;
+  quant2d_kernel<<<(int)(g ? g : 1), 256, 0, ctx->stream>>>(U, V, n, eb_in, d_thr_tab, thr_n, ids_u, ids_v, hist,
+                                                            ctx->d_flag, pair_u, pair_v);
+  count_launch(ctx);
+  return check_launch("quant2d_kernel");
+}
+
+}  // namespace cpsz

@@ -28,6 +28,11 @@ int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int 
                 const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
                 float2* pair_u, float2* pair_v, double* eb_out = nullptr);
 
+// The same quantization for given per-vertex bounds eb_in[n] (learned bounds).
+int launch_quant2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t n, const double* eb_in,
+                   const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
+                   float2* pair_u, float2* pair_v);
+
 // ---- 2D Lorenzo wavefront ------------------------------------------------------
 // One field of the wavefront.  Raster arrays carry their own row pitch (elements).
 struct WaveField {
@@ -159,6 +164,12 @@ int launch_wave3d_planes(cpsz_b200_ctx* ctx, bool decompress, const float4* in, 
 // one field, cells whose CP type differs}; b may be null.
 int launch_cp_check_2d(cpsz_b200_ctx* ctx, const float* Ua, const float* Va, const float* Ub, const float* Vb, int r1,
                        int r2, uint8_t* cells, unsigned long long* counts);
+// Training labels of the learned bound proposer: per vertex idx[s] the largest
+// log2 multiplier t in [0, tmax] of its analytic bound (bisection, `steps`
+// halvings) under which moving the vertex alone to any corner of its bound box
+// keeps the CP codes of its incident triangles.
+int launch_labels_2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, const double* eb_a,
+                     const int* idx, int n, int steps, float tmax, float* out);
 int launch_cp_check_3d(cpsz_b200_ctx* ctx, const float* Ua, const float* Va, const float* Wa, const float* Ub,
                        const float* Vb, const float* Wb, int r1, int r2, int r3, uint8_t* cells,
                        unsigned long long* counts);
@@ -167,6 +178,32 @@ int launch_cp_check_3d(cpsz_b200_ctx* ctx, const float* Ua, const float* Va, con
 // D (128 x 128 fp32, row-major) = A (128 x 128 bf16) * B (128 x 128 bf16)^T on
 // one CTA through shared memory and TMEM (device pointers).
 int launch_umma_selftest(cpsz_b200_ctx* ctx, const void* A, const void* B, float* D);
+
+// MLP 99 (padded 128) -> 128 -> 128 -> 1 with ReLU.  Flat fp32 parameters:
+// W1 [128 x 128] | b1 [128] | W2 [128 x 128] | b2 [128] | w3 [128] | b3.
+constexpr int MLP_PARAMS = 2 * 16384 + 3 * 128 + 1;
+struct MlpParams {
+  float* p;    // master weights
+  float* g;    // gradient accumulators
+  float* m;    // Adam moments
+  float* v;
+  void* w1b;   // bf16 copies of W1 and W2 (tensor-core operands)
+  void* w2b;
+};
+// y[M] from features X (bf16 [M x 128], device) or, with X null, from the
+// features of every vertex of field (U, V) (r1 x r2 = M) with analytic bounds
+// eb_a.  H1 / H2 (optional, bf16 [M x 128]) keep the activations for training.
+int launch_mlp_forward(cpsz_b200_ctx* ctx, const MlpParams& w, const void* X, const float* U, const float* V,
+                       const double* eb_a, int r1, int r2, int M, float* y, void* H1, void* H2);
+// Accumulates the gradients of sum (y - t)^2 * grad_scale / 2 into w.g and the
+// squared error into *loss (device).
+int launch_mlp_backward(cpsz_b200_ctx* ctx, const MlpParams& w, const void* X, const void* H1, const void* H2,
+                        const float* y, const float* t, int M, float grad_scale, float* loss);
+int launch_mlp_adam(cpsz_b200_ctx* ctx, const MlpParams& w, float lr, int step);
+int launch_mlp_cast(cpsz_b200_ctx* ctx, const MlpParams& w);
+// Features (bf16 [n x 128]) of the vertices idx[0..n) of field (U, V).
+int launch_mlp_features(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, const double* eb_a,
+                        const int* idx, int n, void* X);
 
 // ---- generic scans ----------------------------------------------------------------
 size_t scan_u32_tmp_bytes(size_t n);

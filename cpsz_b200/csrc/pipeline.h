@@ -28,8 +28,10 @@ struct StageTap {
 
 int build_wave_items(int nfields, const int* r1s, std::vector<WaveItem>& items);
 
+// eb_ext (optional, device, N doubles): per-vertex bounds to quantize instead
+// of the derived ones (the learned-bound path).
 int compress_2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2, double max_pwr_eb,
-                Blob2D* out, const StageTap* tap);
+                Blob2D* out, const StageTap* tap, const double* eb_ext = nullptr);
 int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_size, size_t r1, size_t r2, float* U,
                   float* V);
 // n fields; blobs back to back into `out` (host or device), offsets[0..n].

@@ -78,6 +78,7 @@ struct Job2D {
   int r1 = 0, r2 = 0, ngroups = 0;
   size_t N = 0, nseg = 0, nblocks = 0;
   double eb = 0;
+  const double* eb_ext = nullptr;  // given per-vertex bounds (device), else derived
   bool dev_in = false;
   size_t ids_bits_cap = 0, codes_bits_cap = 0, blob_cap = 0;
   DevBuf d{};
@@ -339,8 +340,12 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   }
   mark(ctx, "eb2d");
   for (Job2D& j : jobs) {
-    CPSZ_TRY(launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N, j.d.hist_ids,
-                         j.d.pairs[0], j.d.pairs[1]));
+    if (j.eb_ext)
+      CPSZ_TRY(launch_quant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N, j.d.hist_ids,
+                              j.d.pairs[0], j.d.pairs[1]));
+    else
+      CPSZ_TRY(launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N, j.d.hist_ids,
+                           j.d.pairs[0], j.d.pairs[1]));
     CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_hist_ids, j.d.hist_ids, 256 * 8, cudaMemcpyDeviceToHost, st));
   }
   mark(ctx, "eb2d_end");
@@ -481,9 +486,10 @@ int build_wave_items(int nfields, const int* r1s, std::vector<WaveItem>& items) 
 }
 
 int compress_2d(cpsz_b200_ctx* ctx, const float* U_in, const float* V_in, size_t r1s, size_t r2s, double max_pwr_eb,
-                Blob2D* out, const StageTap* tap) {
+                Blob2D* out, const StageTap* tap, const double* eb_ext) {
   std::vector<Job2D> jobs(1);
   CPSZ_TRY(job_init(jobs[0], U_in, V_in, r1s, r2s, max_pwr_eb));
+  jobs[0].eb_ext = eb_ext;
   CPSZ_TRY(arena_reserve(ctx, pass_bytes(jobs)));
   CPSZ_TRY(pinned_reserve(ctx, PINNED_BASE + JOB_PINNED));
   CPSZ_TRY(run_pass(ctx, jobs, tap));

@@ -91,6 +91,46 @@ int cpsz_b200_compress_2d_batch_f32(cpsz_b200_ctx* ctx, int n_fields, const floa
                                     const size_t* r1, const size_t* r2, const double* max_pwr_eb, unsigned char* out,
                                     size_t out_cap, size_t* offsets);
 
+/* ---- learned error bounds (2D offline format, decoder unchanged) ----------
+ * A small MLP (99 -> 128 -> 128 -> 1, ReLU; BF16 tensor-core kernels with FP32
+ * accumulation) proposes per vertex a log2 multiplier t in [0, 16] of the
+ * analytic bound from a vertex's 7x7 (u,v) neighbourhood (normalised by its
+ * largest |value|) and log2 of its analytic bound.  The fallback loop
+ * compresses with the proposals, reconstructs, compares every cell's critical
+ * point exactly with the original, reverts the vertices of offending cells to
+ * their analytic bounds and repeats until no cell differs.  The result is an
+ * ordinary 2D offline blob. */
+typedef struct cpsz_b200_mlp cpsz_b200_mlp;
+size_t cpsz_b200_mlp_param_count(void);
+/* He-initialised MLP on ctx's device (deterministic in seed). */
+int cpsz_b200_mlp_create(cpsz_b200_ctx* ctx, uint64_t seed, cpsz_b200_mlp** mlp);
+int cpsz_b200_mlp_destroy(cpsz_b200_mlp* mlp);
+/* Flat fp32 parameters (host): W1 [128x128] | b1 [128] | W2 [128x128] | b2 [128] | w3 [128] | b3. */
+int cpsz_b200_mlp_get_params(cpsz_b200_mlp* mlp, float* params);
+int cpsz_b200_mlp_set_params(cpsz_b200_mlp* mlp, const float* params);
+/* y[n] for features X (bf16 bits, n x 128, host or device). */
+int cpsz_b200_mlp_forward(cpsz_b200_mlp* mlp, const uint16_t* X, size_t n, float* y);
+/* Forward + backward of mean (y - t)^2 over n samples, then Adam (lr > 0);
+ * grads (optional, host, param_count floats) and loss (mean) out. */
+int cpsz_b200_mlp_train_step(cpsz_b200_mlp* mlp, const uint16_t* X, const float* t, size_t n, float lr, float* grads,
+                             float* loss);
+/* Features (bf16 bits, n x 128) of vertices idx[0..n) of field (U, V) with
+ * analytic bounds eb_analytic[r1*r2]. */
+int cpsz_b200_mlp_features_2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2,
+                              const double* eb_analytic, const int32_t* idx, size_t n, uint16_t* X);
+/* Training labels: per vertex the largest log2 multiplier (bisection, `steps`
+ * halvings of [0, 16]) that keeps its incident cells' CPs when the vertex
+ * alone moves to any corner of its bound box. */
+int cpsz_b200_learned_labels_2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2,
+                                const double* eb_analytic, const int32_t* idx, size_t n, int steps, float* t);
+/* Compression with learned bounds: proposals from `mlp`, or the given
+ * log2_mult[r1*r2] (host or device) when not null.  stats (optional): {compress
+ * passes, vertices reverted, 1 if the loop gave up and fell back to the
+ * analytic bounds, vertices whose enlarged bound was kept}. */
+int cpsz_b200_compress_2d_learned_f32(cpsz_b200_ctx* ctx, cpsz_b200_mlp* mlp, const float* U, const float* V,
+                                      size_t r1, size_t r2, double max_pwr_eb, const float* log2_mult,
+                                      unsigned char* out, size_t out_cap, size_t* blob_size, uint64_t stats[4]);
+
 /* ---- 3D offline (log) CP-preserving compression -------------------------
  * Replaces sz_compress_cp_preserve_3d_offline_log<float>
  * (reference include/sz_compress_cp_preserve_3d.hpp:8,
