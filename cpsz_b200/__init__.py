@@ -82,6 +82,7 @@ def _declare(L):
     L.cpsz_b200_blob_size_3d.restype = _sz
     L.cpsz_b200_libm_tables_prepare.argtypes = [C.c_char_p]
     L.cpsz_b200_debug_eb3d.argtypes = [_vp, _vp, _vp, _vp, _sz, _sz, _sz, C.c_double, _vp, _vp]
+    L.cpsz_b200_debug_eb2d.argtypes = [_vp, _vp, _vp, _sz, _sz, C.c_double, _vp, _vp]
     L.cpsz_b200_debug_libm.argtypes = [_vp, C.c_int, _vp, _sz, _vp]
     L.cpsz_b200_debug_umma_gemm.argtypes = [_vp, _vp, _vp, _vp]
     L.cpsz_b200_mlp_param_count.restype = _sz
@@ -335,6 +336,18 @@ def blob_size_3d(blob: bytes, r1: int, r2: int, r3: int) -> int:
 def libm_tables_prepare(path: str | None = None) -> None:
     """Builds (or loads) the host log2f / exp2f tables the 3D kernels use."""
     _check(lib().cpsz_b200_libm_tables_prepare(path.encode() if path else None))
+
+
+def debug_eb2d(U, V, max_pwr_eb: float, ctx: Context | None = None):
+    """Per-vertex 2D analytic bound (float64) and id bytes (2N; 255 = precision 0) from the GPU kernel."""
+    U = np.ascontiguousarray(U, np.float32)
+    V = np.ascontiguousarray(V, np.float32)
+    r1, r2 = U.shape
+    eb = np.empty(U.shape, np.float64)
+    ids = np.empty(2 * U.size, np.uint8)
+    _check(lib().cpsz_b200_debug_eb2d(_h(ctx), U.ctypes.data, V.ctypes.data, r1, r2, float(max_pwr_eb),
+                                      eb.ctypes.data, ids.ctypes.data))
+    return eb, ids
 
 
 def debug_eb3d(U, V, W, max_pwr_eb: float, ctx: Context | None = None):

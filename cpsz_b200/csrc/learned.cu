@@ -85,8 +85,8 @@ __global__ void revert_kernel(uint8_t* __restrict__ revert, const double* __rest
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     if (revert[i]) {
       revert[i] = 0;
+      c += eb[i] != eb_a[i];
       eb[i] = eb_a[i];
-      c++;
     }
   for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
@@ -125,7 +125,8 @@ int ensure_scratch(cpsz_b200_mlp* m, size_t bytes) {
 
 }  // namespace
 
-// The fallback loop (see the file comment).  stats: {compress passes,
+// The fallback loop (see the file comment).  stats: {passes (reconstruction
+// passes + the final compression),
 // vertices reverted, 1 if the loop gave up and the analytic bounds were used
 // everywhere, vertices whose enlarged bound was kept}.
 int compress_2d_learned(cpsz_b200_ctx* ctx, cpsz_b200_mlp* mlp, const float* U_in, const float* V_in, size_t r1s,
@@ -190,9 +191,12 @@ int compress_2d_learned(cpsz_b200_ctx* ctx, cpsz_b200_mlp* mlp, const float* U_i
   count_launch(ctx);
   CPSZ_TRY(check_launch("scale_bounds_kernel"));
   CPSZ_TRY(launch_cp_check_2d(ctx, dU, dV, nullptr, nullptr, r1, r2, cells_a, counts + 8));
+  // the loop's passes stop after the Lorenzo stage (the reconstruction is all
+  // the check needs); one full compression follows with the final bounds
   StageTap tap;
   tap.recon[0] = rec_u;
   tap.recon[1] = rec_v;
+  tap.recon_only = true;
   uint64_t reverted = 0;
   int it = 0;
   unsigned long long h[4] = {0, 0, 0, 0};
@@ -216,11 +220,13 @@ int compress_2d_learned(cpsz_b200_ctx* ctx, cpsz_b200_mlp* mlp, const float* U_i
   if (fallback) {
     // not converged: the analytic bounds everywhere (the plain compressor)
     CPSZ_TRY(compress_2d(ctx, dU, dV, r1s, r2s, max_pwr_eb, out, nullptr, nullptr));
+  } else {
+    CPSZ_TRY(compress_2d(ctx, dU, dV, r1s, r2s, max_pwr_eb, out, nullptr, eb));
   }
   unsigned long long enlarged = 0;
   CPSZ_CUDA_TRY(cudaMemcpy(&enlarged, counts + 4, 8, cudaMemcpyDeviceToHost));
   if (stats) {
-    stats[0] = (uint64_t)it + 1;
+    stats[0] = (uint64_t)it + 2;
     stats[1] = reverted;
     stats[2] = fallback ? 1 : 0;
     stats[3] = fallback ? 0 : enlarged - reverted;

@@ -24,6 +24,7 @@ struct StageTap {
   uint16_t* codes_blocks[2] = {nullptr, nullptr};
   float* unpred[2] = {nullptr, nullptr};
   float* recon[2] = {nullptr, nullptr};      // compressor-side reconstruction (raster)
+  bool recon_only = false;                   // stop after the Lorenzo stage (no blob)
 };
 
 int build_wave_items(int nfields, const int* r1s, std::vector<WaveItem>& items);

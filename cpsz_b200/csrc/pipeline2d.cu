@@ -383,6 +383,11 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   CPSZ_CUDA_TRY(cudaMemsetAsync(queue, 0, 64, st));
   mark(ctx, "wave2d_compress");
   CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, 0));
+  if (tap && tap->recon_only) {
+    int flag = 0;
+    CPSZ_TRY(read_flag(ctx, &flag));
+    return flag ? flag_error(flag) : CPSZ_OK;
+  }
   mark(ctx, "blocks+hist+unpred");
 
   // ---- stage 3: block order, histograms, unpredictables ----
