@@ -52,6 +52,8 @@ WORKLOADS = {
     "3d_256x256x256_eb0.05": ("3d", (256, 256, 256), 0.05, "cfg2"),
     # 256 fields, sides uniform in [128, 4096], eb in {0.01, 0.05, 0.1}, one flow per 40x40 cells
     "batch_256x2d_cfg3": ("batch", None, None, "cfg3"),
+    # the cfg1 field with learned bounds (trained proposer, fallback loop to 0 CP differences)
+    "learned_2d_8192x8192_eb0.1": ("learned", (8192, 8192), 0.1, "cfg1"),
 }
 DEFAULT = "2d_8192x8192_eb0.1"
 
@@ -157,7 +159,7 @@ def reference_samples(workload: str, fields, eb):
     """Tiles of the workload sized for ~1 s of reference CPU work each."""
     kind = WORKLOADS[workload][0]
     tiles = []
-    if kind == "2d":
+    if kind in ("2d", "learned"):
         U, V = fields
         s = 1024
         for i in range(0, U.shape[0] - s + 1, s):
@@ -192,6 +194,7 @@ def run_reference(args, rank, world):
         fields, eb = make_fields(args.workload)
         tiles = reference_samples(args.workload, fields, eb)
         tile_ebs = [eb] * len(tiles)
+        kind = "2d" if kind == "learned" else kind
     cores = os.cpu_count() or 1
     tmp = tempfile.mkdtemp(prefix="cpsz_ref_")
     paths = []
@@ -363,6 +366,59 @@ def run_product(args, rank, world, device):
     }
 
 
+def run_learned(args, rank, world, device):
+    """Learned-bound compression of the cfg1 field: every step runs the MLP over
+    all vertices, the fallback loop's reconstruction passes and the final
+    compression (fields resident in HBM, blob written to HBM); the plain
+    compressor's ratio and the exact CP comparison are reported beside it."""
+    import torch
+
+    import cpsz_b200
+    from cpsz_b200 import learned
+
+    kind, shape, eb, _ = WORKLOADS[args.workload]
+    fields, eb = make_fields("2d_8192x8192_eb0.1", seed_offset=rank)
+    raw = sum(a.nbytes for a in fields)
+    ctx = cpsz_b200.Context(device)
+    mlp = learned.load(ctx)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=device)
+    dev = [torch.from_numpy(a).to(f"cuda:{device}") for a in fields]
+    out = torch.empty(raw + (64 << 20), dtype=torch.uint8, device=f"cuda:{device}")
+    clk = Clocks(device).__enter__()
+    for _ in range(args.warmup):
+        size, st = cpsz_b200.compress_2d_learned(*dev, eb, mlp=mlp, out=out, ctx=ctx)
+    torch.cuda.synchronize(device)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    launches0 = ctx.kernel_launches
+    try:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            size, st = cpsz_b200.compress_2d_learned(*dev, eb, mlp=mlp, out=out, ctx=ctx)
+        ev1.record(stream)
+        torch.cuda.synchronize(device)
+    finally:
+        clk.__exit__(None, None, None)
+    ms = ev0.elapsed_time(ev1) / args.steps
+    launches = (ctx.kernel_launches - launches0) // max(args.steps, 1)
+    blob = out[:size].cpu().numpy().tobytes()
+    plain = cpsz_b200.sz_compress_cp_preserve_2d_offline(*fields, max_pwr_eb=eb, ctx=ctx)
+    dU, dV = cpsz_b200.sz_decompress_cp_preserve_2d_offline(blob, *shape, ctx=ctx)
+    cp = cpsz_b200.cp_check_2d(fields[0], fields[1], dU, dV, ctx=ctx)
+    z_learned = len(cpsz_b200.sz_lossless_compress(blob, 3))
+    z_plain = len(cpsz_b200.sz_lossless_compress(plain, 3))
+    return {
+        "metric": "compress_GBps", "value": round(raw * world / (ms / 1e3) / 1e9, 3), "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f64+f32", "data": "synthetic",
+        "config": {"workload": args.workload, "eb": eb, "points": int(raw // 8), "inputs_exceed_l2": True,
+                   "parallelism": f"replicas{world}", "value_io": "fields resident in HBM, blob written to HBM"},
+        "ratio": round(raw / z_learned, 4), "ratio_pre_zstd": round(raw / size, 4),
+        "plain_ratio": round(raw / z_plain, 4), "plain_ratio_pre_zstd": round(raw / len(plain), 4),
+        "cp_check": cp, "loop": st, "cpu_baseline": None, "clocks": clk.summary(), "gpu_launches": launches,
+    }
+
+
 def make_batch(seed_offset: int = 0):
     from cpsz_b200 import workloads as W
 
@@ -484,8 +540,8 @@ def main():
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    if WORKLOADS[args.workload][0] == "batch":
-        line = run_batch(args, rank, world, local)
+    if WORKLOADS[args.workload][0] in ("batch", "learned"):
+        line = (run_batch if WORKLOADS[args.workload][0] == "batch" else run_learned)(args, rank, world, local)
         if world > 1:
             import torch.distributed as dist
 
