@@ -31,7 +31,7 @@ __global__ void __launch_bounds__(NT) eb2d_kernel(const float* __restrict__ U, c
                                                   int thr_n, uint8_t* __restrict__ ids_u, uint8_t* __restrict__ ids_v,
                                                   unsigned long long* __restrict__ hist, int* __restrict__ flag,
                                                   float2* __restrict__ pair_u, float2* __restrict__ pair_v,
-                                                  double* __restrict__ eb_out) {
+                                                  double* __restrict__ eb_out, int row_begin, int row_end) {
   __shared__ float su[TY + 2][TX + 3];
   __shared__ float sv[TY + 2][TX + 3];
   __shared__ double tri[2][CY][CX];
@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(NT) eb2d_kernel(const float* __restrict__ U, c
   __shared__ unsigned int shist[256];
 
   const int tid = threadIdx.x;
-  const int i0 = blockIdx.y * TY, j0 = blockIdx.x * TX;
+  const int i0 = row_begin + blockIdx.y * TY, j0 = blockIdx.x * TX;
   for (int k = tid; k < 256; k += NT) shist[k] = 0;
   for (int k = tid; k < thr_n; k += NT) tab[k] = thr_tab[k];
   // vertex halo: rows i0-1 .. i0+TY, cols j0-1 .. j0+TX
@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(NT) eb2d_kernel(const float* __restrict__ U, c
   for (int k = tid; k < TY * TX; k += NT) {
     int a = k / TX, b = k % TX;
     int gi = i0 + a, gj = j0 + b;
-    if (gi >= r1 || gj >= r2) continue;
+    if (gi >= row_end || gj >= r2) continue;
     // vertex (gi, gj) is local (a+1, b+1); cell (gi-1+x, gj-1+y) is tri[.][a+x][b+y]
     double eb = max_pwr_eb;
     bool up = gi >= 1, left = gj >= 1, down = gi < r1 - 1, right = gj < r2 - 1;
@@ -131,10 +131,12 @@ __global__ void __launch_bounds__(NT) eb2d_kernel(const float* __restrict__ U, c
 
 int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, double max_pwr_eb,
                 const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
-                float2* pair_u, float2* pair_v, double* eb_out) {
-  dim3 grid((r2 + TX - 1) / TX, (r1 + TY - 1) / TY);
+                float2* pair_u, float2* pair_v, double* eb_out, int row_begin, int row_end) {
+  if (row_end < 0) row_end = r1;
+  if (row_end <= row_begin) return CPSZ_OK;
+  dim3 grid((r2 + TX - 1) / TX, (row_end - row_begin + TY - 1) / TY);
   eb2d_kernel<<<grid, NT, 0, ctx->stream>>>(U, V, r1, r2, max_pwr_eb, d_thr_tab, thr_n, ids_u, ids_v, hist,
-                                            ctx->d_flag, pair_u, pair_v, eb_out);
+                                            ctx->d_flag, pair_u, pair_v, eb_out, row_begin, row_end);
   count_launch(ctx);
   return check_launch("eb2d_kernel");
 }

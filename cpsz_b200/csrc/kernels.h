@@ -24,9 +24,11 @@ constexpr int FLAG_RAW_RANGE = 8;     // an unpredictable-value index fell outsi
 constexpr int FLAG_OUT_CAPACITY = 16; // an output stream did not fit its buffer
 
 // ---- 2D error bounds ---------------------------------------------------------
+// Rows [row_begin, row_end) of the vertex outputs (row_end < 0: all rows); the
+// kernel reads rows row_begin - 1 .. row_end of U and V.
 int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, double max_pwr_eb,
                 const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
-                float2* pair_u, float2* pair_v, double* eb_out = nullptr);
+                float2* pair_u, float2* pair_v, double* eb_out = nullptr, int row_begin = 0, int row_end = -1);
 
 // The same quantization for given per-vertex bounds eb_in[n] (learned bounds).
 int launch_quant2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t n, const double* eb_in,

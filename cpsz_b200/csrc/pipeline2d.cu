@@ -331,21 +331,44 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   mark(ctx, "h2d+setup");
   CPSZ_CUDA_TRY(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), st));
   CPSZ_CUDA_TRY(cudaMemcpyAsync(thr_tab, qt.t, QUANT_TAB_MAX * 8, cudaMemcpyHostToDevice, st));
-  for (Job2D& j : jobs) {
-    if (!j.dev_in) {
-      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.U, j.U_in, 4 * j.N, cudaMemcpyHostToDevice, st));
-      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.V, j.V_in, 4 * j.N, cudaMemcpyHostToDevice, st));
-    }
-    CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.hist_ids, 0, 256 * 8, st));
-  }
+  for (Job2D& j : jobs) CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.hist_ids, 0, 256 * 8, st));
   mark(ctx, "eb2d");
   for (Job2D& j : jobs) {
-    if (j.eb_ext)
-      CPSZ_TRY(launch_quant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N, j.d.hist_ids,
-                              j.d.pairs[0], j.d.pairs[1]));
-    else
-      CPSZ_TRY(launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N, j.d.hist_ids,
-                           j.d.pairs[0], j.d.pairs[1]));
+    if (j.dev_in) {
+      if (j.eb_ext)
+        CPSZ_TRY(launch_quant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
+                                j.d.hist_ids, j.d.pairs[0], j.d.pairs[1]));
+      else
+        CPSZ_TRY(launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
+                             j.d.hist_ids, j.d.pairs[0], j.d.pairs[1]));
+    } else {
+      // Host input: row chunks go up on the second stream and the bound kernel
+      // runs band by band as soon as a band's rows and the row below it are
+      // on the device, so the transfer overlaps the bound derivation.
+      const int K = (j.N >= ((size_t)1 << 22) && !j.eb_ext) ? cpsz_b200_ctx::kUploadChunks : 1;
+      const int R = (int)align_up((size_t)(j.r1 + K - 1) / K, 16);
+      const int nch = (j.r1 + R - 1) / R;
+      CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[2], st));
+      CPSZ_CUDA_TRY(cudaStreamWaitEvent(ctx->aux, ctx->ev[2], 0));
+      for (int c = 0; c < nch; c++) {
+        const size_t off = (size_t)c * R * j.r2;
+        const size_t cnt = (size_t)(std::min(j.r1, (c + 1) * R) - c * R) * j.r2;
+        CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.U + off, j.U_in + off, 4 * cnt, cudaMemcpyHostToDevice, ctx->aux));
+        CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.V + off, j.V_in + off, 4 * cnt, cudaMemcpyHostToDevice, ctx->aux));
+        CPSZ_CUDA_TRY(cudaEventRecord(ctx->up_ev[c], ctx->aux));
+      }
+      for (int c = 0; c < nch; c++) {
+        CPSZ_CUDA_TRY(cudaStreamWaitEvent(st, ctx->up_ev[c], 0));
+        if (c + 1 < nch) CPSZ_CUDA_TRY(cudaStreamWaitEvent(st, ctx->up_ev[c + 1], 0));
+        if (j.eb_ext)
+          CPSZ_TRY(launch_quant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
+                                  j.d.hist_ids, j.d.pairs[0], j.d.pairs[1]));
+        else
+          CPSZ_TRY(launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
+                               j.d.hist_ids, j.d.pairs[0], j.d.pairs[1], nullptr, c * R,
+                               std::min(j.r1, (c + 1) * R)));
+      }
+    }
     CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_hist_ids, j.d.hist_ids, 256 * 8, cudaMemcpyDeviceToHost, st));
   }
   mark(ctx, "eb2d_end");

@@ -249,6 +249,7 @@ int cpsz_b200_ctx_create(int device, cpsz_b200_ctx** out) {
   CPSZ_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   CPSZ_CUDA_TRY(cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking));
   for (auto& ev : c->ev) CPSZ_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  for (auto& ev : c->up_ev) CPSZ_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   CPSZ_CUDA_TRY(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
   CPSZ_CUDA_TRY(cudaMalloc((void**)&c->d_flag, 64));
   CPSZ_CUDA_TRY(cudaMemset(c->d_flag, 0, 64));
@@ -270,6 +271,8 @@ int cpsz_b200_ctx_destroy(cpsz_b200_ctx* c) {
   if (c->libm_mem) cudaFree(c->libm_mem);
   delete (cpsz::LibmTables*)c->libm_view;
   for (auto& ev : c->ev)
+    if (ev) cudaEventDestroy(ev);
+  for (auto& ev : c->up_ev)
     if (ev) cudaEventDestroy(ev);
   for (auto& ev : c->tev)
     if (ev) cudaEventDestroy(ev);

@@ -72,6 +72,9 @@ struct cpsz_b200_ctx {
   cudaStream_t stream = nullptr;
   cudaStream_t aux = nullptr;  // second stream for overlapping independent stages
   cudaEvent_t ev[8] = {};
+  // chunked host-to-device uploads (one event per chunk, recorded on `aux`)
+  static constexpr int kUploadChunks = 8;
+  cudaEvent_t up_ev[kUploadChunks] = {};
   cpsz::Arena arena;
   void* pinned = nullptr;
   size_t pinned_cap = 0;
