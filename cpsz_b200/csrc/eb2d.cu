@@ -56,19 +56,23 @@ __global__ void __launch_bounds__(NT) eb2d_kernel(const float* __restrict__ U, c
     sv[a][b] = v;
   }
   __syncthreads();
-  // cells (ci, cj) = (i0-1+a, j0-1+b), a in [0, CY), b in [0, CX)
-  for (int k = tid; k < CY * CX; k += NT) {
-    int a = k / CX, b = k % CX;
-    int ci = i0 - 1 + a, cj = j0 - 1 + b;
-    double e0 = 0, e1 = 0;
+  // triangles of cells (ci, cj) = (i0-1+a, j0-1+b), a in [0, CY), b in [0, CX);
+  // one triangle per thread and round (2 * 561 triangles over 256 threads)
+  for (int k = tid; k < 2 * CY * CX; k += NT) {
+    const int kind = k >= CY * CX;
+    const int c = k - kind * CY * CX;
+    const int a = c / CX, b = c % CX;
+    const int ci = i0 - 1 + a, cj = j0 - 1 + b;
+    double e = 0;
     if (ci >= 0 && ci < r1 - 1 && cj >= 0 && cj < r2 - 1) {
-      // upper: offsets {0, r2, r2+1} -> (a,b), (a+1,b), (a+1,b+1)
-      e0 = dev::tri_eb(su[a][b], su[a + 1][b], su[a + 1][b + 1], sv[a][b], sv[a + 1][b], sv[a + 1][b + 1], 0);
-      // lower: offsets {0, 1, r2+1} -> (a,b), (a,b+1), (a+1,b+1)
-      e1 = dev::tri_eb(su[a][b], su[a][b + 1], su[a + 1][b + 1], sv[a][b], sv[a][b + 1], sv[a + 1][b + 1], 1);
+      // upper: offsets {0, r2, r2+1} -> (a,b), (a+1,b), (a+1,b+1);
+      // lower: offsets {0, 1, r2+1} -> (a,b), (a,b+1), (a+1,b+1).
+      // One call site keeps a single copy of the bound code in the
+      // instruction cache.
+      const int a1 = a + (kind == 0), b1 = b + (kind == 1);
+      e = dev::tri_eb(su[a][b], su[a1][b1], su[a + 1][b + 1], sv[a][b], sv[a1][b1], sv[a + 1][b + 1], kind);
     }
-    tri[0][a][b] = e0;
-    tri[1][a][b] = e1;
+    tri[kind][a][b] = e;
   }
   __syncthreads();
   const double thr = tab[0];

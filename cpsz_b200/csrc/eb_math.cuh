@@ -118,6 +118,20 @@ __device__ __forceinline__ void adjugate(float x0, float x1, float x2, float y0,
   c[3] = (x0 - x2) / det;
 }
 
+// (det / x >= 1) of the reference for det != 0, decided exactly without a
+// division: the rounded quotient is >= 1 iff the exact one is >= 1 - 2^-54
+// (the midpoint below 1, which rounds to the even neighbour 1).
+__device__ __forceinline__ bool quotient_at_least_one(double det, double x) {
+  if (!isfinite(det) || !isfinite(x)) return det / x >= 1;
+  if (x == 0) return signbit(x) ? det < 0 : det > 0;  // det / (+-0) = +-inf
+  if ((det < 0) != (x < 0)) return false;
+  const double a = fabs(det), b = fabs(x);
+  if (a >= b) return true;
+  if (a < 0.5 * b) return false;
+  // b/2 <= a < b: b - a is exact (Sterbenz), and so is the scaling by 2^54
+  return (b - a) * 18014398509481984.0 <= b;
+}
+
 // max_eb_to_keep_position_and_type<float>: src/sz_compress_cp_preserve_2d.cpp:125-172.
 // kind 0 = "upper" triangle X = {{0,0},{1,0},{1,1}}, kind 1 = "lower"
 // X = {{0,0},{0,1},{1,1}}, passed as x = X[.][1], y = X[.][0].
@@ -131,9 +145,9 @@ __device__ __forceinline__ double tri_eb(float u0, float u1, float u2, float v0,
   double det = u0v1 - u1v0 + u1v2 - u2v1 + u2v0 - u0v2;
   double eb = 0;
   if (det != 0) {
-    bool f1 = (det / (u2v0 - u0v2) >= 1);
-    bool f2 = (det / (u1v2 - u2v1) >= 1);
-    bool f3 = (det / (u0v1 - u1v0) >= 1);
+    bool f1 = quotient_at_least_one(det, u2v0 - u0v2);
+    bool f2 = quotient_at_least_one(det, u1v2 - u2v1);
+    bool f3 = quotient_at_least_one(det, u0v1 - u1v0);
     if (f1 && f2 && f3) {
       double eb1 = minf_d(off2(u2v0, -u0v2), off4(u0v1, -u1v0, u1v2, -u2v1));
       double eb2 = minf_d(off2(u1v2, -u2v1), off4(u0v1, -u1v0, u2v0, -u0v2));
@@ -144,6 +158,24 @@ __device__ __forceinline__ double tri_eb(float u0, float u1, float u2, float v0,
       double eb4 = minf_d(eb3, keep_sign_eigen(u0, u1, u2, v0, v1, v2, c[0], c[1], c[2], c[3]));
       eb = minf_d(eb1, eb2);
       eb = minf_d(eb, eb4);
+    } else if (isfinite(u0v1) && isfinite(u1v0) && isfinite(u0v2) && isfinite(u2v0) && isfinite(u1v2) &&
+               isfinite(u2v1)) {
+      // All products finite: every keep-sign bound is a finite non-negative
+      // double, MAX / MINF are plain max / min, and a flag whose first bound
+      // cannot raise eb leaves it unchanged without its second bound.
+      eb = 0;
+      if (!f1) {
+        const double e1 = off2(u2v0, -u0v2);
+        if (e1 > eb) eb = max_d(eb, minf_d(e1, off4(u0v1, -u1v0, u1v2, -u2v1)));
+      }
+      if (!f2) {
+        const double e1 = off2(u1v2, -u2v1);
+        if (e1 > eb) eb = max_d(eb, minf_d(e1, off4(u0v1, -u1v0, u2v0, -u0v2)));
+      }
+      if (!f3) {
+        const double e1 = off2(u0v1, -u1v0);
+        if (e1 > eb) eb = max_d(eb, minf_d(e1, off4(u1v2, -u2v1, u2v0, -u0v2)));
+      }
     } else {
       eb = 0;
       if (!f1) eb = max_d(eb, minf_d(off2(u2v0, -u0v2), off4(u0v1, -u1v0, u1v2, -u2v1)));

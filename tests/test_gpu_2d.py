@@ -100,3 +100,35 @@ def test_gpu_rejects_corrupt_blobs(ctx):
     # the context is still usable afterwards
     du, dv = cpsz_b200.sz_decompress_cp_preserve_2d_offline(bytes(blob), 64, 64, ctx=ctx)
     assert np.isfinite(du).all()
+
+
+def test_gpu_eb2d_nonfinite_signed_zero_and_overflow(ctx, oracle):
+    """Products beyond FLT_MAX, NaN / inf inputs, signed zeros and exact ties:
+    the bound kernel's division-free flags and pruned sign bounds fall back to
+    the literal arithmetic exactly."""
+    rng = np.random.default_rng(12)
+    shape = (40, 45)
+    U = rng.normal(size=shape).astype(np.float32)
+    V = rng.normal(size=shape).astype(np.float32)
+    U[5:8] *= 3e30
+    V[:, 7] *= 2e25
+    U[10, 10] = np.nan
+    V[20, 3] = np.inf
+    U[25:30, 25:30] = -0.0
+    V[25:30, 27] = 0.0
+    U[33:, :] = np.round(U[33:, :] * 2) / 2  # repeated values -> exact ties
+    V[33:, :] = np.round(V[33:, :] * 2) / 2
+    for eb in (0.1, 0.01):
+        e, ids = cpsz_b200.debug_eb2d(U, V, eb, ctx=ctx)
+        assert_bits_equal(e.ravel(), oracle.eb_2d(U, V, eb).ravel(), nan_equal=True)
+    # A NaN bound (NaN / inf input, or products beyond FLT_MAX) has no
+    # quantization id: the reference indexes out of range, the GPU path reports
+    # unsupported input.  Whole blobs are compared for large but finite products.
+    with pytest.raises(cpsz_b200.CpszError):
+        cpsz_b200.sz_compress_cp_preserve_2d_offline(U, V, max_pwr_eb=0.1, ctx=ctx)
+    U[10, 10] = 1.5
+    V[20, 3] = -2.5
+    U[5:8] /= 1e12
+    V[:, 7] /= 1e7
+    blob = cpsz_b200.sz_compress_cp_preserve_2d_offline(U, V, max_pwr_eb=0.1, ctx=ctx)
+    assert_blob_equal_2d(blob, oracle.compress_2d(U, V, 0.1))
