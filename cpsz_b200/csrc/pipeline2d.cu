@@ -414,7 +414,8 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   mark(ctx, "blocks+hist+unpred");
 
   // ---- stage 3: block order, histograms, unpredictables ----
-  for (Job2D& j : jobs)
+  for (int k = 0; k < nj; k++) {
+    Job2D& j = jobs[k];
     for (int f = 0; f < 2; f++) {
       CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.hist_codes[f], 0, 65536 * 8, st));
       CPSZ_TRY(launch_raster_to_blocks_u16(ctx, j.d.craster[f], j.r2, j.r1, j.r2, j.d.cblocks[f], j.d.hist_codes[f]));
@@ -425,51 +426,64 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_hist_codes + (size_t)f * 65536, j.d.hist_codes[f], 65536 * 8,
                                     cudaMemcpyDeviceToHost, st));
       CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_nunpred + f, j.d.seg_off[f] + j.nseg, 4, cudaMemcpyDeviceToHost, st));
+      CPSZ_CUDA_TRY(cudaEventRecord(ctx->job_ev[2 * k + f], st));
     }
+  }
   mark(ctx, "host_trees");
-  CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[1], st));
 
-  // host: id trees while the GPU runs the wavefront, then the code trees
+  // host: the id trees (their histograms arrived while the wavefront ran) and
+  // their bit packing, which the GPU runs right after stage 3 while the host
+  // builds the code trees
+  auto tree_failure = [&]() {
+    int fl = 0;
+    CPSZ_TRY(read_flag(ctx, &fl));
+    if (fl) return flag_error(fl);
+    return set_error(CPSZ_ERR_UNSUPPORTED, "Huffman tree construction failed (code longer than 64 bits)");
+  };
   CPSZ_CUDA_TRY(cudaEventSynchronize(ctx->ev[0]));
   parallel_for(nj, [&](int k) { jobs[k].tree_ok[0] = huff_build(jobs[k].h_hist_ids, 256, 2048, &jobs[k].cb[0]); });
-  CPSZ_CUDA_TRY(cudaEventSynchronize(ctx->ev[1]));
-  int flag = 0;
-  CPSZ_TRY(read_flag(ctx, &flag));
-  if (flag) return flag_error(flag);
+  for (Job2D& j : jobs) {
+    if (!j.tree_ok[0]) return tree_failure();
+    j.sec_bytes[0] = huff_section_bytes(j.cb[0]);
+    j.bits_bytes[0] = (j.cb[0].total_bits + 7) / 8;
+    if (j.bits_bytes[0] + 8 > j.ids_bits_cap) return set_error(CPSZ_ERR_UNSUPPORTED, "Huffman stream larger than its bound");
+    CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.enc_code[0], j.cb[0].code.data(), 256 * 8, cudaMemcpyHostToDevice, st));
+    CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.enc_len[0], j.cb[0].len.data(), 256, cudaMemcpyHostToDevice, st));
+    CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.bits[0], 0, align_up(j.bits_bytes[0], 4) + 8, st));
+    CPSZ_TRY(launch_huff_encode_u8(ctx, j.d.ids, 2 * j.N, true, HuffEncTable{j.d.enc_code[0], j.d.enc_len[0], 256},
+                                   j.d.bits[0], j.ids_bits_cap, nullptr, j.d.enc_tmp[0]));
+  }
+  // code trees, each as soon as its histogram is on the host
   parallel_for(2 * nj, [&](int q) {
     Job2D& j = jobs[q / 2];
     const int f = q % 2;
-    j.tree_ok[1 + f] = huff_build(j.h_hist_codes + (size_t)f * 65536, 65536, 131072, &j.cb[1 + f]);
+    j.tree_ok[1 + f] = cudaEventSynchronize(ctx->job_ev[q]) == cudaSuccess &&
+                       huff_build(j.h_hist_codes + (size_t)f * 65536, 65536, 131072, &j.cb[1 + f]);
   });
-  for (Job2D& j : jobs) {
-    for (int k = 0; k < 3; k++)
-      if (!j.tree_ok[k]) return set_error(CPSZ_ERR_UNSUPPORTED, "Huffman tree construction failed (code longer than 64 bits)");
-    j.n_unpred[0] = j.h_nunpred[0];
-    j.n_unpred[1] = j.h_nunpred[1];
-  }
 
-  // ---- stage 4: bit packing ----
+  // ---- stage 4: bit packing of the codes ----
   mark(ctx, "huffman_encode");
   for (Job2D& j : jobs) {
-    for (int k = 0; k < 3; k++) {
+    if (!j.tree_ok[1] || !j.tree_ok[2]) return tree_failure();
+    j.n_unpred[0] = j.h_nunpred[0];
+    j.n_unpred[1] = j.h_nunpred[1];
+    for (int k = 1; k < 3; k++) {
       j.sec_bytes[k] = huff_section_bytes(j.cb[k]);
       j.bits_bytes[k] = (j.cb[k].total_bits + 7) / 8;
-    }
-    if (j.bits_bytes[0] + 8 > j.ids_bits_cap || j.bits_bytes[1] + 8 > j.codes_bits_cap ||
-        j.bits_bytes[2] + 8 > j.codes_bits_cap)
-      return set_error(CPSZ_ERR_UNSUPPORTED, "Huffman stream larger than its bound");
-    for (int k = 0; k < 3; k++) {
-      const size_t bins = k ? 65536 : 256;
-      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.enc_code[k], j.cb[k].code.data(), bins * 8, cudaMemcpyHostToDevice, st));
-      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.enc_len[k], j.cb[k].len.data(), bins, cudaMemcpyHostToDevice, st));
+      if (j.bits_bytes[k] + 8 > j.codes_bits_cap)
+        return set_error(CPSZ_ERR_UNSUPPORTED, "Huffman stream larger than its bound");
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.enc_code[k], j.cb[k].code.data(), 65536 * 8, cudaMemcpyHostToDevice, st));
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.enc_len[k], j.cb[k].len.data(), 65536, cudaMemcpyHostToDevice, st));
       CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.bits[k], 0, align_up(j.bits_bytes[k], 4) + 8, st));
+      CPSZ_TRY(launch_huff_encode_u16(ctx, j.d.cblocks[k - 1], j.N,
+                                      HuffEncTable{j.d.enc_code[k], j.d.enc_len[k], 65536}, j.d.bits[k],
+                                      j.codes_bits_cap, nullptr, j.d.enc_tmp[k]));
     }
-    CPSZ_TRY(launch_huff_encode_u8(ctx, j.d.ids, 2 * j.N, true, HuffEncTable{j.d.enc_code[0], j.d.enc_len[0], 256},
-                                   j.d.bits[0], j.ids_bits_cap, nullptr, j.d.enc_tmp[0]));
-    for (int f = 0; f < 2; f++)
-      CPSZ_TRY(launch_huff_encode_u16(ctx, j.d.cblocks[f], j.N,
-                                      HuffEncTable{j.d.enc_code[1 + f], j.d.enc_len[1 + f], 65536}, j.d.bits[1 + f],
-                                      j.codes_bits_cap, nullptr, j.d.enc_tmp[1 + f]));
+  }
+  {
+    int flag = 0;
+    CPSZ_TRY(read_flag(ctx, &flag));
+    if (flag) return flag_error(flag);
   }
 
   // ---- stage 5: blob assembly in device memory ----

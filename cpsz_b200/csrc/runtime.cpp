@@ -250,6 +250,7 @@ int cpsz_b200_ctx_create(int device, cpsz_b200_ctx** out) {
   CPSZ_CUDA_TRY(cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking));
   for (auto& ev : c->ev) CPSZ_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   for (auto& ev : c->up_ev) CPSZ_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  for (auto& ev : c->job_ev) CPSZ_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   CPSZ_CUDA_TRY(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
   CPSZ_CUDA_TRY(cudaMalloc((void**)&c->d_flag, 64));
   CPSZ_CUDA_TRY(cudaMemset(c->d_flag, 0, 64));
@@ -273,6 +274,8 @@ int cpsz_b200_ctx_destroy(cpsz_b200_ctx* c) {
   for (auto& ev : c->ev)
     if (ev) cudaEventDestroy(ev);
   for (auto& ev : c->up_ev)
+    if (ev) cudaEventDestroy(ev);
+  for (auto& ev : c->job_ev)
     if (ev) cudaEventDestroy(ev);
   for (auto& ev : c->tev)
     if (ev) cudaEventDestroy(ev);

@@ -75,6 +75,9 @@ struct cpsz_b200_ctx {
   // chunked host-to-device uploads (one event per chunk, recorded on `aux`)
   static constexpr int kUploadChunks = 8;
   cudaEvent_t up_ev[kUploadChunks] = {};
+  // per (field, component) "histogram on the host" events of a compression pass
+  static constexpr int kJobEvents = 64;
+  cudaEvent_t job_ev[kJobEvents] = {};
   cpsz::Arena arena;
   void* pinned = nullptr;
   size_t pinned_cap = 0;
