@@ -43,7 +43,7 @@ struct WaveField {
   const float2* pair;
   uint16_t* codes;     // compress: quantization codes out (raster)
   float* out;          // compress: reconstruction (optional tap); decompress: decoded field
-  // last row of every 256-row group, ngroups * r2 tagged words
+  // last row of every WAVE_GROUP_ROWS-row group, ngroups * r2 tagged words
   // ((column + 1) << 32 | float bits); zeroed before every launch
   unsigned long long* gbnd;
   long long pair_pitch, code_pitch, out_pitch;
@@ -56,7 +56,7 @@ struct WaveItem {
   int field;
   int group;
 };
-constexpr int WAVE_WARPS = 8;
+constexpr int WAVE_WARPS = 4;
 constexpr int WAVE_GROUP_ROWS = WAVE_WARPS * 32;
 // Items must be ordered so that (field, g-1) precedes (field, g).
 int launch_wave2d(cpsz_b200_ctx* ctx, bool decompress, const WaveField* d_fields, const WaveItem* d_items,

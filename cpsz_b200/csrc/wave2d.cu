@@ -25,7 +25,8 @@
 //    row pitch makes the per-step accesses tile[l][t] bank-conflict free.
 //    Points outside the field are staged as pairs that reconstruct to 0, so a
 //    step has no bounds branches;
-//  * a CTA owns a 256-row group (8 warps).  Warp w takes the row above from
+//  * a CTA owns a WAVE_GROUP_ROWS-row group (WAVE_WARPS warps; 128 rows, 4
+//    warps: one warp per scheduler).  Warp w takes the row above from
 //    warp w-1 through a shared-memory ring of tagged words, 8 columns at a
 //    time (one warp-uniform tag test per 8 steps); lane 31 stores one tagged
 //    word per step.  The CTA's first warp takes the previous group's last row
