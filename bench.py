@@ -185,10 +185,9 @@ def run_reference(args, rank, world):
     use_ref = os.path.exists(oracle.REF_SO)
     if kind == "batch":
         # whole fields of the batch (the smaller ones), each with its own bound
-        bf, bebs = make_batch()
-        order = sorted(range(len(bf)), key=lambda k: bf[k][0].size)
-        tiles = [bf[k] for k in order if bf[k][0].size <= 1_500_000]
-        tile_ebs = [bebs[k] for k in order if bf[k][0].size <= 1_500_000]
+        lay = batch_layout()
+        order = sorted(range(len(lay)), key=lambda k: lay[k][0] * lay[k][1])
+        tiles, tile_ebs = make_batch([k for k in order if lay[k][0] * lay[k][1] <= 1_500_000])
         kind = "2d"
     else:
         fields, eb = make_fields(args.workload)
@@ -411,7 +410,7 @@ def run_learned(args, rank, world, device):
         "metric": "compress_GBps", "value": round(raw * world / (ms / 1e3) / 1e9, 3), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "bf16+f64+f32", "data": "synthetic",
-        "config": {"workload": args.workload, "eb": eb, "points": int(raw // 8), "inputs_exceed_l2": True,
+        "config": {"workload": args.workload, "tuning": _tuning_tag(), "eb": eb, "points": int(raw // 8), "inputs_exceed_l2": True,
                    "parallelism": f"replicas{world}", "value_io": "fields resident in HBM, blob written to HBM"},
         "ratio": round(raw / z_learned, 4), "ratio_pre_zstd": round(raw / size, 4),
         "plain_ratio": round(raw / z_plain, 4), "plain_ratio_pre_zstd": round(raw / len(plain), 4),
@@ -419,36 +418,64 @@ def run_learned(args, rank, world, device):
     }
 
 
-def make_batch(seed_offset: int = 0):
+def batch_layout():
+    """(r1, r2, seed, eb) of the 256 fields of the batched workload."""
     from cpsz_b200 import workloads as W
 
-    lay = W.batch_layout(3 + 1000 * seed_offset, 256, 128, 4096)
-    fields = [W.cfg3_field(r1, r2, sd) for r1, r2, sd, _ in lay]
-    return fields, [eb for *_, eb in lay]
+    return W.batch_layout(3, 256, 128, 4096)
+
+
+def make_batch(idx=None):
+    """Host fields and bounds of the batch's fields `idx` (all when None)."""
+    from cpsz_b200 import workloads as W
+
+    lay = batch_layout()
+    idx = range(len(lay)) if idx is None else idx
+    return [W.cfg3_field(*lay[k][:3]) for k in idx], [lay[k][3] for k in idx]
 
 
 def run_batch(args, rank, world, device):
-    """The batched workload: every step compresses all 256 fields with one
-    batched call (fields resident in HBM, blobs written to HBM); the same
-    fields through one single-field call each, and end to end from host
-    memory, are reported beside it."""
+    """The batched workload, sharded by field across the ranks (greedy size
+    balance, cpsz_b200/shard.py): each step every rank compresses the fields it
+    owns with one batched call (fields resident in HBM, blobs written to HBM)
+    and the ranks sum-all-reduce the per-field blob sizes, which places every
+    blob in the batch's concatenation.  The same fields through one
+    single-field call each, and the sharded call end to end from host memory,
+    are reported beside it."""
     import torch
 
     import cpsz_b200
+    from cpsz_b200 import shard
 
-    fields, ebs = make_batch(rank)
+    lay = batch_layout()
+    n_all = len(lay)
+    own = shard.partition([r1 * r2 for r1, r2, _, _ in lay], world)[rank]
+    fields, ebs = make_batch(own)
+    raw_all = sum(8 * r1 * r2 for r1, r2, _, _ in lay)
     raw = sum(U.nbytes + V.nbytes for U, V in fields)
     ctx = cpsz_b200.Context(device)
     stream = torch.cuda.ExternalStream(ctx.stream, device=device)
     dev = [(torch.from_numpy(U).to(f"cuda:{device}"), torch.from_numpy(V).to(f"cuda:{device}")) for U, V in fields]
     out = torch.empty(raw + (256 << 20), dtype=torch.uint8, device=f"cuda:{device}")
-    clk = Clocks(device).__enter__()
-    for _ in range(args.warmup):
-        offsets = cpsz_b200.compress_2d_batch(dev, ebs, out=out, ctx=ctx)
-    torch.cuda.synchronize(device)
+    sizes = torch.zeros(n_all, dtype=torch.int64, device=f"cuda:{device}")
+    own_t = torch.tensor(own, dtype=torch.int64, device=f"cuda:{device}")
     if world > 1:
         import torch.distributed as dist
 
+    def step():
+        offsets = cpsz_b200.compress_2d_batch(dev, ebs, out=out, ctx=ctx)
+        if world > 1:
+            with torch.cuda.stream(stream):
+                sizes.zero_()
+                sizes.index_copy_(0, own_t, torch.from_numpy(np.diff(offsets).astype(np.int64)).to(sizes.device))
+                dist.all_reduce(sizes)
+        return offsets
+
+    clk = Clocks(device).__enter__()
+    for _ in range(args.warmup):
+        offsets = step()
+    torch.cuda.synchronize(device)
+    if world > 1:
         dist.barrier()
     launches0 = ctx.kernel_launches
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -456,7 +483,7 @@ def run_batch(args, rank, world, device):
     try:
         ev0.record(stream)
         for _ in range(args.steps):
-            offsets = cpsz_b200.compress_2d_batch(dev, ebs, out=out, ctx=ctx)
+            offsets = step()
         ev1.record(stream)
         torch.cuda.synchronize(device)
     finally:
@@ -464,8 +491,6 @@ def run_batch(args, rank, world, device):
     launches = (ctx.kernel_launches - launches0) // max(args.steps, 1)
     ms = ev0.elapsed_time(ev1) / args.steps
     if world > 1:
-        import torch.distributed as dist
-
         t = torch.tensor([ms], device=f"cuda:{device}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
@@ -477,37 +502,47 @@ def run_batch(args, rank, world, device):
     ev1.record(stream)
     torch.cuda.synchronize(device)
     per_field_ms = ev0.elapsed_time(ev1)
-    # end to end: host fields in, blobs into pinned host memory
-    h_out = torch.empty(raw + (256 << 20), dtype=torch.uint8).pin_memory().numpy()
-    cpsz_b200.compress_2d_batch(fields, ebs, out=h_out, ctx=ctx)
+    # end to end through the sharded call: host fields in, blobs back in host memory
+    shapes = [(r1, r2) for r1, r2, _, _ in lay]
+    all_ebs = [e for *_, e in lay]
+    pos = {k: i for i, k in enumerate(own)}
+    res = shard.compress_2d_batch_sharded(shapes, all_ebs, lambda k: fields[pos[k]], ctx=ctx)
+    if world > 1:
+        dist.barrier()
     t0 = time.perf_counter()
-    cpsz_b200.compress_2d_batch(fields, ebs, out=h_out, ctx=ctx)
+    res = shard.compress_2d_batch_sharded(shapes, all_ebs, lambda k: fields[pos[k]], ctx=ctx)
     e2e_ms = (time.perf_counter() - t0) * 1e3
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    total_blob = int(res.offsets[-1])
     return {
-        "metric": "compress_GBps", "value": round(raw * world / (ms / 1e3) / 1e9, 3), "unit": "GB/s", "n_gpus": world,
+        "metric": "compress_GBps", "value": round(raw_all / (ms / 1e3) / 1e9, 3), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
-        "config": {"workload": args.workload, "fields": len(fields), "points": int(raw // 8),
-                   "inputs_exceed_l2": True, "parallelism": f"replicas{world}",
-                   "value_io": "fields resident in HBM, blobs written to HBM"},
-        "ratio_pre_zstd": round(raw / blob_bytes, 4),
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
+        "config": {"workload": args.workload, "tuning": _tuning_tag(), "fields": n_all, "points": int(raw_all // 8),
+                   "inputs_exceed_l2": True, "parallelism": f"field-sharded{world}",
+                   "value_io": "fields resident in HBM, blobs written to HBM; per-field sizes all-reduced"},
+        "ratio_pre_zstd": round(raw_all / total_blob, 4),
         "per_field_calls_GBps": round(raw / (per_field_ms / 1e3) / 1e9, 3),
-        "e2e": {"value": round(raw / (e2e_ms / 1e3) / 1e9, 3), "unit": "GB/s", "h2d_bytes_per_step": raw,
+        "e2e": {"value": round(raw_all / (e2e_ms / 1e3) / 1e9, 3), "unit": "GB/s", "h2d_bytes_per_step": raw,
                 "d2h_bytes_per_step": blob_bytes, "host_input": "pageable numpy arrays"},
         "cpu_baseline": None, "clocks": clk.summary(), "gpu_launches": launches,
     }
 
 
 def stage_times(ctx):
-    import ctypes as C
+    return ctx.stage_times()
+
+
+def _tuning_tag():
+    import os
 
     import cpsz_b200
 
-    names = (C.c_char_p * 24)()
-    ms = (C.c_float * 24)()
-    n = C.c_int()
-    cpsz_b200._check(cpsz_b200.lib().cpsz_b200_ctx_stage_times(ctx.handle, 24, names, ms, C.byref(n)))
-    return {names[i].decode(): ms[i] for i in range(n.value)}
+    src = cpsz_b200.tuning_source()
+    return os.path.basename(src) if src else "built-in defaults"
 
 
 def main():
@@ -567,7 +602,7 @@ def main():
         "metric": "compress_GBps", "value": round(r["value"], 3), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(r["ms"], 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32", "data": "synthetic",
-        "config": {"workload": args.workload, "eb": r["eb"], "points": int(raw // (4 * (2 if kind == "2d" else 3))),
+        "config": {"workload": args.workload, "tuning": _tuning_tag(), "eb": r["eb"], "points": int(raw // (4 * (2 if kind == "2d" else 3))),
                    "inputs_exceed_l2": True, "parallelism": f"replicas{world}",
                    "value_io": "fields resident in HBM, blob written to HBM"},
         "ratio": round(raw / r["lossless"], 4), "ratio_pre_zstd": round(raw / r["blob"], 4),

@@ -96,6 +96,15 @@ def _declare(L):
     L.cpsz_b200_learned_labels_2d.argtypes = [_vp, _vp, _vp, _sz, _sz, _vp, _vp, _sz, C.c_int, _vp]
     L.cpsz_b200_compress_2d_learned_f32.argtypes = [_vp, _vp, _vp, _vp, _sz, _sz, C.c_double, _vp, _vp, _sz,
                                                     C.POINTER(_sz), _vp]
+    L.cpsz_b200_ctx_set_timing.argtypes = [_vp, C.c_int]
+    L.cpsz_b200_ctx_stage_times.argtypes = [_vp, C.c_int, _vp, _vp, C.POINTER(C.c_int)]
+    L.cpsz_b200_tuning_param_count.restype = C.c_int
+    L.cpsz_b200_tuning_param_info.argtypes = [C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_int),
+                                              C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.cpsz_b200_tuning_set.argtypes = [C.c_char_p, _sz, C.c_int]
+    L.cpsz_b200_tuning_get.argtypes = [C.c_char_p, _sz, C.POINTER(C.c_int)]
+    L.cpsz_b200_tuning_load.argtypes = [C.c_char_p]
+    L.cpsz_b200_tuning_source.restype = C.c_char_p
     if hasattr(L, "cpsz_b200_cp_check_2d"):
         L.cpsz_b200_cp_check_2d.argtypes = [_vp, _vp, _vp, _vp, _vp, _sz, _sz, _vp, C.POINTER(C.c_uint64)]
         L.cpsz_b200_cp_check_3d.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _sz, _sz, _vp,
@@ -152,6 +161,57 @@ class Context:
         v = _vp()
         _check(lib().cpsz_b200_ctx_stream(self.handle, C.byref(v)))
         return v.value or 0
+
+    def set_timing(self, on: bool = True) -> None:
+        """Per-stage CUDA-event timing of the following calls (``cpsz_b200_ctx_set_timing``)."""
+        _check(lib().cpsz_b200_ctx_set_timing(self.handle, int(bool(on))))
+
+    def stage_times(self) -> dict:
+        """{stage name: ms} of the last call made with timing on; repeated names are summed."""
+        names = (C.c_char_p * 24)()
+        ms = (C.c_float * 24)()
+        n = C.c_int()
+        _check(lib().cpsz_b200_ctx_stage_times(self.handle, 24, names, ms, C.byref(n)))
+        out: dict = {}
+        for k in range(n.value):
+            nm = names[k].decode()
+            out[nm] = out.get(nm, 0.0) + float(ms[k])
+        return out
+
+
+# ---- launch-shape tuning table (output-invariant parameters) ----------------
+
+def tuning_params() -> dict:
+    """{name: (default, lo, hi)} of every launch-shape parameter."""
+    L = lib()
+    out = {}
+    for k in range(L.cpsz_b200_tuning_param_count()):
+        nm, d, lo, hi = C.c_char_p(), C.c_int(), C.c_int(), C.c_int()
+        _check(L.cpsz_b200_tuning_param_info(k, C.byref(nm), C.byref(d), C.byref(lo), C.byref(hi)))
+        out[nm.value.decode()] = (d.value, lo.value, hi.value)
+    return out
+
+
+def tuning_set(param: str, value: int, min_points: int = 0) -> None:
+    _check(lib().cpsz_b200_tuning_set(param.encode(), int(min_points), int(value)))
+
+
+def tuning_get(param: str, points: int) -> int:
+    v = C.c_int()
+    _check(lib().cpsz_b200_tuning_get(param.encode(), int(points), C.byref(v)))
+    return v.value
+
+
+def tuning_clear() -> None:
+    _check(lib().cpsz_b200_tuning_clear())
+
+
+def tuning_load(path: str | None = None) -> None:
+    _check(lib().cpsz_b200_tuning_load(path.encode() if path else None))
+
+
+def tuning_source() -> str:
+    return (lib().cpsz_b200_tuning_source() or b"").decode()
 
 
 def _h(ctx):

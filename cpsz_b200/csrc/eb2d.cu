@@ -13,25 +13,26 @@
 // component: the id, or 255 when the bound is <= thr (precision 0, Huffman
 // symbol 0).  A shared-memory histogram of the Huffman symbols is folded into
 // a global one.
+//
+// The tile shape and block size are template parameters; the launch-shape
+// table ("eb2d.tile", tuning.h) picks one of six instantiations per field
+// size.  Every shape computes the same bytes: each vertex's bound is the same
+// minimum over the same six triangles, whichever tile evaluates them.
 #include "eb_math.cuh"
 #include "kernels.h"
+#include "tuning.h"
 
 namespace cpsz {
 
-namespace {
-constexpr int TX = 32;
-constexpr int TY = 16;
-constexpr int NT = 256;
-constexpr int CX = TX + 1;  // cells per tile row
-constexpr int CY = TY + 1;
-}  // namespace
-
+template <int TX, int TY, int NT>
 __global__ void __launch_bounds__(NT) eb2d_kernel(const float* __restrict__ U, const float* __restrict__ V, int r1,
                                                   int r2, double max_pwr_eb, const double* __restrict__ thr_tab,
                                                   int thr_n, uint8_t* __restrict__ ids_u, uint8_t* __restrict__ ids_v,
                                                   unsigned long long* __restrict__ hist, int* __restrict__ flag,
                                                   float2* __restrict__ pair_u, float2* __restrict__ pair_v,
                                                   double* __restrict__ eb_out, int row_begin, int row_end) {
+  constexpr int CX = TX + 1;  // cells per tile row
+  constexpr int CY = TY + 1;
   __shared__ float su[TY + 2][TX + 3];
   __shared__ float sv[TY + 2][TX + 3];
   __shared__ double tri[2][CY][CX];
@@ -57,7 +58,7 @@ __global__ void __launch_bounds__(NT) eb2d_kernel(const float* __restrict__ U, c
   }
   __syncthreads();
   // triangles of cells (ci, cj) = (i0-1+a, j0-1+b), a in [0, CY), b in [0, CX);
-  // one triangle per thread and round (2 * 561 triangles over 256 threads)
+  // one triangle per thread and round (2 * 561 triangles over 256 threads at 32x16)
   for (int k = tid; k < 2 * CY * CX; k += NT) {
     const int kind = k >= CY * CX;
     const int c = k - kind * CY * CX;
@@ -138,9 +139,19 @@ int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int 
                 float2* pair_u, float2* pair_v, double* eb_out, int row_begin, int row_end) {
   if (row_end < 0) row_end = r1;
   if (row_end <= row_begin) return CPSZ_OK;
-  dim3 grid((r2 + TX - 1) / TX, (row_end - row_begin + TY - 1) / TY);
-  eb2d_kernel<<<grid, NT, 0, ctx->stream>>>(U, V, r1, r2, max_pwr_eb, d_thr_tab, thr_n, ids_u, ids_v, hist,
-                                            ctx->d_flag, pair_u, pair_v, eb_out, row_begin, row_end);
+  auto go = [&](auto kernel, int tx, int ty, int nt) {
+    dim3 grid((r2 + tx - 1) / tx, (row_end - row_begin + ty - 1) / ty);
+    kernel<<<grid, nt, 0, ctx->stream>>>(U, V, r1, r2, max_pwr_eb, d_thr_tab, thr_n, ids_u, ids_v, hist, ctx->d_flag,
+                                         pair_u, pair_v, eb_out, row_begin, row_end);
+  };
+  switch (tune_get(TUNE_EB2D_TILE, (size_t)r1 * r2)) {
+    case 1: go(eb2d_kernel<32, 8, 128>, 32, 8, 128); break;
+    case 2: go(eb2d_kernel<64, 8, 256>, 64, 8, 256); break;
+    case 3: go(eb2d_kernel<32, 32, 256>, 32, 32, 256); break;
+    case 4: go(eb2d_kernel<64, 16, 256>, 64, 16, 256); break;
+    case 5: go(eb2d_kernel<32, 16, 128>, 32, 16, 128); break;
+    default: go(eb2d_kernel<32, 16, 256>, 32, 16, 256); break;
+  }
   count_launch(ctx);
   return check_launch("eb2d_kernel");
 }

@@ -58,9 +58,10 @@ struct WaveItem {
 };
 constexpr int WAVE_WARPS = 4;
 constexpr int WAVE_GROUP_ROWS = WAVE_WARPS * 32;
-// Items must be ordered so that (field, g-1) precedes (field, g).
+// Items must be ordered so that (field, g-1) precedes (field, g).  `points`
+// (all fields of the launch together) keys the launch-shape table.
 int launch_wave2d(cpsz_b200_ctx* ctx, bool decompress, const WaveField* d_fields, const WaveItem* d_items,
-                  int n_items, int* d_queue, int max_ctas);
+                  int n_items, int* d_queue, size_t points);
 
 // ---- block-order plumbing (12 x 12 blocks) ---------------------------------------
 // Raster (pitched) -> 12x12-block order, and back.  Histogram of the block-order

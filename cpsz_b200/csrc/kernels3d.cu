@@ -10,6 +10,7 @@
 
 #include "eb_math.cuh"
 #include "kernels.h"
+#include "tuning.h"
 #include "libm_dev.cuh"
 
 namespace cpsz {
@@ -361,13 +362,15 @@ int launch_eb3d(cpsz_b200_ctx* ctx, const float* U, const float* V, const float*
   dim3 grid((r3 + EB_TK - 1) / EB_TK, (r2 + EB_TJ - 1) / EB_TJ, 1);
   if (grid.y > 65535)
     return set_error(CPSZ_ERR_UNSUPPORTED, "3D field with r2 = %d exceeds the bound kernel's grid", r2);
-  // split i so that the grid fills the GPU about four times over
+  // split i so that the grid covers the GPU `fill` times (two CTAs per SM each)
   const long long cols = (long long)grid.x * grid.y;
-  long long want = (4LL * ctx->num_sms * 2 + cols - 1) / cols;
+  const size_t points = (size_t)r1 * r2 * r3;
+  const int fill = tune_get(TUNE_EB3D_FILL, points), min_chunk = tune_get(TUNE_EB3D_MIN_CHUNK, points);
+  long long want = ((long long)fill * ctx->num_sms * 2 + cols - 1) / cols;
   if (want < 1) want = 1;
   if (want > r1) want = r1;
   int chunk = (int)((r1 + want - 1) / want);
-  if (chunk < 8) chunk = 8 < r1 ? 8 : r1;
+  if (chunk < min_chunk) chunk = min_chunk < r1 ? min_chunk : r1;
   grid.z = (r1 + chunk - 1) / chunk;
   eb3d_kernel<<<grid, EB_NT, 0, ctx->stream>>>(U, V, W, r1, r2, r3, chunk, max_pwr_eb, d_thr, thr_n, id_q, eb_out,
                                                 ctx->d_flag);

@@ -33,6 +33,7 @@
 
 #include "huffman_host.h"
 #include "kernels.h"
+#include "tuning.h"
 #include "pipeline.h"
 
 namespace cpsz {
@@ -345,7 +346,7 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       // Host input: row chunks go up on the second stream and the bound kernel
       // runs band by band as soon as a band's rows and the row below it are
       // on the device, so the transfer overlaps the bound derivation.
-      const int K = (j.N >= ((size_t)1 << 22) && !j.eb_ext) ? cpsz_b200_ctx::kUploadChunks : 1;
+      const int K = (j.N >= ((size_t)1 << 22) && !j.eb_ext) ? tune_get(TUNE_H2D_CHUNKS, j.N) : 1;
       const int R = (int)align_up((size_t)(j.r1 + K - 1) / K, 16);
       const int nch = (j.r1 + R - 1) / R;
       CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[2], st));
@@ -405,7 +406,9 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   CPSZ_CUDA_TRY(cudaMemcpyAsync(d_items, items.data(), n_items * sizeof(WaveItem), cudaMemcpyHostToDevice, st));
   CPSZ_CUDA_TRY(cudaMemsetAsync(queue, 0, 64, st));
   mark(ctx, "wave2d_compress");
-  CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, 0));
+  size_t pass_points = 0;
+  for (const Job2D& j : jobs) pass_points += j.N;
+  CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points));
   if (tap && tap->recon_only) {
     int flag = 0;
     CPSZ_TRY(read_flag(ctx, &flag));
@@ -769,7 +772,7 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
   CPSZ_CUDA_TRY(cudaMemsetAsync(gbnd, 0, 2 * (size_t)ngroups * r2 * 8, st));
   CPSZ_CUDA_TRY(cudaMemsetAsync(queue, 0, 64, st));
   mark(ctx, "wave2d_decompress");
-  CPSZ_TRY(launch_wave2d(ctx, true, dfields, ditems, n_items, queue, 0));
+  CPSZ_TRY(launch_wave2d(ctx, true, dfields, ditems, n_items, queue, (size_t)r1 * r2));
   mark(ctx, "d2h");
   if (!dev_out) {
     CPSZ_CUDA_TRY(cudaMemcpyAsync(U_out, dU, 4 * N, cudaMemcpyDeviceToHost, st));

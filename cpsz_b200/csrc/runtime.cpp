@@ -2,6 +2,7 @@
 #include "runtime.h"
 
 #include "libm.h"
+#include "tuning.h"
 
 #include <cfloat>
 #include <cmath>
@@ -236,6 +237,7 @@ int cpsz_b200_version(void) { return 10000; }
 
 int cpsz_b200_ctx_create(int device, cpsz_b200_ctx** out) {
   if (!out) return set_error(CPSZ_ERR_INVALID, "ctx_create: null output");
+  CPSZ_TRY(tune_autoload());
   int n = 0;
   cudaError_t e = cudaGetDeviceCount(&n);
   if (e != cudaSuccess || n == 0) {

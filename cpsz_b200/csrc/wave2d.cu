@@ -55,6 +55,7 @@
 // Decompression adds the precomputed 2(code - 32768) * p (0 when id = 0) or
 // takes the stored raw value.
 #include "kernels.h"
+#include "tuning.h"
 
 namespace cpsz {
 
@@ -329,7 +330,7 @@ __global__ void __launch_bounds__(WAVE_WARPS * 32, 1) wave2d_kernel(const WaveFi
 }  // namespace
 
 int launch_wave2d(cpsz_b200_ctx* ctx, bool decompress, const WaveField* d_fields, const WaveItem* d_items,
-                  int n_items, int* d_queue, int max_ctas) {
+                  int n_items, int* d_queue, size_t points) {
   static bool attr_set[2] = {false, false};
   if (!attr_set[decompress]) {
     cudaError_t e = decompress ? cudaFuncSetAttribute(wave2d_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -345,8 +346,9 @@ int launch_wave2d(cpsz_b200_ctx* ctx, bool decompress, const WaveField* d_fields
   else
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wave2d_kernel<false>, WAVE_WARPS * 32, kDynSmem);
   if (per_sm < 1) return set_error(CPSZ_ERR_CUDA, "wave2d kernel does not fit on an SM");
+  const int cap = tune_get(TUNE_WAVE2D_CTAS_PER_SM, points);
+  if (cap > 0 && per_sm > cap) per_sm = cap;
   int grid = ctx->num_sms * per_sm;
-  if (max_ctas > 0 && grid > max_ctas) grid = max_ctas;
   if (grid > n_items) grid = n_items;
   if (grid < 1) return CPSZ_OK;
   if (decompress)

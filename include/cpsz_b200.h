@@ -55,6 +55,26 @@ int cpsz_b200_ctx_stream(cpsz_b200_ctx* ctx, void** stream);
 int cpsz_b200_ctx_set_timing(cpsz_b200_ctx* ctx, int on);
 int cpsz_b200_ctx_stage_times(cpsz_b200_ctx* ctx, int max_stages, const char** names, float* ms, int* n_stages);
 
+/* ---- launch-shape tuning table (no reference counterpart) -----------------
+ * Parameters that change how kernels are launched and never what they compute
+ * (every blob is byte-identical for every value): "eb2d.tile" (0..5: 32x16/256
+ * threads, 32x8/128, 64x8/256, 32x32/256, 64x16/256, 32x16/128),
+ * "wave2d.ctas_per_sm" (0 = occupancy limit), "eb3d.fill", "eb3d.min_chunk",
+ * "h2d.chunks".  An entry applies to fields of >= min_points points; the
+ * largest such threshold wins.  The first cpsz_b200_ctx_create() loads
+ * $CPSZ_B200_TUNING (empty or "none": no table) or else tuning_b200.json of the
+ * package directory when present; a malformed table fails ctx creation.  Any
+ * explicit set / clear / load replaces that automatic load. */
+int cpsz_b200_tuning_param_count(void);
+int cpsz_b200_tuning_param_info(int index, const char** name, int* def, int* lo, int* hi);
+int cpsz_b200_tuning_set(const char* param, size_t min_points, int value);
+int cpsz_b200_tuning_get(const char* param, size_t points, int* value);
+int cpsz_b200_tuning_clear(void);
+/* path NULL: the package's tuning_b200.json. */
+int cpsz_b200_tuning_load(const char* path);
+/* Path of the table last loaded ("" if none). */
+const char* cpsz_b200_tuning_source(void);
+
 /* ---- 2D offline CP-preserving compression -------------------------------
  * Replaces sz_compress_cp_preserve_2d_offline<float>
  * (reference include/sz_compress_cp_preserve_2d.hpp:10,
