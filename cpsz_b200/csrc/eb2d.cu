@@ -30,9 +30,11 @@ __global__ void __launch_bounds__(NT) eb2d_kernel(const float* __restrict__ U, c
                                                   int thr_n, uint8_t* __restrict__ ids_u, uint8_t* __restrict__ ids_v,
                                                   unsigned long long* __restrict__ hist, int* __restrict__ flag,
                                                   float2* __restrict__ pair_u, float2* __restrict__ pair_v,
-                                                  double* __restrict__ eb_out, int row_begin, int row_end) {
+                                                  double* __restrict__ eb_out, int row_begin, int row_end,
+                                                  unsigned long long* __restrict__ band_done) {
   constexpr int CX = TX + 1;  // cells per tile row
   constexpr int CY = TY + 1;
+  static_assert(WAVE_GROUP_ROWS % TY == 0, "a tile's rows must lie in one wavefront group");
   __shared__ float su[TY + 2][TX + 3];
   __shared__ float sv[TY + 2][TX + 3];
   __shared__ double tri[2][CY][CX];
@@ -132,17 +134,29 @@ __global__ void __launch_bounds__(NT) eb2d_kernel(const float* __restrict__ U, c
   __syncthreads();
   for (int k = tid; k < 256; k += NT)
     if (shist[k]) atomicAdd(&hist[k], (unsigned long long)shist[k]);
+  if (band_done) {
+    // every thread's outputs are visible device-wide before the tile counts
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) {
+      const int rows = min(TY, row_end - i0), cols = min(TX, r2 - j0);
+      atomicAdd(&band_done[i0 / WAVE_GROUP_ROWS], (unsigned long long)rows * cols);
+    }
+  }
 }
 
 int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, double max_pwr_eb,
                 const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
-                float2* pair_u, float2* pair_v, double* eb_out, int row_begin, int row_end) {
+                float2* pair_u, float2* pair_v, double* eb_out, int row_begin, int row_end,
+                unsigned long long* band_done) {
   if (row_end < 0) row_end = r1;
   if (row_end <= row_begin) return CPSZ_OK;
+  if (band_done && row_begin % WAVE_GROUP_ROWS)
+    return set_error(CPSZ_ERR_INVALID, "eb2d band start %d is not a multiple of %d", row_begin, WAVE_GROUP_ROWS);
   auto go = [&](auto kernel, int tx, int ty, int nt) {
     dim3 grid((r2 + tx - 1) / tx, (row_end - row_begin + ty - 1) / ty);
     kernel<<<grid, nt, 0, ctx->stream>>>(U, V, r1, r2, max_pwr_eb, d_thr_tab, thr_n, ids_u, ids_v, hist, ctx->d_flag,
-                                         pair_u, pair_v, eb_out, row_begin, row_end);
+                                         pair_u, pair_v, eb_out, row_begin, row_end, band_done);
   };
   switch (tune_get(TUNE_EB2D_TILE, (size_t)r1 * r2)) {
     case 1: go(eb2d_kernel<32, 8, 128>, 32, 8, 128); break;

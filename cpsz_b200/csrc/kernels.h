@@ -25,10 +25,16 @@ constexpr int FLAG_OUT_CAPACITY = 16; // an output stream did not fit its buffer
 
 // ---- 2D error bounds ---------------------------------------------------------
 // Rows [row_begin, row_end) of the vertex outputs (row_end < 0: all rows); the
-// kernel reads rows row_begin - 1 .. row_end of U and V.
+// kernel reads rows row_begin - 1 .. row_end of U and V.  With `band_done`
+// (one counter per WAVE_GROUP_ROWS-row group, zeroed beforehand), every tile
+// adds the number of vertices it finished to its group's counter after its
+// outputs are visible device-wide (row_begin must then be a multiple of
+// WAVE_GROUP_ROWS), so a concurrently running wavefront can start on a group
+// as soon as its counter reaches rows x r2.
 int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, double max_pwr_eb,
                 const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
-                float2* pair_u, float2* pair_v, double* eb_out = nullptr, int row_begin = 0, int row_end = -1);
+                float2* pair_u, float2* pair_v, double* eb_out = nullptr, int row_begin = 0, int row_end = -1,
+                unsigned long long* band_done = nullptr);
 
 // The same quantization for given per-vertex bounds eb_in[n] (learned bounds).
 int launch_quant2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t n, const double* eb_in,
@@ -51,6 +57,10 @@ struct WaveField {
   // optional diagnostics: per (group, warp) 4 counters {start clock, end clock,
   // spins waiting for the row above, spins waiting for ring credit}
   long long* trace;
+  // optional: per-group counters of input points written by a concurrently
+  // running producer (launch_eb2d's band_done); an item starts once its
+  // group's counter reaches rows x r2 (bounded wait, then FLAG_TIMEOUT)
+  const unsigned long long* band_done;
 };
 struct WaveItem {
   int field;
@@ -59,9 +69,13 @@ struct WaveItem {
 constexpr int WAVE_WARPS = 4;
 constexpr int WAVE_GROUP_ROWS = WAVE_WARPS * 32;
 // Items must be ordered so that (field, g-1) precedes (field, g).  `points`
-// (all fields of the launch together) keys the launch-shape table.
+// (all fields of the launch together) keys the launch-shape table.  The launch
+// goes to `stream` (default: the context's stream); `concurrent` marks a
+// launch that runs beside its producer (fields with band_done): at most one
+// CTA per SM then, which leaves every SM room for the producer's CTAs, so the
+// producer always progresses while wavefront CTAs wait on it.
 int launch_wave2d(cpsz_b200_ctx* ctx, bool decompress, const WaveField* d_fields, const WaveItem* d_items,
-                  int n_items, int* d_queue, size_t points);
+                  int n_items, int* d_queue, size_t points, cudaStream_t stream = nullptr, bool concurrent = false);
 
 // ---- block-order plumbing (12 x 12 blocks) ---------------------------------------
 // Raster (pitched) -> 12x12-block order, and back.  Histogram of the block-order

@@ -61,6 +61,7 @@ struct DevBuf {
   uint16_t* cblocks[2];
   unsigned long long* hist_codes[2];
   unsigned long long* gbnd;
+  unsigned long long* band;  // per-group counters of finished eb2d vertices
   unsigned int* seg_cnt[2];
   unsigned int* seg_off[2];
   void* scan_tmp[2];
@@ -167,6 +168,7 @@ size_t job_bytes(const Job2D& j) {
   add(4 * N);                           // codes blocks
   add(2 * 65536 * 8);                   // hist codes
   add(2 * (size_t)j.ngroups * j.r2 * 8);  // boundary rows (tagged words)
+  add((size_t)j.ngroups * 8);             // eb2d group counters
   add(2 * 2 * (j.nseg + 1) * 4);
   add(2 * segment_scan_tmp_bytes(j.r1, j.r2));
   add(2 * 4 * N);  // unpred
@@ -200,6 +202,7 @@ int job_alloc(cpsz_b200_ctx* ctx, Job2D& j) {
     d.hist_codes[f] = (unsigned long long*)A(65536 * 8);
   }
   d.gbnd = (unsigned long long*)A(2 * (size_t)j.ngroups * j.r2 * 8);
+  d.band = (unsigned long long*)A((size_t)j.ngroups * 8);
   for (int f = 0; f < 2; f++) {
     d.seg_cnt[f] = (unsigned int*)A((j.nseg + 1) * 4);
     d.seg_off[f] = (unsigned int*)A((j.nseg + 1) * 4);
@@ -327,27 +330,84 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     jobs[k].h_nunpred = (unsigned int*)(jobs[k].h_hist_codes + 2 * 65536);
   }
 
-  // ---- stage 1: inputs and error bounds ----
+  // Derived bounds (eb2d) signal per 128-row group, so the wavefront runs
+  // beside them on the high-priority stream and starts on a group as soon as
+  // its pairs are written.  Given bounds (quant2d) are not row-ordered: the
+  // wavefront then follows them on the main stream.
+  bool overlap = true;
+  for (const Job2D& j : jobs) overlap &= j.eb_ext == nullptr;
+
+  // ---- setup: flags, tables, wavefront descriptors ----
   reset_marks(ctx);
   mark(ctx, "h2d+setup");
   CPSZ_CUDA_TRY(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), st));
   CPSZ_CUDA_TRY(cudaMemcpyAsync(thr_tab, qt.t, QUANT_TAB_MAX * 8, cudaMemcpyHostToDevice, st));
   for (Job2D& j : jobs) CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.hist_ids, 0, 256 * 8, st));
+  std::vector<WaveField> hf(2 * nj);
+  std::vector<int> r1v(2 * nj);
+  for (int k = 0; k < nj; k++) {
+    Job2D& j = jobs[k];
+    CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.gbnd, 0, 2 * (size_t)j.ngroups * j.r2 * 8, st));
+    if (overlap) CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.band, 0, (size_t)j.ngroups * 8, st));
+    for (int f = 0; f < 2; f++) {
+      WaveField& F = hf[2 * k + f];
+      F.pair = j.d.pairs[f];
+      F.codes = j.d.craster[f];
+      F.trace = (nj == 1 && ctx->d_wave_trace && ctx->wave_trace_len >= 2 * (size_t)j.ngroups * WAVE_WARPS * 4)
+                    ? ctx->d_wave_trace + (size_t)f * j.ngroups * WAVE_WARPS * 4
+                    : nullptr;
+      F.out = tap ? tap->recon[f] : nullptr;
+      F.gbnd = j.d.gbnd + (size_t)f * j.ngroups * j.r2;
+      F.pair_pitch = j.r2;
+      F.code_pitch = j.r2;
+      F.out_pitch = j.r2;
+      F.r1 = j.r1;
+      F.r2 = j.r2;
+      F.band_done = overlap ? j.d.band : nullptr;
+      r1v[2 * k + f] = j.r1;
+    }
+  }
+  std::vector<WaveItem> items;
+  const int n_items = build_wave_items(2 * nj, r1v.data(), items);
+  CPSZ_CUDA_TRY(cudaMemcpyAsync(d_fields, hf.data(), hf.size() * sizeof(WaveField), cudaMemcpyHostToDevice, st));
+  CPSZ_CUDA_TRY(cudaMemcpyAsync(d_items, items.data(), n_items * sizeof(WaveItem), cudaMemcpyHostToDevice, st));
+  CPSZ_CUDA_TRY(cudaMemsetAsync(queue, 0, 64, st));
+  size_t pass_points = 0;
+  for (const Job2D& j : jobs) pass_points += j.N;
+  // a wavefront launched beside its producer must be finished before this
+  // call returns on any path (its workspace is reused by the next call)
+  struct HiDrain {
+    cudaStream_t s = nullptr;
+    ~HiDrain() {
+      if (s) cudaStreamSynchronize(s);
+    }
+  } hi_drain;
+  if (overlap) {
+    hi_drain.s = ctx->hi;
+    CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[3], st));
+    CPSZ_CUDA_TRY(cudaStreamWaitEvent(ctx->hi, ctx->ev[3], 0));
+    CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points, ctx->hi, true));
+    CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[4], ctx->hi));
+  }
+
+  // ---- stage 1: inputs and error bounds ----
   mark(ctx, "eb2d");
   for (Job2D& j : jobs) {
+    unsigned long long* band = overlap ? j.d.band : nullptr;
     if (j.dev_in) {
       if (j.eb_ext)
         CPSZ_TRY(launch_quant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
                                 j.d.hist_ids, j.d.pairs[0], j.d.pairs[1]));
       else
         CPSZ_TRY(launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
-                             j.d.hist_ids, j.d.pairs[0], j.d.pairs[1]));
+                             j.d.hist_ids, j.d.pairs[0], j.d.pairs[1], nullptr, 0, -1, band));
     } else {
       // Host input: row chunks go up on the second stream and the bound kernel
       // runs band by band as soon as a band's rows and the row below it are
-      // on the device, so the transfer overlaps the bound derivation.
+      // on the device, so the transfer overlaps the bound derivation.  Bands
+      // start on wavefront group boundaries.
       const int K = (j.N >= ((size_t)1 << 22) && !j.eb_ext) ? tune_get(TUNE_H2D_CHUNKS, j.N) : 1;
-      const int R = (int)align_up((size_t)(j.r1 + K - 1) / K, 16);
+      const int R = (int)align_up((size_t)(j.r1 + K - 1) / K, WAVE_GROUP_ROWS);
       const int nch = (j.r1 + R - 1) / R;
       CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[2], st));
       CPSZ_CUDA_TRY(cudaStreamWaitEvent(ctx->aux, ctx->ev[2], 0));
@@ -367,48 +427,19 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
         else
           CPSZ_TRY(launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
                                j.d.hist_ids, j.d.pairs[0], j.d.pairs[1], nullptr, c * R,
-                               std::min(j.r1, (c + 1) * R)));
+                               std::min(j.r1, (c + 1) * R), band));
       }
     }
     CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_hist_ids, j.d.hist_ids, 256 * 8, cudaMemcpyDeviceToHost, st));
   }
-  mark(ctx, "eb2d_end");
   CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[0], st));
   if (tap && tap->ids)
     CPSZ_CUDA_TRY(cudaMemcpyAsync(tap->ids, jobs[0].d.ids, 2 * jobs[0].N, cudaMemcpyDeviceToDevice, st));
 
   // ---- stage 2: one persistent wavefront over every field of the pass ----
-  std::vector<WaveField> hf(2 * nj);
-  std::vector<int> r1v(2 * nj);
-  for (int k = 0; k < nj; k++) {
-    Job2D& j = jobs[k];
-    CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.gbnd, 0, 2 * (size_t)j.ngroups * j.r2 * 8, st));
-    for (int f = 0; f < 2; f++) {
-      WaveField& F = hf[2 * k + f];
-      F.pair = j.d.pairs[f];
-      F.codes = j.d.craster[f];
-      F.trace = (nj == 1 && ctx->d_wave_trace && ctx->wave_trace_len >= 2 * (size_t)j.ngroups * WAVE_WARPS * 4)
-                    ? ctx->d_wave_trace + (size_t)f * j.ngroups * WAVE_WARPS * 4
-                    : nullptr;
-      F.out = tap ? tap->recon[f] : nullptr;
-      F.gbnd = j.d.gbnd + (size_t)f * j.ngroups * j.r2;
-      F.pair_pitch = j.r2;
-      F.code_pitch = j.r2;
-      F.out_pitch = j.r2;
-      F.r1 = j.r1;
-      F.r2 = j.r2;
-      r1v[2 * k + f] = j.r1;
-    }
-  }
-  std::vector<WaveItem> items;
-  const int n_items = build_wave_items(2 * nj, r1v.data(), items);
-  CPSZ_CUDA_TRY(cudaMemcpyAsync(d_fields, hf.data(), hf.size() * sizeof(WaveField), cudaMemcpyHostToDevice, st));
-  CPSZ_CUDA_TRY(cudaMemcpyAsync(d_items, items.data(), n_items * sizeof(WaveItem), cudaMemcpyHostToDevice, st));
-  CPSZ_CUDA_TRY(cudaMemsetAsync(queue, 0, 64, st));
   mark(ctx, "wave2d_compress");
-  size_t pass_points = 0;
-  for (const Job2D& j : jobs) pass_points += j.N;
-  CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points));
+  if (overlap) CPSZ_CUDA_TRY(cudaStreamWaitEvent(st, ctx->ev[4], 0));
+  else CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points));
   if (tap && tap->recon_only) {
     int flag = 0;
     CPSZ_TRY(read_flag(ctx, &flag));
@@ -750,7 +781,7 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
     CPSZ_CUDA_TRY(cudaMemcpyAsync(h_cnt + f, seg_off[f] + nseg, 4, cudaMemcpyDeviceToHost, st));
   }
   // ---- wavefront ----
-  WaveField hf[2];
+  WaveField hf[2] = {};
   for (int f = 0; f < 2; f++) {
     WaveField& F = hf[f];
     F.pair = raw[f];

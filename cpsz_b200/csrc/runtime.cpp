@@ -250,6 +250,13 @@ int cpsz_b200_ctx_create(int device, cpsz_b200_ctx** out) {
   c->device = device;
   CPSZ_CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   CPSZ_CUDA_TRY(cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking));
+  {
+    // the block scheduler dispatches a higher-priority stream's CTAs first as
+    // SMs free up, so a consumer launched beside its producer starts early
+    int lo_pri = 0, hi_pri = 0;
+    CPSZ_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo_pri, &hi_pri));
+    CPSZ_CUDA_TRY(cudaStreamCreateWithPriority(&c->hi, cudaStreamNonBlocking, hi_pri));
+  }
   for (auto& ev : c->ev) CPSZ_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   for (auto& ev : c->up_ev) CPSZ_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   for (auto& ev : c->job_ev) CPSZ_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
@@ -268,6 +275,7 @@ int cpsz_b200_ctx_destroy(cpsz_b200_ctx* c) {
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
   cudaStreamSynchronize(c->aux);
+  if (c->hi) cudaStreamSynchronize(c->hi);
   if (c->arena.base) cudaFree(c->arena.base);
   if (c->pinned) cudaFreeHost(c->pinned);
   if (c->d_flag) cudaFree(c->d_flag);
@@ -283,6 +291,7 @@ int cpsz_b200_ctx_destroy(cpsz_b200_ctx* c) {
     if (ev) cudaEventDestroy(ev);
   cudaStreamDestroy(c->stream);
   cudaStreamDestroy(c->aux);
+  if (c->hi) cudaStreamDestroy(c->hi);
   for (auto& d : g_default_ctx)
     if (d == c) d = nullptr;
   delete c;

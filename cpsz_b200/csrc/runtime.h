@@ -71,6 +71,7 @@ struct cpsz_b200_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t aux = nullptr;  // second stream for overlapping independent stages
+  cudaStream_t hi = nullptr;   // highest-priority stream: consumers that run beside their producer
   cudaEvent_t ev[8] = {};
   // chunked host-to-device uploads (one event per chunk, recorded on `aux`)
   static constexpr int kUploadChunks = 8;

@@ -34,7 +34,13 @@
 //    per window and loaded coalesced one window ahead;
 //  * CTAs are persistent and pull (field, group) items from a device work
 //    queue (atomic counter).  An item's predecessor (same field, previous
-//    group) was dequeued earlier by a running CTA, so every wait ends.
+//    group) was dequeued earlier by a running CTA, so every wait ends;
+//  * compression runs beside its producer: the bound kernel (eb2d) counts the
+//    points it has finished per group, and an item starts when its group's
+//    count is complete (one thread polls with ld.acquire.gpu, every thread
+//    then acquires before its first load).  Such a launch keeps to one CTA per
+//    SM, so each SM keeps room for the producer's CTAs and the producer
+//    cannot be starved by waiting consumers.
 //
 // Tagged words are 64-bit (column + 1) << 32 | float bits, written and read as
 // single aligned 64-bit accesses, so a reader that sees the expected tag holds
@@ -66,6 +72,7 @@ constexpr int RING = 128;
 constexpr int TP = 33;         // tile row pitch (elements)
 constexpr int TILE = 32 * TP;  // elements per tile
 constexpr long long SPIN_LIMIT = 1ll << 22;
+constexpr long long BAND_WAIT_NS = 4000000000ll;  // producer wait limit (4 s)
 
 // exact float of an integer |n| < 2^22 without the conversion unit
 __device__ __forceinline__ float small_int_to_float(int n) {
@@ -85,6 +92,11 @@ __device__ __forceinline__ long long globaltimer_ns() {
   long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
+}
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
@@ -321,6 +333,27 @@ __global__ void __launch_bounds__(WAVE_WARPS * 32, 1) wave2d_kernel(const WaveFi
     if (it >= n_items) break;
     const WaveItem item = items[it];
     const WaveField F = fields[item.field];
+    if (F.band_done) {
+      // the producer (eb2d) runs concurrently: wait until every input point of
+      // this group is written; one thread polls, then every thread acquires
+      const unsigned long long* cnt = F.band_done + item.group;
+      const unsigned long long target =
+          (unsigned long long)min(WAVE_GROUP_ROWS, F.r1 - item.group * WAVE_GROUP_ROWS) * (unsigned long long)F.r2;
+      if (threadIdx.x == 0 && ld_acquire(cnt) < target) {
+        const long long t0 = globaltimer_ns();
+        while (ld_acquire(cnt) < target) {
+          // a wait that already gave up (this launch or the producer failed)
+          // ends every later wait at once
+          if ((*(volatile int*)flag & FLAG_TIMEOUT) || globaltimer_ns() - t0 > BAND_WAIT_NS) {
+            atomicOr(flag, FLAG_TIMEOUT);
+            break;
+          }
+          __nanosleep(256);
+        }
+      }
+      __syncthreads();
+      (void)ld_acquire(cnt);
+    }
     if (item.group * WAVE_GROUP_ROWS + warp * 32 < F.r1)
       run_strip<DECOMP>(F, item.group, warp, lane, sh, tiles[warp], flag);
     __syncthreads();
@@ -330,7 +363,8 @@ __global__ void __launch_bounds__(WAVE_WARPS * 32, 1) wave2d_kernel(const WaveFi
 }  // namespace
 
 int launch_wave2d(cpsz_b200_ctx* ctx, bool decompress, const WaveField* d_fields, const WaveItem* d_items,
-                  int n_items, int* d_queue, size_t points) {
+                  int n_items, int* d_queue, size_t points, cudaStream_t stream, bool concurrent) {
+  if (!stream) stream = ctx->stream;
   static bool attr_set[2] = {false, false};
   if (!attr_set[decompress]) {
     cudaError_t e = decompress ? cudaFuncSetAttribute(wave2d_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -348,15 +382,16 @@ int launch_wave2d(cpsz_b200_ctx* ctx, bool decompress, const WaveField* d_fields
   if (per_sm < 1) return set_error(CPSZ_ERR_CUDA, "wave2d kernel does not fit on an SM");
   const int cap = tune_get(TUNE_WAVE2D_CTAS_PER_SM, points);
   if (cap > 0 && per_sm > cap) per_sm = cap;
+  if (concurrent) per_sm = 1;
   int grid = ctx->num_sms * per_sm;
   if (grid > n_items) grid = n_items;
   if (grid < 1) return CPSZ_OK;
   if (decompress)
-    wave2d_kernel<true><<<grid, WAVE_WARPS * 32, kDynSmem, ctx->stream>>>(d_fields, d_items, n_items, d_queue,
-                                                                          ctx->d_flag);
+    wave2d_kernel<true><<<grid, WAVE_WARPS * 32, kDynSmem, stream>>>(d_fields, d_items, n_items, d_queue,
+                                                                     ctx->d_flag);
   else
-    wave2d_kernel<false><<<grid, WAVE_WARPS * 32, kDynSmem, ctx->stream>>>(d_fields, d_items, n_items, d_queue,
-                                                                           ctx->d_flag);
+    wave2d_kernel<false><<<grid, WAVE_WARPS * 32, kDynSmem, stream>>>(d_fields, d_items, n_items, d_queue,
+                                                                      ctx->d_flag);
   count_launch(ctx);
   return check_launch("wave2d_kernel");
 }
