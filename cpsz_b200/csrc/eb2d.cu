@@ -145,6 +145,22 @@ __global__ void __launch_bounds__(NT) eb2d_kernel(const float* __restrict__ U, c
   }
 }
 
+int preload_eb2d() {
+  // With lazy module loading a kernel's first launch loads its module, and a
+  // load may wait for running kernels; a wavefront already waiting on eb2d
+  // would then never see it start.  Querying the attributes loads each
+  // instantiation up front.
+  cudaFuncAttributes a;
+  const void* fns[] = {(const void*)eb2d_kernel<32, 16, 256>, (const void*)eb2d_kernel<32, 8, 128>,
+                       (const void*)eb2d_kernel<64, 8, 256>,  (const void*)eb2d_kernel<32, 32, 256>,
+                       (const void*)eb2d_kernel<64, 16, 256>, (const void*)eb2d_kernel<32, 16, 128>};
+  for (const void* f : fns) {
+    cudaError_t e = cudaFuncGetAttributes(&a, f);
+    if (e != cudaSuccess) return set_error(CPSZ_ERR_CUDA, "loading eb2d_kernel: %s", cudaGetErrorString(e));
+  }
+  return CPSZ_OK;
+}
+
 int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, double max_pwr_eb,
                 const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
                 float2* pair_u, float2* pair_v, double* eb_out, int row_begin, int row_end,

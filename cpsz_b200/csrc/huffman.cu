@@ -188,18 +188,60 @@ constexpr int HIST_NT = 512;
 constexpr int HIST_LO = 32768 - 4096;  // shared window of the code histogram
 constexpr int HIST_W = 8192;
 
+// Codes concentrate on 32768 and its neighbours (prediction errors of zero and
+// one quantum): those three are counted in registers and reduced once per
+// warp, so the shared-memory atomics see only the spread-out remainder (no
+// 32-way same-address conflicts).  Reads are 16-byte vectors where aligned.
+__device__ __forceinline__ void hist_add(unsigned int* sh, unsigned long long* hist, unsigned v, unsigned& c_lo,
+                                         unsigned& c_mid, unsigned& c_hi) {
+  const unsigned d = v - 32767u;
+  if (d < 3u) {
+    c_lo += d == 0u;
+    c_mid += d == 1u;
+    c_hi += d == 2u;
+  } else if (v == 0u) {
+    atomicAdd(&sh[HIST_W], 1u);
+  } else if (v - (unsigned)HIST_LO < (unsigned)HIST_W) {
+    atomicAdd(&sh[v - HIST_LO], 1u);
+  } else {
+    atomicAdd(&hist[v], 1ull);
+  }
+}
+
 __global__ void __launch_bounds__(HIST_NT) hist_u16_kernel(const uint16_t* __restrict__ s, size_t n,
                                                            unsigned long long* __restrict__ hist) {
   __shared__ unsigned int sh[HIST_W + 1];  // window + symbol 0
   for (int k = threadIdx.x; k <= HIST_W; k += HIST_NT) sh[k] = 0;
   __syncthreads();
-  size_t stride = (size_t)gridDim.x * HIST_NT;
-  for (size_t i = (size_t)blockIdx.x * HIST_NT + threadIdx.x; i < n; i += stride) {
-    int v = s[i];
-    int w = v - HIST_LO;
-    if (v == 0) atomicAdd(&sh[HIST_W], 1u);
-    else if ((unsigned)w < (unsigned)HIST_W) atomicAdd(&sh[w], 1u);
-    else atomicAdd(&hist[v], 1ull);
+  unsigned c_lo = 0, c_mid = 0, c_hi = 0;
+  const size_t stride = (size_t)gridDim.x * HIST_NT;
+  const size_t t0 = (size_t)blockIdx.x * HIST_NT + threadIdx.x;
+  // elements before the first 16-byte boundary, the vector body, the tail
+  const size_t head = ((16 - ((uintptr_t)s & 15)) & 15) / 2;
+  const size_t h = head < n ? head : n;
+  if (t0 < h) hist_add(sh, hist, s[t0], c_lo, c_mid, c_hi);
+  const size_t nv = (n - h) / 8;
+  const uint4* sv = reinterpret_cast<const uint4*>(s + h);
+  for (size_t i = t0; i < nv; i += stride) {
+    const uint4 w = __ldcs(sv + i);
+    const unsigned ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      hist_add(sh, hist, ws[q] & 0xffffu, c_lo, c_mid, c_hi);
+      hist_add(sh, hist, ws[q] >> 16, c_lo, c_mid, c_hi);
+    }
+  }
+  for (size_t i = h + nv * 8 + t0; i < n; i += stride) hist_add(sh, hist, s[i], c_lo, c_mid, c_hi);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    c_lo += __shfl_down_sync(0xffffffffu, c_lo, o);
+    c_mid += __shfl_down_sync(0xffffffffu, c_mid, o);
+    c_hi += __shfl_down_sync(0xffffffffu, c_hi, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (c_lo) atomicAdd(&sh[32767 - HIST_LO], c_lo);
+    if (c_mid) atomicAdd(&sh[32768 - HIST_LO], c_mid);
+    if (c_hi) atomicAdd(&sh[32769 - HIST_LO], c_hi);
   }
   __syncthreads();
   for (int k = threadIdx.x; k < HIST_W; k += HIST_NT)

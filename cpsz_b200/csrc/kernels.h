@@ -36,6 +36,10 @@ int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int 
                 float2* pair_u, float2* pair_v, double* eb_out = nullptr, int row_begin = 0, int row_end = -1,
                 unsigned long long* band_done = nullptr);
 
+// Loads every eb2d instantiation (required before a consumer that waits on
+// eb2d is launched: a lazily loaded first launch could wait for it).
+int preload_eb2d();
+
 // The same quantization for given per-vertex bounds eb_in[n] (learned bounds).
 int launch_quant2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t n, const double* eb_in,
                    const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
@@ -70,12 +74,19 @@ constexpr int WAVE_WARPS = 4;
 constexpr int WAVE_GROUP_ROWS = WAVE_WARPS * 32;
 // Items must be ordered so that (field, g-1) precedes (field, g).  `points`
 // (all fields of the launch together) keys the launch-shape table.  The launch
-// goes to `stream` (default: the context's stream); `concurrent` marks a
-// launch that runs beside its producer (fields with band_done): at most one
-// CTA per SM then, which leaves every SM room for the producer's CTAs, so the
-// producer always progresses while wavefront CTAs wait on it.
+// goes to `stream` (default: the context's stream).  Modes:
+//   WAVE_ALONE   the only wavefront launch on the queue: the tuned CTAs per SM;
+//   WAVE_BESIDE  runs beside its producer (fields with band_done): one CTA per
+//                SM, which leaves every SM room for the producer's CTAs, so
+//                the producer always progresses while wavefront CTAs wait;
+//   WAVE_JOIN    launched once the producer is done, while a WAVE_BESIDE launch
+//                on the same queue still runs: the remaining CTAs per SM pull
+//                from the shared queue (no launch when none remain).
+// Every dequeued item belongs to a resident CTA, whichever launch it is in, so
+// the waits between items of one field end in every mode.
+enum WaveMode { WAVE_ALONE = 0, WAVE_BESIDE = 1, WAVE_JOIN = 2 };
 int launch_wave2d(cpsz_b200_ctx* ctx, bool decompress, const WaveField* d_fields, const WaveItem* d_items,
-                  int n_items, int* d_queue, size_t points, cudaStream_t stream = nullptr, bool concurrent = false);
+                  int n_items, int* d_queue, size_t points, cudaStream_t stream = nullptr, int mode = WAVE_ALONE);
 
 // ---- block-order plumbing (12 x 12 blocks) ---------------------------------------
 // Raster (pitched) -> 12x12-block order, and back.  Histogram of the block-order

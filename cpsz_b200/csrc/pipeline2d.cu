@@ -330,12 +330,14 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     jobs[k].h_nunpred = (unsigned int*)(jobs[k].h_hist_codes + 2 * 65536);
   }
 
-  // Derived bounds (eb2d) signal per 128-row group, so the wavefront runs
-  // beside them on the high-priority stream and starts on a group as soon as
-  // its pairs are written.  Given bounds (quant2d) are not row-ordered: the
-  // wavefront then follows them on the main stream.
-  bool overlap = true;
-  for (const Job2D& j : jobs) overlap &= j.eb_ext == nullptr;
+  // Derived bounds (eb2d) signal per 128-row group, so for one field the
+  // wavefront runs beside them on the high-priority stream and starts on a
+  // group as soon as its pairs are written: its items (group-major over the
+  // two components) come in the order eb2d finishes them.  A batch's items
+  // are group-major across fields while eb2d finishes field after field, so a
+  // batch (and given bounds, quant2d, which are not row-ordered) runs the
+  // wavefront after the bounds with every CTA slot.
+  const bool overlap = nj == 1 && jobs[0].eb_ext == nullptr;
 
   // ---- setup: flags, tables, wavefront descriptors ----
   reset_marks(ctx);
@@ -383,10 +385,11 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     }
   } hi_drain;
   if (overlap) {
+    CPSZ_TRY(preload_eb2d());
     hi_drain.s = ctx->hi;
     CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[3], st));
     CPSZ_CUDA_TRY(cudaStreamWaitEvent(ctx->hi, ctx->ev[3], 0));
-    CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points, ctx->hi, true));
+    CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points, ctx->hi, WAVE_BESIDE));
     CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[4], ctx->hi));
   }
 
@@ -411,24 +414,28 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       const int nch = (j.r1 + R - 1) / R;
       CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[2], st));
       CPSZ_CUDA_TRY(cudaStreamWaitEvent(ctx->aux, ctx->ev[2], 0));
+      // band c needs chunks c and c + 1; it is enqueued right after chunk
+      // c + 1's copy call (a copy from pageable memory returns only once the
+      // host has staged it, so enqueueing every copy first would hold the
+      // bands back until the whole field was staged)
+      auto band_launch = [&](int c) -> int {
+        CPSZ_CUDA_TRY(cudaStreamWaitEvent(st, ctx->up_ev[c], 0));
+        if (c + 1 < nch) CPSZ_CUDA_TRY(cudaStreamWaitEvent(st, ctx->up_ev[c + 1], 0));
+        if (j.eb_ext)
+          return launch_quant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
+                                j.d.hist_ids, j.d.pairs[0], j.d.pairs[1]);
+        return launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N, j.d.hist_ids,
+                           j.d.pairs[0], j.d.pairs[1], nullptr, c * R, std::min(j.r1, (c + 1) * R), band);
+      };
       for (int c = 0; c < nch; c++) {
         const size_t off = (size_t)c * R * j.r2;
         const size_t cnt = (size_t)(std::min(j.r1, (c + 1) * R) - c * R) * j.r2;
         CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.U + off, j.U_in + off, 4 * cnt, cudaMemcpyHostToDevice, ctx->aux));
         CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.V + off, j.V_in + off, 4 * cnt, cudaMemcpyHostToDevice, ctx->aux));
         CPSZ_CUDA_TRY(cudaEventRecord(ctx->up_ev[c], ctx->aux));
+        if (c >= 1) CPSZ_TRY(band_launch(c - 1));
       }
-      for (int c = 0; c < nch; c++) {
-        CPSZ_CUDA_TRY(cudaStreamWaitEvent(st, ctx->up_ev[c], 0));
-        if (c + 1 < nch) CPSZ_CUDA_TRY(cudaStreamWaitEvent(st, ctx->up_ev[c + 1], 0));
-        if (j.eb_ext)
-          CPSZ_TRY(launch_quant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
-                                  j.d.hist_ids, j.d.pairs[0], j.d.pairs[1]));
-        else
-          CPSZ_TRY(launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
-                               j.d.hist_ids, j.d.pairs[0], j.d.pairs[1], nullptr, c * R,
-                               std::min(j.r1, (c + 1) * R), band));
-      }
+      CPSZ_TRY(band_launch(nch - 1));
     }
     CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_hist_ids, j.d.hist_ids, 256 * 8, cudaMemcpyDeviceToHost, st));
   }
@@ -438,8 +445,13 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
 
   // ---- stage 2: one persistent wavefront over every field of the pass ----
   mark(ctx, "wave2d_compress");
-  if (overlap) CPSZ_CUDA_TRY(cudaStreamWaitEvent(st, ctx->ev[4], 0));
-  else CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points));
+  if (overlap) {
+    // the bounds are done: the rest of each SM joins the running wavefront
+    CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points, st, WAVE_JOIN));
+    CPSZ_CUDA_TRY(cudaStreamWaitEvent(st, ctx->ev[4], 0));
+  } else {
+    CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points));
+  }
   if (tap && tap->recon_only) {
     int flag = 0;
     CPSZ_TRY(read_flag(ctx, &flag));
@@ -447,20 +459,27 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   }
   mark(ctx, "blocks+hist+unpred");
 
-  // ---- stage 3: block order, histograms, unpredictables ----
+  // ---- stage 3: code histograms first (the host builds the code trees from
+  // them while the GPU converts to block order and gathers unpredictables) ----
   for (int k = 0; k < nj; k++) {
     Job2D& j = jobs[k];
     for (int f = 0; f < 2; f++) {
       CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.hist_codes[f], 0, 65536 * 8, st));
-      CPSZ_TRY(launch_raster_to_blocks_u16(ctx, j.d.craster[f], j.r2, j.r1, j.r2, j.d.cblocks[f], j.d.hist_codes[f]));
+      CPSZ_TRY(launch_hist_u16(ctx, j.d.craster[f], j.N, j.d.hist_codes[f]));
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_hist_codes + (size_t)f * 65536, j.d.hist_codes[f], 65536 * 8,
+                                    cudaMemcpyDeviceToHost, st));
+      CPSZ_CUDA_TRY(cudaEventRecord(ctx->job_ev[2 * k + f], st));
+    }
+  }
+  for (int k = 0; k < nj; k++) {
+    Job2D& j = jobs[k];
+    for (int f = 0; f < 2; f++) {
+      CPSZ_TRY(launch_raster_to_blocks_u16(ctx, j.d.craster[f], j.r2, j.r1, j.r2, j.d.cblocks[f], nullptr));
       CPSZ_TRY(launch_segment_scan(ctx, j.d.craster[f], j.r2, j.r1, j.r2, j.d.seg_cnt[f], j.d.seg_off[f],
                                    j.d.scan_tmp[f]));
       CPSZ_TRY(launch_gather_unpred(ctx, j.d.craster[f], j.r2, f ? j.d.V : j.d.U, j.r2, j.r1, j.r2, j.d.seg_off[f],
                                     j.d.unpred[f]));
-      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_hist_codes + (size_t)f * 65536, j.d.hist_codes[f], 65536 * 8,
-                                    cudaMemcpyDeviceToHost, st));
       CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_nunpred + f, j.d.seg_off[f] + j.nseg, 4, cudaMemcpyDeviceToHost, st));
-      CPSZ_CUDA_TRY(cudaEventRecord(ctx->job_ev[2 * k + f], st));
     }
   }
   mark(ctx, "host_trees");
@@ -499,8 +518,6 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   mark(ctx, "huffman_encode");
   for (Job2D& j : jobs) {
     if (!j.tree_ok[1] || !j.tree_ok[2]) return tree_failure();
-    j.n_unpred[0] = j.h_nunpred[0];
-    j.n_unpred[1] = j.h_nunpred[1];
     for (int k = 1; k < 3; k++) {
       j.sec_bytes[k] = huff_section_bytes(j.cb[k]);
       j.bits_bytes[k] = (j.cb[k].total_bits + 7) / 8;
@@ -516,8 +533,12 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   }
   {
     int flag = 0;
-    CPSZ_TRY(read_flag(ctx, &flag));
+    CPSZ_TRY(read_flag(ctx, &flag));  // synchronizes the stream: the counts below have landed
     if (flag) return flag_error(flag);
+  }
+  for (Job2D& j : jobs) {
+    j.n_unpred[0] = j.h_nunpred[0];
+    j.n_unpred[1] = j.h_nunpred[1];
   }
 
   // ---- stage 5: blob assembly in device memory ----

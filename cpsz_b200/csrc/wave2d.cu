@@ -363,7 +363,7 @@ __global__ void __launch_bounds__(WAVE_WARPS * 32, 1) wave2d_kernel(const WaveFi
 }  // namespace
 
 int launch_wave2d(cpsz_b200_ctx* ctx, bool decompress, const WaveField* d_fields, const WaveItem* d_items,
-                  int n_items, int* d_queue, size_t points, cudaStream_t stream, bool concurrent) {
+                  int n_items, int* d_queue, size_t points, cudaStream_t stream, int mode) {
   if (!stream) stream = ctx->stream;
   static bool attr_set[2] = {false, false};
   if (!attr_set[decompress]) {
@@ -382,7 +382,9 @@ int launch_wave2d(cpsz_b200_ctx* ctx, bool decompress, const WaveField* d_fields
   if (per_sm < 1) return set_error(CPSZ_ERR_CUDA, "wave2d kernel does not fit on an SM");
   const int cap = tune_get(TUNE_WAVE2D_CTAS_PER_SM, points);
   if (cap > 0 && per_sm > cap) per_sm = cap;
-  if (concurrent) per_sm = 1;
+  if (mode == WAVE_BESIDE) per_sm = 1;
+  if (mode == WAVE_JOIN) per_sm -= 1;
+  if (per_sm < 1) return CPSZ_OK;
   int grid = ctx->num_sms * per_sm;
   if (grid > n_items) grid = n_items;
   if (grid < 1) return CPSZ_OK;
