@@ -199,6 +199,107 @@ __global__ void __launch_bounds__(SCAN_NT) scan_down_kernel(const unsigned int* 
   if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = part[gridDim.x];
 }
 
+// ---- strips: a 12-row block row cut into runs of STRIP_BLOCKS blocks ----------------
+// A strip's blocks are consecutive in block order, so its block-order image is
+// one contiguous range: the strip is staged in shared memory with coalesced
+// row reads and written out with coalesced block-order writes.
+constexpr int STRIP_BLOCKS = 32;
+constexpr int STRIP_W = STRIP_BLOCKS * BS;  // 384 columns
+constexpr int STRIP_NT = 256;
+
+struct StripGeom {
+  int bi, h, c0, W, nb, wl;
+  long long out0;  // block-order position of the strip's first element
+};
+__device__ __forceinline__ StripGeom strip_geom(long long s, int r1, int r2, int nsc) {
+  StripGeom g;
+  g.bi = (int)(s / nsc);
+  const int sc = (int)(s - (long long)g.bi * nsc);
+  g.h = min(BS, r1 - g.bi * BS);
+  g.c0 = sc * STRIP_W;
+  g.W = min(STRIP_W, r2 - g.c0);
+  g.nb = (g.W + BS - 1) / BS;
+  g.wl = g.W - (g.nb - 1) * BS;  // width of the strip's last block (12 unless it ends the row)
+  g.out0 = (long long)g.bi * BS * r2 + (long long)sc * STRIP_BLOCKS * BS * g.h;
+  return g;
+}
+// block-order offset o inside the strip -> (row, column) inside the strip
+__device__ __forceinline__ void strip_rc(const StripGeom& g, int o, int& li, int& col) {
+  const int b = o / (BS * g.h);
+  const int rem = o - b * BS * g.h;
+  const int w = (b == g.nb - 1) ? g.wl : BS;
+  li = rem / w;
+  col = b * BS + (rem - li * w);
+}
+
+__global__ void __launch_bounds__(STRIP_NT) r2b_strip_kernel(const uint16_t* __restrict__ raster, long long pitch,
+                                                             int r1, int r2, int nsc, uint16_t* __restrict__ blocks,
+                                                             unsigned int* __restrict__ strip_cnt) {
+  __shared__ uint16_t t[BS][STRIP_W + 2];
+  __shared__ unsigned int wsum[STRIP_NT / 32];
+  const StripGeom g = strip_geom(blockIdx.x, r1, r2, nsc);
+  const uint16_t* src = raster + (long long)g.bi * BS * pitch + g.c0;
+  for (int li = 0; li < g.h; li++)
+    for (int c = threadIdx.x; c < g.W; c += STRIP_NT) t[li][c] = src[(long long)li * pitch + c];
+  __syncthreads();
+  unsigned int z = 0;
+  uint16_t* dst = blocks + g.out0;
+  const int n = g.h * g.W;
+  for (int o = threadIdx.x; o < n; o += STRIP_NT) {
+    int li, col;
+    strip_rc(g, o, li, col);
+    const uint16_t v = t[li][col];
+    dst[o] = v;
+    z += v == 0;
+  }
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) z += __shfl_down_sync(0xffffffffu, z, d);
+  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = z;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int tot = 0;
+    for (int w = 0; w < STRIP_NT / 32; w++) tot += wsum[w];
+    strip_cnt[blockIdx.x] = tot;
+  }
+}
+
+// Unpredictable values (code 0) of each strip in block order, at the strip's
+// offset (exclusive scan of the counts).  Strips without any return at once.
+__global__ void __launch_bounds__(STRIP_NT) gather_strip_kernel(const uint16_t* __restrict__ raster, long long pitch,
+                                                                const float* __restrict__ x, long long x_pitch,
+                                                                int r1, int r2, int nsc,
+                                                                const unsigned int* __restrict__ strip_off,
+                                                                float* __restrict__ unpred) {
+  __shared__ unsigned int wsum[STRIP_NT / 32];
+  const unsigned int base = strip_off[blockIdx.x];
+  if (strip_off[blockIdx.x + 1] == base) return;
+  const StripGeom g = strip_geom(blockIdx.x, r1, r2, nsc);
+  const int n = g.h * g.W;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned int run = base;
+  for (int o0 = 0; o0 < n; o0 += STRIP_NT) {
+    const int o = o0 + threadIdx.x;
+    int li = 0, col = 0;
+    bool z = false;
+    if (o < n) {
+      strip_rc(g, o, li, col);
+      z = raster[(long long)(g.bi * BS + li) * pitch + g.c0 + col] == 0;
+    }
+    const unsigned int m = __ballot_sync(0xffffffffu, z);
+    if (lane == 0) wsum[warp] = __popc(m);
+    __syncthreads();
+    unsigned int before = 0, tot = 0;
+    for (int w = 0; w < STRIP_NT / 32; w++) {
+      const unsigned int c = wsum[w];
+      before += (w < warp) ? c : 0u;
+      tot += c;
+    }
+    if (z) unpred[run + before + __popc(m & ((1u << lane) - 1u))] = x[(long long)(g.bi * BS + li) * x_pitch + g.c0 + col];
+    run += tot;
+    __syncthreads();
+  }
+}
+
 inline long long nseg_of(int r1, int r2) { return (long long)r1 * ((r2 - 1) / BS + 1); }
 inline unsigned grid_of(long long n) { return (unsigned)((n + NT - 1) / NT); }
 
@@ -241,6 +342,34 @@ int launch_blocks_to_raster_u16(cpsz_b200_ctx* ctx, const uint16_t* blocks, int 
 }
 
 size_t segment_scan_tmp_bytes(int r1, int r2) { return scan_u32_tmp_bytes((size_t)nseg_of(r1, r2)); }
+
+size_t strip_count(int r1, int r2) {
+  const long long nbx = (r1 + BS - 1) / BS, nsc = (r2 + STRIP_W - 1) / STRIP_W;
+  return (size_t)(nbx * nsc);
+}
+
+int launch_r2b_strips(cpsz_b200_ctx* ctx, const uint16_t* raster, long long pitch, int r1, int r2, uint16_t* blocks,
+                      unsigned int* strip_cnt, unsigned int* strip_off, void* scan_tmp) {
+  const size_t ns = strip_count(r1, r2);
+  if (ns == 0) return CPSZ_OK;
+  if (ns > 0x7fffffffu) return set_error(CPSZ_ERR_UNSUPPORTED, "field of %zu strips", ns);
+  const int nsc = (r2 + STRIP_W - 1) / STRIP_W;
+  r2b_strip_kernel<<<(unsigned)ns, STRIP_NT, 0, ctx->stream>>>(raster, pitch, r1, r2, nsc, blocks, strip_cnt);
+  count_launch(ctx);
+  CPSZ_TRY(check_launch("r2b_strip_kernel"));
+  return launch_scan_u32(ctx, strip_cnt, strip_off, ns, scan_tmp);
+}
+
+int launch_gather_strips(cpsz_b200_ctx* ctx, const uint16_t* raster, long long pitch, const float* x,
+                         long long x_pitch, int r1, int r2, const unsigned int* strip_off, float* unpred) {
+  const size_t ns = strip_count(r1, r2);
+  if (ns == 0) return CPSZ_OK;
+  const int nsc = (r2 + STRIP_W - 1) / STRIP_W;
+  gather_strip_kernel<<<(unsigned)ns, STRIP_NT, 0, ctx->stream>>>(raster, pitch, x, x_pitch, r1, r2, nsc, strip_off,
+                                                                  unpred);
+  count_launch(ctx);
+  return check_launch("gather_strip_kernel");
+}
 
 int launch_segment_scan(cpsz_b200_ctx* ctx, const uint16_t* codes_raster, long long pitch, int r1, int r2,
                         unsigned int* seg_count, unsigned int* seg_off, void* scan_tmp) {

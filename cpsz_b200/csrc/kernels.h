@@ -100,6 +100,16 @@ int launch_blocks_to_raster_u16(cpsz_b200_ctx* ctx, const uint16_t* blocks, int 
                                 long long pitch, const uint8_t* ids = nullptr, float2* pair = nullptr);
 // Zero-code counts per row segment (one 12-wide block row) in block order,
 // exclusive-scanned into seg_off (size r1*nby+1; seg_off[r1*nby] = total).
+// Compression side, one pass per field: codes raster -> 12x12-block order plus
+// the unpredictable count of every strip (a 12-row block row cut into runs of
+// 32 blocks) and its exclusive scan strip_off[0..n] (strip_off[n] = total);
+// then the unpredictable values in block order.  Strip arrays hold
+// strip_count(r1, r2) + 1 entries (never more than the segment arrays).
+size_t strip_count(int r1, int r2);
+int launch_r2b_strips(cpsz_b200_ctx* ctx, const uint16_t* raster, long long pitch, int r1, int r2, uint16_t* blocks,
+                      unsigned int* strip_cnt, unsigned int* strip_off, void* scan_tmp);
+int launch_gather_strips(cpsz_b200_ctx* ctx, const uint16_t* raster, long long pitch, const float* x,
+                         long long x_pitch, int r1, int r2, const unsigned int* strip_off, float* unpred);
 int launch_segment_scan(cpsz_b200_ctx* ctx, const uint16_t* codes_raster, long long pitch, int r1, int r2,
                         unsigned int* seg_count, unsigned int* seg_off, void* scan_tmp);
 size_t segment_scan_tmp_bytes(int r1, int r2);

@@ -337,7 +337,7 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   // are group-major across fields while eb2d finishes field after field, so a
   // batch (and given bounds, quant2d, which are not row-ordered) runs the
   // wavefront after the bounds with every CTA slot.
-  const bool overlap = nj == 1 && jobs[0].eb_ext == nullptr;
+  const bool overlap = nj == 1 && jobs[0].eb_ext == nullptr && tune_get(TUNE_WAVE2D_OVERLAP, jobs[0].N) != 0;
 
   // ---- setup: flags, tables, wavefront descriptors ----
   reset_marks(ctx);
@@ -474,12 +474,12 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   for (int k = 0; k < nj; k++) {
     Job2D& j = jobs[k];
     for (int f = 0; f < 2; f++) {
-      CPSZ_TRY(launch_raster_to_blocks_u16(ctx, j.d.craster[f], j.r2, j.r1, j.r2, j.d.cblocks[f], nullptr));
-      CPSZ_TRY(launch_segment_scan(ctx, j.d.craster[f], j.r2, j.r1, j.r2, j.d.seg_cnt[f], j.d.seg_off[f],
-                                   j.d.scan_tmp[f]));
-      CPSZ_TRY(launch_gather_unpred(ctx, j.d.craster[f], j.r2, f ? j.d.V : j.d.U, j.r2, j.r1, j.r2, j.d.seg_off[f],
+      CPSZ_TRY(launch_r2b_strips(ctx, j.d.craster[f], j.r2, j.r1, j.r2, j.d.cblocks[f], j.d.seg_cnt[f],
+                                 j.d.seg_off[f], j.d.scan_tmp[f]));
+      CPSZ_TRY(launch_gather_strips(ctx, j.d.craster[f], j.r2, f ? j.d.V : j.d.U, j.r2, j.r1, j.r2, j.d.seg_off[f],
                                     j.d.unpred[f]));
-      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_nunpred + f, j.d.seg_off[f] + j.nseg, 4, cudaMemcpyDeviceToHost, st));
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_nunpred + f, j.d.seg_off[f] + strip_count(j.r1, j.r2), 4,
+                                    cudaMemcpyDeviceToHost, st));
     }
   }
   mark(ctx, "host_trees");

@@ -27,6 +27,7 @@ const TuneInfo kInfo[TUNE_COUNT] = {
     {"eb3d.fill", 4, 1, 32},
     {"eb3d.min_chunk", 8, 1, 256},
     {"h2d.chunks", 8, 1, 8},
+    {"wave2d.overlap", 1, 0, 1},
 };
 
 struct Entry {
@@ -243,6 +244,13 @@ void suppress_autoload() { std::call_once(g_once, [] {}); }
 const TuneInfo& tune_info(int p) { return kInfo[p]; }
 
 int tune_get(TuneParam p, size_t points) {
+  if (p == TUNE_WAVE2D_OVERLAP) {
+    static const bool env_off = [] {
+      const char* e = getenv("CPSZ_B200_OVERLAP");
+      return e && !strcmp(e, "0");
+    }();
+    if (env_off) return 0;
+  }
   std::shared_lock<std::shared_mutex> lk(g_mu);
   int v = kInfo[p].def;
   for (const Entry& e : g_tab[p]) {

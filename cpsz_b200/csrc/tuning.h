@@ -25,6 +25,9 @@ enum TuneParam {
   TUNE_EB3D_FILL,           // eb3d: split i so the grid covers the SMs this many times
   TUNE_EB3D_MIN_CHUNK,      // eb3d: fewest i-planes one CTA marches over
   TUNE_H2D_CHUNKS,          // host-input uploads: row chunks overlapped with eb2d
+  TUNE_WAVE2D_OVERLAP,      // 1: the wavefront runs beside eb2d (0: after it; tools
+                            // that serialize kernels need 0, also set by
+                            // the environment variable CPSZ_B200_OVERLAP=0)
   TUNE_COUNT
 };
 

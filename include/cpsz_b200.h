@@ -60,7 +60,9 @@ int cpsz_b200_ctx_stage_times(cpsz_b200_ctx* ctx, int max_stages, const char** n
  * (every blob is byte-identical for every value): "eb2d.tile" (0..5: 32x16/256
  * threads, 32x8/128, 64x8/256, 32x32/256, 64x16/256, 32x16/128),
  * "wave2d.ctas_per_sm" (0 = occupancy limit), "eb3d.fill", "eb3d.min_chunk",
- * "h2d.chunks".  An entry applies to fields of >= min_points points; the
+ * "h2d.chunks", "wave2d.overlap" (1: the Lorenzo wavefront runs beside the
+ * bound kernel; 0: after it -- needed under tools that serialize kernels,
+ * also forced by the environment variable CPSZ_B200_OVERLAP=0).  An entry applies to fields of >= min_points points; the
  * largest such threshold wins.  The first cpsz_b200_ctx_create() loads
  * $CPSZ_B200_TUNING (empty or "none": no table) or else tuning_b200.json of the
  * package directory when present; a malformed table fails ctx creation.  Any

@@ -29,6 +29,9 @@ def test_eb2d_tiles_and_wave_shapes_give_equal_blobs(ctx, oracle, shape):
         cpsz_b200.tuning_set("eb2d.tile", v)
         assert cpsz_b200.sz_compress_cp_preserve_2d_offline(U, V, max_pwr_eb=0.1, ctx=ctx) == ref, v
     cpsz_b200.tuning_clear()
+    cpsz_b200.tuning_set("wave2d.overlap", 0)
+    assert cpsz_b200.sz_compress_cp_preserve_2d_offline(U, V, max_pwr_eb=0.1, ctx=ctx) == ref
+    cpsz_b200.tuning_clear()
     for v in (1, 2, 3):
         cpsz_b200.tuning_set("wave2d.ctas_per_sm", v)
         b = cpsz_b200.sz_compress_cp_preserve_2d_offline(U, V, max_pwr_eb=0.1, ctx=ctx)

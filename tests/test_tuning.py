@@ -22,7 +22,8 @@ def _restore_table():
 
 def test_parameters_and_defaults():
     p = cpsz_b200.tuning_params()
-    assert set(p) == {"eb2d.tile", "wave2d.ctas_per_sm", "eb3d.fill", "eb3d.min_chunk", "h2d.chunks"}
+    assert set(p) == {"eb2d.tile", "wave2d.ctas_per_sm", "eb3d.fill", "eb3d.min_chunk", "h2d.chunks",
+                      "wave2d.overlap"}
     for name, (d, lo, hi) in p.items():
         assert lo <= d <= hi
     cpsz_b200.tuning_clear()
