@@ -223,80 +223,142 @@ __device__ __forceinline__ StripGeom strip_geom(long long s, int r1, int r2, int
   g.out0 = (long long)g.bi * BS * r2 + (long long)sc * STRIP_BLOCKS * BS * g.h;
   return g;
 }
-// block-order offset o inside the strip -> (row, column) inside the strip
-__device__ __forceinline__ void strip_rc(const StripGeom& g, int o, int& li, int& col) {
-  const int b = o / (BS * g.h);
-  const int rem = o - b * BS * g.h;
-  const int w = (b == g.nb - 1) ? g.wl : BS;
-  li = rem / w;
-  col = b * BS + (rem - li * w);
+// One pass per component.  A CTA takes the next strip in ticket order (tickets
+// go out in the order CTAs start, so every earlier strip belongs to a CTA that
+// is running or done), stages it, writes its block-order image, publishes its
+// unpredictable count, finds the count of all earlier strips by a decoupled
+// look-back over their published words (Merrill & Garland, "Single-pass
+// Parallel Prefix Scan with Decoupled Look-back", 2016) and writes its
+// unpredictable values in block order.  Status words: 2-bit state (0 = not
+// yet, AGG = the strip's own count, PRE = inclusive prefix) over a 62-bit count.
+constexpr unsigned long long ST_AGG = 1ull << 62, ST_PRE = 2ull << 62, ST_VAL = (1ull << 62) - 1;
+constexpr long long LOOKBACK_SPIN = 1ll << 24;
+constexpr unsigned FULLM = 0xffffffffu;
+
+struct StripPass {
+  const uint16_t* raster;
+  const float* x;
+  uint16_t* blocks;
+  float* unpred;
+  unsigned long long* status;  // ns words, then the ticket and the field total (u32 each); zeroed
+};
+
+__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
-__global__ void __launch_bounds__(STRIP_NT) r2b_strip_kernel(const uint16_t* __restrict__ raster, long long pitch,
-                                                             int r1, int r2, int nsc, uint16_t* __restrict__ blocks,
-                                                             unsigned int* __restrict__ strip_cnt) {
+__global__ void __launch_bounds__(STRIP_NT) strip_pass_kernel(StripPass P0, StripPass P1, long long pitch,
+                                                              long long x_pitch, int r1, int r2, int nsc,
+                                                              unsigned int ns, int* flag) {
   __shared__ uint16_t t[BS][STRIP_W + 2];
-  __shared__ unsigned int wsum[STRIP_NT / 32];
-  const StripGeom g = strip_geom(blockIdx.x, r1, r2, nsc);
-  const uint16_t* src = raster + (long long)g.bi * BS * pitch + g.c0;
+  __shared__ unsigned int bz[STRIP_BLOCKS], bpre[STRIP_BLOCKS];
+  __shared__ unsigned int s_idx;
+  __shared__ unsigned long long s_excl;
+  const StripPass P = blockIdx.y ? P1 : P0;
+  unsigned int* ticket = reinterpret_cast<unsigned int*>(P.status + ns);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_idx = atomicAdd(ticket, 1u);
+  __syncthreads();
+  const unsigned int s = s_idx;
+  const StripGeom g = strip_geom(s, r1, r2, nsc);
+  const uint16_t* src = P.raster + (long long)g.bi * BS * pitch + g.c0;
   for (int li = 0; li < g.h; li++)
     for (int c = threadIdx.x; c < g.W; c += STRIP_NT) t[li][c] = src[(long long)li * pitch + c];
   __syncthreads();
-  unsigned int z = 0;
-  uint16_t* dst = blocks + g.out0;
-  const int n = g.h * g.W;
-  for (int o = threadIdx.x; o < n; o += STRIP_NT) {
-    int li, col;
-    strip_rc(g, o, li, col);
-    const uint16_t v = t[li][col];
-    dst[o] = v;
-    z += v == 0;
+  // block-order image, one warp per block: element k of block b is row k / w,
+  // column k % w (w = 12 except a row's last block); the float quotient is
+  // exact here because (k + 0.5) / w stays >= 1/24 away from an integer
+  for (int b = warp; b < g.nb; b += STRIP_NT / 32) {
+    const int w = (b == g.nb - 1) ? g.wl : BS;
+    const float inv_w = 1.0f / (float)w;
+    const int nk = g.h * w;
+    uint16_t* dst = P.blocks + g.out0 + (long long)b * BS * g.h;
+    unsigned int z = 0;
+    for (int k = lane; k < nk; k += 32) {
+      const int li = (int)(((float)k + 0.5f) * inv_w);
+      const uint16_t v = t[li][b * BS + (k - li * w)];
+      dst[k] = v;
+      z += v == 0;
+    }
+    z = __reduce_add_sync(FULLM, z);
+    if (lane == 0) bz[b] = z;
   }
-#pragma unroll
-  for (int d = 16; d > 0; d >>= 1) z += __shfl_down_sync(0xffffffffu, z, d);
-  if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = z;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned int tot = 0;
-    for (int w = 0; w < STRIP_NT / 32; w++) tot += wsum[w];
-    strip_cnt[blockIdx.x] = tot;
+  if (warp == 0) {
+    const unsigned int v = lane < g.nb ? bz[lane] : 0u;
+    unsigned int inc = v;  // inclusive scan of the block counts
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const unsigned int y = __shfl_up_sync(FULLM, inc, d);
+      if (lane >= d) inc += y;
+    }
+    bpre[lane] = inc - v;
+    const unsigned long long tot = __shfl_sync(FULLM, inc, 31);
+    unsigned long long excl = 0;
+    if (s == 0) {
+      if (lane == 0) st_release64(&P.status[0], ST_PRE | tot);
+    } else {
+      if (lane == 0) st_release64(&P.status[s], ST_AGG | tot);
+      long long p = (long long)s - 1;
+      long long spins = 0;
+      for (;;) {
+        const long long q = p - lane;
+        const unsigned long long w = q >= 0 ? ld_acquire64(&P.status[q]) : ST_PRE;  // before strip 0: prefix 0
+        const unsigned int pre_m = __ballot_sync(FULLM, (w & ~ST_VAL) == ST_PRE);
+        const unsigned int none_m = __ballot_sync(FULLM, (w & ~ST_VAL) == 0);
+        const int last = pre_m ? __ffs(pre_m) - 1 : 31;  // the nearest prefix, or the whole window
+        const unsigned int upto = last == 31 ? FULLM : ((1u << (last + 1)) - 1u);
+        if (none_m & upto) {  // a nearer strip has not published yet
+          if (++spins > LOOKBACK_SPIN) {
+            if (lane == 0) atomicOr(flag, FLAG_TIMEOUT);
+            break;
+          }
+          __nanosleep(64);
+          continue;
+        }
+        unsigned long long add = lane <= last ? (w & ST_VAL) : 0ull;
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) add += __shfl_xor_sync(FULLM, add, d);
+        excl += add;
+        if (pre_m) break;
+        p -= 32;
+      }
+      if (lane == 0) st_release64(&P.status[s], ST_PRE | (excl + tot));
+    }
+    if (lane == 0) {
+      s_excl = excl;
+      if (s == ns - 1) ticket[1] = (unsigned int)(excl + tot);
+    }
   }
-}
-
-// Unpredictable values (code 0) of each strip in block order, at the strip's
-// offset (exclusive scan of the counts).  Strips without any return at once.
-__global__ void __launch_bounds__(STRIP_NT) gather_strip_kernel(const uint16_t* __restrict__ raster, long long pitch,
-                                                                const float* __restrict__ x, long long x_pitch,
-                                                                int r1, int r2, int nsc,
-                                                                const unsigned int* __restrict__ strip_off,
-                                                                float* __restrict__ unpred) {
-  __shared__ unsigned int wsum[STRIP_NT / 32];
-  const unsigned int base = strip_off[blockIdx.x];
-  if (strip_off[blockIdx.x + 1] == base) return;
-  const StripGeom g = strip_geom(blockIdx.x, r1, r2, nsc);
-  const int n = g.h * g.W;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  unsigned int run = base;
-  for (int o0 = 0; o0 < n; o0 += STRIP_NT) {
-    const int o = o0 + threadIdx.x;
-    int li = 0, col = 0;
-    bool z = false;
-    if (o < n) {
-      strip_rc(g, o, li, col);
-      z = raster[(long long)(g.bi * BS + li) * pitch + g.c0 + col] == 0;
+  __syncthreads();
+  // unpredictable values, in block order
+  const unsigned long long excl = s_excl;
+  for (int b = warp; b < g.nb; b += STRIP_NT / 32) {
+    if (bz[b] == 0) continue;
+    const int w = (b == g.nb - 1) ? g.wl : BS;
+    const float inv_w = 1.0f / (float)w;
+    const int nk = g.h * w;
+    unsigned long long run = excl + bpre[b];
+    for (int k0 = 0; k0 < nk; k0 += 32) {
+      const int k = k0 + lane;
+      int li = 0, col = 0;
+      bool z = false;
+      if (k < nk) {
+        li = (int)(((float)k + 0.5f) * inv_w);
+        col = b * BS + (k - li * w);
+        z = t[li][col] == 0;
+      }
+      const unsigned int m = __ballot_sync(FULLM, z);
+      if (z)
+        P.unpred[run + __popc(m & ((1u << lane) - 1u))] =
+            P.x[(long long)(g.bi * BS + li) * x_pitch + g.c0 + col];
+      run += __popc(m);
     }
-    const unsigned int m = __ballot_sync(0xffffffffu, z);
-    if (lane == 0) wsum[warp] = __popc(m);
-    __syncthreads();
-    unsigned int before = 0, tot = 0;
-    for (int w = 0; w < STRIP_NT / 32; w++) {
-      const unsigned int c = wsum[w];
-      before += (w < warp) ? c : 0u;
-      tot += c;
-    }
-    if (z) unpred[run + before + __popc(m & ((1u << lane) - 1u))] = x[(long long)(g.bi * BS + li) * x_pitch + g.c0 + col];
-    run += tot;
-    __syncthreads();
   }
 }
 
@@ -348,27 +410,28 @@ size_t strip_count(int r1, int r2) {
   return (size_t)(nbx * nsc);
 }
 
-int launch_r2b_strips(cpsz_b200_ctx* ctx, const uint16_t* raster, long long pitch, int r1, int r2, uint16_t* blocks,
-                      unsigned int* strip_cnt, unsigned int* strip_off, void* scan_tmp) {
+size_t strip_scratch_bytes(int r1, int r2) { return 8 * strip_count(r1, r2) + 8; }
+
+int launch_strip_pass(cpsz_b200_ctx* ctx, const uint16_t* const raster[2], long long pitch, const float* const x[2],
+                      long long x_pitch, int r1, int r2, uint16_t* const blocks[2], float* const unpred[2],
+                      void* const scratch[2]) {
   const size_t ns = strip_count(r1, r2);
   if (ns == 0) return CPSZ_OK;
   if (ns > 0x7fffffffu) return set_error(CPSZ_ERR_UNSUPPORTED, "field of %zu strips", ns);
   const int nsc = (r2 + STRIP_W - 1) / STRIP_W;
-  r2b_strip_kernel<<<(unsigned)ns, STRIP_NT, 0, ctx->stream>>>(raster, pitch, r1, r2, nsc, blocks, strip_cnt);
+  StripPass P[2];
+  for (int f = 0; f < 2; f++) {
+    CPSZ_CUDA_TRY(cudaMemsetAsync(scratch[f], 0, strip_scratch_bytes(r1, r2), ctx->stream));
+    P[f] = StripPass{raster[f], x[f], blocks[f], unpred[f], (unsigned long long*)scratch[f]};
+  }
+  strip_pass_kernel<<<dim3((unsigned)ns, 2), STRIP_NT, 0, ctx->stream>>>(P[0], P[1], pitch, x_pitch, r1, r2, nsc,
+                                                                         (unsigned)ns, ctx->d_flag);
   count_launch(ctx);
-  CPSZ_TRY(check_launch("r2b_strip_kernel"));
-  return launch_scan_u32(ctx, strip_cnt, strip_off, ns, scan_tmp);
+  return check_launch("strip_pass_kernel");
 }
 
-int launch_gather_strips(cpsz_b200_ctx* ctx, const uint16_t* raster, long long pitch, const float* x,
-                         long long x_pitch, int r1, int r2, const unsigned int* strip_off, float* unpred) {
-  const size_t ns = strip_count(r1, r2);
-  if (ns == 0) return CPSZ_OK;
-  const int nsc = (r2 + STRIP_W - 1) / STRIP_W;
-  gather_strip_kernel<<<(unsigned)ns, STRIP_NT, 0, ctx->stream>>>(raster, pitch, x, x_pitch, r1, r2, nsc, strip_off,
-                                                                  unpred);
-  count_launch(ctx);
-  return check_launch("gather_strip_kernel");
+const unsigned int* strip_total(const void* scratch, int r1, int r2) {
+  return (const unsigned int*)((const char*)scratch + 8 * strip_count(r1, r2) + 4);
 }
 
 int launch_segment_scan(cpsz_b200_ctx* ctx, const uint16_t* codes_raster, long long pitch, int r1, int r2,

@@ -98,18 +98,20 @@ int launch_raster_to_blocks_u16(cpsz_b200_ctx* ctx, const uint16_t* raster, long
 // raw flag bits = (code == 0)).
 int launch_blocks_to_raster_u16(cpsz_b200_ctx* ctx, const uint16_t* blocks, int r1, int r2, uint16_t* raster,
                                 long long pitch, const uint8_t* ids = nullptr, float2* pair = nullptr);
+// Compression side, one launch for both components of a field: codes raster
+// -> 12x12-block order and the unpredictable values (code 0) in block order,
+// in a single pass over strips (a 12-row block row cut into runs of 32
+// blocks) with a decoupled look-back for the unpredictables' offsets.
+// scratch[f]: strip_scratch_bytes(r1, r2) bytes (zeroed by the launch); after
+// it, *strip_total(scratch[f], ...) holds the component's unpredictable count.
+size_t strip_count(int r1, int r2);
+size_t strip_scratch_bytes(int r1, int r2);
+int launch_strip_pass(cpsz_b200_ctx* ctx, const uint16_t* const raster[2], long long pitch, const float* const x[2],
+                      long long x_pitch, int r1, int r2, uint16_t* const blocks[2], float* const unpred[2],
+                      void* const scratch[2]);
+const unsigned int* strip_total(const void* scratch, int r1, int r2);
 // Zero-code counts per row segment (one 12-wide block row) in block order,
 // exclusive-scanned into seg_off (size r1*nby+1; seg_off[r1*nby] = total).
-// Compression side, one pass per field: codes raster -> 12x12-block order plus
-// the unpredictable count of every strip (a 12-row block row cut into runs of
-// 32 blocks) and its exclusive scan strip_off[0..n] (strip_off[n] = total);
-// then the unpredictable values in block order.  Strip arrays hold
-// strip_count(r1, r2) + 1 entries (never more than the segment arrays).
-size_t strip_count(int r1, int r2);
-int launch_r2b_strips(cpsz_b200_ctx* ctx, const uint16_t* raster, long long pitch, int r1, int r2, uint16_t* blocks,
-                      unsigned int* strip_cnt, unsigned int* strip_off, void* scan_tmp);
-int launch_gather_strips(cpsz_b200_ctx* ctx, const uint16_t* raster, long long pitch, const float* x,
-                         long long x_pitch, int r1, int r2, const unsigned int* strip_off, float* unpred);
 int launch_segment_scan(cpsz_b200_ctx* ctx, const uint16_t* codes_raster, long long pitch, int r1, int r2,
                         unsigned int* seg_count, unsigned int* seg_off, void* scan_tmp);
 size_t segment_scan_tmp_bytes(int r1, int r2);

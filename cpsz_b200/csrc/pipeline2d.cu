@@ -62,9 +62,7 @@ struct DevBuf {
   unsigned long long* hist_codes[2];
   unsigned long long* gbnd;
   unsigned long long* band;  // per-group counters of finished eb2d vertices
-  unsigned int* seg_cnt[2];
-  unsigned int* seg_off[2];
-  void* scan_tmp[2];
+  void* strip[2];            // strip-pass look-back words and counters
   float* unpred[2];
   unsigned long long* enc_code[3];
   uint8_t* enc_len[3];
@@ -169,8 +167,7 @@ size_t job_bytes(const Job2D& j) {
   add(2 * 65536 * 8);                   // hist codes
   add(2 * (size_t)j.ngroups * j.r2 * 8);  // boundary rows (tagged words)
   add((size_t)j.ngroups * 8);             // eb2d group counters
-  add(2 * 2 * (j.nseg + 1) * 4);
-  add(2 * segment_scan_tmp_bytes(j.r1, j.r2));
+  add(2 * strip_scratch_bytes(j.r1, j.r2));
   add(2 * 4 * N);  // unpred
   add(256 * 9);
   add(2 * 65536 * 9);
@@ -204,9 +201,7 @@ int job_alloc(cpsz_b200_ctx* ctx, Job2D& j) {
   d.gbnd = (unsigned long long*)A(2 * (size_t)j.ngroups * j.r2 * 8);
   d.band = (unsigned long long*)A((size_t)j.ngroups * 8);
   for (int f = 0; f < 2; f++) {
-    d.seg_cnt[f] = (unsigned int*)A((j.nseg + 1) * 4);
-    d.seg_off[f] = (unsigned int*)A((j.nseg + 1) * 4);
-    d.scan_tmp[f] = A(segment_scan_tmp_bytes(j.r1, j.r2));
+    d.strip[f] = A(strip_scratch_bytes(j.r1, j.r2));
     d.unpred[f] = (float*)A(4 * N);
   }
   d.enc_code[0] = (unsigned long long*)A(256 * 8);
@@ -473,14 +468,11 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   }
   for (int k = 0; k < nj; k++) {
     Job2D& j = jobs[k];
-    for (int f = 0; f < 2; f++) {
-      CPSZ_TRY(launch_r2b_strips(ctx, j.d.craster[f], j.r2, j.r1, j.r2, j.d.cblocks[f], j.d.seg_cnt[f],
-                                 j.d.seg_off[f], j.d.scan_tmp[f]));
-      CPSZ_TRY(launch_gather_strips(ctx, j.d.craster[f], j.r2, f ? j.d.V : j.d.U, j.r2, j.r1, j.r2, j.d.seg_off[f],
-                                    j.d.unpred[f]));
-      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_nunpred + f, j.d.seg_off[f] + strip_count(j.r1, j.r2), 4,
+    const float* x[2] = {j.d.U, j.d.V};
+    CPSZ_TRY(launch_strip_pass(ctx, j.d.craster, j.r2, x, j.r2, j.r1, j.r2, j.d.cblocks, j.d.unpred, j.d.strip));
+    for (int f = 0; f < 2; f++)
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_nunpred + f, strip_total(j.d.strip[f], j.r1, j.r2), 4,
                                     cudaMemcpyDeviceToHost, st));
-    }
   }
   mark(ctx, "host_trees");
 
