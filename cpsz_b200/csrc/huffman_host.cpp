@@ -12,6 +12,7 @@
 // convert_HuffTree_to_bytes_anyStates, :357-499).
 #include "huffman_host.h"
 
+#include <algorithm>
 #include <cstring>
 
 #include "kernels.h"
@@ -71,10 +72,10 @@ class Heap {
 
 // Per-thread scratch reused by every build on the thread.
 struct Scratch {
-  std::vector<uint32_t> leaf_sym, L, R, C;
-  std::vector<uint8_t> T;
-  std::vector<int> kids;
-  std::vector<unsigned long long> heap;
+  std::vector<uint32_t> leaf_sym, L, R, C, size, pre;
+  std::vector<uint8_t> T, leaf_len;
+  std::vector<int> kids, depth;
+  std::vector<unsigned long long> heap, leaf_freq, leaf_code, ncode;
 };
 Scratch& scratch() {
   static thread_local Scratch s;
@@ -101,9 +102,14 @@ bool huff_build(const unsigned long long* hist, size_t bins, size_t state_num, H
   // the merge loop and the walk stay cache-resident.
   Scratch& sc = scratch();
   std::vector<uint32_t>& leaf_sym = sc.leaf_sym;
+  std::vector<unsigned long long>& leaf_freq = sc.leaf_freq;
   leaf_sym.clear();
+  leaf_freq.clear();
   for (size_t s = 0; s < bins; s++)
-    if (hist[s]) leaf_sym.push_back((uint32_t)s);
+    if (hist[s]) {
+      leaf_sym.push_back((uint32_t)s);
+      leaf_freq.push_back(hist[s]);
+    }
   const size_t distinct = leaf_sym.size();
   if (distinct == 0) {
     set_error(CPSZ_ERR_INVALID, "Huffman: empty histogram");
@@ -112,7 +118,7 @@ bool huff_build(const unsigned long long* hist, size_t bins, size_t state_num, H
   std::vector<int>& kids = sc.kids;  // (left, right) of merged node distinct + m
   if (kids.size() < 2 * distinct) kids.resize(2 * distinct);
   Heap heap(sc.heap, 2 * distinct);
-  for (size_t d = 0; d < distinct; d++) heap.insert(hist[leaf_sym[d]], (int)d);
+  for (size_t d = 0; d < distinct; d++) heap.insert(leaf_freq[d], (int)d);
   int next_node = (int)distinct;
   while (heap.size() > 1) {
     // new_node(0, 0, qremove(), qremove()): the first removal becomes the
@@ -125,63 +131,81 @@ bool huff_build(const unsigned long long* hist, size_t bins, size_t state_num, H
     heap.insert((second >> Heap::kShift) + (first >> Heap::kShift), next_node++);
   }
   const int root = heap.top();
-  out->code.assign(bins, 0);
-  out->len.assign(bins, 0);
   out->distinct = distinct;
   out->max_len = 0;
   out->total_bits = 0;
-  size_t node_count = 0;
-  for (size_t s = 0; s < state_num && s < bins; s++)
-    if (hist[s]) node_count++;
-  node_count = node_count * 2 - 1;
+  // leaves are in symbol order: those below state_num are a prefix
+  const size_t below = (size_t)(std::lower_bound(leaf_sym.begin(), leaf_sym.end(), (uint32_t)std::min(state_num, bins)) -
+                                leaf_sym.begin());
+  const size_t node_count = below * 2 - 1;
   const size_t nn = (size_t)next_node;
   if (node_count != nn) {
     set_error(CPSZ_ERR_UNSUPPORTED, "Huffman: symbols beyond state_num");
     return false;
   }
-  // One pre-order walk: codes (left 0 / right 1, build_code) and the
-  // serialization's node numbering (pad_tree_*: a node's number is its
-  // pre-order position; L/R hold the children's numbers).
+  // Codes (left 0 / right 1, build_code) and the serialization's node
+  // numbering (pad_tree_*: a node's number is its pre-order position; L/R
+  // hold the children's numbers), without walking the tree: a merged node is
+  // created after both its children, so subtree sizes follow in creation
+  // order, and pre-order numbers, depths and codes in reverse creation order
+  // (pre(left) = pre(node) + 1, pre(right) = pre(node) + 1 + size(left)).
+  // Each pass reads the merge list sequentially; no load depends on the last.
   std::vector<uint32_t>&L = sc.L, &R = sc.R, &C = sc.C;
   std::vector<uint8_t>& T = sc.T;
+  std::vector<unsigned long long>& leaf_code = sc.leaf_code;
+  std::vector<uint8_t>& leaf_len = sc.leaf_len;
+  std::vector<uint32_t>&size = sc.size, &pre = sc.pre;
+  std::vector<unsigned long long>& ncode = sc.ncode;
+  std::vector<int>& depth = sc.depth;
   L.assign(nn, 0);
   R.assign(nn, 0);
   C.assign(nn, 0);
   T.assign(nn, 0);
-  struct Frame {
-    int node, parent, side, depth;
-    unsigned long long bits;
-  };
-  std::vector<Frame> st;
-  st.reserve(160);
-  st.push_back(Frame{root, -1, 0, 0, 0ull});
-  uint32_t next = 0;
-  while (!st.empty()) {
-    const Frame f = st.back();
-    st.pop_back();
-    const uint32_t i = next++;
-    if (f.parent >= 0) (f.side ? R : L)[f.parent] = i;
-    if (f.node < (int)distinct) {
-      const uint32_t c = leaf_sym[f.node];
-      C[i] = c;
-      T[i] = 1;
-      if (f.depth > 64) {
-        set_error(CPSZ_ERR_UNSUPPORTED, "Huffman code longer than 64 bits");
-        return false;
-      }
-      out->code[c] = f.bits;
-      out->len[c] = (uint8_t)f.depth;
-      if (f.depth > out->max_len) out->max_len = f.depth;
-      out->total_bits += hist[c] * (unsigned long long)f.depth;
-      continue;
-    }
-    if (f.depth >= 64) {
-      set_error(CPSZ_ERR_UNSUPPORTED, "Huffman code longer than 64 bits");
-      return false;
-    }
-    const int m = f.node - (int)distinct;
-    st.push_back(Frame{kids[2 * m + 1], (int)i, 1, f.depth + 1, (f.bits << 1) | 1ull});
-    st.push_back(Frame{kids[2 * m], (int)i, 0, f.depth + 1, f.bits << 1});
+  size.resize(nn);
+  pre.resize(nn);
+  ncode.resize(nn);
+  depth.resize(nn);
+  leaf_code.resize(distinct);
+  leaf_len.resize(distinct);
+  const size_t nm = nn - distinct;
+  for (size_t d = 0; d < distinct; d++) size[d] = 1;
+  for (size_t m = 0; m < nm; m++) size[distinct + m] = size[kids[2 * m]] + size[kids[2 * m + 1]] + 1;
+  pre[root] = 0;
+  depth[root] = 0;
+  ncode[root] = 0;
+  int deepest = 0;
+  for (size_t m = nm; m-- > 0;) {
+    const size_t node = distinct + m;
+    const int l = kids[2 * m], r = kids[2 * m + 1];
+    const uint32_t p = pre[node];
+    const int dc = depth[node] + 1;
+    pre[l] = p + 1;
+    pre[r] = p + 1 + size[l];
+    depth[l] = depth[r] = dc;
+    ncode[l] = ncode[node] << 1;
+    ncode[r] = (ncode[node] << 1) | 1ull;
+    L[p] = p + 1;
+    R[p] = p + 1 + size[l];
+    deepest = dc > deepest ? dc : deepest;
+  }
+  if (deepest > 64) {
+    set_error(CPSZ_ERR_UNSUPPORTED, "Huffman code longer than 64 bits");
+    return false;
+  }
+  for (size_t d = 0; d < distinct; d++) {
+    const uint32_t i = pre[d];
+    C[i] = leaf_sym[d];
+    T[i] = 1;
+    leaf_code[d] = ncode[d];
+    leaf_len[d] = (uint8_t)depth[d];
+    out->total_bits += leaf_freq[d] * (unsigned long long)depth[d];
+  }
+  out->max_len = deepest;
+  out->code.assign(bins, 0);
+  out->len.assign(bins, 0);
+  for (size_t d = 0; d < distinct; d++) {
+    out->code[leaf_sym[d]] = leaf_code[d];
+    out->len[leaf_sym[d]] = leaf_len[d];
   }
   const size_t tsz = tree_size_for(node_count);
   out->tree_bytes.assign(8 + 4 + tsz, 0);
