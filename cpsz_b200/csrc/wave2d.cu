@@ -25,13 +25,20 @@
 //    row pitch makes the per-step accesses tile[l][t] bank-conflict free.
 //    Points outside the field are staged as pairs that reconstruct to 0, so a
 //    step has no bounds branches;
-//  * a CTA owns a WAVE_GROUP_ROWS-row group (WAVE_WARPS warps; 128 rows, 4
-//    warps: one warp per scheduler).  Warp w takes the row above from
-//    warp w-1 through a shared-memory ring of tagged words, 8 columns at a
-//    time (one warp-uniform tag test per 8 steps); lane 31 stores one tagged
-//    word per step.  The CTA's first warp takes the previous group's last row
-//    from global memory, a whole 32-column window at a time, validated once
-//    per window and loaded coalesced one window ahead;
+//  * the staging and draining run in a helper warp paired with each compute
+//    warp (same scheduler; a named barrier per window), so the compute warp's
+//    instruction stream holds only the recurrence, and the helper's
+//    instructions issue in the compute warp's dependency stalls;
+//  * a step has no branches: the hand-off below and the test tap are single
+//    predicated stores, and the tap is a template parameter (a branch in the
+//    step splits it into basic blocks the compiler cannot overlap);
+//  * a CTA owns a WAVE_GROUP_ROWS-row group (WAVE_WARPS compute warps; 128
+//    rows, 4 warps: one per scheduler, plus their helpers).  Warp w takes the
+//    row above from warp w-1 through a shared-memory ring of tagged words, 8
+//    columns at a time (one warp-uniform tag test per 8 steps); lane 31
+//    stores one tagged word per step.  The CTA's first warp takes the previous
+//    group's last row from global memory, a whole 32-column window at a time,
+//    validated once per window and loaded coalesced one window ahead;
 //  * CTAs are persistent and pull (field, group) items from a device work
 //    queue (atomic counter).  An item's predecessor (same field, previous
 //    group) was dequeued earlier by a running CTA, so every wait ends;
@@ -52,7 +59,9 @@
 //   y = |x - pred| / p = |x - pred| * (1/p) is exact in float, and the
 //   reference's capacity test |diff|/p + 1 < 65536 is y < 65535 (y + 1 is
 //   exact in double below 2^16);
-//   (int)((|diff|/p + 1) / 2) = (trunc(y) + 1) >> 1;
+//   (int)((|diff|/p + 1) / 2) = (trunc(y) + 1) >> 1 = floor(y/2 + 1/2), taken
+//   without a conversion: y/2 + 1/2 rounded down keeps its floor, and that
+//   plus 2^23 rounded down is 2^23 + floor exactly;
 //   the reference's (float)((double)pred + (double)(2q) * p) equals the float
 //   sum pred + 2q*p: 2q*p is exact in float (|2q| < 2^17), and whenever the
 //   exact sum does not fit a double one addend lies below 2^-5 ulp of the
@@ -74,10 +83,6 @@ constexpr int TILE = 32 * TP;  // elements per tile
 constexpr long long SPIN_LIMIT = 1ll << 22;
 constexpr long long BAND_WAIT_NS = 4000000000ll;  // producer wait limit (4 s)
 
-// exact float of an integer |n| < 2^22 without the conversion unit
-__device__ __forceinline__ float small_int_to_float(int n) {
-  return __int_as_float(0x4B400000 + n) - 12582912.0f;
-}
 __device__ __forceinline__ unsigned long long tagged(int c, float v) {
   return ((unsigned long long)(unsigned)(c + 1) << 32) | (unsigned long long)__float_as_uint(v);
 }
@@ -100,6 +105,19 @@ __device__ __forceinline__ unsigned long long ld_acquire(const unsigned long lon
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+// Named barrier of one compute warp and its helper warp (ids 1..WAVE_WARPS).
+__device__ __forceinline__ void pair_sync(int strip) { asm volatile("bar.sync %0, 64;" ::"r"(1 + strip) : "memory"); }
+// Stores that only some lanes perform, as single predicated instructions: the
+// per-step hand-off then never splits the warp into divergent paths.
+__device__ __forceinline__ void st_u64_if(bool p, void* addr, unsigned long long v) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %0, 0;\n\t@q st.volatile.u64 [%1], %2;\n\t}" ::"r"((unsigned)p),
+               "l"(addr), "l"(v));
+}
+__device__ __forceinline__ void st_global_f32_if(bool p, void* g, float v) {
+  asm volatile("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %0, 0;\n\t@q st.global.f32 [%1], %2;\n\t}" ::"r"((unsigned)p),
+               "l"(g), "f"(v)
+               : "memory");
+}
 
 struct WarpTiles {
   float2 in[2][TILE];
@@ -113,8 +131,60 @@ struct Shared {
 };
 
 constexpr size_t kDynSmem = sizeof(WarpTiles) * WAVE_WARPS;
+constexpr int WAVE_THREADS = 2 * WAVE_WARPS * 32;  // compute warps, then one helper warp each
+
+// ---- helper warp: stages window k of its strip and writes window k-2's outputs ----
+// stage window k: row l, columns [32k - l, 32k - l + 32); lane t takes column t
+template <bool DECOMP>
+__device__ __forceinline__ void tile_fill(const WaveField& F, WarpTiles& T, long long row0, int nrows, int lane,
+                                          int k, int buf) {
+  // staged pair of a point outside the field: reconstructs to 0
+  const float2 pad = DECOMP ? make_float2(0.f, __int_as_float(1)) : make_float2(0.f, __int_as_float(0x7FC00000));
+  const float2* rp = F.pair + row0 * F.pair_pitch;
+  int c = 32 * k + lane;
+  float2* d = &T.in[buf][lane];
+#pragma unroll 4
+  for (int l = 0; l < 32; l++, c--, d += TP, rp += F.pair_pitch) {
+    if (l < nrows && (unsigned)c < (unsigned)F.r2) cp_async8(d, rp + c);
+    else *d = pad;
+  }
+  cp_commit();
+}
+// write window k's outputs: row l, columns [32k - l, 32k - l + 32)
+template <bool DECOMP>
+__device__ __forceinline__ void tile_drain(const WaveField& F, const WarpTiles& T, long long row0, int nrows, int lane,
+                                           int k, int buf) {
+  int c = 32 * k + lane;
+  const uint32_t* s = &T.out[buf][lane];
+  long long r = row0;
+  for (int l = 0; l < nrows; l++, c--, s += TP, r++) {
+    if ((unsigned)c < (unsigned)F.r2) {
+      const uint32_t v = *s;
+      if (DECOMP) F.out[r * F.out_pitch + c] = __uint_as_float(v);
+      else F.codes[r * F.code_pitch + c] = (uint16_t)v;
+    }
+  }
+}
 
 template <bool DECOMP>
+__device__ __forceinline__ void run_helper(const WaveField& F, int group, int strip, int lane, WarpTiles& T) {
+  const long long row0 = (long long)group * WAVE_GROUP_ROWS + strip * 32;
+  const int nrows = min(32, F.r1 - (int)row0);
+  const int nwin = (F.r2 + 31 + 31) / 32;  // windows that contain any step
+  tile_fill<DECOMP>(F, T, row0, nrows, lane, 0, 0);
+  cp_wait_all();
+  for (int k = 0; k < nwin; k++) {
+    pair_sync(strip);  // the compute warp starts window k (tiles buf = k & 1)
+    if (k + 1 < nwin) tile_fill<DECOMP>(F, T, row0, nrows, lane, k + 1, (k + 1) & 1);
+    if (k >= 1) tile_drain<DECOMP>(F, T, row0, nrows, lane, k - 1, (k - 1) & 1);
+    cp_wait_all();
+  }
+  pair_sync(strip);  // the compute warp has finished the last window
+  tile_drain<DECOMP>(F, T, row0, nrows, lane, nwin - 1, (nwin - 1) & 1);
+}
+
+// ---- compute warp: the recurrence over its 32 rows ----
+template <bool DECOMP, bool TAP>
 __device__ __forceinline__ void run_strip(const WaveField& F, int group, int warp, int lane, Shared& sh,
                                           WarpTiles& T, int* flag) {
   const int r1 = F.r1, r2 = F.r2;
@@ -128,8 +198,6 @@ __device__ __forceinline__ void run_strip(const WaveField& F, int group, int war
   const bool below_ring = has_below && !below_global;
   const unsigned long long* gb_in = above_global ? F.gbnd + (size_t)(group - 1) * r2 : nullptr;
   unsigned long long* gb_out = F.gbnd + (size_t)group * r2;
-  // staged pair of a point outside the field: reconstructs to 0
-  const float2 pad = DECOMP ? make_float2(0.f, __int_as_float(1)) : make_float2(0.f, __int_as_float(0x7FC00000));
 
   int credit = RING;  // ring columns this warp may write before re-reading its consumer's progress
   bool aborted = false;
@@ -137,33 +205,6 @@ __device__ __forceinline__ void run_strip(const WaveField& F, int group, int war
   const long long t_start = F.trace ? globaltimer_ns() : 0;
   float outPrev = 0.f, upPrev = 0.f;
   const int nwin = (r2 + 31 + 31) / 32;  // windows that contain any step
-  const float2* rows_in = F.pair + (long long)row0 * F.pair_pitch;
-
-  // stage window k: row l, columns [32k - l, 32k - l + 32); lane t takes column t
-  auto fill = [&](int k, int buf) {
-    const float2* rp = rows_in;
-    int c = 32 * k + lane;
-    float2* d = &T.in[buf][lane];
-#pragma unroll 4
-    for (int l = 0; l < 32; l++, c--, d += TP, rp += F.pair_pitch) {
-      if (l < nrows && (unsigned)c < (unsigned)r2) cp_async8(d, rp + c);
-      else *d = pad;
-    }
-    cp_commit();
-  };
-  // write window k's outputs: row l, columns [32k - l, 32k - l + 32)
-  auto drain = [&](int k, int buf) {
-    int c = 32 * k + lane;
-    const uint32_t* s = &T.out[buf][lane];
-    long long r = row0;
-    for (int l = 0; l < nrows; l++, c--, s += TP, r++) {
-      if ((unsigned)c < (unsigned)r2) {
-        const uint32_t v = *s;
-        if (DECOMP) F.out[r * F.out_pitch + c] = __uint_as_float(v);
-        else F.codes[r * F.code_pitch + c] = (uint16_t)v;
-      }
-    }
-  };
   auto ring_word = [&](int c) -> unsigned long long {
     return *(volatile unsigned long long*)&sh.ring[warp - 1][c & (RING - 1)];
   };
@@ -174,14 +215,10 @@ __device__ __forceinline__ void run_strip(const WaveField& F, int group, int war
     return (c < r2) ? __ldcg(gb_in + c) : 0ull;
   };
 
-  fill(0, 0);
   if (above_global) gnext = gload(0);
   for (int k = 0; k < nwin; k++) {
     const int buf = k & 1;
-    cp_wait_all();
-    __syncwarp();
-    if (k + 1 < nwin) fill(k + 1, buf ^ 1);
-    if (k >= 1) drain(k - 1, buf ^ 1);
+    pair_sync(warp);  // window k is staged; window k-1's outputs are handed to the helper
     if (above_global) {
       // the whole window of the row above must be present: one poll per window
       gcur = gnext;
@@ -203,7 +240,6 @@ __device__ __forceinline__ void run_strip(const WaveField& F, int group, int war
       spin_above += spins;
       gnext = gload(k + 1);
     }
-    __syncwarp();
     const float2* tin = &T.in[buf][lane * TP];
     uint32_t* to = &T.out[buf][lane * TP];
 #pragma unroll 1
@@ -246,6 +282,10 @@ __device__ __forceinline__ void run_strip(const WaveField& F, int group, int war
 #pragma unroll
         for (int j = 0; j < 8; j++) ab[j] = 0.f;
       }
+      if (aborted) {
+#pragma unroll
+        for (int j = 0; j < 8; j++) ab[j] = 0.f;
+      }
       // ---- ring credit for the 8 columns lane 31 writes in this block ----
       if (below_ring) {
         const int cmax = cb - 24;
@@ -269,7 +309,7 @@ __device__ __forceinline__ void run_strip(const WaveField& F, int group, int war
       for (int j = 0; j < 8; j++) {
         const int t = tb + j;
         const float shfl = __shfl_up_sync(FULL, outPrev, 1);
-        const float U = (lane == 0) ? (aborted ? 0.f : ab[j]) : shfl;
+        const float U = (lane == 0) ? ab[j] : shfl;
         const float pred = (outPrev + U) - upPrev;
         const float2 e = tin[t];
         float out;
@@ -280,32 +320,35 @@ __device__ __forceinline__ void run_strip(const WaveField& F, int group, int war
           const float x = e.x, inv = e.y;  // inv = 1/p (NaN for precision 0)
           const float p = __int_as_float(0x7F000000 - __float_as_int(inv));
           const float diff = x - pred;
-          const float y = fabsf(diff) * inv;
-          const int qa = ((int)fminf(y, 65536.0f) + 1) >> 1;
-          const int q = (diff > 0.f) ? qa : -qa;
-          const float dec = pred + small_int_to_float(2 * q) * p;
-          const bool ok = (y < 65535.0f) & (fabsf(dec - x) <= p);
+          // q = (trunc(y) + 1) >> 1 = floor(y/2 + 1/2) for y = |diff|/p >= 0.
+          // y/2 = |diff| * (inv/2) is exact; rounding y/2 + 1/2 down keeps
+          // its floor, and rounding that plus 2^23 down yields 2^23 + floor
+          // exactly (for y >= 2^24 the point is unpredictable anyway).
+          const float h = fabsf(diff) * (0.5f * inv);
+          const float mq = __fadd_rd(__fadd_rd(h, 0.5f), 8388608.0f);
+          const float qf = mq - 8388608.0f;
+          // 0 - qf keeps q = 0 a +0 addend (as the decoder's 2(code - 32768) * p is)
+          const float dec = pred + ((diff > 0.f) ? qf : 0.f - qf) * (p + p);
+          const bool ok = (h < 32767.5f) & (fabsf(dec - x) <= p);
           out = ok ? dec : x;
-          to[t] = ok ? (uint32_t)(q + 32768) : 0u;
-          if (F.out) {  // optional reconstruction tap (tests)
+          const int qa = __float_as_int(mq) - 0x4B000000;
+          to[t] = ok ? (uint32_t)(((diff > 0.f) ? qa : -qa) + 32768) : 0u;
+          if (TAP) {  // optional reconstruction tap (tests)
             const int c = cb + j - lane;
-            if (lane < nrows && (unsigned)c < (unsigned)r2) F.out[(long long)(row0 + lane) * F.out_pitch + c] = out;
+            st_global_f32_if((lane < nrows) & ((unsigned)c < (unsigned)r2),
+                             F.out + (long long)(row0 + lane) * F.out_pitch + c, out);
           }
         }
         // lane 31 hands its row down (column cb + j - 31)
         const int c31 = cb + j - 31;
-        if (lane == 31 && (unsigned)c31 < (unsigned)r2) {
-          if (below_ring) *(volatile unsigned long long*)&sh.ring[warp][c31 & (RING - 1)] = tagged(c31, out);
-          else if (below_global) __stcg(gb_out + c31, tagged(c31, out));
-        }
+        const bool w31 = (lane == 31) & ((unsigned)c31 < (unsigned)r2) & has_below;
+        st_u64_if(w31, below_ring ? (void*)&sh.ring[warp][c31 & (RING - 1)] : (void*)(gb_out + c31), tagged(c31, out));
         upPrev = U;
         outPrev = out;
       }
     }
   }
-  cp_wait_all();
-  __syncwarp();
-  drain(nwin - 1, (nwin - 1) & 1);
+  pair_sync(warp);  // the last window's outputs go to the helper
   if (lane == 0 && above_ring) sh.cons[warp] = r2 + RING;
   if (F.trace && lane == 0) {
     long long* tr = F.trace + ((long long)group * WAVE_WARPS + warp) * 4;
@@ -317,13 +360,14 @@ __device__ __forceinline__ void run_strip(const WaveField& F, int group, int war
 }
 
 template <bool DECOMP>
-__global__ void __launch_bounds__(WAVE_WARPS * 32, 1) wave2d_kernel(const WaveField* __restrict__ fields,
-                                                                    const WaveItem* __restrict__ items, int n_items,
-                                                                    int* queue, int* flag) {
+__global__ void __launch_bounds__(WAVE_THREADS, 1) wave2d_kernel(const WaveField* __restrict__ fields,
+                                                                 const WaveItem* __restrict__ items, int n_items,
+                                                                 int* queue, int* flag) {
   __shared__ Shared sh;
   extern __shared__ __align__(16) unsigned char dyn[];
   WarpTiles* tiles = reinterpret_cast<WarpTiles*>(dyn);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int strip = warp % WAVE_WARPS;  // the strip a compute warp runs, or its helper serves
   for (;;) {
     if (threadIdx.x == 0) sh.item = atomicAdd(queue, 1);
     for (int k = threadIdx.x; k < WAVE_WARPS * RING; k += blockDim.x) (&sh.ring[0][0])[k] = 0ull;
@@ -354,8 +398,13 @@ __global__ void __launch_bounds__(WAVE_WARPS * 32, 1) wave2d_kernel(const WaveFi
       __syncthreads();
       (void)ld_acquire(cnt);
     }
-    if (item.group * WAVE_GROUP_ROWS + warp * 32 < F.r1)
-      run_strip<DECOMP>(F, item.group, warp, lane, sh, tiles[warp], flag);
+    if (item.group * WAVE_GROUP_ROWS + strip * 32 < F.r1) {
+      if (warp < WAVE_WARPS) {
+        if (!DECOMP && F.out) run_strip<DECOMP, true>(F, item.group, strip, lane, sh, tiles[strip], flag);
+        else run_strip<DECOMP, false>(F, item.group, strip, lane, sh, tiles[strip], flag);
+      }
+      else run_helper<DECOMP>(F, item.group, strip, lane, tiles[strip]);
+    }
     __syncthreads();
   }
 }
@@ -376,9 +425,9 @@ int launch_wave2d(cpsz_b200_ctx* ctx, bool decompress, const WaveField* d_fields
   }
   int per_sm = 0;
   if (decompress)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wave2d_kernel<true>, WAVE_WARPS * 32, kDynSmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wave2d_kernel<true>, WAVE_THREADS, kDynSmem);
   else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wave2d_kernel<false>, WAVE_WARPS * 32, kDynSmem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wave2d_kernel<false>, WAVE_THREADS, kDynSmem);
   if (per_sm < 1) return set_error(CPSZ_ERR_CUDA, "wave2d kernel does not fit on an SM");
   const int cap = tune_get(TUNE_WAVE2D_CTAS_PER_SM, points);
   if (cap > 0 && per_sm > cap) per_sm = cap;
@@ -389,10 +438,10 @@ int launch_wave2d(cpsz_b200_ctx* ctx, bool decompress, const WaveField* d_fields
   if (grid > n_items) grid = n_items;
   if (grid < 1) return CPSZ_OK;
   if (decompress)
-    wave2d_kernel<true><<<grid, WAVE_WARPS * 32, kDynSmem, stream>>>(d_fields, d_items, n_items, d_queue,
+    wave2d_kernel<true><<<grid, WAVE_THREADS, kDynSmem, stream>>>(d_fields, d_items, n_items, d_queue,
                                                                      ctx->d_flag);
   else
-    wave2d_kernel<false><<<grid, WAVE_WARPS * 32, kDynSmem, stream>>>(d_fields, d_items, n_items, d_queue,
+    wave2d_kernel<false><<<grid, WAVE_THREADS, kDynSmem, stream>>>(d_fields, d_items, n_items, d_queue,
                                                                       ctx->d_flag);
   count_launch(ctx);
   return check_launch("wave2d_kernel");
