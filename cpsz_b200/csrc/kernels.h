@@ -85,6 +85,8 @@ constexpr int WAVE_GROUP_ROWS = WAVE_WARPS * 32;
 // Every dequeued item belongs to a resident CTA, whichever launch it is in, so
 // the waits between items of one field end in every mode.
 enum WaveMode { WAVE_ALONE = 0, WAVE_BESIDE = 1, WAVE_JOIN = 2 };
+// Loads every wavefront kernel (call before a WAVE_BESIDE launch).
+int preload_wave2d();
 int launch_wave2d(cpsz_b200_ctx* ctx, bool decompress, const WaveField* d_fields, const WaveItem* d_items,
                   int n_items, int* d_queue, size_t points, cudaStream_t stream = nullptr, int mode = WAVE_ALONE);
 

@@ -381,6 +381,7 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   } hi_drain;
   if (overlap) {
     CPSZ_TRY(preload_eb2d());
+    CPSZ_TRY(preload_wave2d());
     hi_drain.s = ctx->hi;
     CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[3], st));
     CPSZ_CUDA_TRY(cudaStreamWaitEvent(ctx->hi, ctx->ev[3], 0));
