@@ -398,15 +398,17 @@ def libm_tables_prepare(path: str | None = None) -> None:
     _check(lib().cpsz_b200_libm_tables_prepare(path.encode() if path else None))
 
 
-def debug_eb2d(U, V, max_pwr_eb: float, ctx: Context | None = None):
-    """Per-vertex 2D analytic bound (float64) and id bytes (2N; 255 = precision 0) from the GPU kernel."""
+def debug_eb2d(U, V, max_pwr_eb: float, ctx: Context | None = None, exact: bool = True):
+    """Per-vertex 2D analytic bound (float64) and id bytes (2N; 255 = precision 0) from the GPU kernel.
+
+    exact=False runs the compressor's filtered path and returns (None, ids)."""
     U = np.ascontiguousarray(U, np.float32)
     V = np.ascontiguousarray(V, np.float32)
     r1, r2 = U.shape
-    eb = np.empty(U.shape, np.float64)
+    eb = np.empty(U.shape, np.float64) if exact else None
     ids = np.empty(2 * U.size, np.uint8)
     _check(lib().cpsz_b200_debug_eb2d(_h(ctx), U.ctypes.data, V.ctypes.data, r1, r2, float(max_pwr_eb),
-                                      eb.ctypes.data, ids.ctypes.data))
+                                      eb.ctypes.data if exact else None, ids.ctypes.data))
     return eb, ids
 
 

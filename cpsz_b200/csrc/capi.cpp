@@ -153,7 +153,7 @@ int cpsz_b200_debug_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, siz
   unsigned long long* dh = nullptr;
   CPSZ_CUDA_TRY(cudaMalloc((void**)&dU, 4 * N));
   CPSZ_CUDA_TRY(cudaMalloc((void**)&dV, 4 * N));
-  CPSZ_CUDA_TRY(cudaMalloc((void**)&deb, 8 * N));
+  if (eb_out) CPSZ_CUDA_TRY(cudaMalloc((void**)&deb, 8 * N));
   CPSZ_CUDA_TRY(cudaMalloc((void**)&dids, 2 * N));
   CPSZ_CUDA_TRY(cudaMalloc((void**)&dtab, QUANT_TAB_MAX * 8));
   CPSZ_CUDA_TRY(cudaMalloc((void**)&dh, 256 * 8));

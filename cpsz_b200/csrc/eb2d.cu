@@ -24,8 +24,10 @@
 
 namespace cpsz {
 
-template <int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT) eb2d_kernel(const float* __restrict__ U, const float* __restrict__ V, int r1,
+// 64 registers a thread at most (2048 threads an SM): with the wavefront
+// beside it, three 256-thread CTAs of this kernel still fit on an SM.
+template <int TX, int TY, int NT, bool FAST>
+__global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const float* __restrict__ U, const float* __restrict__ V, int r1,
                                                   int r2, double max_pwr_eb, const double* __restrict__ thr_tab,
                                                   int thr_n, uint8_t* __restrict__ ids_u, uint8_t* __restrict__ ids_v,
                                                   unsigned long long* __restrict__ hist, int* __restrict__ flag,
@@ -73,54 +75,99 @@ __global__ void __launch_bounds__(NT) eb2d_kernel(const float* __restrict__ U, c
       // One call site keeps a single copy of the bound code in the
       // instruction cache.
       const int a1 = a + (kind == 0), b1 = b + (kind == 1);
-      e = dev::tri_eb(su[a][b], su[a1][b1], su[a + 1][b + 1], sv[a][b], sv[a1][b1], sv[a + 1][b + 1], kind);
+      if (FAST)
+        e = dev::tri_eb_filtered(su[a][b], su[a1][b1], su[a + 1][b + 1], sv[a][b], sv[a1][b1], sv[a + 1][b + 1],
+                                 kind);
+      else
+        e = dev::tri_eb(su[a][b], su[a1][b1], su[a + 1][b + 1], sv[a][b], sv[a1][b1], sv[a + 1][b + 1], kind);
     }
     tri[kind][a][b] = e;
   }
   __syncthreads();
   const double thr = tab[0];
+  // id of a quantized bound e (-1 for precision 0), before the range check
+  auto quant = [&](double e) -> int {
+    if (e <= thr) return -1;
+    const int ex = (int)((__double_as_longlong(e) >> 52) & 0x7ff) - 1023;
+    return dev::count_thresholds(tab, thr_n, e, (ex + 52) >> 1);
+  };
   for (int k = tid; k < TY * TX; k += NT) {
     int a = k / TX, b = k % TX;
     int gi = i0 + a, gj = j0 + b;
     if (gi >= row_end || gj >= r2) continue;
     // vertex (gi, gj) is local (a+1, b+1); cell (gi-1+x, gj-1+y) is tri[.][a+x][b+y]
-    double eb = max_pwr_eb;
     bool up = gi >= 1, left = gj >= 1, down = gi < r1 - 1, right = gj < r2 - 1;
-    if (up && left) {
-      eb = dev::minf_d(eb, tri[0][a][b]);
-      eb = dev::minf_d(eb, tri[1][a][b]);
+    const float uu = su[a + 1][b + 1], vv = sv[a + 1][b + 1];
+    // the reference's chain eb = MINF(eb, triangle bound) over the six triangles
+    auto vertex_eb = [&](auto&& tri_at) {
+      double eb = max_pwr_eb;
+      if (up && left) {
+        eb = dev::minf_d(eb, tri_at(0, a, b));
+        eb = dev::minf_d(eb, tri_at(1, a, b));
+      }
+      if (up && right) eb = dev::minf_d(eb, tri_at(0, a, b + 1));
+      if (down && left) eb = dev::minf_d(eb, tri_at(1, a + 1, b));
+      if (down && right) {
+        eb = dev::minf_d(eb, tri_at(0, a + 1, b + 1));
+        eb = dev::minf_d(eb, tri_at(1, a + 1, b + 1));
+      }
+      return eb;
+    };
+    int code[2];
+    double eb = 0;
+    if (FAST) {
+      // enclosure of the vertex bound from the filtered triangle bounds
+      double m = INFINITY;
+      bool nan = false;
+      auto take = [&](double t) {
+        nan |= isnan(t);
+        m = fmin(m, t);
+      };
+      if (up && left) {
+        take(tri[0][a][b]);
+        take(tri[1][a][b]);
+      }
+      if (up && right) take(tri[0][a][b + 1]);
+      if (down && left) take(tri[1][a + 1][b]);
+      if (down && right) {
+        take(tri[0][a + 1][b + 1]);
+        take(tri[1][a + 1][b + 1]);
+      }
+      const double lo = fmin(max_pwr_eb, m * (1.0 - dev::FILTER_REL) - dev::FILTER_ABS);
+      const double hi = fmin(max_pwr_eb, m * (1.0 + dev::FILTER_REL) + dev::FILTER_ABS);
+      code[0] = quant((double)fabsf(uu) * lo);
+      code[1] = quant((double)fabsf(vv) * lo);
+      // the upper end has the same id iff it stays below the next threshold
+      auto stays = [&](int c, double e) { return c < 0 ? e <= thr : (c + 1 >= thr_n || e < tab[c + 1]); };
+      if (nan || !stays(code[0], (double)fabsf(uu) * hi) || !stays(code[1], (double)fabsf(vv) * hi)) {
+        // the enclosure straddles a threshold (or a bound is NaN): exact bounds
+        eb = vertex_eb([&](int kind, int ca, int cb) {
+          const int a1 = ca + (kind == 0), b1 = cb + (kind == 1);
+          return dev::tri_eb_exact(su[ca][cb], su[a1][b1], su[ca + 1][cb + 1], sv[ca][cb], sv[a1][b1],
+                                   sv[ca + 1][cb + 1], kind);
+        });
+        code[0] = quant((double)fabsf(uu) * eb);
+        code[1] = quant((double)fabsf(vv) * eb);
+      }
+    } else {
+      eb = vertex_eb([&](int kind, int ca, int cb) { return tri[kind][ca][cb]; });
+      code[0] = quant((double)fabsf(uu) * eb);
+      code[1] = quant((double)fabsf(vv) * eb);
     }
-    if (up && right) eb = dev::minf_d(eb, tri[0][a][b + 1]);
-    if (down && left) eb = dev::minf_d(eb, tri[1][a + 1][b]);
-    if (down && right) {
-      eb = dev::minf_d(eb, tri[0][a + 1][b + 1]);
-      eb = dev::minf_d(eb, tri[1][a + 1][b + 1]);
-    }
-    float uu = su[a + 1][b + 1], vv = sv[a + 1][b + 1];
-    uint8_t code[2];
     int sym[2];
-    double ev[2] = {(double)fabsf(uu) * eb, (double)fabsf(vv) * eb};
 #pragma unroll
     for (int c = 0; c < 2; c++) {
-      double e = ev[c];
-      if (e <= thr) {
-        code[c] = ID_ZERO;
-        sym[c] = 0;
-      } else {
-        int ex = (int)((__double_as_longlong(e) >> 52) & 0x7ff) - 1023;
-        int id = dev::count_thresholds(tab, thr_n, e, (ex + 52) >> 1);
-        if (id > ID_MAX_2D) {
-          atomicOr(flag, FLAG_ID_OVERFLOW);
-          id = ID_MAX_2D;
-        }
-        code[c] = (uint8_t)id;
-        sym[c] = id;
+      if (code[c] > ID_MAX_2D) {
+        atomicOr(flag, FLAG_ID_OVERFLOW);
+        code[c] = ID_MAX_2D;
       }
+      sym[c] = code[c] < 0 ? 0 : code[c];
+      if (code[c] < 0) code[c] = ID_ZERO;
     }
     size_t g = (size_t)gi * r2 + gj;
-    if (eb_out) eb_out[g] = eb;
-    ids_u[g] = code[0];
-    ids_v[g] = code[1];
+    if (!FAST && eb_out) eb_out[g] = eb;
+    ids_u[g] = (uint8_t)code[0];
+    ids_v[g] = (uint8_t)code[1];
     if (pair_u) {
       // the wavefront's input: value and 1/precision = 2^(52 - 2 id) (NaN for precision 0)
       pair_u[g] = make_float2(uu, code[0] == ID_ZERO ? __int_as_float(0x7FC00000)
@@ -151,9 +198,12 @@ int preload_eb2d() {
   // would then never see it start.  Querying the attributes loads each
   // instantiation up front.
   cudaFuncAttributes a;
-  const void* fns[] = {(const void*)eb2d_kernel<32, 16, 256>, (const void*)eb2d_kernel<32, 8, 128>,
-                       (const void*)eb2d_kernel<64, 8, 256>,  (const void*)eb2d_kernel<32, 32, 256>,
-                       (const void*)eb2d_kernel<64, 16, 256>, (const void*)eb2d_kernel<32, 16, 128>};
+  const void* fns[] = {(const void*)eb2d_kernel<32, 16, 256, true>,  (const void*)eb2d_kernel<32, 8, 128, true>,
+                       (const void*)eb2d_kernel<64, 8, 256, true>,   (const void*)eb2d_kernel<32, 32, 256, true>,
+                       (const void*)eb2d_kernel<64, 16, 256, true>,  (const void*)eb2d_kernel<32, 16, 128, true>,
+                       (const void*)eb2d_kernel<32, 16, 256, false>, (const void*)eb2d_kernel<32, 8, 128, false>,
+                       (const void*)eb2d_kernel<64, 8, 256, false>,  (const void*)eb2d_kernel<32, 32, 256, false>,
+                       (const void*)eb2d_kernel<64, 16, 256, false>, (const void*)eb2d_kernel<32, 16, 128, false>};
   for (const void* f : fns) {
     cudaError_t e = cudaFuncGetAttributes(&a, f);
     if (e != cudaSuccess) return set_error(CPSZ_ERR_CUDA, "loading eb2d_kernel: %s", cudaGetErrorString(e));
@@ -174,13 +224,22 @@ int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int 
     kernel<<<grid, nt, 0, ctx->stream>>>(U, V, r1, r2, max_pwr_eb, d_thr_tab, thr_n, ids_u, ids_v, hist, ctx->d_flag,
                                          pair_u, pair_v, eb_out, row_begin, row_end, band_done);
   };
-  switch (tune_get(TUNE_EB2D_TILE, (size_t)r1 * r2)) {
-    case 1: go(eb2d_kernel<32, 8, 128>, 32, 8, 128); break;
-    case 2: go(eb2d_kernel<64, 8, 256>, 64, 8, 256); break;
-    case 3: go(eb2d_kernel<32, 32, 256>, 32, 32, 256); break;
-    case 4: go(eb2d_kernel<64, 16, 256>, 64, 16, 256); break;
-    case 5: go(eb2d_kernel<32, 16, 128>, 32, 16, 128); break;
-    default: go(eb2d_kernel<32, 16, 256>, 32, 16, 256); break;
+  // filtered bounds unless the caller wants the bounds themselves (or an
+  // unusual max_pwr_eb takes the reference's NaN paths)
+  const bool fast = eb_out == nullptr && max_pwr_eb >= 0 && max_pwr_eb <= 1e300;
+  switch (tune_get(TUNE_EB2D_TILE, (size_t)r1 * r2) + (fast ? 0 : 6)) {
+    case 1: go(eb2d_kernel<32, 8, 128, true>, 32, 8, 128); break;
+    case 2: go(eb2d_kernel<64, 8, 256, true>, 64, 8, 256); break;
+    case 3: go(eb2d_kernel<32, 32, 256, true>, 32, 32, 256); break;
+    case 4: go(eb2d_kernel<64, 16, 256, true>, 64, 16, 256); break;
+    case 5: go(eb2d_kernel<32, 16, 128, true>, 32, 16, 128); break;
+    case 0: go(eb2d_kernel<32, 16, 256, true>, 32, 16, 256); break;
+    case 7: go(eb2d_kernel<32, 8, 128, false>, 32, 8, 128); break;
+    case 8: go(eb2d_kernel<64, 8, 256, false>, 64, 8, 256); break;
+    case 9: go(eb2d_kernel<32, 32, 256, false>, 32, 32, 256); break;
+    case 10: go(eb2d_kernel<64, 16, 256, false>, 64, 16, 256); break;
+    case 11: go(eb2d_kernel<32, 16, 128, false>, 32, 16, 128); break;
+    default: go(eb2d_kernel<32, 16, 256, false>, 32, 16, 256); break;
   }
   count_launch(ctx);
   return check_launch("eb2d_kernel");

@@ -186,6 +186,105 @@ __device__ __forceinline__ double tri_eb(float u0, float u1, float u2, float v0,
   return eb;
 }
 
+static __device__ __noinline__ double tri_eb_exact(float u0, float u1, float u2, float v0, float v1, float v2,
+                                                   int kind) {
+  return tri_eb(u0, u1, u2, v0, v1, v2, kind);
+}
+
+// ---- filtered 2D bound ------------------------------------------------------
+// The compressor uses a vertex's bound only through the id of |u| * eb and
+// |v| * eb, and ids change only at thresholds a factor 4 apart.  So the
+// ordinary triangles (no critical point, finite products: 98 % and more of a
+// field) get their sign-keeping bounds from a float evaluation with a proven
+// enclosure of the reference's double result, and a vertex whose enclosure
+// straddles a threshold is recomputed exactly.
+//
+// Enclosure of keep_sign2(P, N) = |sqrt P - sqrt N| / (sqrt P + sqrt N) for
+// finite P, N > 0 (P and N are the reference's own double sums):
+//  * the reference's double evaluation r_ref (two square roots, a difference,
+//    a sum, a quotient, each rounded to nearest, u = 2^-53) differs from the
+//    real value r by at most 4.1 u r + 1.01 u;
+//  * the float evaluation r_a = |P - N| / (P + N + 2 sqrt(P N)) (the same real
+//    value; P, N scaled by a power of two into [0, 2] first, so nothing
+//    overflows; the larger lands in [1, 2), and an underflowed product moves
+//    the denominator by < 2^-70 of itself), with round-to-nearest conversions,
+//    product and sums (2^-24 each), sqrt.approx.f32 (relative error below
+//    2^-22) and div.approx.f32 (2 ulp), has a relative error below 2^-19;
+//  so r_ref lies in [r_a (1 - REL) - ABS, r_a (1 + REL) + ABS] with the
+//  margins below (REL about 5x, ABS about 30x the sums).  The triangle bound
+//  is a max of mins of such values, and the vertex bound a min of triangle
+//  bounds: all monotone, so the same affine enclosure holds for them.
+constexpr double FILTER_REL = 1e-5;
+constexpr double FILTER_ABS = 3.552713678800501e-15;  // 2^-48
+
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float y;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float div_approx(float a, float b) {
+  float y;
+  asm("div.approx.f32 %0, %1, %2;" : "=f"(y) : "f"(a), "f"(b));
+  return y;
+}
+__device__ __forceinline__ double keep_sign2_approx(double P, double N) {
+  if ((N == 0) || (P == 0)) return 1;
+  // scale by 2^-e, e the exponent of the larger (P, N are normal doubles):
+  // subtracting e from both exponent fields is exact
+  const long long m = __double_as_longlong(P > N ? P : N) & 0x7ff0000000000000ll;
+  const long long sh = m - (1023ll << 52);
+  const float pf = (float)__longlong_as_double(__double_as_longlong(P) - sh);
+  const float nf = (float)__longlong_as_double(__double_as_longlong(N) - sh);
+  const float df = (float)(fabs(P - N) * __longlong_as_double((2046ll << 52) - m));
+  const float den = pf + nf + 2.f * sqrt_approx(pf * nf);
+  return (double)div_approx(df, den);
+}
+__device__ __forceinline__ double off2_approx(double a, double b) {
+  double p = 0, n = 0;
+  acc(a, p, n);
+  acc(b, p, n);
+  return keep_sign2_approx(p, n);
+}
+__device__ __forceinline__ double off4_approx(double a, double b, double c, double d) {
+  double p = 0, n = 0;
+  acc(a, p, n);
+  acc(b, p, n);
+  acc(c, p, n);
+  acc(d, p, n);
+  return keep_sign2_approx(p, n);
+}
+
+// Filtered triangle bound: the exact tri_eb for det == 0, critical-point
+// triangles and non-finite products (NaN possible there); otherwise the same
+// max over failing flags of min(off2, off4), of the float approximations.
+__device__ __forceinline__ double tri_eb_filtered(float u0, float u1, float u2, float v0, float v1, float v2,
+                                                  int kind) {
+  const double u0v1 = (double)(u0 * v1), u1v0 = (double)(u1 * v0), u0v2 = (double)(u0 * v2);
+  const double u2v0 = (double)(u2 * v0), u1v2 = (double)(u1 * v2), u2v1 = (double)(u2 * v1);
+  const double det = u0v1 - u1v0 + u1v2 - u2v1 + u2v0 - u0v2;
+  if (det == 0) return 0;
+  const bool f1 = quotient_at_least_one(det, u2v0 - u0v2);
+  const bool f2 = quotient_at_least_one(det, u1v2 - u2v1);
+  const bool f3 = quotient_at_least_one(det, u0v1 - u1v0);
+  if ((f1 && f2 && f3) || !(isfinite(u0v1) && isfinite(u1v0) && isfinite(u0v2) && isfinite(u2v0) &&
+                            isfinite(u1v2) && isfinite(u2v1)))
+    return tri_eb_exact(u0, u1, u2, v0, v1, v2, kind);
+  double eb = 0;
+  if (!f1) {
+    const double e1 = off2_approx(u2v0, -u0v2);
+    if (e1 > eb) eb = max_d(eb, minf_d(e1, off4_approx(u0v1, -u1v0, u1v2, -u2v1)));
+  }
+  if (!f2) {
+    const double e1 = off2_approx(u1v2, -u2v1);
+    if (e1 > eb) eb = max_d(eb, minf_d(e1, off4_approx(u0v1, -u1v0, u2v0, -u0v2)));
+  }
+  if (!f3) {
+    const double e1 = off2_approx(u0v1, -u1v0);
+    if (e1 > eb) eb = max_d(eb, minf_d(e1, off4_approx(u1v2, -u2v1, u2v0, -u0v2)));
+  }
+  return eb;
+}
+
 // ---- 3D (src/sz_compress_cp_preserve_3d.cpp:266-358) --------------------------
 
 // acbrt1: include/sz_cp_preserve_utils.hpp:173-184 (the reference's own

@@ -236,7 +236,10 @@ size_t cpsz_b200_blob_size_2d(const unsigned char* blob);
 
 /* ---- diagnostics (no reference counterpart) ---------------------------------
  * The 2D bound kernel alone: per-vertex bound before quantization (eb_out, N
- * doubles) and id bytes (id_codes, 2N; 255 = precision 0).  Host buffers. */
+ * doubles) and id bytes (id_codes, 2N; 255 = precision 0).  Host buffers.
+ * With eb_out the kernel evaluates every bound exactly; with eb_out = NULL it
+ * takes the compressor's filtered path (ids only), which must give the same
+ * ids. */
 int cpsz_b200_debug_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2,
                          double max_pwr_eb, double* eb_out, uint8_t* id_codes);
 /* The 3D bound kernel alone: per-vertex bound (N doubles) and id bytes (N;
