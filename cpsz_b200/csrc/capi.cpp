@@ -8,6 +8,7 @@
 #include "cpsz_b200.hpp"
 #include "huffman_host.h"
 #include "pipeline.h"
+#include "transfer.h"
 
 // system libzstd.so.1 (linked directly; the image has no zstd.h)
 extern "C" {
@@ -20,19 +21,9 @@ const char* ZSTD_getErrorName(size_t code);
 
 namespace cpsz {
 
-int copy_out(cpsz_b200_ctx* ctx, void* dst, const void* d_src, size_t n) {
-  if (!n) return CPSZ_OK;
-  cudaMemcpyKind k = is_device_ptr(dst) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-  CPSZ_CUDA_TRY(cudaMemcpyAsync(dst, d_src, n, k, ctx->stream));
-  return CPSZ_OK;
-}
+int copy_out(cpsz_b200_ctx* ctx, void* dst, const void* d_src, size_t n) { return d2h(ctx, dst, d_src, n, ctx->stream); }
 
-int copy_in(cpsz_b200_ctx* ctx, void* d_dst, const void* src, size_t n) {
-  if (!n) return CPSZ_OK;
-  cudaMemcpyKind k = is_device_ptr(src) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-  CPSZ_CUDA_TRY(cudaMemcpyAsync(d_dst, src, n, k, ctx->stream));
-  return CPSZ_OK;
-}
+int copy_in(cpsz_b200_ctx* ctx, void* d_dst, const void* src, size_t n) { return h2d(ctx, d_dst, src, n, ctx->stream); }
 
 }  // namespace cpsz
 
@@ -56,14 +47,15 @@ int cpsz_b200_compress_2d_offline_f32(cpsz_b200_ctx* ctx, const float* U, const 
   CPSZ_TRY(compress_2d(ctx, U, V, r1, r2, max_pwr_eb, &b, nullptr));
   unsigned char* h = (unsigned char*)malloc(b.size ? b.size : 1);
   if (!h) return set_error(CPSZ_ERR_NOMEM, "host blob of %zu bytes", b.size);
-  CPSZ_TRY(pinned_reserve(ctx, b.size));
-  cudaError_t e = cudaMemcpyAsync(ctx->pinned, b.d_blob, b.size, cudaMemcpyDeviceToHost, ctx->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-  if (e != cudaSuccess) {
-    free(h);
-    return set_error(CPSZ_ERR_CUDA, "blob download: %s", cudaGetErrorString(e));
+  int rc = d2h(ctx, h, b.d_blob, b.size, ctx->stream);
+  if (rc == CPSZ_OK) {
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) rc = set_error(CPSZ_ERR_CUDA, "blob download: %s", cudaGetErrorString(e));
   }
-  memcpy(h, ctx->pinned, b.size);
+  if (rc != CPSZ_OK) {
+    free(h);
+    return rc;
+  }
   *blob = h;
   *blob_size = b.size;
   return CPSZ_OK;
@@ -267,18 +259,15 @@ int cpsz_b200_compress_3d_offline_log_f32(cpsz_b200_ctx* ctx, const float* U, co
   CPSZ_TRY(compress_3d(ctx, U, V, W, r1, r2, r3, max_pwr_eb, &b));
   unsigned char* h = (unsigned char*)malloc(b.size ? b.size : 1);
   if (!h) return set_error(CPSZ_ERR_NOMEM, "host blob of %zu bytes", b.size);
-  int rc = pinned_reserve(ctx, b.size);
+  int rc = d2h(ctx, h, b.d_blob, b.size, ctx->stream);
+  if (rc == CPSZ_OK) {
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) rc = set_error(CPSZ_ERR_CUDA, "blob download: %s", cudaGetErrorString(e));
+  }
   if (rc != CPSZ_OK) {
     free(h);
     return rc;
   }
-  cudaError_t e = cudaMemcpyAsync(ctx->pinned, b.d_blob, b.size, cudaMemcpyDeviceToHost, ctx->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-  if (e != cudaSuccess) {
-    free(h);
-    return set_error(CPSZ_ERR_CUDA, "blob download: %s", cudaGetErrorString(e));
-  }
-  memcpy(h, ctx->pinned, b.size);
   *blob = h;
   *blob_size = b.size;
   return CPSZ_OK;

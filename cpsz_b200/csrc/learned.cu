@@ -14,6 +14,7 @@
 
 #include "cpsz_b200.h"
 #include "kernels.h"
+#include "transfer.h"
 #include "pipeline.h"
 
 struct cpsz_b200_mlp {
@@ -166,8 +167,8 @@ int compress_2d_learned(cpsz_b200_ctx* ctx, cpsz_b200_mlp* mlp, const float* U_i
   const float* dV = V_in;
   if (!dev_in) {
     float* h = (float*)take(8 * N);
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(h, U_in, 4 * N, cudaMemcpyHostToDevice, st));
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(h + N, V_in, 4 * N, cudaMemcpyHostToDevice, st));
+    CPSZ_TRY(h2d(ctx, h, U_in, 4 * N, st));
+    CPSZ_TRY(h2d(ctx, h + N, V_in, 4 * N, st));
     dU = h;
     dV = h + N;
   }
@@ -249,18 +250,8 @@ int resolve(cpsz_b200_ctx*& ctx) {
 }
 
 // Host or device source -> device destination.
-int upload(cpsz_b200_ctx* ctx, void* dst, const void* src, size_t n) {
-  if (!n) return CPSZ_OK;
-  CPSZ_CUDA_TRY(cudaMemcpyAsync(dst, src, n, is_device_ptr(src) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
-                                ctx->stream));
-  return CPSZ_OK;
-}
-int download(cpsz_b200_ctx* ctx, void* dst, const void* src, size_t n) {
-  if (!n) return CPSZ_OK;
-  CPSZ_CUDA_TRY(cudaMemcpyAsync(dst, src, n, is_device_ptr(dst) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
-                                ctx->stream));
-  return CPSZ_OK;
-}
+int upload(cpsz_b200_ctx* ctx, void* dst, const void* src, size_t n) { return h2d(ctx, dst, src, n, ctx->stream); }
+int download(cpsz_b200_ctx* ctx, void* dst, const void* src, size_t n) { return d2h(ctx, dst, src, n, ctx->stream); }
 
 // training scratch layout for n samples: X | H1 | H2 (bf16 n x 128) | y | t (f32) | loss
 struct TrainBufs {

@@ -35,6 +35,7 @@
 #include "kernels.h"
 #include "tuning.h"
 #include "pipeline.h"
+#include "transfer.h"
 
 namespace cpsz {
 
@@ -391,6 +392,11 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
 
   // ---- stage 1: inputs and error bounds ----
   mark(ctx, "eb2d");
+  // host-input uploads run on the second stream, after the pass's setup (once
+  // per pass: per field it would hold each upload behind the previous field's
+  // bound kernels)
+  CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[2], st));
+  CPSZ_CUDA_TRY(cudaStreamWaitEvent(ctx->aux, ctx->ev[2], 0));
   for (Job2D& j : jobs) {
     unsigned long long* band = overlap ? j.d.band : nullptr;
     if (j.dev_in) {
@@ -408,8 +414,6 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       const int K = (j.N >= ((size_t)1 << 22) && !j.eb_ext) ? tune_get(TUNE_H2D_CHUNKS, j.N) : 1;
       const int R = (int)align_up((size_t)(j.r1 + K - 1) / K, WAVE_GROUP_ROWS);
       const int nch = (j.r1 + R - 1) / R;
-      CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[2], st));
-      CPSZ_CUDA_TRY(cudaStreamWaitEvent(ctx->aux, ctx->ev[2], 0));
       // band c needs chunks c and c + 1; it is enqueued right after chunk
       // c + 1's copy call (a copy from pageable memory returns only once the
       // host has staged it, so enqueueing every copy first would hold the
@@ -618,8 +622,7 @@ int compress_2d_batch(cpsz_b200_ctx* ctx, int n, const float* const* U, const fl
       const Job2D& j = jobs[q];
       if (at + j.size > out_cap)
         return set_error(CPSZ_ERR_INVALID, "output capacity %zu < %zu bytes of blobs", out_cap, at + j.size);
-      CPSZ_CUDA_TRY(cudaMemcpyAsync(out + at, j.d.blob, j.size,
-                                    dev_out ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
+      CPSZ_TRY(d2h(ctx, out + at, j.d.blob, j.size, ctx->stream));
       at += j.size;
       offsets[k0 + q + 1] = at;
     }
@@ -744,7 +747,7 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
     dtmp[k] = A(huff_decode_tmp_bytes(h.nbytes * 8));
     const size_t off_bits = (k == 0) ? BLOB_HDR + h.bits_offset : fv[k - 1].huff_off + h.bits_offset;
     CPSZ_CUDA_TRY(cudaMemsetAsync(bits[k], 0, h.nbytes + 64, st));
-    if (h.nbytes) CPSZ_CUDA_TRY(cudaMemcpyAsync(bits[k], blob + off_bits, h.nbytes, cudaMemcpyHostToDevice, st));
+    if (h.nbytes) CPSZ_TRY(h2d(ctx, bits[k], blob + off_bits, h.nbytes, st));
     uint32_t* lut = (uint32_t*)t;
     uint32_t* child = lut + (1u << HUFF_LUT_BITS);
     uint32_t* sym = child + h.child.size();
@@ -770,7 +773,7 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
     seg_off[f] = (unsigned int*)A((nseg + 1) * 4);
     scan_tmp[f] = A(segment_scan_tmp_bytes(r1, r2));
     if (fv[f].n_unpred)
-      CPSZ_CUDA_TRY(cudaMemcpyAsync(unpred[f], blob + fv[f].unpred_off, 4 * fv[f].n_unpred, cudaMemcpyHostToDevice, st));
+      CPSZ_TRY(h2d(ctx, unpred[f], blob + fv[f].unpred_off, 4 * fv[f].n_unpred, st));
   }
   unsigned long long* gbnd = (unsigned long long*)A(2 * (size_t)ngroups * r2 * 8);
   int* queue = (int*)A(64);
@@ -820,8 +823,8 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
   CPSZ_TRY(launch_wave2d(ctx, true, dfields, ditems, n_items, queue, (size_t)r1 * r2));
   mark(ctx, "d2h");
   if (!dev_out) {
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(U_out, dU, 4 * N, cudaMemcpyDeviceToHost, st));
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(V_out, dV, 4 * N, cudaMemcpyDeviceToHost, st));
+    CPSZ_TRY(d2h(ctx, U_out, dU, 4 * N, st));
+    CPSZ_TRY(d2h(ctx, V_out, dV, 4 * N, st));
   }
   mark(ctx, "end");
   int flag = 0;

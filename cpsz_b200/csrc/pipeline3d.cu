@@ -22,6 +22,7 @@
 
 #include "huffman_host.h"
 #include "kernels.h"
+#include "transfer.h"
 #include "pipeline.h"
 
 namespace cpsz {
@@ -109,9 +110,9 @@ int compress_3d(cpsz_b200_ctx* ctx, const float* U_in, const float* V_in, const 
     dW = W_in;
   } else {
     float* h = (float*)A(12 * N);
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(h, U_in, 4 * N, cudaMemcpyHostToDevice, st));
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(h + N, V_in, 4 * N, cudaMemcpyHostToDevice, st));
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(h + 2 * N, W_in, 4 * N, cudaMemcpyHostToDevice, st));
+    CPSZ_TRY(h2d(ctx, h, U_in, 4 * N, st));
+    CPSZ_TRY(h2d(ctx, h + N, V_in, 4 * N, st));
+    CPSZ_TRY(h2d(ctx, h + 2 * N, W_in, 4 * N, st));
     dU = h;
     dV = h + N;
     dW = h + 2 * N;
@@ -345,7 +346,7 @@ int decompress_3d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
     if (!dtmp[k]) return set_error(CPSZ_ERR_NOMEM, "workspace layout overflow");
     CPSZ_CUDA_TRY(cudaMemsetAsync(bits[k], 0, h.nbytes + 64, st));
     if (h.nbytes)
-      CPSZ_CUDA_TRY(cudaMemcpyAsync(bits[k], blob + sec_at[k] + h.bits_offset, h.nbytes, cudaMemcpyHostToDevice, st));
+      CPSZ_TRY(h2d(ctx, bits[k], blob + sec_at[k] + h.bits_offset, h.nbytes, st));
     uint32_t* lut = (uint32_t*)t;
     uint32_t* child = lut + (1u << HUFF_LUT_BITS);
     uint32_t* sym = child + h.child.size();
@@ -363,8 +364,8 @@ int decompress_3d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
   float4* rec = (float4*)A(16 * N);
   if (!rec) return set_error(CPSZ_ERR_NOMEM, "workspace layout overflow");
   CPSZ_CUDA_TRY(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), st));
-  CPSZ_CUDA_TRY(cudaMemcpyAsync(signs, blob + 8, 3 * smap, cudaMemcpyHostToDevice, st));
-  if (n_unpred) CPSZ_CUDA_TRY(cudaMemcpyAsync(unpred, blob + unpred_at, 4 * n_unpred, cudaMemcpyHostToDevice, st));
+  CPSZ_TRY(h2d(ctx, signs, blob + 8, 3 * smap, st));
+  if (n_unpred) CPSZ_TRY(h2d(ctx, unpred, blob + unpred_at, 4 * n_unpred, st));
   reset_marks(ctx);
   mark(ctx, "huffman_decode");
   CPSZ_TRY(launch_huff_decode(ctx, bits[0], hs[0].nbytes, N, tab[0], ids, 1, dtmp[0]));
@@ -377,9 +378,9 @@ int decompress_3d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
   CPSZ_TRY(launch_wave3d_planes(ctx, true, pairs, rec, nullptr, signs, smap, &lt, dU, dV, dW, r1, r2, r3));
   mark(ctx, "d2h");
   if (!dev_out) {
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(U_out, dU, 4 * N, cudaMemcpyDeviceToHost, st));
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(V_out, dV, 4 * N, cudaMemcpyDeviceToHost, st));
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(W_out, dW, 4 * N, cudaMemcpyDeviceToHost, st));
+    CPSZ_TRY(d2h(ctx, U_out, dU, 4 * N, st));
+    CPSZ_TRY(d2h(ctx, V_out, dV, 4 * N, st));
+    CPSZ_TRY(d2h(ctx, W_out, dW, 4 * N, st));
   }
   mark(ctx, "end");
   int flag = 0;

@@ -260,6 +260,7 @@ int cpsz_b200_ctx_create(int device, cpsz_b200_ctx** out) {
   for (auto& ev : c->ev) CPSZ_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   for (auto& ev : c->up_ev) CPSZ_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   for (auto& ev : c->job_ev) CPSZ_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  for (auto& ev : c->stage_ev) CPSZ_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   CPSZ_CUDA_TRY(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
   CPSZ_CUDA_TRY(cudaMalloc((void**)&c->d_flag, 64));
   CPSZ_CUDA_TRY(cudaMemset(c->d_flag, 0, 64));
@@ -278,6 +279,7 @@ int cpsz_b200_ctx_destroy(cpsz_b200_ctx* c) {
   if (c->hi) cudaStreamSynchronize(c->hi);
   if (c->arena.base) cudaFree(c->arena.base);
   if (c->pinned) cudaFreeHost(c->pinned);
+  if (c->stage) cudaFreeHost(c->stage);
   if (c->d_flag) cudaFree(c->d_flag);
   if (c->libm_mem) cudaFree(c->libm_mem);
   delete (cpsz::LibmTables*)c->libm_view;
@@ -286,6 +288,8 @@ int cpsz_b200_ctx_destroy(cpsz_b200_ctx* c) {
   for (auto& ev : c->up_ev)
     if (ev) cudaEventDestroy(ev);
   for (auto& ev : c->job_ev)
+    if (ev) cudaEventDestroy(ev);
+  for (auto& ev : c->stage_ev)
     if (ev) cudaEventDestroy(ev);
   for (auto& ev : c->tev)
     if (ev) cudaEventDestroy(ev);

@@ -80,6 +80,11 @@ struct cpsz_b200_ctx {
   static constexpr int kJobEvents = 64;
   cudaEvent_t job_ev[kJobEvents] = {};
   cpsz::Arena arena;
+  // pinned ring for bulk copies of pageable host memory (transfer.h)
+  static constexpr int kStageSlots = 4;
+  static constexpr size_t kStageBytes = (size_t)16 << 20;
+  void* stage = nullptr;
+  cudaEvent_t stage_ev[kStageSlots] = {};
   void* pinned = nullptr;
   size_t pinned_cap = 0;
   uint64_t launches = 0;
