@@ -307,6 +307,26 @@ __device__ __forceinline__ float keep_sign_3d(float positive, float negative) {
   return fabsf(P - N) / (P + N);
 }
 
+// acbrt1 for x0 >= +0 (finite or not): the bit pattern is a non-negative int,
+// for which the divisions by 4, 16 and 256 are exact right shifts.
+__device__ __forceinline__ float acbrt1_nonneg(float x0) {
+  int ix = __float_as_int(x0);
+  ix = (ix >> 2) + (ix >> 4);
+  ix = ix + (ix >> 4);
+  ix = ix + (ix >> 8);
+  ix = 0x2a5137a0 + ix;
+  float x = __int_as_float(ix);
+  x = 0.33333333f * (2.0f * x + x0 / (x * x));
+  x = 0.33333333f * (2.0f * x + x0 / (x * x));
+  return x;
+}
+// keep_sign_3d for non-negative arguments (every sum of magnitudes)
+__device__ __forceinline__ float keep_sign_3d_nonneg(float positive, float negative) {
+  if (positive == 0 && negative == 0) return 0;
+  float P = acbrt1_nonneg(positive), N = acbrt1_nonneg(negative);
+  return fabsf(P - N) / (P + N);
+}
+
 __device__ __forceinline__ int sgnf(float v) { return (0.0f < v) - (v < 0.0f); }
 __device__ __forceinline__ bool same_direction(float a, float b, float c, float d) {
   int s = sgnf(a);
@@ -382,20 +402,20 @@ static __device__ __noinline__ double tet_eb(float u0, float u1, float u2, float
     // max/min: a flag whose first bound cannot raise eb leaves it unchanged,
     // and its second bound need not be evaluated.
     if (!flag0) {
-      const float e1 = keep_sign_3d(p_m0, n_m0);
-      if (e1 > eb) eb = maxf_(eb, minf_(e1, keep_sign_3d(sp0, sn0)));
+      const float e1 = keep_sign_3d_nonneg(p_m0, n_m0);
+      if (e1 > eb) eb = maxf_(eb, minf_(e1, keep_sign_3d_nonneg(sp0, sn0)));
     }
     if (!flag1) {
-      const float e1 = keep_sign_3d(p_m1, n_m1);
-      if (e1 > eb) eb = maxf_(eb, minf_(e1, keep_sign_3d(sp1, sn1)));
+      const float e1 = keep_sign_3d_nonneg(p_m1, n_m1);
+      if (e1 > eb) eb = maxf_(eb, minf_(e1, keep_sign_3d_nonneg(sp1, sn1)));
     }
     if (!flag2) {
-      const float e1 = keep_sign_3d(p_m2, n_m2);
-      if (e1 > eb) eb = maxf_(eb, minf_(e1, keep_sign_3d(sp2, sn2)));
+      const float e1 = keep_sign_3d_nonneg(p_m2, n_m2);
+      if (e1 > eb) eb = maxf_(eb, minf_(e1, keep_sign_3d_nonneg(sp2, sn2)));
     }
     if (!flag3) {
-      const float e1 = keep_sign_3d(p_m3, n_m3);
-      if (e1 > eb) eb = maxf_(eb, minf_(e1, keep_sign_3d(sp3, sn3)));
+      const float e1 = keep_sign_3d_nonneg(p_m3, n_m3);
+      if (e1 > eb) eb = maxf_(eb, minf_(e1, keep_sign_3d_nonneg(sp3, sn3)));
     }
     return eb;
   }
