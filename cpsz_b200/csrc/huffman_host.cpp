@@ -13,6 +13,7 @@
 #include "huffman_host.h"
 
 #include <algorithm>
+#include <cstdint>
 #include <cstring>
 
 #include "kernels.h"
@@ -27,9 +28,12 @@ namespace {
 // one 8-byte load per visited slot.
 class Heap {
  public:
-  // `storage` keeps its capacity across calls (fresh pages cost a fault each)
-  Heap(std::vector<unsigned long long>& storage, size_t cap) : q_(storage) {
-    if (q_.size() < cap + 2) q_.resize(cap + 2);
+  // `storage` keeps its capacity across calls (fresh pages cost a fault each);
+  // slot 0 of the heap sits on a 64-byte boundary, so the 8 great-grandchildren
+  // 8i..8i+7 of slot i share one cache line.
+  Heap(std::vector<unsigned long long>& storage, size_t cap) {
+    if (storage.size() < cap + 2 + 8) storage.resize(cap + 2 + 8);
+    q_ = (unsigned long long*)(((uintptr_t)storage.data() + 63) & ~(uintptr_t)63);
   }
   void insert(unsigned long long f, int n) {
     const unsigned long long e = (f << kShift) | (unsigned long long)n;
@@ -41,23 +45,42 @@ class Heap {
     }
     q_[i] = e;
   }
-  // Removes the top entry and returns its key (freq << kShift | node).
+  // Removes the top entry and returns its key (freq << kShift | node).  The
+  // hole at the top moves down to a leaf, each step taking the right child
+  // only when its frequency is strictly smaller; the last entry then fills it.
   unsigned long long remove_key() {
-    int i = 1, l;
-    const unsigned long long n = q_[1];
+    unsigned long long* q = q_;
+    const unsigned long long n = q[1];
     end_--;
-    const unsigned long long* q = q_.data();
-    const int lim = (int)q_.size() - 8;
-    while ((l = i << 1) < end_) {
-      // the 8 great-grandchildren share one cache line: fetch it two levels early
-      if (4 * l < lim) __builtin_prefetch(q + 4 * l);
-      // branch-free child choice (the comparison is data-dependent and
-      // mispredicts half the time)
-      l += (int)((l + 1 < end_) & ((q[l + 1] >> kShift) < (q[l] >> kShift)));
-      q_[i] = q[l];
+    const size_t end = (size_t)end_;
+    size_t i = 1;
+    // Three levels per step while all 8 great-grandchildren are in the heap:
+    // the children and grandchildren load together, the choices are
+    // register selects (they are data-dependent and would mispredict), and
+    // one load of the chosen grandchild's pair completes the step.
+    while (8 * i + 7 < end) {
+      const unsigned long long* c = q + 2 * i;
+      const unsigned long long* g = q + 4 * i;
+      const unsigned long long c0 = c[0], c1 = c[1], g0 = g[0], g1 = g[1], g2 = g[2], g3 = g[3];
+      const size_t s1 = (c1 >> kShift) < (c0 >> kShift);
+      const unsigned long long cv = s1 ? c1 : c0, ga = s1 ? g2 : g0, gb = s1 ? g3 : g1;
+      const size_t s2 = (gb >> kShift) < (ga >> kShift);
+      const unsigned long long gv = s2 ? gb : ga;
+      const size_t k = 2 * s1 + s2;  // the chosen grandchild is 4i + k
+      const unsigned long long ha = q[8 * i + 2 * k], hb = q[8 * i + 2 * k + 1];
+      const size_t s3 = (hb >> kShift) < (ha >> kShift);
+      q[i] = cv;
+      q[2 * i + s1] = gv;
+      q[4 * i + k] = s3 ? hb : ha;
+      i = 8 * i + 2 * k + s3;
+    }
+    size_t l;
+    while ((l = 2 * i) < end) {
+      l += (size_t)((l + 1 < end) & ((q[l + 1] >> kShift) < (q[l] >> kShift)));
+      q[i] = q[l];
       i = l;
     }
-    q_[i] = q_[end_];
+    q[i] = q[end];
     return n;
   }
   int size() const { return end_ - 1; }
@@ -66,7 +89,7 @@ class Heap {
   static constexpr unsigned long long kMask = (1ull << kShift) - 1;
 
  private:
-  std::vector<unsigned long long>& q_;
+  unsigned long long* q_;
   int end_ = 1;
 };
 
