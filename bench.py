@@ -349,7 +349,7 @@ def run_product(args, rank, world, device):
     # algorithmic bytes per launch of each stage's dominant kernel
     alg = {"eb2d": 4 * comps * n + comps * n,  # read fields, write one id byte per component
            "wave2d_compress": 4 * comps * n + comps * n + 2 * comps * n,  # fields + ids in, u16 codes out
-           "eb3d": 4 * 3 * n + 8 * n, "wave3d_compress": 0}
+           "eb3d": 4 * 3 * n + n, "wave3d_compress": 0}  # read fields, write one id byte
     # DRAM bytes per point of a launch, read + write, from one ncu capture of the
     # kernel on the 4096^2 case (394.0 MB for 16.8 M vertices), scaled to this
     # launch by its points

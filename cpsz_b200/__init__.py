@@ -84,6 +84,7 @@ def _declare(L):
     L.cpsz_b200_debug_eb3d.argtypes = [_vp, _vp, _vp, _vp, _sz, _sz, _sz, C.c_double, _vp, _vp]
     L.cpsz_b200_debug_eb2d.argtypes = [_vp, _vp, _vp, _sz, _sz, C.c_double, _vp, _vp]
     L.cpsz_b200_debug_libm.argtypes = [_vp, C.c_int, _vp, _sz, _vp]
+    L.cpsz_b200_debug_filter_premises.argtypes = [_vp, _vp, _sz]
     L.cpsz_b200_debug_umma_gemm.argtypes = [_vp, _vp, _vp, _vp]
     L.cpsz_b200_mlp_param_count.restype = _sz
     L.cpsz_b200_mlp_create.argtypes = [_vp, C.c_uint64, C.POINTER(_vp)]
@@ -524,6 +525,18 @@ def compress_2d_learned(U, V, max_pwr_eb: float = 0.1, mlp: Mlp | None = None, l
     if ret_bytes:
         return out[:n.value].tobytes(), st
     return n.value, st
+
+
+def debug_filter_premises(ctx: Context | None = None) -> dict:
+    """Exhaustive maxima, on this device, of the operations whose error bounds
+    the filtered 2D / 3D bounds rely on: acbrt1 relative error above / below a
+    double cube root ("acbrt1_hi", "acbrt1_lo"), the relative errors of
+    rcp.approx, ex2.approx and sqrt.approx, and lg2.approx's absolute error
+    per binade ("lg2": {e: max over [2^e, 2^(e+1))}, e = -126..0)."""
+    out = np.zeros(132, np.float64)
+    _check(lib().cpsz_b200_debug_filter_premises(_h(ctx), out.ctypes.data, out.size))
+    return {"acbrt1_hi": out[0], "acbrt1_lo": out[1], "rcp": out[2], "ex2": out[3], "sqrt": out[4],
+            "lg2": {e: out[5 + e + 126] for e in range(-126, 1)}}
 
 
 def debug_libm(which: str, x, ctx: Context | None = None):

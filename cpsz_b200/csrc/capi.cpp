@@ -391,6 +391,29 @@ int cpsz_b200_debug_libm(cpsz_b200_ctx* ctx, int which, const float* in, size_t 
   return rc;
 }
 
+int cpsz_b200_debug_filter_premises(cpsz_b200_ctx* ctx, double* out, size_t n) {
+  RESOLVE(ctx);
+  if (!out || n < (size_t)FP_COUNT) return set_error(CPSZ_ERR_INVALID, "need %d output doubles", (int)FP_COUNT);
+  unsigned* d = nullptr;
+  CPSZ_CUDA_TRY(cudaMalloc((void**)&d, FP_COUNT * sizeof(unsigned)));
+  unsigned h[FP_COUNT];
+  int rc = launch_filter_premises(ctx, d);
+  if (rc == CPSZ_OK) {
+    const cudaError_t e = cudaMemcpyAsync(h, d, sizeof h, cudaMemcpyDeviceToHost, ctx->stream);
+    const cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess || e2 != cudaSuccess)
+      rc = set_error(CPSZ_ERR_CUDA, "filter premises: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+  }
+  cudaFree(d);
+  if (rc != CPSZ_OK) return rc;
+  for (int i = 0; i < FP_COUNT; i++) {
+    float f;
+    memcpy(&f, &h[i], 4);
+    out[i] = f;
+  }
+  return CPSZ_OK;
+}
+
 // ---- exact critical-point checker ----------------------------------------------------
 
 namespace {

@@ -327,6 +327,74 @@ __device__ __forceinline__ float keep_sign_3d_nonneg(float positive, float negat
   return fabsf(P - N) / (P + N);
 }
 
+// ---- filtered 3D sign-keeping bounds -----------------------------------------
+// A tet's bound with finite magnitudes is max over the unflagged minors i of
+// min(K(p_i, n_i), K(sp_i, sn_i)), K = keep_sign_3d: one of its (up to) 8
+// values.  Each K gets a cheap enclosure [k~ - DELTA, k~ + DELTA]; only the
+// values the enclosures cannot rule out are computed exactly (one per tet
+// in 97 % of the tets of a smooth field, against seven), and the result is
+// the reference's float.
+//
+// Enclosure.  For normal P, N > 0 write c = acbrt1 = cbrt (1 + e); over every
+// normal float e lies in [-7.14e-8, 1.21e-6] (checked exhaustively against a
+// double cube root), so l = ln(c(P) / c(N)) = ln(P / N) / 3 + ln(1 + e_P) -
+// ln(1 + e_N) is within 1.28e-6 of ln(P / N) / 3.  The exact-arithmetic
+// value |c(P) - c(N)| / (c(P) + c(N)) is tanh(|l| / 2), whose slope in l is
+// (1 - K^2) / 2 <= 1/2; the reference's float evaluation (difference, sum,
+// quotient) adds at most 3u (u = 2^-24).  The approximation: r = min / max
+// (rcp.approx and a product), d = |lg2(r)| (lg2.approx), s = 2^(-d / 3)
+// (a product by -1/3 and ex2.approx), k~ = (1 - s) / (1 + s) (rcp.approx).
+// Exhaustive maxima of the .ftz.f32 approximations over the inputs they get
+// here: rcp relative 9.9e-8 on all normal floats below 2^126; ex2 relative
+// 1.44e-7 on [-87, 0]; lg2 absolute, per binade of r, 1.6e-7 on [1, 2),
+// 2.2e-7 on [1/2, 1), 2.7e-7 on [1/4, 1/2), then about one ulp of the result
+// (3.9e-7 on [2^-4, 2^-2), 6.3e-7 down to 2^-8, ..., 7.8e-6 below 2^-64).
+// Distance of k~ to the exact-arithmetic value, term by term: 6.4e-7 (the
+// cube roots, above); (ln 2 / 6) (1 - K^2) (2.3e-7 + lg2 error) for r and
+// d, at most 8.1e-8 (on [2^-5, 2^-4)) since 1 - K^2 <= 4 s / (1 + s)^2
+// falls faster than the lg2 error grows; 4.0e-8 (the product by -1/3, also
+// damped); 7.2e-8 (ex2, through the slope 2 s / (1 + s)^2 <= 1/2); 3u +
+// 9.9e-8 (the last three operations).  With the reference's 3u: 1.29e-6 in
+// all, below DELTA less the rounding of k~ +- DELTA (6e-8).
+//
+// Other operands.  A ratio below 2^-126 flushes to 0 and gives k~ = 1; the
+// cube roots then differ by a factor above 2^41, and K is 1 exactly.  Both
+// zero: k~ = 0 = K.  One zero and the other >= 2^-60: k~ = 1 (r = 0) and K
+// >= 1 - 2 acbrt1(0) / acbrt1(2^-60) - 3u > 1 - 4e-7.  No enclosure (the
+// value is always computed exactly): a subnormal operand, a zero beside a
+// value below 2^-60, and a larger operand >= 2^126 (its rcp.approx flushes).
+constexpr float KS3_DELTA = 1.5e-6f;
+
+__device__ __forceinline__ float lg2_approx(float x) {
+  float y;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+// Enclosure [lo, hi] of keep_sign_3d(P, N) for finite P, N >= 0 ([-1, 2]
+// where there is none: every K lies in [0, 1]).  On non-negative floats the
+// order of the bit patterns is the order of the values.
+__device__ __forceinline__ void ks3_enclose(float P, float N, float& lo, float& hi) {
+  const unsigned bp = __float_as_uint(P), bn = __float_as_uint(N);
+  const unsigned mn = umin(bp, bn), mx = umax(bp, bn);
+  const float r = __uint_as_float(mn) * rcp_approx(__uint_as_float(mx));
+  const float d = fabsf(lg2_approx(r));
+  const float s = ex2_approx(d * -0.333333343f);
+  const float k = mx == 0u ? 0.f : (1.f - s) * rcp_approx(1.f + s);
+  const bool known = (mn >= 0x00800000u && mx < 0x7e800000u) || (mn == 0u && (mx == 0u || mx >= (67u << 23)));
+  lo = known ? k - KS3_DELTA : -1.f;
+  hi = known ? k + KS3_DELTA : 2.f;
+}
+
 __device__ __forceinline__ int sgnf(float v) { return (0.0f < v) - (v < 0.0f); }
 __device__ __forceinline__ bool same_direction(float a, float b, float c, float d) {
   int s = sgnf(a);
@@ -350,7 +418,7 @@ __device__ __forceinline__ bool quotient_above_one(double M, double Mi) {
   return (a - b) * 9007199254740992.0 > b;
 }
 
-static __device__ __noinline__ double tet_eb(float u0, float u1, float u2, float u3, float v0, float v1, float v2, float v3,
+static __device__ __forceinline__ double tet_eb(float u0, float u1, float u2, float u3, float v0, float v1, float v2, float v3,
                                       float w0, float w1, float w2, float w3) {
   double u3v1w2 = u3 * v1 * w2, u3v2w1 = u3 * v2 * w1, u3v2w0 = u3 * v2 * w0, u3v0w2 = u3 * v0 * w2,
          u3v0w1 = u3 * v0 * w1, u3v1w0 = u3 * v1 * w0;
@@ -398,26 +466,54 @@ static __device__ __noinline__ double tet_eb(float u0, float u1, float u2, float
   if (isfinite(sp0) && isfinite(sp1) && isfinite(sp2) && isfinite(sp3) && isfinite(sn0) && isfinite(sn1) &&
       isfinite(sn2) && isfinite(sn3)) {
     // Every magnitude is finite (each appears in three of the sums), so every
-    // keep_sign_3d value is a finite non-negative float and MAX/MINF are plain
-    // max/min: a flag whose first bound cannot raise eb leaves it unchanged,
-    // and its second bound need not be evaluated.
-    if (!flag0) {
-      const float e1 = keep_sign_3d_nonneg(p_m0, n_m0);
-      if (e1 > eb) eb = maxf_(eb, minf_(e1, keep_sign_3d_nonneg(sp0, sn0)));
+    // keep_sign_3d value is a finite float in [0, 1] and MAX/MINF are plain
+    // max/min: eb = max(0, max over unflagged i of min(A_i, B_i)), A_i =
+    // K(p_i, n_i), B_i = K(sp_i, sn_i).  With enclosures of all eight
+    // values, a minor whose min cannot reach the largest lower bound of a
+    // min is dropped, and of a kept minor only a value that can be its min
+    // is computed (value 2i + side is bit 2i + side of `need`).
+    float lo[8], hi[8];
+    ks3_enclose(p_m0, n_m0, lo[0], hi[0]);
+    ks3_enclose(sp0, sn0, lo[1], hi[1]);
+    ks3_enclose(p_m1, n_m1, lo[2], hi[2]);
+    ks3_enclose(sp1, sn1, lo[3], hi[3]);
+    ks3_enclose(p_m2, n_m2, lo[4], hi[4]);
+    ks3_enclose(sp2, sn2, lo[5], hi[5]);
+    ks3_enclose(p_m3, n_m3, lo[6], hi[6]);
+    ks3_enclose(sp3, sn3, lo[7], hi[7]);
+    const bool unf[4] = {!flag0, !flag1, !flag2, !flag3};
+    float LO = -2.f;  // a lower bound of the result
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+      if (unf[i]) LO = fmaxf(LO, fminf(lo[2 * i], lo[2 * i + 1]));
+    unsigned need = 0;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      if (!unf[i] || fminf(hi[2 * i], hi[2 * i + 1]) < LO) continue;
+      if (lo[2 * i] <= hi[2 * i + 1]) need |= 1u << (2 * i);          // A_i can be the min
+      if (lo[2 * i + 1] <= hi[2 * i]) need |= 1u << (2 * i + 1);      // B_i can be the min
     }
-    if (!flag1) {
-      const float e1 = keep_sign_3d_nonneg(p_m1, n_m1);
-      if (e1 > eb) eb = maxf_(eb, minf_(e1, keep_sign_3d_nonneg(sp1, sn1)));
+    // one exact evaluation per set bit, in ascending order (a minor's two
+    // values are adjacent): the min within a minor, the max across minors
+    float cur = 0.f;
+    int cur_i = -1;
+    while (need) {
+      const int k = __ffs(need) - 1;
+      need &= need - 1;
+      const float P = (k & 4) ? ((k & 2) ? ((k & 1) ? sp3 : p_m3) : ((k & 1) ? sp2 : p_m2))
+                              : ((k & 2) ? ((k & 1) ? sp1 : p_m1) : ((k & 1) ? sp0 : p_m0));
+      const float N = (k & 4) ? ((k & 2) ? ((k & 1) ? sn3 : n_m3) : ((k & 1) ? sn2 : n_m2))
+                              : ((k & 2) ? ((k & 1) ? sn1 : n_m1) : ((k & 1) ? sn0 : n_m0));
+      const float v = keep_sign_3d_nonneg(P, N);
+      if ((k >> 1) != cur_i) {
+        eb = maxf_(eb, cur);
+        cur = v;
+        cur_i = k >> 1;
+      } else {
+        cur = minf_(cur, v);
+      }
     }
-    if (!flag2) {
-      const float e1 = keep_sign_3d_nonneg(p_m2, n_m2);
-      if (e1 > eb) eb = maxf_(eb, minf_(e1, keep_sign_3d_nonneg(sp2, sn2)));
-    }
-    if (!flag3) {
-      const float e1 = keep_sign_3d_nonneg(p_m3, n_m3);
-      if (e1 > eb) eb = maxf_(eb, minf_(e1, keep_sign_3d_nonneg(sp3, sn3)));
-    }
-    return eb;
+    return maxf_(eb, cur);
   }
   if (!flag0) eb = maxf_(eb, minf_(keep_sign_3d(p_m0, n_m0), keep_sign_3d(sp0, sn0)));
   if (!flag1) eb = maxf_(eb, minf_(keep_sign_3d(p_m1, n_m1), keep_sign_3d(sp1, sn1)));

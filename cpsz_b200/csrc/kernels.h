@@ -178,6 +178,10 @@ int launch_eb3d(cpsz_b200_ctx* ctx, const float* U, const float* V, const float*
 // sign_words 32-bit words.
 int launch_log3d(cpsz_b200_ctx* ctx, const float* U, const float* V, const float* W, const uint8_t* id_q, size_t n,
                  const LibmFn& L, float4* pairs, uint32_t* signs, size_t sign_words);
+// Exhaustive maxima of the operations the filtered bounds rely on
+// (selfcheck.cu), FP_COUNT floats as bit patterns in d_out (device).
+enum FilterPremise { FP_ACBRT_HI = 0, FP_ACBRT_LO = 1, FP_RCP = 2, FP_EX2 = 3, FP_SQRT = 4, FP_LG2 = 5, FP_COUNT = 132 };
+int launch_filter_premises(cpsz_b200_ctx* ctx, unsigned* d_out);
 // Host-library log2f (which 0) / exp2f (which 1) of n device floats.
 int launch_libm_eval(cpsz_b200_ctx* ctx, int which, const float* in, size_t n, const LibmTables& L, float* out);
 // Raster compaction in chunks: chunk_count() chunks; counts of predicted

@@ -257,6 +257,15 @@ int cpsz_b200_debug_libm(cpsz_b200_ctx* ctx, int which, const float* in, size_t 
  * row above, spins waiting for ring credit}.  With out != NULL, copies len
  * counters out. */
 int cpsz_b200_debug_wave_trace(cpsz_b200_ctx* ctx, size_t len, long long* out);
+/* Exhaustive maxima, measured on this device, of the operations whose error
+ * bounds the filtered 2D / 3D bound evaluations rely on (no reference
+ * counterpart): out[0] / out[1] the largest relative error of the
+ * reference's acbrt1 cube root above / below a double cube root over all
+ * positive normal floats; out[2] rcp.approx.ftz.f32 (relative, normal floats
+ * below 2^126); out[3] ex2.approx.ftz.f32 (relative, [-87, 0]); out[4]
+ * sqrt.approx.f32 (relative, positive normal floats); out[5 + e + 126]
+ * lg2.approx.ftz.f32 (absolute) on [2^e, 2^(e+1)), e = -126..0.  n >= 132. */
+int cpsz_b200_debug_filter_premises(cpsz_b200_ctx* ctx, double* out, size_t n);
 /* Host-computed quantization thresholds (which = 2 or 3): t[k] is the smallest
  * bound with id >= k under the host libm's log2 (256 doubles). */
 int cpsz_b200_debug_quant_table(int which, double* t, int* n);
