@@ -197,12 +197,14 @@ int launch_compact3d(cpsz_b200_ctx* ctx, const ushort4* codes, uint8_t* ids, con
 // flag) for the others.  Short streams raise FLAG_RAW_RANGE.
 int launch_prep3d(cpsz_b200_ctx* ctx, const uint8_t* ids, size_t n, const unsigned* chunk_off, const uint16_t* codes,
                   size_t n_codes, const float* unpred, size_t n_unpred, float4* pairs);
-// Lorenzo recursion, one launch per anti-diagonal plane.  Compress: in =
+// Lorenzo recursion in one persistent launch (wave3d.cu).  Compress: in =
 // log3d pairs, codes out (0,0,0 for unpredictable points).  Decompress: in =
-// prep3d pairs, decoded U, V, W out.  rec: reconstructed log values (scratch).
-int launch_wave3d_planes(cpsz_b200_ctx* ctx, bool decompress, const float4* in, float4* rec, ushort4* codes,
-                         const uint8_t* signs, size_t sign_bytes, const LibmTables* L, float* U, float* V, float* W,
-                         int r1, int r2, int r3);
+// prep3d pairs, decoded U, V, W out.  rec: reconstructed log values
+// (scratch); scratch: wave3d_scratch_bytes(r1, r2) of device memory.
+size_t wave3d_scratch_bytes(int r1, int r2);
+int launch_wave3d(cpsz_b200_ctx* ctx, bool decompress, const float4* in, float4* rec, ushort4* codes,
+                  const uint8_t* signs, size_t sign_bytes, const LibmTables* L, float* U, float* V, float* W, int r1,
+                  int r2, int r3, void* scratch);
 
 // ---- exact critical-point checker -----------------------------------------------------
 // Per-cell CP codes of field a (0 none, 1 + type) into `cells` (optional,

@@ -84,6 +84,7 @@ int compress_3d(cpsz_b200_ctx* ctx, const float* U_in, const float* V_in, const 
   add(6 * N);          // compacted codes
   add(12 * N);         // unpredictable triples
   add(3 * sign_words * 4);
+  add(wave3d_scratch_bytes(r1, r2));
   add(256 * 8);
   add(65536 * 8);
   add(QUANT_TAB_MAX * 8);
@@ -127,6 +128,7 @@ int compress_3d(cpsz_b200_ctx* ctx, const float* U_in, const float* V_in, const 
   uint16_t* codes_out = (uint16_t*)A(6 * N);
   float* unpred = (float*)A(12 * N);
   uint32_t* signs = (uint32_t*)A(3 * sign_words * 4);
+  void* wave_sync = A(wave3d_scratch_bytes(r1, r2));
   unsigned long long* hist_ids = (unsigned long long*)A(256 * 8);
   unsigned long long* hist_codes = (unsigned long long*)A(65536 * 8);
   double* thr_tab = (double*)A(QUANT_TAB_MAX * 8);
@@ -149,8 +151,8 @@ int compress_3d(cpsz_b200_ctx* ctx, const float* U_in, const float* V_in, const 
   mark(ctx, "log3d");
   CPSZ_TRY(launch_log3d(ctx, dU, dV, dW, ids, N, lt.log2f, pairs, signs, sign_words));
   mark(ctx, "wave3d_compress");
-  CPSZ_TRY(launch_wave3d_planes(ctx, false, pairs, rec, codes, nullptr, 0, &lt, nullptr, nullptr, nullptr, r1, r2,
-                                r3));
+  CPSZ_TRY(launch_wave3d(ctx, false, pairs, rec, codes, nullptr, 0, &lt, nullptr, nullptr, nullptr, r1, r2, r3,
+                          wave_sync));
   mark(ctx, "compact+hist");
   CPSZ_TRY(launch_chunk_count_3d(ctx, true, codes, N, chunk_cnt));
   CPSZ_TRY(launch_scan_u32(ctx, chunk_cnt, chunk_off, nchunks, scan_tmp));
@@ -321,6 +323,7 @@ int decompress_3d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
   add(scan_u32_tmp_bytes(nchunks));
   add(16 * N);
   add(16 * N);
+  add(wave3d_scratch_bytes(r1, r2));
   CPSZ_TRY(arena_reserve(ctx, bytes));
   CPSZ_TRY(pinned_reserve(ctx, 4096));
   auto A = [&](size_t b) { return arena_alloc(ctx, b); };
@@ -362,7 +365,8 @@ int decompress_3d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
   void* scan_tmp = A(scan_u32_tmp_bytes(nchunks));
   float4* pairs = (float4*)A(16 * N);
   float4* rec = (float4*)A(16 * N);
-  if (!rec) return set_error(CPSZ_ERR_NOMEM, "workspace layout overflow");
+  void* wave_sync = A(wave3d_scratch_bytes(r1, r2));
+  if (!wave_sync) return set_error(CPSZ_ERR_NOMEM, "workspace layout overflow");
   CPSZ_CUDA_TRY(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), st));
   CPSZ_TRY(h2d(ctx, signs, blob + 8, 3 * smap, st));
   if (n_unpred) CPSZ_TRY(h2d(ctx, unpred, blob + unpred_at, 4 * n_unpred, st));
@@ -375,7 +379,7 @@ int decompress_3d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
   CPSZ_TRY(launch_scan_u32(ctx, chunk_cnt, chunk_off, nchunks, scan_tmp));
   CPSZ_TRY(launch_prep3d(ctx, ids, N, chunk_off, codes, n_codes, unpred, n_unpred, pairs));
   mark(ctx, "wave3d_decompress");
-  CPSZ_TRY(launch_wave3d_planes(ctx, true, pairs, rec, nullptr, signs, smap, &lt, dU, dV, dW, r1, r2, r3));
+  CPSZ_TRY(launch_wave3d(ctx, true, pairs, rec, nullptr, signs, smap, &lt, dU, dV, dW, r1, r2, r3, wave_sync));
   mark(ctx, "d2h");
   if (!dev_out) {
     CPSZ_TRY(d2h(ctx, U_out, dU, 4 * N, st));
