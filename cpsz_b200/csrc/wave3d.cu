@@ -21,7 +21,7 @@
 //    below) hold smaller tickets, taken by CTAs that are already running:
 //    every wait ends;
 //  * a unit publishes its progress (steps done by all its planes) every
-//    W3_PUB steps after a fence.  Step t's loads need the unit of the planes
+//    W3_PUB steps: after the step barrier one thread fences and stores it.  Step t's loads need the unit of the planes
 //    below at >= t + P + 1 and the unit of the rows below at >= t + 33; the
 //    latter covers the unit below and behind, which that unit waited for;
 //  * loads go through L2 (cp.async.cg: another SM's writes must not meet a
@@ -208,6 +208,11 @@ __global__ void __launch_bounds__(W3_THREADS, 1) wave3d_kernel(const W3Args a) {
     for (int tp = 0; tp < W3_DIN; tp++) issue_in(tp);
     for (int tp = -3; tp < W3_DD; tp++) issue_dep(tp);
     cp_commit();
+    // W3_DD empty groups stand for steps -W3_DD .. -1, so that the wait of
+    // step t (all but the newest W3_DD groups) covers the prologue's group
+    // from step 0 on
+#pragma unroll
+    for (int e = 0; e < W3_DD; e++) cp_commit();
 #pragma unroll 1
     for (int t = 0; t < t_end; t++) {
       // step t reads slots t-1 .. t-3 and input slot t: slot t-1 came with the
@@ -216,7 +221,12 @@ __global__ void __launch_bounds__(W3_THREADS, 1) wave3d_kernel(const W3Args a) {
       wait_for(t + W3_DD);
       cp_wait<W3_DD>();
       __syncthreads();
-      if (threadIdx.x == 0 && t > 0 && (t % W3_PUB == 0)) st_release_s32(prog + u, t);
+      // every plane has finished step t-1 (the barrier above): thread 0's fence
+      // makes the CTA's writes visible before its progress
+      if (threadIdx.x == 0 && t > 0 && (t % W3_PUB == 0)) {
+        __threadfence();
+        st_release_s32(prog + u, t);
+      }
       issue_in(t + W3_DIN);
       issue_dep(t + W3_DD);
       cp_commit();
@@ -285,12 +295,13 @@ __global__ void __launch_bounds__(W3_THREADS, 1) wave3d_kernel(const W3Args a) {
         if (act) a.rec[idx] = res;
       }
       M.ring[p + 1][t % W3_SR][lane + 1] = act ? res : Z;
-      if ((t + 1) % W3_PUB == 0) __threadfence();  // published at the next step's barrier
     }
     asm volatile("cp.async.wait_all;" ::: "memory");  // no copy into the rings is left in flight
-    __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) st_release_s32(prog + u, t_end);
+    if (threadIdx.x == 0) {
+      __threadfence();
+      st_release_s32(prog + u, t_end);
+    }
   }
 }
 

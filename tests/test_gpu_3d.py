@@ -129,6 +129,28 @@ def test_gpu_3d_device_arrays(ctx, oracle):
         assert_bits_equal(x.cpu().numpy(), y)
 
 
+def test_gpu_3d_repeatable(ctx, oracle):
+    """The persistent wavefront's units run in whatever order the GPU
+    schedules them; every run must give the oracle's blob and decode.  Many
+    runs of one field (rows not a multiple of 32, a partial last plane group)
+    would expose a read of a ring entry or input that has not landed, or of
+    another unit's output before it was published."""
+    torch = pytest.importorskip("torch")
+    U, V, Wf = W.field_3d(23, 61, 97, 101, 10, 7.0)
+    ref = oracle.compress_3d(U, V, Wf, 0.05)
+    d = [torch.from_numpy(a).cuda() for a in (U, V, Wf)]
+    out = torch.zeros(len(ref) + 65536, dtype=torch.uint8, device="cuda")
+    for _ in range(16):
+        n = cpsz_b200.compress_3d_into(*d, *U.shape, 0.05, out, ctx=ctx)
+        assert n == len(ref) and out[:n].cpu().numpy().tobytes() == ref
+    dec = oracle.decompress_3d(ref, *U.shape)
+    outs = [torch.empty(U.shape, dtype=torch.float32, device="cuda") for _ in range(3)]
+    for _ in range(8):
+        cpsz_b200.sz_decompress_cp_preserve_3d_online_log(ref, *U.shape, *outs, ctx=ctx)
+        for x, y in zip(outs, dec):
+            assert_bits_equal(x.cpu().numpy(), y)
+
+
 def test_gpu_3d_rejects_bad_input(ctx):
     U, V, Wf = W.field_3d(1, 6, 6, 6, 2, 3.0)
     blob = cpsz_b200.sz_compress_cp_preserve_3d_offline_log(U, V, Wf, max_pwr_eb=0.1, ctx=ctx)
