@@ -507,15 +507,26 @@ def run_batch(args, rank, world, device):
     ev1.record(stream)
     torch.cuda.synchronize(device)
     per_field_ms = ev0.elapsed_time(ev1)
-    # end to end through the sharded call: host fields in, blobs back in host memory
+    # end to end through the sharded call: fields in pinned host memory, blobs
+    # back into a pinned host buffer (the batched call writes them back to back)
     shapes = [(r1, r2) for r1, r2, _, _ in lay]
     all_ebs = [e for *_, e in lay]
     pos = {k: i for i, k in enumerate(own)}
-    res = shard.compress_2d_batch_sharded(shapes, all_ebs, lambda k: fields[pos[k]], ctx=ctx)
+    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()
+    h_fields = [(pin(U), pin(V)) for U, V in fields]
+    h_out = torch.empty(raw + (256 << 20), dtype=torch.uint8).pin_memory().numpy()
+
+    def pinned_compress(fs, es):
+        offs = cpsz_b200.compress_2d_batch(fs, es, out=h_out, ctx=ctx)
+        return [h_out[int(offs[q]):int(offs[q + 1])] for q in range(len(fs))]
+
+    res = shard.compress_2d_batch_sharded(shapes, all_ebs, lambda k: h_fields[pos[k]], ctx=ctx,
+                                          compress=pinned_compress)
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
-    res = shard.compress_2d_batch_sharded(shapes, all_ebs, lambda k: fields[pos[k]], ctx=ctx)
+    res = shard.compress_2d_batch_sharded(shapes, all_ebs, lambda k: h_fields[pos[k]], ctx=ctx,
+                                          compress=pinned_compress)
     e2e_ms = (time.perf_counter() - t0) * 1e3
     if world > 1:
         t = torch.tensor([e2e_ms], device=f"cuda:{device}")
@@ -532,7 +543,7 @@ def run_batch(args, rank, world, device):
         "ratio_pre_zstd": round(raw_all / total_blob, 4),
         "per_field_calls_GBps": round(raw / (per_field_ms / 1e3) / 1e9, 3),
         "e2e": {"value": round(raw_all / (e2e_ms / 1e3) / 1e9, 3), "unit": "GB/s", "h2d_bytes_per_step": raw,
-                "d2h_bytes_per_step": blob_bytes, "host_input": "pageable numpy arrays"},
+                "d2h_bytes_per_step": blob_bytes, "host_input": "pinned host memory"},
         "cpu_baseline": None, "clocks": clk.summary(), "gpu_launches": launches,
     }
 

@@ -42,7 +42,7 @@ SWEEP = {
     "wave2d.overlap": ("2d", "eb2d+wave2d_compress", [0, 1], 0),
     "eb2d.tile": ("2d", "eb2d+wave2d_compress", [0, 1, 2, 3, 4, 5], 0),
     "wave2d.ctas_per_sm": ("2d", "wave2d_compress", [0, 1, 2, 3, 4], 0),
-    "h2d.chunks": ("2d_host", "e2e", [1, 2, 4, 8], 1 << 22),
+    "h2d.chunks": ("2d_host", "e2e", [1, 2, 4, 8, 16, 24, 32], 1 << 22),
     "eb3d.fill": ("3d", "eb3d", [1, 2, 4, 8, 16], 0),
     "eb3d.min_chunk": ("3d", "eb3d", [4, 8, 16, 32], 0),
 }

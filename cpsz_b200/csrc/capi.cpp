@@ -66,6 +66,13 @@ int cpsz_b200_compress_2d_offline_f32_into(cpsz_b200_ctx* ctx, const float* U, c
   if (!out || !blob_size) return set_error(CPSZ_ERR_INVALID, "null output pointer");
   RESOLVE(ctx);
   Blob2D b;
+  if (host_kind(out) != HOST_DEVICE) {
+    // host memory: the sections are written there as they are produced
+    CPSZ_TRY(compress_2d(ctx, U, V, r1, r2, max_pwr_eb, &b, nullptr, nullptr, out, out_cap));
+    *blob_size = b.size;
+    CPSZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return CPSZ_OK;
+  }
   CPSZ_TRY(compress_2d(ctx, U, V, r1, r2, max_pwr_eb, &b, nullptr));
   *blob_size = b.size;
   if (b.size > out_cap) return set_error(CPSZ_ERR_INVALID, "output capacity %zu < blob size %zu", out_cap, b.size);

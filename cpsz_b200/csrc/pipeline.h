@@ -30,9 +30,12 @@ struct StageTap {
 int build_wave_items(int nfields, const int* r1s, std::vector<WaveItem>& items);
 
 // eb_ext (optional, device, N doubles): per-vertex bounds to quantize instead
-// of the derived ones (the learned-bound path).
+// of the derived ones (the learned-bound path).  host_out (optional, host
+// memory of host_cap bytes): the blob is written there directly (out->d_blob
+// is then not set).
 int compress_2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2, double max_pwr_eb,
-                Blob2D* out, const StageTap* tap, const double* eb_ext = nullptr);
+                Blob2D* out, const StageTap* tap, const double* eb_ext = nullptr, unsigned char* host_out = nullptr,
+                size_t host_cap = 0);
 int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_size, size_t r1, size_t r2, float* U,
                   float* V);
 // n fields; blobs back to back into `out` (host or device), offsets[0..n].

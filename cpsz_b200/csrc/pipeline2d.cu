@@ -91,6 +91,10 @@ struct Job2D {
   size_t n_unpred[2] = {0, 0};
   size_t sec_bytes[3] = {0, 0, 0}, bits_bytes[3] = {0, 0, 0};
   size_t size = 0;  // blob bytes
+  // host output: the blob is written straight into host memory (sections
+  // copied from their device buffers), not assembled in device memory
+  unsigned char* host_out = nullptr;
+  size_t host_cap = 0;
 };
 
 int read_flag(cpsz_b200_ctx* ctx, int* out) {
@@ -225,20 +229,33 @@ int job_alloc(cpsz_b200_ctx* ctx, Job2D& j) {
 // Blob assembly of one field in device memory (header, id tree, two field
 // blobs); the small host-made pieces go up in one copy and are scattered
 // with device-to-device copies.
-int job_assemble(cpsz_b200_ctx* ctx, Job2D& j) {
-  cudaStream_t st = ctx->stream;
+// The reference's 2D blob (sz_compress_cp_preserve_2d_offline,
+// src/sz_compress_cp_preserve_2d.cpp): header, the id stream's Huffman
+// section, then per component its header, unpredictable floats, the all-zero
+// block indicator and the code stream's Huffman section.  Every small piece is
+// staged in `small`; the bit streams and unpredictable floats go to bit_dst /
+// unpred_dst.
+struct BlobLayout {
+  struct Piece {
+    size_t dst, src, n;
+  };
+  size_t total = 0, bit_dst[3] = {0, 0, 0}, unpred_dst[2] = {0, 0};
+  std::vector<uint8_t> small;
+  std::vector<Piece> pieces;
+};
+
+// offset of the id stream's bits (known once the id tree is)
+size_t ids_bits_at(const Job2D& j) { return BLOB_HDR + j.cb[0].tree_bytes.size() + 8; }
+
+int job_layout(const Job2D& j, BlobLayout& L) {
   const size_t ind_bytes = (j.nblocks + 7) / 8;
   size_t field_size[2];
   for (int f = 0; f < 2; f++) field_size[f] = FIELD_HDR + 4 * j.n_unpred[f] + ind_bytes + j.sec_bytes[1 + f];
   const size_t total = BLOB_HDR + j.sec_bytes[0] + field_size[0] + field_size[1];
-  if (total > j.blob_cap) return set_error(CPSZ_ERR_UNSUPPORTED, "blob larger than its bound");
-  std::vector<uint8_t> small;
-  struct Piece {
-    size_t dst, src, n;
-  };
-  std::vector<Piece> pieces;
+  L.total = total;
+  std::vector<uint8_t>& small = L.small;
   auto stage = [&](size_t dst, const void* p, size_t n) {
-    pieces.push_back(Piece{dst, small.size(), n});
+    L.pieces.push_back(BlobLayout::Piece{dst, small.size(), n});
     small.insert(small.end(), (const uint8_t*)p, (const uint8_t*)p + n);
   };
   {
@@ -253,7 +270,8 @@ int job_assemble(cpsz_b200_ctx* ctx, Job2D& j) {
     stage(0, hdr, BLOB_HDR);
   }
   size_t at = BLOB_HDR;
-  size_t bit_dst[3], unpred_dst[2];
+  size_t* bit_dst = L.bit_dst;
+  size_t* unpred_dst = L.unpred_dst;
   auto stage_huff = [&](int k) {
     stage(at, j.cb[k].tree_bytes.data(), j.cb[k].tree_bytes.size());
     at += j.cb[k].tree_bytes.size();
@@ -283,15 +301,28 @@ int job_assemble(cpsz_b200_ctx* ctx, Job2D& j) {
     stage_huff(1 + f);
   }
   if (at != total) return set_error(CPSZ_ERR_INVALID, "internal: blob layout mismatch (%zu != %zu)", at, total);
+  return CPSZ_OK;
+}
+
+int job_assemble(cpsz_b200_ctx* ctx, Job2D& j) {
+  cudaStream_t st = ctx->stream;
+  BlobLayout L;
+  CPSZ_TRY(job_layout(j, L));
+  const size_t total = L.total;
+  if (total > j.blob_cap) return set_error(CPSZ_ERR_UNSUPPORTED, "blob larger than its bound");
+  const std::vector<uint8_t>& small = L.small;
+  const std::vector<BlobLayout::Piece>& pieces = L.pieces;
+  const size_t* bit_dst = L.bit_dst;
+  const size_t* unpred_dst = L.unpred_dst;
   uint8_t* blob = j.d.blob;
   uint8_t* d_small = blob + align_up(total, 256);
   if (align_up(total, 256) + small.size() > j.blob_cap) {
-    for (const Piece& p : pieces)
+    for (const BlobLayout::Piece& p : pieces)
       CPSZ_CUDA_TRY(cudaMemcpyAsync(blob + p.dst, small.data() + p.src, p.n, cudaMemcpyHostToDevice, st));
   } else {
     // pageable source: the runtime stages it before returning, so `small` may go
     CPSZ_CUDA_TRY(cudaMemcpyAsync(d_small, small.data(), small.size(), cudaMemcpyHostToDevice, st));
-    for (const Piece& p : pieces)
+    for (const BlobLayout::Piece& p : pieces)
       CPSZ_CUDA_TRY(cudaMemcpyAsync(blob + p.dst, d_small + p.src, p.n, cudaMemcpyDeviceToDevice, st));
   }
   for (int k = 0; k < 3; k++)
@@ -410,17 +441,19 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       // Host input: row chunks go up on the second stream and the bound kernel
       // runs band by band as soon as a band's rows and the row below it are
       // on the device, so the transfer overlaps the bound derivation.  Bands
-      // start on wavefront group boundaries.
+      // start on wavefront group boundaries.  Chunk c carries its band's rows
+      // and the next band's first row (which chunk c + 1 writes again, with
+      // the same bytes), so band c waits for chunk c alone and only the last
+      // band's bounds follow the end of the transfer.
       const int K = (j.N >= ((size_t)1 << 22) && !j.eb_ext) ? tune_get(TUNE_H2D_CHUNKS, j.N) : 1;
       const int R = (int)align_up((size_t)(j.r1 + K - 1) / K, WAVE_GROUP_ROWS);
       const int nch = (j.r1 + R - 1) / R;
-      // band c needs chunks c and c + 1; it is enqueued right after chunk
-      // c + 1's copy call (a copy from pageable memory returns only once the
-      // host has staged it, so enqueueing every copy first would hold the
-      // bands back until the whole field was staged)
+      // band c is enqueued right after chunk c's copy call (a copy from
+      // pageable memory returns only once the host has staged it, so
+      // enqueueing every copy first would hold the bands back until the whole
+      // field was staged)
       auto band_launch = [&](int c) -> int {
         CPSZ_CUDA_TRY(cudaStreamWaitEvent(st, ctx->up_ev[c], 0));
-        if (c + 1 < nch) CPSZ_CUDA_TRY(cudaStreamWaitEvent(st, ctx->up_ev[c + 1], 0));
         if (j.eb_ext)
           return launch_quant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
                                 j.d.hist_ids, j.d.pairs[0], j.d.pairs[1]);
@@ -429,13 +462,12 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       };
       for (int c = 0; c < nch; c++) {
         const size_t off = (size_t)c * R * j.r2;
-        const size_t cnt = (size_t)(std::min(j.r1, (c + 1) * R) - c * R) * j.r2;
+        const size_t cnt = (size_t)(std::min(j.r1, (c + 1) * R + 1) - c * R) * j.r2;
         CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.U + off, j.U_in + off, 4 * cnt, cudaMemcpyHostToDevice, ctx->aux));
         CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.V + off, j.V_in + off, 4 * cnt, cudaMemcpyHostToDevice, ctx->aux));
         CPSZ_CUDA_TRY(cudaEventRecord(ctx->up_ev[c], ctx->aux));
-        if (c >= 1) CPSZ_TRY(band_launch(c - 1));
+        CPSZ_TRY(band_launch(c));
       }
-      CPSZ_TRY(band_launch(nch - 1));
     }
     CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_hist_ids, j.d.hist_ids, 256 * 8, cudaMemcpyDeviceToHost, st));
   }
@@ -479,7 +511,15 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_nunpred + f, strip_total(j.d.strip[f], j.r1, j.r2), 4,
                                     cudaMemcpyDeviceToHost, st));
   }
+  CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[5], st));  // the unpredictable counts are on the host
   mark(ctx, "host_trees");
+  // Host output (one field): the sections are copied from their device
+  // buffers straight into the caller's memory, each right after its producer
+  // when that memory is page-locked (the copies then overlap the rest), else
+  // once everything is done; no blob is assembled in device memory.
+  Job2D* hj = (nj == 1 && jobs[0].host_out) ? &jobs[0] : nullptr;
+  const bool h_async = hj && host_kind(hj->host_out) == HOST_PINNED;
+  BlobLayout hl;
 
   // host: the id trees (their histograms arrived while the wavefront ran) and
   // their bit packing, which the GPU runs right after stage 3 while the host
@@ -503,6 +543,12 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     CPSZ_TRY(launch_huff_encode_u8(ctx, j.d.ids, 2 * j.N, true, HuffEncTable{j.d.enc_code[0], j.d.enc_len[0], 256},
                                    j.d.bits[0], j.ids_bits_cap, nullptr, j.d.enc_tmp[0]));
   }
+  if (h_async) {
+    const size_t at = ids_bits_at(*hj);
+    if (at + hj->bits_bytes[0] > hj->host_cap)
+      return set_error(CPSZ_ERR_INVALID, "output capacity %zu too small for the blob", hj->host_cap);
+    CPSZ_TRY(d2h(ctx, hj->host_out + at, hj->d.bits[0], hj->bits_bytes[0], st));
+  }
   // code trees, each as soon as its histogram is on the host
   parallel_for(2 * nj, [&](int q) {
     Job2D& j = jobs[q / 2];
@@ -520,12 +566,30 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       j.bits_bytes[k] = (j.cb[k].total_bits + 7) / 8;
       if (j.bits_bytes[k] + 8 > j.codes_bits_cap)
         return set_error(CPSZ_ERR_UNSUPPORTED, "Huffman stream larger than its bound");
+    }
+  }
+  if (hj) {
+    // every section size is known: lay the blob out in the caller's memory
+    CPSZ_CUDA_TRY(cudaEventSynchronize(ctx->ev[5]));
+    hj->n_unpred[0] = hj->h_nunpred[0];
+    hj->n_unpred[1] = hj->h_nunpred[1];
+    CPSZ_TRY(job_layout(*hj, hl));
+    if (hl.total > hj->host_cap)
+      return set_error(CPSZ_ERR_INVALID, "output capacity %zu < blob size %zu", hj->host_cap, hl.total);
+    for (const BlobLayout::Piece& pc : hl.pieces) memcpy(hj->host_out + pc.dst, hl.small.data() + pc.src, pc.n);
+    if (h_async)
+      for (int f = 0; f < 2; f++)
+        CPSZ_TRY(d2h(ctx, hj->host_out + hl.unpred_dst[f], hj->d.unpred[f], 4 * hj->n_unpred[f], st));
+  }
+  for (Job2D& j : jobs) {
+    for (int k = 1; k < 3; k++) {
       CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.enc_code[k], j.cb[k].code.data(), 65536 * 8, cudaMemcpyHostToDevice, st));
       CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.enc_len[k], j.cb[k].len.data(), 65536, cudaMemcpyHostToDevice, st));
       CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.bits[k], 0, align_up(j.bits_bytes[k], 4) + 8, st));
       CPSZ_TRY(launch_huff_encode_u16(ctx, j.d.cblocks[k - 1], j.N,
                                       HuffEncTable{j.d.enc_code[k], j.d.enc_len[k], 65536}, j.d.bits[k],
                                       j.codes_bits_cap, nullptr, j.d.enc_tmp[k]));
+      if (h_async) CPSZ_TRY(d2h(ctx, j.host_out + hl.bit_dst[k], j.d.bits[k], j.bits_bytes[k], st));
     }
   }
   {
@@ -538,9 +602,20 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     j.n_unpred[1] = j.h_nunpred[1];
   }
 
-  // ---- stage 5: blob assembly in device memory ----
+  // ---- stage 5: blob assembly in device memory (or, for host output, the
+  // sections not yet copied) ----
   mark(ctx, "blob_assembly");
-  for (Job2D& j : jobs) CPSZ_TRY(job_assemble(ctx, j));
+  if (hj) {
+    if (!h_async) {
+      CPSZ_TRY(d2h(ctx, hj->host_out + hl.bit_dst[0], hj->d.bits[0], hj->bits_bytes[0], st));
+      for (int f = 0; f < 2; f++)
+        CPSZ_TRY(d2h(ctx, hj->host_out + hl.unpred_dst[f], hj->d.unpred[f], 4 * hj->n_unpred[f], st));
+      for (int k = 1; k < 3; k++) CPSZ_TRY(d2h(ctx, hj->host_out + hl.bit_dst[k], hj->d.bits[k], hj->bits_bytes[k], st));
+    }
+    hj->size = hl.total;
+  } else {
+    for (Job2D& j : jobs) CPSZ_TRY(job_assemble(ctx, j));
+  }
   mark(ctx, "end");
   if (tap) {
     Job2D& j = jobs[0];
@@ -580,14 +655,16 @@ int build_wave_items(int nfields, const int* r1s, std::vector<WaveItem>& items) 
 }
 
 int compress_2d(cpsz_b200_ctx* ctx, const float* U_in, const float* V_in, size_t r1s, size_t r2s, double max_pwr_eb,
-                Blob2D* out, const StageTap* tap, const double* eb_ext) {
+                Blob2D* out, const StageTap* tap, const double* eb_ext, unsigned char* host_out, size_t host_cap) {
   std::vector<Job2D> jobs(1);
   CPSZ_TRY(job_init(jobs[0], U_in, V_in, r1s, r2s, max_pwr_eb));
   jobs[0].eb_ext = eb_ext;
+  jobs[0].host_out = host_out;
+  jobs[0].host_cap = host_cap;
   CPSZ_TRY(arena_reserve(ctx, pass_bytes(jobs)));
   CPSZ_TRY(pinned_reserve(ctx, PINNED_BASE + JOB_PINNED));
   CPSZ_TRY(run_pass(ctx, jobs, tap));
-  out->d_blob = jobs[0].d.blob;
+  out->d_blob = host_out ? nullptr : jobs[0].d.blob;
   out->size = jobs[0].size;
   out->n_unpred[0] = jobs[0].n_unpred[0];
   out->n_unpred[1] = jobs[0].n_unpred[1];

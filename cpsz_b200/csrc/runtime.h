@@ -74,7 +74,7 @@ struct cpsz_b200_ctx {
   cudaStream_t hi = nullptr;   // highest-priority stream: consumers that run beside their producer
   cudaEvent_t ev[8] = {};
   // chunked host-to-device uploads (one event per chunk, recorded on `aux`)
-  static constexpr int kUploadChunks = 8;
+  static constexpr int kUploadChunks = 32;
   cudaEvent_t up_ev[kUploadChunks] = {};
   // per (field, component) "histogram on the host" events of a compression pass
   static constexpr int kJobEvents = 64;

@@ -26,7 +26,7 @@ const TuneInfo kInfo[TUNE_COUNT] = {
     {"wave2d.ctas_per_sm", 0, 0, 16},
     {"eb3d.fill", 4, 1, 32},
     {"eb3d.min_chunk", 8, 1, 256},
-    {"h2d.chunks", 8, 1, 8},
+    {"h2d.chunks", 8, 1, 32},
     {"wave2d.overlap", 1, 0, 1},
 };
 

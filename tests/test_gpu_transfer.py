@@ -32,6 +32,33 @@ def test_2d_pageable_pinned_and_device_give_equal_results(ctx, shape):
         assert x.tobytes() == y.cpu().numpy().tobytes()
 
 
+@pytest.mark.parametrize("shape", [(1024, 1536), (8192, 8192)])
+def test_2d_blob_written_straight_to_host_memory(ctx, shape):
+    """A host output buffer gets the blob section by section (the bit streams
+    and unpredictable floats copied from their device buffers as soon as they
+    are produced when it is page-locked, after the whole pass otherwise): the
+    bytes equal the device-assembled blob, repeatedly, and a buffer one byte
+    short is refused."""
+    torch = pytest.importorskip("torch")
+    U, V = W.cfg0_like(71, *shape)
+    dev = [torch.from_numpy(a).cuda() for a in (U, V)]
+    d_out = torch.zeros(U.nbytes * 3, dtype=torch.uint8, device="cuda")
+    n = cpsz_b200.compress_2d_into(*dev, *shape, 0.1, d_out, ctx=ctx)
+    ref = d_out[:n].cpu().numpy().tobytes()
+    pinned = [torch.from_numpy(a).pin_memory().numpy() for a in (U, V)]
+    h_pin = torch.zeros(n + 64, dtype=torch.uint8).pin_memory().numpy()
+    h_page = np.zeros(n + 64, np.uint8)
+    for _ in range(3):
+        h_pin[:] = 0x5A
+        assert cpsz_b200.compress_2d_into(*pinned, *shape, 0.1, h_pin, ctx=ctx) == n
+        assert h_pin[:n].tobytes() == ref
+    assert cpsz_b200.compress_2d_into(U, V, *shape, 0.1, h_page, ctx=ctx) == n
+    assert h_page[:n].tobytes() == ref
+    for buf in (h_pin[:n - 1], h_page[:n - 1]):
+        with pytest.raises(cpsz_b200.CpszError, match="output capacity"):
+            cpsz_b200.compress_2d_into(*pinned, *shape, 0.1, buf, ctx=ctx)
+
+
 def test_3d_pageable_and_device_give_equal_results(ctx):
     torch = pytest.importorskip("torch")
     U, V, Wf = W.field_3d(71, 130, 97, 101, n_flows=12, sigma=8.0)

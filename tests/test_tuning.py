@@ -53,7 +53,7 @@ def test_lookup_by_field_size():
 
 
 @pytest.mark.parametrize("name,value", [("eb2d.tile", 6), ("eb2d.tile", -1), ("h2d.chunks", 0),
-                                        ("h2d.chunks", 9), ("nope", 1)])
+                                        ("h2d.chunks", 33), ("nope", 1)])
 def test_set_rejects_bad_values(name, value):
     with pytest.raises(cpsz_b200.CpszError):
         cpsz_b200.tuning_set(name, value)
