@@ -46,29 +46,49 @@ __global__ void scale_bounds_kernel(const double* __restrict__ eb_a, const float
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(enlarged, c);
 }
 
-// Marks the vertices of every cell whose CP code differs (cells_a: original,
-// cells_b: reconstruction) and that still carry a proposed bound; counts the
-// differing cells and the cells with nothing left to revert.
+// Cell c's CP code differs between the original (cells_a) and the
+// reconstruction (cells_b): revert its vertices whose
+// bound was enlarged (counts[0] cells differing, counts[1] of them with no
+// enlarged vertex left).
+__device__ __forceinline__ void mark_cell(long long c, int r2, const double* __restrict__ eb,
+                                          const double* __restrict__ eb_a, uint8_t* __restrict__ revert,
+                                          unsigned long long& stuck) {
+  const long long q = c >> 1;
+  const int k = (int)(c & 1);
+  const int i = (int)(q / (r2 - 1)), j = (int)(q - (long long)i * (r2 - 1));
+  const size_t p[3] = {(size_t)i * r2 + j, (size_t)(i + (k == 0)) * r2 + j + (k == 1), (size_t)(i + 1) * r2 + j + 1};
+  bool any = false;
+  for (int t = 0; t < 3; t++)
+    if (eb[p[t]] != eb_a[p[t]]) {
+      revert[p[t]] = 1;
+      any = true;
+    }
+  stuck += !any;
+}
+
+// Differing cells are rare: 16 cells per load, a byte loop only where a
+// 16-byte word differs (ca and cb are 16-byte aligned).
 __global__ void mark_kernel(const uint8_t* __restrict__ ca, const uint8_t* __restrict__ cb, int r1, int r2,
                             const double* __restrict__ eb, const double* __restrict__ eb_a, uint8_t* __restrict__ revert,
                             unsigned long long* __restrict__ counts) {
   const long long ncell = 2LL * (r1 - 1) * (r2 - 1);
+  const long long nvec = ncell / 16;
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x, nt = (long long)gridDim.x * blockDim.x;
   unsigned long long diff = 0, stuck = 0;
-  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < ncell;
-       c += (long long)gridDim.x * blockDim.x) {
+  for (long long v = tid; v < nvec; v += nt) {
+    const uint4 x = __ldg(reinterpret_cast<const uint4*>(ca) + v), y = __ldg(reinterpret_cast<const uint4*>(cb) + v);
+    if (x.x == y.x && x.y == y.y && x.z == y.z && x.w == y.w) continue;
+    for (int e = 0; e < 16; e++) {
+      const long long c = 16 * v + e;
+      if (ca[c] == cb[c]) continue;
+      diff++;
+      mark_cell(c, r2, eb, eb_a, revert, stuck);
+    }
+  }
+  for (long long c = 16 * nvec + tid; c < ncell; c += nt) {
     if (ca[c] == cb[c]) continue;
     diff++;
-    const long long q = c >> 1;
-    const int k = (int)(c & 1);
-    const int i = (int)(q / (r2 - 1)), j = (int)(q - (long long)i * (r2 - 1));
-    const size_t p[3] = {(size_t)i * r2 + j, (size_t)(i + (k == 0)) * r2 + j + (k == 1), (size_t)(i + 1) * r2 + j + 1};
-    bool any = false;
-    for (int t = 0; t < 3; t++)
-      if (eb[p[t]] != eb_a[p[t]]) {
-        revert[p[t]] = 1;
-        any = true;
-      }
-    stuck += !any;
+    mark_cell(c, r2, eb, eb_a, revert, stuck);
   }
   for (int o = 16; o; o >>= 1) {
     diff += __shfl_xor_sync(0xffffffffu, diff, o);
@@ -80,15 +100,28 @@ __global__ void mark_kernel(const uint8_t* __restrict__ ca, const uint8_t* __res
   }
 }
 
+__device__ __forceinline__ void revert_one(size_t i, uint8_t* __restrict__ revert, const double* __restrict__ eb_a,
+                                           double* __restrict__ eb, unsigned long long& c) {
+  revert[i] = 0;
+  c += eb[i] != eb_a[i];
+  eb[i] = eb_a[i];
+}
+
+// Marked vertices get their analytic bound back (16 flags per load; revert is
+// 16-byte aligned).
 __global__ void revert_kernel(uint8_t* __restrict__ revert, const double* __restrict__ eb_a, double* __restrict__ eb,
                               size_t n, unsigned long long* __restrict__ count) {
   unsigned long long c = 0;
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-    if (revert[i]) {
-      revert[i] = 0;
-      c += eb[i] != eb_a[i];
-      eb[i] = eb_a[i];
-    }
+  const size_t nvec = n / 16;
+  const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x, nt = (size_t)gridDim.x * blockDim.x;
+  for (size_t v = tid; v < nvec; v += nt) {
+    const uint4 x = reinterpret_cast<const uint4*>(revert)[v];
+    if ((x.x | x.y | x.z | x.w) == 0) continue;
+    for (int e = 0; e < 16; e++)
+      if (revert[16 * v + e]) revert_one(16 * v + e, revert, eb_a, eb, c);
+  }
+  for (size_t i = 16 * nvec + tid; i < n; i += nt)
+    if (revert[i]) revert_one(i, revert, eb_a, eb, c);
   for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
 }
