@@ -254,6 +254,44 @@ namespace {
 // Quantization of given per-vertex bounds (the learned-bound path): the same
 // id arithmetic, symbols and wavefront pairs as eb2d_kernel, with the bound
 // read from eb_in instead of derived from the triangles.
+// One vertex of the given-bound quantization: ids and wavefront pairs of
+// U and V (the id of |x| * eb against the threshold table, ID_ZERO at or
+// below thr); sym[] gets the histogram symbols.
+__device__ __forceinline__ void quant2d_vertex(size_t g, const float* __restrict__ U, const float* __restrict__ V,
+                                               const double* __restrict__ eb_in, const double* tab, int thr_n,
+                                               uint8_t* __restrict__ ids_u, uint8_t* __restrict__ ids_v,
+                                               int* __restrict__ flag, float2* __restrict__ pair_u,
+                                               float2* __restrict__ pair_v, int sym[2]) {
+  const double thr = tab[0];
+  const double eb = eb_in[g];
+  const float uu = U[g], vv = V[g];
+  uint8_t code[2];
+  const double ev[2] = {(double)fabsf(uu) * eb, (double)fabsf(vv) * eb};
+#pragma unroll
+  for (int c = 0; c < 2; c++) {
+    const double e = ev[c];
+    if (e <= thr) {
+      code[c] = ID_ZERO;
+      sym[c] = 0;
+    } else {
+      int ex = (int)((__double_as_longlong(e) >> 52) & 0x7ff) - 1023;
+      int id = dev::count_thresholds(tab, thr_n, e, (ex + 52) >> 1);
+      if (id > ID_MAX_2D) {
+        atomicOr(flag, FLAG_ID_OVERFLOW);
+        id = ID_MAX_2D;
+      }
+      code[c] = (uint8_t)id;
+      sym[c] = id;
+    }
+  }
+  ids_u[g] = code[0];
+  ids_v[g] = code[1];
+  pair_u[g] = make_float2(uu, code[0] == ID_ZERO ? __int_as_float(0x7FC00000)
+                                                 : __int_as_float((127 + 52 - 2 * (int)code[0]) << 23));
+  pair_v[g] = make_float2(vv, code[1] == ID_ZERO ? __int_as_float(0x7FC00000)
+                                                 : __int_as_float((127 + 52 - 2 * (int)code[1]) << 23));
+}
+
 __global__ void __launch_bounds__(256) quant2d_kernel(const float* __restrict__ U, const float* __restrict__ V,
                                                       size_t n, const double* __restrict__ eb_in,
                                                       const double* __restrict__ thr_tab, int thr_n,
@@ -265,42 +303,46 @@ __global__ void __launch_bounds__(256) quant2d_kernel(const float* __restrict__ 
   for (int k = threadIdx.x; k < 256; k += blockDim.x) shist[k] = 0;
   for (int k = threadIdx.x; k < thr_n; k += blockDim.x) tab[k] = thr_tab[k];
   __syncthreads();
-  const double thr = tab[0];
   for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (size_t)gridDim.x * blockDim.x) {
-    const double eb = eb_in[g];
-    const float uu = U[g], vv = V[g];
-    uint8_t code[2];
     int sym[2];
-    const double ev[2] = {(double)fabsf(uu) * eb, (double)fabsf(vv) * eb};
-#pragma unroll
-    for (int c = 0; c < 2; c++) {
-      const double e = ev[c];
-      if (e <= thr) {
-        code[c] = ID_ZERO;
-        sym[c] = 0;
-      } else {
-        int ex = (int)((__double_as_longlong(e) >> 52) & 0x7ff) - 1023;
-        int id = dev::count_thresholds(tab, thr_n, e, (ex + 52) >> 1);
-        if (id > ID_MAX_2D) {
-          atomicOr(flag, FLAG_ID_OVERFLOW);
-          id = ID_MAX_2D;
-        }
-        code[c] = (uint8_t)id;
-        sym[c] = id;
-      }
-    }
-    ids_u[g] = code[0];
-    ids_v[g] = code[1];
-    pair_u[g] = make_float2(uu, code[0] == ID_ZERO ? __int_as_float(0x7FC00000)
-                                                   : __int_as_float((127 + 52 - 2 * (int)code[0]) << 23));
-    pair_v[g] = make_float2(vv, code[1] == ID_ZERO ? __int_as_float(0x7FC00000)
-                                                   : __int_as_float((127 + 52 - 2 * (int)code[1]) << 23));
+    quant2d_vertex(g, U, V, eb_in, tab, thr_n, ids_u, ids_v, flag, pair_u, pair_v, sym);
     atomicAdd(&shist[sym[0]], 1u);
     atomicAdd(&shist[sym[1]], 1u);
   }
   __syncthreads();
   for (int k = threadIdx.x; k < 256; k += blockDim.x)
     if (shist[k]) atomicAdd(&hist[k], (unsigned long long)shist[k]);
+}
+
+// The same for the vertices whose mask byte is set (16 mask bytes per load;
+// mask is 16-byte aligned), clearing it; no histogram.
+__global__ void __launch_bounds__(256) requant2d_kernel(const float* __restrict__ U, const float* __restrict__ V,
+                                                        size_t n, const double* __restrict__ eb_in,
+                                                        const double* __restrict__ thr_tab, int thr_n,
+                                                        uint8_t* __restrict__ ids_u, uint8_t* __restrict__ ids_v,
+                                                        int* __restrict__ flag, float2* __restrict__ pair_u,
+                                                        float2* __restrict__ pair_v, uint8_t* __restrict__ mask) {
+  __shared__ double tab[QUANT_TAB_MAX];
+  for (int k = threadIdx.x; k < thr_n; k += blockDim.x) tab[k] = thr_tab[k];
+  __syncthreads();
+  const size_t nvec = n / 16, tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t nt = (size_t)gridDim.x * blockDim.x;
+  int sym[2];
+  for (size_t v = tid; v < nvec; v += nt) {
+    const uint4 x = reinterpret_cast<const uint4*>(mask)[v];
+    if ((x.x | x.y | x.z | x.w) == 0) continue;
+    for (int e = 0; e < 16; e++) {
+      const size_t g = 16 * v + e;
+      if (!mask[g]) continue;
+      quant2d_vertex(g, U, V, eb_in, tab, thr_n, ids_u, ids_v, flag, pair_u, pair_v, sym);
+      mask[g] = 0;
+    }
+  }
+  for (size_t g = 16 * nvec + tid; g < n; g += nt)
+    if (mask[g]) {
+      quant2d_vertex(g, U, V, eb_in, tab, thr_n, ids_u, ids_v, flag, pair_u, pair_v, sym);
+      mask[g] = 0;
+    }
 }
 
 }  // namespace
@@ -314,6 +356,17 @@ int launch_quant2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t n,
                                                             ctx->d_flag, pair_u, pair_v);
   count_launch(ctx);
   return check_launch("quant2d_kernel");
+}
+
+int launch_requant2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t n, const double* eb_in,
+                     const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, float2* pair_u,
+                     float2* pair_v, uint8_t* mask) {
+  size_t g = (n / 16 + 255) / 256;
+  if (g > (size_t)ctx->num_sms * 8) g = (size_t)ctx->num_sms * 8;
+  requant2d_kernel<<<(int)(g ? g : 1), 256, 0, ctx->stream>>>(U, V, n, eb_in, d_thr_tab, thr_n, ids_u, ids_v,
+                                                              ctx->d_flag, pair_u, pair_v, mask);
+  count_launch(ctx);
+  return check_launch("requant2d_kernel");
 }
 
 }  // namespace cpsz

@@ -44,6 +44,11 @@ int preload_eb2d();
 int launch_quant2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t n, const double* eb_in,
                    const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
                    float2* pair_u, float2* pair_v);
+// launch_quant2d for the vertices whose mask byte is set (clearing it), into
+// ids / pairs that hold every other vertex's values already; no histogram.
+int launch_requant2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t n, const double* eb_in,
+                     const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, float2* pair_u,
+                     float2* pair_v, uint8_t* mask);
 
 // ---- 2D Lorenzo wavefront ------------------------------------------------------
 // One field of the wavefront.  Raster arrays carry their own row pitch (elements).

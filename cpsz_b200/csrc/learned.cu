@@ -100,17 +100,21 @@ __global__ void mark_kernel(const uint8_t* __restrict__ ca, const uint8_t* __res
   }
 }
 
-__device__ __forceinline__ void revert_one(size_t i, uint8_t* __restrict__ revert, const double* __restrict__ eb_a,
-                                           double* __restrict__ eb, unsigned long long& c) {
+__device__ __forceinline__ void revert_one(size_t i, uint8_t* __restrict__ revert, uint8_t* __restrict__ requant,
+                                           const double* __restrict__ eb_a, double* __restrict__ eb,
+                                           unsigned long long& c) {
   revert[i] = 0;
+  requant[i] = 1;
   c += eb[i] != eb_a[i];
   eb[i] = eb_a[i];
 }
 
-// Marked vertices get their analytic bound back (16 flags per load; revert is
-// 16-byte aligned).
-__global__ void revert_kernel(uint8_t* __restrict__ revert, const double* __restrict__ eb_a, double* __restrict__ eb,
-                              size_t n, unsigned long long* __restrict__ count) {
+// Marked vertices get their analytic bound back and are flagged for
+// quantization in the next pass (16 flags per load; revert is 16-byte
+// aligned).
+__global__ void revert_kernel(uint8_t* __restrict__ revert, uint8_t* __restrict__ requant,
+                              const double* __restrict__ eb_a, double* __restrict__ eb, size_t n,
+                              unsigned long long* __restrict__ count) {
   unsigned long long c = 0;
   const size_t nvec = n / 16;
   const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x, nt = (size_t)gridDim.x * blockDim.x;
@@ -118,10 +122,10 @@ __global__ void revert_kernel(uint8_t* __restrict__ revert, const double* __rest
     const uint4 x = reinterpret_cast<const uint4*>(revert)[v];
     if ((x.x | x.y | x.z | x.w) == 0) continue;
     for (int e = 0; e < 16; e++)
-      if (revert[16 * v + e]) revert_one(16 * v + e, revert, eb_a, eb, c);
+      if (revert[16 * v + e]) revert_one(16 * v + e, revert, requant, eb_a, eb, c);
   }
   for (size_t i = 16 * nvec + tid; i < n; i += nt)
-    if (revert[i]) revert_one(i, revert, eb_a, eb, c);
+    if (revert[i]) revert_one(i, revert, requant, eb_a, eb, c);
   for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
 }
@@ -177,7 +181,7 @@ int compress_2d_learned(cpsz_b200_ctx* ctx, cpsz_b200_mlp* mlp, const float* U_i
   DevMem mem;
   const size_t bytes = align_up(8 * N, 256) * 2 + align_up(QUANT_TAB_MAX * 8, 256) + align_up(4 * N, 256) * 3 +
                        align_up(2 * N, 256) +
-                       align_up(ncell, 256) * 2 + align_up(N, 256) + 4096 + (dev_in ? 0 : align_up(8 * N, 256));
+                       align_up(ncell, 256) * 2 + align_up(N, 256) * 2 + 4096 + (dev_in ? 0 : align_up(8 * N, 256));
   CPSZ_TRY(mem.alloc(bytes));
   uint8_t* w = (uint8_t*)mem.p;
   auto take = [&](size_t b) {
@@ -195,6 +199,7 @@ int compress_2d_learned(cpsz_b200_ctx* ctx, cpsz_b200_mlp* mlp, const float* U_i
   uint8_t* cells_a = (uint8_t*)take(ncell);
   uint8_t* cells_b = (uint8_t*)take(ncell);
   uint8_t* revert = (uint8_t*)take(N);
+  uint8_t* requant = (uint8_t*)take(N);  // vertices reverted since the last pass (quantized again)
   unsigned long long* counts = (unsigned long long*)take(4096);
   const float* dU = U_in;
   const float* dV = V_in;
@@ -209,6 +214,7 @@ int compress_2d_learned(cpsz_b200_ctx* ctx, cpsz_b200_mlp* mlp, const float* U_i
   CPSZ_CUDA_TRY(cudaMemcpyAsync(thr_tab, qt.t, QUANT_TAB_MAX * 8, cudaMemcpyHostToDevice, st));
   CPSZ_CUDA_TRY(cudaMemsetAsync(counts, 0, 4096, st));
   CPSZ_CUDA_TRY(cudaMemsetAsync(revert, 0, N, st));
+  CPSZ_CUDA_TRY(cudaMemsetAsync(requant, 0, N, st));
   CPSZ_CUDA_TRY(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), st));
   // analytic bounds (the hist / pair outputs are not needed here)
   CPSZ_TRY(launch_eb2d(ctx, dU, dV, r1, r2, max_pwr_eb, thr_tab, qt.n, ids, ids + N, counts + 64, nullptr, nullptr,
@@ -235,13 +241,16 @@ int compress_2d_learned(cpsz_b200_ctx* ctx, cpsz_b200_mlp* mlp, const float* U_i
   int it = 0;
   unsigned long long h[4] = {0, 0, 0, 0};
   for (;; it++) {
+    // after the first pass only the vertices reverted since are quantized
+    // again; the rest of the quantization stays in the compressor's workspace
+    tap.requant = it > 0 ? requant : nullptr;
     CPSZ_TRY(compress_2d(ctx, dU, dV, r1s, r2s, max_pwr_eb, out, &tap, eb));
     CPSZ_CUDA_TRY(cudaMemsetAsync(counts, 0, 32, st));
     CPSZ_TRY(launch_cp_check_2d(ctx, rec_u, rec_v, nullptr, nullptr, r1, r2, cells_b, counts + 8));
     mark_kernel<<<grid_of(ctx, ncell), 256, 0, st>>>(cells_a, cells_b, r1, r2, eb, eb_a, revert, counts);
     count_launch(ctx);
     CPSZ_TRY(check_launch("mark_kernel"));
-    revert_kernel<<<grid_of(ctx, N), 256, 0, st>>>(revert, eb_a, eb, N, counts + 2);
+    revert_kernel<<<grid_of(ctx, N), 256, 0, st>>>(revert, requant, eb_a, eb, N, counts + 2);
     count_launch(ctx);
     CPSZ_TRY(check_launch("revert_kernel"));
     CPSZ_CUDA_TRY(cudaMemcpyAsync(h, counts, 32, cudaMemcpyDeviceToHost, st));

@@ -25,6 +25,11 @@ struct StageTap {
   float* unpred[2] = {nullptr, nullptr};
   float* recon[2] = {nullptr, nullptr};      // compressor-side reconstruction (raster)
   bool recon_only = false;                   // stop after the Lorenzo stage (no blob)
+  // With given bounds and recon_only: the vertices (N bytes, 16-byte aligned)
+  // whose bound changed since the previous recon_only pass over the same
+  // field on this context, whose workspace (ids, wavefront pairs) nothing has
+  // touched since.  Only they are quantized again; the mask is cleared.
+  uint8_t* requant = nullptr;
 };
 
 int build_wave_items(int nfields, const int* r1s, std::vector<WaveItem>& items);

@@ -431,7 +431,10 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   for (Job2D& j : jobs) {
     unsigned long long* band = overlap ? j.d.band : nullptr;
     if (j.dev_in) {
-      if (j.eb_ext)
+      if (j.eb_ext && nj == 1 && tap && tap->recon_only && tap->requant)
+        CPSZ_TRY(launch_requant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
+                                  j.d.pairs[0], j.d.pairs[1], tap->requant));
+      else if (j.eb_ext)
         CPSZ_TRY(launch_quant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
                                 j.d.hist_ids, j.d.pairs[0], j.d.pairs[1]));
       else
