@@ -143,11 +143,11 @@ __device__ void flush(Tally t, unsigned long long* counts) {
 __global__ void __launch_bounds__(256) cp2d_kernel(const float* __restrict__ Ua, const float* __restrict__ Va,
                                                    const float* __restrict__ Ub, const float* __restrict__ Vb, int r1,
                                                    int r2, uint8_t* __restrict__ cells,
-                                                   unsigned long long* __restrict__ counts) {
+                                                   unsigned long long* __restrict__ counts, long long q0) {
   Tally t;
   const long long ncube = (long long)(r1 - 1) * (r2 - 1);
   const bool with_b = Ub != nullptr;
-  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < ncube;
+  for (long long q = q0 + (long long)blockIdx.x * blockDim.x + threadIdx.x; q < ncube;
        q += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(q / (r2 - 1)), j = (int)(q - (long long)i * (r2 - 1));
     const size_t p00 = (size_t)i * r2 + j, p10 = p00 + r2, p11 = p10 + 1, p01 = p00 + 1;
@@ -492,12 +492,15 @@ __global__ void labels2d_kernel(const float* __restrict__ U, const float* __rest
 }  // namespace
 
 int launch_cp_check_2d(cpsz_b200_ctx* ctx, const float* Ua, const float* Va, const float* Ub, const float* Vb, int r1,
-                       int r2, uint8_t* cells, unsigned long long* counts) {
+                       int r2, uint8_t* cells, unsigned long long* counts, int row0) {
   if (r1 < 2 || r2 < 2) return CPSZ_OK;
-  const long long n = (long long)(r1 - 1) * (r2 - 1);
+  if (row0 < 0) row0 = 0;
+  if (row0 >= r1 - 1) return CPSZ_OK;
+  const long long q0 = (long long)row0 * (r2 - 1);
+  const long long n = (long long)(r1 - 1) * (r2 - 1) - q0;
   long long g = (n + 255) / 256;
   if (g > (long long)ctx->num_sms * 16) g = (long long)ctx->num_sms * 16;
-  cp2d_kernel<<<(int)g, 256, 0, ctx->stream>>>(Ua, Va, Ub, Vb, r1, r2, cells, counts);
+  cp2d_kernel<<<(int)g, 256, 0, ctx->stream>>>(Ua, Va, Ub, Vb, r1, r2, cells, counts, q0);
   count_launch(ctx);
   return check_launch("cp2d_kernel");
 }

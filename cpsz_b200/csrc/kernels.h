@@ -216,7 +216,8 @@ int launch_wave3d(cpsz_b200_ctx* ctx, bool decompress, const float4* in, float4*
 // device) and counts[0..3] += {CPs in a, CPs in b, cells with a CP in exactly
 // one field, cells whose CP type differs}; b may be null.
 int launch_cp_check_2d(cpsz_b200_ctx* ctx, const float* Ua, const float* Va, const float* Ub, const float* Vb, int r1,
-                       int r2, uint8_t* cells, unsigned long long* counts);
+                       int r2, uint8_t* cells, unsigned long long* counts,
+                       int row0 = 0);
 // Training labels of the learned bound proposer: per vertex idx[s] the largest
 // log2 multiplier t in [0, tmax] of its analytic bound (bisection, `steps`
 // halvings) under which moving the vertex alone to any corner of its bound box

@@ -102,32 +102,41 @@ __global__ void mark_kernel(const uint8_t* __restrict__ ca, const uint8_t* __res
 
 __device__ __forceinline__ void revert_one(size_t i, uint8_t* __restrict__ revert, uint8_t* __restrict__ requant,
                                            const double* __restrict__ eb_a, double* __restrict__ eb,
-                                           unsigned long long& c) {
+                                           unsigned long long& c, size_t& first) {
   revert[i] = 0;
   requant[i] = 1;
   c += eb[i] != eb_a[i];
   eb[i] = eb_a[i];
+  first = i < first ? i : first;
 }
 
 // Marked vertices get their analytic bound back and are flagged for
 // quantization in the next pass (16 flags per load; revert is 16-byte
-// aligned).
+// aligned); first gets the lowest flagged vertex index (atomic min).
 __global__ void revert_kernel(uint8_t* __restrict__ revert, uint8_t* __restrict__ requant,
                               const double* __restrict__ eb_a, double* __restrict__ eb, size_t n,
-                              unsigned long long* __restrict__ count) {
+                              unsigned long long* __restrict__ count, unsigned long long* __restrict__ first_out) {
   unsigned long long c = 0;
+  size_t first = ~(size_t)0;
   const size_t nvec = n / 16;
   const size_t tid = (size_t)blockIdx.x * blockDim.x + threadIdx.x, nt = (size_t)gridDim.x * blockDim.x;
   for (size_t v = tid; v < nvec; v += nt) {
     const uint4 x = reinterpret_cast<const uint4*>(revert)[v];
     if ((x.x | x.y | x.z | x.w) == 0) continue;
     for (int e = 0; e < 16; e++)
-      if (revert[16 * v + e]) revert_one(16 * v + e, revert, requant, eb_a, eb, c);
+      if (revert[16 * v + e]) revert_one(16 * v + e, revert, requant, eb_a, eb, c, first);
   }
   for (size_t i = 16 * nvec + tid; i < n; i += nt)
-    if (revert[i]) revert_one(i, revert, requant, eb_a, eb, c);
-  for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-  if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+    if (revert[i]) revert_one(i, revert, requant, eb_a, eb, c, first);
+  for (int o = 16; o; o >>= 1) {
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+    const size_t f = __shfl_xor_sync(0xffffffffu, first, o);
+    first = f < first ? f : first;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (c) atomicAdd(count, c);
+    if (first != ~(size_t)0) atomicMin(first_out, (unsigned long long)first);
+  }
 }
 
 int grid_of(cpsz_b200_ctx* ctx, size_t n) {
@@ -239,21 +248,31 @@ int compress_2d_learned(cpsz_b200_ctx* ctx, cpsz_b200_mlp* mlp, const float* U_i
   tap.recon_only = true;
   uint64_t reverted = 0;
   int it = 0;
-  unsigned long long h[4] = {0, 0, 0, 0};
+  unsigned long long h[7] = {0, 0, 0, 0, 0, 0, 0};
   for (;; it++) {
-    // after the first pass only the vertices reverted since are quantized
-    // again; the rest of the quantization stays in the compressor's workspace
-    tap.requant = it > 0 ? requant : nullptr;
+    // After the first pass only the vertices reverted since are quantized
+    // again (the rest of the quantization stays in the compressor's
+    // workspace), and the recursion and the check start at the row group of
+    // the first of them: rows above it reconstruct as before.
+    int first_group = 0;
+    if (it > 0) {
+      first_group = (int)(h[6] / (unsigned long long)r2) / WAVE_GROUP_ROWS;
+      tap.requant = requant;
+      tap.first_group = first_group;
+    }
     CPSZ_TRY(compress_2d(ctx, dU, dV, r1s, r2s, max_pwr_eb, out, &tap, eb));
     CPSZ_CUDA_TRY(cudaMemsetAsync(counts, 0, 32, st));
-    CPSZ_TRY(launch_cp_check_2d(ctx, rec_u, rec_v, nullptr, nullptr, r1, r2, cells_b, counts + 8));
+    CPSZ_CUDA_TRY(cudaMemsetAsync(counts + 6, 0xff, 8, st));
+    // cells of row first_group * WAVE_GROUP_ROWS - 1 on touch the changed rows
+    CPSZ_TRY(launch_cp_check_2d(ctx, rec_u, rec_v, nullptr, nullptr, r1, r2, cells_b, counts + 8,
+                                first_group * WAVE_GROUP_ROWS - 1));
     mark_kernel<<<grid_of(ctx, ncell), 256, 0, st>>>(cells_a, cells_b, r1, r2, eb, eb_a, revert, counts);
     count_launch(ctx);
     CPSZ_TRY(check_launch("mark_kernel"));
-    revert_kernel<<<grid_of(ctx, N), 256, 0, st>>>(revert, requant, eb_a, eb, N, counts + 2);
+    revert_kernel<<<grid_of(ctx, N), 256, 0, st>>>(revert, requant, eb_a, eb, N, counts + 2, counts + 6);
     count_launch(ctx);
     CPSZ_TRY(check_launch("revert_kernel"));
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(h, counts, 32, cudaMemcpyDeviceToHost, st));
+    CPSZ_CUDA_TRY(cudaMemcpyAsync(h, counts, 56, cudaMemcpyDeviceToHost, st));
     CPSZ_CUDA_TRY(cudaStreamSynchronize(st));
     reverted += h[2];
     // clean, or nothing left to revert (every offending cell already analytic)

@@ -30,6 +30,10 @@ struct StageTap {
   // field on this context, whose workspace (ids, wavefront pairs) nothing has
   // touched since.  Only they are quantized again; the mask is cleared.
   uint8_t* requant = nullptr;
+  // With requant: the first WAVE_GROUP_ROWS-row group holding one of those
+  // vertices.  The groups above keep the previous pass's reconstruction (the
+  // recursion reads only rows above and to the left) and are not run again.
+  int first_group = 0;
 };
 
 int build_wave_items(int nfields, const int* r1s, std::vector<WaveItem>& items);

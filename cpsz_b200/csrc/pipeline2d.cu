@@ -374,9 +374,17 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   for (Job2D& j : jobs) CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.hist_ids, 0, 256 * 8, st));
   std::vector<WaveField> hf(2 * nj);
   std::vector<int> r1v(2 * nj);
+  // a pass that quantizes again only some vertices starts the recursion at
+  // their first row group: the groups above (and their boundary rows, which
+  // the first group run reads) are the previous pass's
+  const int g0 = (nj == 1 && tap && tap->recon_only && tap->requant && jobs[0].eb_ext)
+                     ? std::min(std::max(tap->first_group, 0), jobs[0].ngroups)
+                     : 0;
   for (int k = 0; k < nj; k++) {
     Job2D& j = jobs[k];
-    CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.gbnd, 0, 2 * (size_t)j.ngroups * j.r2 * 8, st));
+    for (int f = 0; f < 2; f++)
+      CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.gbnd + ((size_t)f * j.ngroups + g0) * j.r2, 0,
+                                    (size_t)(j.ngroups - g0) * j.r2 * 8, st));
     if (overlap) CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.band, 0, (size_t)j.ngroups * 8, st));
     for (int f = 0; f < 2; f++) {
       WaveField& F = hf[2 * k + f];
@@ -397,7 +405,10 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     }
   }
   std::vector<WaveItem> items;
-  const int n_items = build_wave_items(2 * nj, r1v.data(), items);
+  build_wave_items(2 * nj, r1v.data(), items);
+  if (g0 > 0) items.erase(std::remove_if(items.begin(), items.end(), [&](const WaveItem& w) { return w.group < g0; }),
+                          items.end());
+  const int n_items = (int)items.size();
   CPSZ_CUDA_TRY(cudaMemcpyAsync(d_fields, hf.data(), hf.size() * sizeof(WaveField), cudaMemcpyHostToDevice, st));
   CPSZ_CUDA_TRY(cudaMemcpyAsync(d_items, items.data(), n_items * sizeof(WaveItem), cudaMemcpyHostToDevice, st));
   CPSZ_CUDA_TRY(cudaMemsetAsync(queue, 0, 64, st));

@@ -441,6 +441,7 @@ int preload_wave2d() {
 
 int launch_wave2d(cpsz_b200_ctx* ctx, bool decompress, const WaveField* d_fields, const WaveItem* d_items,
                   int n_items, int* d_queue, size_t points, cudaStream_t stream, int mode) {
+  if (n_items <= 0) return CPSZ_OK;
   if (!stream) stream = ctx->stream;
   static bool attr_set[3] = {false, false, false};
   const bool beside = mode == WAVE_BESIDE && !decompress;
