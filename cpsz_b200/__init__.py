@@ -85,6 +85,7 @@ def _declare(L):
     L.cpsz_b200_debug_eb2d.argtypes = [_vp, _vp, _vp, _sz, _sz, C.c_double, _vp, _vp]
     L.cpsz_b200_debug_libm.argtypes = [_vp, C.c_int, _vp, _sz, _vp]
     L.cpsz_b200_debug_filter_premises.argtypes = [_vp, _vp, _sz]
+    L.cpsz_b200_mlp_propose_2d.argtypes = [_vp, _vp, _vp, _sz, _sz, _vp, _vp]
     L.cpsz_b200_debug_umma_gemm.argtypes = [_vp, _vp, _vp, _vp]
     L.cpsz_b200_mlp_param_count.restype = _sz
     L.cpsz_b200_mlp_create.argtypes = [_vp, C.c_uint64, C.POINTER(_vp)]
@@ -468,8 +469,12 @@ class Mlp:
         return loss.value, g
 
     def close(self):
+        # the MLP lives on its context's stream: once the context is closed
+        # there is nothing left to release through it (its device memory goes
+        # with the process)
         if getattr(self, "handle", None):
-            lib().cpsz_b200_mlp_destroy(self.handle)
+            if getattr(self.ctx, "handle", None):
+                lib().cpsz_b200_mlp_destroy(self.handle)
             self.handle = None
 
     def __del__(self):
@@ -488,6 +493,17 @@ def mlp_features_2d(U, V, eb_analytic, idx, ctx: Context | None = None) -> np.nd
     _check(lib().cpsz_b200_mlp_features_2d(_h(ctx), U.ctypes.data, V.ctypes.data, U.shape[0], U.shape[1],
                                            eb.ctypes.data, idx.ctypes.data, idx.size, X.ctypes.data))
     return X
+
+
+def mlp_propose_2d(mlp, U, V, eb_analytic) -> np.ndarray:
+    """The proposer's raw outputs (log2 multipliers) for every vertex of (U, V)."""
+    U = np.ascontiguousarray(U, np.float32)
+    V = np.ascontiguousarray(V, np.float32)
+    eb = np.ascontiguousarray(eb_analytic, np.float64)
+    y = np.empty(U.shape, np.float32)
+    _check(lib().cpsz_b200_mlp_propose_2d(mlp.handle, U.ctypes.data, V.ctypes.data, U.shape[0], U.shape[1],
+                                          eb.ctypes.data, y.ctypes.data))
+    return y
 
 
 def learned_labels_2d(U, V, eb_analytic, idx, steps: int = 16, ctx: Context | None = None) -> np.ndarray:

@@ -479,6 +479,36 @@ int cpsz_b200_mlp_features_2d(cpsz_b200_ctx* ctx, const float* U, const float* V
   return CPSZ_OK;
 }
 
+int cpsz_b200_mlp_propose_2d(cpsz_b200_mlp* mlp, const float* U, const float* V, size_t r1, size_t r2,
+                             const double* eb_analytic, float* y) {
+  if (!mlp) return set_error(CPSZ_ERR_INVALID, "null MLP");
+  cpsz_b200_ctx* ctx = mlp->ctx;
+  CPSZ_TRY(resolve(ctx));
+  if (!U || !V || !eb_analytic || !y) return set_error(CPSZ_ERR_INVALID, "null argument");
+  if (r1 * r2 == 0 || r1 * r2 > (size_t)INT32_MAX) return set_error(CPSZ_ERR_UNSUPPORTED, "field size out of range");
+  const size_t N = r1 * r2;
+  DevMem mem;
+  CPSZ_TRY(mem.alloc(8 * N + 8 * N + 4 * N + 4096));
+  uint8_t* p = (uint8_t*)mem.p;
+  float* dU = (float*)p;
+  float* dV = dU + N;
+  double* deb = (double*)(p + 8 * N);
+  float* dy = (float*)(p + 16 * N);
+  CPSZ_TRY(upload(ctx, dU, U, 4 * N));
+  CPSZ_TRY(upload(ctx, dV, V, 4 * N));
+  CPSZ_TRY(upload(ctx, deb, eb_analytic, 8 * N));
+  CPSZ_TRY(pinned_reserve(ctx, 4096));
+  CPSZ_CUDA_TRY(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+  CPSZ_TRY(launch_mlp_forward(ctx, mlp->w, nullptr, dU, dV, deb, (int)r1, (int)r2, (int)N, dy, nullptr, nullptr));
+  CPSZ_TRY(download(ctx, y, dy, 4 * N));
+  int flag = 0;
+  CPSZ_CUDA_TRY(cudaMemcpyAsync(ctx->pinned, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CPSZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  flag = *(int*)ctx->pinned;
+  if (flag & FLAG_TIMEOUT) return set_error(CPSZ_ERR_TIMEOUT, "a bounded device-side wait gave up");
+  return CPSZ_OK;
+}
+
 int cpsz_b200_learned_labels_2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2,
                                 const double* eb_analytic, const int32_t* idx, size_t n, int steps, float* t_out) {
   CPSZ_TRY(resolve(ctx));

@@ -248,6 +248,127 @@ __global__ void __launch_bounds__(128, 1) mlp_fwd_kernel(FwdArgs a) {
   if (warp == 0) umma::tmem_dealloc(tmem, 256);
 }
 
+// The forward pass on field features with two 128-row tiles in flight per
+// CTA: warps 0-3 and 4-7 are two independent pipelines (features -> layer 1
+// on the tensor cores -> epilogue -> layer 2 -> epilogue), each with its own
+// operand tiles, TMEM columns (256 each of the CTA's 512), mbarrier and named
+// barrier, so one pipeline's feature gathers overlap the other's MMAs and
+// epilogues.  The weights are shared.  Same arithmetic per row as
+// mlp_fwd_kernel<true>.
+constexpr int FWD2_SMEM = 6 * umma::TILE_BYTES + 64;
+
+__device__ __forceinline__ void group_sync(int g) { asm volatile("bar.sync %0, 128;" ::"r"(1 + g) : "memory"); }
+// AND of v over the 128 threads of group g (a named barrier)
+__device__ __forceinline__ bool group_and(int g, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, %2, 128, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(1 + g)
+      : "memory");
+  return r != 0;
+}
+
+__global__ void __launch_bounds__(256, 1) mlp_fwd2_kernel(FwdArgs a) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  const int tid = threadIdx.x, warp = tid >> 5, g = warp >> 2, gt = tid & 127;
+  uint8_t* W1s = smem;
+  uint8_t* W2s = smem + umma::TILE_BYTES;
+  uint8_t* Xs = smem + (2 + 2 * g) * umma::TILE_BYTES;
+  uint8_t* As = smem + (3 + 2 * g) * umma::TILE_BYTES;
+  uint64_t* mbars = (uint64_t*)(smem + 6 * umma::TILE_BYTES);
+  uint64_t* mbar = mbars + g;
+  uint32_t* tslot = (uint32_t*)(mbars + 2);
+  const float* b1 = a.p + 16384;
+  const float* b2 = a.p + 2 * 16384 + 128;
+  const float* w3 = a.p + 2 * 16384 + 256;
+  const float b3 = a.p[2 * 16384 + 384];
+  load_weight_tile(W1s, a.w1b, false);
+  load_weight_tile(W2s, a.w2b, false);
+  if (gt == 0) umma::mbar_init(mbar, 1);
+  if (warp == 0) {
+    umma::tmem_alloc(tslot, 512);
+    umma::tmem_relinquish();
+  }
+  umma::tc_fence_before();
+  __syncthreads();
+  umma::tc_fence_after();
+  const uint32_t tbase = *tslot;
+  const uint32_t tmem = tbase + 256 * g;  // this pipeline's columns
+  const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+  uint32_t phase = 0;
+  bool ok = true;
+  const int ntiles = (a.M + 127) / 128;
+  for (int tile = 2 * blockIdx.x + g; tile < ntiles && ok; tile += 2 * gridDim.x) {
+    const int row = tile * 128 + gt;
+    const bool valid = row < a.M;
+    {
+      float f[128];
+      if (valid) {
+        const int i = row / a.r2, j = row - (row / a.r2) * a.r2;
+        vertex_features(a.U, a.V, a.r1, a.r2, i, j, a.eb_a[row], f);
+      } else {
+        for (int k = 0; k < MLP_FEAT; k++) f[k] = 0.f;
+      }
+      for (int k = MLP_FEAT; k < 128; k++) f[k] = 0.f;
+      for (int c = 0; c < 128; c += 8) store_row_chunk(Xs, gt, c, f + c);
+    }
+    umma::fence_async_shared();
+    umma::tc_fence_before();
+    group_sync(g);
+    umma::tc_fence_after();
+    if (gt == 0) {
+      umma::gemm_tile(tmem, umma::smem_addr(Xs), umma::smem_addr(W1s), false);
+      umma::mma_commit(mbar);
+    }
+    // every thread of the pipeline takes the same branch after a bounded wait
+    ok = group_and(g, umma::mbar_wait(mbar, phase, WAIT_LIMIT));
+    phase ^= 1;
+    umma::tc_fence_after();
+    if (!ok) break;
+    // epilogue 1: h1 = relu(x W1^T + b1) -> bf16 operand of layer 2
+    for (int c = 0; c < 128; c += 16) {
+      float v[16];
+      umma::tmem_ld16(lane_addr + c, v);
+#pragma unroll
+      for (int q = 0; q < 16; q++) v[q] = fmaxf(v[q] + b1[c + q], 0.f);
+      store_row_chunk(As, gt, c, v);
+      store_row_chunk(As, gt, c + 8, v + 8);
+    }
+    umma::fence_async_shared();
+    umma::tc_fence_before();
+    group_sync(g);
+    umma::tc_fence_after();
+    if (gt == 0) {
+      umma::gemm_tile(tmem + 128, umma::smem_addr(As), umma::smem_addr(W2s), false);
+      umma::mma_commit(mbar);
+    }
+    ok = group_and(g, umma::mbar_wait(mbar, phase, WAIT_LIMIT));
+    phase ^= 1;
+    umma::tc_fence_after();
+    if (!ok) break;
+    // epilogue 2: h2 = relu(h1 W2^T + b2); y = h2 . w3 + b3
+    float acc = b3;
+    for (int c = 0; c < 128; c += 16) {
+      float v[16];
+      umma::tmem_ld16(lane_addr + 128 + c, v);
+#pragma unroll
+      for (int q = 0; q < 16; q++) {
+        v[q] = fmaxf(v[q] + b2[c + q], 0.f);
+        acc += v[q] * w3[c + q];
+      }
+    }
+    if (valid) a.y[row] = acc;
+    umma::tc_fence_before();
+    group_sync(g);
+    umma::tc_fence_after();
+  }
+  if (!ok && gt == 0) atomicOr(a.flag, FLAG_TIMEOUT);
+  umma::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) umma::tmem_dealloc(tbase, 512);
+}
+
 struct BwdArgs {
   const __nv_bfloat16* X;
   const __nv_bfloat16* H1;
@@ -478,12 +599,21 @@ int launch_mlp_forward(cpsz_b200_ctx* ctx, const MlpParams& w, const void* X, co
   if (!attr) {
     CPSZ_TRY(set_smem(mlp_fwd_kernel<false>, FWD_SMEM));
     CPSZ_TRY(set_smem(mlp_fwd_kernel<true>, FWD_SMEM));
+    CPSZ_TRY(set_smem(mlp_fwd2_kernel, FWD2_SMEM));
     attr = true;
   }
   if (M <= 0) return CPSZ_OK;
   FwdArgs a{(const __nv_bfloat16*)X, U, V, eb_a, r1, r2, M, (const __nv_bfloat16*)w.w1b, (const __nv_bfloat16*)w.w2b,
             w.p, y, (__nv_bfloat16*)H1, (__nv_bfloat16*)H2, ctx->d_flag};
   const int ntiles = (M + 127) / 128;
+  if (!X && !H1 && !H2) {
+    // field features, no activations kept: two tiles in flight per CTA
+    const int pairs = (ntiles + 1) / 2;
+    const int grid2 = pairs < ctx->num_sms ? pairs : ctx->num_sms;
+    mlp_fwd2_kernel<<<grid2, 256, FWD2_SMEM, ctx->stream>>>(a);
+    count_launch(ctx);
+    return check_launch("mlp_fwd2_kernel");
+  }
   const int grid = ntiles < ctx->num_sms ? ntiles : ctx->num_sms;
   if (X) mlp_fwd_kernel<false><<<grid, 128, FWD_SMEM, ctx->stream>>>(a);
   else mlp_fwd_kernel<true><<<grid, 128, FWD_SMEM, ctx->stream>>>(a);

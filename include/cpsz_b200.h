@@ -140,6 +140,12 @@ int cpsz_b200_mlp_train_step(cpsz_b200_mlp* mlp, const uint16_t* X, const float*
  * analytic bounds eb_analytic[r1*r2]. */
 int cpsz_b200_mlp_features_2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2,
                               const double* eb_analytic, const int32_t* idx, size_t n, uint16_t* X);
+/* The proposer's raw outputs (log2 multipliers before clamping) for every
+ * vertex of field (U, V) with analytic bounds eb_analytic[r1*r2]: the
+ * features computed on the device and both layers on the tensor cores, as
+ * the learned compression does.  Host or device buffers; y gets r1*r2 floats. */
+int cpsz_b200_mlp_propose_2d(cpsz_b200_mlp* mlp, const float* U, const float* V, size_t r1, size_t r2,
+                             const double* eb_analytic, float* y);
 /* Training labels: per vertex the largest log2 multiplier (bisection, `steps`
  * halvings of [0, 16]) that keeps its incident cells' CPs when the vertex
  * alone moves to any corner of its bound box. */

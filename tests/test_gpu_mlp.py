@@ -84,6 +84,20 @@ def test_mlp_features_match_reference(ctx, oracle):
     assert np.array_equal(X, ref)
 
 
+@pytest.mark.parametrize("shape", [(300, 257), (61, 1030)])
+def test_mlp_field_proposals_equal_feature_path(ctx, oracle, shape):
+    """The proposer over a whole field (features built on the device, two
+    128-row tiles in flight per CTA) gives bit for bit the floats of the
+    feature rows of every vertex run through the plain forward pass."""
+    U, V = W.cfg0_like(9, *shape)
+    eb = oracle.eb_2d(U, V, 0.1).ravel()
+    mlp = cpsz_b200.Mlp(ctx, seed=3)
+    y = cpsz_b200.mlp_propose_2d(mlp, U, V, eb)
+    X = cpsz_b200.mlp_features_2d(U, V, eb, np.arange(U.size, dtype=np.int32), ctx=ctx)
+    ref = np.asarray(mlp.forward(X), np.float32).ravel()
+    assert np.array_equal(y.ravel().view(np.uint32), ref.view(np.uint32))
+
+
 def _label_ref(U, V, eb, v, steps=16, tmax=16.0):
     r1, r2 = U.shape
     i, j = divmod(v, r2)
