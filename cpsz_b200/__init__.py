@@ -53,6 +53,7 @@ def _declare(L):
     L.cpsz_b200_ctx_create.argtypes = [C.c_int, C.POINTER(_vp)]
     L.cpsz_b200_ctx_destroy.argtypes = [_vp]
     L.cpsz_b200_ctx_kernel_launches.argtypes = [_vp, C.POINTER(C.c_uint64)]
+    L.cpsz_b200_ctx_graph_stats.argtypes = [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.cpsz_b200_ctx_stream.argtypes = [_vp, C.POINTER(_vp)]
     L.cpsz_b200_compress_2d_offline_f32.argtypes = [_vp, _vp, _vp, _sz, _sz, C.c_double, C.POINTER(_vp), C.POINTER(_sz)]
     L.cpsz_b200_compress_2d_offline_f32_into.argtypes = [_vp, _vp, _vp, _sz, _sz, C.c_double, _vp, _sz, C.POINTER(_sz)]
@@ -157,6 +158,13 @@ class Context:
         v = C.c_uint64()
         _check(lib().cpsz_b200_ctx_kernel_launches(self.handle, C.byref(v)))
         return v.value
+
+    @property
+    def graph_stats(self) -> tuple:
+        """(graphs captured, batch passes replayed from a captured graph)."""
+        c, r = C.c_uint64(), C.c_uint64()
+        _check(lib().cpsz_b200_ctx_graph_stats(self.handle, C.byref(c), C.byref(r)))
+        return c.value, r.value
 
     @property
     def stream(self) -> int:

@@ -432,100 +432,172 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[4], ctx->hi));
   }
 
-  // ---- stage 1: inputs and error bounds ----
-  mark(ctx, "eb2d");
-  // host-input uploads run on the second stream, after the pass's setup (once
-  // per pass: per field it would hold each upload behind the previous field's
-  // bound kernels)
-  CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[2], st));
-  CPSZ_CUDA_TRY(cudaStreamWaitEvent(ctx->aux, ctx->ev[2], 0));
-  for (Job2D& j : jobs) {
-    unsigned long long* band = overlap ? j.d.band : nullptr;
-    if (j.dev_in) {
-      if (j.eb_ext && nj == 1 && tap && tap->recon_only && tap->requant)
-        CPSZ_TRY(launch_requant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
-                                  j.d.pairs[0], j.d.pairs[1], tap->requant));
-      else if (j.eb_ext)
-        CPSZ_TRY(launch_quant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
-                                j.d.hist_ids, j.d.pairs[0], j.d.pairs[1]));
-      else
-        CPSZ_TRY(launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
-                             j.d.hist_ids, j.d.pairs[0], j.d.pairs[1], nullptr, 0, -1, band));
+  // Stages 1-3 (bounds, wavefront, code histograms, block order) are the
+  // pass's device work before the host builds the code trees.  A batch whose
+  // fields are all in device memory captures them once into a CUDA graph,
+  // kept on the context and replayed while the pass is the same (fields,
+  // shapes, bounds, workspace, tuning table); events the host waits on are
+  // recorded as external events of the graph.
+  bool all_dev_in = true;
+  for (const Job2D& j : jobs) all_dev_in = all_dev_in && j.dev_in;
+  bool capturing = false;
+  auto record = [&](cudaEvent_t e) {
+    return capturing ? cudaEventRecordWithFlags(e, st, cudaEventRecordExternal) : cudaEventRecord(e, st);
+  };
+  auto stages_1_2 = [&]() -> int {
+    // ---- stage 1: inputs and error bounds ----
+    mark(ctx, "eb2d");
+    // host-input uploads run on the second stream, after the pass's setup (once
+    // per pass: per field it would hold each upload behind the previous field's
+    // bound kernels)
+    if (!all_dev_in) {
+      CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[2], st));
+      CPSZ_CUDA_TRY(cudaStreamWaitEvent(ctx->aux, ctx->ev[2], 0));
+    }
+    for (Job2D& j : jobs) {
+      unsigned long long* band = overlap ? j.d.band : nullptr;
+      if (j.dev_in) {
+        if (j.eb_ext && nj == 1 && tap && tap->recon_only && tap->requant)
+          CPSZ_TRY(launch_requant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
+                                    j.d.pairs[0], j.d.pairs[1], tap->requant));
+        else if (j.eb_ext)
+          CPSZ_TRY(launch_quant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
+                                  j.d.hist_ids, j.d.pairs[0], j.d.pairs[1]));
+        else
+          CPSZ_TRY(launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
+                               j.d.hist_ids, j.d.pairs[0], j.d.pairs[1], nullptr, 0, -1, band));
+      } else {
+        // Host input: row chunks go up on the second stream and the bound kernel
+        // runs band by band as soon as a band's rows and the row below it are
+        // on the device, so the transfer overlaps the bound derivation.  Bands
+        // start on wavefront group boundaries.  Chunk c carries its band's rows
+        // and the next band's first row (which chunk c + 1 writes again, with
+        // the same bytes), so band c waits for chunk c alone and only the last
+        // band's bounds follow the end of the transfer.
+        const int K = (j.N >= ((size_t)1 << 22) && !j.eb_ext) ? tune_get(TUNE_H2D_CHUNKS, j.N) : 1;
+        const int R = (int)align_up((size_t)(j.r1 + K - 1) / K, WAVE_GROUP_ROWS);
+        const int nch = (j.r1 + R - 1) / R;
+        // band c is enqueued right after chunk c's copy call (a copy from
+        // pageable memory returns only once the host has staged it, so
+        // enqueueing every copy first would hold the bands back until the whole
+        // field was staged)
+        auto band_launch = [&](int c) -> int {
+          CPSZ_CUDA_TRY(cudaStreamWaitEvent(st, ctx->up_ev[c], 0));
+          if (j.eb_ext)
+            return launch_quant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
+                                  j.d.hist_ids, j.d.pairs[0], j.d.pairs[1]);
+          return launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N, j.d.hist_ids,
+                             j.d.pairs[0], j.d.pairs[1], nullptr, c * R, std::min(j.r1, (c + 1) * R), band);
+        };
+        for (int c = 0; c < nch; c++) {
+          const size_t off = (size_t)c * R * j.r2;
+          const size_t cnt = (size_t)(std::min(j.r1, (c + 1) * R + 1) - c * R) * j.r2;
+          CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.U + off, j.U_in + off, 4 * cnt, cudaMemcpyHostToDevice, ctx->aux));
+          CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.V + off, j.V_in + off, 4 * cnt, cudaMemcpyHostToDevice, ctx->aux));
+          CPSZ_CUDA_TRY(cudaEventRecord(ctx->up_ev[c], ctx->aux));
+          CPSZ_TRY(band_launch(c));
+        }
+      }
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_hist_ids, j.d.hist_ids, 256 * 8, cudaMemcpyDeviceToHost, st));
+    }
+    CPSZ_CUDA_TRY(record(ctx->ev[0]));
+    if (tap && tap->ids)
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(tap->ids, jobs[0].d.ids, 2 * jobs[0].N, cudaMemcpyDeviceToDevice, st));
+
+    // ---- stage 2: one persistent wavefront over every field of the pass ----
+    mark(ctx, "wave2d_compress");
+    if (overlap) {
+      // the bounds are done: the rest of each SM joins the running wavefront
+      CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points, st, WAVE_JOIN));
+      CPSZ_CUDA_TRY(cudaStreamWaitEvent(st, ctx->ev[4], 0));
     } else {
-      // Host input: row chunks go up on the second stream and the bound kernel
-      // runs band by band as soon as a band's rows and the row below it are
-      // on the device, so the transfer overlaps the bound derivation.  Bands
-      // start on wavefront group boundaries.  Chunk c carries its band's rows
-      // and the next band's first row (which chunk c + 1 writes again, with
-      // the same bytes), so band c waits for chunk c alone and only the last
-      // band's bounds follow the end of the transfer.
-      const int K = (j.N >= ((size_t)1 << 22) && !j.eb_ext) ? tune_get(TUNE_H2D_CHUNKS, j.N) : 1;
-      const int R = (int)align_up((size_t)(j.r1 + K - 1) / K, WAVE_GROUP_ROWS);
-      const int nch = (j.r1 + R - 1) / R;
-      // band c is enqueued right after chunk c's copy call (a copy from
-      // pageable memory returns only once the host has staged it, so
-      // enqueueing every copy first would hold the bands back until the whole
-      // field was staged)
-      auto band_launch = [&](int c) -> int {
-        CPSZ_CUDA_TRY(cudaStreamWaitEvent(st, ctx->up_ev[c], 0));
-        if (j.eb_ext)
-          return launch_quant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
-                                j.d.hist_ids, j.d.pairs[0], j.d.pairs[1]);
-        return launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N, j.d.hist_ids,
-                           j.d.pairs[0], j.d.pairs[1], nullptr, c * R, std::min(j.r1, (c + 1) * R), band);
-      };
-      for (int c = 0; c < nch; c++) {
-        const size_t off = (size_t)c * R * j.r2;
-        const size_t cnt = (size_t)(std::min(j.r1, (c + 1) * R + 1) - c * R) * j.r2;
-        CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.U + off, j.U_in + off, 4 * cnt, cudaMemcpyHostToDevice, ctx->aux));
-        CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.V + off, j.V_in + off, 4 * cnt, cudaMemcpyHostToDevice, ctx->aux));
-        CPSZ_CUDA_TRY(cudaEventRecord(ctx->up_ev[c], ctx->aux));
-        CPSZ_TRY(band_launch(c));
+      CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points));
+    }
+    return CPSZ_OK;
+  };
+  auto stage_3 = [&]() -> int {
+    mark(ctx, "blocks+hist+unpred");
+
+    // ---- stage 3: code histograms first (the host builds the code trees from
+    // them while the GPU converts to block order and gathers unpredictables) ----
+    for (int k = 0; k < nj; k++) {
+      Job2D& j = jobs[k];
+      for (int f = 0; f < 2; f++) {
+        CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.hist_codes[f], 0, 65536 * 8, st));
+        CPSZ_TRY(launch_hist_u16(ctx, j.d.craster[f], j.N, j.d.hist_codes[f]));
+        CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_hist_codes + (size_t)f * 65536, j.d.hist_codes[f], 65536 * 8,
+                                      cudaMemcpyDeviceToHost, st));
+        CPSZ_CUDA_TRY(record(ctx->job_ev[2 * k + f]));
       }
     }
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_hist_ids, j.d.hist_ids, 256 * 8, cudaMemcpyDeviceToHost, st));
-  }
-  CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[0], st));
-  if (tap && tap->ids)
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(tap->ids, jobs[0].d.ids, 2 * jobs[0].N, cudaMemcpyDeviceToDevice, st));
-
-  // ---- stage 2: one persistent wavefront over every field of the pass ----
-  mark(ctx, "wave2d_compress");
-  if (overlap) {
-    // the bounds are done: the rest of each SM joins the running wavefront
-    CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points, st, WAVE_JOIN));
-    CPSZ_CUDA_TRY(cudaStreamWaitEvent(st, ctx->ev[4], 0));
-  } else {
-    CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points));
-  }
-  if (tap && tap->recon_only) {
-    int flag = 0;
-    CPSZ_TRY(read_flag(ctx, &flag));
-    return flag ? flag_error(flag) : CPSZ_OK;
-  }
-  mark(ctx, "blocks+hist+unpred");
-
-  // ---- stage 3: code histograms first (the host builds the code trees from
-  // them while the GPU converts to block order and gathers unpredictables) ----
-  for (int k = 0; k < nj; k++) {
-    Job2D& j = jobs[k];
-    for (int f = 0; f < 2; f++) {
-      CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.hist_codes[f], 0, 65536 * 8, st));
-      CPSZ_TRY(launch_hist_u16(ctx, j.d.craster[f], j.N, j.d.hist_codes[f]));
-      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_hist_codes + (size_t)f * 65536, j.d.hist_codes[f], 65536 * 8,
-                                    cudaMemcpyDeviceToHost, st));
-      CPSZ_CUDA_TRY(cudaEventRecord(ctx->job_ev[2 * k + f], st));
+    for (int k = 0; k < nj; k++) {
+      Job2D& j = jobs[k];
+      const float* x[2] = {j.d.U, j.d.V};
+      CPSZ_TRY(launch_strip_pass(ctx, j.d.craster, j.r2, x, j.r2, j.r1, j.r2, j.d.cblocks, j.d.unpred, j.d.strip));
+      for (int f = 0; f < 2; f++)
+        CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_nunpred + f, strip_total(j.d.strip[f], j.r1, j.r2), 4,
+                                      cudaMemcpyDeviceToHost, st));
+    }
+    CPSZ_CUDA_TRY(record(ctx->ev[5]));  // the unpredictable counts are on the host
+    return CPSZ_OK;
+  };
+  const bool use_graph = nj > 1 && all_dev_in && !tap && !ctx->timing && !overlap;
+  bool done = false;
+  if (use_graph) {
+    std::vector<uint64_t> key = {(uint64_t)nj, (uint64_t)(uintptr_t)ctx->arena.base, (uint64_t)(uintptr_t)ctx->pinned,
+                                 tune_generation()};
+    for (const Job2D& j : jobs) {
+      uint64_t ebits;
+      memcpy(&ebits, &j.eb, 8);
+      key.insert(key.end(), {(uint64_t)(uintptr_t)j.U_in, (uint64_t)(uintptr_t)j.V_in, (uint64_t)j.r1,
+                             (uint64_t)j.r2, ebits});
+    }
+    auto& cache = ctx->pass_graphs;
+    auto hit = std::find_if(cache.begin(), cache.end(), [&](const cpsz_b200_ctx::PassGraph& g) { return g.key == key; });
+    if (hit != cache.end()) {
+      std::rotate(hit, hit + 1, cache.end());  // most recently used last
+      CPSZ_CUDA_TRY(cudaGraphLaunch(cache.back().exec, st));
+      count_launch(ctx, cache.back().launches);
+      ctx->graph_replays++;
+      done = true;
+    } else {
+      if (cache.size() >= cpsz_b200_ctx::kMaxPassGraphs) {
+        cudaGraphExecDestroy(cache.front().exec);
+        cache.erase(cache.begin());
+      }
+      const uint64_t launches0 = ctx->launches;
+      if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        capturing = true;
+        int rc = stages_1_2();
+        if (rc == CPSZ_OK) rc = stage_3();
+        capturing = false;
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(st, &graph);
+        cudaGraphExec_t exec = nullptr;
+        if (rc == CPSZ_OK && e == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+          cache.push_back(cpsz_b200_ctx::PassGraph{key, exec, (int)(ctx->launches - launches0)});
+          done = cudaGraphLaunch(exec, st) == cudaSuccess;
+          ctx->graph_captures += done;
+        }
+        if (graph) cudaGraphDestroy(graph);
+      }
+      if (!done) {
+        // capture unavailable or failed: the same work, launched directly
+        cudaGetLastError();
+        clear_error();
+        ctx->launches = launches0;
+      }
     }
   }
-  for (int k = 0; k < nj; k++) {
-    Job2D& j = jobs[k];
-    const float* x[2] = {j.d.U, j.d.V};
-    CPSZ_TRY(launch_strip_pass(ctx, j.d.craster, j.r2, x, j.r2, j.r1, j.r2, j.d.cblocks, j.d.unpred, j.d.strip));
-    for (int f = 0; f < 2; f++)
-      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_nunpred + f, strip_total(j.d.strip[f], j.r1, j.r2), 4,
-                                    cudaMemcpyDeviceToHost, st));
+  if (!done) {
+    CPSZ_TRY(stages_1_2());
+    if (tap && tap->recon_only) {
+      int flag = 0;
+      CPSZ_TRY(read_flag(ctx, &flag));
+      return flag ? flag_error(flag) : CPSZ_OK;
+    }
+    CPSZ_TRY(stage_3());
   }
-  CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[5], st));  // the unpredictable counts are on the host
   mark(ctx, "host_trees");
   // Host output (one field): the sections are copied from their device
   // buffers straight into the caller's memory, each right after its producer

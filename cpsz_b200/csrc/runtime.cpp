@@ -277,6 +277,7 @@ int cpsz_b200_ctx_destroy(cpsz_b200_ctx* c) {
   cudaStreamSynchronize(c->stream);
   cudaStreamSynchronize(c->aux);
   if (c->hi) cudaStreamSynchronize(c->hi);
+  for (auto& g : c->pass_graphs) cudaGraphExecDestroy(g.exec);
   if (c->arena.base) cudaFree(c->arena.base);
   if (c->pinned) cudaFreeHost(c->pinned);
   if (c->stage) cudaFreeHost(c->stage);
@@ -308,6 +309,13 @@ int cpsz_b200_ctx_kernel_launches(cpsz_b200_ctx* ctx, uint64_t* count) {
   if (!ctx) return rc;
   if (!count) return set_error(CPSZ_ERR_INVALID, "null count");
   *count = ctx->launches;
+  return CPSZ_OK;
+}
+
+int cpsz_b200_ctx_graph_stats(cpsz_b200_ctx* ctx, uint64_t* captures, uint64_t* replays) {
+  if (!ctx || !captures || !replays) return set_error(CPSZ_ERR_INVALID, "null argument");
+  *captures = ctx->graph_captures;
+  *replays = ctx->graph_replays;
   return CPSZ_OK;
 }
 

@@ -73,6 +73,16 @@ struct cpsz_b200_ctx {
   cudaStream_t aux = nullptr;  // second stream for overlapping independent stages
   cudaStream_t hi = nullptr;   // highest-priority stream: consumers that run beside their producer
   cudaEvent_t ev[8] = {};
+  // batch passes' device work captured as CUDA graphs (pipeline2d.cu), each
+  // replayed while its pass recurs; least recently used first
+  struct PassGraph {
+    std::vector<uint64_t> key;
+    cudaGraphExec_t exec = nullptr;
+    int launches = 0;
+  };
+  static constexpr size_t kMaxPassGraphs = 64;
+  std::vector<PassGraph> pass_graphs;
+  uint64_t graph_captures = 0, graph_replays = 0;
   // chunked host-to-device uploads (one event per chunk, recorded on `aux`)
   static constexpr int kUploadChunks = 32;
   cudaEvent_t up_ev[kUploadChunks] = {};

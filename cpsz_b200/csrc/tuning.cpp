@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <shared_mutex>
 #include <string>
@@ -37,6 +38,7 @@ struct Entry {
 
 std::shared_mutex g_mu;
 std::vector<Entry> g_tab[TUNE_COUNT];  // sorted by min_points, unique thresholds
+std::atomic<uint64_t> g_gen{0};        // bumped by every change of the table
 std::once_flag g_once;
 int g_auto_rc = CPSZ_OK;
 std::string g_auto_err, g_loaded_from;
@@ -219,6 +221,7 @@ int load_file(const std::string& path, bool missing_ok) {
   std::unique_lock<std::shared_mutex> lk(g_mu);
   for (int p = 0; p < TUNE_COUNT; p++) g_tab[p] = std::move(t[p]);
   g_loaded_from = path;
+  g_gen++;
   return CPSZ_OK;
 }
 
@@ -242,6 +245,8 @@ void suppress_autoload() { std::call_once(g_once, [] {}); }
 }  // namespace
 
 const TuneInfo& tune_info(int p) { return kInfo[p]; }
+
+uint64_t tune_generation() { return g_gen.load(); }
 
 int tune_get(TuneParam p, size_t points) {
   if (p == TUNE_WAVE2D_OVERLAP) {
@@ -297,6 +302,7 @@ int cpsz_b200_tuning_set(const char* param, size_t min_points, int value) {
   suppress_autoload();
   std::unique_lock<std::shared_mutex> lk(g_mu);
   put(g_tab[p], min_points, value);
+  g_gen++;
   return CPSZ_OK;
 }
 
@@ -313,6 +319,7 @@ int cpsz_b200_tuning_clear(void) {
   std::unique_lock<std::shared_mutex> lk(g_mu);
   for (auto& v : g_tab) v.clear();
   g_loaded_from.clear();
+  g_gen++;
   return CPSZ_OK;
 }
 

@@ -15,6 +15,8 @@
 // package directory (the parent of the library's directory) when present.
 #pragma once
 
+#include <cstdint>
+
 #include <cstddef>
 
 namespace cpsz {
@@ -40,5 +42,7 @@ const TuneInfo& tune_info(int p);
 int tune_get(TuneParam p, size_t points);
 // Loads the default table once (no-op afterwards); returns a CPSZ status.
 int tune_autoload();
+// Changes with every change of the table (cached launch sequences key on it).
+uint64_t tune_generation();
 
 }  // namespace cpsz

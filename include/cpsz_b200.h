@@ -47,6 +47,9 @@ int cpsz_b200_ctx_create(int device, cpsz_b200_ctx** ctx);
 int cpsz_b200_ctx_destroy(cpsz_b200_ctx* ctx);
 /* Number of kernels this context has launched so far (for launch accounting). */
 int cpsz_b200_ctx_kernel_launches(cpsz_b200_ctx* ctx, uint64_t* count);
+/* Batch passes run from CUDA graphs on this context: graphs captured, and
+ * passes replayed from a graph captured earlier. */
+int cpsz_b200_ctx_graph_stats(cpsz_b200_ctx* ctx, uint64_t* captures, uint64_t* replays);
 /* Stream of the context as an opaque handle (a cudaStream_t). */
 int cpsz_b200_ctx_stream(cpsz_b200_ctx* ctx, void** stream);
 /* Per-stage timing: when on, each call records CUDA events on the context's

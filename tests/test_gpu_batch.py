@@ -50,3 +50,50 @@ def test_batch_rejects_small_output(ctx):
     fields, ebs = _batch(3, 3, 50, 60)
     with pytest.raises(cpsz_b200.CpszError):
         cpsz_b200.compress_2d_batch(fields, ebs, out=np.zeros(100, np.uint8), ctx=ctx)
+
+
+def test_batch_graph_capture_and_replay(ctx):
+    """A batch of device fields runs its pre-tree device work from a CUDA graph:
+    the first call captures it, a repeated identical call replays it, and a
+    change of a bound or of the tuning table captures again.  Every result
+    equals the single-field compressor's blobs, and a replay counts the same
+    kernels as the call that captured."""
+    torch = pytest.importorskip("torch")
+    fields, ebs = _batch(24, 3, 40, 400)
+    dev = [(torch.from_numpy(U).cuda(), torch.from_numpy(V).cuda()) for U, V in fields]
+    out = torch.zeros(64 << 20, dtype=torch.uint8, device="cuda")
+
+    def run(e):
+        before = ctx.kernel_launches
+        offs = cpsz_b200.compress_2d_batch(dev, e, out=out, ctx=ctx)
+        host = out[:int(offs[-1])].cpu().numpy().tobytes()
+        return [host[int(offs[k]):int(offs[k + 1])] for k in range(len(dev))], ctx.kernel_launches - before
+
+    def singles(e):
+        return [cpsz_b200.sz_compress_cp_preserve_2d_offline(U, V, max_pwr_eb=b, ctx=ctx) for (U, V), b in zip(fields, e)]
+
+    ref = singles(ebs)
+    c0, r0 = ctx.graph_stats
+    first, n_first = run(ebs)
+    assert first == ref
+    c1, r1 = ctx.graph_stats
+    assert c1 == c0 + 1 and r1 == r0  # one pass, captured
+    for k in range(3):
+        again, n_again = run(ebs)
+        assert again == ref
+        assert n_again == n_first
+        assert ctx.graph_stats == (c1, r1 + k + 1)  # replayed
+    ebs2 = list(ebs)
+    ebs2[5] = 0.02 if ebs2[5] != 0.02 else 0.03
+    changed, _ = run(ebs2)
+    assert changed == singles(ebs2)
+    assert ctx.graph_stats[0] == c1 + 1  # a new bound: captured again
+    try:
+        cpsz_b200.tuning_set("eb2d.tile", 1, min_points=0)
+        retuned, _ = run(ebs)
+        assert retuned == ref
+        assert ctx.graph_stats[0] == c1 + 2  # a new launch shape: captured again
+    finally:
+        cpsz_b200.tuning_clear()
+        cpsz_b200.tuning_load()
+    assert run(ebs)[0] == ref
