@@ -3,11 +3,9 @@
 //
 // The reference emits quantization codes and unpredictable values in 12x12
 // block order (blocks row-major, rows inside a block, src/sz_compress_3d.cpp:
-// 126-193).  A "segment" is one row of one block (up to 12 points, contiguous
-// in block order); segments are numbered in block order:
-//   ord = bi*12*nby + bj*h + li,   h = rows of block-row bi (12, or the remainder),
-// and element (i, j) sits at block-order position
-//   bi*12*r2 + bj*12*h + li*w + lj,   w = columns of block bj.
+// 126-193): element (i, j) sits at block-order position
+//   bi*12*r2 + bj*12*h + li*w + lj,   h = rows of block-row bi (12, or the
+//   remainder), w = columns of block bj (12, or the remainder).
 #include <algorithm>
 
 #include "kernels.h"
@@ -17,103 +15,7 @@ namespace cpsz {
 namespace {
 
 constexpr int BS = 12;
-constexpr int NT = 256;
-
-struct Seg {
-  int i, j0, w;
-  long long pos;  // block-order position of the segment's first element
-};
-
-__device__ __forceinline__ Seg seg_of(long long ord, int r1, int r2, int nby) {
-  long long per_brow = (long long)BS * nby;
-  int bi = (int)(ord / per_brow);
-  int rem = (int)(ord - (long long)bi * per_brow);
-  int h = min(BS, r1 - bi * BS);
-  int bj = rem / h, li = rem - bj * h;
-  int w = min(BS, r2 - bj * BS);
-  Seg s;
-  s.i = bi * BS + li;
-  s.j0 = bj * BS;
-  s.w = w;
-  s.pos = (long long)bi * BS * r2 + (long long)bj * BS * h + (long long)li * w;
-  return s;
-}
-
-__global__ void __launch_bounds__(NT) r2b_kernel(const uint16_t* __restrict__ raster, long long pitch, int r1, int r2,
-                                                 int nby, long long nseg, uint16_t* __restrict__ blocks) {
-  long long ord = (long long)blockIdx.x * NT + threadIdx.x;
-  if (ord >= nseg) return;
-  Seg s = seg_of(ord, r1, r2, nby);
-  const uint16_t* src = raster + (long long)s.i * pitch + s.j0;
-  for (int k = 0; k < s.w; k++) blocks[s.pos + k] = src[k];
-}
-
-// Decompression side of a point: the addend 2(code - 32768) * p that the
-// wavefront adds to its prediction (p = 4^id * 2^-52, 0 for id 0;
-// src/sz_decompress_cp_preserve_2d.cpp:30-34, include/sz_decompression_utils.hpp:65-73),
-// or a raw flag for code 0 (the raw value is scattered in afterwards).
-__global__ void __launch_bounds__(NT) b2r_kernel(const uint16_t* __restrict__ blocks, int r1, int r2, int nby,
-                                                 long long nseg, uint16_t* __restrict__ raster, long long pitch,
-                                                 const uint8_t* __restrict__ ids, float2* __restrict__ pair) {
-  long long ord = (long long)blockIdx.x * NT + threadIdx.x;
-  if (ord >= nseg) return;
-  Seg s = seg_of(ord, r1, r2, nby);
-  uint16_t* dst = raster + (long long)s.i * pitch + s.j0;
-  for (int k = 0; k < s.w; k++) dst[k] = blocks[s.pos + k];
-  if (pair) {
-    const long long base = (long long)s.i * r2 + s.j0;
-    for (int k = 0; k < s.w; k++) {
-      const int code = blocks[s.pos + k];
-      const int id = ids[base + k];
-      const float p = id ? __int_as_float((2 * id - 52 + 127) << 23) : 0.f;
-      pair[base + k] = make_float2((float)(2 * (code - 32768)) * p, __int_as_float(code == 0 ? 1 : 0));
-    }
-  }
-}
-
-__global__ void __launch_bounds__(NT) seg_count_kernel(const uint16_t* __restrict__ raster, long long pitch, int r1,
-                                                       int r2, int nby, long long nseg, unsigned int* __restrict__ cnt) {
-  long long ord = (long long)blockIdx.x * NT + threadIdx.x;
-  if (ord >= nseg) return;
-  Seg s = seg_of(ord, r1, r2, nby);
-  const uint16_t* src = raster + (long long)s.i * pitch + s.j0;
-  unsigned int c = 0;
-  for (int k = 0; k < s.w; k++) c += (src[k] == 0);
-  cnt[ord] = c;
-}
-
-__global__ void __launch_bounds__(NT) gather_kernel(const uint16_t* __restrict__ raster, long long pitch,
-                                                    const float* __restrict__ x, long long x_pitch, int r1, int r2,
-                                                    int nby, long long nseg, const unsigned int* __restrict__ off,
-                                                    float* __restrict__ unpred) {
-  long long ord = (long long)blockIdx.x * NT + threadIdx.x;
-  if (ord >= nseg) return;
-  Seg s = seg_of(ord, r1, r2, nby);
-  const uint16_t* src = raster + (long long)s.i * pitch + s.j0;
-  const float* xs = x + (long long)s.i * x_pitch + s.j0;
-  unsigned int o = off[ord];
-  for (int k = 0; k < s.w; k++)
-    if (src[k] == 0) unpred[o++] = xs[k];
-}
-
-__global__ void __launch_bounds__(NT) scatter_kernel(const uint16_t* __restrict__ raster, long long pitch,
-                                                     const float* __restrict__ unpred, unsigned long long n_unpred,
-                                                     int r1, int r2, int nby, long long nseg,
-                                                     const unsigned int* __restrict__ off,
-                                                     float2* __restrict__ pairs, int* flag) {
-  long long ord = (long long)blockIdx.x * NT + threadIdx.x;
-  if (ord >= nseg) return;
-  Seg s = seg_of(ord, r1, r2, nby);
-  const uint16_t* src = raster + (long long)s.i * pitch + s.j0;
-  float2* xs = pairs + (long long)s.i * r2 + s.j0;
-  unsigned long long o = off[ord];
-  for (int k = 0; k < s.w; k++)
-    if (src[k] == 0) {
-      if (o < n_unpred) xs[k].x = unpred[o];
-      else atomicOr(flag, FLAG_RAW_RANGE);
-      o++;
-    }
-}
+constexpr unsigned FULLM = 0xffffffffu;
 
 // ---- generic exclusive scan (u32) ---------------------------------------------------
 constexpr int SCAN_NT = 1024;
@@ -201,11 +103,15 @@ __global__ void __launch_bounds__(SCAN_NT) scan_down_kernel(const unsigned int* 
 
 // ---- strips: a 12-row block row cut into runs of STRIP_BLOCKS blocks ----------------
 // A strip's blocks are consecutive in block order, so its block-order image is
-// one contiguous range: the strip is staged in shared memory with coalesced
-// row reads and written out with coalesced block-order writes.
+// one contiguous range.  A CTA stages the strip in shared memory as rows and
+// moves it between the two orders with 16-byte global loads and stores on both
+// sides (a thread issues all of its loads before it stores any: the kernels
+// are bound by memory latency, not by instructions).
 constexpr int STRIP_BLOCKS = 32;
 constexpr int STRIP_W = STRIP_BLOCKS * BS;  // 384 columns
 constexpr int STRIP_NT = 256;
+constexpr int STRIP_TP = STRIP_W + 8;  // shared row pitch in u16: 784 bytes, 16-byte rows
+constexpr int STRIP_VEC = (BS * STRIP_W / 8 + STRIP_NT - 1) / STRIP_NT;  // 16-byte vectors per thread: 3
 
 struct StripGeom {
   int bi, h, c0, W, nb, wl;
@@ -223,125 +129,247 @@ __device__ __forceinline__ StripGeom strip_geom(long long s, int r1, int r2, int
   g.out0 = (long long)g.bi * BS * r2 + (long long)sc * STRIP_BLOCKS * BS * g.h;
   return g;
 }
-// One pass per component.  A CTA takes the next strip in ticket order (tickets
-// go out in the order CTAs start, so every earlier strip belongs to a CTA that
-// is running or done), stages it, writes its block-order image, publishes its
-// unpredictable count, finds the count of all earlier strips by a decoupled
-// look-back over their published words (Merrill & Garland, "Single-pass
-// Parallel Prefix Scan with Decoupled Look-back", 2016) and writes its
-// unpredictable values in block order.  Status words: 2-bit state (0 = not
-// yet, AGG = the strip's own count, PRE = inclusive prefix) over a 62-bit count.
+
+// Element e of a strip's block-order image: block b, row li and column lj
+// inside it (w = the block's width).  Every block but the last is 12 wide, so
+// b = e / (12 h) clamped to the last block.
+struct StripPos {
+  int b, li, lj, w;
+};
+__device__ __forceinline__ StripPos strip_pos(const StripGeom& g, int e) {
+  StripPos p;
+  p.b = min(e / (BS * g.h), g.nb - 1);
+  const int k = e - p.b * BS * g.h;
+  p.w = p.b == g.nb - 1 ? g.wl : BS;
+  p.li = k / p.w;
+  p.lj = k - p.li * p.w;
+  return p;
+}
+__device__ __forceinline__ void strip_next(const StripGeom& g, StripPos& p) {
+  if (++p.lj == p.w) {
+    p.lj = 0;
+    if (++p.li == g.h) {
+      p.li = 0;
+      ++p.b;
+      p.w = p.b == g.nb - 1 ? g.wl : BS;
+    }
+  }
+}
+
+// The scalar head and tail that align a strip's block-order range to 16
+// bytes: elements [0, head) and [head + 8 nvec, E) go one by one, the nvec
+// vectors between them 8 at a time.  An unaligned base takes the scalar path.
+struct StripSplit {
+  int E, head, nvec;
+};
+__device__ __forceinline__ StripSplit strip_split(const StripGeom& g, const uint16_t* base) {
+  StripSplit sp;
+  sp.E = g.h * g.W;
+  sp.head = sp.E;
+  sp.nvec = 0;
+  if ((reinterpret_cast<uintptr_t>(base) & 15) == 0) {
+    sp.head = min(sp.E, (int)((8 - (g.out0 & 7)) & 7));
+    sp.nvec = (sp.E - sp.head) >> 3;
+  }
+  return sp;
+}
+
+// Decoupled look-back (Merrill & Garland, "Single-pass Parallel Prefix Scan
+// with Decoupled Look-back", 2016) over the strips' published unpredictable
+// counts.  A CTA takes the next strip in ticket order (tickets go out in the
+// order CTAs start, so every earlier strip belongs to a CTA that is running or
+// done).  Status words: 2-bit state (0 = not yet, AGG = the strip's own count,
+// PRE = inclusive prefix) over a 62-bit count.  A word carries its count
+// itself and nothing else is read on its strength, so relaxed loads and
+// stores suffice; every lane keeps LB_DEPTH loads in flight, so one L2 round
+// trip covers 32 * LB_DEPTH strips (with one load per lane the look-back
+// could not keep pace with tens of thousands of strips: windows of in-flight
+// strips that had not yet published their prefix grew to hundreds).
 constexpr unsigned long long ST_AGG = 1ull << 62, ST_PRE = 2ull << 62, ST_VAL = (1ull << 62) - 1;
 constexpr long long LOOKBACK_SPIN = 1ll << 24;
-constexpr unsigned FULLM = 0xffffffffu;
+constexpr int LB_DEPTH = 4;
+
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Warp 0 of a strip's CTA: the exclusive prefix of its blocks' zero counts
+// (bpre), its own count published, and the count of all earlier strips
+// (s_excl); the last strip also stores the component's total beside the
+// ticket.  A look-back that waits past its bound sets FLAG_TIMEOUT.
+__device__ __forceinline__ void strip_prefix(unsigned long long* status, unsigned int s, unsigned int ns,
+                                             const StripGeom& g, const unsigned int* bz, unsigned int* bpre,
+                                             unsigned long long* s_excl, int lane, int* flag) {
+  const unsigned int v = lane < g.nb ? bz[lane] : 0u;
+  unsigned int inc = v;  // inclusive scan of the block counts
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const unsigned int y = __shfl_up_sync(FULLM, inc, d);
+    if (lane >= d) inc += y;
+  }
+  bpre[lane] = inc - v;
+  const unsigned long long tot = __shfl_sync(FULLM, inc, 31);
+  unsigned long long excl = 0;
+  if (s == 0) {
+    if (lane == 0) st_relaxed64(&status[0], ST_PRE | tot);
+  } else {
+    if (lane == 0) st_relaxed64(&status[s], ST_AGG | tot);
+    long long p = (long long)s - 1;  // the nearest strip not yet summed
+    long long spins = 0;
+    bool done = false;
+    while (!done) {
+      unsigned long long w[LB_DEPTH];
+#pragma unroll
+      for (int m = 0; m < LB_DEPTH; m++) {
+        const long long q = p - 32 * m - lane;
+        w[m] = q >= 0 ? ld_relaxed64(&status[q]) : ST_PRE;  // before strip 0: prefix 0
+      }
+      // the windows in order, nearest first; a window with an unpublished
+      // strip before its nearest prefix is read again from there
+      bool wait = false;
+#pragma unroll
+      for (int m = 0; m < LB_DEPTH; m++) {
+        if (done || wait) continue;
+        const unsigned int pre_m = __ballot_sync(FULLM, (w[m] & ~ST_VAL) == ST_PRE);
+        const unsigned int none_m = __ballot_sync(FULLM, (w[m] & ~ST_VAL) == 0);
+        const int last = pre_m ? __ffs(pre_m) - 1 : 31;  // the nearest prefix, or the whole window
+        const unsigned int upto = last == 31 ? FULLM : ((1u << (last + 1)) - 1u);
+        if (none_m & upto) {
+          wait = true;
+          continue;
+        }
+        unsigned long long add = lane <= last ? (w[m] & ST_VAL) : 0ull;
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) add += __shfl_xor_sync(FULLM, add, d);
+        excl += add;
+        p -= 32;
+        done = pre_m != 0;
+      }
+      if (wait) {
+        if (++spins > LOOKBACK_SPIN) {
+          if (lane == 0) atomicOr(flag, FLAG_TIMEOUT);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    if (lane == 0) st_relaxed64(&status[s], ST_PRE | (excl + tot));
+  }
+  if (lane == 0) {
+    *s_excl = excl;
+    if (s == ns - 1) reinterpret_cast<unsigned int*>(status + ns)[1] = (unsigned int)(excl + tot);
+  }
+}
+
+__device__ __forceinline__ unsigned int lanemask_lt(int lane) { return (1u << lane) - 1u; }
 
 struct StripPass {
   const uint16_t* raster;
   const float* x;
   uint16_t* blocks;
   float* unpred;
-  unsigned long long* status;  // ns words, then the ticket and the field total (u32 each); zeroed
+  unsigned long long* status;  // ns words, then the ticket and the component total (u32 each); zeroed
 };
 
-__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long* p) {
-  unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release64(unsigned long long* p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-
+// Compression, one launch for both components: codes raster -> block order,
+// and the unpredictable values (code 0) in block order.
 __global__ void __launch_bounds__(STRIP_NT) strip_pass_kernel(StripPass P0, StripPass P1, long long pitch,
                                                               long long x_pitch, int r1, int r2, int nsc,
                                                               unsigned int ns, int* flag) {
-  __shared__ uint16_t t[BS][STRIP_W + 2];
+  __shared__ __align__(16) uint16_t t[BS][STRIP_TP];
   __shared__ unsigned int bz[STRIP_BLOCKS], bpre[STRIP_BLOCKS];
   __shared__ unsigned int s_idx;
   __shared__ unsigned long long s_excl;
   const StripPass P = blockIdx.y ? P1 : P0;
-  unsigned int* ticket = reinterpret_cast<unsigned int*>(P.status + ns);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (threadIdx.x == 0) s_idx = atomicAdd(ticket, 1u);
+  if (threadIdx.x == 0) s_idx = atomicAdd(reinterpret_cast<unsigned int*>(P.status + ns), 1u);
+  if (threadIdx.x < STRIP_BLOCKS) bz[threadIdx.x] = 0;
   __syncthreads();
   const unsigned int s = s_idx;
   const StripGeom g = strip_geom(s, r1, r2, nsc);
+
+  // rows into shared memory
   const uint16_t* src = P.raster + (long long)g.bi * BS * pitch + g.c0;
-  for (int li = 0; li < g.h; li++)
-    for (int c = threadIdx.x; c < g.W; c += STRIP_NT) t[li][c] = src[(long long)li * pitch + c];
-  __syncthreads();
-  // block-order image, one warp per block: element k of block b is row k / w,
-  // column k % w (w = 12 except a row's last block); the float quotient is
-  // exact here because (k + 0.5) / w stays >= 1/24 away from an integer
-  for (int b = warp; b < g.nb; b += STRIP_NT / 32) {
-    const int w = (b == g.nb - 1) ? g.wl : BS;
-    const float inv_w = 1.0f / (float)w;
-    const int nk = g.h * w;
-    uint16_t* dst = P.blocks + g.out0 + (long long)b * BS * g.h;
-    unsigned int z = 0;
-    for (int k = lane; k < nk; k += 32) {
-      const int li = (int)(((float)k + 0.5f) * inv_w);
-      const uint16_t v = t[li][b * BS + (k - li * w)];
-      dst[k] = v;
-      z += v == 0;
-    }
-    z = __reduce_add_sync(FULLM, z);
-    if (lane == 0) bz[b] = z;
-  }
-  __syncthreads();
-  if (warp == 0) {
-    const unsigned int v = lane < g.nb ? bz[lane] : 0u;
-    unsigned int inc = v;  // inclusive scan of the block counts
+  if (((reinterpret_cast<uintptr_t>(P.raster) | (uintptr_t)(2 * pitch)) & 15) == 0) {
+    const int nv = g.W >> 3, tot = g.h * nv;  // c0 is a multiple of 8, so every row's vectors are aligned
+    uint4 v[STRIP_VEC];
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const unsigned int y = __shfl_up_sync(FULLM, inc, d);
-      if (lane >= d) inc += y;
-    }
-    bpre[lane] = inc - v;
-    const unsigned long long tot = __shfl_sync(FULLM, inc, 31);
-    unsigned long long excl = 0;
-    if (s == 0) {
-      if (lane == 0) st_release64(&P.status[0], ST_PRE | tot);
-    } else {
-      if (lane == 0) st_release64(&P.status[s], ST_AGG | tot);
-      long long p = (long long)s - 1;
-      long long spins = 0;
-      for (;;) {
-        const long long q = p - lane;
-        const unsigned long long w = q >= 0 ? ld_acquire64(&P.status[q]) : ST_PRE;  // before strip 0: prefix 0
-        const unsigned int pre_m = __ballot_sync(FULLM, (w & ~ST_VAL) == ST_PRE);
-        const unsigned int none_m = __ballot_sync(FULLM, (w & ~ST_VAL) == 0);
-        const int last = pre_m ? __ffs(pre_m) - 1 : 31;  // the nearest prefix, or the whole window
-        const unsigned int upto = last == 31 ? FULLM : ((1u << (last + 1)) - 1u);
-        if (none_m & upto) {  // a nearer strip has not published yet
-          if (++spins > LOOKBACK_SPIN) {
-            if (lane == 0) atomicOr(flag, FLAG_TIMEOUT);
-            break;
-          }
-          __nanosleep(64);
-          continue;
-        }
-        unsigned long long add = lane <= last ? (w & ST_VAL) : 0ull;
-#pragma unroll
-        for (int d = 16; d > 0; d >>= 1) add += __shfl_xor_sync(FULLM, add, d);
-        excl += add;
-        if (pre_m) break;
-        p -= 32;
+    for (int it = 0; it < STRIP_VEC; it++) {
+      const int q = threadIdx.x + it * STRIP_NT;
+      if (q < tot) {
+        const int li = q / nv;
+        v[it] = __ldg(reinterpret_cast<const uint4*>(src + (long long)li * pitch) + (q - li * nv));
       }
-      if (lane == 0) st_release64(&P.status[s], ST_PRE | (excl + tot));
     }
-    if (lane == 0) {
-      s_excl = excl;
-      if (s == ns - 1) ticket[1] = (unsigned int)(excl + tot);
+#pragma unroll
+    for (int it = 0; it < STRIP_VEC; it++) {
+      const int q = threadIdx.x + it * STRIP_NT;
+      if (q < tot) {
+        const int li = q / nv;
+        reinterpret_cast<uint4*>(&t[li][0])[q - li * nv] = v[it];
+      }
+    }
+    const int rem = g.W - 8 * nv;  // the field's last columns
+    for (int q = threadIdx.x; q < g.h * rem; q += STRIP_NT) {
+      const int li = q / rem, c = 8 * nv + (q - li * rem);
+      t[li][c] = src[(long long)li * pitch + c];
+    }
+  } else {
+#pragma unroll 6
+    for (int q = threadIdx.x; q < g.h * g.W; q += STRIP_NT) {
+      const int li = q / g.W, c = q - li * g.W;
+      t[li][c] = src[(long long)li * pitch + c];
     }
   }
   __syncthreads();
+
+  // block-order image, 8 elements per 16-byte store; zero codes counted per
+  // block (shared atomics only where a thread met zeros)
+  uint16_t* dst = P.blocks + g.out0;
+  const StripSplit sp = strip_split(g, dst);
+  for (int q = threadIdx.x; q < sp.nvec; q += STRIP_NT) {
+    const int e0 = sp.head + 8 * q;
+    StripPos p = strip_pos(g, e0);
+    unsigned int w32[4];
+    int zb = p.b;
+    unsigned int z = 0;
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+      if (p.b != zb) {
+        if (z) atomicAdd(&bz[zb], z);
+        zb = p.b;
+        z = 0;
+      }
+      const unsigned int v = t[p.li][p.b * BS + p.lj];
+      z += v == 0;
+      w32[m >> 1] = (m & 1) ? (w32[m >> 1] | (v << 16)) : v;
+      strip_next(g, p);
+    }
+    if (z) atomicAdd(&bz[zb], z);
+    *reinterpret_cast<uint4*>(dst + e0) = make_uint4(w32[0], w32[1], w32[2], w32[3]);
+  }
+  const int tail0 = sp.head + 8 * sp.nvec;
+  for (int q = threadIdx.x; q < sp.head + (sp.E - tail0); q += STRIP_NT) {
+    const int e = q < sp.head ? q : tail0 + (q - sp.head);
+    const StripPos p = strip_pos(g, e);
+    const uint16_t v = t[p.li][p.b * BS + p.lj];
+    dst[e] = v;
+    if (v == 0) atomicAdd(&bz[p.b], 1u);
+  }
+  __syncthreads();
+  if (warp == 0) strip_prefix(P.status, s, ns, g, bz, bpre, &s_excl, lane, flag);
+  __syncthreads();
+
   // unpredictable values, in block order
   const unsigned long long excl = s_excl;
   for (int b = warp; b < g.nb; b += STRIP_NT / 32) {
     if (bz[b] == 0) continue;
     const int w = (b == g.nb - 1) ? g.wl : BS;
-    const float inv_w = 1.0f / (float)w;
     const int nk = g.h * w;
     unsigned long long run = excl + bpre[b];
     for (int k0 = 0; k0 < nk; k0 += 32) {
@@ -349,21 +377,162 @@ __global__ void __launch_bounds__(STRIP_NT) strip_pass_kernel(StripPass P0, Stri
       int li = 0, col = 0;
       bool z = false;
       if (k < nk) {
-        li = (int)(((float)k + 0.5f) * inv_w);
+        li = k / w;
         col = b * BS + (k - li * w);
         z = t[li][col] == 0;
       }
       const unsigned int m = __ballot_sync(FULLM, z);
-      if (z)
-        P.unpred[run + __popc(m & ((1u << lane) - 1u))] =
-            P.x[(long long)(g.bi * BS + li) * x_pitch + g.c0 + col];
+      if (z) P.unpred[run + __popc(m & lanemask_lt(lane))] = P.x[(long long)(g.bi * BS + li) * x_pitch + g.c0 + col];
       run += __popc(m);
     }
   }
 }
 
-inline long long nseg_of(int r1, int r2) { return (long long)r1 * ((r2 - 1) / BS + 1); }
-inline unsigned grid_of(long long n) { return (unsigned)((n + NT - 1) / NT); }
+struct StripUnpass {
+  const uint16_t* blocks;      // block-order codes
+  const uint8_t* ids;          // the component's error-bound ids, raster order (pitch r2)
+  const float* unpred;         // unpredictable values, block order
+  unsigned long long n_unpred;
+  float2* pair;                // raster (pitch r2)
+  unsigned long long* status;  // as in StripPass
+};
+
+// Decompression side of a point: the addend 2(code - 32768) * p that the
+// wavefront adds to its prediction (p = 4^id * 2^-52, 0 for id 0;
+// src/sz_decompress_cp_preserve_2d.cpp:30-34, include/sz_decompression_utils.hpp:65-73),
+// or for code 0 the raw flag with the raw value in .x.
+__device__ __forceinline__ float2 dec_pair(unsigned int code, unsigned int id) {
+  const float p = id ? __int_as_float((int)(2 * id - 52 + 127) << 23) : 0.f;
+  return make_float2((float)(2 * ((int)code - 32768)) * p, __int_as_float(code == 0 ? 1 : 0));
+}
+
+// Decompression, one launch for both components: block-order codes -> the
+// raster pairs the wavefront reads, with the unpredictable values (block
+// order) scattered into the pairs of the zero codes.  The last strip stores
+// the number of zero codes, which the host checks against the stored list.
+__global__ void __launch_bounds__(STRIP_NT) strip_unpass_kernel(StripUnpass P0, StripUnpass P1, int r1, int r2,
+                                                                int nsc, unsigned int ns, int* flag) {
+  __shared__ __align__(16) uint16_t t[BS][STRIP_TP];
+  __shared__ unsigned int bz[STRIP_BLOCKS], bpre[STRIP_BLOCKS];
+  __shared__ unsigned int s_idx;
+  __shared__ unsigned long long s_excl;
+  const StripUnpass P = blockIdx.y ? P1 : P0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_idx = atomicAdd(reinterpret_cast<unsigned int*>(P.status + ns), 1u);
+  if (threadIdx.x < STRIP_BLOCKS) bz[threadIdx.x] = 0;
+  __syncthreads();
+  const unsigned int s = s_idx;
+  const StripGeom g = strip_geom(s, r1, r2, nsc);
+
+  // block-order codes into shared rows, zero codes counted per block
+  const uint16_t* src = P.blocks + g.out0;
+  const StripSplit sp = strip_split(g, src);
+  {
+    uint4 v[STRIP_VEC];
+#pragma unroll
+    for (int it = 0; it < STRIP_VEC; it++) {
+      const int q = threadIdx.x + it * STRIP_NT;
+      if (q < sp.nvec) v[it] = __ldg(reinterpret_cast<const uint4*>(src + sp.head + 8 * q));
+    }
+#pragma unroll
+    for (int it = 0; it < STRIP_VEC; it++) {
+      const int q = threadIdx.x + it * STRIP_NT;
+      if (q < sp.nvec) {
+        const unsigned int w32[4] = {v[it].x, v[it].y, v[it].z, v[it].w};
+        StripPos p = strip_pos(g, sp.head + 8 * q);
+        int zb = p.b;
+        unsigned int z = 0;
+#pragma unroll
+        for (int m = 0; m < 8; m++) {
+          if (p.b != zb) {
+            if (z) atomicAdd(&bz[zb], z);
+            zb = p.b;
+            z = 0;
+          }
+          const uint16_t c = (uint16_t)(w32[m >> 1] >> ((m & 1) * 16));
+          t[p.li][p.b * BS + p.lj] = c;
+          z += c == 0;
+          strip_next(g, p);
+        }
+        if (z) atomicAdd(&bz[zb], z);
+      }
+    }
+  }
+  const int tail0 = sp.head + 8 * sp.nvec;
+  for (int q = threadIdx.x; q < sp.head + (sp.E - tail0); q += STRIP_NT) {
+    const int e = q < sp.head ? q : tail0 + (q - sp.head);
+    const StripPos p = strip_pos(g, e);
+    const uint16_t c = src[e];
+    t[p.li][p.b * BS + p.lj] = c;
+    if (c == 0) atomicAdd(&bz[p.b], 1u);
+  }
+  __syncthreads();
+  if (warp == 0) strip_prefix(P.status, s, ns, g, bz, bpre, &s_excl, lane, flag);
+
+  // raster pairs (the other warps start while warp 0 looks back)
+  const long long row0 = (long long)g.bi * BS;
+  if ((r2 & 3) == 0 && ((reinterpret_cast<uintptr_t>(P.ids) & 3) | (reinterpret_cast<uintptr_t>(P.pair) & 15)) == 0) {
+    // 4 columns per item (W is a multiple of 4 here): one u32 of ids in, two 16-byte pair stores out
+    constexpr int ROW_VEC = (BS * STRIP_W / 4 + STRIP_NT - 1) / STRIP_NT;  // 5
+    const int nq = g.W >> 2, tot = g.h * nq;
+    unsigned int idv[ROW_VEC];
+#pragma unroll
+    for (int u = 0; u < ROW_VEC; u++) {
+      const int q = threadIdx.x + u * STRIP_NT;
+      if (q < tot) {
+        const int li = q / nq;
+        idv[u] = __ldg(reinterpret_cast<const unsigned int*>(P.ids + (row0 + li) * r2 + g.c0) + (q - li * nq));
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < ROW_VEC; u++) {
+      const int q = threadIdx.x + u * STRIP_NT;
+      if (q < tot) {
+        const int li = q / nq, c = 4 * (q - li * nq);
+        const uint2 cw = *reinterpret_cast<const uint2*>(&t[li][c]);
+        const float2 a = dec_pair(cw.x & 0xffffu, idv[u] & 0xffu), b = dec_pair(cw.x >> 16, (idv[u] >> 8) & 0xffu);
+        const float2 d = dec_pair(cw.y & 0xffffu, (idv[u] >> 16) & 0xffu), e = dec_pair(cw.y >> 16, idv[u] >> 24);
+        float4* out = reinterpret_cast<float4*>(P.pair + (row0 + li) * r2 + g.c0 + c);
+        out[0] = make_float4(a.x, a.y, b.x, b.y);
+        out[1] = make_float4(d.x, d.y, e.x, e.y);
+      }
+    }
+  } else {
+#pragma unroll 6
+    for (int q = threadIdx.x; q < g.h * g.W; q += STRIP_NT) {
+      const int li = q / g.W, c = q - li * g.W;
+      const long long gi = (row0 + li) * r2 + g.c0 + c;
+      P.pair[gi] = dec_pair(t[li][c], P.ids[gi]);
+    }
+  }
+  __syncthreads();  // the raw values below overwrite .x of pairs stored above
+
+  // unpredictable values, in block order
+  const unsigned long long excl = s_excl;
+  for (int b = warp; b < g.nb; b += STRIP_NT / 32) {
+    if (bz[b] == 0) continue;
+    const int w = (b == g.nb - 1) ? g.wl : BS;
+    const int nk = g.h * w;
+    unsigned long long run = excl + bpre[b];
+    for (int k0 = 0; k0 < nk; k0 += 32) {
+      const int k = k0 + lane;
+      int li = 0, col = 0;
+      bool z = false;
+      if (k < nk) {
+        li = k / w;
+        col = b * BS + (k - li * w);
+        z = t[li][col] == 0;
+      }
+      const unsigned int m = __ballot_sync(FULLM, z);
+      if (z) {
+        const unsigned long long o = run + __popc(m & lanemask_lt(lane));
+        if (o < P.n_unpred) P.pair[(row0 + li) * r2 + g.c0 + col].x = P.unpred[o];
+        else atomicOr(flag, FLAG_RAW_RANGE);
+      }
+      run += __popc(m);
+    }
+  }
+}
 
 }  // namespace
 
@@ -383,28 +552,6 @@ int launch_scan_u32(cpsz_b200_ctx* ctx, const unsigned int* in, unsigned int* ou
   return check_launch("scan_u32");
 }
 
-int launch_raster_to_blocks_u16(cpsz_b200_ctx* ctx, const uint16_t* raster, long long pitch, int r1, int r2,
-                                uint16_t* blocks, unsigned long long* hist) {
-  long long nseg = nseg_of(r1, r2);
-  int nby = (r2 - 1) / BS + 1;
-  r2b_kernel<<<grid_of(nseg), NT, 0, ctx->stream>>>(raster, pitch, r1, r2, nby, nseg, blocks);
-  count_launch(ctx);
-  CPSZ_TRY(check_launch("r2b_kernel"));
-  if (hist) return launch_hist_u16(ctx, blocks, (size_t)r1 * r2, hist);
-  return CPSZ_OK;
-}
-
-int launch_blocks_to_raster_u16(cpsz_b200_ctx* ctx, const uint16_t* blocks, int r1, int r2, uint16_t* raster,
-                                long long pitch, const uint8_t* ids, float2* pair) {
-  long long nseg = nseg_of(r1, r2);
-  int nby = (r2 - 1) / BS + 1;
-  b2r_kernel<<<grid_of(nseg), NT, 0, ctx->stream>>>(blocks, r1, r2, nby, nseg, raster, pitch, ids, pair);
-  count_launch(ctx);
-  return check_launch("b2r_kernel");
-}
-
-size_t segment_scan_tmp_bytes(int r1, int r2) { return scan_u32_tmp_bytes((size_t)nseg_of(r1, r2)); }
-
 size_t strip_count(int r1, int r2) {
   const long long nbx = (r1 + BS - 1) / BS, nsc = (r2 + STRIP_W - 1) / STRIP_W;
   return (size_t)(nbx * nsc);
@@ -412,56 +559,42 @@ size_t strip_count(int r1, int r2) {
 
 size_t strip_scratch_bytes(int r1, int r2) { return 8 * strip_count(r1, r2) + 8; }
 
+const unsigned int* strip_total(const void* scratch, int r1, int r2) {
+  return (const unsigned int*)((const char*)scratch + 8 * strip_count(r1, r2) + 4);
+}
+
 int launch_strip_pass(cpsz_b200_ctx* ctx, const uint16_t* const raster[2], long long pitch, const float* const x[2],
                       long long x_pitch, int r1, int r2, uint16_t* const blocks[2], float* const unpred[2],
                       void* const scratch[2]) {
   const size_t ns = strip_count(r1, r2);
-  if (ns == 0) return CPSZ_OK;
   if (ns > 0x7fffffffu) return set_error(CPSZ_ERR_UNSUPPORTED, "field of %zu strips", ns);
+  for (int f = 0; f < 2; f++)  // the totals of an empty field read 0
+    CPSZ_CUDA_TRY(cudaMemsetAsync(scratch[f], 0, strip_scratch_bytes(r1, r2), ctx->stream));
+  if (ns == 0) return CPSZ_OK;
   const int nsc = (r2 + STRIP_W - 1) / STRIP_W;
   StripPass P[2];
-  for (int f = 0; f < 2; f++) {
-    CPSZ_CUDA_TRY(cudaMemsetAsync(scratch[f], 0, strip_scratch_bytes(r1, r2), ctx->stream));
-    P[f] = StripPass{raster[f], x[f], blocks[f], unpred[f], (unsigned long long*)scratch[f]};
-  }
+  for (int f = 0; f < 2; f++) P[f] = StripPass{raster[f], x[f], blocks[f], unpred[f], (unsigned long long*)scratch[f]};
   strip_pass_kernel<<<dim3((unsigned)ns, 2), STRIP_NT, 0, ctx->stream>>>(P[0], P[1], pitch, x_pitch, r1, r2, nsc,
                                                                          (unsigned)ns, ctx->d_flag);
   count_launch(ctx);
   return check_launch("strip_pass_kernel");
 }
 
-const unsigned int* strip_total(const void* scratch, int r1, int r2) {
-  return (const unsigned int*)((const char*)scratch + 8 * strip_count(r1, r2) + 4);
-}
-
-int launch_segment_scan(cpsz_b200_ctx* ctx, const uint16_t* codes_raster, long long pitch, int r1, int r2,
-                        unsigned int* seg_count, unsigned int* seg_off, void* scan_tmp) {
-  long long nseg = nseg_of(r1, r2);
-  int nby = (r2 - 1) / BS + 1;
-  seg_count_kernel<<<grid_of(nseg), NT, 0, ctx->stream>>>(codes_raster, pitch, r1, r2, nby, nseg, seg_count);
+int launch_strip_unpass(cpsz_b200_ctx* ctx, const uint16_t* const blocks[2], const uint8_t* const ids[2],
+                        const float* const unpred[2], const unsigned long long n_unpred[2], int r1, int r2,
+                        float2* const pair[2], void* const scratch[2]) {
+  const size_t ns = strip_count(r1, r2);
+  if (ns > 0x7fffffffu) return set_error(CPSZ_ERR_UNSUPPORTED, "field of %zu strips", ns);
+  for (int f = 0; f < 2; f++)  // the totals of an empty field read 0
+    CPSZ_CUDA_TRY(cudaMemsetAsync(scratch[f], 0, strip_scratch_bytes(r1, r2), ctx->stream));
+  if (ns == 0) return CPSZ_OK;
+  const int nsc = (r2 + STRIP_W - 1) / STRIP_W;
+  StripUnpass P[2];
+  for (int f = 0; f < 2; f++) P[f] = StripUnpass{blocks[f], ids[f], unpred[f], n_unpred[f], pair[f], (unsigned long long*)scratch[f]};
+  strip_unpass_kernel<<<dim3((unsigned)ns, 2), STRIP_NT, 0, ctx->stream>>>(P[0], P[1], r1, r2, nsc, (unsigned)ns,
+                                                                           ctx->d_flag);
   count_launch(ctx);
-  CPSZ_TRY(check_launch("seg_count_kernel"));
-  return launch_scan_u32(ctx, seg_count, seg_off, (size_t)nseg, scan_tmp);
-}
-
-int launch_gather_unpred(cpsz_b200_ctx* ctx, const uint16_t* codes_raster, long long pitch, const float* x,
-                         long long x_pitch, int r1, int r2, const unsigned int* seg_off, float* unpred) {
-  long long nseg = nseg_of(r1, r2);
-  int nby = (r2 - 1) / BS + 1;
-  gather_kernel<<<grid_of(nseg), NT, 0, ctx->stream>>>(codes_raster, pitch, x, x_pitch, r1, r2, nby, nseg, seg_off,
-                                                       unpred);
-  count_launch(ctx);
-  return check_launch("gather_kernel");
-}
-
-int launch_scatter_unpred(cpsz_b200_ctx* ctx, const uint16_t* codes_raster, long long pitch, const float* unpred,
-                          unsigned long long n_unpred, int r1, int r2, const unsigned int* seg_off, float2* pairs) {
-  long long nseg = nseg_of(r1, r2);
-  int nby = (r2 - 1) / BS + 1;
-  scatter_kernel<<<grid_of(nseg), NT, 0, ctx->stream>>>(codes_raster, pitch, unpred, n_unpred, r1, r2, nby, nseg,
-                                                        seg_off, pairs, ctx->d_flag);
-  count_launch(ctx);
-  return check_launch("scatter_kernel");
+  return check_launch("strip_unpass_kernel");
 }
 
 }  // namespace cpsz

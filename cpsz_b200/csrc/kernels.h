@@ -96,39 +96,27 @@ int launch_wave2d(cpsz_b200_ctx* ctx, bool decompress, const WaveField* d_fields
                   int n_items, int* d_queue, size_t points, cudaStream_t stream = nullptr, int mode = WAVE_ALONE);
 
 // ---- block-order plumbing (12 x 12 blocks) ---------------------------------------
-// Raster (pitched) -> 12x12-block order, and back.  Histogram of the block-order
-// symbols (65536 bins) fused into the forward permutation.
-int launch_raster_to_blocks_u16(cpsz_b200_ctx* ctx, const uint16_t* raster, long long pitch, int r1, int r2,
-                                uint16_t* blocks, unsigned long long* hist);
-// With pair != NULL also writes, per raster point (pitch r2), the
-// decompression pair (addend 2(code - 32768) * 4^id * 2^-52 (0 for id 0),
-// raw flag bits = (code == 0)).
-int launch_blocks_to_raster_u16(cpsz_b200_ctx* ctx, const uint16_t* blocks, int r1, int r2, uint16_t* raster,
-                                long long pitch, const uint8_t* ids = nullptr, float2* pair = nullptr);
-// Compression side, one launch for both components of a field: codes raster
-// -> 12x12-block order and the unpredictable values (code 0) in block order,
-// in a single pass over strips (a 12-row block row cut into runs of 32
-// blocks) with a decoupled look-back for the unpredictables' offsets.
+// Both directions run as one pass over strips (a 12-row block row cut into
+// runs of 32 blocks), one launch for both components of a field, with a
+// decoupled look-back for the unpredictable values' offsets.
 // scratch[f]: strip_scratch_bytes(r1, r2) bytes (zeroed by the launch); after
-// it, *strip_total(scratch[f], ...) holds the component's unpredictable count.
+// it, *strip_total(scratch[f], ...) holds the component's number of zero codes.
 size_t strip_count(int r1, int r2);
 size_t strip_scratch_bytes(int r1, int r2);
+const unsigned int* strip_total(const void* scratch, int r1, int r2);
+// Compression: codes raster -> 12x12-block order, and the values x at zero
+// codes (unpredictable) into unpred[f] in block order.
 int launch_strip_pass(cpsz_b200_ctx* ctx, const uint16_t* const raster[2], long long pitch, const float* const x[2],
                       long long x_pitch, int r1, int r2, uint16_t* const blocks[2], float* const unpred[2],
                       void* const scratch[2]);
-const unsigned int* strip_total(const void* scratch, int r1, int r2);
-// Zero-code counts per row segment (one 12-wide block row) in block order,
-// exclusive-scanned into seg_off (size r1*nby+1; seg_off[r1*nby] = total).
-int launch_segment_scan(cpsz_b200_ctx* ctx, const uint16_t* codes_raster, long long pitch, int r1, int r2,
-                        unsigned int* seg_count, unsigned int* seg_off, void* scan_tmp);
-size_t segment_scan_tmp_bytes(int r1, int r2);
-// Compress: gather x at zero-code positions into block order (unpred list).
-int launch_gather_unpred(cpsz_b200_ctx* ctx, const uint16_t* codes_raster, long long pitch, const float* x,
-                         long long x_pitch, int r1, int r2, const unsigned int* seg_off, float* unpred);
-// Decompress: scatter the unpred list into the .x of the raster pairs (pitch
-// r2) at zero-code positions.
-int launch_scatter_unpred(cpsz_b200_ctx* ctx, const uint16_t* codes_raster, long long pitch, const float* unpred,
-                          unsigned long long n_unpred, int r1, int r2, const unsigned int* seg_off, float2* pairs);
+// Decompression: block-order codes -> per raster point (pitch r2) the pair the
+// wavefront reads: (addend 2(code - 32768) * 4^id * 2^-52 (0 for id 0), raw
+// flag bits 0), or for code 0 (raw value, raw flag bits 1), the raw values
+// taken from unpred[f] in block order (an index past n_unpred[f] raises
+// FLAG_RAW_RANGE).
+int launch_strip_unpass(cpsz_b200_ctx* ctx, const uint16_t* const blocks[2], const uint8_t* const ids[2],
+                        const float* const unpred[2], const unsigned long long n_unpred[2], int r1, int r2,
+                        float2* const pair[2], void* const scratch[2]);
 
 // ---- Huffman -------------------------------------------------------------------
 // Codebook for the encoder: per symbol, code right-aligned (bit len-1 = first bit).

@@ -606,6 +606,22 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   Job2D* hj = (nj == 1 && jobs[0].host_out) ? &jobs[0] : nullptr;
   const bool h_async = hj && host_kind(hj->host_out) == HOST_PINNED;
   BlobLayout hl;
+  // Page-locked output: each section's copy runs on the aux stream behind its
+  // producer, so the next producer does not wait for it.  The main stream
+  // joins aux before the pass ends; on an early return the guard drains aux, so
+  // no copy out of the workspace outlives the call.
+  struct AuxDrain {
+    cudaStream_t s = nullptr;
+    ~AuxDrain() {
+      if (s) cudaStreamSynchronize(s);
+    }
+  } aux_drain;
+  auto d2h_beside = [&](void* dst, const void* src, size_t n) -> int {
+    CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[6], st));
+    CPSZ_CUDA_TRY(cudaStreamWaitEvent(ctx->aux, ctx->ev[6], 0));
+    aux_drain.s = ctx->aux;
+    return d2h(ctx, dst, src, n, ctx->aux);
+  };
 
   // host: the id trees (their histograms arrived while the wavefront ran) and
   // their bit packing, which the GPU runs right after stage 3 while the host
@@ -633,7 +649,7 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     const size_t at = ids_bits_at(*hj);
     if (at + hj->bits_bytes[0] > hj->host_cap)
       return set_error(CPSZ_ERR_INVALID, "output capacity %zu too small for the blob", hj->host_cap);
-    CPSZ_TRY(d2h(ctx, hj->host_out + at, hj->d.bits[0], hj->bits_bytes[0], st));
+    CPSZ_TRY(d2h_beside(hj->host_out + at, hj->d.bits[0], hj->bits_bytes[0]));
   }
   // code trees, each as soon as its histogram is on the host
   parallel_for(2 * nj, [&](int q) {
@@ -665,7 +681,7 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     for (const BlobLayout::Piece& pc : hl.pieces) memcpy(hj->host_out + pc.dst, hl.small.data() + pc.src, pc.n);
     if (h_async)
       for (int f = 0; f < 2; f++)
-        CPSZ_TRY(d2h(ctx, hj->host_out + hl.unpred_dst[f], hj->d.unpred[f], 4 * hj->n_unpred[f], st));
+        CPSZ_TRY(d2h_beside(hj->host_out + hl.unpred_dst[f], hj->d.unpred[f], 4 * hj->n_unpred[f]));
   }
   for (Job2D& j : jobs) {
     for (int k = 1; k < 3; k++) {
@@ -675,8 +691,12 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       CPSZ_TRY(launch_huff_encode_u16(ctx, j.d.cblocks[k - 1], j.N,
                                       HuffEncTable{j.d.enc_code[k], j.d.enc_len[k], 65536}, j.d.bits[k],
                                       j.codes_bits_cap, nullptr, j.d.enc_tmp[k]));
-      if (h_async) CPSZ_TRY(d2h(ctx, j.host_out + hl.bit_dst[k], j.d.bits[k], j.bits_bytes[k], st));
+      if (h_async) CPSZ_TRY(d2h_beside(j.host_out + hl.bit_dst[k], j.d.bits[k], j.bits_bytes[k]));
     }
+  }
+  if (aux_drain.s) {  // the section copies join the main stream
+    CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[7], ctx->aux));
+    CPSZ_CUDA_TRY(cudaStreamWaitEvent(st, ctx->ev[7], 0));
   }
   {
     int flag = 0;
@@ -845,7 +865,7 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
   const int r1 = (int)r1s, r2 = (int)r2s;
   const size_t N = r1s * r2s;
   const int nby = (r2 - 1) / BS + 1, nbx = (r1 - 1) / BS + 1;
-  const size_t nseg = (size_t)r1 * nby, nblocks = (size_t)nbx * nby;
+  const size_t nblocks = (size_t)nbx * nby;
   const int ngroups = (r1 + WAVE_GROUP_ROWS - 1) / WAVE_GROUP_ROWS;
   int base;
   double thr;
@@ -883,12 +903,10 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
     add(huff_decode_tmp_bytes(hs[k]->nbytes * 8));
   }
   add(4 * N);  // codes blocks
-  add(4 * N);  // codes raster
   add(8 * N);  // (pairs: the raw raster below holds 16 N)
   add(8 * N);  // raw raster
   add(2 * 4 * N);  // unpred lists
-  add(2 * 2 * (nseg + 1) * 4);
-  add(2 * segment_scan_tmp_bytes(r1, r2));
+  add(2 * strip_scratch_bytes(r1, r2));
   add(2 * (size_t)ngroups * r2 * 8);
   add(64);
   add(2 * sizeof(WaveField) + 2 * (size_t)ngroups * sizeof(WaveItem));
@@ -922,19 +940,14 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
     tab[k] = HuffDecTable{lut, child, sym, leaf, h.node_count, h.root_is_leaf ? 1 : 0, h.root_sym};
   }
   uint16_t* cblocks[2];
-  uint16_t* craster[2];
   float2* raw[2];  // (addend, raw flag) per point; .x holds the raw value where the code is 0
   float* unpred[2];
-  unsigned int *seg_cnt[2], *seg_off[2];
-  void* scan_tmp[2];
+  void* strip[2];
   for (int f = 0; f < 2; f++) {
     cblocks[f] = (uint16_t*)A(2 * N);
-    craster[f] = (uint16_t*)A(2 * N);
     raw[f] = (float2*)A(8 * N);
     unpred[f] = (float*)A(4 * fv[f].n_unpred + 4);
-    seg_cnt[f] = (unsigned int*)A((nseg + 1) * 4);
-    seg_off[f] = (unsigned int*)A((nseg + 1) * 4);
-    scan_tmp[f] = A(segment_scan_tmp_bytes(r1, r2));
+    strip[f] = A(strip_scratch_bytes(r1, r2));
     if (fv[f].n_unpred)
       CPSZ_TRY(h2d(ctx, unpred[f], blob + fv[f].unpred_off, 4 * fv[f].n_unpred, st));
   }
@@ -951,14 +964,17 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
   CPSZ_TRY(launch_huff_decode(ctx, bits[0], hid.nbytes, 2 * N, tab[0], ids, 1, dtmp[0]));
   for (int f = 0; f < 2; f++)
     CPSZ_TRY(launch_huff_decode(ctx, bits[1 + f], fv[f].huff.nbytes, N, tab[1 + f], cblocks[f], 2, dtmp[1 + f]));
-  // ---- raster codes, unpredictable scatter ----
+  // ---- raster pairs, unpredictable scatter ----
   mark(ctx, "raster+scatter");
   unsigned int* h_cnt = (unsigned int*)ctx->pinned + 16;
-  for (int f = 0; f < 2; f++) {
-    CPSZ_TRY(launch_blocks_to_raster_u16(ctx, cblocks[f], r1, r2, craster[f], r2, ids + (size_t)f * N, raw[f]));
-    CPSZ_TRY(launch_segment_scan(ctx, craster[f], r2, r1, r2, seg_cnt[f], seg_off[f], scan_tmp[f]));
-    CPSZ_TRY(launch_scatter_unpred(ctx, craster[f], r2, unpred[f], fv[f].n_unpred, r1, r2, seg_off[f], raw[f]));
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(h_cnt + f, seg_off[f] + nseg, 4, cudaMemcpyDeviceToHost, st));
+  {
+    const uint16_t* cb[2] = {cblocks[0], cblocks[1]};
+    const uint8_t* idf[2] = {ids, ids + N};
+    const float* un[2] = {unpred[0], unpred[1]};
+    const unsigned long long nun[2] = {fv[0].n_unpred, fv[1].n_unpred};
+    CPSZ_TRY(launch_strip_unpass(ctx, cb, idf, un, nun, r1, r2, raw, strip));
+    for (int f = 0; f < 2; f++)
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(h_cnt + f, strip_total(strip[f], r1, r2), 4, cudaMemcpyDeviceToHost, st));
   }
   // ---- wavefront ----
   WaveField hf[2] = {};
