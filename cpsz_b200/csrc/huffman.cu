@@ -286,13 +286,63 @@ __device__ __forceinline__ int decode_one(const BitReader& br, const uint32_t* l
   return 0;
 }
 
+// A sequential reader: the next bits MSB-first in a 64-bit register, refilled
+// a word at a time, so a symbol found by the table costs no memory access.
+// Holds at least 32 valid bits between symbols.
+struct BitCursor {
+  const uint32_t* w;
+  unsigned long long buf;
+  unsigned long long wi;  // the next word to load
+  int nb;                 // valid bits in buf
+  __device__ __forceinline__ void seek(unsigned long long pos) {
+    wi = pos >> 5;
+    const unsigned long long a = bswap32(__ldg(w + wi)), b = bswap32(__ldg(w + wi + 1));
+    buf = ((a << 32) | b) << (pos & 31);
+    nb = 64 - (int)(pos & 31);
+    wi += 2;
+  }
+  __device__ __forceinline__ void skip(int l) {  // 1 <= l <= 32
+    buf <<= l;
+    nb -= l;
+    if (nb <= 32) {
+      buf |= (unsigned long long)bswap32(__ldg(w + wi)) << (32 - nb);
+      nb += 32;
+      wi++;
+    }
+  }
+};
+
+// decode_one on the cursor, which sits at `pos`; advances it past the symbol.
+__device__ __forceinline__ int decode_cur(BitCursor& c, const BitReader& br, const uint32_t* lut,
+                                          const HuffDecTable& T, unsigned long long pos, uint32_t* sym) {
+  const uint32_t e = lut[(uint32_t)(c.buf >> (64 - HUFF_LUT_BITS))];
+  if (!(e & 0x80)) {
+    *sym = e >> 8;
+    const int l = (int)(e & 0x7f);
+    c.skip(l);
+    return l;
+  }
+  const int l = decode_one(br, lut, T, pos, sym);  // a code longer than the table: walk the tree
+  if (l > 0) c.seek(pos + l);
+  return l;
+}
+
 __device__ __forceinline__ void load_lut(uint32_t* slut, const uint32_t* lut) {
   for (int k = threadIdx.x; k < (1 << HUFF_LUT_BITS); k += blockDim.x) slut[k] = lut[k];
   __syncthreads();
 }
 
-// Phase 1/2: decode subsequence t from start[t] (or nominal) to its limit, or
-// from the predecessor's exit when `resync` and that differs.
+// Count word bit: the subsequence's decode ran into an invalid code (possible
+// from an unsynchronised start; on the true path only in a corrupt stream).
+constexpr unsigned int DEC_INVALID = 0x80000000u;
+
+// Phase 1: decode subsequence t from its nominal start to its limit.
+// Phase 2 (resync): subsequence t restarts from its predecessor's exit when
+// that differs from its start.  Huffman codes resynchronise within a few
+// symbols, so the new path runs in lockstep with the previous one (always
+// advancing the one behind): once both reach the same bit position the rest
+// equals the previous decode, whose exit and count (less the symbols before
+// that position) carry over.
 __global__ void __launch_bounds__(DEC_NT) dec_scan_kernel(BitReader br, HuffDecTable T, unsigned long long nbits,
                                                           int nsub, unsigned long long* __restrict__ start,
                                                           unsigned long long* __restrict__ end,
@@ -302,42 +352,78 @@ __global__ void __launch_bounds__(DEC_NT) dec_scan_kernel(BitReader br, HuffDecT
   load_lut(slut, T.lut);
   int t = blockIdx.x * DEC_NT + threadIdx.x;
   if (t >= nsub) return;
-  unsigned long long s;
-  if (!resync) {
-    s = (unsigned long long)t * DEC_S;
-    start[t] = s;
-  } else {
-    if (t == 0) return;
-    s = end[t - 1];
-    if (s == start[t]) return;
-    start[t] = s;
-    *changed = 1;
-  }
   unsigned long long lim = (unsigned long long)(t + 1) * DEC_S;
   if (lim > nbits) lim = nbits;
-  unsigned long long pos = s;
-  unsigned int c = 0;
-  while (pos < lim) {
-    uint32_t sym;
-    int l = decode_one(br, slut, T, pos, &sym);
+  uint32_t sym;
+  if (!resync) {
+    unsigned long long pos = (unsigned long long)t * DEC_S;
+    start[t] = pos;
+    BitCursor cur{br.w};
+    cur.seek(pos);
+    unsigned int c = 0;
+    while (pos < lim) {
+      const int l = decode_cur(cur, br, slut, T, pos, &sym);
+      if (l == 0) {
+        if (t == 0) atomicOr(flag, FLAG_HUFF_CORRUPT);
+        c |= DEC_INVALID;
+        pos = lim;
+        break;
+      }
+      pos += l;
+      c++;
+    }
+    end[t] = pos;
+    cnt[t] = c;
+    return;
+  }
+  if (t == 0) return;
+  const unsigned long long s = end[t - 1], s_old = start[t];
+  if (s == s_old) return;
+  const unsigned long long e_old = end[t];
+  const unsigned int c_old = cnt[t];
+  start[t] = s;
+  *changed = 1;
+  unsigned long long a = s, b = s_old;  // the new path, the previous one
+  unsigned int ca = 0, cb = 0;
+  bool old_ok = true;
+  while (a < lim) {
+    if (old_ok && b < a) {  // b < a < lim: still on the previous decode
+      const int l = decode_one(br, slut, T, b, &sym);
+      if (l == 0) old_ok = false;
+      b += l;
+      cb++;
+      continue;
+    }
+    if (old_ok && a == b) {
+      if (c_old & DEC_INVALID) atomicOr(flag, FLAG_HUFF_CORRUPT);
+      end[t] = e_old;
+      cnt[t] = ca + ((c_old & ~DEC_INVALID) - cb);
+      return;
+    }
+    const int l = decode_one(br, slut, T, a, &sym);
     if (l == 0) {
-      // an unsynchronised start may run into invalid paths only on a corrupt stream
-      if (resync || t == 0) atomicOr(flag, FLAG_HUFF_CORRUPT);
-      pos = lim;
+      atomicOr(flag, FLAG_HUFF_CORRUPT);
+      a = lim;
       break;
     }
-    pos += l;
-    c++;
+    a += l;
+    ca++;
   }
-  end[t] = pos;
-  cnt[t] = c;
+  end[t] = a;
+  cnt[t] = ca;
 }
 
+// Phase 3: subsequence t writes its symbols from output index off[t].  A
+// thread's symbols are packed into aligned 64-bit stores (single stores at the
+// unaligned head and tail of its range): one store per symbol, each to its
+// own line, made the write rate the limit.
 template <class Out>
 __global__ void __launch_bounds__(DEC_NT) dec_write_kernel(BitReader br, HuffDecTable T, unsigned long long nbits,
                                                            int nsub, const unsigned long long* __restrict__ start,
                                                            const unsigned long long* __restrict__ off,
                                                            size_t n, Out* __restrict__ out) {
+  constexpr int PER = 8 / sizeof(Out);
+  constexpr int SB = 8 * sizeof(Out);
   __shared__ uint32_t slut[1 << HUFF_LUT_BITS];
   load_lut(slut, T.lut);
   int t = blockIdx.x * DEC_NT + threadIdx.x;
@@ -346,13 +432,29 @@ __global__ void __launch_bounds__(DEC_NT) dec_write_kernel(BitReader br, HuffDec
   if (lim > nbits) lim = nbits;
   unsigned long long pos = start[t];
   unsigned long long o = off[t];
+  const bool packed = (reinterpret_cast<uintptr_t>(out) & 7) == 0;
+  BitCursor cur{br.w};
+  cur.seek(pos);
+  unsigned long long acc = 0;
+  int na = 0;  // symbols in acc, which starts at an aligned index
   while (pos < lim && o < n) {
     uint32_t sym;
-    int l = decode_one(br, slut, T, pos, &sym);
+    const int l = decode_cur(cur, br, slut, T, pos, &sym);
     if (l == 0) break;
-    out[o++] = (Out)sym;
     pos += l;
+    if (na == 0 && (!packed || (o % PER) != 0)) {
+      out[o++] = (Out)sym;
+      continue;
+    }
+    acc |= (unsigned long long)(Out)sym << (SB * na);
+    o++;
+    if (++na == PER) {
+      *reinterpret_cast<unsigned long long*>(out + (o - PER)) = acc;
+      acc = 0;
+      na = 0;
+    }
   }
+  for (int k = 0; k < na; k++) out[o - na + k] = (Out)(acc >> (SB * k));
 }
 
 __global__ void fill_kernel_u8(uint8_t* out, size_t n, uint8_t v) {
@@ -364,7 +466,7 @@ __global__ void fill_kernel_u16(uint16_t* out, size_t n, uint16_t v) {
 
 __global__ void u32_to_u64_kernel(const unsigned int* in, unsigned long long* out, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) out[i] = in[i];
+  if (i < n) out[i] = in[i] & ~DEC_INVALID;
 }
 
 __global__ void check_total_kernel(const unsigned long long* off, int nsub, size_t n, int* flag) {
