@@ -698,19 +698,25 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[7], ctx->aux));
     CPSZ_CUDA_TRY(cudaStreamWaitEvent(st, ctx->ev[7], 0));
   }
-  {
-    int flag = 0;
-    CPSZ_TRY(read_flag(ctx, &flag));  // synchronizes the stream: the counts below have landed
-    if (flag) return flag_error(flag);
-  }
+  // ---- stage 5: blob assembly in device memory, enqueued behind the encoders
+  // (the unpredictable counts it needs are on the host since stage 3), or, for
+  // host output, the sections not yet copied ----
+  CPSZ_CUDA_TRY(cudaEventSynchronize(ctx->ev[5]));
   for (Job2D& j : jobs) {
     j.n_unpred[0] = j.h_nunpred[0];
     j.n_unpred[1] = j.h_nunpred[1];
   }
-
-  // ---- stage 5: blob assembly in device memory (or, for host output, the
-  // sections not yet copied) ----
   mark(ctx, "blob_assembly");
+  int assembled = CPSZ_OK;
+  if (!hj)
+    for (Job2D& j : jobs)
+      if ((assembled = job_assemble(ctx, j)) != CPSZ_OK) break;
+  {
+    int flag = 0;
+    CPSZ_TRY(read_flag(ctx, &flag));  // synchronizes the stream; a kernel's error outranks the assembly's
+    if (flag) return flag_error(flag);
+  }
+  if (assembled != CPSZ_OK) return assembled;
   if (hj) {
     if (!h_async) {
       CPSZ_TRY(d2h(ctx, hj->host_out + hl.bit_dst[0], hj->d.bits[0], hj->bits_bytes[0], st));
@@ -719,8 +725,6 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       for (int k = 1; k < 3; k++) CPSZ_TRY(d2h(ctx, hj->host_out + hl.bit_dst[k], hj->d.bits[k], hj->bits_bytes[k], st));
     }
     hj->size = hl.total;
-  } else {
-    for (Job2D& j : jobs) CPSZ_TRY(job_assemble(ctx, j));
   }
   mark(ctx, "end");
   if (tap) {
