@@ -349,8 +349,11 @@ __global__ void __launch_bounds__(DEC_NT) dec_scan_kernel(BitReader br, HuffDecT
                                                           unsigned int* __restrict__ cnt, int resync,
                                                           int* __restrict__ changed, int* flag) {
   __shared__ uint32_t slut[1 << HUFF_LUT_BITS];
-  load_lut(slut, T.lut);
   int t = blockIdx.x * DEC_NT + threadIdx.x;
+  // a resynchronisation round leaves at once the blocks with no start to
+  // move (most of them after the first round), without loading the table
+  if (resync && !__syncthreads_or(t > 0 && t < nsub && end[t - 1] != start[t])) return;
+  load_lut(slut, T.lut);
   if (t >= nsub) return;
   unsigned long long lim = (unsigned long long)(t + 1) * DEC_S;
   if (lim > nbits) lim = nbits;
