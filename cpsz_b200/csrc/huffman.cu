@@ -467,9 +467,14 @@ __global__ void fill_kernel_u16(uint16_t* out, size_t n, uint16_t v) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) out[i] = v;
 }
 
-__global__ void u32_to_u64_kernel(const unsigned int* in, unsigned long long* out, int n) {
+__global__ void u32_to_u64_kernel(const unsigned int* in, unsigned long long* out, int n, unsigned int mask) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) out[i] = in[i] & ~DEC_INVALID;
+  if (i < n) out[i] = in[i] & mask;
+}
+
+__global__ void clear_invalid_kernel(unsigned int* cnt, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) cnt[i] &= ~DEC_INVALID;
 }
 
 __global__ void check_total_kernel(const unsigned long long* off, int nsub, size_t n, int* flag) {
@@ -505,7 +510,7 @@ int launch_hist_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, unsigned 
 
 size_t huff_decode_tmp_bytes(size_t nbits) {
   size_t nsub = (nbits + DEC_S - 1) / DEC_S + 1;
-  return align_up(nsub + 1, 32) * 8 * 3 + align_up(nsub + 1, 32) * 4 * 2 + 4096;
+  return align_up(nsub + 1, 32) * 8 * 3 + align_up(nsub + 1, 32) * 4 * 2 + 4096 + scan_u32_tmp_bytes(nsub + 1);
 }
 
 int launch_huff_decode(cpsz_b200_ctx* ctx, const uint8_t* bytes, size_t nbytes, size_t n, HuffDecTable tab, void* out,
@@ -547,9 +552,20 @@ int launch_huff_decode(cpsz_b200_ctx* ctx, const uint8_t* bytes, size_t nbytes, 
     CPSZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     if (!*h_changed) break;
   }
-  unsigned long long* cnt64 = end;  // reuse: exits no longer needed after the final round
-  u32_to_u64_kernel<<<(nsub + 255) / 256, 256, 0, ctx->stream>>>(cnt, cnt64, nsub);
-  scan_u64_kernel<<<1, 1024, 0, ctx->stream>>>(cnt64, off, (size_t)nsub);
+  // output offsets: a device-wide u32 scan when every offset fits 32 bits (a
+  // subsequence decodes at most one symbol per bit, plus the one crossing its
+  // end), else one CTA over 64-bit counts; the exits are no longer needed
+  // after the final round, so their array holds the counts' copy
+  if (nbits + (unsigned long long)nsub < (1ull << 32)) {
+    unsigned int* off32 = reinterpret_cast<unsigned int*>(end);
+    clear_invalid_kernel<<<(nsub + 255) / 256, 256, 0, ctx->stream>>>(cnt, nsub);
+    CPSZ_TRY(launch_scan_u32(ctx, cnt, off32, (size_t)nsub, p + 256));  // off32[nsub] = the total
+    u32_to_u64_kernel<<<(nsub + 256) / 256, 256, 0, ctx->stream>>>(off32, off, nsub + 1, 0xffffffffu);
+  } else {
+    unsigned long long* cnt64 = end;
+    u32_to_u64_kernel<<<(nsub + 255) / 256, 256, 0, ctx->stream>>>(cnt, cnt64, nsub, ~DEC_INVALID);
+    scan_u64_kernel<<<1, 1024, 0, ctx->stream>>>(cnt64, off, (size_t)nsub);
+  }
   check_total_kernel<<<1, 1, 0, ctx->stream>>>(off, nsub, n, ctx->d_flag);
   if (out_bytes_per_sym == 1)
     dec_write_kernel<uint8_t><<<grid, DEC_NT, 0, ctx->stream>>>(br, tab, nbits, nsub, start, off, n, (uint8_t*)out);
