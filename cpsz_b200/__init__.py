@@ -55,6 +55,8 @@ def _declare(L):
     L.cpsz_b200_ctx_kernel_launches.argtypes = [_vp, C.POINTER(C.c_uint64)]
     L.cpsz_b200_ctx_graph_stats.argtypes = [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.cpsz_b200_ctx_stream.argtypes = [_vp, C.POINTER(_vp)]
+    L.cpsz_b200_ctx_wave_reruns.argtypes = [_vp, C.POINTER(C.c_uint64)]
+    L.cpsz_b200_debug_band_wait.argtypes = [_vp, C.c_longlong, C.c_int]
     L.cpsz_b200_compress_2d_offline_f32.argtypes = [_vp, _vp, _vp, _sz, _sz, C.c_double, C.POINTER(_vp), C.POINTER(_sz)]
     L.cpsz_b200_compress_2d_offline_f32_into.argtypes = [_vp, _vp, _vp, _sz, _sz, C.c_double, _vp, _sz, C.POINTER(_sz)]
     L.cpsz_b200_decompress_2d_offline_f32.argtypes = [_vp, C.c_char_p, _sz, _sz, _sz, _vp, _vp]
@@ -165,6 +167,19 @@ class Context:
         c, r = C.c_uint64(), C.c_uint64()
         _check(lib().cpsz_b200_ctx_graph_stats(self.handle, C.byref(c), C.byref(r)))
         return c.value, r.value
+
+    @property
+    def wave_reruns(self) -> int:
+        """Passes whose wavefront ran again after the bounds because a wait
+        beside the bound kernel gave up (``cpsz_b200_ctx_wave_reruns``)."""
+        v = C.c_uint64()
+        _check(lib().cpsz_b200_ctx_wave_reruns(self.handle, C.byref(v)))
+        return v.value
+
+    def debug_band_wait(self, wait_ns: int = 0, unreachable: bool = False) -> None:
+        """Limit of the wavefront's per-group wait for the bounds (0 = default);
+        ``unreachable`` makes every such wait run out (``cpsz_b200_debug_band_wait``)."""
+        _check(lib().cpsz_b200_debug_band_wait(self.handle, int(wait_ns), int(bool(unreachable))))
 
     @property
     def stream(self) -> int:

@@ -18,6 +18,14 @@
 // table ("eb2d.tile", tuning.h) picks one of six instantiations per field
 // size.  Every shape computes the same bytes: each vertex's bound is the same
 // minimum over the same six triangles, whichever tile evaluates them.
+//
+// CTAs are persistent: the grid holds as many CTAs as fit on the device (one
+// per SM fewer when the Lorenzo wavefront runs beside the kernel) and each
+// takes tiles in row-major order with a grid stride, so row groups complete
+// in order.  A kernel enqueued first and holding a fixed number of slots per
+// SM leaves exactly one slot on every SM for the wavefront launched after it.
+#include <algorithm>
+
 #include "eb_math.cuh"
 #include "kernels.h"
 #include "tuning.h"
@@ -33,7 +41,8 @@ __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const f
                                                   unsigned long long* __restrict__ hist, int* __restrict__ flag,
                                                   float2* __restrict__ pair_u, float2* __restrict__ pair_v,
                                                   double* __restrict__ eb_out, int row_begin, int row_end,
-                                                  unsigned long long* __restrict__ band_done) {
+                                                  unsigned long long* __restrict__ band_done, int tiles_x,
+                                                  int ntiles) {
   constexpr int CX = TX + 1;  // cells per tile row
   constexpr int CY = TY + 1;
   static_assert(WAVE_GROUP_ROWS % TY == 0, "a tile's rows must lie in one wavefront group");
@@ -44,152 +53,155 @@ __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const f
   __shared__ unsigned int shist[256];
 
   const int tid = threadIdx.x;
-  const int i0 = row_begin + blockIdx.y * TY, j0 = blockIdx.x * TX;
   for (int k = tid; k < 256; k += NT) shist[k] = 0;
   for (int k = tid; k < thr_n; k += NT) tab[k] = thr_tab[k];
-  // vertex halo: rows i0-1 .. i0+TY, cols j0-1 .. j0+TX
-  for (int k = tid; k < (TY + 2) * (TX + 2); k += NT) {
-    int a = k / (TX + 2), b = k % (TX + 2);
-    int gi = i0 - 1 + a, gj = j0 - 1 + b;
-    float u = 0.f, v = 0.f;
-    if (gi >= 0 && gi < r1 && gj >= 0 && gj < r2) {
-      size_t g = (size_t)gi * r2 + gj;
-      u = U[g];
-      v = V[g];
-    }
-    su[a][b] = u;
-    sv[a][b] = v;
-  }
-  __syncthreads();
-  // triangles of cells (ci, cj) = (i0-1+a, j0-1+b), a in [0, CY), b in [0, CX);
-  // one triangle per thread and round (2 * 561 triangles over 256 threads at 32x16)
-  for (int k = tid; k < 2 * CY * CX; k += NT) {
-    const int kind = k >= CY * CX;
-    const int c = k - kind * CY * CX;
-    const int a = c / CX, b = c % CX;
-    const int ci = i0 - 1 + a, cj = j0 - 1 + b;
-    double e = 0;
-    if (ci >= 0 && ci < r1 - 1 && cj >= 0 && cj < r2 - 1) {
-      // upper: offsets {0, r2, r2+1} -> (a,b), (a+1,b), (a+1,b+1);
-      // lower: offsets {0, 1, r2+1} -> (a,b), (a,b+1), (a+1,b+1).
-      // One call site keeps a single copy of the bound code in the
-      // instruction cache.
-      const int a1 = a + (kind == 0), b1 = b + (kind == 1);
-      if (FAST)
-        e = dev::tri_eb_filtered(su[a][b], su[a1][b1], su[a + 1][b + 1], sv[a][b], sv[a1][b1], sv[a + 1][b + 1],
-                                 kind);
-      else
-        e = dev::tri_eb(su[a][b], su[a1][b1], su[a + 1][b + 1], sv[a][b], sv[a1][b1], sv[a + 1][b + 1], kind);
-    }
-    tri[kind][a][b] = e;
-  }
-  __syncthreads();
-  const double thr = tab[0];
-  // id of a quantized bound e (-1 for precision 0), before the range check
-  auto quant = [&](double e) -> int {
-    if (e <= thr) return -1;
-    const int ex = (int)((__double_as_longlong(e) >> 52) & 0x7ff) - 1023;
-    return dev::count_thresholds(tab, thr_n, e, (ex + 52) >> 1);
-  };
-  for (int k = tid; k < TY * TX; k += NT) {
-    int a = k / TX, b = k % TX;
-    int gi = i0 + a, gj = j0 + b;
-    if (gi >= row_end || gj >= r2) continue;
-    // vertex (gi, gj) is local (a+1, b+1); cell (gi-1+x, gj-1+y) is tri[.][a+x][b+y]
-    bool up = gi >= 1, left = gj >= 1, down = gi < r1 - 1, right = gj < r2 - 1;
-    const float uu = su[a + 1][b + 1], vv = sv[a + 1][b + 1];
-    // the reference's chain eb = MINF(eb, triangle bound) over the six triangles
-    auto vertex_eb = [&](auto&& tri_at) {
-      double eb = max_pwr_eb;
-      if (up && left) {
-        eb = dev::minf_d(eb, tri_at(0, a, b));
-        eb = dev::minf_d(eb, tri_at(1, a, b));
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int i0 = row_begin + (tile / tiles_x) * TY, j0 = (tile % tiles_x) * TX;
+    __syncthreads();  // the previous tile's readers of su / sv / tri are done
+    // vertex halo: rows i0-1 .. i0+TY, cols j0-1 .. j0+TX
+    for (int k = tid; k < (TY + 2) * (TX + 2); k += NT) {
+      int a = k / (TX + 2), b = k % (TX + 2);
+      int gi = i0 - 1 + a, gj = j0 - 1 + b;
+      float u = 0.f, v = 0.f;
+      if (gi >= 0 && gi < r1 && gj >= 0 && gj < r2) {
+        size_t g = (size_t)gi * r2 + gj;
+        u = U[g];
+        v = V[g];
       }
-      if (up && right) eb = dev::minf_d(eb, tri_at(0, a, b + 1));
-      if (down && left) eb = dev::minf_d(eb, tri_at(1, a + 1, b));
-      if (down && right) {
-        eb = dev::minf_d(eb, tri_at(0, a + 1, b + 1));
-        eb = dev::minf_d(eb, tri_at(1, a + 1, b + 1));
+      su[a][b] = u;
+      sv[a][b] = v;
+    }
+    __syncthreads();
+    // triangles of cells (ci, cj) = (i0-1+a, j0-1+b), a in [0, CY), b in [0, CX);
+    // one triangle per thread and round (2 * 561 triangles over 256 threads at 32x16)
+    for (int k = tid; k < 2 * CY * CX; k += NT) {
+      const int kind = k >= CY * CX;
+      const int c = k - kind * CY * CX;
+      const int a = c / CX, b = c % CX;
+      const int ci = i0 - 1 + a, cj = j0 - 1 + b;
+      double e = 0;
+      if (ci >= 0 && ci < r1 - 1 && cj >= 0 && cj < r2 - 1) {
+        // upper: offsets {0, r2, r2+1} -> (a,b), (a+1,b), (a+1,b+1);
+        // lower: offsets {0, 1, r2+1} -> (a,b), (a,b+1), (a+1,b+1).
+        // One call site keeps a single copy of the bound code in the
+        // instruction cache.
+        const int a1 = a + (kind == 0), b1 = b + (kind == 1);
+        if (FAST)
+          e = dev::tri_eb_filtered(su[a][b], su[a1][b1], su[a + 1][b + 1], sv[a][b], sv[a1][b1], sv[a + 1][b + 1],
+                                   kind);
+        else
+          e = dev::tri_eb(su[a][b], su[a1][b1], su[a + 1][b + 1], sv[a][b], sv[a1][b1], sv[a + 1][b + 1], kind);
       }
-      return eb;
+      tri[kind][a][b] = e;
+    }
+    __syncthreads();
+    const double thr = tab[0];
+    // id of a quantized bound e (-1 for precision 0), before the range check
+    auto quant = [&](double e) -> int {
+      if (e <= thr) return -1;
+      const int ex = (int)((__double_as_longlong(e) >> 52) & 0x7ff) - 1023;
+      return dev::count_thresholds(tab, thr_n, e, (ex + 52) >> 1);
     };
-    int code[2];
-    double eb = 0;
-    if (FAST) {
-      // enclosure of the vertex bound from the filtered triangle bounds
-      double m = INFINITY;
-      bool nan = false;
-      auto take = [&](double t) {
-        nan |= isnan(t);
-        m = fmin(m, t);
+    for (int k = tid; k < TY * TX; k += NT) {
+      int a = k / TX, b = k % TX;
+      int gi = i0 + a, gj = j0 + b;
+      if (gi >= row_end || gj >= r2) continue;
+      // vertex (gi, gj) is local (a+1, b+1); cell (gi-1+x, gj-1+y) is tri[.][a+x][b+y]
+      bool up = gi >= 1, left = gj >= 1, down = gi < r1 - 1, right = gj < r2 - 1;
+      const float uu = su[a + 1][b + 1], vv = sv[a + 1][b + 1];
+      // the reference's chain eb = MINF(eb, triangle bound) over the six triangles
+      auto vertex_eb = [&](auto&& tri_at) {
+        double eb = max_pwr_eb;
+        if (up && left) {
+          eb = dev::minf_d(eb, tri_at(0, a, b));
+          eb = dev::minf_d(eb, tri_at(1, a, b));
+        }
+        if (up && right) eb = dev::minf_d(eb, tri_at(0, a, b + 1));
+        if (down && left) eb = dev::minf_d(eb, tri_at(1, a + 1, b));
+        if (down && right) {
+          eb = dev::minf_d(eb, tri_at(0, a + 1, b + 1));
+          eb = dev::minf_d(eb, tri_at(1, a + 1, b + 1));
+        }
+        return eb;
       };
-      if (up && left) {
-        take(tri[0][a][b]);
-        take(tri[1][a][b]);
-      }
-      if (up && right) take(tri[0][a][b + 1]);
-      if (down && left) take(tri[1][a + 1][b]);
-      if (down && right) {
-        take(tri[0][a + 1][b + 1]);
-        take(tri[1][a + 1][b + 1]);
-      }
-      const double lo = fmin(max_pwr_eb, m * (1.0 - dev::FILTER_REL) - dev::FILTER_ABS);
-      const double hi = fmin(max_pwr_eb, m * (1.0 + dev::FILTER_REL) + dev::FILTER_ABS);
-      code[0] = quant((double)fabsf(uu) * lo);
-      code[1] = quant((double)fabsf(vv) * lo);
-      // the upper end has the same id iff it stays below the next threshold
-      auto stays = [&](int c, double e) { return c < 0 ? e <= thr : (c + 1 >= thr_n || e < tab[c + 1]); };
-      if (nan || !stays(code[0], (double)fabsf(uu) * hi) || !stays(code[1], (double)fabsf(vv) * hi)) {
-        // the enclosure straddles a threshold (or a bound is NaN): exact bounds
-        eb = vertex_eb([&](int kind, int ca, int cb) {
-          const int a1 = ca + (kind == 0), b1 = cb + (kind == 1);
-          return dev::tri_eb_exact(su[ca][cb], su[a1][b1], su[ca + 1][cb + 1], sv[ca][cb], sv[a1][b1],
-                                   sv[ca + 1][cb + 1], kind);
-        });
+      int code[2];
+      double eb = 0;
+      if (FAST) {
+        // enclosure of the vertex bound from the filtered triangle bounds
+        double m = INFINITY;
+        bool nan = false;
+        auto take = [&](double t) {
+          nan |= isnan(t);
+          m = fmin(m, t);
+        };
+        if (up && left) {
+          take(tri[0][a][b]);
+          take(tri[1][a][b]);
+        }
+        if (up && right) take(tri[0][a][b + 1]);
+        if (down && left) take(tri[1][a + 1][b]);
+        if (down && right) {
+          take(tri[0][a + 1][b + 1]);
+          take(tri[1][a + 1][b + 1]);
+        }
+        const double lo = fmin(max_pwr_eb, m * (1.0 - dev::FILTER_REL) - dev::FILTER_ABS);
+        const double hi = fmin(max_pwr_eb, m * (1.0 + dev::FILTER_REL) + dev::FILTER_ABS);
+        code[0] = quant((double)fabsf(uu) * lo);
+        code[1] = quant((double)fabsf(vv) * lo);
+        // the upper end has the same id iff it stays below the next threshold
+        auto stays = [&](int c, double e) { return c < 0 ? e <= thr : (c + 1 >= thr_n || e < tab[c + 1]); };
+        if (nan || !stays(code[0], (double)fabsf(uu) * hi) || !stays(code[1], (double)fabsf(vv) * hi)) {
+          // the enclosure straddles a threshold (or a bound is NaN): exact bounds
+          eb = vertex_eb([&](int kind, int ca, int cb) {
+            const int a1 = ca + (kind == 0), b1 = cb + (kind == 1);
+            return dev::tri_eb_exact(su[ca][cb], su[a1][b1], su[ca + 1][cb + 1], sv[ca][cb], sv[a1][b1],
+                                     sv[ca + 1][cb + 1], kind);
+          });
+          code[0] = quant((double)fabsf(uu) * eb);
+          code[1] = quant((double)fabsf(vv) * eb);
+        }
+      } else {
+        eb = vertex_eb([&](int kind, int ca, int cb) { return tri[kind][ca][cb]; });
         code[0] = quant((double)fabsf(uu) * eb);
         code[1] = quant((double)fabsf(vv) * eb);
       }
-    } else {
-      eb = vertex_eb([&](int kind, int ca, int cb) { return tri[kind][ca][cb]; });
-      code[0] = quant((double)fabsf(uu) * eb);
-      code[1] = quant((double)fabsf(vv) * eb);
-    }
-    int sym[2];
-#pragma unroll
-    for (int c = 0; c < 2; c++) {
-      if (code[c] > ID_MAX_2D) {
-        atomicOr(flag, FLAG_ID_OVERFLOW);
-        code[c] = ID_MAX_2D;
+      int sym[2];
+  #pragma unroll
+      for (int c = 0; c < 2; c++) {
+        if (code[c] > ID_MAX_2D) {
+          atomicOr(flag, FLAG_ID_OVERFLOW);
+          code[c] = ID_MAX_2D;
+        }
+        sym[c] = code[c] < 0 ? 0 : code[c];
+        if (code[c] < 0) code[c] = ID_ZERO;
       }
-      sym[c] = code[c] < 0 ? 0 : code[c];
-      if (code[c] < 0) code[c] = ID_ZERO;
+      size_t g = (size_t)gi * r2 + gj;
+      if (!FAST && eb_out) eb_out[g] = eb;
+      ids_u[g] = (uint8_t)code[0];
+      ids_v[g] = (uint8_t)code[1];
+      if (pair_u) {
+        // the wavefront's input: value and 1/precision = 2^(52 - 2 id) (NaN for precision 0)
+        pair_u[g] = make_float2(uu, code[0] == ID_ZERO ? __int_as_float(0x7FC00000)
+                                                       : __int_as_float((127 + 52 - 2 * (int)code[0]) << 23));
+        pair_v[g] = make_float2(vv, code[1] == ID_ZERO ? __int_as_float(0x7FC00000)
+                                                       : __int_as_float((127 + 52 - 2 * (int)code[1]) << 23));
+      }
+      atomicAdd(&shist[sym[0]], 1u);
+      atomicAdd(&shist[sym[1]], 1u);
     }
-    size_t g = (size_t)gi * r2 + gj;
-    if (!FAST && eb_out) eb_out[g] = eb;
-    ids_u[g] = (uint8_t)code[0];
-    ids_v[g] = (uint8_t)code[1];
-    if (pair_u) {
-      // the wavefront's input: value and 1/precision = 2^(52 - 2 id) (NaN for precision 0)
-      pair_u[g] = make_float2(uu, code[0] == ID_ZERO ? __int_as_float(0x7FC00000)
-                                                     : __int_as_float((127 + 52 - 2 * (int)code[0]) << 23));
-      pair_v[g] = make_float2(vv, code[1] == ID_ZERO ? __int_as_float(0x7FC00000)
-                                                     : __int_as_float((127 + 52 - 2 * (int)code[1]) << 23));
+    if (band_done) {
+      // every thread's outputs are visible device-wide before the tile counts
+      __threadfence();
+      __syncthreads();
+      if (tid == 0) {
+        const int rows = min(TY, row_end - i0), cols = min(TX, r2 - j0);
+        atomicAdd(&band_done[i0 / WAVE_GROUP_ROWS], (unsigned long long)rows * cols);
+      }
     }
-    atomicAdd(&shist[sym[0]], 1u);
-    atomicAdd(&shist[sym[1]], 1u);
-  }
+  }  // tiles
   __syncthreads();
   for (int k = tid; k < 256; k += NT)
     if (shist[k]) atomicAdd(&hist[k], (unsigned long long)shist[k]);
-  if (band_done) {
-    // every thread's outputs are visible device-wide before the tile counts
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) {
-      const int rows = min(TY, row_end - i0), cols = min(TX, r2 - j0);
-      atomicAdd(&band_done[i0 / WAVE_GROUP_ROWS], (unsigned long long)rows * cols);
-    }
-  }
 }
 
 int preload_eb2d() {
@@ -219,10 +231,23 @@ int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int 
   if (row_end <= row_begin) return CPSZ_OK;
   if (band_done && row_begin % WAVE_GROUP_ROWS)
     return set_error(CPSZ_ERR_INVALID, "eb2d band start %d is not a multiple of %d", row_begin, WAVE_GROUP_ROWS);
+  int err = CPSZ_OK;
   auto go = [&](auto kernel, int tx, int ty, int nt) {
-    dim3 grid((r2 + tx - 1) / tx, (row_end - row_begin + ty - 1) / ty);
-    kernel<<<grid, nt, 0, ctx->stream>>>(U, V, r1, r2, max_pwr_eb, d_thr_tab, thr_n, ids_u, ids_v, hist, ctx->d_flag,
-                                         pair_u, pair_v, eb_out, row_begin, row_end, band_done);
+    const int tiles_x = (r2 + tx - 1) / tx;
+    const long long ntiles = (long long)tiles_x * ((row_end - row_begin + ty - 1) / ty);
+    if (ntiles > INT32_MAX) {
+      err = set_error(CPSZ_ERR_UNSUPPORTED, "eb2d: %lld tiles", ntiles);
+      return;
+    }
+    // persistent grid: the CTAs that fit, one per SM fewer beside the wavefront
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, nt, 0);
+    if (band_done && per_sm > 1) per_sm -= 1;
+    if (per_sm < 1) per_sm = 1;
+    const long long grid = std::min<long long>(ntiles, (long long)per_sm * ctx->num_sms);
+    kernel<<<(unsigned)grid, nt, 0, ctx->stream>>>(U, V, r1, r2, max_pwr_eb, d_thr_tab, thr_n, ids_u, ids_v, hist,
+                                                   ctx->d_flag, pair_u, pair_v, eb_out, row_begin, row_end,
+                                                   band_done, tiles_x, (int)ntiles);
   };
   // filtered bounds unless the caller wants the bounds themselves (or an
   // unusual max_pwr_eb takes the reference's NaN paths)
@@ -241,6 +266,7 @@ int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int 
     case 11: go(eb2d_kernel<32, 16, 128, false>, 32, 16, 128); break;
     default: go(eb2d_kernel<32, 16, 256, false>, 32, 16, 256); break;
   }
+  if (err != CPSZ_OK) return err;
   count_launch(ctx);
   return check_launch("eb2d_kernel");
 }

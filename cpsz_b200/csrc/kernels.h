@@ -68,8 +68,12 @@ struct WaveField {
   long long* trace;
   // optional: per-group counters of input points written by a concurrently
   // running producer (launch_eb2d's band_done); an item starts once its
-  // group's counter reaches rows x r2 (bounded wait, then FLAG_TIMEOUT)
+  // group's counter reaches rows x r2 + band_extra (bounded wait of
+  // band_wait_ns, then FLAG_TIMEOUT).  band_extra is 0 except in the test
+  // that makes the wait run out on purpose.
   const unsigned long long* band_done;
+  long long band_wait_ns;
+  unsigned long long band_extra;
 };
 struct WaveItem {
   int field;

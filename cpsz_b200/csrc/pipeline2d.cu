@@ -104,6 +104,10 @@ int read_flag(cpsz_b200_ctx* ctx, int* out) {
   return CPSZ_OK;
 }
 
+// Pinned word receiving the device flag right after the wavefront of a pass
+// whose wavefront ran beside the bound kernel.
+int* wave_flag_snapshot(cpsz_b200_ctx* ctx) { return (int*)((char*)ctx->pinned + 2048); }
+
 int flag_error(int flag) {
   if (flag & FLAG_TIMEOUT) return set_error(CPSZ_ERR_TIMEOUT, "a bounded device-side wait gave up");
   if (flag & FLAG_ID_OVERFLOW)
@@ -401,6 +405,8 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       F.r1 = j.r1;
       F.r2 = j.r2;
       F.band_done = overlap ? j.d.band : nullptr;
+      F.band_wait_ns = ctx->band_wait_ns;
+      F.band_extra = ctx->band_unreachable ? 1 : 0;
       r1v[2 * k + f] = j.r1;
     }
   }
@@ -423,13 +429,17 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     }
   } hi_drain;
   if (overlap) {
+    // The consumer (the wavefront on the high-priority stream) depends on the
+    // setup above only, and is enqueued after its producer (eb2d, stage 1):
+    // kernels that run one after the other -- under a tool that serialises
+    // launches, or on a device too busy to co-schedule them -- then run the
+    // bounds first and the wavefront finds every group complete.  When they do
+    // run together, the wavefront's CTAs take SMs as eb2d's CTAs retire.
     CPSZ_TRY(preload_eb2d());
     CPSZ_TRY(preload_wave2d());
     hi_drain.s = ctx->hi;
     CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[3], st));
     CPSZ_CUDA_TRY(cudaStreamWaitEvent(ctx->hi, ctx->ev[3], 0));
-    CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points, ctx->hi, WAVE_BESIDE));
-    CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[4], ctx->hi));
   }
 
   // Stages 1-3 (bounds, wavefront, code histograms, block order) are the
@@ -500,6 +510,11 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       }
       CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_hist_ids, j.d.hist_ids, 256 * 8, cudaMemcpyDeviceToHost, st));
     }
+    if (overlap) {
+      // every producer launch is enqueued: now the consumer beside them
+      CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points, ctx->hi, WAVE_BESIDE));
+      CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[4], ctx->hi));
+    }
     CPSZ_CUDA_TRY(record(ctx->ev[0]));
     if (tap && tap->ids)
       CPSZ_CUDA_TRY(cudaMemcpyAsync(tap->ids, jobs[0].d.ids, 2 * jobs[0].N, cudaMemcpyDeviceToDevice, st));
@@ -510,6 +525,9 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       // the bounds are done: the rest of each SM joins the running wavefront
       CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points, st, WAVE_JOIN));
       CPSZ_CUDA_TRY(cudaStreamWaitEvent(st, ctx->ev[4], 0));
+      // the flag as the wavefront left it, read by the host once the code
+      // histograms (enqueued after it) have arrived
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(wave_flag_snapshot(ctx), ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
     } else {
       CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points));
     }
@@ -652,12 +670,36 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     CPSZ_TRY(d2h_beside(hj->host_out + at, hj->d.bits[0], hj->bits_bytes[0]));
   }
   // code trees, each as soon as its histogram is on the host
-  parallel_for(2 * nj, [&](int q) {
-    Job2D& j = jobs[q / 2];
-    const int f = q % 2;
-    j.tree_ok[1 + f] = cudaEventSynchronize(ctx->job_ev[q]) == cudaSuccess &&
-                       huff_build(j.h_hist_codes + (size_t)f * 65536, 65536, 131072, &j.cb[1 + f]);
-  });
+  auto code_trees = [&]() {
+    parallel_for(2 * nj, [&](int q) {
+      Job2D& j = jobs[q / 2];
+      const int f = q % 2;
+      j.tree_ok[1 + f] = cudaEventSynchronize(ctx->job_ev[q]) == cudaSuccess &&
+                         huff_build(j.h_hist_codes + (size_t)f * 65536, 65536, 131072, &j.cb[1 + f]);
+    });
+  };
+  code_trees();
+  if (overlap) {
+    // The histograms are on the host, so is the flag snapshot taken before
+    // them.  A wavefront wait that gave up (the bound kernel was held back
+    // for seconds: a saturated or time-sliced device) left codes from
+    // incomplete inputs; the bounds are complete now, so the wavefront and
+    // everything after it runs again, after the bounds, and the pass goes on.
+    // The id stream's packing, already enqueued, depends on the bounds only.
+    const int snap = *(volatile int*)wave_flag_snapshot(ctx);
+    if (snap & FLAG_TIMEOUT) {
+      if (snap != FLAG_TIMEOUT) return flag_error(snap);
+      CPSZ_CUDA_TRY(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), st));
+      for (WaveField& F : hf) F.band_done = nullptr;
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(d_fields, hf.data(), hf.size() * sizeof(WaveField), cudaMemcpyHostToDevice, st));
+      for (Job2D& j : jobs) CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.gbnd, 0, 2 * (size_t)j.ngroups * j.r2 * 8, st));
+      CPSZ_CUDA_TRY(cudaMemsetAsync(queue, 0, 64, st));
+      CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points));
+      CPSZ_TRY(stage_3());
+      code_trees();
+      ctx->wave_reruns++;
+    }
+  }
 
   // ---- stage 4: bit packing of the codes ----
   mark(ctx, "huffman_encode");

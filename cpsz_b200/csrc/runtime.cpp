@@ -319,6 +319,20 @@ int cpsz_b200_ctx_graph_stats(cpsz_b200_ctx* ctx, uint64_t* captures, uint64_t* 
   return CPSZ_OK;
 }
 
+int cpsz_b200_ctx_wave_reruns(cpsz_b200_ctx* ctx, uint64_t* reruns) {
+  if (!ctx || !reruns) return set_error(CPSZ_ERR_INVALID, "null argument");
+  *reruns = ctx->wave_reruns;
+  return CPSZ_OK;
+}
+
+int cpsz_b200_debug_band_wait(cpsz_b200_ctx* ctx, long long wait_ns, int unreachable) {
+  if (!ctx) return set_error(CPSZ_ERR_INVALID, "null argument");
+  if (wait_ns < 0) return set_error(CPSZ_ERR_INVALID, "negative wait limit");
+  ctx->band_wait_ns = wait_ns;
+  ctx->band_unreachable = unreachable != 0;
+  return CPSZ_OK;
+}
+
 int cpsz_b200_ctx_set_timing(cpsz_b200_ctx* ctx, int on) {
   int rc;
   ctx = resolve_ctx(ctx, &rc);

@@ -109,6 +109,14 @@ struct cpsz_b200_ctx {
   // optional wavefront trace (diagnostics): 4 counters per (field, group, warp)
   long long* d_wave_trace = nullptr;
   size_t wave_trace_len = 0;
+  // The wavefront that runs beside the bound kernel waits per row group for
+  // the bounds (limit band_wait_ns, 0 = the kernel's default).  When a wait
+  // gives up, the pass runs its wavefront again after the bounds
+  // (wave_reruns counts these).  band_unreachable (diagnostics only) makes
+  // every such wait run out, to exercise that path.
+  long long band_wait_ns = 0;
+  bool band_unreachable = false;
+  uint64_t wave_reruns = 0;
   // device copy of the host log2f / exp2f tables (libm.h), uploaded on first use
   void* libm_mem = nullptr;
   void* libm_view = nullptr;  // cpsz::LibmTables*

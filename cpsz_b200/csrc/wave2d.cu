@@ -381,13 +381,15 @@ __device__ __forceinline__ void wave2d_body(const WaveField* __restrict__ fields
       // this group is written; one thread polls, then every thread acquires
       const unsigned long long* cnt = F.band_done + item.group;
       const unsigned long long target =
-          (unsigned long long)min(WAVE_GROUP_ROWS, F.r1 - item.group * WAVE_GROUP_ROWS) * (unsigned long long)F.r2;
+          (unsigned long long)min(WAVE_GROUP_ROWS, F.r1 - item.group * WAVE_GROUP_ROWS) * (unsigned long long)F.r2 +
+          F.band_extra;
+      const long long limit = F.band_wait_ns > 0 ? F.band_wait_ns : BAND_WAIT_NS;
       if (threadIdx.x == 0 && ld_acquire(cnt) < target) {
         const long long t0 = globaltimer_ns();
         while (ld_acquire(cnt) < target) {
           // a wait that already gave up (this launch or the producer failed)
           // ends every later wait at once
-          if ((*(volatile int*)flag & FLAG_TIMEOUT) || globaltimer_ns() - t0 > BAND_WAIT_NS) {
+          if ((*(volatile int*)flag & FLAG_TIMEOUT) || globaltimer_ns() - t0 > limit) {
             atomicOr(flag, FLAG_TIMEOUT);
             break;
           }

@@ -50,6 +50,12 @@ int cpsz_b200_ctx_kernel_launches(cpsz_b200_ctx* ctx, uint64_t* count);
 /* Batch passes run from CUDA graphs on this context: graphs captured, and
  * passes replayed from a graph captured earlier. */
 int cpsz_b200_ctx_graph_stats(cpsz_b200_ctx* ctx, uint64_t* captures, uint64_t* replays);
+/* Single-field compressions run the Lorenzo wavefront beside the bound kernel,
+ * each row group waiting (bounded) for its bounds.  If such a wait gives up
+ * (the bound kernel was held back, e.g. on a saturated or time-sliced device),
+ * the pass runs its wavefront again after the bounds and still returns the
+ * same blob; this counts those re-runs on the context. */
+int cpsz_b200_ctx_wave_reruns(cpsz_b200_ctx* ctx, uint64_t* reruns);
 /* Stream of the context as an opaque handle (a cudaStream_t). */
 int cpsz_b200_ctx_stream(cpsz_b200_ctx* ctx, void** stream);
 /* Per-stage timing: when on, each call records CUDA events on the context's
@@ -64,8 +70,10 @@ int cpsz_b200_ctx_stage_times(cpsz_b200_ctx* ctx, int max_stages, const char** n
  * threads, 32x8/128, 64x8/256, 32x32/256, 64x16/256, 32x16/128),
  * "wave2d.ctas_per_sm" (0 = occupancy limit), "eb3d.fill", "eb3d.min_chunk",
  * "h2d.chunks", "wave2d.overlap" (1: the Lorenzo wavefront runs beside the
- * bound kernel; 0: after it -- needed under tools that serialize kernels,
- * also forced by the environment variable CPSZ_B200_OVERLAP=0).  An entry applies to fields of >= min_points points; the
+ * bound kernel, enqueued after it, so tools that serialise kernels run it
+ * after the bounds; 0: after the bounds on every SM -- also forced by the
+ * environment variable CPSZ_B200_OVERLAP=0).  An entry applies to fields of
+ * >= min_points points; the
  * largest such threshold wins.  The first cpsz_b200_ctx_create() loads
  * $CPSZ_B200_TUNING (empty or "none": no table) or else tuning_b200.json of the
  * package directory when present; a malformed table fails ctx creation.  Any
@@ -120,7 +128,10 @@ int cpsz_b200_compress_2d_batch_f32(cpsz_b200_ctx* ctx, int n_fields, const floa
  * A small MLP (99 -> 128 -> 128 -> 1, ReLU; BF16 tensor-core kernels with FP32
  * accumulation) proposes per vertex a log2 multiplier t in [0, 16] of the
  * analytic bound from a vertex's 7x7 (u,v) neighbourhood (normalised by its
- * largest |value|) and log2 of its analytic bound.  The fallback loop
+ * largest |value|) and log2 of its analytic bound.  A proposed bound is
+ * eb_analytic * 2^t capped at max_pwr_eb, so every point keeps the plain
+ * compressor's point-wise relative bound; only bounds the critical points
+ * tighten below max_pwr_eb are loosened.  The fallback loop
  * compresses with the proposals, reconstructs, compares every cell's critical
  * point exactly with the original, reverts the vertices of offending cells to
  * their analytic bounds and repeats until no cell differs.  The result is an
@@ -226,16 +237,21 @@ int cpsz_b200_huffman_encode_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t
  * every GPU loading it keeps until process exit, which limits n to 67,108,864
  * symbols per call (larger n is rejected with CPSZ_ERR_INVALID).
  * All pointers are device memory: sym (n symbols), code/len (codebook from
- * cpsz_b200_huffman_codebook), out (out_cap bytes, 4-byte aligned, zeroed by
- * the call), total_bits (one uint64, receives the bit count).  The work is
+ * cpsz_b200_huffman_codebook: every length must be at most 64 bits, which that
+ * function guarantees -- the packer's shared-memory buffer is sized for it),
+ * out (out_cap bytes, 4-byte aligned, out_cap a multiple of 4, zeroed by the
+ * call), total_bits (one uint64, receives the bit count).  The work is
  * enqueued on `stream` (a cudaStream_t; NULL = legacy default stream) and the
  * call returns without waiting; a stream longer than out_cap is cut off at the
  * capacity, which the caller detects as (*total_bits + 7) / 8 > out_cap.
- * The first call on a device looks up the scratch array's device address
- * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture.  All calls on a device share the one array, so
- * calls whose GPU work overlaps (concurrent streams, threads) race and must be
- * serialised by the caller. */
+ * Every call looks up the scratch array's device address
+ * (cudaGetSymbolAddress) in the calling thread's current device and context,
+ * so the address stays valid after a device reset and in a context the caller
+ * made current; the first call on a device also loads the library's kernels
+ * there, so make it before any stream capture.  All calls on a device share
+ * the one array, which keeps the last call's contents (the call clears what
+ * must start at zero), so calls whose GPU work overlaps (concurrent streams,
+ * threads) race and must be serialised by the caller. */
 int cpsz_b200_huffman_encode_u16_noalloc(const uint16_t* sym, size_t n, const uint64_t* code, const uint8_t* len,
                                          unsigned char* out, size_t out_cap, uint64_t* total_bits, void* stream);
 
@@ -255,6 +271,11 @@ int cpsz_b200_debug_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, siz
  * 255 = bound not positive).  Host buffers. */
 int cpsz_b200_debug_eb3d(cpsz_b200_ctx* ctx, const float* U, const float* V, const float* W, size_t r1, size_t r2,
                          size_t r3, double max_pwr_eb, double* eb_out, uint8_t* id_codes);
+/* The wavefront's per-group wait for the bound kernel: limit wait_ns (0 = the
+ * default of 4 s); unreachable != 0 makes every such wait run out (its target
+ * is one point more than the group holds), which exercises the re-run path
+ * (cpsz_b200_ctx_wave_reruns) without stalling any kernel beyond the limit. */
+int cpsz_b200_debug_band_wait(cpsz_b200_ctx* ctx, long long wait_ns, int unreachable);
 /* Tensor-core self-check: D (128x128 fp32) = A (128x128 bf16 bits) * B^T
  * (128x128 bf16 bits), row-major host arrays, through tcgen05 / TMEM. */
 int cpsz_b200_debug_umma_gemm(cpsz_b200_ctx* ctx, const uint16_t* A, const uint16_t* B, float* D);

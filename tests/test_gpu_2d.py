@@ -132,3 +132,57 @@ def test_gpu_eb2d_nonfinite_signed_zero_and_overflow(ctx, oracle):
     V[:, 7] /= 1e7
     blob = cpsz_b200.sz_compress_cp_preserve_2d_offline(U, V, max_pwr_eb=0.1, ctx=ctx)
     assert_blob_equal_2d(blob, oracle.compress_2d(U, V, 0.1))
+
+
+def test_gpu_wavefront_wait_that_gives_up_reruns(oracle):
+    """The wavefront beside the bound kernel waits (bounded) per row group for
+    its bounds.  With every such wait made to run out (target one point more
+    than a group holds, 1 ms limit), the pass runs its wavefront again after
+    the bounds and still returns the oracle's blob."""
+    torch = pytest.importorskip("torch")
+    c = cpsz_b200.Context(0)  # own context: the setting stays off the shared one
+    try:
+        c.debug_band_wait(1_000_000, unreachable=True)
+        for r1, r2, seed, dev in ((600, 700, 5, False), (1500, 1300, 6, False), (700, 900, 7, True)):
+            U, V = W.cfg0_like(seed, r1, r2)
+            n0 = c.wave_reruns
+            if dev:
+                a = cpsz_b200.sz_compress_cp_preserve_2d_offline(torch.from_numpy(U).cuda(),
+                                                                 torch.from_numpy(V).cuda(), max_pwr_eb=0.1, ctx=c)
+            else:
+                a = cpsz_b200.sz_compress_cp_preserve_2d_offline(U, V, max_pwr_eb=0.1, ctx=c)
+            assert c.wave_reruns == n0 + 1
+            assert_blob_equal_2d(a, oracle.compress_2d(U, V, 0.1))
+        c.debug_band_wait(0, unreachable=False)
+        U, V = W.cfg0_like(8, 640, 480)
+        n0 = c.wave_reruns
+        a = cpsz_b200.sz_compress_cp_preserve_2d_offline(U, V, max_pwr_eb=0.1, ctx=c)
+        assert c.wave_reruns == n0
+        assert_blob_equal_2d(a, oracle.compress_2d(U, V, 0.1))
+    finally:
+        c.close()
+
+
+def test_gpu_serialised_launches_need_no_rerun(tmp_path):
+    """With every launch serialised (CUDA_LAUNCH_BLOCKING=1, as under tools that
+    run kernels one at a time) the bound kernel, enqueued first, completes
+    before the wavefront starts: the blob equals the oracle's and no wait gives
+    up.  Runs in a child process so the setting applies from CUDA's start."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = (
+        "import sys; sys.path.insert(0, sys.argv[1]);"
+        "import cpsz_b200; from cpsz_b200 import workloads as W; from oracle import Oracle;"
+        "from tests._util import assert_blob_equal_2d;"
+        "c = cpsz_b200.Context(0); U, V = W.cfg0_like(9, 1100, 900);"
+        "a = cpsz_b200.sz_compress_cp_preserve_2d_offline(U, V, max_pwr_eb=0.1, ctx=c);"
+        "assert_blob_equal_2d(a, Oracle().compress_2d(U, V, 0.1));"
+        "print('reruns', c.wave_reruns)"
+    )
+    env = dict(os.environ, CUDA_LAUNCH_BLOCKING="1")
+    r = subprocess.run([sys.executable, "-c", code, root], env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "reruns 0" in r.stdout
