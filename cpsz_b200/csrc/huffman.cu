@@ -22,8 +22,6 @@
 // rounds), then counts are scanned and every thread decodes again, writing its
 // symbols.  Lookup is a 2^12-entry first-level table with a bit-serial tree
 // walk for longer codes.
-#include <mutex>
-
 #include "kernels.h"
 
 namespace cpsz {
@@ -596,24 +594,18 @@ static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocCo
 
 namespace {
 
-std::mutex g_noalloc_mu;
-unsigned long long* g_noalloc_addr[64] = {};  // device address of the array, per device
-
-// Resolves the array's device address on the current device (once per device).
+// The array's device address in the calling thread's current context.  It is
+// looked up on every call (a lookup, no allocation): an address cached once
+// per device would go stale after a device reset, or in a context the caller
+// created and made current itself, and kernels given it would write to memory
+// that is no longer the array.
 int noalloc_scratch(unsigned long long** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return set_error(CPSZ_ERR_NO_DEVICE, "no CUDA device: %s", cudaGetErrorString(e));
-  if (dev < 0 || dev >= 64) return set_error(CPSZ_ERR_INVALID, "device %d out of range", dev);
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess)
-      return set_error(CPSZ_ERR_CUDA, "cudaGetSymbolAddress of the no-alloc scratch: %s", cudaGetErrorString(e));
-    g_noalloc_addr[dev] = (unsigned long long*)p;
-  }
-  *out = g_noalloc_addr[dev];
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess)
+    return set_error(e == cudaErrorNoDevice ? CPSZ_ERR_NO_DEVICE : CPSZ_ERR_CUDA,
+                     "cudaGetSymbolAddress of the no-alloc scratch: %s", cudaGetErrorString(e));
+  *out = (unsigned long long*)p;
   return CPSZ_OK;
 }
 
@@ -628,6 +620,9 @@ extern "C" int cpsz_b200_huffman_encode_u16_noalloc(const uint16_t* sym, size_t 
   clear_error();
   if (!sym || !code || !len || !out || !total_bits) return set_error(CPSZ_ERR_INVALID, "null pointer argument");
   if (((uintptr_t)out & 3) != 0) return set_error(CPSZ_ERR_INVALID, "output must be 4-byte aligned");
+  // the packer stores whole 32-bit words: a capacity that is not a multiple of
+  // 4 would leave its last bytes unwritten without the overflow rule noticing
+  if (out_cap % 4 != 0) return set_error(CPSZ_ERR_INVALID, "out_cap (%zu) must be a multiple of 4", out_cap);
   if (n > kNoAllocMaxSymbols)
     return set_error(CPSZ_ERR_INVALID, "%zu symbols exceed the no-alloc maximum of %zu symbols per call", n,
                      kNoAllocMaxSymbols);

@@ -31,7 +31,7 @@ def test_no_alloc_matches_context_encoder_twice():
             d_sym = torch.from_numpy(sym.view(np.int16)).cuda()
             d_code = torch.from_numpy(code.view(np.int64)).cuda()
             d_len = torch.from_numpy(ln).cuda()
-            cap = (int((hist * ln.astype(np.uint64)).sum()) + 7) // 8 + 64
+            cap = ((int((hist * ln.astype(np.uint64)).sum()) + 7) // 8 + 64) // 4 * 4
             ref = torch.zeros(cap, dtype=torch.uint8, device="cuda")
             ref_bits = cpsz_b200.huffman_encode_u16(d_sym, d_code, d_len, ref, ctx=ctx)
             for _ in range(2):  # two calls in a row share the scratch array
@@ -57,3 +57,34 @@ def test_no_alloc_rejects_oversized_stream():
                                                 buf.data_ptr(), 64, bits.data_ptr(), None)
     assert rc == 1
     assert b"exceed the no-alloc maximum" in L.cpsz_b200_last_error()
+
+
+def test_no_alloc_capacity_rules():
+    """out_cap must be a multiple of 4 (the packer stores whole words); a buffer
+    short of the stream gets the stream's prefix and the full bit count, so the
+    caller sees the overflow as (total_bits + 7) / 8 > out_cap."""
+    torch = pytest.importorskip("torch")
+    ctx = cpsz_b200.Context(0)
+    try:
+        sym, hist = _case(13, 300_001)
+        code, ln, _ = cpsz_b200.huffman_codebook(hist, 131072)
+        d_sym = torch.from_numpy(sym.view(np.int16)).cuda()
+        d_code = torch.from_numpy(code.view(np.int64)).cuda()
+        d_len = torch.from_numpy(ln).cuda()
+        need = (int((hist * ln.astype(np.uint64)).sum()) + 7) // 8
+        full = torch.zeros((need + 64) // 4 * 4, dtype=torch.uint8, device="cuda")
+        ref_bits = cpsz_b200.huffman_encode_u16(d_sym, d_code, d_len, full, ctx=ctx)
+        bits = torch.zeros(1, dtype=torch.int64, device="cuda")
+        odd = torch.zeros(need + 3 - (need + 3) % 4 + 2, dtype=torch.uint8, device="cuda")
+        with pytest.raises(cpsz_b200.CpszError) as ei:
+            cpsz_b200.huffman_encode_u16_noalloc(d_sym, d_code, d_len, odd, bits)
+        assert ei.value.code == 1 and "multiple of 4" in str(ei.value)
+        short_cap = (need - 1) // 4 * 4  # one to four bytes short of the stream
+        short = torch.full((short_cap,), 0xAB, dtype=torch.uint8, device="cuda")
+        cpsz_b200.huffman_encode_u16_noalloc(d_sym, d_code, d_len, short, bits)
+        torch.cuda.synchronize()
+        assert int(bits.item()) == ref_bits
+        assert (int(bits.item()) + 7) // 8 > short_cap
+        assert torch.equal(short, full[:short_cap])
+    finally:
+        ctx.close()
