@@ -33,14 +33,22 @@ namespace {
 
 constexpr float TMAX = 16.f;  // largest log2 multiplier proposed
 
+// Proposed bound eb_a * 2^m, m clamped to [0, TMAX], and never above the
+// caller's point-wise relative bound max_pwr_eb: a vertex's relative error
+// stays within what the plain compressor promises (its analytic bound is
+// min(max_pwr_eb, bounds of its triangles), src/sz_compress_cp_preserve_2d.cpp:195-218),
+// so the learned form only loosens bounds the critical points constrain.
 __global__ void scale_bounds_kernel(const double* __restrict__ eb_a, const float* __restrict__ mult, size_t n,
-                                    double* __restrict__ eb, unsigned long long* __restrict__ enlarged) {
+                                    double max_pwr_eb, double* __restrict__ eb,
+                                    unsigned long long* __restrict__ enlarged) {
   unsigned long long c = 0;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     float m = mult[i];
     m = (m == m) ? fminf(fmaxf(m, 0.f), TMAX) : 0.f;
-    eb[i] = eb_a[i] * exp2((double)m);
-    c += eb[i] != eb_a[i];
+    const double a = eb_a[i];
+    const double e = a * exp2((double)m);
+    eb[i] = e > max_pwr_eb ? (a > max_pwr_eb ? a : max_pwr_eb) : e;
+    c += eb[i] != a;
   }
   for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(enlarged, c);
@@ -236,7 +244,7 @@ int compress_2d_learned(cpsz_b200_ctx* ctx, cpsz_b200_mlp* mlp, const float* U_i
   } else {
     CPSZ_TRY(launch_mlp_forward(ctx, mlp->w, nullptr, dU, dV, eb_a, r1, r2, (int)N, mult, nullptr, nullptr));
   }
-  scale_bounds_kernel<<<grid_of(ctx, N), 256, 0, st>>>(eb_a, mult, N, eb, counts + 4);
+  scale_bounds_kernel<<<grid_of(ctx, N), 256, 0, st>>>(eb_a, mult, N, max_pwr_eb, eb, counts + 4);
   count_launch(ctx);
   CPSZ_TRY(check_launch("scale_bounds_kernel"));
   CPSZ_TRY(launch_cp_check_2d(ctx, dU, dV, nullptr, nullptr, r1, r2, cells_a, counts + 8));

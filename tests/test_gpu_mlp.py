@@ -162,3 +162,51 @@ def test_learned_compress_with_mlp(ctx):
     dU, dV = cpsz_b200.sz_decompress_cp_preserve_2d_offline(blob, *U.shape, ctx=ctx)
     r = cpsz_b200.cp_check_2d(U, V, dU, dV, ctx=ctx)
     assert r["lost_or_spurious"] == 0 and r["type_changed"] == 0, (r, st)
+
+
+def _within_relative_bound(x, d, eb):
+    x64 = x.astype(np.float64)
+    return int(np.count_nonzero(np.abs(d.astype(np.float64) - x64) > eb * np.abs(x64)))
+
+
+def test_trained_proposer_gains_over_plain(ctx, oracle):
+    """The committed proposer (trained on seeds 1000-1063, margin chosen on seed
+    99991) on a held-out 2048^2 field of the same generator: a smaller ZSTD'd
+    blob than the plain compressor's, no critical point lost, added or
+    retyped, every point within max_pwr_eb of its value, and the blob decodes
+    identically through the plain decoder of the oracle."""
+    from cpsz_b200 import learned
+
+    U, V = W.cfg0_like(123457, 2048, 2048)
+    eb = 0.1
+    mlp = learned.load(ctx)
+    try:
+        plain = cpsz_b200.sz_compress_cp_preserve_2d_offline(U, V, max_pwr_eb=eb, ctx=ctx)
+        blob, st = cpsz_b200.compress_2d_learned(U, V, eb, mlp=mlp, ctx=ctx)
+    finally:
+        mlp.close()
+    dU, dV = cpsz_b200.sz_decompress_cp_preserve_2d_offline(blob, *U.shape, ctx=ctx)
+    r = cpsz_b200.cp_check_2d(U, V, dU, dV, ctx=ctx)
+    assert r["cps_a"] > 0
+    assert r["lost_or_spurious"] == 0 and r["type_changed"] == 0, (r, st)
+    assert _within_relative_bound(U, dU, eb) == 0 and _within_relative_bound(V, dV, eb) == 0
+    z_plain = len(cpsz_b200.sz_lossless_compress(plain, 3))
+    z_learned = len(cpsz_b200.sz_lossless_compress(blob, 3))
+    raw = U.nbytes + V.nbytes
+    print(f"held-out 2048^2: ratio plain {raw / z_plain:.3f}, learned {raw / z_learned:.3f}; {st}")
+    assert z_learned < z_plain
+    ou, ov = oracle.decompress_2d(blob, *U.shape)
+    assert np.array_equal(ou.view(np.uint32), dU.view(np.uint32))
+    assert np.array_equal(ov.view(np.uint32), dV.view(np.uint32))
+
+
+def test_learned_bounds_never_exceed_max_pwr_eb(ctx):
+    """Multipliers far beyond any useful size are capped at max_pwr_eb: the
+    decode keeps the plain compressor's point-wise relative bound."""
+    U, V = W.cfg0_like(33, 400, 500)
+    for eb in (0.1, 0.01):
+        blob, st = cpsz_b200.compress_2d_learned(U, V, eb, log2_mult=np.full(U.shape, 16.0, np.float32), ctx=ctx)
+        dU, dV = cpsz_b200.sz_decompress_cp_preserve_2d_offline(blob, *U.shape, ctx=ctx)
+        assert _within_relative_bound(U, dU, eb) == 0 and _within_relative_bound(V, dV, eb) == 0
+        r = cpsz_b200.cp_check_2d(U, V, dU, dV, ctx=ctx)
+        assert r["lost_or_spurious"] == 0 and r["type_changed"] == 0, (r, st)
