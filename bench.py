@@ -137,40 +137,69 @@ def make_fields(workload: str, seed_offset: int = 0):
 
 
 # ---- reference arm ----------------------------------------------------------------------
+#
+# The reference's own CPU implementation (oracle/_ref: its sources compiled
+# here; the C restatement when that is absent) on the same workload, one
+# single-threaded process per host core.  The arm never loads the product
+# library: inputs come from the oracle's C generator, which builds the
+# product's seeded fields bit for bit (tests/test_oracle_gen.py).
 
-def _ref_worker(args):
-    """One bounded sample of the workload through the reference CPU implementation."""
-    kind, arr_paths, eb, use_ref = args
+def oracle_fields(workload: str, seed_offset: int = 0):
+    """The workload's fields from the oracle's generator (no product code)."""
+    from oracle import Oracle
+
+    O = Oracle()
+    kind, shape, eb, gen = WORKLOADS[workload]
+    if gen == "cfg1":
+        return O.field_2d(1 + seed_offset, 8192, 8192, 2000, 60.0), eb
+    if gen == "cfg0":
+        return O.field_2d(0 + seed_offset, 2400, 3600, 200, 40.0), eb
+    if gen == "cfg0like":
+        r1, r2 = shape
+        return O.field_2d(5 + seed_offset, r1, r2, max(1, round(200 / (2400 * 3600) * r1 * r2)), 40.0), eb
+    if gen == "cfg2":
+        return O.field_3d(2 + seed_offset, *shape, 500, 20.0), eb
+    raise KeyError(workload)
+
+
+def _ref_child(conn, kind, field_src, use_ref):
+    """One reference process: loads (or generates) its fields once, then on
+    every request compresses all of them and replies with the seconds taken."""
     sys.path.insert(0, ROOT)
     import oracle
 
-    arrs = [np.load(p, mmap_mode="r") for p in arr_paths]
     impl = oracle.Reference() if use_ref else oracle.Oracle()
-    arrs = [np.ascontiguousarray(a) for a in arrs]
-    t = time.perf_counter()
-    if kind == "2d":
-        blob = impl.compress_2d(arrs[0], arrs[1], eb)
-    else:
-        blob = impl.compress_3d(arrs[0], arrs[1], arrs[2], eb)
-    return time.perf_counter() - t, len(blob)
+    fields = []
+    if field_src[0] == "files":
+        for paths, eb in field_src[1]:
+            fields.append(([np.ascontiguousarray(np.load(p)) for p in paths], eb))
+    else:  # ("batch", [(r1, r2, seed, eb), ...]): this process's fields of the batch
+        O = oracle.Oracle()
+        for r1, r2, seed, eb in field_src[1]:
+            fields.append((list(O.field_2d(seed, r1, r2, max(1, (r1 * r2) // 1600), 40.0)), eb))
+    conn.send(sum(a.nbytes for arrs, _ in fields for a in arrs))
+    while conn.recv():
+        t0 = time.perf_counter()
+        for arrs, eb in fields:
+            if kind == "3d":
+                impl.compress_3d(arrs[0], arrs[1], arrs[2], eb)
+            else:
+                impl.compress_2d(arrs[0], arrs[1], eb)
+        conn.send(time.perf_counter() - t0)
+    conn.close()
 
 
-def reference_samples(workload: str, fields, eb):
-    """Tiles of the workload sized for ~1 s of reference CPU work each."""
-    kind = WORKLOADS[workload][0]
-    tiles = []
-    if kind in ("2d", "learned"):
-        U, V = fields
-        s = 1024
-        for i in range(0, U.shape[0] - s + 1, s):
-            for j in range(0, U.shape[1] - s + 1, s):
-                tiles.append((U[i:i + s, j:j + s], V[i:i + s, j:j + s]))
-    else:
-        U, V, Wf = fields
-        s = 96
-        for i in range(0, U.shape[0] - s + 1, s):
-            tiles.append(tuple(a[i:i + s, :s, :s] for a in (U, V, Wf)))
-    return tiles
+def _host_procs(per_proc_bytes: float) -> int:
+    """Processes to run: one per host core, as many as memory holds."""
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    try:
+        import psutil
+
+        avail = psutil.virtual_memory().available
+        cores = min(cores, max(1, int(avail * 0.7 // per_proc_bytes)))
+    except Exception:
+        pass
+    return max(1, cores)
 
 
 def run_reference(args, rank, world):
@@ -181,52 +210,81 @@ def run_reference(args, rank, world):
 
     if rank != 0:
         return None
-    kind = WORKLOADS[args.workload][0]
+    wk = WORKLOADS[args.workload][0]
     use_ref = os.path.exists(oracle.REF_SO)
-    if kind == "batch":
-        # whole fields of the batch (the smaller ones), each with its own bound
-        lay = batch_layout()
-        order = sorted(range(len(lay)), key=lambda k: lay[k][0] * lay[k][1])
-        tiles, tile_ebs = make_batch([k for k in order if lay[k][0] * lay[k][1] <= 1_500_000])
+    tmp = None
+    if wk == "batch":
+        # the whole batch each step: its fields split over the processes by
+        # greedy size balance, each process generating the fields it owns
+        lay = oracle.Oracle().batch_layout(3, 256, 128, 4096)
+        nproc = _host_procs(2.5e9)
+        bins = [[] for _ in range(nproc)]
+        load = [0] * nproc
+        for k in sorted(range(len(lay)), key=lambda k: -lay[k][0] * lay[k][1]):
+            q = load.index(min(load))
+            bins[q].append(lay[k])
+            load[q] += lay[k][0] * lay[k][1]
+        srcs = [("batch", b) for b in bins if b]
         kind = "2d"
+        sample = f"the whole 256-field batch per step, split over {len(srcs)} single-threaded processes"
     else:
-        fields, eb = make_fields(args.workload)
-        tiles = reference_samples(args.workload, fields, eb)
-        tile_ebs = [eb] * len(tiles)
-        kind = "2d" if kind == "learned" else kind
-    cores = os.cpu_count() or 1
-    tmp = tempfile.mkdtemp(prefix="cpsz_ref_")
-    paths = []
-    for k, t in enumerate(tiles[:max(cores, 1) * 2]):
-        ps = []
-        for c, a in enumerate(t):
-            p = os.path.join(tmp, f"t{k}_{c}.npy")
-            np.save(p, np.ascontiguousarray(a))
-            ps.append(p)
-        paths.append(ps)
+        fields, eb = oracle_fields(args.workload)
+        kind = "3d" if wk == "3d" else "2d"
+        if kind == "3d":
+            # a 192^3 block of the field per process (the whole 384^3 field takes
+            # about 45 s per process, too long for a step)
+            fields = tuple(np.ascontiguousarray(a[:192, :192, :192]) for a in fields)
+        nbytes = sum(a.nbytes for a in fields)
+        nproc = _host_procs(4.0 * nbytes + 0.5e9)
+        tmp = tempfile.mkdtemp(prefix="cpsz_ref_")
+        paths = []
+        for c, a in enumerate(fields):
+            p = os.path.join(tmp, f"f{c}.npy")
+            np.save(p, a)
+            paths.append(p)
+        del fields
+        srcs = [("files", [(paths, eb)])] * nproc
+        what = "192^3 block" if kind == "3d" else f"whole {'x'.join(map(str, WORKLOADS[args.workload][1]))} field"
+        sample = f"the {what} per process, {nproc} single-threaded processes compressing concurrently per step"
     ctxm = mp.get_context("spawn")
-    times = []
-    total_bytes = 0
-    with ctxm.Pool(cores) as pool:
-        jobs = [(kind, p, tile_ebs[k], use_ref) for k, p in enumerate(paths[:cores])]
+    procs, conns = [], []
+    try:
+        for src in srcs:
+            a, b = ctxm.Pipe()
+            pr = ctxm.Process(target=_ref_child, args=(b, kind, src, use_ref), daemon=True)
+            pr.start()
+            procs.append(pr)
+            conns.append(a)
+        step_bytes = sum(c.recv() for c in conns)
+        times = []
         for step in range(args.warmup + args.steps):
             t0 = time.perf_counter()
-            res = pool.map(_ref_worker, jobs)
-            dt = time.perf_counter() - t0
+            for c in conns:
+                c.send(True)
+            for c in conns:
+                c.recv()
             if step >= args.warmup:
-                times.append(dt)
-                total_bytes = sum(np.load(p, mmap_mode="r").nbytes for job in jobs for p in job[1])
+                times.append(time.perf_counter() - t0)
+        for c in conns:
+            c.send(False)
+        for pr in procs:
+            pr.join(timeout=60)
+    finally:
+        for pr in procs:
+            if pr.is_alive():
+                pr.terminate()
+        if tmp:
+            import shutil
+
+            shutil.rmtree(tmp, ignore_errors=True)
     per_step = statistics.mean(times)
-    gbs = total_bytes / per_step / 1e9
-    what = ("whole fields of the batch (up to 1.5M points each)" if WORKLOADS[args.workload][0] == "batch"
-            else f"{'1024x1024' if kind == '2d' else '96^3'} tiles of the workload")
-    sample = f"{len(jobs)} independent {what}, one per process, compressed concurrently per step"
+    gbs = step_bytes / per_step / 1e9
     line = {
         "impl": "reference", "metric": "compress_GBps", "value": round(gbs, 4), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(per_step * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
         "data": "synthetic", "config": {"workload": args.workload},
-        "cpu_baseline": {"value": round(gbs, 4), "unit": "GB/s", "cores": len(jobs),
+        "cpu_baseline": {"value": round(gbs, 4), "unit": "GB/s", "cores": len(srcs),
                          "kind": "reference" if use_ref else "port", "sample": sample},
         "e2e": {"value": round(gbs, 4), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -235,32 +293,71 @@ def run_reference(args, rank, world):
 
 # ---- product arm -----------------------------------------------------------------------
 
-def cpu_baseline_single(workload, fields, eb, budget_s=12.0):
-    """The reference CPU implementation (1 core, as the reference is single-threaded)
-    on 1024x1024 (2D) / 96^3 (3D) tiles of the workload for about budget_s seconds."""
+def _meaninfo_padding_2d(blob: bytes) -> np.ndarray:
+    """False at the 3 padding bytes of each field's meanInfo<float> record,
+    which the reference writes uninitialised (src/sz_compress_3d.cpp:222)."""
+    import struct
+
+    m = np.ones(len(blob), bool)
+    eb_size, u_size, _ = struct.unpack_from("<QQQ", blob, 12)
+    for off in (36 + eb_size, 36 + eb_size + u_size):
+        m[off + 10: off + 13] = False
+    return m
+
+
+def cpu_baseline_single(workload, fields, eb, gpu_blob=None):
+    """The reference CPU implementation (1 core: the reference is
+    single-threaded), ZSTD timed apart.  2D: the whole field (about 10 s at
+    8192^2), whose blob is also compared with the GPU's (`parity`); 3D: the
+    first 96^3 blocks of the field for about 12 s."""
     import oracle
 
     use_ref = os.path.exists(oracle.REF_SO)
     impl = oracle.Reference() if use_ref else oracle.Oracle()
-    tiles = reference_samples(workload, fields, eb)
     kind = WORKLOADS[workload][0]
-    t_total, nbytes, n = 0.0, 0, 0
+    parity = None
     zt = 0.0
-    while t_total < budget_s and n < len(tiles):
-        t = [np.ascontiguousarray(a) for a in tiles[n]]
+    if kind in ("2d", "learned"):
+        U, V = (np.ascontiguousarray(a) for a in fields)
         t0 = time.perf_counter()
-        blob = impl.compress_2d(t[0], t[1], eb) if kind == "2d" else impl.compress_3d(t[0], t[1], t[2], eb)
-        t_total += time.perf_counter() - t0
-        if use_ref:
+        blob = impl.compress_2d(U, V, eb)
+        t_total = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        impl.zstd_compress(blob) if use_ref else None
+        zt = time.perf_counter() - t0
+        nbytes = U.nbytes + V.nbytes
+        sample = f"the whole {U.shape[0]}x{U.shape[1]} field, 1 thread, {t_total:.1f} s"
+        if gpu_blob is not None:
+            same = len(blob) == len(gpu_blob)
+            if same:
+                x = np.frombuffer(blob, np.uint8)
+                y = np.frombuffer(gpu_blob, np.uint8)
+                same = bool(((x == y) | ~_meaninfo_padding_2d(blob)).all())
+            parity = {"blob_equal_reference": same, "bytes": len(blob),
+                      "compared": "whole blob against the reference's own compressor on the same field "
+                                  "(the 6 indeterminate meanInfo padding bytes masked)"}
+    else:
+        s = 96
+        U, V, Wf = fields
+        t_total, nbytes, n = 0.0, 0, 0
+        for i in range(0, U.shape[0] - s + 1, s):
+            t = [np.ascontiguousarray(a[i:i + s, :s, :s]) for a in (U, V, Wf)]
             t0 = time.perf_counter()
-            impl.zstd_compress(blob)
-            zt += time.perf_counter() - t0
-        nbytes += sum(a.nbytes for a in t)
-        n += 1
+            blob = impl.compress_3d(t[0], t[1], t[2], eb)
+            t_total += time.perf_counter() - t0
+            if use_ref:
+                t0 = time.perf_counter()
+                impl.zstd_compress(blob)
+                zt += time.perf_counter() - t0
+            nbytes += sum(a.nbytes for a in t)
+            n += 1
+            if t_total > 12.0:
+                break
+        sample = f"{n} blocks 96^3 of the workload, 1 thread, {t_total:.1f} s"
+    if use_ref:
+        sample += f"; host ZSTD stage separately {nbytes / max(zt, 1e-9) / 1e9:.3f} GB/s"
     return {"value": round(nbytes / t_total / 1e9, 5), "unit": "GB/s", "cores": 1,
-            "kind": "reference" if use_ref else "port",
-            "sample": f"{n} tiles {'1024x1024' if kind == '2d' else '96^3'} of the workload, 1 thread, "
-                      f"{t_total:.1f} s; host ZSTD stage separately {nbytes / max(zt, 1e-9) / 1e9:.3f} GB/s"}
+            "kind": "reference" if use_ref else "port", "sample": sample}, parity
 
 
 def run_product(args, rank, world, device):
@@ -342,6 +439,10 @@ def run_product(args, rank, world, device):
         decompress(blob, *shape, *outs, ctx=ctx)
     dec_ms = (time.perf_counter() - t0) * 1e3 / args.steps
     lossless = cpsz_b200.sz_lossless_compress(blob, 3)
+    # the timed blob's decode against the input: exact critical-point
+    # comparison of every cell (lost, spurious or retyped) and the point-wise
+    # relative bound |decoded - x| <= max_pwr_eb * |x|
+    check = cp_and_bound_check(kind, fields, outs, eb, ctx)
 
     stages = {k: statistics.mean(v) for k, v in stage_acc.items()}
     n = int(np.prod(shape))
@@ -366,8 +467,25 @@ def run_product(args, rank, world, device):
     return {
         "value": value, "ms": ms, "e2e_ms": e2e_ms, "dec_ms": dec_ms, "blob": len(blob), "size_dev": size,
         "lossless": len(lossless), "raw": raw_bytes, "stages": stages, "roofline": roof, "launches": launches,
-        "clocks": clk.summary(), "fields": fields, "eb": eb,
+        "clocks": clk.summary(), "fields": fields, "eb": eb, "blob_bytes": blob, "check": check,
     }
+
+
+def cp_and_bound_check(kind, fields, decoded, eb, ctx):
+    """{cp_errors, cps, bound_violations} of a decode: CP cells compared with
+    the exact checker on the GPU; the bound checked on the host in double."""
+    import cpsz_b200
+
+    if kind == "3d":
+        c = cpsz_b200.cp_check_3d(*fields, *decoded, ctx=ctx)
+    else:
+        c = cpsz_b200.cp_check_2d(*fields, *decoded, ctx=ctx)
+    viol = 0
+    for x, d in zip(fields, decoded):
+        x64 = x.astype(np.float64)
+        viol += int(np.count_nonzero(np.abs(d.astype(np.float64) - x64) > eb * np.abs(x64)))
+    return {"cp_errors": int(c["lost_or_spurious"] + c["type_changed"]), "cps": int(c["cps_a"]),
+            "bound_violations": viol}
 
 
 def run_learned(args, rank, world, device):
@@ -601,10 +719,12 @@ def main():
         if rank == 0:
             print(json.dumps(line))
         return
+    kind = WORKLOADS[args.workload][0]
     r = run_product(args, rank, world, local)
-    cpu = None
+    cpu, parity = None, None
     if rank == 0 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_single(args.workload, r["fields"], r["eb"])
+        cpu, parity = cpu_baseline_single(args.workload, r["fields"], r["eb"],
+                                          r["blob_bytes"] if kind == "2d" else None)
     if world > 1:
         import torch.distributed as dist
 
@@ -612,7 +732,6 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return
-    kind = WORKLOADS[args.workload][0]
     raw = r["raw"]
     line = {
         "metric": "compress_GBps", "value": round(r["value"], 3), "unit": "GB/s", "n_gpus": world,
@@ -626,7 +745,7 @@ def main():
         "e2e": {"value": round(raw / (r["e2e_ms"] / 1e3) / 1e9, 3), "unit": "GB/s", "h2d_bytes_per_step": raw,
                 "d2h_bytes_per_step": r["blob"]},
         "roofline": r["roofline"], "stages_ms": {k: round(v, 4) for k, v in r["stages"].items()},
-        "cpu_baseline": cpu, "clocks": r["clocks"], "gpu_launches": r["launches"],
+        "cpu_baseline": cpu, "parity": parity, **r["check"], "clocks": r["clocks"], "gpu_launches": r["launches"],
     }
     print(json.dumps(line))
 

@@ -32,15 +32,19 @@ _sz = C.c_size_t
 
 
 def build_oracle(force: bool = False) -> str:
-    srcs = [os.path.join(HERE, f) for f in ("cpsz_oracle.c", "cpsz_oracle_huffman.c", "cpsz_oracle_3d.c", "cpsz_oracle.h")]
+    srcs = [os.path.join(HERE, f) for f in ("cpsz_oracle.c", "cpsz_oracle_huffman.c", "cpsz_oracle_3d.c",
+                                            "cpsz_oracle_gen.c", "cpsz_oracle.h")]
     if force or not os.path.exists(ORACLE_SO) or any(os.path.getmtime(s) > os.path.getmtime(ORACLE_SO) for s in srcs):
         subprocess.run(["make", "-s", "-C", HERE], check=True)
     return ORACLE_SO
 
 
-def build_reference(ref_dir: str = "/root/reference") -> str | None:
-    """Compile the reference sources into oracle/_ref when they are present."""
-    if os.path.isdir(os.path.join(ref_dir, "src")):
+def build_reference(ref_dir: str | None = None) -> str | None:
+    """Compile the reference sources into oracle/_ref when they are present
+    (``ref_dir``, else the environment variable ``CPSZ_REF_DIR``); returns the
+    library path, or None when it is neither built nor buildable here."""
+    ref_dir = ref_dir or os.environ.get("CPSZ_REF_DIR")
+    if ref_dir and os.path.isdir(os.path.join(ref_dir, "src")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_DIR={ref_dir}"], check=True)
     return REF_SO if os.path.exists(REF_SO) else None
 
@@ -79,6 +83,35 @@ class Oracle:
         L.cpo_free.argtypes = [C.c_void_p]
         L.cpo_log2f_array.argtypes = [_f32p, _sz, _f32p]
         L.cpo_exp2f_array.argtypes = [_f32p, _sz, _f32p]
+        L.cpo_generate_field_2d.argtypes = [C.c_uint64, _sz, _sz, C.c_int, C.c_double, C.c_double, _f32p, _f32p]
+        L.cpo_generate_field_3d.argtypes = [C.c_uint64, _sz, _sz, _sz, C.c_int, C.c_double, C.c_double, _f32p,
+                                            _f32p, _f32p]
+        L.cpo_batch_layout.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p]
+
+    # -- seeded workloads (the same fields as cpsz_b200.workloads, built without the product) --
+    def field_2d(self, seed, r1, r2, n_flows, sigma, noise=0.01):
+        U = np.empty((r1, r2), np.float32)
+        V = np.empty((r1, r2), np.float32)
+        if self.lib.cpo_generate_field_2d(seed, r1, r2, n_flows, sigma, noise, U, V):
+            raise ValueError("oracle generator: bad arguments or out of memory")
+        return U, V
+
+    def field_3d(self, seed, r1, r2, r3, n_flows, sigma, noise=0.01):
+        out = [np.empty((r1, r2, r3), np.float32) for _ in range(3)]
+        if self.lib.cpo_generate_field_3d(seed, r1, r2, r3, n_flows, sigma, noise, *out):
+            raise ValueError("oracle generator: bad arguments or out of memory")
+        return tuple(out)
+
+    def batch_layout(self, base_seed=3, n_fields=256, lo=128, hi=4096):
+        r1 = np.empty(n_fields, np.uint64)
+        r2 = np.empty(n_fields, np.uint64)
+        seeds = np.empty(n_fields, np.uint64)
+        ebs = np.empty(n_fields, np.float64)
+        if self.lib.cpo_batch_layout(base_seed, n_fields, lo, hi, r1.ctypes.data, r2.ctypes.data,
+                                     seeds.ctypes.data, ebs.ctypes.data):
+            raise ValueError("oracle batch layout: bad arguments")
+        return [(int(a), int(b), int(s), float(e)) for a, b, s, e in zip(r1, r2, seeds, ebs)]
 
     # -- 2D --
     def eb_2d(self, U, V, eb):

@@ -1,9 +1,9 @@
 """Generates tests/golden/*.npz from the reference's own implementation.
 
 Run where the reference sources are present (they are compiled into
-oracle/_ref by `make -C oracle ref`):
+oracle/_ref by `make -C oracle ref`), naming their directory:
 
-    python tests/golden/make_golden.py
+    CPSZ_REF_DIR=<reference source tree> python tests/golden/make_golden.py
 
 Each fixture holds the input field(s), the reference's compressed blob and the
 reference's decompressed field(s).  Inputs come from the seeded generators in
