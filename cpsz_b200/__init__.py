@@ -8,6 +8,8 @@ reference (C++)                                here
 =============================================  =====================================================
 ``sz_compress_cp_preserve_2d_offline<float>``  :func:`sz_compress_cp_preserve_2d_offline`
 ``sz_decompress_cp_preserve_2d_offline``       :func:`sz_decompress_cp_preserve_2d_offline`
+``sz_compress_cp_preserve_2d_offline_log``     :func:`sz_compress_cp_preserve_2d_offline_log`
+``sz_decompress_cp_preserve_2d_offline_log``   :func:`sz_decompress_cp_preserve_2d_offline_log`
 ``sz_compress_cp_preserve_3d_offline_log``     :func:`sz_compress_cp_preserve_3d_offline_log`
 ``sz_decompress_cp_preserve_3d_online_log``    :func:`sz_decompress_cp_preserve_3d_online_log`
 ``sz_lossless_compress/decompress`` (ZSTD)     :func:`sz_lossless_compress` / :func:`sz_lossless_decompress`
@@ -60,6 +62,13 @@ def _declare(L):
     L.cpsz_b200_compress_2d_offline_f32.argtypes = [_vp, _vp, _vp, _sz, _sz, C.c_double, C.POINTER(_vp), C.POINTER(_sz)]
     L.cpsz_b200_compress_2d_offline_f32_into.argtypes = [_vp, _vp, _vp, _sz, _sz, C.c_double, _vp, _sz, C.POINTER(_sz)]
     L.cpsz_b200_decompress_2d_offline_f32.argtypes = [_vp, C.c_char_p, _sz, _sz, _sz, _vp, _vp]
+    L.cpsz_b200_compress_2d_offline_log_f32.argtypes = [_vp, _vp, _vp, _sz, _sz, C.c_double, C.POINTER(_vp),
+                                                        C.POINTER(_sz)]
+    L.cpsz_b200_compress_2d_offline_log_f32_into.argtypes = [_vp, _vp, _vp, _sz, _sz, C.c_double, _vp, _sz,
+                                                             C.POINTER(_sz)]
+    L.cpsz_b200_decompress_2d_offline_log_f32.argtypes = [_vp, C.c_char_p, _sz, _sz, _sz, _vp, _vp]
+    L.cpsz_b200_blob_size_2d_log.argtypes = [C.c_char_p, _sz, _sz]
+    L.cpsz_b200_blob_size_2d_log.restype = _sz
     L.cpsz_b200_compress_2d_stages.argtypes = [_vp, _vp, _vp, _sz, _sz, C.c_double, _vp, _vp, _vp, _vp, _vp, _vp]
     L.cpsz_b200_blob_size_2d.argtypes = [C.c_char_p]
     L.cpsz_b200_blob_size_2d.restype = _sz
@@ -69,6 +78,9 @@ def _declare(L):
     L.cpsz_b200_huffman_codebook.argtypes = [_vp, _sz, _sz, _vp, _vp, _vp, C.POINTER(_sz)]
     L.cpsz_b200_huffman_encode_u16.argtypes = [_vp, _vp, _sz, _vp, _vp, _vp, _sz, C.POINTER(C.c_uint64)]
     L.cpsz_b200_huffman_encode_u16_noalloc.argtypes = [_vp, _sz, _vp, _vp, _vp, _sz, _vp, _vp]
+    L.cpsz_b200_lossless_bound.argtypes = [_sz]
+    L.cpsz_b200_lossless_bound.restype = _sz
+    L.cpsz_b200_lossless_compress.argtypes = [_vp, _vp, _sz, _vp, _sz, C.POINTER(_sz)]
     L.cpsz_b200_zstd_compress.argtypes = [C.c_char_p, _sz, C.c_int, C.POINTER(_vp), C.POINTER(_sz)]
     L.cpsz_b200_zstd_decompress.argtypes = [C.c_char_p, _sz, _vp, _sz]
     for name in ("cpsz_b200_compress_3d_offline_log_f32", "cpsz_b200_decompress_3d_online_log_f32",
@@ -344,6 +356,51 @@ def sz_decompress_cp_preserve_2d_offline(blob: bytes, r1: int, r2: int, U=None, 
     if ku is not U or kv is not V:
         raise TypeError("output arrays must be C-contiguous float32")
     _check(lib().cpsz_b200_decompress_2d_offline_f32(_h(ctx), blob, len(blob), r1, r2, pu, pv))
+    return U, V
+
+
+def sz_compress_cp_preserve_2d_offline_log(U, V, r1: int | None = None, r2: int | None = None,
+                                           max_pwr_eb: float = 0.1, ctx: Context | None = None) -> bytes:
+    """GPU ``sz_compress_cp_preserve_2d_offline_log<float>``: returns the blob (bytes)."""
+    pu, ku, su = _ptr(U)
+    pv, kv, sv = _ptr(V)
+    if r1 is None:
+        r1, r2 = su
+    if su != sv or int(np.prod(su)) != r1 * r2:
+        raise ValueError("U and V must both hold r1*r2 floats")
+    out = _vp()
+    n = _sz()
+    _check(lib().cpsz_b200_compress_2d_offline_log_f32(_h(ctx), pu, pv, r1, r2, float(max_pwr_eb), C.byref(out),
+                                                       C.byref(n)))
+    try:
+        return C.string_at(out, n.value)
+    finally:
+        C.CDLL(None).free(out)
+
+
+def compress_2d_log_into(U, V, r1, r2, max_pwr_eb, out, ctx: Context | None = None) -> int:
+    """The offline_log compressor into caller memory ``out`` (host or device uint8); returns the blob size."""
+    pu, ku, _ = _ptr(U)
+    pv, kv, _ = _ptr(V)
+    po, ko, so = _ptr(out, np.uint8)
+    n = _sz()
+    _check(lib().cpsz_b200_compress_2d_offline_log_f32_into(_h(ctx), pu, pv, r1, r2, float(max_pwr_eb), po,
+                                                            int(np.prod(so)), C.byref(n)))
+    return n.value
+
+
+def sz_decompress_cp_preserve_2d_offline_log(blob: bytes, r1: int, r2: int, U=None, V=None,
+                                             ctx: Context | None = None):
+    """GPU ``sz_decompress_cp_preserve_2d_offline_log<float>``: returns (U, V)."""
+    if U is None:
+        U = np.empty((r1, r2), np.float32)
+    if V is None:
+        V = np.empty((r1, r2), np.float32)
+    pu, ku, _ = _ptr(U)
+    pv, kv, _ = _ptr(V)
+    if ku is not U or kv is not V:
+        raise TypeError("output arrays must be C-contiguous float32")
+    _check(lib().cpsz_b200_decompress_2d_offline_log_f32(_h(ctx), blob, len(blob), r1, r2, pu, pv))
     return U, V
 
 
@@ -688,6 +745,24 @@ def huffman_encode_u16_noalloc(sym, code, ln, out, total_bits, stream: int = 0) 
 
 
 # ---- lossless stage (host ZSTD, as the reference) -------------------------------------
+
+def lossless_compress_gpu(data, out=None, ctx: Context | None = None):
+    """GPU Zstandard frame of `data` (bytes / host uint8 array, or a device
+    uint8 array).  Returns bytes, or with `out` (host or device uint8 array)
+    the frame size written there."""
+    if isinstance(data, (bytes, bytearray, memoryview)):
+        data = np.frombuffer(bytes(data), np.uint8)
+    pi, ki, si = _ptr(data, np.uint8)
+    n = int(np.prod(si))
+    size = _sz()
+    if out is None:
+        buf = np.empty(lib().cpsz_b200_lossless_bound(n), np.uint8)
+        _check(lib().cpsz_b200_lossless_compress(_h(ctx), pi, n, buf.ctypes.data, buf.size, C.byref(size)))
+        return buf[:size.value].tobytes()
+    po, ko, so = _ptr(out, np.uint8)
+    _check(lib().cpsz_b200_lossless_compress(_h(ctx), pi, n, po, int(np.prod(so)), C.byref(size)))
+    return size.value
+
 
 def sz_lossless_compress(data: bytes, level: int = 3) -> bytes:
     out = _vp()

@@ -395,14 +395,17 @@ struct StripUnpass {
   unsigned long long n_unpred;
   float2* pair;                // raster (pitch r2)
   unsigned long long* status;  // as in StripPass
+  int id_shift;                // p = 2^(id_shift * id) * 2^-52: 2 (offline), 1 (offline_log)
 };
 
 // Decompression side of a point: the addend 2(code - 32768) * p that the
-// wavefront adds to its prediction (p = 4^id * 2^-52, 0 for id 0;
-// src/sz_decompress_cp_preserve_2d.cpp:30-34, include/sz_decompression_utils.hpp:65-73),
-// or for code 0 the raw flag with the raw value in .x.
-__device__ __forceinline__ float2 dec_pair(unsigned int code, unsigned int id) {
-  const float p = id ? __int_as_float((int)(2 * id - 52 + 127) << 23) : 0.f;
+// wavefront adds to its prediction (p = 4^id * 2^-52 for the offline blob,
+// 2^id * 2^-52 for the offline_log one, 0 for id 0;
+// src/sz_decompress_cp_preserve_2d.cpp:30-34 and :76-80,
+// include/sz_decompression_utils.hpp:65-73), or for code 0 the raw flag with
+// the raw value in .x.
+__device__ __forceinline__ float2 dec_pair(unsigned int code, unsigned int id, int shift) {
+  const float p = id ? __int_as_float((int)(shift * (int)id - 52 + 127) << 23) : 0.f;
   return make_float2((float)(2 * ((int)code - 32768)) * p, __int_as_float(code == 0 ? 1 : 0));
 }
 
@@ -490,8 +493,10 @@ __global__ void __launch_bounds__(STRIP_NT) strip_unpass_kernel(StripUnpass P0, 
       if (q < tot) {
         const int li = q / nq, c = 4 * (q - li * nq);
         const uint2 cw = *reinterpret_cast<const uint2*>(&t[li][c]);
-        const float2 a = dec_pair(cw.x & 0xffffu, idv[u] & 0xffu), b = dec_pair(cw.x >> 16, (idv[u] >> 8) & 0xffu);
-        const float2 d = dec_pair(cw.y & 0xffffu, (idv[u] >> 16) & 0xffu), e = dec_pair(cw.y >> 16, idv[u] >> 24);
+        const float2 a = dec_pair(cw.x & 0xffffu, idv[u] & 0xffu, P.id_shift),
+                     b = dec_pair(cw.x >> 16, (idv[u] >> 8) & 0xffu, P.id_shift);
+        const float2 d = dec_pair(cw.y & 0xffffu, (idv[u] >> 16) & 0xffu, P.id_shift),
+                     e = dec_pair(cw.y >> 16, idv[u] >> 24, P.id_shift);
         float4* out = reinterpret_cast<float4*>(P.pair + (row0 + li) * r2 + g.c0 + c);
         out[0] = make_float4(a.x, a.y, b.x, b.y);
         out[1] = make_float4(d.x, d.y, e.x, e.y);
@@ -502,7 +507,7 @@ __global__ void __launch_bounds__(STRIP_NT) strip_unpass_kernel(StripUnpass P0, 
     for (int q = threadIdx.x; q < g.h * g.W; q += STRIP_NT) {
       const int li = q / g.W, c = q - li * g.W;
       const long long gi = (row0 + li) * r2 + g.c0 + c;
-      P.pair[gi] = dec_pair(t[li][c], P.ids[gi]);
+      P.pair[gi] = dec_pair(t[li][c], P.ids[gi], P.id_shift);
     }
   }
   __syncthreads();  // the raw values below overwrite .x of pairs stored above
@@ -582,7 +587,7 @@ int launch_strip_pass(cpsz_b200_ctx* ctx, const uint16_t* const raster[2], long 
 
 int launch_strip_unpass(cpsz_b200_ctx* ctx, const uint16_t* const blocks[2], const uint8_t* const ids[2],
                         const float* const unpred[2], const unsigned long long n_unpred[2], int r1, int r2,
-                        float2* const pair[2], void* const scratch[2]) {
+                        float2* const pair[2], void* const scratch[2], int id_shift) {
   const size_t ns = strip_count(r1, r2);
   if (ns > 0x7fffffffu) return set_error(CPSZ_ERR_UNSUPPORTED, "field of %zu strips", ns);
   for (int f = 0; f < 2; f++)  // the totals of an empty field read 0
@@ -590,7 +595,8 @@ int launch_strip_unpass(cpsz_b200_ctx* ctx, const uint16_t* const blocks[2], con
   if (ns == 0) return CPSZ_OK;
   const int nsc = (r2 + STRIP_W - 1) / STRIP_W;
   StripUnpass P[2];
-  for (int f = 0; f < 2; f++) P[f] = StripUnpass{blocks[f], ids[f], unpred[f], n_unpred[f], pair[f], (unsigned long long*)scratch[f]};
+  for (int f = 0; f < 2; f++)
+    P[f] = StripUnpass{blocks[f], ids[f], unpred[f], n_unpred[f], pair[f], (unsigned long long*)scratch[f], id_shift};
   strip_unpass_kernel<<<dim3((unsigned)ns, 2), STRIP_NT, 0, ctx->stream>>>(P[0], P[1], r1, r2, nsc, (unsigned)ns,
                                                                            ctx->d_flag);
   count_launch(ctx);

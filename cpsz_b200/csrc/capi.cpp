@@ -89,6 +89,58 @@ int cpsz_b200_decompress_2d_offline_f32(cpsz_b200_ctx* ctx, const unsigned char*
   return CPSZ_OK;
 }
 
+int cpsz_b200_compress_2d_offline_log_f32(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2,
+                                          double max_pwr_eb, unsigned char** blob, size_t* blob_size) {
+  if (!blob || !blob_size) return set_error(CPSZ_ERR_INVALID, "null output pointer");
+  *blob = nullptr;
+  *blob_size = 0;
+  RESOLVE(ctx);
+  Blob2D b;
+  CPSZ_TRY(compress_2d(ctx, U, V, r1, r2, max_pwr_eb, &b, nullptr, nullptr, nullptr, 0, true));
+  unsigned char* h = (unsigned char*)malloc(b.size ? b.size : 1);
+  if (!h) return set_error(CPSZ_ERR_NOMEM, "host blob of %zu bytes", b.size);
+  int rc = d2h(ctx, h, b.d_blob, b.size, ctx->stream);
+  if (rc == CPSZ_OK) {
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) rc = set_error(CPSZ_ERR_CUDA, "blob download: %s", cudaGetErrorString(e));
+  }
+  if (rc != CPSZ_OK) {
+    free(h);
+    return rc;
+  }
+  *blob = h;
+  *blob_size = b.size;
+  return CPSZ_OK;
+}
+
+int cpsz_b200_compress_2d_offline_log_f32_into(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1,
+                                               size_t r2, double max_pwr_eb, unsigned char* out, size_t out_cap,
+                                               size_t* blob_size) {
+  if (!out || !blob_size) return set_error(CPSZ_ERR_INVALID, "null output pointer");
+  RESOLVE(ctx);
+  Blob2D b;
+  if (host_kind(out) != HOST_DEVICE) {
+    CPSZ_TRY(compress_2d(ctx, U, V, r1, r2, max_pwr_eb, &b, nullptr, nullptr, out, out_cap, true));
+    *blob_size = b.size;
+    CPSZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    return CPSZ_OK;
+  }
+  CPSZ_TRY(compress_2d(ctx, U, V, r1, r2, max_pwr_eb, &b, nullptr, nullptr, nullptr, 0, true));
+  *blob_size = b.size;
+  if (b.size > out_cap) return set_error(CPSZ_ERR_INVALID, "output capacity %zu < blob size %zu", out_cap, b.size);
+  CPSZ_TRY(copy_out(ctx, out, b.d_blob, b.size));
+  CPSZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return CPSZ_OK;
+}
+
+int cpsz_b200_decompress_2d_offline_log_f32(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_size,
+                                            size_t r1, size_t r2, float* U, float* V) {
+  RESOLVE(ctx);
+  CPSZ_TRY(decompress_2d(ctx, blob, blob_size, r1, r2, U, V, true));
+  CPSZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return CPSZ_OK;
+}
+
 int cpsz_b200_compress_2d_stages(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2,
                                  double max_pwr_eb, int32_t* ids, int32_t* codes_u, int32_t* codes_v, float* recon_u,
                                  float* recon_v, size_t* n_unpred) {
@@ -196,7 +248,7 @@ int cpsz_b200_debug_wave_trace(cpsz_b200_ctx* ctx, size_t len, long long* out) {
 }
 
 int cpsz_b200_debug_quant_table(int which, double* t, int* n) {
-  const QuantTable& q = which == 3 ? quant_table_3d() : quant_table_2d();
+  const QuantTable& q = which == 3 ? quant_table_3d() : which == 1 ? quant_table_2d_log() : quant_table_2d();
   if (t) memcpy(t, q.t, sizeof(q.t));
   if (n) *n = q.n;
   return CPSZ_OK;
@@ -514,6 +566,48 @@ size_t cpsz_b200_blob_size_2d(const unsigned char* blob) {
   return 36 + (size_t)s[0] + (size_t)s[1] + (size_t)s[2];
 }
 
+size_t cpsz_b200_blob_size_2d_log(const unsigned char* blob, size_t r1, size_t r2) {
+  if (!blob || !r1 || !r2) return 0;
+  unsigned long long s[3];
+  memcpy(s, blob + 12, 24);
+  return 36 + (size_t)s[0] + 2 * ((r1 * r2 - 1) / 8 + 1) + (size_t)s[1] + (size_t)s[2];
+}
+
+size_t cpsz_b200_lossless_bound(size_t n) { return zstd_frame_bound(n); }
+
+int cpsz_b200_lossless_compress(cpsz_b200_ctx* ctx, const unsigned char* in, size_t n, unsigned char* out,
+                                size_t out_cap, size_t* out_size) {
+  if ((!in && n) || !out || !out_size) return set_error(CPSZ_ERR_INVALID, "null pointer argument");
+  RESOLVE(ctx);
+  *out_size = 0;
+  const bool dev_in = n == 0 || is_device_ptr(in);
+  const bool dev_out = is_device_ptr(out);
+  const size_t bound = zstd_frame_bound(n);
+  size_t bytes = align_up(zstd_tmp_bytes(n), 256) + 256;
+  if (!dev_in) bytes += align_up(n, 256) + 256;
+  if (!dev_out) bytes += align_up(bound, 256) + 256;
+  CPSZ_TRY(arena_reserve(ctx, bytes));
+  void* tmp = arena_alloc(ctx, zstd_tmp_bytes(n));
+  const uint8_t* d_in = (const uint8_t*)in;
+  if (!dev_in) {
+    uint8_t* p = (uint8_t*)arena_alloc(ctx, n);
+    CPSZ_TRY(h2d(ctx, p, in, n, ctx->stream));
+    d_in = p;
+  }
+  uint8_t* d_out = dev_out ? out : (uint8_t*)arena_alloc(ctx, bound);
+  if (!d_out || !tmp) return set_error(CPSZ_ERR_NOMEM, "workspace layout overflow");
+  CPSZ_CUDA_TRY(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+  size_t fsize = 0;
+  CPSZ_TRY(launch_zstd_frame(ctx, d_in, n, d_out, dev_out ? out_cap : bound, &fsize, tmp));
+  *out_size = fsize;
+  if (!dev_out) {
+    if (fsize > out_cap) return set_error(CPSZ_ERR_INVALID, "output capacity %zu < frame size %zu", out_cap, fsize);
+    CPSZ_TRY(d2h(ctx, out, d_out, fsize, ctx->stream));
+  }
+  CPSZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return CPSZ_OK;
+}
+
 int cpsz_b200_zstd_compress(const unsigned char* data, size_t n, int level, unsigned char** out, size_t* out_size) {
   if (!out || !out_size || (!data && n)) return set_error(CPSZ_ERR_INVALID, "null pointer");
   size_t cap = ZSTD_compressBound(n);
@@ -594,6 +688,62 @@ template unsigned char* sz_compress_cp_preserve_2d_offline<double>(const double*
                                                                    size_t&, bool, double);
 template void sz_decompress_cp_preserve_2d_offline<float>(const unsigned char*, size_t, size_t, float*&, float*&);
 template void sz_decompress_cp_preserve_2d_offline<double>(const unsigned char*, size_t, size_t, double*&, double*&);
+
+template <typename T>
+unsigned char* sz_compress_cp_preserve_2d_offline_log(const T* U, const T* V, size_t r1, size_t r2,
+                                                      size_t& compressed_size, bool transpose, double max_pwr_eb) {
+  (void)transpose;  // ignored by the reference as well
+  compressed_size = 0;
+  if (sizeof(T) != sizeof(float)) {
+    set_error(CPSZ_ERR_UNSUPPORTED, "only float fields are supported on the GPU path");
+    return nullptr;
+  }
+  unsigned char* blob = nullptr;
+  size_t size = 0;
+  if (cpsz_b200_compress_2d_offline_log_f32(nullptr, (const float*)U, (const float*)V, r1, r2, max_pwr_eb, &blob,
+                                            &size) != CPSZ_OK)
+    return nullptr;
+  compressed_size = size;
+  return blob;
+}
+
+template <typename T>
+void sz_decompress_cp_preserve_2d_offline_log(const unsigned char* compressed, size_t r1, size_t r2, T*& U, T*& V) {
+  if (U) free(U);
+  if (V) free(V);
+  U = nullptr;
+  V = nullptr;
+  if (sizeof(T) != sizeof(float)) {
+    set_error(CPSZ_ERR_UNSUPPORTED, "only float fields are supported on the GPU path");
+    return;
+  }
+  size_t n = r1 * r2;
+  T* u = (T*)malloc(n * sizeof(T));
+  T* v = (T*)malloc(n * sizeof(T));
+  if (!u || !v) {
+    free(u);
+    free(v);
+    set_error(CPSZ_ERR_NOMEM, "output fields");
+    return;
+  }
+  size_t blob_size = cpsz_b200_blob_size_2d_log(compressed, r1, r2);
+  if (cpsz_b200_decompress_2d_offline_log_f32(nullptr, compressed, blob_size, r1, r2, (float*)u, (float*)v) !=
+      CPSZ_OK) {
+    free(u);
+    free(v);
+    return;
+  }
+  U = u;
+  V = v;
+}
+
+template unsigned char* sz_compress_cp_preserve_2d_offline_log<float>(const float*, const float*, size_t, size_t,
+                                                                      size_t&, bool, double);
+template unsigned char* sz_compress_cp_preserve_2d_offline_log<double>(const double*, const double*, size_t, size_t,
+                                                                       size_t&, bool, double);
+template void sz_decompress_cp_preserve_2d_offline_log<float>(const unsigned char*, size_t, size_t, float*&, float*&);
+template void sz_decompress_cp_preserve_2d_offline_log<double>(const unsigned char*, size_t, size_t, double*&,
+                                                               double*&);
 
 template <typename T>
 unsigned char* sz_compress_cp_preserve_3d_offline_log(const T* U, const T* V, const T* W, size_t r1, size_t r2,

@@ -19,11 +19,12 @@
 // size.  Every shape computes the same bytes: each vertex's bound is the same
 // minimum over the same six triangles, whichever tile evaluates them.
 //
-// CTAs are persistent: the grid holds as many CTAs as fit on the device (one
-// per SM fewer when the Lorenzo wavefront runs beside the kernel) and each
-// takes tiles in row-major order with a grid stride, so row groups complete
-// in order.  A kernel enqueued first and holding a fixed number of slots per
-// SM leaves exactly one slot on every SM for the wavefront launched after it.
+// CTAs are persistent: the grid holds as many CTAs as fit on the device and
+// each takes tiles in row-major order (a grid stride), so row groups complete
+// in order.  Beside the Lorenzo wavefront (which is launched after it) a CTA
+// that finds its SM already holding all but one of the CTAs that fit there
+// leaves at once, and the others take tiles from a counter: every SM keeps
+// room for one wavefront CTA, whatever the hardware's placement of the grid.
 #include <algorithm>
 
 #include "eb_math.cuh"
@@ -42,7 +43,8 @@ __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const f
                                                   float2* __restrict__ pair_u, float2* __restrict__ pair_v,
                                                   double* __restrict__ eb_out, int row_begin, int row_end,
                                                   unsigned long long* __restrict__ band_done, int tiles_x,
-                                                  int ntiles) {
+                                                  int ntiles, int log_ids, unsigned int* __restrict__ sched,
+                                                  int sm_cap) {
   constexpr int CX = TX + 1;  // cells per tile row
   constexpr int CY = TY + 1;
   static_assert(WAVE_GROUP_ROWS % TY == 0, "a tile's rows must lie in one wavefront group");
@@ -53,9 +55,29 @@ __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const f
   __shared__ unsigned int shist[256];
 
   const int tid = threadIdx.x;
+  __shared__ int s_tile;
+  if (sched) {
+    // at most sm_cap CTAs of this launch per SM (the others leave at once), so
+    // a wavefront launched after it finds room on every SM; tiles then come
+    // from a counter, in row-major order
+    if (tid == 0) {
+      unsigned smid;
+      asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+      s_tile = (smid >= 256u || atomicAdd(&sched[1 + smid], 1u) < (unsigned)sm_cap) ? 1 : 0;
+    }
+    __syncthreads();
+    if (!s_tile) return;
+  }
   for (int k = tid; k < 256; k += NT) shist[k] = 0;
   for (int k = tid; k < thr_n; k += NT) tab[k] = thr_tab[k];
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  for (int tile = blockIdx.x;; tile += gridDim.x) {
+    if (sched) {
+      __syncthreads();  // every thread has read the previous s_tile
+      if (tid == 0) s_tile = (int)atomicAdd(&sched[0], 1u);
+      __syncthreads();
+      tile = s_tile;
+    }
+    if (tile >= ntiles) break;
     const int i0 = row_begin + (tile / tiles_x) * TY, j0 = (tile % tiles_x) * TX;
     __syncthreads();  // the previous tile's readers of su / sv / tri are done
     // vertex halo: rows i0-1 .. i0+TY, cols j0-1 .. j0+TX
@@ -100,7 +122,7 @@ __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const f
     auto quant = [&](double e) -> int {
       if (e <= thr) return -1;
       const int ex = (int)((__double_as_longlong(e) >> 52) & 0x7ff) - 1023;
-      return dev::count_thresholds(tab, thr_n, e, (ex + 52) >> 1);
+      return dev::count_thresholds(tab, thr_n, e, (ex + 52) >> (log_ids ? 0 : 1));
     };
     for (int k = tid; k < TY * TX; k += NT) {
       int a = k / TX, b = k % TX;
@@ -109,6 +131,9 @@ __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const f
       // vertex (gi, gj) is local (a+1, b+1); cell (gi-1+x, gj-1+y) is tri[.][a+x][b+y]
       bool up = gi >= 1, left = gj >= 1, down = gi < r1 - 1, right = gj < r2 - 1;
       const float uu = su[a + 1][b + 1], vv = sv[a + 1][b + 1];
+      // Offline: one id per component, of |x| * eb (base 4).  offline_log: one
+      // id of the vertex bound itself (the log2(1 + eb) quantizer's table).
+      const double s0 = log_ids ? 1.0 : (double)fabsf(uu), s1 = (double)fabsf(vv);
       // the reference's chain eb = MINF(eb, triangle bound) over the six triangles
       auto vertex_eb = [&](auto&& tri_at) {
         double eb = max_pwr_eb;
@@ -146,24 +171,24 @@ __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const f
         }
         const double lo = fmin(max_pwr_eb, m * (1.0 - dev::FILTER_REL) - dev::FILTER_ABS);
         const double hi = fmin(max_pwr_eb, m * (1.0 + dev::FILTER_REL) + dev::FILTER_ABS);
-        code[0] = quant((double)fabsf(uu) * lo);
-        code[1] = quant((double)fabsf(vv) * lo);
+        code[0] = quant(s0 * lo);
+        code[1] = log_ids ? -1 : quant(s1 * lo);
         // the upper end has the same id iff it stays below the next threshold
         auto stays = [&](int c, double e) { return c < 0 ? e <= thr : (c + 1 >= thr_n || e < tab[c + 1]); };
-        if (nan || !stays(code[0], (double)fabsf(uu) * hi) || !stays(code[1], (double)fabsf(vv) * hi)) {
+        if (nan || !stays(code[0], s0 * hi) || (!log_ids && !stays(code[1], s1 * hi))) {
           // the enclosure straddles a threshold (or a bound is NaN): exact bounds
           eb = vertex_eb([&](int kind, int ca, int cb) {
             const int a1 = ca + (kind == 0), b1 = cb + (kind == 1);
             return dev::tri_eb_exact(su[ca][cb], su[a1][b1], su[ca + 1][cb + 1], sv[ca][cb], sv[a1][b1],
                                      sv[ca + 1][cb + 1], kind);
           });
-          code[0] = quant((double)fabsf(uu) * eb);
-          code[1] = quant((double)fabsf(vv) * eb);
+          code[0] = quant(s0 * eb);
+          code[1] = log_ids ? -1 : quant(s1 * eb);
         }
       } else {
         eb = vertex_eb([&](int kind, int ca, int cb) { return tri[kind][ca][cb]; });
-        code[0] = quant((double)fabsf(uu) * eb);
-        code[1] = quant((double)fabsf(vv) * eb);
+        code[0] = quant(s0 * eb);
+        code[1] = log_ids ? -1 : quant(s1 * eb);
       }
       int sym[2];
   #pragma unroll
@@ -178,7 +203,7 @@ __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const f
       size_t g = (size_t)gi * r2 + gj;
       if (!FAST && eb_out) eb_out[g] = eb;
       ids_u[g] = (uint8_t)code[0];
-      ids_v[g] = (uint8_t)code[1];
+      if (!log_ids) ids_v[g] = (uint8_t)code[1];
       if (pair_u) {
         // the wavefront's input: value and 1/precision = 2^(52 - 2 id) (NaN for precision 0)
         pair_u[g] = make_float2(uu, code[0] == ID_ZERO ? __int_as_float(0x7FC00000)
@@ -187,7 +212,7 @@ __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const f
                                                        : __int_as_float((127 + 52 - 2 * (int)code[1]) << 23));
       }
       atomicAdd(&shist[sym[0]], 1u);
-      atomicAdd(&shist[sym[1]], 1u);
+      if (!log_ids) atomicAdd(&shist[sym[1]], 1u);
     }
     if (band_done) {
       // every thread's outputs are visible device-wide before the tile counts
@@ -226,8 +251,10 @@ int preload_eb2d() {
 int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, double max_pwr_eb,
                 const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
                 float2* pair_u, float2* pair_v, double* eb_out, int row_begin, int row_end,
-                unsigned long long* band_done) {
+                unsigned long long* band_done, bool log_ids, unsigned int* sched) {
   if (row_end < 0) row_end = r1;
+  if (log_ids && (pair_u || pair_v || ids_v))
+    return set_error(CPSZ_ERR_INVALID, "eb2d: the log-domain ids have no wavefront pairs and one stream");
   if (row_end <= row_begin) return CPSZ_OK;
   if (band_done && row_begin % WAVE_GROUP_ROWS)
     return set_error(CPSZ_ERR_INVALID, "eb2d band start %d is not a multiple of %d", row_begin, WAVE_GROUP_ROWS);
@@ -239,15 +266,16 @@ int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int 
       err = set_error(CPSZ_ERR_UNSUPPORTED, "eb2d: %lld tiles", ntiles);
       return;
     }
-    // persistent grid: the CTAs that fit, one per SM fewer beside the wavefront
+    // persistent grid: the CTAs that fit; with `sched` (beside the wavefront)
+    // one per SM fewer stay, each SM keeping room for a wavefront CTA
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, nt, 0);
-    if (band_done && per_sm > 1) per_sm -= 1;
     if (per_sm < 1) per_sm = 1;
+    const int cap = sched ? std::max(1, per_sm - 1) : per_sm;
     const long long grid = std::min<long long>(ntiles, (long long)per_sm * ctx->num_sms);
     kernel<<<(unsigned)grid, nt, 0, ctx->stream>>>(U, V, r1, r2, max_pwr_eb, d_thr_tab, thr_n, ids_u, ids_v, hist,
                                                    ctx->d_flag, pair_u, pair_v, eb_out, row_begin, row_end,
-                                                   band_done, tiles_x, (int)ntiles);
+                                                   band_done, tiles_x, (int)ntiles, log_ids ? 1 : 0, sched, cap);
   };
   // filtered bounds unless the caller wants the bounds themselves (or an
   // unusual max_pwr_eb takes the reference's NaN paths)

@@ -31,10 +31,15 @@ constexpr int FLAG_OUT_CAPACITY = 16; // an output stream did not fit its buffer
 // outputs are visible device-wide (row_begin must then be a multiple of
 // WAVE_GROUP_ROWS), so a concurrently running wavefront can start on a group
 // as soon as its counter reaches rows x r2.
+// log_ids: the offline_log form -- one id per vertex, of the vertex bound
+// itself against quant_table_2d_log() (ids_v, pair_u and pair_v null).
 int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, double max_pwr_eb,
                 const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
                 float2* pair_u, float2* pair_v, double* eb_out = nullptr, int row_begin = 0, int row_end = -1,
-                unsigned long long* band_done = nullptr);
+                unsigned long long* band_done = nullptr, bool log_ids = false, unsigned int* sched = nullptr);
+// sched (optional, EB2D_SCHED_WORDS zeroed words): the launch keeps at most
+// one CTA per SM fewer than fit, leaving every SM room for a wavefront CTA.
+constexpr int EB2D_SCHED_WORDS = 257;
 
 // Loads every eb2d instantiation (required before a consumer that waits on
 // eb2d is launched: a lazily loaded first launch could wait for it).
@@ -118,9 +123,23 @@ int launch_strip_pass(cpsz_b200_ctx* ctx, const uint16_t* const raster[2], long 
 // flag bits 0), or for code 0 (raw value, raw flag bits 1), the raw values
 // taken from unpred[f] in block order (an index past n_unpred[f] raises
 // FLAG_RAW_RANGE).
+// id_shift: 2 for the offline ids (p = 4^id * 2^-52), 1 for the offline_log
+// ids (p = 2^id * 2^-52).
 int launch_strip_unpass(cpsz_b200_ctx* ctx, const uint16_t* const blocks[2], const uint8_t* const ids[2],
                         const float* const unpred[2], const unsigned long long n_unpred[2], int r1, int r2,
-                        float2* const pair[2], void* const scratch[2]);
+                        float2* const pair[2], void* const scratch[2], int id_shift = 2);
+
+// ---- 2D offline_log (log2d.cu) ------------------------------------------------------
+// Compression: per vertex the host library's log2f of |U| and |V| (-100 for 0)
+// as wavefront pairs (log, 1/precision = 2^(52 - id), NaN for ID_ZERO) and as
+// plain arrays, and the sign maps (value > 0, MSB-first bit streams;
+// ceil(n / 32) words each).
+int launch_log2d(cpsz_b200_ctx* ctx, const float* U, const float* V, const uint8_t* ids, size_t n, const LibmFn& L,
+                 float2* pair_u, float2* pair_v, float* log_u, float* log_v, uint32_t* sign_u, uint32_t* sign_v);
+// Decompression, in place: decoded logs below -99 -> 0, others -> +-exp2f(log)
+// with the stored sign (the host library's exp2f).
+int launch_exp2d(cpsz_b200_ctx* ctx, float* U, float* V, const uint8_t* sign_u, const uint8_t* sign_v, size_t n,
+                 const LibmFn& Ex);
 
 // ---- Huffman -------------------------------------------------------------------
 // Codebook for the encoder: per symbol, code right-aligned (bit len-1 = first bit).
@@ -250,6 +269,15 @@ int launch_mlp_cast(cpsz_b200_ctx* ctx, const MlpParams& w);
 // Features (bf16 [n x 128]) of the vertices idx[0..n) of field (U, V).
 int launch_mlp_features(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, const double* eb_a,
                         const int* idx, int n, void* X);
+
+// ---- lossless stage: Zstandard frames (zstd_enc.cu) -------------------------------------
+// Largest frame for n input bytes; device scratch of a call on n bytes.
+size_t zstd_frame_bound(size_t n);
+size_t zstd_tmp_bytes(size_t n);
+// d_in (n bytes) -> a Zstandard frame at d_out (device, out_cap bytes);
+// synchronises the stream once to learn the frame size (*out_size).
+int launch_zstd_frame(cpsz_b200_ctx* ctx, const uint8_t* d_in, size_t n, uint8_t* d_out, size_t out_cap,
+                      size_t* out_size, void* tmp);
 
 // ---- generic scans ----------------------------------------------------------------
 size_t scan_u32_tmp_bytes(size_t n);

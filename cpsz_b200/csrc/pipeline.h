@@ -42,11 +42,13 @@ int build_wave_items(int nfields, const int* r1s, std::vector<WaveItem>& items);
 // of the derived ones (the learned-bound path).  host_out (optional, host
 // memory of host_cap bytes): the blob is written there directly (out->d_blob
 // is then not set).
+// log_form: the offline_log blob (src/sz_compress_cp_preserve_2d.cpp:285-379)
+// instead of the offline one.
 int compress_2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2, double max_pwr_eb,
                 Blob2D* out, const StageTap* tap, const double* eb_ext = nullptr, unsigned char* host_out = nullptr,
-                size_t host_cap = 0);
+                size_t host_cap = 0, bool log_form = false);
 int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_size, size_t r1, size_t r2, float* U,
-                  float* V);
+                  float* V, bool log_form = false);
 // n fields; blobs back to back into `out` (host or device), offsets[0..n].
 int compress_2d_batch(cpsz_b200_ctx* ctx, int n, const float* const* U, const float* const* V, const size_t* r1,
                       const size_t* r2, const double* ebs, unsigned char* out, size_t out_cap, size_t* offsets);

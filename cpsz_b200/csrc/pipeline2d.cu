@@ -50,6 +50,8 @@ constexpr size_t PINNED_BASE = 4096;  // the flag word and scalars live below
 // sub-batch limits: fields per pass (pinned staging) and points per pass (workspace)
 constexpr int BATCH_MAX_FIELDS = 32;
 constexpr size_t BATCH_MAX_POINTS = (size_t)1 << 27;
+// the bound kernel's placement words of every upload band of a pass
+constexpr size_t SCHED_BYTES = (size_t)cpsz_b200_ctx::kUploadChunks * EB2D_SCHED_WORDS * 4;
 
 struct DevBuf {
   // arena sub-allocations of one field
@@ -70,6 +72,8 @@ struct DevBuf {
   void* enc_tmp[3];
   uint32_t* bits[3];
   uint8_t* blob;
+  float* logs[2];       // offline_log: log2f |U|, |V| (the unpredictable values it stores)
+  uint32_t* signs[2];   // offline_log: sign maps
 };
 
 // One field of a compression pass (a pass holds one or more fields).
@@ -95,6 +99,10 @@ struct Job2D {
   // copied from their device buffers), not assembled in device memory
   unsigned char* host_out = nullptr;
   size_t host_cap = 0;
+  // the offline_log form: base 2, one id stream of N symbols, the two sign
+  // maps (device, MSB-first bit streams) between the id section and the fields
+  bool log_form = false;
+  const uint32_t* d_signs[2] = {nullptr, nullptr};
 };
 
 int read_flag(cpsz_b200_ctx* ctx, int* out) {
@@ -157,7 +165,8 @@ int job_init(Job2D& j, const float* U, const float* V, size_t r1s, size_t r2s, d
   // bit streams: Huffman averages < log2(distinct) + 1 bits per symbol
   j.ids_bits_cap = (2 * j.N * 9 + 7) / 8 + 64;
   j.codes_bits_cap = (j.N * 17 + 7) / 8 + 64;
-  j.blob_cap = BLOB_HDR + 2 * FIELD_HDR + 8 * j.N + 2 * ((j.nblocks + 7) / 8) + 3 * (12 + 1 + 13 * 131072 + 8) +
+  j.blob_cap = BLOB_HDR + 2 * FIELD_HDR + 8 * j.N + 2 * ((j.nblocks + 7) / 8) + 2 * (j.N / 8 + 1) +
+               3 * (12 + 1 + 13 * 131072 + 8) +
                j.ids_bits_cap + 2 * j.codes_bits_cap + 64;
   return CPSZ_OK;
 }
@@ -185,6 +194,10 @@ size_t job_bytes(const Job2D& j) {
   add(j.ids_bits_cap);
   add(2 * j.codes_bits_cap);
   add(j.blob_cap);
+  if (j.log_form) {
+    add(2 * 4 * N);                        // log values
+    add(2 * 4 * ((N + 31) / 32));          // sign maps
+  }
   return bytes;
 }
 
@@ -227,6 +240,15 @@ int job_alloc(cpsz_b200_ctx* ctx, Job2D& j) {
   d.bits[2] = (uint32_t*)A(j.codes_bits_cap);
   d.blob = (uint8_t*)A(j.blob_cap);
   if (!d.blob) return set_error(CPSZ_ERR_NOMEM, "workspace layout overflow");
+  if (j.log_form) {
+    d.logs[0] = (float*)A(4 * N);
+    d.logs[1] = (float*)A(4 * N);
+    d.signs[0] = (uint32_t*)A(4 * ((N + 31) / 32));
+    d.signs[1] = (uint32_t*)A(4 * ((N + 31) / 32));
+    if (!d.signs[1]) return set_error(CPSZ_ERR_NOMEM, "workspace layout overflow");
+    j.d_signs[0] = d.signs[0];
+    j.d_signs[1] = d.signs[1];
+  }
   return CPSZ_OK;
 }
 
@@ -243,7 +265,7 @@ struct BlobLayout {
   struct Piece {
     size_t dst, src, n;
   };
-  size_t total = 0, bit_dst[3] = {0, 0, 0}, unpred_dst[2] = {0, 0};
+  size_t total = 0, bit_dst[3] = {0, 0, 0}, unpred_dst[2] = {0, 0}, sign_dst = 0, sign_bytes = 0;
   std::vector<uint8_t> small;
   std::vector<Piece> pieces;
 };
@@ -255,8 +277,10 @@ int job_layout(const Job2D& j, BlobLayout& L) {
   const size_t ind_bytes = (j.nblocks + 7) / 8;
   size_t field_size[2];
   for (int f = 0; f < 2; f++) field_size[f] = FIELD_HDR + 4 * j.n_unpred[f] + ind_bytes + j.sec_bytes[1 + f];
-  const size_t total = BLOB_HDR + j.sec_bytes[0] + field_size[0] + field_size[1];
+  const size_t sign_bytes = j.log_form ? (j.N - 1) / 8 + 1 : 0;
+  const size_t total = BLOB_HDR + j.sec_bytes[0] + 2 * sign_bytes + field_size[0] + field_size[1];
   L.total = total;
+  L.sign_bytes = sign_bytes;
   std::vector<uint8_t>& small = L.small;
   auto stage = [&](size_t dst, const void* p, size_t n) {
     L.pieces.push_back(BlobLayout::Piece{dst, small.size(), n});
@@ -264,7 +288,7 @@ int job_layout(const Job2D& j, BlobLayout& L) {
   };
   {
     uint8_t hdr[BLOB_HDR];
-    const int base = 4;
+    const int base = j.log_form ? 2 : 4;
     const double thr = DBL_EPSILON;
     memcpy(hdr, &base, 4);
     memcpy(hdr + 4, &thr, 8);
@@ -286,6 +310,8 @@ int job_layout(const Job2D& j, BlobLayout& L) {
     at += j.bits_bytes[k];
   };
   stage_huff(0);
+  L.sign_dst = at;  // offline_log: sign maps of U and V (copied from the device)
+  at += 2 * sign_bytes;
   std::vector<uint8_t> zeros(ind_bytes, 0);
   for (int f = 0; f < 2; f++) {
     uint8_t fh[FIELD_HDR];
@@ -336,6 +362,9 @@ int job_assemble(cpsz_b200_ctx* ctx, Job2D& j) {
     if (j.n_unpred[f])
       CPSZ_CUDA_TRY(
           cudaMemcpyAsync(blob + unpred_dst[f], j.d.unpred[f], 4 * j.n_unpred[f], cudaMemcpyDeviceToDevice, st));
+  for (int f = 0; f < 2 && L.sign_bytes; f++)
+    CPSZ_CUDA_TRY(cudaMemcpyAsync(blob + L.sign_dst + f * L.sign_bytes, j.d_signs[f], L.sign_bytes,
+                                  cudaMemcpyDeviceToDevice, st));
   j.size = total;
   return CPSZ_OK;
 }
@@ -344,7 +373,11 @@ int job_assemble(cpsz_b200_ctx* ctx, Job2D& j) {
 int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) {
   cudaStream_t st = ctx->stream;
   const int nj = (int)jobs.size();
-  const QuantTable& qt = quant_table_2d();
+  // the offline_log form runs as a pass of one field
+  const bool log_form = nj == 1 && jobs[0].log_form;
+  const QuantTable& qt = log_form ? quant_table_2d_log() : quant_table_2d();
+  LibmTables libm{};
+  if (log_form) CPSZ_TRY(libm_tables_device(ctx, &libm));
   // pass-wide device pieces
   double* thr_tab = (double*)arena_alloc(ctx, QUANT_TAB_MAX * 8);
   int* queue = (int*)arena_alloc(ctx, 64);
@@ -352,7 +385,9 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   int total_groups = 0;
   for (const Job2D& j : jobs) total_groups += j.ngroups;
   WaveItem* d_items = (WaveItem*)arena_alloc(ctx, 2 * (size_t)total_groups * sizeof(WaveItem));
-  if (!d_items) return set_error(CPSZ_ERR_NOMEM, "workspace layout overflow");
+  // per upload band, the bound kernel's CTA placement and tile counter (overlap only)
+  unsigned int* sched = (unsigned int*)arena_alloc(ctx, SCHED_BYTES);
+  if (!d_items || !sched) return set_error(CPSZ_ERR_NOMEM, "workspace layout overflow");
   for (Job2D& j : jobs) CPSZ_TRY(job_alloc(ctx, j));
   for (int k = 0; k < nj; k++) {
     uint8_t* base = (uint8_t*)ctx->pinned + PINNED_BASE + (size_t)k * JOB_PINNED;
@@ -368,7 +403,8 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   // are group-major across fields while eb2d finishes field after field, so a
   // batch (and given bounds, quant2d, which are not row-ordered) runs the
   // wavefront after the bounds with every CTA slot.
-  const bool overlap = nj == 1 && jobs[0].eb_ext == nullptr && tune_get(TUNE_WAVE2D_OVERLAP, jobs[0].N) != 0;
+  const bool overlap =
+      nj == 1 && jobs[0].eb_ext == nullptr && !log_form && tune_get(TUNE_WAVE2D_OVERLAP, jobs[0].N) != 0;
 
   // ---- setup: flags, tables, wavefront descriptors ----
   reset_marks(ctx);
@@ -389,7 +425,10 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     for (int f = 0; f < 2; f++)
       CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.gbnd + ((size_t)f * j.ngroups + g0) * j.r2, 0,
                                     (size_t)(j.ngroups - g0) * j.r2 * 8, st));
-    if (overlap) CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.band, 0, (size_t)j.ngroups * 8, st));
+    if (overlap) {
+      CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.band, 0, (size_t)j.ngroups * 8, st));
+      CPSZ_CUDA_TRY(cudaMemsetAsync(sched, 0, SCHED_BYTES, st));
+    }
     for (int f = 0; f < 2; f++) {
       WaveField& F = hf[2 * k + f];
       F.pair = j.d.pairs[f];
@@ -466,7 +505,18 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     }
     for (Job2D& j : jobs) {
       unsigned long long* band = overlap ? j.d.band : nullptr;
-      if (j.dev_in) {
+      if (j.log_form) {
+        // offline_log: the fields whole, one id per vertex, then the logs,
+        // wavefront pairs and sign maps
+        if (!j.dev_in) {
+          CPSZ_TRY(h2d(ctx, j.d.U, j.U_in, 4 * j.N, st));
+          CPSZ_TRY(h2d(ctx, j.d.V, j.V_in, 4 * j.N, st));
+        }
+        CPSZ_TRY(launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, nullptr, j.d.hist_ids,
+                             nullptr, nullptr, nullptr, 0, -1, nullptr, true));
+        CPSZ_TRY(launch_log2d(ctx, j.d.U, j.d.V, j.d.ids, j.N, libm.log2f, j.d.pairs[0], j.d.pairs[1], j.d.logs[0],
+                              j.d.logs[1], j.d.signs[0], j.d.signs[1]));
+      } else if (j.dev_in) {
         if (j.eb_ext && nj == 1 && tap && tap->recon_only && tap->requant)
           CPSZ_TRY(launch_requant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
                                     j.d.pairs[0], j.d.pairs[1], tap->requant));
@@ -475,7 +525,8 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
                                   j.d.hist_ids, j.d.pairs[0], j.d.pairs[1]));
         else
           CPSZ_TRY(launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
-                               j.d.hist_ids, j.d.pairs[0], j.d.pairs[1], nullptr, 0, -1, band));
+                               j.d.hist_ids, j.d.pairs[0], j.d.pairs[1], nullptr, 0, -1, band, false,
+                               overlap ? sched : nullptr));
       } else {
         // Host input: row chunks go up on the second stream and the bound kernel
         // runs band by band as soon as a band's rows and the row below it are
@@ -497,7 +548,8 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
             return launch_quant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
                                   j.d.hist_ids, j.d.pairs[0], j.d.pairs[1]);
           return launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N, j.d.hist_ids,
-                             j.d.pairs[0], j.d.pairs[1], nullptr, c * R, std::min(j.r1, (c + 1) * R), band);
+                             j.d.pairs[0], j.d.pairs[1], nullptr, c * R, std::min(j.r1, (c + 1) * R), band, false,
+                             overlap ? sched + (size_t)c * EB2D_SCHED_WORDS : nullptr);
         };
         for (int c = 0; c < nch; c++) {
           const size_t off = (size_t)c * R * j.r2;
@@ -550,7 +602,7 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     }
     for (int k = 0; k < nj; k++) {
       Job2D& j = jobs[k];
-      const float* x[2] = {j.d.U, j.d.V};
+      const float* x[2] = {j.log_form ? j.d.logs[0] : j.d.U, j.log_form ? j.d.logs[1] : j.d.V};
       CPSZ_TRY(launch_strip_pass(ctx, j.d.craster, j.r2, x, j.r2, j.r1, j.r2, j.d.cblocks, j.d.unpred, j.d.strip));
       for (int f = 0; f < 2; f++)
         CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_nunpred + f, strip_total(j.d.strip[f], j.r1, j.r2), 4,
@@ -660,7 +712,8 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.enc_code[0], j.cb[0].code.data(), 256 * 8, cudaMemcpyHostToDevice, st));
     CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.enc_len[0], j.cb[0].len.data(), 256, cudaMemcpyHostToDevice, st));
     CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.bits[0], 0, align_up(j.bits_bytes[0], 4) + 8, st));
-    CPSZ_TRY(launch_huff_encode_u8(ctx, j.d.ids, 2 * j.N, true, HuffEncTable{j.d.enc_code[0], j.d.enc_len[0], 256},
+    CPSZ_TRY(launch_huff_encode_u8(ctx, j.d.ids, j.log_form ? j.N : 2 * j.N, true,
+                                   HuffEncTable{j.d.enc_code[0], j.d.enc_len[0], 256},
                                    j.d.bits[0], j.ids_bits_cap, nullptr, j.d.enc_tmp[0]));
   }
   if (h_async) {
@@ -722,8 +775,11 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       return set_error(CPSZ_ERR_INVALID, "output capacity %zu < blob size %zu", hj->host_cap, hl.total);
     for (const BlobLayout::Piece& pc : hl.pieces) memcpy(hj->host_out + pc.dst, hl.small.data() + pc.src, pc.n);
     if (h_async)
-      for (int f = 0; f < 2; f++)
+      for (int f = 0; f < 2; f++) {
         CPSZ_TRY(d2h_beside(hj->host_out + hl.unpred_dst[f], hj->d.unpred[f], 4 * hj->n_unpred[f]));
+        if (hl.sign_bytes)
+          CPSZ_TRY(d2h_beside(hj->host_out + hl.sign_dst + f * hl.sign_bytes, hj->d_signs[f], hl.sign_bytes));
+      }
   }
   for (Job2D& j : jobs) {
     for (int k = 1; k < 3; k++) {
@@ -762,8 +818,11 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   if (hj) {
     if (!h_async) {
       CPSZ_TRY(d2h(ctx, hj->host_out + hl.bit_dst[0], hj->d.bits[0], hj->bits_bytes[0], st));
-      for (int f = 0; f < 2; f++)
+      for (int f = 0; f < 2; f++) {
         CPSZ_TRY(d2h(ctx, hj->host_out + hl.unpred_dst[f], hj->d.unpred[f], 4 * hj->n_unpred[f], st));
+        if (hl.sign_bytes)
+          CPSZ_TRY(d2h(ctx, hj->host_out + hl.sign_dst + f * hl.sign_bytes, hj->d_signs[f], hl.sign_bytes, st));
+      }
       for (int k = 1; k < 3; k++) CPSZ_TRY(d2h(ctx, hj->host_out + hl.bit_dst[k], hj->d.bits[k], hj->bits_bytes[k], st));
     }
     hj->size = hl.total;
@@ -790,7 +849,7 @@ size_t pass_bytes(const std::vector<Job2D>& jobs) {
     total_groups += j.ngroups;
   }
   bytes += align_up(QUANT_TAB_MAX * 8, 256) + 256 + 512 + align_up(2 * jobs.size() * sizeof(WaveField), 256) + 256 +
-           align_up(2 * (size_t)total_groups * sizeof(WaveItem), 256) + 256;
+           align_up(2 * (size_t)total_groups * sizeof(WaveItem), 256) + 256 + align_up(SCHED_BYTES, 256) + 256;
   return bytes;
 }
 
@@ -807,9 +866,13 @@ int build_wave_items(int nfields, const int* r1s, std::vector<WaveItem>& items) 
 }
 
 int compress_2d(cpsz_b200_ctx* ctx, const float* U_in, const float* V_in, size_t r1s, size_t r2s, double max_pwr_eb,
-                Blob2D* out, const StageTap* tap, const double* eb_ext, unsigned char* host_out, size_t host_cap) {
+                Blob2D* out, const StageTap* tap, const double* eb_ext, unsigned char* host_out, size_t host_cap,
+                bool log_form) {
+  if (log_form && (tap || eb_ext))
+    return set_error(CPSZ_ERR_INVALID, "the offline_log form takes neither stage taps nor given bounds");
   std::vector<Job2D> jobs(1);
   CPSZ_TRY(job_init(jobs[0], U_in, V_in, r1s, r2s, max_pwr_eb));
+  jobs[0].log_form = log_form;
   jobs[0].eb_ext = eb_ext;
   jobs[0].host_out = host_out;
   jobs[0].host_cap = host_cap;
@@ -902,7 +965,7 @@ int parse_field(const unsigned char* blob, size_t off, size_t size, size_t N, si
 }  // namespace
 
 int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_size, size_t r1s, size_t r2s, float* U_out,
-                  float* V_out) {
+                  float* V_out, bool log_form) {
   if (!blob || !U_out || !V_out) return set_error(CPSZ_ERR_INVALID, "null pointer argument");
   if (r1s == 0 || r2s == 0) return set_error(CPSZ_ERR_INVALID, "empty field");
   if (r1s > (1u << 30) || r2s > (1u << 30) || r1s * r2s > (size_t)INT32_MAX)
@@ -921,11 +984,17 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
   memcpy(&eb_size, blob + 12, 8);
   memcpy(&u_size, blob + 20, 8);
   memcpy(&v_size, blob + 28, 8);
-  if (base != 4 || thr != DBL_EPSILON)
-    return set_error(CPSZ_ERR_UNSUPPORTED, "blob quantizer (base %d, thr %g) is not the offline compressor's", base, thr);
+  if (base != (log_form ? 2 : 4) || thr != DBL_EPSILON)
+    return set_error(CPSZ_ERR_UNSUPPORTED, "blob quantizer (base %d, thr %g) is not the offline%s compressor's", base,
+                     thr, log_form ? "_log" : "");
+  // offline_log: the sign maps of U and V follow the id section
+  const size_t sign_bytes = log_form ? (N - 1) / 8 + 1 : 0;
   const size_t avail = blob_size - BLOB_HDR;
-  if (eb_size > avail || u_size > avail - eb_size || v_size > avail - eb_size - u_size)
+  if (eb_size > avail || 2 * sign_bytes > avail - eb_size || u_size > avail - eb_size - 2 * sign_bytes ||
+      v_size > avail - eb_size - 2 * sign_bytes - u_size)
     return set_error(CPSZ_ERR_FORMAT, "section sizes exceed the blob");
+  const size_t fields_at = BLOB_HDR + eb_size + 2 * sign_bytes;
+  const size_t n_ids = log_form ? N : 2 * N;
   HuffDecoderHost hid;
   if (!huff_parse(blob + BLOB_HDR, eb_size, 2047, &hid)) return CPSZ_ERR_FORMAT;
   if (hid.section_bytes > eb_size) return set_error(CPSZ_ERR_FORMAT, "id section overruns");
@@ -933,8 +1002,10 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
     if (s > (uint32_t)ID_MAX_2D)
       return set_error(CPSZ_ERR_UNSUPPORTED, "error-bound id %u beyond the supported range (<= %d)", s, ID_MAX_2D);
   FieldView fv[2];
-  CPSZ_TRY(parse_field(blob, BLOB_HDR + eb_size, u_size, N, nblocks, &fv[0]));
-  CPSZ_TRY(parse_field(blob, BLOB_HDR + eb_size + u_size, v_size, N, nblocks, &fv[1]));
+  CPSZ_TRY(parse_field(blob, fields_at, u_size, N, nblocks, &fv[0]));
+  CPSZ_TRY(parse_field(blob, fields_at + u_size, v_size, N, nblocks, &fv[1]));
+  LibmTables libm{};
+  if (log_form) CPSZ_TRY(libm_tables_device(ctx, &libm));
   const bool dev_out = is_device_ptr(U_out) && is_device_ptr(V_out);
 
   // ---- workspace ----
@@ -942,7 +1013,8 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
   size_t bytes = 0;
   auto add = [&](size_t b) { bytes += align_up(b, 256) + 256; };
   if (!dev_out) add(8 * N);
-  add(2 * N);  // ids
+  add(n_ids);  // ids
+  add(2 * sign_bytes + 16);
   for (int k = 0; k < 3; k++) {
     add(hs[k]->nbytes + 64);
     add((1u << HUFF_LUT_BITS) * 4 + hs[k]->child.size() * 4 + hs[k]->sym.size() * 4 + hs[k]->leaf.size());
@@ -962,7 +1034,9 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
   cudaStream_t st = ctx->stream;
   float* dU = dev_out ? U_out : (float*)A(4 * N);
   float* dV = dev_out ? V_out : (float*)A(4 * N);
-  uint8_t* ids = (uint8_t*)A(2 * N);
+  uint8_t* ids = (uint8_t*)A(n_ids);
+  uint8_t* signs = (uint8_t*)A(2 * sign_bytes + 16);
+  if (sign_bytes) CPSZ_TRY(h2d(ctx, signs, blob + BLOB_HDR + eb_size, 2 * sign_bytes, st));
   uint8_t* bits[3];
   HuffDecTable tab[3];
   void* dtmp[3];
@@ -1007,7 +1081,7 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
   mark(ctx, "huffman_decode");
 
   // ---- Huffman decode ----
-  CPSZ_TRY(launch_huff_decode(ctx, bits[0], hid.nbytes, 2 * N, tab[0], ids, 1, dtmp[0]));
+  CPSZ_TRY(launch_huff_decode(ctx, bits[0], hid.nbytes, n_ids, tab[0], ids, 1, dtmp[0]));
   for (int f = 0; f < 2; f++)
     CPSZ_TRY(launch_huff_decode(ctx, bits[1 + f], fv[f].huff.nbytes, N, tab[1 + f], cblocks[f], 2, dtmp[1 + f]));
   // ---- raster pairs, unpredictable scatter ----
@@ -1015,10 +1089,11 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
   unsigned int* h_cnt = (unsigned int*)ctx->pinned + 16;
   {
     const uint16_t* cb[2] = {cblocks[0], cblocks[1]};
-    const uint8_t* idf[2] = {ids, ids + N};
+    // offline_log: one id stream for both components, base 2
+    const uint8_t* idf[2] = {ids, log_form ? ids : ids + N};
     const float* un[2] = {unpred[0], unpred[1]};
     const unsigned long long nun[2] = {fv[0].n_unpred, fv[1].n_unpred};
-    CPSZ_TRY(launch_strip_unpass(ctx, cb, idf, un, nun, r1, r2, raw, strip));
+    CPSZ_TRY(launch_strip_unpass(ctx, cb, idf, un, nun, r1, r2, raw, strip, log_form ? 1 : 2));
     for (int f = 0; f < 2; f++)
       CPSZ_CUDA_TRY(cudaMemcpyAsync(h_cnt + f, strip_total(strip[f], r1, r2), 4, cudaMemcpyDeviceToHost, st));
   }
@@ -1046,6 +1121,10 @@ int decompress_2d(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_siz
   CPSZ_CUDA_TRY(cudaMemsetAsync(queue, 0, 64, st));
   mark(ctx, "wave2d_decompress");
   CPSZ_TRY(launch_wave2d(ctx, true, dfields, ditems, n_items, queue, (size_t)r1 * r2));
+  if (log_form) {
+    mark(ctx, "exp2d");
+    CPSZ_TRY(launch_exp2d(ctx, dU, dV, signs, signs + sign_bytes, N, libm.exp2f));
+  }
   mark(ctx, "d2h");
   if (!dev_out) {
     CPSZ_TRY(d2h(ctx, U_out, dU, 4 * N, st));

@@ -63,6 +63,16 @@ static int id_3d(double r) {
   return (int)(log2(abs_eb / thr) / log2(2.0));
 }
 
+// id of the 2D offline_log quantizer for a relative bound r
+// (src/sz_compress_cp_preserve_2d.cpp:345-350: log2(1 + r), base 2, thr =
+// DBL_EPSILON); 0 at or below the threshold.
+static int id_2d_log(double r) {
+  const double thr = DBL_EPSILON;
+  const double e = log2(1 + r);
+  if (e <= thr) return 0;
+  return (int)(log2(e / thr) / log2(2.0));
+}
+
 // Smallest positive double x in [lo, hi] with f(x) >= k, by bisection on the
 // (monotone) bit patterns of positive doubles.
 template <class F>
@@ -110,6 +120,20 @@ const QuantTable& quant_table_2d() {
     // e ranges over |U| * eb; the upper end keeps e / thr finite (ids beyond
     // the table's 255 are rejected by the kernel anyway).
     build_table(T, id_2d, DBL_EPSILON, 1e280);
+  });
+  return T;
+}
+
+const QuantTable& quant_table_2d_log() {
+  static QuantTable T;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    T.thr = DBL_EPSILON;
+    T.base = 2;
+    // t[0]: the largest r whose log-domain bound log2(1 + r) is still <= thr
+    // (precision 0); ids count thresholds above it
+    const double first = first_at_least([](double r) { return log2(1 + r) > DBL_EPSILON ? 1 : 0; }, 1, DBL_MIN, 1.0);
+    build_table(T, id_2d_log, bitsd(dbits(first) - 1), 1e300);
   });
   return T;
 }
@@ -266,6 +290,7 @@ int cpsz_b200_ctx_create(int device, cpsz_b200_ctx** out) {
   CPSZ_CUDA_TRY(cudaMemset(c->d_flag, 0, 64));
   // Tables are built once per process, before any stream capture.
   (void)quant_table_2d();
+  (void)quant_table_2d_log();
   (void)quant_table_3d();
   *out = c;
   return CPSZ_OK;

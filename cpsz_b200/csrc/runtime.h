@@ -54,6 +54,9 @@ struct QuantTable {
 };
 // 2D: base 4, thr = DBL_EPSILON, applied to e = |U| * eb.
 const QuantTable& quant_table_2d();
+// 2D offline_log: id of log2(1 + eb) with base 2, thr = DBL_EPSILON, over the
+// relative bound eb directly; t[0] is the largest eb with precision 0.
+const QuantTable& quant_table_2d_log();
 // 3D: id of abs_eb = log2(1 + required_eb) with base 2, thr = FLT_EPSILON;
 // thresholds are over required_eb directly (log2(1+x) folded in).
 const QuantTable& quant_table_3d();

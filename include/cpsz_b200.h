@@ -111,6 +111,26 @@ int cpsz_b200_compress_2d_offline_f32_into(cpsz_b200_ctx* ctx, const float* U, c
 int cpsz_b200_decompress_2d_offline_f32(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_size, size_t r1,
                                         size_t r2, float* U, float* V);
 
+/* ---- 2D offline_log CP-preserving compression ----------------------------
+ * Replaces sz_compress_cp_preserve_2d_offline_log<float>
+ * (reference include/sz_compress_cp_preserve_2d.hpp:14,
+ *  src/sz_compress_cp_preserve_2d.cpp:285-379): the offline per-vertex bound
+ * taken to the log domain (log2(1 + eb), base 2, one id stream), U and V
+ * compressed as log2f|x| with their sign maps.  Same arguments and output
+ * conventions as cpsz_b200_compress_2d_offline_f32 / _into. */
+int cpsz_b200_compress_2d_offline_log_f32(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2,
+                                          double max_pwr_eb, unsigned char** blob, size_t* blob_size);
+int cpsz_b200_compress_2d_offline_log_f32_into(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1,
+                                               size_t r2, double max_pwr_eb, unsigned char* out, size_t out_cap,
+                                               size_t* blob_size);
+/* Replaces sz_decompress_cp_preserve_2d_offline_log<float>
+ * (reference include/sz_decompress_cp_preserve_2d.hpp:15,
+ *  src/sz_decompress_cp_preserve_2d.cpp:56-99). */
+int cpsz_b200_decompress_2d_offline_log_f32(cpsz_b200_ctx* ctx, const unsigned char* blob, size_t blob_size,
+                                            size_t r1, size_t r2, float* U, float* V);
+/* Size of a 2D offline_log blob of an r1 x r2 field from its header. */
+size_t cpsz_b200_blob_size_2d_log(const unsigned char* blob, size_t r1, size_t r2);
+
 /* ---- batched 2D compression (many independent fields) ----------------------
  * Compresses n_fields fields in passes of up to 32 fields: every kernel stage
  * runs for all fields of a pass, the Lorenzo wavefront is one persistent
@@ -296,8 +316,9 @@ int cpsz_b200_debug_wave_trace(cpsz_b200_ctx* ctx, size_t len, long long* out);
  * sqrt.approx.f32 (relative, positive normal floats); out[5 + e + 126]
  * lg2.approx.ftz.f32 (absolute) on [2^e, 2^(e+1)), e = -126..0.  n >= 132. */
 int cpsz_b200_debug_filter_premises(cpsz_b200_ctx* ctx, double* out, size_t n);
-/* Host-computed quantization thresholds (which = 2 or 3): t[k] is the smallest
- * bound with id >= k under the host libm's log2 (256 doubles). */
+/* Host-computed quantization thresholds (which = 2: 2D offline, 1: 2D
+ * offline_log, 3: 3D): t[k] is the smallest bound with id >= k under the host
+ * libm's log2 (256 doubles); t[0] is the largest bound quantized to precision 0. */
 int cpsz_b200_debug_quant_table(int which, double* t, int* n);
 
 /* ---- exact critical-point checker -----------------------------------------
@@ -327,6 +348,18 @@ int cpsz_b200_generate_field_3d(uint64_t seed, size_t r1, size_t r2, size_t r3, 
                                 double noise_std, float* U, float* V, float* W);
 int cpsz_b200_batch_layout(uint64_t base_seed, int n_fields, int lo, int hi, size_t* r1, size_t* r2, uint64_t* seeds,
                            double* ebs);
+
+/* ---- GPU lossless stage ----------------------------------------------------
+ * Replaces the reference's host ZSTD stage (sz_lossless_compress,
+ * src/sz_lossless.cpp:11-26) on the GPU: `in` (n bytes, host or device) becomes
+ * a standard Zstandard frame at `out` (host or device, out_cap bytes; at most
+ * cpsz_b200_lossless_bound(n)), which ZSTD_decompress -- and so the
+ * reference's sz_lossless_decompress -- reads back.  32 KB blocks encoded
+ * independently (greedy matches within the block, raw literals, sequences
+ * with the predefined FSE tables); the frame is larger than ZSTD level 3's. */
+size_t cpsz_b200_lossless_bound(size_t n);
+int cpsz_b200_lossless_compress(cpsz_b200_ctx* ctx, const unsigned char* in, size_t n, unsigned char* out,
+                                size_t out_cap, size_t* out_size);
 
 /* ---- host lossless stage (ZSTD level 3, as src/sz_lossless.cpp:11-26) ---- */
 int cpsz_b200_zstd_compress(const unsigned char* data, size_t n, int level, unsigned char** out, size_t* out_size);

@@ -23,6 +23,16 @@ unsigned char* sz_compress_cp_preserve_2d_offline(const T* U, const T* V, size_t
 template <typename T>
 void sz_decompress_cp_preserve_2d_offline(const unsigned char* compressed, size_t r1, size_t r2, T*& U, T*& V);
 
+// include/sz_compress_cp_preserve_2d.hpp:14 (reference)
+template <typename T>
+unsigned char* sz_compress_cp_preserve_2d_offline_log(const T* U, const T* V, size_t r1, size_t r2,
+                                                      size_t& compressed_size, bool transpose = false,
+                                                      double max_pwr_eb = 0.1);
+
+// include/sz_decompress_cp_preserve_2d.hpp:15 (reference)
+template <typename T>
+void sz_decompress_cp_preserve_2d_offline_log(const unsigned char* compressed, size_t r1, size_t r2, T*& U, T*& V);
+
 // include/sz_compress_cp_preserve_3d.hpp:8 (reference)
 template <typename T>
 unsigned char* sz_compress_cp_preserve_3d_offline_log(const T* U, const T* V, const T* W, size_t r1, size_t r2,

@@ -68,6 +68,9 @@ class Oracle:
         L.cpo_compress_2d_offline.argtypes = [_f32p, _f32p, _sz, _sz, C.c_double, C.POINTER(_sz)]
         L.cpo_compress_2d_offline.restype = C.c_void_p
         L.cpo_decompress_2d_offline.argtypes = [C.c_char_p, _sz, _sz, _sz, _f32p, _f32p]
+        L.cpo_compress_2d_offline_log.argtypes = [_f32p, _f32p, _sz, _sz, C.c_double, C.POINTER(_sz)]
+        L.cpo_compress_2d_offline_log.restype = C.c_void_p
+        L.cpo_decompress_2d_offline_log.argtypes = [C.c_char_p, _sz, _sz, _sz, _f32p, _f32p]
         L.cpo_huffman_encode.argtypes = [_sz, _i32p, _sz, C.c_void_p]
         L.cpo_huffman_encode.restype = _sz
         L.cpo_huffman_encode_bound.argtypes = [_sz, _sz]
@@ -151,6 +154,20 @@ class Oracle:
             raise ValueError(f"oracle: malformed 2D blob (code {rc})")
         return U, V
 
+    def compress_2d_log(self, U, V, eb) -> bytes:
+        r1, r2 = U.shape
+        sz = _sz()
+        p = self.lib.cpo_compress_2d_offline_log(_c(U), _c(V), r1, r2, eb, C.byref(sz))
+        return _take_blob(self.lib, p, sz.value)
+
+    def decompress_2d_log(self, blob: bytes, r1, r2):
+        U = np.empty((r1, r2), np.float32)
+        V = np.empty((r1, r2), np.float32)
+        rc = self.lib.cpo_decompress_2d_offline_log(blob, len(blob), r1, r2, U, V)
+        if rc:
+            raise ValueError(f"oracle: malformed 2D log blob (code {rc})")
+        return U, V
+
     def huffman_encode(self, state_num, sym) -> bytes:
         sym = np.ascontiguousarray(sym, np.int32)
         cap = self.lib.cpo_huffman_encode_bound(state_num, sym.size)
@@ -212,6 +229,9 @@ class Reference:
         L.cpsz_ref_compress_2d_offline_f32.argtypes = [_f32p, _f32p, _sz, _sz, C.c_double, C.POINTER(_sz)]
         L.cpsz_ref_compress_2d_offline_f32.restype = C.c_void_p
         L.cpsz_ref_decompress_2d_offline_f32.argtypes = [C.c_char_p, _sz, _sz, _f32p, _f32p]
+        L.cpsz_ref_compress_2d_offline_log_f32.argtypes = [_f32p, _f32p, _sz, _sz, C.c_double, C.POINTER(_sz)]
+        L.cpsz_ref_compress_2d_offline_log_f32.restype = C.c_void_p
+        L.cpsz_ref_decompress_2d_offline_log_f32.argtypes = [C.c_char_p, _sz, _sz, _f32p, _f32p]
         L.cpsz_ref_compress_3d_offline_log_f32.argtypes = [_f32p, _f32p, _f32p, _sz, _sz, _sz, C.c_double, C.POINTER(_sz)]
         L.cpsz_ref_compress_3d_offline_log_f32.restype = C.c_void_p
         L.cpsz_ref_decompress_3d_online_log_f32.argtypes = [C.c_char_p, _sz, _sz, _sz, _f32p, _f32p, _f32p]
@@ -231,6 +251,18 @@ class Reference:
         U = np.empty((r1, r2), np.float32)
         V = np.empty((r1, r2), np.float32)
         self.lib.cpsz_ref_decompress_2d_offline_f32(blob, r1, r2, U, V)
+        return U, V
+
+    def compress_2d_log(self, U, V, eb) -> bytes:
+        r1, r2 = U.shape
+        sz = _sz()
+        p = self.lib.cpsz_ref_compress_2d_offline_log_f32(_c(U), _c(V), r1, r2, eb, C.byref(sz))
+        return _take_blob(self.lib, p, sz.value)
+
+    def decompress_2d_log(self, blob: bytes, r1, r2):
+        U = np.empty((r1, r2), np.float32)
+        V = np.empty((r1, r2), np.float32)
+        self.lib.cpsz_ref_decompress_2d_offline_log_f32(blob, r1, r2, U, V)
         return U, V
 
     def compress_3d(self, U, V, W, eb) -> bytes:
@@ -278,6 +310,17 @@ def ref_2d_in_bounds(oracle_blob: bytes, r1: int, r2: int) -> bool:
     eb_size, u_size, v_size = struct.unpack_from("<QQQ", oracle_blob, 12)
     est = int(n * 4 * 1.2)
     return u_size + 16 <= est and v_size + 16 <= est and eb_size + 16 <= 2 * n * 4
+
+
+def ref_2d_log_in_bounds(oracle_blob: bytes, r1: int, r2: int) -> bool:
+    """The offline_log form: the id section goes into N*sizeof(int) bytes
+    (src/sz_compress_cp_preserve_2d.cpp:352) and each field blob into
+    (size_t)(N*sizeof(float)*1.2) bytes, each plus the packer's write-ahead."""
+    import struct
+    n = r1 * r2
+    eb_size, u_size, v_size = struct.unpack_from("<QQQ", oracle_blob, 12)
+    est = int(n * 4 * 1.2)
+    return u_size + 16 <= est and v_size + 16 <= est and eb_size + 16 <= n * 4
 
 
 def ref_3d_in_bounds(oracle_blob: bytes, r1: int, r2: int, r3: int) -> bool:

@@ -444,6 +444,132 @@ int cpo_decompress_2d_offline(const unsigned char* blob, size_t blob_size, size_
   return rc;
 }
 
+/* ---- 2D offline_log pair ---------------------------------------------------- */
+
+/* convertIntArray2ByteArray_fast_1b_to_result_sz: src/sz_compression_utils.cpp:31-52
+ * (bit 7 - j of byte b holds element 8b + j). */
+static void pack_bits_2d(const unsigned char* bits, size_t n, unsigned char* out) {
+  size_t nb = (n % 8 == 0) ? n / 8 : n / 8 + 1;
+  for (size_t b = 0; b < nb; b++) {
+    int tmp = 0;
+    for (size_t j = 0; j < 8 && b * 8 + j < n; j++)
+      if (bits[b * 8 + j] == 1) tmp |= 1 << (7 - j);
+    out[b] = (unsigned char)tmp;
+  }
+}
+
+/* log_transform: include/sz_cp_preserve_utils.hpp:205-221 (log2f of |x|, -100 for 0,
+ * sign = x > 0). */
+static float* log_transform_2d(const float* data, unsigned char* sign, size_t n) {
+  float* out = (float*)malloc(n * sizeof(float));
+  for (size_t i = 0; i < n; i++) {
+    sign[i] = 0;
+    if (data[i] != 0) {
+      sign[i] = (data[i] > 0);
+      out[i] = (data[i] > 0) ? log2f(data[i]) : log2f(-data[i]);
+    } else {
+      out[i] = -100;
+    }
+  }
+  return out;
+}
+
+/* sz_compress_cp_preserve_2d_offline_log<float>: src/sz_compress_cp_preserve_2d.cpp:285-379.
+ * The per-vertex bound is the offline one; it is taken to the log domain as
+ * log2(1 + eb) and quantized with base 2 and threshold DBL_EPSILON (one id
+ * stream for both components); U and V are compressed as log2f values. */
+unsigned char* cpo_compress_2d_offline_log(const float* U, const float* V, size_t r1, size_t r2, double max_pwr_eb,
+                                           size_t* size) {
+  size_t n = r1 * r2;
+  double* eb = (double*)malloc(n * sizeof(double));
+  cpo_eb_2d(U, V, r1, r2, max_pwr_eb, eb);
+  size_t smap = (n - 1) / 8 + 1;
+  unsigned char* signs = (unsigned char*)malloc(2 * smap);
+  unsigned char* sign = (unsigned char*)malloc(n);
+  float* log_u = log_transform_2d(U, sign, n);
+  pack_bits_2d(sign, n, signs);
+  float* log_v = log_transform_2d(V, sign, n);
+  pack_bits_2d(sign, n, signs + smap);
+  free(sign);
+  int* ids = (int*)malloc(n * sizeof(int));
+  const int base = 2;
+  const double log2_of_base = log2(base);
+  const double threshold = DBL_EPSILON;
+  for (size_t i = 0; i < n; i++) {
+    eb[i] = log2(1 + eb[i]);
+    ids[i] = eb_exp_quantize(&eb[i], base, log2_of_base, threshold);
+  }
+  unsigned char* ceb = (unsigned char*)calloc(cpo_huffman_encode_bound(2 * 1024, n), 1);
+  size_t ceb_size = cpo_huffman_encode(2 * 1024, ids, n, ceb);
+  free(ids);
+  size_t cu_size = 0, cv_size = 0;
+  unsigned char* cu = cpo_compress_2d_with_eb(log_u, eb, r1, r2, &cu_size);
+  free(log_u);
+  unsigned char* cv = cpo_compress_2d_with_eb(log_v, eb, r1, r2, &cv_size);
+  free(log_v);
+  free(eb);
+  size_t total = sizeof(int) + sizeof(double) + 3 * sizeof(size_t) + ceb_size + 2 * smap + cu_size + cv_size;
+  unsigned char* out = (unsigned char*)malloc(total);
+  unsigned char* p = out;
+  put_bytes(&p, &base, sizeof(int));
+  put_bytes(&p, &threshold, sizeof(double));
+  put_bytes(&p, &ceb_size, sizeof(size_t));
+  put_bytes(&p, &cu_size, sizeof(size_t));
+  put_bytes(&p, &cv_size, sizeof(size_t));
+  put_bytes(&p, ceb, ceb_size);
+  put_bytes(&p, signs, 2 * smap);
+  put_bytes(&p, cu, cu_size);
+  put_bytes(&p, cv, cv_size);
+  free(ceb);
+  free(signs);
+  free(cu);
+  free(cv);
+  *size = total;
+  return out;
+}
+
+/* sz_decompress_cp_preserve_2d_offline_log<float>: src/sz_decompress_cp_preserve_2d.cpp:56-99
+ * (exp2f of the decoded log values, -99 and below decode to 0). */
+int cpo_decompress_2d_offline_log(const unsigned char* blob, size_t blob_size, size_t r1, size_t r2, float* U,
+                                  float* V) {
+  const unsigned char* p = blob;
+  size_t n = r1 * r2, smap = (n - 1) / 8 + 1;
+  if (blob_size < 4 + 8 + 24) return 1;
+  int base;
+  double threshold;
+  size_t eb_size, u_size, v_size;
+  memcpy(&base, p, 4); p += 4;
+  memcpy(&threshold, p, 8); p += 8;
+  memcpy(&eb_size, p, 8); p += 8;
+  memcpy(&u_size, p, 8); p += 8;
+  memcpy(&v_size, p, 8); p += 8;
+  size_t hdr = (size_t)(p - blob);
+  if (eb_size > blob_size - hdr || 2 * smap > blob_size - hdr - eb_size ||
+      u_size > blob_size - hdr - eb_size - 2 * smap || v_size > blob_size - hdr - eb_size - 2 * smap - u_size)
+    return 2;
+  int* type = (int*)malloc(n * sizeof(int));
+  if (!cpo_huffman_decode(2 * 1024, n, p, eb_size, type)) { free(type); return 3; }
+  p += eb_size;
+  double* eb = (double*)malloc(n * sizeof(double));
+  for (size_t i = 0; i < n; i++) eb[i] = (type[i] == 0) ? 0 : pow(base, type[i]) * threshold;
+  free(type);
+  const unsigned char* su = p;
+  const unsigned char* sv = p + smap;
+  p += 2 * smap;
+  int rc = 0;
+  if (!decompress_2d_with_eb(p, u_size, eb, r1, r2, U)) rc = 4;
+  p += u_size;
+  if (!rc && !decompress_2d_with_eb(p, v_size, eb, r1, r2, V)) rc = 5;
+  free(eb);
+  if (rc) return rc;
+  for (size_t i = 0; i < n; i++) {
+    int bu = (su[i / 8] >> (7 - i % 8)) & 1, bv = (sv[i / 8] >> (7 - i % 8)) & 1;
+    U[i] = (U[i] < -99) ? 0 : (bu ? exp2f(U[i]) : -exp2f(U[i]));
+    V[i] = (V[i] < -99) ? 0 : (bv ? exp2f(V[i]) : -exp2f(V[i]));
+  }
+  return 0;
+}
+
 void cpo_free(void* p) { free(p); }
 
 /* The host C library's single-precision log2f / exp2f over arrays: the

@@ -50,6 +50,13 @@ unsigned char* cpo_compress_2d_offline(const float* U, const float* V, size_t r1
  * Returns 0 on success, nonzero on a malformed blob. */
 int cpo_decompress_2d_offline(const unsigned char* blob, size_t blob_size, size_t r1, size_t r2, float* U, float* V);
 
+/* sz_compress_cp_preserve_2d_offline_log<float> (src/sz_compress_cp_preserve_2d.cpp:285-379). */
+unsigned char* cpo_compress_2d_offline_log(const float* U, const float* V, size_t r1, size_t r2, double max_pwr_eb,
+                                           size_t* size);
+/* sz_decompress_cp_preserve_2d_offline_log<float> (src/sz_decompress_cp_preserve_2d.cpp:56-99). */
+int cpo_decompress_2d_offline_log(const unsigned char* blob, size_t blob_size, size_t r1, size_t r2, float* U,
+                                  float* V);
+
 /* ---- Huffman (SZ-1.x codec, src/sz_huffman.cpp) -------------------------- */
 
 /* Huffman_encode_tree_and_data (src/sz_compression_utils.cpp:62-82): writes

@@ -6,6 +6,8 @@
 // Wrapped entry points (reference file:line):
 //   sz_compress_cp_preserve_2d_offline     include/sz_compress_cp_preserve_2d.hpp:10
 //   sz_decompress_cp_preserve_2d_offline   include/sz_decompress_cp_preserve_2d.hpp:11
+//   sz_compress_cp_preserve_2d_offline_log include/sz_compress_cp_preserve_2d.hpp:14
+//   sz_decompress_cp_preserve_2d_offline_log include/sz_decompress_cp_preserve_2d.hpp:15
 //   sz_compress_cp_preserve_3d_offline_log include/sz_compress_cp_preserve_3d.hpp:8
 //   sz_decompress_cp_preserve_3d_online_log include/sz_decompress_cp_preserve_3d.hpp:11
 //   sz_lossless_compress / _decompress     include/sz_lossless.hpp:13-14
@@ -55,6 +57,28 @@ int cpsz_ref_decompress_2d_offline_f32(const unsigned char* blob, size_t r1, siz
   float* U = nullptr;
   float* V = nullptr;
   sz_decompress_cp_preserve_2d_offline<float>(blob, r1, r2, U, V);
+  memcpy(U_out, U, r1 * r2 * sizeof(float));
+  memcpy(V_out, V, r1 * r2 * sizeof(float));
+  free(U);
+  free(V);
+  return 0;
+}
+
+unsigned char* cpsz_ref_compress_2d_offline_log_f32(const float* U, const float* V, size_t r1, size_t r2,
+                                                    double max_pwr_eb, size_t* out_size) {
+  Quiet q;
+  size_t sz = 0;
+  unsigned char* p = sz_compress_cp_preserve_2d_offline_log<float>(U, V, r1, r2, sz, false, max_pwr_eb);
+  *out_size = sz;
+  return p;
+}
+
+int cpsz_ref_decompress_2d_offline_log_f32(const unsigned char* blob, size_t r1, size_t r2, float* U_out,
+                                           float* V_out) {
+  Quiet q;
+  float* U = nullptr;
+  float* V = nullptr;
+  sz_decompress_cp_preserve_2d_offline_log<float>(blob, r1, r2, U, V);
   memcpy(U_out, U, r1 * r2 * sizeof(float));
   memcpy(V_out, V, r1 * r2 * sizeof(float));
   free(U);

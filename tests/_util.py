@@ -26,6 +26,25 @@ def padding_mask_2d(blob: bytes) -> np.ndarray:
     return m
 
 
+def padding_mask_2d_log(blob: bytes, n: int) -> np.ndarray:
+    """The same for a 2D offline_log blob of n points (its field blobs follow
+    the id section and the two sign maps)."""
+    m = np.ones(len(blob), bool)
+    eb_size, u_size, v_size = struct.unpack_from("<QQQ", blob, 12)
+    at = 36 + eb_size + 2 * ((n - 1) // 8 + 1)
+    for off in (at, at + u_size):
+        m[off + 10: off + 13] = False
+    return m
+
+
+def assert_blob_equal_2d_log(a: bytes, b: bytes, n: int):
+    assert len(a) == len(b), f"blob sizes differ: {len(a)} vs {len(b)}"
+    x = np.frombuffer(a, np.uint8)
+    y = np.frombuffer(b, np.uint8)
+    bad = np.nonzero((x != y) & padding_mask_2d_log(a, n))[0]
+    assert bad.size == 0, f"{bad.size} bytes differ, first at {bad[:8].tolist()}"
+
+
 def assert_blob_equal_2d(a: bytes, b: bytes):
     assert len(a) == len(b), f"blob sizes differ: {len(a)} vs {len(b)}"
     x = np.frombuffer(a, np.uint8)

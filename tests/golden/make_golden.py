@@ -20,7 +20,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from cpsz_b200 import workloads as W  # noqa: E402
-from oracle import Oracle, Reference, build_reference, ref_2d_in_bounds, ref_3d_in_bounds  # noqa: E402
+from oracle import (Oracle, Reference, build_reference, ref_2d_in_bounds, ref_2d_log_in_bounds,  # noqa: E402
+                    ref_3d_in_bounds)
 
 CASES_2D = [  # (name, r1, r2, eb, seed)
     ("2d_33x47_eb0.1", 33, 47, 0.1, 11),
@@ -30,11 +31,27 @@ CASES_2D = [  # (name, r1, r2, eb, seed)
     ("2d_100x120_eb0.1", 100, 120, 0.1, 15),
     ("2d_37x300_eb0.05", 37, 300, 0.05, 16),
 ]
+CASES_2D_LOG = [  # (name, r1, r2, eb, seed, zeros): the offline_log pair; `zeros` plants exact zeros
+    ("2dlog_33x47_eb0.1", 33, 47, 0.1, 31, False),
+    ("2dlog_64x64_eb0.01", 64, 64, 0.01, 32, False),
+    ("2dlog_100x120_eb0.05", 100, 120, 0.05, 33, False),
+    ("2dlog_40x50_zeros_eb0.1", 40, 50, 0.1, 34, True),
+]
 CASES_3D = [  # (name, r1, r2, r3, eb, seed)
     ("3d_16x16x16_eb0.05", 16, 16, 16, 0.05, 21),
     ("3d_33x20x17_eb0.1", 33, 20, 17, 0.1, 22),
     ("3d_24x30x28_eb0.01", 24, 30, 28, 0.01, 23),
 ]
+
+
+def log_case(seed, r1, r2, zeros):
+    """A cfg0-like field; with `zeros`, every 7th point of U and every 5th of V
+    set to exactly 0 (logs of -100 and sign bits 0 in the offline_log blob)."""
+    U, V = W.cfg0_like(seed, r1, r2)
+    if zeros:
+        U.ravel()[::7] = 0
+        V.ravel()[::5] = 0
+    return U, V
 
 
 def main():
@@ -49,6 +66,16 @@ def main():
             continue
         blob = R.compress_2d(U, V, eb)
         du, dv = R.decompress_2d(blob, r1, r2)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), U=U, V=V, eb=eb,
+                            blob=np.frombuffer(blob, np.uint8), dU=du, dV=dv)
+        print("wrote", name, len(blob))
+    for name, r1, r2, eb, seed, zeros in CASES_2D_LOG:
+        U, V = log_case(seed, r1, r2, zeros)
+        if not ref_2d_log_in_bounds(O.compress_2d_log(U, V, eb), r1, r2):
+            print("skip (reference scratch too small):", name)
+            continue
+        blob = R.compress_2d_log(U, V, eb)
+        du, dv = R.decompress_2d_log(blob, r1, r2)
         np.savez_compressed(os.path.join(HERE, name + ".npz"), U=U, V=V, eb=eb,
                             blob=np.frombuffer(blob, np.uint8), dU=du, dV=dv)
         print("wrote", name, len(blob))

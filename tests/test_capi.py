@@ -12,6 +12,8 @@ DROP_IN = [
     "_Z36sz_decompress_cp_preserve_2d_offlineIfEvPKhmmRPT_S4_",
     "_Z38sz_compress_cp_preserve_3d_offline_logIfEPhPKT_S3_S3_mmmRmbd",
     "_Z39sz_decompress_cp_preserve_3d_online_logIfEvPKhmmmRPT_S4_S4_",
+    "_Z38sz_compress_cp_preserve_2d_offline_logIfEPhPKT_S3_mmRmbd",
+    "_Z40sz_decompress_cp_preserve_2d_offline_logIfEvPKhmmRPT_S4_",
 ]
 
 

@@ -97,3 +97,62 @@ def test_batch_graph_capture_and_replay(ctx):
         cpsz_b200.tuning_clear()
         cpsz_b200.tuning_load()
     assert run(ebs)[0] == ref
+
+
+def test_sharded_batch_with_the_gpu_compressor(ctx, oracle, tmp_path):
+    """The field-sharded batch (cpsz_b200.shard) driving the GPU batch
+    compressor, on one rank: every blob equals the oracle's and the written
+    file is the blobs' concatenation in field order."""
+    from cpsz_b200 import shard
+
+    fields, ebs = _batch(9, 5, 1, 500)
+    shapes = [U.shape for U, _ in fields]
+    out = str(tmp_path / "batch.bin")
+    r = shard.compress_2d_batch_sharded(shapes, ebs, lambda k: fields[k], ctx=ctx, out_path=out)
+    assert r.own == list(range(len(fields)))
+    data = open(out, "rb").read()
+    assert len(data) == int(r.offsets[-1])
+    for k, ((U, V), eb) in enumerate(zip(fields, ebs)):
+        assert_blob_equal_2d(r.blobs[k], oracle.compress_2d(U, V, eb))
+        assert data[int(r.offsets[k]):int(r.offsets[k + 1])] == r.blobs[k]
+
+
+def _nccl_rank(rank, port, out_path, res_path):
+    import os
+
+    import torch
+    import torch.distributed as dist
+
+    from cpsz_b200 import shard
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    torch.cuda.set_device(0)
+    dist.init_process_group("nccl", rank=rank, world_size=1)
+    try:
+        c = cpsz_b200.Context(0)
+        fields, ebs = _batch(6, 6, 8, 300)
+        r = shard.compress_2d_batch_sharded([U.shape for U, _ in fields], ebs, lambda k: fields[k], ctx=c,
+                                            out_path=out_path)
+        np.save(res_path, r.offsets)
+        c.close()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_batch_over_nccl_one_rank(oracle, tmp_path):
+    """The same through an initialised NCCL process group (one rank, so the
+    size all-reduce runs on the device)."""
+    import socket
+
+    import torch.multiprocessing as mp
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    out, res = str(tmp_path / "b.bin"), str(tmp_path / "offs.npy")
+    mp.spawn(_nccl_rank, args=(port, out, res), nprocs=1, join=True)
+    offs = np.load(res)
+    data = open(out, "rb").read()
+    fields, ebs = _batch(6, 6, 8, 300)
+    for k, ((U, V), eb) in enumerate(zip(fields, ebs)):
+        assert_blob_equal_2d(data[int(offs[k]):int(offs[k + 1])], oracle.compress_2d(U, V, eb))

@@ -2,7 +2,7 @@
 import numpy as np
 import pytest
 
-from tests._util import assert_bits_equal, assert_blob_equal_2d, golden_cases
+from tests._util import assert_bits_equal, assert_blob_equal_2d, assert_blob_equal_2d_log, golden_cases
 
 
 @pytest.mark.parametrize("path", golden_cases("2d_"), ids=lambda p: p.split("/")[-1])
@@ -12,6 +12,17 @@ def test_oracle_2d_matches_reference_fixture(oracle, path):
     blob = oracle.compress_2d(U, V, eb)
     assert_blob_equal_2d(blob, g["blob"].tobytes())
     du, dv = oracle.decompress_2d(g["blob"].tobytes(), *U.shape)
+    assert_bits_equal(du, g["dU"])
+    assert_bits_equal(dv, g["dV"])
+
+
+@pytest.mark.parametrize("path", golden_cases("2dlog_"), ids=lambda p: p.split("/")[-1])
+def test_oracle_2d_log_matches_reference_fixture(oracle, path):
+    g = np.load(path)
+    U, V, eb = g["U"], g["V"], float(g["eb"])
+    blob = oracle.compress_2d_log(U, V, eb)
+    assert_blob_equal_2d_log(blob, g["blob"].tobytes(), U.size)
+    du, dv = oracle.decompress_2d_log(g["blob"].tobytes(), *U.shape)
     assert_bits_equal(du, g["dU"])
     assert_bits_equal(dv, g["dV"])
 

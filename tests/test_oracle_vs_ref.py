@@ -4,8 +4,8 @@ import numpy as np
 import pytest
 
 from cpsz_b200 import workloads as W
-from oracle import ref_2d_in_bounds, ref_3d_in_bounds
-from tests._util import assert_bits_equal, assert_blob_equal_2d
+from oracle import ref_2d_in_bounds, ref_2d_log_in_bounds, ref_3d_in_bounds
+from tests._util import assert_bits_equal, assert_blob_equal_2d, assert_blob_equal_2d_log
 
 
 @pytest.mark.parametrize("r1,r2,eb,seed", [(200, 300, 0.1, 6), (517, 611, 0.1, 7), (300, 257, 0.01, 8),
@@ -20,6 +20,20 @@ def test_2d_blob_and_decode_identical(oracle, reference, r1, r2, eb, seed):
     da = oracle.decompress_2d(a, r1, r2)
     db = reference.decompress_2d(b, r1, r2)
     for x, y in zip(da, db):
+        assert_bits_equal(x, y)
+
+
+@pytest.mark.parametrize("r1,r2,eb,seed", [(200, 300, 0.1, 16), (317, 211, 0.01, 17), (64, 900, 0.05, 18)])
+def test_2d_log_blob_and_decode_identical(oracle, reference, r1, r2, eb, seed):
+    U, V = W.cfg0_like(seed, r1, r2)
+    U.ravel()[::11] = 0  # logs of -100
+    V.ravel()[::13] = -V.ravel()[::13]
+    a = oracle.compress_2d_log(U, V, eb)
+    if not ref_2d_log_in_bounds(a, r1, r2):
+        pytest.skip("workload exceeds the reference's fixed scratch buffers")
+    b = reference.compress_2d_log(U, V, eb)
+    assert_blob_equal_2d_log(a, b, U.size)
+    for x, y in zip(oracle.decompress_2d_log(a, r1, r2), reference.decompress_2d_log(b, r1, r2)):
         assert_bits_equal(x, y)
 
 

@@ -51,3 +51,29 @@ def test_3d_table_matches_log2_quantizer():
             x = _walk(t[k], d)
             if x > 0:
                 assert int(np.searchsorted(t[1:n], x, side="right")) == ref(x), (k, d)
+
+
+def test_2d_log_table_matches_log2_quantizer():
+    """offline_log: id of log2(1 + eb) with base 2 and threshold DBL_EPSILON
+    (src/sz_compress_cp_preserve_2d.cpp:345-350); t[0] is the largest bound
+    that quantizes to precision 0."""
+    t, n = _table(1)
+    thr = 2.0 ** -52
+
+    def prec0(r):
+        return math.log2(1 + r) <= thr
+
+    def ref(r):
+        a = math.log2(1 + r)
+        return 0 if a <= thr else int(math.log2(a / thr) / math.log2(2))
+
+    assert prec0(t[0]) and not prec0(np.nextafter(t[0], np.inf))
+    for k in range(1, n):
+        for d in range(-40, 41):
+            x = _walk(t[k], d)
+            if x > t[0]:
+                assert int(np.searchsorted(t[1:n], x, side="right")) == ref(x), (k, d)
+    rng = np.random.default_rng(1)
+    for x in 10.0 ** rng.uniform(-15.4, 0, 20000):
+        if x > t[0]:
+            assert int(np.searchsorted(t[1:n], x, side="right")) == ref(x)
