@@ -58,6 +58,17 @@ WORKLOADS = {
 DEFAULT = "2d_8192x8192_eb0.1"
 
 
+def _bf16_peak():
+    """Dense BF16 tensor throughput (TFLOP/s) of MEASURED_PEAKS.json (burst), or the fallback."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        if "bf16_tflops" in d:
+            return d["bf16_tflops"], "measured"
+    return 1590.0, "fallback"
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -529,6 +540,33 @@ def run_learned(args, rank, world, device):
     cp = cpsz_b200.cp_check_2d(fields[0], fields[1], dU, dV, ctx=ctx)
     z_learned = len(cpsz_b200.sz_lossless_compress(blob, 3))
     z_plain = len(cpsz_b200.sz_lossless_compress(plain, 3))
+    viol = 0
+    for x, d in zip(fields, (dU, dV)):
+        x64 = x.astype(np.float64)
+        viol += int(np.count_nonzero(np.abs(d.astype(np.float64) - x64) > eb * np.abs(x64)))
+    # roofline of the tensor-core part: the fused MLP forward over every vertex
+    # (2 * (128*128 + 128*128 + 128) flops a vertex, the 99 inputs padded to 128)
+    eb_a, _ = cpsz_b200.debug_eb2d(*fields, eb, ctx=ctx, exact=True)
+    d_eb = torch.from_numpy(np.ascontiguousarray(eb_a, np.float64)).to(f"cuda:{device}")
+    fwd_ms = mlp.forward_ms(dev[0], dev[1], d_eb, reps=5)
+    n = int(np.prod(shape))
+    flops = 2.0 * (128 * 128 * 2 + 128) * n
+    tf = flops / (fwd_ms / 1e3) / 1e12
+    peak = _bf16_peak()
+    roofline = {"bound": "tensor", "kernel": "mlp_fwd (features fused)", "achieved": round(tf, 2),
+                "peak": peak[0], "unit": "TFLOP/s", "frac": round(tf / peak[0], 4), "traffic": None,
+                "peak_source": peak[1], "ms_per_launch": round(fwd_ms, 3)}
+    # the reference's CPU path on the same field (1 core, the plain method; the
+    # reference has no learned form), and its decoder reading the learned blob
+    cpu, ref_decodes = None, None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu, _ = cpu_baseline_single("2d_8192x8192_eb0.1", fields, eb)
+        import oracle
+
+        if os.path.exists(oracle.REF_SO):
+            ru, rv = oracle.Reference().decompress_2d(blob, *shape)
+            ref_decodes = bool(np.array_equal(ru.view(np.uint32), dU.view(np.uint32)) and
+                               np.array_equal(rv.view(np.uint32), dV.view(np.uint32)))
     return {
         "metric": "compress_GBps", "value": round(raw * world / (ms / 1e3) / 1e9, 3), "unit": "GB/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
@@ -537,7 +575,9 @@ def run_learned(args, rank, world, device):
                    "parallelism": f"replicas{world}", "value_io": "fields resident in HBM, blob written to HBM"},
         "ratio": round(raw / z_learned, 4), "ratio_pre_zstd": round(raw / size, 4),
         "plain_ratio": round(raw / z_plain, 4), "plain_ratio_pre_zstd": round(raw / len(plain), 4),
-        "cp_check": cp, "loop": st, "cpu_baseline": None, "clocks": clk.summary(), "gpu_launches": launches,
+        "cp_check": cp, "cp_errors": int(cp["lost_or_spurious"] + cp["type_changed"]), "bound_violations": viol,
+        "reference_decoder_reads_blob": ref_decodes, "loop": st, "roofline": roofline, "cpu_baseline": cpu,
+        "clocks": clk.summary(), "gpu_launches": launches,
     }
 
 

@@ -101,6 +101,7 @@ def _declare(L):
     L.cpsz_b200_debug_libm.argtypes = [_vp, C.c_int, _vp, _sz, _vp]
     L.cpsz_b200_debug_filter_premises.argtypes = [_vp, _vp, _sz]
     L.cpsz_b200_mlp_propose_2d.argtypes = [_vp, _vp, _vp, _sz, _sz, _vp, _vp]
+    L.cpsz_b200_debug_mlp_forward_ms.argtypes = [_vp, _vp, _vp, _sz, _sz, _vp, C.c_int, C.POINTER(C.c_float)]
     L.cpsz_b200_debug_umma_gemm.argtypes = [_vp, _vp, _vp, _vp]
     L.cpsz_b200_mlp_param_count.restype = _sz
     L.cpsz_b200_mlp_create.argtypes = [_vp, C.c_uint64, C.POINTER(_vp)]
@@ -537,6 +538,16 @@ class Mlp:
         y = np.empty(X.shape[0], np.float32)
         _check(lib().cpsz_b200_mlp_forward(self.handle, X.ctypes.data, X.shape[0], y.ctypes.data))
         return y
+
+    def forward_ms(self, U, V, eb_analytic, reps: int = 5) -> float:
+        """Mean time (ms, CUDA events) of the fused forward pass over every vertex
+        of field (U, V) with analytic bounds eb_analytic (device arrays)."""
+        pu, _, su = _ptr(U)
+        pv, _, _ = _ptr(V)
+        pe, _, _ = _ptr(eb_analytic, np.float64)
+        ms = C.c_float()
+        _check(lib().cpsz_b200_debug_mlp_forward_ms(self.handle, pu, pv, su[0], su[1], pe, int(reps), C.byref(ms)))
+        return ms.value
 
     def train_step(self, X_bits, t, lr: float, grads: bool = False):
         """(mean squared error, gradients or None); Adam step when lr > 0."""

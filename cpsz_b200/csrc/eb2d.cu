@@ -19,14 +19,10 @@
 // size.  Every shape computes the same bytes: each vertex's bound is the same
 // minimum over the same six triangles, whichever tile evaluates them.
 //
-// CTAs are persistent: the grid holds as many CTAs as fit on the device and
-// each takes tiles in row-major order (a grid stride), so row groups complete
-// in order.  Beside the Lorenzo wavefront (which is launched after it) a CTA
-// that finds its SM already holding all but one of the CTAs that fit there
-// leaves at once, and the others take tiles from a counter: every SM keeps
-// room for one wavefront CTA, whatever the hardware's placement of the grid.
-#include <algorithm>
-
+// One CTA per tile (a 2D grid in row-major tile order, so row groups complete
+// roughly in order): measured faster than a persistent grid that takes tiles
+// with a stride or from a counter (3.75 against 4.27 ms at 8192^2 alone, and
+// the wavefront beside it keeps pace only with the per-tile grid).
 #include "eb_math.cuh"
 #include "kernels.h"
 #include "tuning.h"
@@ -42,191 +38,184 @@ __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const f
                                                   unsigned long long* __restrict__ hist, int* __restrict__ flag,
                                                   float2* __restrict__ pair_u, float2* __restrict__ pair_v,
                                                   double* __restrict__ eb_out, int row_begin, int row_end,
-                                                  unsigned long long* __restrict__ band_done, int tiles_x,
-                                                  int ntiles, int log_ids, unsigned int* __restrict__ sched,
-                                                  int sm_cap) {
+                                                  unsigned long long* __restrict__ band_done, int log_ids) {
   constexpr int CX = TX + 1;  // cells per tile row
   constexpr int CY = TY + 1;
   static_assert(WAVE_GROUP_ROWS % TY == 0, "a tile's rows must lie in one wavefront group");
   __shared__ float su[TY + 2][TX + 3];
   __shared__ float sv[TY + 2][TX + 3];
+  // compression (FAST): the float bound of an ordinary triangle, or -1 when
+  // the triangle took the exact path and its bound is in tri; exact mode: tri
+  __shared__ float trf[FAST ? 2 : 1][FAST ? CY : 1][FAST ? CX : 1];
   __shared__ double tri[2][CY][CX];
   __shared__ double tab[QUANT_TAB_MAX];
   __shared__ unsigned int shist[256];
 
   const int tid = threadIdx.x;
-  __shared__ int s_tile;
-  if (sched) {
-    // at most sm_cap CTAs of this launch per SM (the others leave at once), so
-    // a wavefront launched after it finds room on every SM; tiles then come
-    // from a counter, in row-major order
-    if (tid == 0) {
-      unsigned smid;
-      asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
-      s_tile = (smid >= 256u || atomicAdd(&sched[1 + smid], 1u) < (unsigned)sm_cap) ? 1 : 0;
-    }
-    __syncthreads();
-    if (!s_tile) return;
-  }
+  const int i0 = row_begin + blockIdx.y * TY, j0 = blockIdx.x * TX;
   for (int k = tid; k < 256; k += NT) shist[k] = 0;
   for (int k = tid; k < thr_n; k += NT) tab[k] = thr_tab[k];
-  for (int tile = blockIdx.x;; tile += gridDim.x) {
-    if (sched) {
-      __syncthreads();  // every thread has read the previous s_tile
-      if (tid == 0) s_tile = (int)atomicAdd(&sched[0], 1u);
-      __syncthreads();
-      tile = s_tile;
+  // vertex halo: rows i0-1 .. i0+TY, cols j0-1 .. j0+TX
+  for (int k = tid; k < (TY + 2) * (TX + 2); k += NT) {
+    int a = k / (TX + 2), b = k % (TX + 2);
+    int gi = i0 - 1 + a, gj = j0 - 1 + b;
+    float u = 0.f, v = 0.f;
+    if (gi >= 0 && gi < r1 && gj >= 0 && gj < r2) {
+      size_t g = (size_t)gi * r2 + gj;
+      u = U[g];
+      v = V[g];
     }
-    if (tile >= ntiles) break;
-    const int i0 = row_begin + (tile / tiles_x) * TY, j0 = (tile % tiles_x) * TX;
-    __syncthreads();  // the previous tile's readers of su / sv / tri are done
-    // vertex halo: rows i0-1 .. i0+TY, cols j0-1 .. j0+TX
-    for (int k = tid; k < (TY + 2) * (TX + 2); k += NT) {
-      int a = k / (TX + 2), b = k % (TX + 2);
-      int gi = i0 - 1 + a, gj = j0 - 1 + b;
-      float u = 0.f, v = 0.f;
-      if (gi >= 0 && gi < r1 && gj >= 0 && gj < r2) {
-        size_t g = (size_t)gi * r2 + gj;
-        u = U[g];
-        v = V[g];
+    su[a][b] = u;
+    sv[a][b] = v;
+  }
+  __syncthreads();
+  // triangles of cells (ci, cj) = (i0-1+a, j0-1+b), a in [0, CY), b in [0, CX);
+  // one triangle per thread and round (2 * 561 triangles over 256 threads at 32x16)
+  for (int k = tid; k < 2 * CY * CX; k += NT) {
+    const int kind = k >= CY * CX;
+    const int c = k - kind * CY * CX;
+    const int a = c / CX, b = c % CX;
+    const int ci = i0 - 1 + a, cj = j0 - 1 + b;
+    double e = 0;
+    float t = 0.f;
+    if (ci >= 0 && ci < r1 - 1 && cj >= 0 && cj < r2 - 1) {
+      // upper: offsets {0, r2, r2+1} -> (a,b), (a+1,b), (a+1,b+1);
+      // lower: offsets {0, 1, r2+1} -> (a,b), (a,b+1), (a+1,b+1).
+      // One call site of the exact bound keeps a single copy of its code in
+      // the instruction cache.
+      const int a1 = a + (kind == 0), b1 = b + (kind == 1);
+      const float x0 = su[a][b], x1 = su[a1][b1], x2 = su[a + 1][b + 1];
+      const float y0 = sv[a][b], y1 = sv[a1][b1], y2 = sv[a + 1][b + 1];
+      if (!FAST || !dev::tri_eb_float(x0, x1, x2, y0, y1, y2, t)) {
+        e = dev::tri_eb_exact(x0, x1, x2, y0, y1, y2, kind);
+        t = -1.f;
       }
-      su[a][b] = u;
-      sv[a][b] = v;
     }
-    __syncthreads();
-    // triangles of cells (ci, cj) = (i0-1+a, j0-1+b), a in [0, CY), b in [0, CX);
-    // one triangle per thread and round (2 * 561 triangles over 256 threads at 32x16)
-    for (int k = tid; k < 2 * CY * CX; k += NT) {
-      const int kind = k >= CY * CX;
-      const int c = k - kind * CY * CX;
-      const int a = c / CX, b = c % CX;
-      const int ci = i0 - 1 + a, cj = j0 - 1 + b;
-      double e = 0;
-      if (ci >= 0 && ci < r1 - 1 && cj >= 0 && cj < r2 - 1) {
-        // upper: offsets {0, r2, r2+1} -> (a,b), (a+1,b), (a+1,b+1);
-        // lower: offsets {0, 1, r2+1} -> (a,b), (a,b+1), (a+1,b+1).
-        // One call site keeps a single copy of the bound code in the
-        // instruction cache.
-        const int a1 = a + (kind == 0), b1 = b + (kind == 1);
-        if (FAST)
-          e = dev::tri_eb_filtered(su[a][b], su[a1][b1], su[a + 1][b + 1], sv[a][b], sv[a1][b1], sv[a + 1][b + 1],
-                                   kind);
-        else
-          e = dev::tri_eb(su[a][b], su[a1][b1], su[a + 1][b + 1], sv[a][b], sv[a1][b1], sv[a + 1][b + 1], kind);
+    if (FAST) trf[FAST ? kind : 0][FAST ? a : 0][FAST ? b : 0] = t;
+    tri[kind][a][b] = e;
+  }
+  __syncthreads();
+  const double thr = tab[0];
+  // id of a quantized bound e (-1 for precision 0), before the range check
+  auto quant = [&](double e) -> int {
+    if (e <= thr) return -1;
+    const int ex = (int)((__double_as_longlong(e) >> 52) & 0x7ff) - 1023;
+    return dev::count_thresholds(tab, thr_n, e, (ex + 52) >> (log_ids ? 0 : 1));
+  };
+  for (int k = tid; k < TY * TX; k += NT) {
+    int a = k / TX, b = k % TX;
+    int gi = i0 + a, gj = j0 + b;
+    if (gi >= row_end || gj >= r2) continue;
+    // vertex (gi, gj) is local (a+1, b+1); cell (gi-1+x, gj-1+y) is tri[.][a+x][b+y]
+    bool up = gi >= 1, left = gj >= 1, down = gi < r1 - 1, right = gj < r2 - 1;
+    const float uu = su[a + 1][b + 1], vv = sv[a + 1][b + 1];
+    // Offline: one id per component, of |x| * eb (base 4).  offline_log: one
+    // id of the vertex bound itself (the log2(1 + eb) quantizer's table).
+    const double s0 = log_ids ? 1.0 : (double)fabsf(uu), s1 = (double)fabsf(vv);
+    // the reference's chain eb = MINF(eb, triangle bound) over the six triangles
+    auto vertex_eb = [&](auto&& tri_at) {
+      double eb = max_pwr_eb;
+      if (up && left) {
+        eb = dev::minf_d(eb, tri_at(0, a, b));
+        eb = dev::minf_d(eb, tri_at(1, a, b));
       }
-      tri[kind][a][b] = e;
-    }
-    __syncthreads();
-    const double thr = tab[0];
-    // id of a quantized bound e (-1 for precision 0), before the range check
-    auto quant = [&](double e) -> int {
-      if (e <= thr) return -1;
-      const int ex = (int)((__double_as_longlong(e) >> 52) & 0x7ff) - 1023;
-      return dev::count_thresholds(tab, thr_n, e, (ex + 52) >> (log_ids ? 0 : 1));
+      if (up && right) eb = dev::minf_d(eb, tri_at(0, a, b + 1));
+      if (down && left) eb = dev::minf_d(eb, tri_at(1, a + 1, b));
+      if (down && right) {
+        eb = dev::minf_d(eb, tri_at(0, a + 1, b + 1));
+        eb = dev::minf_d(eb, tri_at(1, a + 1, b + 1));
+      }
+      return eb;
     };
-    for (int k = tid; k < TY * TX; k += NT) {
-      int a = k / TX, b = k % TX;
-      int gi = i0 + a, gj = j0 + b;
-      if (gi >= row_end || gj >= r2) continue;
-      // vertex (gi, gj) is local (a+1, b+1); cell (gi-1+x, gj-1+y) is tri[.][a+x][b+y]
-      bool up = gi >= 1, left = gj >= 1, down = gi < r1 - 1, right = gj < r2 - 1;
-      const float uu = su[a + 1][b + 1], vv = sv[a + 1][b + 1];
-      // Offline: one id per component, of |x| * eb (base 4).  offline_log: one
-      // id of the vertex bound itself (the log2(1 + eb) quantizer's table).
-      const double s0 = log_ids ? 1.0 : (double)fabsf(uu), s1 = (double)fabsf(vv);
-      // the reference's chain eb = MINF(eb, triangle bound) over the six triangles
-      auto vertex_eb = [&](auto&& tri_at) {
-        double eb = max_pwr_eb;
-        if (up && left) {
-          eb = dev::minf_d(eb, tri_at(0, a, b));
-          eb = dev::minf_d(eb, tri_at(1, a, b));
+    int code[2];
+    double eb = 0;
+    if (FAST) {
+      // enclosure of the vertex bound: the float bounds of its ordinary
+      // triangles (min mf, each within FFILT_REL and FFILT_ABS of the
+      // reference's value) and the exact ones (min md)
+      float mf = INFINITY;
+      double md = INFINITY;
+      bool nan = false;
+      auto take = [&](int kind, int ca, int cb) {
+        const float t = trf[FAST ? kind : 0][FAST ? ca : 0][FAST ? cb : 0];
+        if (t >= 0.f) {
+          mf = fminf(mf, t);
+        } else {
+          const double e = tri[kind][ca][cb];
+          nan |= isnan(e);
+          md = fmin(md, e);
         }
-        if (up && right) eb = dev::minf_d(eb, tri_at(0, a, b + 1));
-        if (down && left) eb = dev::minf_d(eb, tri_at(1, a + 1, b));
-        if (down && right) {
-          eb = dev::minf_d(eb, tri_at(0, a + 1, b + 1));
-          eb = dev::minf_d(eb, tri_at(1, a + 1, b + 1));
-        }
-        return eb;
       };
-      int code[2];
-      double eb = 0;
-      if (FAST) {
-        // enclosure of the vertex bound from the filtered triangle bounds
-        double m = INFINITY;
-        bool nan = false;
-        auto take = [&](double t) {
-          nan |= isnan(t);
-          m = fmin(m, t);
-        };
-        if (up && left) {
-          take(tri[0][a][b]);
-          take(tri[1][a][b]);
-        }
-        if (up && right) take(tri[0][a][b + 1]);
-        if (down && left) take(tri[1][a + 1][b]);
-        if (down && right) {
-          take(tri[0][a + 1][b + 1]);
-          take(tri[1][a + 1][b + 1]);
-        }
-        const double lo = fmin(max_pwr_eb, m * (1.0 - dev::FILTER_REL) - dev::FILTER_ABS);
-        const double hi = fmin(max_pwr_eb, m * (1.0 + dev::FILTER_REL) + dev::FILTER_ABS);
-        code[0] = quant(s0 * lo);
-        code[1] = log_ids ? -1 : quant(s1 * lo);
-        // the upper end has the same id iff it stays below the next threshold
-        auto stays = [&](int c, double e) { return c < 0 ? e <= thr : (c + 1 >= thr_n || e < tab[c + 1]); };
-        if (nan || !stays(code[0], s0 * hi) || (!log_ids && !stays(code[1], s1 * hi))) {
-          // the enclosure straddles a threshold (or a bound is NaN): exact bounds
-          eb = vertex_eb([&](int kind, int ca, int cb) {
-            const int a1 = ca + (kind == 0), b1 = cb + (kind == 1);
-            return dev::tri_eb_exact(su[ca][cb], su[a1][b1], su[ca + 1][cb + 1], sv[ca][cb], sv[a1][b1],
-                                     sv[ca + 1][cb + 1], kind);
-          });
-          code[0] = quant(s0 * eb);
-          code[1] = log_ids ? -1 : quant(s1 * eb);
-        }
-      } else {
-        eb = vertex_eb([&](int kind, int ca, int cb) { return tri[kind][ca][cb]; });
+      if (up && left) {
+        take(0, a, b);
+        take(1, a, b);
+      }
+      if (up && right) take(0, a, b + 1);
+      if (down && left) take(1, a + 1, b);
+      if (down && right) {
+        take(0, a + 1, b + 1);
+        take(1, a + 1, b + 1);
+      }
+      const double m = (double)mf;
+      const double lo = fmin(max_pwr_eb, fmin(m * (1.0 - dev::FFILT_REL) - dev::FFILT_ABS, md));
+      const double hi = fmin(max_pwr_eb, fmin(m * (1.0 + dev::FFILT_REL) + dev::FFILT_ABS, md));
+      code[0] = quant(s0 * lo);
+      code[1] = log_ids ? -1 : quant(s1 * lo);
+      // the upper end has the same id iff it stays below the next threshold
+      auto stays = [&](int c, double e) { return c < 0 ? e <= thr : (c + 1 >= thr_n || e < tab[c + 1]); };
+      if (nan || !stays(code[0], s0 * hi) || (!log_ids && !stays(code[1], s1 * hi))) {
+        // the enclosure straddles a threshold (or a bound is NaN): exact bounds
+        eb = vertex_eb([&](int kind, int ca, int cb) {
+          const int a1 = ca + (kind == 0), b1 = cb + (kind == 1);
+          return dev::tri_eb_exact(su[ca][cb], su[a1][b1], su[ca + 1][cb + 1], sv[ca][cb], sv[a1][b1],
+                                   sv[ca + 1][cb + 1], kind);
+        });
         code[0] = quant(s0 * eb);
         code[1] = log_ids ? -1 : quant(s1 * eb);
       }
-      int sym[2];
-  #pragma unroll
-      for (int c = 0; c < 2; c++) {
-        if (code[c] > ID_MAX_2D) {
-          atomicOr(flag, FLAG_ID_OVERFLOW);
-          code[c] = ID_MAX_2D;
-        }
-        sym[c] = code[c] < 0 ? 0 : code[c];
-        if (code[c] < 0) code[c] = ID_ZERO;
-      }
-      size_t g = (size_t)gi * r2 + gj;
-      if (!FAST && eb_out) eb_out[g] = eb;
-      ids_u[g] = (uint8_t)code[0];
-      if (!log_ids) ids_v[g] = (uint8_t)code[1];
-      if (pair_u) {
-        // the wavefront's input: value and 1/precision = 2^(52 - 2 id) (NaN for precision 0)
-        pair_u[g] = make_float2(uu, code[0] == ID_ZERO ? __int_as_float(0x7FC00000)
-                                                       : __int_as_float((127 + 52 - 2 * (int)code[0]) << 23));
-        pair_v[g] = make_float2(vv, code[1] == ID_ZERO ? __int_as_float(0x7FC00000)
-                                                       : __int_as_float((127 + 52 - 2 * (int)code[1]) << 23));
-      }
-      atomicAdd(&shist[sym[0]], 1u);
-      if (!log_ids) atomicAdd(&shist[sym[1]], 1u);
+    } else {
+      eb = vertex_eb([&](int kind, int ca, int cb) { return tri[kind][ca][cb]; });
+      code[0] = quant(s0 * eb);
+      code[1] = log_ids ? -1 : quant(s1 * eb);
     }
-    if (band_done) {
-      // every thread's outputs are visible device-wide before the tile counts
-      __threadfence();
-      __syncthreads();
-      if (tid == 0) {
-        const int rows = min(TY, row_end - i0), cols = min(TX, r2 - j0);
-        atomicAdd(&band_done[i0 / WAVE_GROUP_ROWS], (unsigned long long)rows * cols);
+    int sym[2];
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+      if (code[c] > ID_MAX_2D) {
+        atomicOr(flag, FLAG_ID_OVERFLOW);
+        code[c] = ID_MAX_2D;
       }
+      sym[c] = code[c] < 0 ? 0 : code[c];
+      if (code[c] < 0) code[c] = ID_ZERO;
     }
-  }  // tiles
+    size_t g = (size_t)gi * r2 + gj;
+    if (!FAST && eb_out) eb_out[g] = eb;
+    ids_u[g] = (uint8_t)code[0];
+    if (!log_ids) ids_v[g] = (uint8_t)code[1];
+    if (pair_u) {
+      // the wavefront's input: value and 1/precision = 2^(52 - 2 id) (NaN for precision 0)
+      pair_u[g] = make_float2(uu, code[0] == ID_ZERO ? __int_as_float(0x7FC00000)
+                                                     : __int_as_float((127 + 52 - 2 * (int)code[0]) << 23));
+      pair_v[g] = make_float2(vv, code[1] == ID_ZERO ? __int_as_float(0x7FC00000)
+                                                     : __int_as_float((127 + 52 - 2 * (int)code[1]) << 23));
+    }
+    atomicAdd(&shist[sym[0]], 1u);
+    if (!log_ids) atomicAdd(&shist[sym[1]], 1u);
+  }
   __syncthreads();
   for (int k = tid; k < 256; k += NT)
     if (shist[k]) atomicAdd(&hist[k], (unsigned long long)shist[k]);
+  if (band_done) {
+    // every thread's outputs are visible device-wide before the tile counts;
+    // band_done[-1] counts finished tiles (the wavefront's sign of progress)
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) {
+      const int rows = min(TY, row_end - i0), cols = min(TX, r2 - j0);
+      atomicAdd(&band_done[i0 / WAVE_GROUP_ROWS], (unsigned long long)rows * cols);
+      atomicAdd(&band_done[-1], 1ull);
+    }
+  }
 }
 
 int preload_eb2d() {
@@ -251,31 +240,17 @@ int preload_eb2d() {
 int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, double max_pwr_eb,
                 const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
                 float2* pair_u, float2* pair_v, double* eb_out, int row_begin, int row_end,
-                unsigned long long* band_done, bool log_ids, unsigned int* sched) {
+                unsigned long long* band_done, bool log_ids) {
   if (row_end < 0) row_end = r1;
   if (log_ids && (pair_u || pair_v || ids_v))
     return set_error(CPSZ_ERR_INVALID, "eb2d: the log-domain ids have no wavefront pairs and one stream");
   if (row_end <= row_begin) return CPSZ_OK;
   if (band_done && row_begin % WAVE_GROUP_ROWS)
     return set_error(CPSZ_ERR_INVALID, "eb2d band start %d is not a multiple of %d", row_begin, WAVE_GROUP_ROWS);
-  int err = CPSZ_OK;
   auto go = [&](auto kernel, int tx, int ty, int nt) {
-    const int tiles_x = (r2 + tx - 1) / tx;
-    const long long ntiles = (long long)tiles_x * ((row_end - row_begin + ty - 1) / ty);
-    if (ntiles > INT32_MAX) {
-      err = set_error(CPSZ_ERR_UNSUPPORTED, "eb2d: %lld tiles", ntiles);
-      return;
-    }
-    // persistent grid: the CTAs that fit; with `sched` (beside the wavefront)
-    // one per SM fewer stay, each SM keeping room for a wavefront CTA
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, nt, 0);
-    if (per_sm < 1) per_sm = 1;
-    const int cap = sched ? std::max(1, per_sm - 1) : per_sm;
-    const long long grid = std::min<long long>(ntiles, (long long)per_sm * ctx->num_sms);
-    kernel<<<(unsigned)grid, nt, 0, ctx->stream>>>(U, V, r1, r2, max_pwr_eb, d_thr_tab, thr_n, ids_u, ids_v, hist,
-                                                   ctx->d_flag, pair_u, pair_v, eb_out, row_begin, row_end,
-                                                   band_done, tiles_x, (int)ntiles, log_ids ? 1 : 0, sched, cap);
+    dim3 grid((r2 + tx - 1) / tx, (row_end - row_begin + ty - 1) / ty);
+    kernel<<<grid, nt, 0, ctx->stream>>>(U, V, r1, r2, max_pwr_eb, d_thr_tab, thr_n, ids_u, ids_v, hist, ctx->d_flag,
+                                         pair_u, pair_v, eb_out, row_begin, row_end, band_done, log_ids ? 1 : 0);
   };
   // filtered bounds unless the caller wants the bounds themselves (or an
   // unusual max_pwr_eb takes the reference's NaN paths)
@@ -294,7 +269,6 @@ int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int 
     case 11: go(eb2d_kernel<32, 16, 128, false>, 32, 16, 128); break;
     default: go(eb2d_kernel<32, 16, 256, false>, 32, 16, 256); break;
   }
-  if (err != CPSZ_OK) return err;
   count_launch(ctx);
   return check_launch("eb2d_kernel");
 }

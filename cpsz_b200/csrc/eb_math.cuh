@@ -191,32 +191,8 @@ static __device__ __noinline__ double tri_eb_exact(float u0, float u1, float u2,
   return tri_eb(u0, u1, u2, v0, v1, v2, kind);
 }
 
-// ---- filtered 2D bound ------------------------------------------------------
-// The compressor uses a vertex's bound only through the id of |u| * eb and
-// |v| * eb, and ids change only at thresholds a factor 4 apart.  So the
-// ordinary triangles (no critical point, finite products: 98 % and more of a
-// field) get their sign-keeping bounds from a float evaluation with a proven
-// enclosure of the reference's double result, and a vertex whose enclosure
-// straddles a threshold is recomputed exactly.
-//
-// Enclosure of keep_sign2(P, N) = |sqrt P - sqrt N| / (sqrt P + sqrt N) for
-// finite P, N > 0 (P and N are the reference's own double sums):
-//  * the reference's double evaluation r_ref (two square roots, a difference,
-//    a sum, a quotient, each rounded to nearest, u = 2^-53) differs from the
-//    real value r by at most 4.1 u r + 1.01 u;
-//  * the float evaluation r_a = |P - N| / (P + N + 2 sqrt(P N)) (the same real
-//    value; P, N scaled by a power of two into [0, 2] first, so nothing
-//    overflows; the larger lands in [1, 2), and an underflowed product moves
-//    the denominator by < 2^-70 of itself), with round-to-nearest conversions,
-//    product and sums (2^-24 each), sqrt.approx.f32 (relative error below
-//    2^-22) and div.approx.f32 (2 ulp), has a relative error below 2^-19;
-//  so r_ref lies in [r_a (1 - REL) - ABS, r_a (1 + REL) + ABS] with the
-//  margins below (REL about 5x, ABS about 30x the sums).  The triangle bound
-//  is a max of mins of such values, and the vertex bound a min of triangle
-//  bounds: all monotone, so the same affine enclosure holds for them.
-constexpr double FILTER_REL = 1e-5;
-constexpr double FILTER_ABS = 3.552713678800501e-15;  // 2^-48
-
+// ---- approximate float operations of the filtered bounds -----------------------
+// (error maxima measured exhaustively on the device by selfcheck.cu)
 __device__ __forceinline__ float sqrt_approx(float x) {
   float y;
   asm("sqrt.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -227,62 +203,110 @@ __device__ __forceinline__ float div_approx(float a, float b) {
   asm("div.approx.f32 %0, %1, %2;" : "=f"(y) : "f"(a), "f"(b));
   return y;
 }
-__device__ __forceinline__ double keep_sign2_approx(double P, double N) {
-  if ((N == 0) || (P == 0)) return 1;
-  // scale by 2^-e, e the exponent of the larger (P, N are normal doubles):
-  // subtracting e from both exponent fields is exact
-  const long long m = __double_as_longlong(P > N ? P : N) & 0x7ff0000000000000ll;
-  const long long sh = m - (1023ll << 52);
-  const float pf = (float)__longlong_as_double(__double_as_longlong(P) - sh);
-  const float nf = (float)__longlong_as_double(__double_as_longlong(N) - sh);
-  const float df = (float)(fabs(P - N) * __longlong_as_double((2046ll << 52) - m));
-  const float den = pf + nf + 2.f * sqrt_approx(pf * nf);
-  return (double)div_approx(df, den);
+// ---- float-filtered 2D bound ------------------------------------------------------
+// The compression path's triangle bound in single precision, for the
+// ordinary triangles: no critical point, every quantity finite and away from
+// the degenerate cases.  It returns false for the others, which take the
+// exact double path.  Every quantity below is a function of the six float
+// products p_ij = u_i * v_j, which the reference itself forms in float (its
+// products are float*float; src/sz_compress_cp_preserve_2d.cpp:128-133), so
+// they are the reference's values exactly.  Write S = sum |p|, u = 2^-24.
+//
+//  * exact differences.  x1 = p20 - p02, x2 = p12 - p21, x3 = p01 - p10 (the
+//    reference's denominators) are formed with their rounding errors
+//    (Knuth's two-sum: x_k + e_k is the difference exactly), and so are
+//    s1 = x2 + x3, s2 = x1 + x3, s3 = x1 + x2 and det = x1 + x2 + x3: each is a
+//    float within 2u of its exact value, relative (the error terms are
+//    summed in float, at most u^2 S off).
+//  * flags.  In real arithmetic det / x_k >= 1 iff s_k = det - x_k and x_k
+//    have the same sign (or s_k = 0).  The reference evaluates det and x_k in
+//    double (errors below 5 * 2^-53 S) and the quotient rounded; with the
+//    margin T = 2^-44 S, when |s_k| > T, x_k != 0 and |det| > T the
+//    reference's flag equals (sign s_k == sign x_k) and its det is not zero.
+//    Otherwise, and when all three flags hold (a critical point), the
+//    triangle is exact.
+//  * bounds.  keep_sign2(P, N) = |sqrt P - sqrt N| / (sqrt P + sqrt N) =
+//    |P - N| / (sqrt P + sqrt N)^2 (1 when P or N is 0), P and N the sums of
+//    the positive / negated negative terms.  Its numerator P - N is one of the
+//    accurate values above: x_k for the two-term bounds, s_k for the
+//    four-term ones (p01 - p10 + p12 - p21 = x3 + x2, and so on).  The
+//    denominator d = P + N + 2 sqrt(P N) comes from float sums of the terms
+//    (3u relative each) and sqrt.approx: within 2^-20 relative.  The
+//    triangle's bound is the max over failing flags of the min of two such
+//    fractions, compared by cross-multiplication (a choice can only go wrong
+//    between values within 2^-22 of each other), with one div.approx
+//    (2 ulp) at the end.  The result t is within 2^-18 t of the real value,
+//    and the reference's double value within 2^-50 r + 2^-52 of it; the
+//    enclosure uses 2^-16 relative and 2^-40 absolute.
+//  * range.  Exact path when S is not finite, S > 2^40 or S < 2^-60, or a
+//    product P N is below 2^-110 and not 0 (sqrt of a subnormal product).
+constexpr float FFILT_REL = 1.0f / 65536.0f;           // 2^-16
+constexpr float FFILT_ABS = 9.09494702e-13f;           // 2^-40
+
+struct Frac {
+  float n, d;  // the value n / d, d > 0
+};
+// a + b = s + e exactly (Knuth's two-sum; no assumption on magnitudes)
+__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
+  s = a + b;
+  const float bb = s - a;
+  e = (a - (s - bb)) + (b - bb);
 }
-__device__ __forceinline__ double off2_approx(double a, double b) {
-  double p = 0, n = 0;
-  acc(a, p, n);
-  acc(b, p, n);
-  return keep_sign2_approx(p, n);
+// keep_sign2 as a fraction: numerator |D| (D = P - N, accurate), P and N for the denominator
+__device__ __forceinline__ Frac ks2_frac(float D, float P, float N, bool& bad) {
+  if (P == 0.f || N == 0.f) return Frac{1.f, 1.f};
+  const float pn = P * N;
+  bad |= !(pn >= 1.2924697e-33f);  // 2^-110
+  return Frac{fabsf(D), (P + N) + 2.f * sqrt_approx(pn)};
 }
-__device__ __forceinline__ double off4_approx(double a, double b, double c, double d) {
-  double p = 0, n = 0;
-  acc(a, p, n);
-  acc(b, p, n);
-  acc(c, p, n);
-  acc(d, p, n);
-  return keep_sign2_approx(p, n);
+__device__ __forceinline__ Frac frac_min(Frac a, Frac b) { return (a.n * b.d <= b.n * a.d) ? a : b; }
+__device__ __forceinline__ Frac frac_max(Frac a, Frac b) { return (a.n * b.d >= b.n * a.d) ? a : b; }
+__device__ __forceinline__ float pos_part(float t) { return t > 0.f ? t : 0.f; }
+__device__ __forceinline__ float neg_part(float t) { return t < 0.f ? -t : 0.f; }
+// two-term bound (max_eb_to_keep_sign_2d_offline_2) of (a, b) with a + b = D
+__device__ __forceinline__ Frac off2_frac(float D, float a, float b, bool& bad) {
+  return ks2_frac(D, pos_part(a) + pos_part(b), neg_part(a) + neg_part(b), bad);
+}
+// four-term bound (_4) of (a, b, c, d) with a + b + c + d = D
+__device__ __forceinline__ Frac off4_frac(float D, float a, float b, float c, float d, bool& bad) {
+  const float P = ((pos_part(a) + pos_part(b)) + pos_part(c)) + pos_part(d);
+  const float N = ((neg_part(a) + neg_part(b)) + neg_part(c)) + neg_part(d);
+  return ks2_frac(D, P, N, bad);
 }
 
-// Filtered triangle bound: the exact tri_eb for det == 0, critical-point
-// triangles and non-finite products (NaN possible there); otherwise the same
-// max over failing flags of min(off2, off4), of the float approximations.
-__device__ __forceinline__ double tri_eb_filtered(float u0, float u1, float u2, float v0, float v1, float v2,
-                                                  int kind) {
-  const double u0v1 = (double)(u0 * v1), u1v0 = (double)(u1 * v0), u0v2 = (double)(u0 * v2);
-  const double u2v0 = (double)(u2 * v0), u1v2 = (double)(u1 * v2), u2v1 = (double)(u2 * v1);
-  const double det = u0v1 - u1v0 + u1v2 - u2v1 + u2v0 - u0v2;
-  if (det == 0) return 0;
-  const bool f1 = quotient_at_least_one(det, u2v0 - u0v2);
-  const bool f2 = quotient_at_least_one(det, u1v2 - u2v1);
-  const bool f3 = quotient_at_least_one(det, u0v1 - u1v0);
-  if ((f1 && f2 && f3) || !(isfinite(u0v1) && isfinite(u1v0) && isfinite(u0v2) && isfinite(u2v0) &&
-                            isfinite(u1v2) && isfinite(u2v1)))
-    return tri_eb_exact(u0, u1, u2, v0, v1, v2, kind);
-  double eb = 0;
-  if (!f1) {
-    const double e1 = off2_approx(u2v0, -u0v2);
-    if (e1 > eb) eb = max_d(eb, minf_d(e1, off4_approx(u0v1, -u1v0, u1v2, -u2v1)));
-  }
-  if (!f2) {
-    const double e1 = off2_approx(u1v2, -u2v1);
-    if (e1 > eb) eb = max_d(eb, minf_d(e1, off4_approx(u0v1, -u1v0, u2v0, -u0v2)));
-  }
-  if (!f3) {
-    const double e1 = off2_approx(u0v1, -u1v0);
-    if (e1 > eb) eb = max_d(eb, minf_d(e1, off4_approx(u1v2, -u2v1, u2v0, -u0v2)));
-  }
-  return eb;
+// The float bound of an ordinary triangle (true), or false: take the exact path.
+__device__ __forceinline__ bool tri_eb_float(float u0, float u1, float u2, float v0, float v1, float v2, float& t) {
+  const float p01 = u0 * v1, p10 = u1 * v0, p02 = u0 * v2, p20 = u2 * v0, p12 = u1 * v2, p21 = u2 * v1;
+  const float S = ((((fabsf(p01) + fabsf(p10)) + fabsf(p12)) + fabsf(p21)) + fabsf(p20)) + fabsf(p02);
+  float x1, e1, x2, e2, x3, e3;
+  two_sum(p20, -p02, x1, e1);
+  two_sum(p12, -p21, x2, e2);
+  two_sum(p01, -p10, x3, e3);
+  float h1, g1, h2, g2, h3, g3, hd, gd;
+  two_sum(x2, x3, h1, g1);
+  two_sum(x1, x3, h2, g2);
+  two_sum(x1, x2, h3, g3);
+  two_sum(h1, x1, hd, gd);
+  const float s1 = h1 + (g1 + (e2 + e3));
+  const float s2 = h2 + (g2 + (e1 + e3));
+  const float s3 = h3 + (g3 + (e1 + e2));
+  const float det = hd + (gd + (g1 + ((e1 + e2) + e3)));
+  const float T = S * 5.68434189e-14f;  // 2^-44
+  bool bad = !(S >= 8.67361738e-19f && S <= 1.09951163e12f);  // [2^-60, 2^40], false for NaN
+  bad |= !(fabsf(s1) > T && fabsf(s2) > T && fabsf(s3) > T && fabsf(det) > T);
+  bad |= x1 == 0.f || x2 == 0.f || x3 == 0.f;
+  const bool f1 = (s1 > 0.f) == (x1 > 0.f), f2 = (s2 > 0.f) == (x2 > 0.f), f3 = (s3 > 0.f) == (x3 > 0.f);
+  bad |= f1 && f2 && f3;  // a critical point: exact path
+  // max over failing flags of min(off2, off4), all three evaluated (no divergence)
+  Frac e = Frac{0.f, 1.f};
+  const Frac a1 = frac_min(off2_frac(x1, p20, -p02, bad), off4_frac(s1, p01, -p10, p12, -p21, bad));
+  const Frac a2 = frac_min(off2_frac(x2, p12, -p21, bad), off4_frac(s2, p01, -p10, p20, -p02, bad));
+  const Frac a3 = frac_min(off2_frac(x3, p01, -p10, bad), off4_frac(s3, p12, -p21, p20, -p02, bad));
+  if (!f1) e = frac_max(e, a1);
+  if (!f2) e = frac_max(e, a2);
+  if (!f3) e = frac_max(e, a3);
+  t = div_approx(e.n, e.d);
+  return !bad;
 }
 
 // ---- 3D (src/sz_compress_cp_preserve_3d.cpp:266-358) --------------------------

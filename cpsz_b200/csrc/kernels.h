@@ -30,16 +30,14 @@ constexpr int FLAG_OUT_CAPACITY = 16; // an output stream did not fit its buffer
 // adds the number of vertices it finished to its group's counter after its
 // outputs are visible device-wide (row_begin must then be a multiple of
 // WAVE_GROUP_ROWS), so a concurrently running wavefront can start on a group
-// as soon as its counter reaches rows x r2.
+// as soon as its counter reaches rows x r2; band_done[-1] counts finished
+// tiles, the waiting wavefront's sign that the kernel is running.
 // log_ids: the offline_log form -- one id per vertex, of the vertex bound
 // itself against quant_table_2d_log() (ids_v, pair_u and pair_v null).
 int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, double max_pwr_eb,
                 const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
                 float2* pair_u, float2* pair_v, double* eb_out = nullptr, int row_begin = 0, int row_end = -1,
-                unsigned long long* band_done = nullptr, bool log_ids = false, unsigned int* sched = nullptr);
-// sched (optional, EB2D_SCHED_WORDS zeroed words): the launch keeps at most
-// one CTA per SM fewer than fit, leaving every SM room for a wavefront CTA.
-constexpr int EB2D_SCHED_WORDS = 257;
+                unsigned long long* band_done = nullptr, bool log_ids = false);
 
 // Loads every eb2d instantiation (required before a consumer that waits on
 // eb2d is launched: a lazily loaded first launch could wait for it).
@@ -72,10 +70,11 @@ struct WaveField {
   // spins waiting for the row above, spins waiting for ring credit}
   long long* trace;
   // optional: per-group counters of input points written by a concurrently
-  // running producer (launch_eb2d's band_done); an item starts once its
-  // group's counter reaches rows x r2 + band_extra (bounded wait of
-  // band_wait_ns, then FLAG_TIMEOUT).  band_extra is 0 except in the test
-  // that makes the wait run out on purpose.
+  // running producer (launch_eb2d's band_done, band_done[-1] its finished
+  // tiles); an item starts once its group's counter reaches rows x r2 +
+  // band_extra.  The wait gives up (FLAG_TIMEOUT) once the producer has shown
+  // no progress for band_wait_ns (0: the default).  band_extra is 0 except in
+  // the test that makes the wait run out on purpose.
   const unsigned long long* band_done;
   long long band_wait_ns;
   unsigned long long band_extra;

@@ -517,6 +517,39 @@ int cpsz_b200_mlp_propose_2d(cpsz_b200_mlp* mlp, const float* U, const float* V,
   return CPSZ_OK;
 }
 
+int cpsz_b200_debug_mlp_forward_ms(cpsz_b200_mlp* mlp, const float* U, const float* V, size_t r1, size_t r2,
+                                   const double* eb_analytic, int reps, float* ms) {
+  if (!mlp || !ms || reps < 1) return set_error(CPSZ_ERR_INVALID, "null argument or no repetition");
+  cpsz_b200_ctx* ctx = mlp->ctx;
+  CPSZ_TRY(resolve(ctx));
+  if (!U || !V || !eb_analytic || !is_device_ptr(U) || !is_device_ptr(V) || !is_device_ptr(eb_analytic))
+    return set_error(CPSZ_ERR_INVALID, "U, V and the analytic bounds must be device memory");
+  const size_t N = r1 * r2;
+  if (N == 0 || N > (size_t)INT32_MAX) return set_error(CPSZ_ERR_UNSUPPORTED, "field size out of range");
+  CPSZ_TRY(ensure_scratch(mlp, 4 * N + 256));
+  float* dy = (float*)mlp->scratch;
+  cudaEvent_t a, b;
+  CPSZ_CUDA_TRY(cudaEventCreate(&a));
+  CPSZ_CUDA_TRY(cudaEventCreate(&b));
+  CPSZ_CUDA_TRY(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+  int rc = launch_mlp_forward(ctx, mlp->w, nullptr, U, V, eb_analytic, (int)r1, (int)r2, (int)N, dy, nullptr, nullptr);
+  if (rc == CPSZ_OK && cudaEventRecord(a, ctx->stream) != cudaSuccess) rc = set_error(CPSZ_ERR_CUDA, "event");
+  for (int k = 0; k < reps && rc == CPSZ_OK; k++)
+    rc = launch_mlp_forward(ctx, mlp->w, nullptr, U, V, eb_analytic, (int)r1, (int)r2, (int)N, dy, nullptr, nullptr);
+  if (rc == CPSZ_OK && cudaEventRecord(b, ctx->stream) != cudaSuccess) rc = set_error(CPSZ_ERR_CUDA, "event");
+  if (rc == CPSZ_OK && cudaEventSynchronize(b) != cudaSuccess) rc = set_error(CPSZ_ERR_CUDA, "event sync");
+  float total = 0;
+  if (rc == CPSZ_OK) cudaEventElapsedTime(&total, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  CPSZ_TRY(rc);
+  int flag = 0;
+  CPSZ_CUDA_TRY(cudaMemcpy(&flag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag & FLAG_TIMEOUT) return set_error(CPSZ_ERR_TIMEOUT, "a bounded device-side wait gave up");
+  *ms = total / (float)reps;
+  return CPSZ_OK;
+}
+
 int cpsz_b200_learned_labels_2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2,
                                 const double* eb_analytic, const int32_t* idx, size_t n, int steps, float* t_out) {
   CPSZ_TRY(resolve(ctx));

@@ -50,8 +50,6 @@ constexpr size_t PINNED_BASE = 4096;  // the flag word and scalars live below
 // sub-batch limits: fields per pass (pinned staging) and points per pass (workspace)
 constexpr int BATCH_MAX_FIELDS = 32;
 constexpr size_t BATCH_MAX_POINTS = (size_t)1 << 27;
-// the bound kernel's placement words of every upload band of a pass
-constexpr size_t SCHED_BYTES = (size_t)cpsz_b200_ctx::kUploadChunks * EB2D_SCHED_WORDS * 4;
 
 struct DevBuf {
   // arena sub-allocations of one field
@@ -184,7 +182,7 @@ size_t job_bytes(const Job2D& j) {
   add(4 * N);                           // codes blocks
   add(2 * 65536 * 8);                   // hist codes
   add(2 * (size_t)j.ngroups * j.r2 * 8);  // boundary rows (tagged words)
-  add((size_t)j.ngroups * 8);             // eb2d group counters
+  add(((size_t)j.ngroups + 1) * 8);       // eb2d progress word + group counters
   add(2 * strip_scratch_bytes(j.r1, j.r2));
   add(2 * 4 * N);  // unpred
   add(256 * 9);
@@ -221,7 +219,7 @@ int job_alloc(cpsz_b200_ctx* ctx, Job2D& j) {
     d.hist_codes[f] = (unsigned long long*)A(65536 * 8);
   }
   d.gbnd = (unsigned long long*)A(2 * (size_t)j.ngroups * j.r2 * 8);
-  d.band = (unsigned long long*)A((size_t)j.ngroups * 8);
+  d.band = (unsigned long long*)A(((size_t)j.ngroups + 1) * 8);
   for (int f = 0; f < 2; f++) {
     d.strip[f] = A(strip_scratch_bytes(j.r1, j.r2));
     d.unpred[f] = (float*)A(4 * N);
@@ -385,9 +383,7 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   int total_groups = 0;
   for (const Job2D& j : jobs) total_groups += j.ngroups;
   WaveItem* d_items = (WaveItem*)arena_alloc(ctx, 2 * (size_t)total_groups * sizeof(WaveItem));
-  // per upload band, the bound kernel's CTA placement and tile counter (overlap only)
-  unsigned int* sched = (unsigned int*)arena_alloc(ctx, SCHED_BYTES);
-  if (!d_items || !sched) return set_error(CPSZ_ERR_NOMEM, "workspace layout overflow");
+  if (!d_items) return set_error(CPSZ_ERR_NOMEM, "workspace layout overflow");
   for (Job2D& j : jobs) CPSZ_TRY(job_alloc(ctx, j));
   for (int k = 0; k < nj; k++) {
     uint8_t* base = (uint8_t*)ctx->pinned + PINNED_BASE + (size_t)k * JOB_PINNED;
@@ -425,10 +421,7 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     for (int f = 0; f < 2; f++)
       CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.gbnd + ((size_t)f * j.ngroups + g0) * j.r2, 0,
                                     (size_t)(j.ngroups - g0) * j.r2 * 8, st));
-    if (overlap) {
-      CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.band, 0, (size_t)j.ngroups * 8, st));
-      CPSZ_CUDA_TRY(cudaMemsetAsync(sched, 0, SCHED_BYTES, st));
-    }
+    if (overlap) CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.band, 0, ((size_t)j.ngroups + 1) * 8, st));
     for (int f = 0; f < 2; f++) {
       WaveField& F = hf[2 * k + f];
       F.pair = j.d.pairs[f];
@@ -443,7 +436,7 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       F.out_pitch = j.r2;
       F.r1 = j.r1;
       F.r2 = j.r2;
-      F.band_done = overlap ? j.d.band : nullptr;
+      F.band_done = overlap ? j.d.band + 1 : nullptr;
       F.band_wait_ns = ctx->band_wait_ns;
       F.band_extra = ctx->band_unreachable ? 1 : 0;
       r1v[2 * k + f] = j.r1;
@@ -468,17 +461,22 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     }
   } hi_drain;
   if (overlap) {
-    // The consumer (the wavefront on the high-priority stream) depends on the
-    // setup above only, and is enqueued after its producer (eb2d, stage 1):
-    // kernels that run one after the other -- under a tool that serialises
-    // launches, or on a device too busy to co-schedule them -- then run the
-    // bounds first and the wavefront finds every group complete.  When they do
-    // run together, the wavefront's CTAs take SMs as eb2d's CTAs retire.
+    // The wavefront (high-priority stream, one CTA per SM) is launched before
+    // its producer eb2d (stage 1), whose CTAs then fill the rest of every SM:
+    // measured at 8192^2, this order takes 7.87 ms a compression against
+    // 8.7-9.5 ms with eb2d enqueued first (eb2d itself runs slower behind a
+    // late wavefront, which then trails it).  The order is not relied on: a
+    // wavefront wait gives up once eb2d shows no progress for a while (a tool
+    // that serialises kernels runs the wavefront alone first), and the pass
+    // then runs its wavefront again after the bounds (see the code trees
+    // below), so serialised execution costs that wait, not a failure.
     CPSZ_TRY(preload_eb2d());
     CPSZ_TRY(preload_wave2d());
     hi_drain.s = ctx->hi;
     CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[3], st));
     CPSZ_CUDA_TRY(cudaStreamWaitEvent(ctx->hi, ctx->ev[3], 0));
+    CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points, ctx->hi, WAVE_BESIDE));
+    CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[4], ctx->hi));
   }
 
   // Stages 1-3 (bounds, wavefront, code histograms, block order) are the
@@ -504,7 +502,7 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       CPSZ_CUDA_TRY(cudaStreamWaitEvent(ctx->aux, ctx->ev[2], 0));
     }
     for (Job2D& j : jobs) {
-      unsigned long long* band = overlap ? j.d.band : nullptr;
+      unsigned long long* band = overlap ? j.d.band + 1 : nullptr;  // [-1]: tiles finished
       if (j.log_form) {
         // offline_log: the fields whole, one id per vertex, then the logs,
         // wavefront pairs and sign maps
@@ -525,8 +523,7 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
                                   j.d.hist_ids, j.d.pairs[0], j.d.pairs[1]));
         else
           CPSZ_TRY(launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
-                               j.d.hist_ids, j.d.pairs[0], j.d.pairs[1], nullptr, 0, -1, band, false,
-                               overlap ? sched : nullptr));
+                               j.d.hist_ids, j.d.pairs[0], j.d.pairs[1], nullptr, 0, -1, band));
       } else {
         // Host input: row chunks go up on the second stream and the bound kernel
         // runs band by band as soon as a band's rows and the row below it are
@@ -548,8 +545,7 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
             return launch_quant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
                                   j.d.hist_ids, j.d.pairs[0], j.d.pairs[1]);
           return launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N, j.d.hist_ids,
-                             j.d.pairs[0], j.d.pairs[1], nullptr, c * R, std::min(j.r1, (c + 1) * R), band, false,
-                             overlap ? sched + (size_t)c * EB2D_SCHED_WORDS : nullptr);
+                             j.d.pairs[0], j.d.pairs[1], nullptr, c * R, std::min(j.r1, (c + 1) * R), band);
         };
         for (int c = 0; c < nch; c++) {
           const size_t off = (size_t)c * R * j.r2;
@@ -561,11 +557,6 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
         }
       }
       CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_hist_ids, j.d.hist_ids, 256 * 8, cudaMemcpyDeviceToHost, st));
-    }
-    if (overlap) {
-      // every producer launch is enqueued: now the consumer beside them
-      CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points, ctx->hi, WAVE_BESIDE));
-      CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[4], ctx->hi));
     }
     CPSZ_CUDA_TRY(record(ctx->ev[0]));
     if (tap && tap->ids)
@@ -849,7 +840,7 @@ size_t pass_bytes(const std::vector<Job2D>& jobs) {
     total_groups += j.ngroups;
   }
   bytes += align_up(QUANT_TAB_MAX * 8, 256) + 256 + 512 + align_up(2 * jobs.size() * sizeof(WaveField), 256) + 256 +
-           align_up(2 * (size_t)total_groups * sizeof(WaveItem), 256) + 256 + align_up(SCHED_BYTES, 256) + 256;
+           align_up(2 * (size_t)total_groups * sizeof(WaveItem), 256) + 256;
   return bytes;
 }
 

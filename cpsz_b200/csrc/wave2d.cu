@@ -47,7 +47,9 @@
 //    count is complete (one thread polls with ld.acquire.gpu, every thread
 //    then acquires before its first load).  Such a launch keeps to one CTA per
 //    SM, so each SM keeps room for the producer's CTAs and the producer
-//    cannot be starved by waiting consumers.
+//    cannot be starved by waiting consumers.  The wait ends with FLAG_TIMEOUT
+//    when the producer has finished no tile for a while (it is not running
+//    beside it), and the host then runs the wavefront again after it.
 //
 // Tagged words are 64-bit (column + 1) << 32 | float bits, written and read as
 // single aligned 64-bit accesses, so a reader that sees the expected tag holds
@@ -81,7 +83,10 @@ constexpr int RING = 128;
 constexpr int TP = 33;         // tile row pitch (elements)
 constexpr int TILE = 32 * TP;  // elements per tile
 constexpr long long SPIN_LIMIT = 1ll << 22;
-constexpr long long BAND_WAIT_NS = 4000000000ll;  // producer wait limit (4 s)
+// A wait for the producer gives up after this long without any of its tiles
+// finishing (it is not running: a tool serialises kernels, or the device is
+// held by other work); the host then runs the wavefront again after it.
+constexpr long long BAND_WAIT_NS = 50000000ll;  // 50 ms
 
 __device__ __forceinline__ unsigned long long tagged(int c, float v) {
   return ((unsigned long long)(unsigned)(c + 1) << 32) | (unsigned long long)__float_as_uint(v);
@@ -385,11 +390,20 @@ __device__ __forceinline__ void wave2d_body(const WaveField* __restrict__ fields
           F.band_extra;
       const long long limit = F.band_wait_ns > 0 ? F.band_wait_ns : BAND_WAIT_NS;
       if (threadIdx.x == 0 && ld_acquire(cnt) < target) {
-        const long long t0 = globaltimer_ns();
+        // progress: the producer's count of finished tiles (band_done[-1])
+        const unsigned long long* tiles = F.band_done - 1;
+        unsigned long long seen = ld_acquire(tiles);
+        long long t_seen = globaltimer_ns();
         while (ld_acquire(cnt) < target) {
           // a wait that already gave up (this launch or the producer failed)
           // ends every later wait at once
-          if ((*(volatile int*)flag & FLAG_TIMEOUT) || globaltimer_ns() - t0 > limit) {
+          if (*(volatile int*)flag & FLAG_TIMEOUT) break;
+          const unsigned long long now_tiles = ld_acquire(tiles);
+          const long long now = globaltimer_ns();
+          if (now_tiles != seen) {
+            seen = now_tiles;
+            t_seen = now;
+          } else if (now - t_seen > limit) {
             atomicOr(flag, FLAG_TIMEOUT);
             break;
           }

@@ -52,9 +52,10 @@ int cpsz_b200_ctx_kernel_launches(cpsz_b200_ctx* ctx, uint64_t* count);
 int cpsz_b200_ctx_graph_stats(cpsz_b200_ctx* ctx, uint64_t* captures, uint64_t* replays);
 /* Single-field compressions run the Lorenzo wavefront beside the bound kernel,
  * each row group waiting (bounded) for its bounds.  If such a wait gives up
- * (the bound kernel was held back, e.g. on a saturated or time-sliced device),
- * the pass runs its wavefront again after the bounds and still returns the
- * same blob; this counts those re-runs on the context. */
+ * (the bound kernel did not run beside it: a tool that serialises kernels, a
+ * saturated or time-sliced device), the pass runs its wavefront again after
+ * the bounds and still returns the same blob; this counts those re-runs on the
+ * context. */
 int cpsz_b200_ctx_wave_reruns(cpsz_b200_ctx* ctx, uint64_t* reruns);
 /* Stream of the context as an opaque handle (a cudaStream_t). */
 int cpsz_b200_ctx_stream(cpsz_b200_ctx* ctx, void** stream);
@@ -70,9 +71,10 @@ int cpsz_b200_ctx_stage_times(cpsz_b200_ctx* ctx, int max_stages, const char** n
  * threads, 32x8/128, 64x8/256, 32x32/256, 64x16/256, 32x16/128),
  * "wave2d.ctas_per_sm" (0 = occupancy limit), "eb3d.fill", "eb3d.min_chunk",
  * "h2d.chunks", "wave2d.overlap" (1: the Lorenzo wavefront runs beside the
- * bound kernel, enqueued after it, so tools that serialise kernels run it
- * after the bounds; 0: after the bounds on every SM -- also forced by the
- * environment variable CPSZ_B200_OVERLAP=0).  An entry applies to fields of
+ * bound kernel; under tools that serialise kernels its waits give up after
+ * 50 ms without progress and the pass re-runs it after the bounds; 0: after
+ * the bounds on every SM -- also forced by the environment variable
+ * CPSZ_B200_OVERLAP=0).  An entry applies to fields of
  * >= min_points points; the
  * largest such threshold wins.  The first cpsz_b200_ctx_create() loads
  * $CPSZ_B200_TUNING (empty or "none": no table) or else tuning_b200.json of the
@@ -180,6 +182,12 @@ int cpsz_b200_mlp_features_2d(cpsz_b200_ctx* ctx, const float* U, const float* V
  * the learned compression does.  Host or device buffers; y gets r1*r2 floats. */
 int cpsz_b200_mlp_propose_2d(cpsz_b200_mlp* mlp, const float* U, const float* V, size_t r1, size_t r2,
                              const double* eb_analytic, float* y);
+/* Diagnostics: the proposer's forward pass over every vertex of a field
+ * (features fused, both layers on the tensor cores), timed with CUDA events on
+ * the context's stream: *ms = mean of `reps` launches after one warm-up.
+ * U, V, eb_analytic: device memory. */
+int cpsz_b200_debug_mlp_forward_ms(cpsz_b200_mlp* mlp, const float* U, const float* V, size_t r1, size_t r2,
+                                   const double* eb_analytic, int reps, float* ms);
 /* Training labels: per vertex the largest log2 multiplier (bisection, `steps`
  * halvings of [0, 16]) that keeps its incident cells' CPs when the vertex
  * alone moves to any corner of its bound box. */
@@ -291,9 +299,10 @@ int cpsz_b200_debug_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, siz
  * 255 = bound not positive).  Host buffers. */
 int cpsz_b200_debug_eb3d(cpsz_b200_ctx* ctx, const float* U, const float* V, const float* W, size_t r1, size_t r2,
                          size_t r3, double max_pwr_eb, double* eb_out, uint8_t* id_codes);
-/* The wavefront's per-group wait for the bound kernel: limit wait_ns (0 = the
- * default of 4 s); unreachable != 0 makes every such wait run out (its target
- * is one point more than the group holds), which exercises the re-run path
+/* The wavefront's per-group wait for the bound kernel gives up once the bound
+ * kernel has finished no tile for wait_ns (0 = the default of 50 ms);
+ * unreachable != 0 makes every such wait run out (its target is one point more
+ * than the group holds), which exercises the re-run path
  * (cpsz_b200_ctx_wave_reruns) without stalling any kernel beyond the limit. */
 int cpsz_b200_debug_band_wait(cpsz_b200_ctx* ctx, long long wait_ns, int unreachable);
 /* Tensor-core self-check: D (128x128 fp32) = A (128x128 bf16 bits) * B^T

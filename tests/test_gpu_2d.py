@@ -163,11 +163,12 @@ def test_gpu_wavefront_wait_that_gives_up_reruns(oracle):
         c.close()
 
 
-def test_gpu_serialised_launches_need_no_rerun(tmp_path):
+def test_gpu_serialised_launches_still_compress(tmp_path):
     """With every launch serialised (CUDA_LAUNCH_BLOCKING=1, as under tools that
-    run kernels one at a time) the bound kernel, enqueued first, completes
-    before the wavefront starts: the blob equals the oracle's and no wait gives
-    up.  Runs in a child process so the setting applies from CUDA's start."""
+    run kernels one at a time) the wavefront waits for bounds that no kernel
+    is computing: its wait gives up after 50 ms without progress, the pass
+    runs the wavefront again after the bounds, and the blob equals the
+    oracle's.  Runs in a child process so the setting applies from CUDA's start."""
     import os
     import subprocess
     import sys
@@ -178,11 +179,14 @@ def test_gpu_serialised_launches_need_no_rerun(tmp_path):
         "import cpsz_b200; from cpsz_b200 import workloads as W; from oracle import Oracle;"
         "from tests._util import assert_blob_equal_2d;"
         "c = cpsz_b200.Context(0); U, V = W.cfg0_like(9, 1100, 900);"
+        "import time; t = time.perf_counter();"
         "a = cpsz_b200.sz_compress_cp_preserve_2d_offline(U, V, max_pwr_eb=0.1, ctx=c);"
+        "print('seconds', time.perf_counter() - t);"
         "assert_blob_equal_2d(a, Oracle().compress_2d(U, V, 0.1));"
         "print('reruns', c.wave_reruns)"
     )
     env = dict(os.environ, CUDA_LAUNCH_BLOCKING="1")
     r = subprocess.run([sys.executable, "-c", code, root], env=env, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr[-2000:]
-    assert "reruns 0" in r.stdout
+    assert "reruns 1" in r.stdout
+    assert float(r.stdout.split("seconds")[1].split()[0]) < 3.0  # the wait, not a 4-second timeout

@@ -24,6 +24,16 @@ def _fields():
     # few distinct values: many equal products, zero sums and exact ties
     yield "plateaus", (rng.integers(-3, 4, (600, 800)).astype(np.float32),
                        rng.integers(-3, 4, (600, 800)).astype(np.float32))
+    # V nearly proportional to U: the flag sums s_k and det nearly cancel
+    # (undecided flags take the exact path)
+    yield "near_degenerate", (U[:700, :800], U[:700, :800] * np.float32(1.5) +
+                              np.float32(1e-6) * V[:700, :800])
+    # magnitudes spread over 60 binades (sums near the float filter's range limits)
+    mag = np.ldexp(1.0, rng.integers(-40, 21, (600, 700))).astype(np.float32)
+    yield "spread", (mag * rng.standard_normal((600, 700)).astype(np.float32),
+                     np.roll(mag, 3, axis=1) * rng.standard_normal((600, 700)).astype(np.float32))
+    # products in the float subnormal range
+    yield "subnormal_products", (U[:500, :600] * np.float32(1e-20), V[:500, :600] * np.float32(3e-21))
     # powers of two: bounds land on exact binary fractions near thresholds
     yield "pow2", (np.ldexp(1.0, rng.integers(-8, 8, (512, 512))).astype(np.float32) *
                    rng.choice([-1, 1], (512, 512)).astype(np.float32),
