@@ -54,6 +54,9 @@ WORKLOADS = {
     "batch_256x2d_cfg3": ("batch", None, None, "cfg3"),
     # the cfg1 field with learned bounds (trained proposer, fallback loop to 0 CP differences)
     "learned_2d_8192x8192_eb0.1": ("learned", (8192, 8192), 0.1, "cfg1"),
+    # profiling-size case of the learned path: a held-out field of the proposer's training
+    # generator (cfg0 density, sigma 40) at 2048^2 (34 MB of input)
+    "learned_2d_2048x2048_eb0.1": ("learned", (2048, 2048), 0.1, "cfg0like_heldout"),
 }
 DEFAULT = "2d_8192x8192_eb0.1"
 
@@ -142,6 +145,8 @@ def make_fields(workload: str, seed_offset: int = 0):
         return W.cfg0(0 + seed_offset), eb
     if gen == "cfg0like":
         return W.cfg0_like(5 + seed_offset, *shape), eb
+    if gen == "cfg0like_heldout":
+        return W.cfg0_like(123457 + seed_offset, *shape), eb
     if gen == "cfg2":
         return W.cfg2(2 + seed_offset, shape[0]), eb
     raise KeyError(workload)
@@ -165,9 +170,10 @@ def oracle_fields(workload: str, seed_offset: int = 0):
         return O.field_2d(1 + seed_offset, 8192, 8192, 2000, 60.0), eb
     if gen == "cfg0":
         return O.field_2d(0 + seed_offset, 2400, 3600, 200, 40.0), eb
-    if gen == "cfg0like":
+    if gen in ("cfg0like", "cfg0like_heldout"):
         r1, r2 = shape
-        return O.field_2d(5 + seed_offset, r1, r2, max(1, round(200 / (2400 * 3600) * r1 * r2)), 40.0), eb
+        seed = (5 if gen == "cfg0like" else 123457) + seed_offset
+        return O.field_2d(seed, r1, r2, max(1, round(200 / (2400 * 3600) * r1 * r2)), 40.0), eb
     if gen == "cfg2":
         return O.field_3d(2 + seed_offset, *shape, 500, 20.0), eb
     raise KeyError(workload)
@@ -463,9 +469,9 @@ def run_product(args, rank, world, device):
            "wave2d_compress": 4 * comps * n + comps * n + 2 * comps * n,  # fields + ids in, u16 codes out
            "eb3d": 4 * 3 * n + n, "wave3d_compress": 0}  # read fields, write one id byte
     # DRAM bytes per point of a launch, read + write, from one ncu capture of the
-    # kernel on the 4096^2 case (394.0 MB for 16.8 M vertices), scaled to this
+    # kernel on the 4096^2 case (389.4 MB for 16.8 M vertices), scaled to this
     # launch by its points
-    traffic_per_point = {"eb2d": (135.14496e6 + 258.857216e6) / 4096 ** 2}
+    traffic_per_point = {"eb2d": (134.725632e6 + 254.642176e6) / 4096 ** 2}
     dom = max((k for k in stages if k in alg and alg[k]), key=lambda k: stages[k], default=None)
     peak, peak_kind = measured_peaks()
     roof = None
@@ -510,7 +516,7 @@ def run_learned(args, rank, world, device):
     from cpsz_b200 import learned
 
     kind, shape, eb, _ = WORKLOADS[args.workload]
-    fields, eb = make_fields("2d_8192x8192_eb0.1", seed_offset=rank)
+    fields, eb = make_fields(args.workload, seed_offset=rank)
     raw = sum(a.nbytes for a in fields)
     ctx = cpsz_b200.Context(device)
     mlp = learned.load(ctx)
@@ -553,14 +559,17 @@ def run_learned(args, rank, world, device):
     flops = 2.0 * (128 * 128 * 2 + 128) * n
     tf = flops / (fwd_ms / 1e3) / 1e12
     peak = _bf16_peak()
+    # DRAM bytes of a launch from one ncu capture on the 2048^2 case (72.5 MB for
+    # 4.19 M vertices: fields and exact bounds in, proposals out), scaled by points
+    traffic = round((67.25376e6 + 5.274112e6) / 2048 ** 2 * n)
     roofline = {"bound": "tensor", "kernel": "mlp_fwd (features fused)", "achieved": round(tf, 2),
-                "peak": peak[0], "unit": "TFLOP/s", "frac": round(tf / peak[0], 4), "traffic": None,
+                "peak": peak[0], "unit": "TFLOP/s", "frac": round(tf / peak[0], 4), "traffic": traffic,
                 "peak_source": peak[1], "ms_per_launch": round(fwd_ms, 3)}
     # the reference's CPU path on the same field (1 core, the plain method; the
     # reference has no learned form), and its decoder reading the learned blob
     cpu, ref_decodes = None, None
     if rank == 0 and not args.no_cpu_baseline:
-        cpu, _ = cpu_baseline_single("2d_8192x8192_eb0.1", fields, eb)
+        cpu, _ = cpu_baseline_single(args.workload, fields, eb)
         import oracle
 
         if os.path.exists(oracle.REF_SO):
