@@ -9,6 +9,7 @@
 #include <algorithm>
 
 #include "kernels.h"
+#include "lookback.cuh"
 
 namespace cpsz {
 
@@ -174,29 +175,13 @@ __device__ __forceinline__ StripSplit strip_split(const StripGeom& g, const uint
   return sp;
 }
 
-// Decoupled look-back (Merrill & Garland, "Single-pass Parallel Prefix Scan
-// with Decoupled Look-back", 2016) over the strips' published unpredictable
-// counts.  A CTA takes the next strip in ticket order (tickets go out in the
-// order CTAs start, so every earlier strip belongs to a CTA that is running or
-// done).  Status words: 2-bit state (0 = not yet, AGG = the strip's own count,
-// PRE = inclusive prefix) over a 62-bit count.  A word carries its count
-// itself and nothing else is read on its strength, so relaxed loads and
-// stores suffice; every lane keeps LB_DEPTH loads in flight, so one L2 round
-// trip covers 32 * LB_DEPTH strips (with one load per lane the look-back
-// could not keep pace with tens of thousands of strips: windows of in-flight
-// strips that had not yet published their prefix grew to hundreds).
-constexpr unsigned long long ST_AGG = 1ull << 62, ST_PRE = 2ull << 62, ST_VAL = (1ull << 62) - 1;
+// The strips' unpredictable counts are summed by decoupled look-back
+// (lookback.cuh): a CTA takes the next strip in ticket order, so every
+// earlier strip belongs to a CTA that is running or done.  One load per lane
+// could not keep pace with tens of thousands of strips (windows of in-flight
+// strips that had not yet published their prefix grew to hundreds), hence
+// the look-back's several windows per round trip.
 constexpr long long LOOKBACK_SPIN = 1ll << 24;
-constexpr int LB_DEPTH = 4;
-
-__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long* p) {
-  unsigned long long v;
-  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_relaxed64(unsigned long long* p, unsigned long long v) {
-  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
 
 // Warp 0 of a strip's CTA: the exclusive prefix of its blocks' zero counts
 // (bpre), its own count published, and the count of all earlier strips
@@ -214,52 +199,8 @@ __device__ __forceinline__ void strip_prefix(unsigned long long* status, unsigne
   }
   bpre[lane] = inc - v;
   const unsigned long long tot = __shfl_sync(FULLM, inc, 31);
-  unsigned long long excl = 0;
-  if (s == 0) {
-    if (lane == 0) st_relaxed64(&status[0], ST_PRE | tot);
-  } else {
-    if (lane == 0) st_relaxed64(&status[s], ST_AGG | tot);
-    long long p = (long long)s - 1;  // the nearest strip not yet summed
-    long long spins = 0;
-    bool done = false;
-    while (!done) {
-      unsigned long long w[LB_DEPTH];
-#pragma unroll
-      for (int m = 0; m < LB_DEPTH; m++) {
-        const long long q = p - 32 * m - lane;
-        w[m] = q >= 0 ? ld_relaxed64(&status[q]) : ST_PRE;  // before strip 0: prefix 0
-      }
-      // the windows in order, nearest first; a window with an unpublished
-      // strip before its nearest prefix is read again from there
-      bool wait = false;
-#pragma unroll
-      for (int m = 0; m < LB_DEPTH; m++) {
-        if (done || wait) continue;
-        const unsigned int pre_m = __ballot_sync(FULLM, (w[m] & ~ST_VAL) == ST_PRE);
-        const unsigned int none_m = __ballot_sync(FULLM, (w[m] & ~ST_VAL) == 0);
-        const int last = pre_m ? __ffs(pre_m) - 1 : 31;  // the nearest prefix, or the whole window
-        const unsigned int upto = last == 31 ? FULLM : ((1u << (last + 1)) - 1u);
-        if (none_m & upto) {
-          wait = true;
-          continue;
-        }
-        unsigned long long add = lane <= last ? (w[m] & ST_VAL) : 0ull;
-#pragma unroll
-        for (int d = 16; d > 0; d >>= 1) add += __shfl_xor_sync(FULLM, add, d);
-        excl += add;
-        p -= 32;
-        done = pre_m != 0;
-      }
-      if (wait) {
-        if (++spins > LOOKBACK_SPIN) {
-          if (lane == 0) atomicOr(flag, FLAG_TIMEOUT);
-          break;
-        }
-        __nanosleep(64);
-      }
-    }
-    if (lane == 0) st_relaxed64(&status[s], ST_PRE | (excl + tot));
-  }
+  if (lane == 0) lookback_publish(status, s, tot);
+  const unsigned long long excl = lookback_warp(status, s, tot, lane, LOOKBACK_SPIN, flag);
   if (lane == 0) {
     *s_excl = excl;
     if (s == ns - 1) reinterpret_cast<unsigned int*>(status + ns)[1] = (unsigned int)(excl + tot);

@@ -66,17 +66,15 @@ int cpsz_b200_compress_2d_offline_f32_into(cpsz_b200_ctx* ctx, const float* U, c
   if (!out || !blob_size) return set_error(CPSZ_ERR_INVALID, "null output pointer");
   RESOLVE(ctx);
   Blob2D b;
-  if (host_kind(out) != HOST_DEVICE) {
-    // host memory: the sections are written there as they are produced
-    CPSZ_TRY(compress_2d(ctx, U, V, r1, r2, max_pwr_eb, &b, nullptr, nullptr, out, out_cap));
-    *blob_size = b.size;
-    CPSZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    return CPSZ_OK;
-  }
-  CPSZ_TRY(compress_2d(ctx, U, V, r1, r2, max_pwr_eb, &b, nullptr));
+  // host memory: the sections are written there as they are produced; a
+  // device buffer: the blob is built in place when the buffer has room for
+  // the blob's bound, else copied there
+  CPSZ_TRY(compress_2d(ctx, U, V, r1, r2, max_pwr_eb, &b, nullptr, nullptr, out, out_cap));
   *blob_size = b.size;
-  if (b.size > out_cap) return set_error(CPSZ_ERR_INVALID, "output capacity %zu < blob size %zu", out_cap, b.size);
-  CPSZ_TRY(copy_out(ctx, out, b.d_blob, b.size));
+  if (b.d_blob && b.d_blob != out) {
+    if (b.size > out_cap) return set_error(CPSZ_ERR_INVALID, "output capacity %zu < blob size %zu", out_cap, b.size);
+    CPSZ_TRY(copy_out(ctx, out, b.d_blob, b.size));
+  }
   CPSZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return CPSZ_OK;
 }
@@ -119,16 +117,12 @@ int cpsz_b200_compress_2d_offline_log_f32_into(cpsz_b200_ctx* ctx, const float* 
   if (!out || !blob_size) return set_error(CPSZ_ERR_INVALID, "null output pointer");
   RESOLVE(ctx);
   Blob2D b;
-  if (host_kind(out) != HOST_DEVICE) {
-    CPSZ_TRY(compress_2d(ctx, U, V, r1, r2, max_pwr_eb, &b, nullptr, nullptr, out, out_cap, true));
-    *blob_size = b.size;
-    CPSZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
-    return CPSZ_OK;
-  }
-  CPSZ_TRY(compress_2d(ctx, U, V, r1, r2, max_pwr_eb, &b, nullptr, nullptr, nullptr, 0, true));
+  CPSZ_TRY(compress_2d(ctx, U, V, r1, r2, max_pwr_eb, &b, nullptr, nullptr, out, out_cap, true));
   *blob_size = b.size;
-  if (b.size > out_cap) return set_error(CPSZ_ERR_INVALID, "output capacity %zu < blob size %zu", out_cap, b.size);
-  CPSZ_TRY(copy_out(ctx, out, b.d_blob, b.size));
+  if (b.d_blob && b.d_blob != out) {
+    if (b.size > out_cap) return set_error(CPSZ_ERR_INVALID, "output capacity %zu < blob size %zu", out_cap, b.size);
+    CPSZ_TRY(copy_out(ctx, out, b.d_blob, b.size));
+  }
   CPSZ_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return CPSZ_OK;
 }
@@ -260,8 +254,7 @@ int cpsz_b200_huffman_codebook(const uint64_t* hist, size_t bins, size_t state_n
   if (!hist || !bins || !tree_size) return set_error(CPSZ_ERR_INVALID, "null histogram or tree_size");
   HuffCodebook cb;
   if (!huff_build((const unsigned long long*)hist, bins, state_num, &cb)) return CPSZ_ERR_INVALID;
-  if (code) memcpy(code, cb.code.data(), bins * 8);
-  if (len) memcpy(len, cb.len.data(), bins);
+  huff_tables(cb, bins, (unsigned long long*)code, len);
   if (tree_bytes) {
     if (*tree_size < cb.tree_bytes.size())
       return set_error(CPSZ_ERR_INVALID, "tree buffer of %zu bytes < %zu", *tree_size, cb.tree_bytes.size());

@@ -3,14 +3,14 @@
 // self-synchronising parallel decoder.
 //
 // Encoder.  The reference's packer (encode, src/sz_huffman.cpp:217-320) emits
-// the MSB-first concatenation of the codes, zero padded to a byte.  Here a CTA
-// owns 4096 consecutive symbols: pass 1 sums code lengths per CTA, a scan gives
-// every CTA its starting bit, pass 2 re-reads the symbols, scans the lengths
-// inside the CTA, ORs the codes into a shared-memory word buffer aligned to
-// the global 32-bit word grid, and stores it with plain coalesced stores except
-// for the two edge words, which are shared with the neighbouring CTAs and use
-// atomicOr.  Words are stored byte-swapped so memory holds the big-endian byte
-// stream the reference writes.
+// the MSB-first concatenation of the codes, zero padded to a byte.  Here one
+// persistent kernel reads every symbol once: a tile of 8192 consecutive
+// symbols sums and scans its code lengths, finds its starting bit by a
+// decoupled look-back over the earlier tiles' published bit counts, packs its
+// codes into a shared-memory word buffer aligned to the global 32-bit word
+// grid and stores it with coalesced stores (atomicOr for the two edge words,
+// shared with the neighbouring tiles).  Words are stored byte-swapped so
+// memory holds the big-endian byte stream the reference writes.
 //
 // Decoder.  The reference stream has no chunk index, so decoding uses
 // self-synchronisation (after Weissenberger & Schmidt, ICPP 2018): the stream
@@ -23,44 +23,291 @@
 // symbols.  Lookup is a 2^12-entry first-level table with a bit-serial tree
 // walk for longer codes.
 #include "kernels.h"
+#include "lookback.cuh"
 
 namespace cpsz {
 
 namespace {
 
-constexpr int ENC_NT = 256;
-constexpr int ENC_PER_THREAD = 16;
-constexpr int ENC_PER_CTA = ENC_NT * ENC_PER_THREAD;
+// ---- encoder: one pass with decoupled look-back --------------------------------------
+constexpr int PK_NT = 256;                  // threads per CTA
+constexpr int PK_SPT = 32;                  // symbols per thread (a contiguous run)
+constexpr int PK_TILE = PK_NT * PK_SPT;     // symbols per tile
+constexpr int PK_WORDS = PK_TILE;           // staged words of a tile whose codes are at most 32 bits
+constexpr int PK_WIN = 1536;                // codebook entries cached in shared memory: u16 symbols
+constexpr int PK_WIN_LO = 32768 - PK_WIN / 2;  // [PK_WIN_LO, PK_WIN_LO + PK_WIN) (all 256 for u8)
+constexpr int PK_CTAS_PER_SM = 4;
+constexpr long long PK_SPIN_LIMIT = 1ll << 22;  // look-back polls before giving up (FLAG_TIMEOUT)
 
 __device__ __forceinline__ uint32_t bswap32(uint32_t x) { return __byte_perm(x, 0, 0x0123); }
 
 template <class Sym>
-__device__ __forceinline__ int sym_at(const Sym* s, size_t i, bool map_id_zero) {
-  int v = (int)s[i];
-  if (map_id_zero && v == ID_ZERO) v = 0;
-  return v;
+struct PackWin {
+  static constexpr int lo = sizeof(Sym) == 1 ? 0 : PK_WIN_LO;
+  static constexpr int n = sizeof(Sym) == 1 ? 256 : PK_WIN;
+  static constexpr int per_word = 4 / (int)sizeof(Sym);  // symbols per 32-bit register
+};
+
+struct PackShared {
+  uint32_t words[PK_WORDS];     // the tile's packed bits from its first bit (tile-relative)
+  uint32_t lcode[PK_WIN];       // codes of at most 32 bits, left-aligned (0 for longer codes)
+  uint8_t len[PK_WIN];
+  unsigned int warp_bits[PK_NT / 32];
+  unsigned long long excl;
+  unsigned int tile;
+};
+
+// Code length of symbol s (the cached window, else the global table).
+template <class Sym>
+__device__ __forceinline__ unsigned pk_len(const PackShared& sh, unsigned s, const uint8_t* __restrict__ len) {
+  if (sizeof(Sym) == 1) return sh.len[s];
+  const unsigned d = s - (unsigned)PackWin<Sym>::lo;
+  return d < (unsigned)PackWin<Sym>::n ? sh.len[d] : __ldg(len + s);
+}
+// Left-aligned code of symbol s whose length l is at most 32.
+template <class Sym>
+__device__ __forceinline__ uint32_t pk_lcode(const PackShared& sh, unsigned s, unsigned l,
+                                             const unsigned long long* __restrict__ code) {
+  if (sizeof(Sym) == 1) return sh.lcode[s];
+  const unsigned d = s - (unsigned)PackWin<Sym>::lo;
+  if (d < (unsigned)PackWin<Sym>::n) return sh.lcode[d];
+  return l ? (uint32_t)(__ldg(code + s) << (32 - l)) : 0u;
+}
+
+// Persistent packer.  Tiles of PK_TILE symbols are taken in order from a
+// ticket; thread t of a tile owns its symbols t*32 .. t*32+31.  Per tile:
+//   1. code lengths (kept in registers) summed and scanned in the CTA; the
+//      tile's bit count is published for the look-back (lookback.cuh);
+//   2. the codes are packed tile-relative into the shared word buffer: each
+//      thread appends its codes to a 64-bit register and stores every word
+//      it completes (a word is completed by exactly one thread, which also
+//      zeroes the bits of earlier threads in it); after a barrier each
+//      thread ORs in its last, partial word;
+//   3. warp 0 finds the tile's starting bit (by now the predecessors have
+//      mostly published); the buffer goes out shifted onto the global word
+//      grid with coalesced stores, the two edge words (shared with the
+//      neighbouring tiles) by atomicOr.
+// A tile with a code longer than 32 bits (possible only for skewed
+// histograms) finds its starting bit first and ORs its words straight into
+// global memory.  The stream starts at bit `bit0` (0-31) of out[0].
+template <class Sym, bool MAP0>
+__global__ void __launch_bounds__(PK_NT, PK_CTAS_PER_SM)
+    pack_kernel(const Sym* __restrict__ sym, size_t n, const unsigned long long* __restrict__ code,
+                const uint8_t* __restrict__ len, int nsym, uint32_t* __restrict__ out, size_t cap_words, int bit0,
+                unsigned long long* __restrict__ state, unsigned int* __restrict__ ticket, unsigned long long ntiles,
+                unsigned long long* __restrict__ d_total, int* __restrict__ flag) {
+  using W = PackWin<Sym>;
+  constexpr int NW = PK_SPT / W::per_word;  // registers of packed symbols
+  constexpr int SB = 8 * (int)sizeof(Sym);
+  constexpr unsigned SMASK = sizeof(Sym) == 1 ? 0xffu : 0xffffu;
+  __shared__ PackShared sh;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int i = tid; i < W::n; i += PK_NT) {
+    const int s = W::lo + i;
+    const unsigned l = s < nsym ? len[s] : 0u;
+    sh.len[i] = (uint8_t)l;
+    sh.lcode[i] = (l >= 1 && l <= 32) ? (uint32_t)(code[s] << (32 - l)) : 0u;
+  }
+  const bool vec_ok = ((uintptr_t)sym & 15) == 0;
+  for (;;) {
+    if (tid == 0) sh.tile = atomicAdd(ticket, 1u);
+    __syncthreads();  // also: the codebook window is in place
+    const unsigned long long tile = sh.tile;
+    if (tile >= ntiles) break;
+    const size_t my = (size_t)tile * PK_TILE + (size_t)tid * PK_SPT;
+    const int cnt = my >= n ? 0 : (int)((n - my) < (size_t)PK_SPT ? (n - my) : (size_t)PK_SPT);
+    uint32_t w[NW];
+    if (cnt == PK_SPT && vec_ok) {
+      const uint4* src = reinterpret_cast<const uint4*>(sym + my);
+#pragma unroll
+      for (int q = 0; q < NW / 4; q++) {
+        const uint4 v = __ldcs(src + q);
+        w[4 * q] = v.x;
+        w[4 * q + 1] = v.y;
+        w[4 * q + 2] = v.z;
+        w[4 * q + 3] = v.w;
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < NW; q++) w[q] = 0;
+#pragma unroll
+      for (int k = 0; k < PK_SPT; k++)
+        if (k < cnt) w[k / W::per_word] |= (uint32_t)sym[my + k] << (SB * (k % W::per_word));
+    }
+    auto sym_k = [&](int k) -> unsigned {
+      unsigned s = (w[k / W::per_word] >> (SB * (k % W::per_word))) & SMASK;
+      if (MAP0 && s == ID_ZERO) s = 0;
+      return s;
+    };
+    // 1. lengths, 4 to a register
+    uint32_t lw[PK_SPT / 4];
+    unsigned int bits = 0;
+    bool lng = false;
+#pragma unroll
+    for (int k = 0; k < PK_SPT; k++) {
+      const unsigned l = k < cnt ? pk_len<Sym>(sh, sym_k(k), len) : 0u;
+      bits += l;
+      lng |= l > 32;
+      lw[k / 4] = (k % 4) ? (lw[k / 4] | (l << (8 * (k % 4)))) : l;
+    }
+    unsigned int x = bits;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) sh.warp_bits[warp] = x;
+    const bool any_long = __syncthreads_or(lng) != 0;
+    unsigned int wpre = 0, agg = 0;
+#pragma unroll
+    for (int q = 0; q < PK_NT / 32; q++) {
+      const unsigned int v = sh.warp_bits[q];
+      wpre += q < warp ? v : 0u;
+      agg += v;
+    }
+    const unsigned int tpre = wpre + x - bits;
+    auto len_k = [&](int k) -> unsigned { return (lw[k / 4] >> (8 * (k % 4))) & 255u; };
+    unsigned long long excl;
+
+    if (!any_long) {
+      // 2. tile-relative packing; nobody completes the last partial word
+      if (tid == 0) {
+        lookback_publish(state, tile, agg);
+        if (agg & 31) sh.words[agg >> 5] = 0;
+      }
+      int wi = (int)(tpre >> 5);
+      int nacc = (int)(tpre & 31);  // leading bits of word wi belong to earlier threads
+      unsigned long long acc = 0;   // pending bits, most significant first
+#pragma unroll
+      for (int k = 0; k < PK_SPT; k++) {
+        if (k < cnt) {
+          const unsigned l = len_k(k);
+          acc |= (unsigned long long)pk_lcode<Sym>(sh, sym_k(k), l, code) << (32 - nacc);
+          nacc += (int)l;
+          if (nacc >= 32) {
+            sh.words[wi++] = (uint32_t)(acc >> 32);
+            acc <<= 32;
+            nacc -= 32;
+          }
+        }
+      }
+      __syncthreads();  // every completed word is in place
+      if (bits > 0 && nacc > 0) atomicOr(&sh.words[wi], (uint32_t)(acc >> 32));
+      __syncthreads();
+      // 3. the starting bit, then the words onto the global grid
+      if (warp == 0) {
+        const unsigned long long e = lookback_warp(state, tile, agg, lane, PK_SPIN_LIMIT, flag);
+        if (lane == 0) sh.excl = e;
+      }
+      __syncthreads();
+      excl = sh.excl;
+      const unsigned long long s0 = (unsigned long long)bit0 + excl;
+      const unsigned int shift = (unsigned int)(s0 & 31);
+      const unsigned long long w_lo = s0 >> 5;
+      const int nrel = (int)((agg + 31) >> 5);
+      const int nout = agg ? (int)((shift + agg - 1) >> 5) + 1 : 0;
+      for (int k = tid; k < nout; k += PK_NT) {
+        const unsigned long long g = w_lo + (unsigned long long)k;
+        if (g >= cap_words) {
+          atomicOr(flag, FLAG_OUT_CAPACITY);
+          break;
+        }
+        const uint32_t lo = k < nrel ? sh.words[k] : 0u;
+        const uint32_t hi = k > 0 ? sh.words[k - 1] : 0u;
+        const uint32_t v = bswap32(shift ? __funnelshift_r(lo, hi, shift) : lo);
+        if (k == 0 || k == nout - 1) atomicOr(&out[g], v);  // shared with the neighbouring tiles
+        else out[g] = v;
+      }
+    } else {
+      // a code longer than 32 bits: the starting bit first, every word ORed
+      if (warp == 0) {
+        if (lane == 0) lookback_publish(state, tile, agg);
+        const unsigned long long e = lookback_warp(state, tile, agg, lane, PK_SPIN_LIMIT, flag);
+        if (lane == 0) sh.excl = e;
+      }
+      __syncthreads();
+      excl = sh.excl;
+      const unsigned long long s0 = (unsigned long long)bit0 + excl;
+      const unsigned long long w_lo = s0 >> 5;
+      const unsigned int pos = (unsigned int)(s0 & 31) + tpre;
+      int wi = (int)(pos >> 5);
+      int nacc = (int)(pos & 31);
+      unsigned long long acc = 0;
+      auto emit = [&]() {
+        const unsigned long long g = w_lo + (unsigned long long)wi;
+        if (g < cap_words) atomicOr(&out[g], bswap32((uint32_t)(acc >> 32)));
+        else atomicOr(flag, FLAG_OUT_CAPACITY);
+        wi++;
+      };
+      auto put = [&](uint32_t v, int l) {  // 1 <= l <= 32, v < 2^l
+        acc |= (unsigned long long)v << (64 - nacc - l);
+        nacc += l;
+        if (nacc >= 32) {
+          emit();
+          acc <<= 32;
+          nacc -= 32;
+        }
+      };
+      for (int k = 0; k < cnt; k++) {
+        unsigned s = (unsigned)sym[my + k];
+        if (MAP0 && s == ID_ZERO) s = 0;
+        const int l = __ldg(len + s);
+        const unsigned long long c = __ldg(code + s);
+        if (l > 32) {
+          put((uint32_t)(c >> 32) & (uint32_t)((1ull << (l - 32)) - 1), l - 32);
+          put((uint32_t)c, 32);
+        } else if (l > 0) {
+          put((uint32_t)c & (uint32_t)((1ull << l) - 1), l);
+        }
+      }
+      if (bits > 0 && nacc > 0) emit();
+    }
+    if (tile == ntiles - 1 && tid == 0 && d_total) *d_total = excl + agg;
+    __syncthreads();  // the shared buffers are reused by the next tile
+  }
+}
+
+__global__ void __launch_bounds__(256) codebook_scatter_kernel(const HuffEntry* __restrict__ e, size_t n,
+                                                               unsigned long long* __restrict__ code,
+                                                               uint8_t* __restrict__ len) {
+  const size_t i = (size_t)blockIdx.x * 256 + threadIdx.x;
+  if (i < n) {
+    const HuffEntry v = e[i];
+    code[v.sym] = v.code;
+    len[v.sym] = (uint8_t)v.len;
+  }
+}
+
+size_t pack_scratch_words(size_t n) { return (n + PK_TILE - 1) / PK_TILE + 1; }
+
+// scratch: pack_scratch_words(n) words (ticket, then one state per tile), zeroed here.
+template <class Sym>
+int pack_launch(int num_sms, cudaStream_t st, const Sym* sym, size_t n, bool map_id_zero, HuffEncTable tab,
+                uint32_t* out, size_t out_cap_bytes, int bit0, unsigned long long* scratch,
+                unsigned long long* d_total_bits, int* flag) {
+  if (n == 0) return CPSZ_OK;
+  if (bit0 < 0 || bit0 > 31) return set_error(CPSZ_ERR_INVALID, "internal: stream start bit %d", bit0);
+  const unsigned long long ntiles = (n + PK_TILE - 1) / PK_TILE;
+  CPSZ_CUDA_TRY(cudaMemsetAsync(scratch, 0, (ntiles + 1) * 8, st));
+  const unsigned long long cap = (unsigned long long)num_sms * PK_CTAS_PER_SM;
+  const unsigned grid = (unsigned)(ntiles < cap ? ntiles : cap);
+  auto k = pack_kernel<Sym, false>;
+  if constexpr (sizeof(Sym) == 1) {
+    if (map_id_zero) k = pack_kernel<Sym, true>;
+  }
+  k<<<grid, PK_NT, 0, st>>>(sym, n, tab.code, tab.len, tab.nsym, out, out_cap_bytes / 4, bit0, scratch + 1,
+                            reinterpret_cast<unsigned int*>(scratch), ntiles, d_total_bits, flag);
+  return check_launch("pack_kernel");
 }
 
 template <class Sym>
-__global__ void __launch_bounds__(ENC_NT) enc_count_kernel(const Sym* __restrict__ sym, size_t n, bool map_id_zero,
-                                                           const uint8_t* __restrict__ len,
-                                                           unsigned long long* __restrict__ cta_bits) {
-  __shared__ unsigned int red[ENC_NT / 32];
-  size_t base = (size_t)blockIdx.x * ENC_PER_CTA;
-  unsigned int bits = 0;
-#pragma unroll 4
-  for (int k = 0; k < ENC_PER_THREAD; k++) {
-    size_t i = base + (size_t)k * ENC_NT + threadIdx.x;
-    if (i < n) bits += len[sym_at(sym, i, map_id_zero)];
-  }
-  for (int o = 16; o; o >>= 1) bits += __shfl_xor_sync(0xffffffffu, bits, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = bits;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned long long t = 0;
-    for (int w = 0; w < ENC_NT / 32; w++) t += red[w];
-    cta_bits[blockIdx.x] = t;
-  }
+int encode_impl(cpsz_b200_ctx* ctx, const Sym* sym, size_t n, bool map_id_zero, HuffEncTable tab, uint32_t* out,
+                size_t out_cap_bytes, unsigned long long* d_total_bits, void* tmp, int bit0) {
+  if (n == 0) return CPSZ_OK;
+  CPSZ_TRY(pack_launch<Sym>(ctx->num_sms, ctx->stream, sym, n, map_id_zero, tab, out, out_cap_bytes, bit0,
+                            (unsigned long long*)tmp, d_total_bits, ctx->d_flag));
+  count_launch(ctx);
+  return CPSZ_OK;
 }
 
 // Exclusive scan of the per-CTA bit counts (single CTA, sequential over chunks).
@@ -96,89 +343,6 @@ __global__ void __launch_bounds__(1024) scan_u64_kernel(const unsigned long long
     __syncthreads();
   }
   if (threadIdx.x == 0) out[n] = carry;
-}
-
-template <class Sym>
-__global__ void __launch_bounds__(ENC_NT) enc_write_kernel(const Sym* __restrict__ sym, size_t n, bool map_id_zero,
-                                                           const unsigned long long* __restrict__ code,
-                                                           const uint8_t* __restrict__ len,
-                                                           const unsigned long long* __restrict__ cta_off,
-                                                           uint32_t* __restrict__ out, size_t cap_words,
-                                                           int* __restrict__ flag) {
-  extern __shared__ uint32_t sbuf[];
-  __shared__ unsigned int warp_tot[ENC_NT / 32];
-  const size_t base = (size_t)blockIdx.x * ENC_PER_CTA;
-  const unsigned long long start = cta_off[blockIdx.x];
-  const unsigned long long end = cta_off[blockIdx.x + 1];
-  if (start == end) return;
-  const int shift = (int)(start & 31);
-  const int nwords = (int)(((end - 1) >> 5) - (start >> 5) + 1);
-  for (int k = threadIdx.x; k < nwords; k += ENC_NT) sbuf[k] = 0;
-  // thread t owns symbols base + t*16 .. +15 (contiguous run for in-order packing)
-  const size_t my = base + (size_t)threadIdx.x * ENC_PER_THREAD;
-  int s_loc[ENC_PER_THREAD];
-  unsigned int bits = 0;
-#pragma unroll
-  for (int k = 0; k < ENC_PER_THREAD; k++) {
-    size_t i = my + k;
-    s_loc[k] = (i < n) ? sym_at(sym, i, map_id_zero) : -1;
-    if (s_loc[k] >= 0) bits += len[s_loc[k]];
-  }
-  unsigned int x = bits;
-  for (int o = 1; o < 32; o <<= 1) {
-    unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
-    if ((threadIdx.x & 31) >= o) x += y;
-  }
-  if ((threadIdx.x & 31) == 31) warp_tot[threadIdx.x >> 5] = x;
-  __syncthreads();
-  unsigned int pre = x - bits;
-  for (int w = 0; w < (int)(threadIdx.x >> 5); w++) pre += warp_tot[w];
-  unsigned int pos = (unsigned int)shift + pre;  // bit position inside sbuf
-#pragma unroll
-  for (int k = 0; k < ENC_PER_THREAD; k++) {
-    if (s_loc[k] < 0) break;
-    int l = len[s_loc[k]];
-    unsigned long long c = code[s_loc[k]];
-    while (l > 0) {
-      int wi = pos >> 5, off = pos & 31;
-      int room = 32 - off;
-      int take = l < room ? l : room;
-      uint32_t part = (uint32_t)((c >> (l - take)) & ((take == 32) ? 0xffffffffull : ((1ull << take) - 1)));
-      atomicOr(&sbuf[wi], part << (room - take));
-      pos += take;
-      l -= take;
-    }
-  }
-  __syncthreads();
-  const size_t w0 = start >> 5;
-  for (int k = threadIdx.x; k < nwords; k += ENC_NT) {
-    if (w0 + k >= cap_words) {
-      atomicOr(flag, FLAG_OUT_CAPACITY);
-      break;
-    }
-    uint32_t v = bswap32(sbuf[k]);
-    if (k == 0 || k == nwords - 1) atomicOr(&out[w0 + k], v);
-    else out[w0 + k] = v;
-  }
-}
-
-template <class Sym>
-int encode_impl(cpsz_b200_ctx* ctx, const Sym* sym, size_t n, bool map_id_zero, HuffEncTable tab, uint32_t* out,
-                size_t out_cap_bytes, unsigned long long* d_total_bits, void* tmp) {
-  if (n == 0) return CPSZ_OK;
-  size_t nb = (n + ENC_PER_CTA - 1) / ENC_PER_CTA;
-  unsigned long long* cta_bits = (unsigned long long*)tmp;
-  unsigned long long* cta_off = cta_bits + align_up(nb, 32);
-  enc_count_kernel<Sym><<<(unsigned)nb, ENC_NT, 0, ctx->stream>>>(sym, n, map_id_zero, tab.len, cta_bits);
-  scan_u64_kernel<<<1, 1024, 0, ctx->stream>>>(cta_bits, cta_off, nb);
-  // shared word buffer for the worst case of 64-bit codes (32 KB)
-  size_t smem = ((size_t)ENC_PER_CTA * 64) / 32 * 4 + 16;
-  enc_write_kernel<Sym><<<(unsigned)nb, ENC_NT, smem, ctx->stream>>>(sym, n, map_id_zero, tab.code, tab.len,
-                                                                       cta_off, out, out_cap_bytes / 4, ctx->d_flag);
-  if (d_total_bits)
-    cudaMemcpyAsync(d_total_bits, cta_off + nb, sizeof(unsigned long long), cudaMemcpyDeviceToDevice, ctx->stream);
-  count_launch(ctx, 3);
-  return check_launch("huffman encode");
 }
 
 // ---- histogram -------------------------------------------------------------------
@@ -481,19 +645,25 @@ __global__ void check_total_kernel(const unsigned long long* off, int nsub, size
 
 }  // namespace
 
-size_t huff_encode_tmp_bytes(size_t n) {
-  size_t nb = (n + ENC_PER_CTA - 1) / ENC_PER_CTA;
-  return (align_up(nb, 32) + nb + 1 + 32) * sizeof(unsigned long long);
+int launch_codebook_scatter(cpsz_b200_ctx* ctx, const HuffEntry* d_entries, size_t n, unsigned long long* code,
+                            uint8_t* len) {
+  if (n == 0) return CPSZ_OK;
+  codebook_scatter_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(d_entries, n, code, len);
+  count_launch(ctx);
+  return check_launch("codebook_scatter_kernel");
 }
 
+size_t huff_encode_tmp_bytes(size_t n) { return align_up(pack_scratch_words(n), 32) * sizeof(unsigned long long); }
+
 int launch_huff_encode_u8(cpsz_b200_ctx* ctx, const uint8_t* sym, size_t n, bool map_id_zero, HuffEncTable tab,
-                          uint32_t* out_words, size_t out_cap_bytes, unsigned long long* d_total_bits, void* tmp) {
-  return encode_impl<uint8_t>(ctx, sym, n, map_id_zero, tab, out_words, out_cap_bytes, d_total_bits, tmp);
+                          uint32_t* out_words, size_t out_cap_bytes, unsigned long long* d_total_bits, void* tmp,
+                          int bit0) {
+  return encode_impl<uint8_t>(ctx, sym, n, map_id_zero, tab, out_words, out_cap_bytes, d_total_bits, tmp, bit0);
 }
 
 int launch_huff_encode_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, HuffEncTable tab, uint32_t* out_words,
-                           size_t out_cap_bytes, unsigned long long* d_total_bits, void* tmp) {
-  return encode_impl<uint16_t>(ctx, sym, n, false, tab, out_words, out_cap_bytes, d_total_bits, tmp);
+                           size_t out_cap_bytes, unsigned long long* d_total_bits, void* tmp, int bit0) {
+  return encode_impl<uint16_t>(ctx, sym, n, false, tab, out_words, out_cap_bytes, d_total_bits, tmp, bit0);
 }
 
 int launch_hist_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, unsigned long long* hist) {
@@ -580,17 +750,16 @@ int launch_huff_decode(cpsz_b200_ctx* ctx, const uint8_t* bytes, size_t nbytes, 
 // memory for its own pool at start-up, a plugin that is only handed
 // preallocated buffers by its host framework, or a real-time loop where a
 // cudaMalloc (which may synchronise the device) is not allowed.  For them
-// this entry point packs a symbol stream with the same kernels as
-// cpsz_b200_huffman_encode_u16 but takes its scratch -- the per-CTA bit
-// counts and their scan -- from a fixed array in this file instead of a
-// context workspace.  The array (about 260 KB) lives on every GPU that loads
+// this entry point packs a symbol stream with the same kernel as
+// cpsz_b200_huffman_encode_u16 but takes its scratch -- the tile ticket and
+// the per-tile look-back states -- from a fixed array in this file instead of
+// a context workspace.  The array (about 64 KB) lives on every GPU that loads
 // the library until the process exits, and it bounds the stream length.
 
 constexpr size_t kNoAllocMaxSymbols = size_t(1) << 26;  // 67,108,864 symbols per call
-constexpr size_t kNoAllocMaxCtas = kNoAllocMaxSymbols / ENC_PER_CTA;
-constexpr size_t kNoAllocCounts = kNoAllocMaxCtas + 32;  // per-CTA bit counts (+ padding)
-// layout: [counts: kNoAllocCounts][offsets: kNoAllocMaxCtas + 1][flag word]
-static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocCounts + kNoAllocMaxCtas + 1 + 1];
+constexpr size_t kNoAllocTiles = kNoAllocMaxSymbols / PK_TILE;
+// layout: [ticket][tile states: kNoAllocTiles][flag word]
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[1 + kNoAllocTiles + 1];
 
 namespace {
 
@@ -629,23 +798,18 @@ extern "C" int cpsz_b200_huffman_encode_u16_noalloc(const uint16_t* sym, size_t 
   unsigned long long* scratch = nullptr;
   CPSZ_TRY(noalloc_scratch(&scratch));
   cudaStream_t st = (cudaStream_t)stream;
-  unsigned long long* cta_bits = scratch;
-  unsigned long long* cta_off = scratch + kNoAllocCounts;
-  int* flag = (int*)(cta_off + kNoAllocMaxCtas + 1);
-  // the packer ORs the edge words of every CTA: the output starts at zero
+  int* flag = (int*)(scratch + 1 + kNoAllocTiles);
+  // the packer ORs the edge words of every tile: the output starts at zero
   CPSZ_CUDA_TRY(cudaMemsetAsync(out, 0, out_cap, st));
   CPSZ_CUDA_TRY(cudaMemsetAsync(flag, 0, sizeof(unsigned long long), st));
   if (n == 0) {
     CPSZ_CUDA_TRY(cudaMemsetAsync(total_bits, 0, sizeof(uint64_t), st));
     return CPSZ_OK;
   }
-  const size_t nb = (n + ENC_PER_CTA - 1) / ENC_PER_CTA;
-  enc_count_kernel<uint16_t><<<(unsigned)nb, ENC_NT, 0, st>>>(sym, n, false, len, cta_bits);
-  scan_u64_kernel<<<1, 1024, 0, st>>>(cta_bits, cta_off, nb);
-  const size_t smem = ((size_t)ENC_PER_CTA * 64) / 32 * 4 + 16;
-  enc_write_kernel<uint16_t><<<(unsigned)nb, ENC_NT, smem, st>>>(sym, n, false,
-                                                                 (const unsigned long long*)code, len, cta_off,
-                                                                 (uint32_t*)out, out_cap / 4, flag);
-  CPSZ_CUDA_TRY(cudaMemcpyAsync(total_bits, cta_off + nb, sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
+  int dev = 0, sms = 0;
+  CPSZ_CUDA_TRY(cudaGetDevice(&dev));
+  CPSZ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  CPSZ_TRY(pack_launch<uint16_t>(sms, st, sym, n, false, HuffEncTable{(const unsigned long long*)code, len, 65536},
+                                 (uint32_t*)out, out_cap, 0, scratch, (unsigned long long*)total_bits, flag));
   return check_launch("huffman no-alloc encode");
 }

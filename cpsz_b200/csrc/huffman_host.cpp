@@ -224,12 +224,8 @@ bool huff_build(const unsigned long long* hist, size_t bins, size_t state_num, H
     out->total_bits += leaf_freq[d] * (unsigned long long)depth[d];
   }
   out->max_len = deepest;
-  out->code.assign(bins, 0);
-  out->len.assign(bins, 0);
-  for (size_t d = 0; d < distinct; d++) {
-    out->code[leaf_sym[d]] = leaf_code[d];
-    out->len[leaf_sym[d]] = leaf_len[d];
-  }
+  out->entries.resize(distinct);
+  for (size_t d = 0; d < distinct; d++) out->entries[d] = HuffEntry{leaf_code[d], leaf_sym[d], leaf_len[d]};
   const size_t tsz = tree_size_for(node_count);
   out->tree_bytes.assign(8 + 4 + tsz, 0);
   size_t at = 0;
@@ -248,6 +244,28 @@ bool huff_build(const unsigned long long* hist, size_t bins, size_t state_num, H
   for (size_t i = 0; i < node_count; i++) put<uint32_t>(out->tree_bytes, at, C[i]);
   for (size_t i = 0; i < node_count; i++) put<uint8_t>(out->tree_bytes, at, T[i]);
   return true;
+}
+
+int huff_upload(cpsz_b200_ctx* ctx, const HuffCodebook& cb, HuffEntry* h_stage, HuffEntry* d_ent,
+                unsigned long long* code, uint8_t* len) {
+  const size_t n = cb.entries.size();
+  const HuffEntry* src = cb.entries.data();
+  if (h_stage) {
+    memcpy(h_stage, src, n * sizeof(HuffEntry));
+    src = h_stage;
+  }
+  CPSZ_CUDA_TRY(cudaMemcpyAsync(d_ent, src, n * sizeof(HuffEntry), cudaMemcpyHostToDevice, ctx->stream));
+  return launch_codebook_scatter(ctx, d_ent, n, code, len);
+}
+
+void huff_tables(const HuffCodebook& cb, size_t bins, unsigned long long* code, uint8_t* len) {
+  if (code) memset(code, 0, bins * sizeof(unsigned long long));
+  if (len) memset(len, 0, bins);
+  for (const HuffEntry& e : cb.entries) {
+    if (e.sym >= bins) continue;
+    if (code) code[e.sym] = e.code;
+    if (len) len[e.sym] = (uint8_t)e.len;
+  }
 }
 
 bool huff_parse(const unsigned char* p, size_t avail, size_t max_symbol, HuffDecoderHost* out) {

@@ -7,11 +7,12 @@
 #include <cstdint>
 #include <vector>
 
+#include "kernels.h"
+
 namespace cpsz {
 
 struct HuffCodebook {
-  std::vector<unsigned long long> code;  // right-aligned code per symbol
-  std::vector<uint8_t> len;              // 0 = symbol absent
+  std::vector<HuffEntry> entries;        // the symbols that occur, ascending, with their codes
   std::vector<uint8_t> tree_bytes;       // node_count(8) tree_size(4) tree(tree_size)
   unsigned long long total_bits = 0;     // sum over symbols of freq * len
   int max_len = 0;
@@ -23,6 +24,17 @@ struct HuffCodebook {
 // Returns false (with an error set) if the histogram is empty or a code would
 // exceed 64 bits.
 bool huff_build(const unsigned long long* hist, size_t bins, size_t state_num, HuffCodebook* out);
+
+// Device tables of the codebook: its entries go up to d_ent (room for
+// cb.entries.size()) on ctx->stream and are scattered into code / len.  With
+// h_stage (page-locked, room for the entries) the entries are copied there
+// first, so the upload is asynchronous; without, they go up from the
+// codebook's own (pageable) memory.
+int huff_upload(cpsz_b200_ctx* ctx, const HuffCodebook& cb, HuffEntry* h_stage, HuffEntry* d_ent,
+                unsigned long long* code, uint8_t* len);
+
+// Full per-symbol tables over `bins` symbols (code right-aligned; len 0 = absent).
+void huff_tables(const HuffCodebook& cb, size_t bins, unsigned long long* code, uint8_t* len);
 
 // Section size: 8 + 4 + tree_size + 8 + ceil(total_bits/8).
 inline size_t huff_section_bytes(const HuffCodebook& cb) { return cb.tree_bytes.size() + 8 + (cb.total_bits + 7) / 8; }

@@ -141,6 +141,17 @@ int launch_exp2d(cpsz_b200_ctx* ctx, float* U, float* V, const uint8_t* sign_u, 
                  const LibmFn& Ex);
 
 // ---- Huffman -------------------------------------------------------------------
+// One codebook entry of a symbol that occurs (code right-aligned, bit len-1 = first bit).
+struct HuffEntry {
+  unsigned long long code;
+  uint32_t sym;
+  uint32_t len;
+};
+// Device codebook tables from n entries: code[e.sym] = e.code, len[e.sym] =
+// e.len.  Entries of symbols not in the list keep what the tables held: the
+// packer looks up only symbols that occur.
+int launch_codebook_scatter(cpsz_b200_ctx* ctx, const HuffEntry* d_entries, size_t n, unsigned long long* code,
+                            uint8_t* len);
 // Codebook for the encoder: per symbol, code right-aligned (bit len-1 = first bit).
 struct HuffEncTable {
   const unsigned long long* code;
@@ -152,10 +163,15 @@ struct HuffEncTable {
 // ceil(bits/8) bytes rounded up to 4).
 size_t huff_encode_tmp_bytes(size_t n);
 // Words at or beyond out_cap_bytes / 4 are not written (FLAG_OUT_CAPACITY is raised).
+// The stream starts at bit bit0 (0-31, most significant first) of out_words[0];
+// the bits before it are left as they are (the first word is ORed), so a
+// stream can be written straight after other bytes.  tmp: huff_encode_tmp_bytes(n).
 int launch_huff_encode_u8(cpsz_b200_ctx* ctx, const uint8_t* sym, size_t n, bool map_id_zero, HuffEncTable tab,
-                          uint32_t* out_words, size_t out_cap_bytes, unsigned long long* d_total_bits, void* tmp);
+                          uint32_t* out_words, size_t out_cap_bytes, unsigned long long* d_total_bits, void* tmp,
+                          int bit0 = 0);
 int launch_huff_encode_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, HuffEncTable tab,
-                           uint32_t* out_words, size_t out_cap_bytes, unsigned long long* d_total_bits, void* tmp);
+                           uint32_t* out_words, size_t out_cap_bytes, unsigned long long* d_total_bits, void* tmp,
+                           int bit0 = 0);
 // Histograms (global, 64-bit bins).
 int launch_hist_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, unsigned long long* hist);
 

@@ -39,9 +39,11 @@ struct StageTap {
 int build_wave_items(int nfields, const int* r1s, std::vector<WaveItem>& items);
 
 // eb_ext (optional, device, N doubles): per-vertex bounds to quantize instead
-// of the derived ones (the learned-bound path).  host_out (optional, host
-// memory of host_cap bytes): the blob is written there directly (out->d_blob
-// is then not set).
+// of the derived ones (the learned-bound path).  host_out (optional, of
+// host_cap bytes): host memory gets the blob written there directly
+// (out->d_blob is then not set); a device buffer with room for the blob's
+// bound gets the blob built in place (out->d_blob == host_out), else the blob
+// is built in the workspace (out->d_blob) and the caller copies it.
 // log_form: the offline_log blob (src/sz_compress_cp_preserve_2d.cpp:285-379)
 // instead of the offline one.
 int compress_2d(cpsz_b200_ctx* ctx, const float* U, const float* V, size_t r1, size_t r2, double max_pwr_eb,

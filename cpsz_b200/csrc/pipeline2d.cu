@@ -25,12 +25,11 @@
 //   FIELD = int 12 | char 0 | int 32768 | meanInfo<float>{false,0} (8 B) | size_t 0
 //         | size_t n_unpred | float[n_unpred] | ceil(nblocks/8) zero bytes | HUF(codes, 131072 states, N)
 #include <algorithm>
-#include <atomic>
 #include <cfloat>
 #include <cstring>
-#include <thread>
 #include <vector>
 
+#include "host_pool.h"
 #include "huffman_host.h"
 #include "kernels.h"
 #include "tuning.h"
@@ -44,8 +43,9 @@ namespace {
 constexpr int BS = 12;
 constexpr size_t FIELD_HDR = 4 + 1 + 4 + 8 + 8 + 8;  // up to and including n_unpred
 constexpr size_t BLOB_HDR = 4 + 8 + 8 + 8 + 8;
-// pinned staging per field: id histogram, two code histograms, unpredictable counts
-constexpr size_t JOB_PINNED = (256 + 2 * 65536) * 8 + 64;
+// pinned staging per field: id histogram, two code histograms, unpredictable
+// counts, the id codebook's entries
+constexpr size_t JOB_PINNED = (256 + 2 * 65536) * 8 + 64 + 256 * sizeof(HuffEntry);
 constexpr size_t PINNED_BASE = 4096;  // the flag word and scalars live below
 // sub-batch limits: fields per pass (pinned staging) and points per pass (workspace)
 constexpr int BATCH_MAX_FIELDS = 32;
@@ -67,9 +67,11 @@ struct DevBuf {
   float* unpred[2];
   unsigned long long* enc_code[3];
   uint8_t* enc_len[3];
+  HuffEntry* enc_ent[3];  // codebook entries as uploaded
   void* enc_tmp[3];
   uint32_t* bits[3];
   uint8_t* blob;
+  uint8_t* stage;       // the blob's small pieces and their descriptors, as uploaded
   float* logs[2];       // offline_log: log2f |U|, |V| (the unpredictable values it stores)
   uint32_t* signs[2];   // offline_log: sign maps
 };
@@ -88,11 +90,19 @@ struct Job2D {
   unsigned long long* h_hist_ids = nullptr;    // pinned
   unsigned long long* h_hist_codes = nullptr;  // pinned, 2 x 65536
   unsigned int* h_nunpred = nullptr;           // pinned, 2
+  HuffEntry* h_ids_ent = nullptr;              // pinned, 256
   HuffCodebook cb[3];
   bool tree_ok[3] = {false, false, false};
   size_t n_unpred[2] = {0, 0};
   size_t sec_bytes[3] = {0, 0, 0}, bits_bytes[3] = {0, 0, 0};
   size_t size = 0;  // blob bytes
+  // device output: the blob is built in place at blob_base (blob_room bytes
+  // there), the caller's buffer when it is a device buffer with room for the
+  // blob's bound, else the workspace blob
+  unsigned char* dev_out = nullptr;
+  size_t dev_cap = 0;
+  uint8_t* blob_base = nullptr;
+  size_t blob_room = 0;
   // host output: the blob is written straight into host memory (sections
   // copied from their device buffers), not assembled in device memory
   unsigned char* host_out = nullptr;
@@ -124,24 +134,14 @@ int flag_error(int flag) {
   return CPSZ_OK;
 }
 
-// Runs f(0..n-1) on up to hardware_concurrency host threads.
-template <class Fn>
-void parallel_for(int n, Fn f) {
-  unsigned nt = std::thread::hardware_concurrency();
-  if (nt < 1) nt = 1;
-  if ((int)nt > n) nt = (unsigned)n;
-  if (nt <= 1) {
-    for (int i = 0; i < n; i++) f(i);
-    return;
-  }
-  std::atomic<int> next{0};
-  std::vector<std::thread> th;
-  for (unsigned t = 0; t < nt; t++)
-    th.emplace_back([&] {
-      for (int i = next++; i < n; i = next++) f(i);
-    });
-  for (auto& t : th) t.join();
-}
+// While it lives, the launch wrappers (which all enqueue on ctx->stream) run
+// on stream s instead of the context's main stream.
+struct OnStream {
+  cpsz_b200_ctx* ctx;
+  cudaStream_t saved;
+  OnStream(cpsz_b200_ctx* c, cudaStream_t s) : ctx(c), saved(c->stream) { c->stream = s; }
+  ~OnStream() { ctx->stream = saved; }
+};
 
 int job_init(Job2D& j, const float* U, const float* V, size_t r1s, size_t r2s, double eb) {
   if (!U || !V) return set_error(CPSZ_ERR_INVALID, "null input field");
@@ -169,6 +169,13 @@ int job_init(Job2D& j, const float* U, const float* V, size_t r1s, size_t r2s, d
   return CPSZ_OK;
 }
 
+// Bound of the blob's small pieces (header, three trees with their stream
+// sizes, field headers, indicators) and their descriptors.
+size_t stage_bytes(const Job2D& j) {
+  const size_t tree = 12 + 1 + 13 * std::min<size_t>(131072, 2 * j.N + 1) + 8;
+  return BLOB_HDR + 2 * FIELD_HDR + 2 * ((j.nblocks + 7) / 8) + (12 + 1 + 13 * 512 + 8) + 2 * tree + 64 + 24 * 32;
+}
+
 // Workspace of one field (each piece padded as the arena pads it).
 size_t job_bytes(const Job2D& j) {
   size_t bytes = 0;
@@ -187,11 +194,15 @@ size_t job_bytes(const Job2D& j) {
   add(2 * 4 * N);  // unpred
   add(256 * 9);
   add(2 * 65536 * 9);
+  add(256 * sizeof(HuffEntry));
+  add(std::min<size_t>(65536, N) * sizeof(HuffEntry));
+  add(std::min<size_t>(65536, N) * sizeof(HuffEntry));
   add(huff_encode_tmp_bytes(2 * N));
   add(2 * huff_encode_tmp_bytes(N));
   add(j.ids_bits_cap);
   add(2 * j.codes_bits_cap);
   add(j.blob_cap);
+  add(stage_bytes(j));
   if (j.log_form) {
     add(2 * 4 * N);                        // log values
     add(2 * 4 * ((N + 31) / 32));          // sign maps
@@ -230,6 +241,9 @@ int job_alloc(cpsz_b200_ctx* ctx, Job2D& j) {
     d.enc_code[f] = (unsigned long long*)A(65536 * 8);
     d.enc_len[f] = (uint8_t*)A(65536);
   }
+  d.enc_ent[0] = (HuffEntry*)A(256 * sizeof(HuffEntry));
+  d.enc_ent[1] = (HuffEntry*)A(std::min<size_t>(65536, N) * sizeof(HuffEntry));
+  d.enc_ent[2] = (HuffEntry*)A(std::min<size_t>(65536, N) * sizeof(HuffEntry));
   d.enc_tmp[0] = A(huff_encode_tmp_bytes(2 * N));
   d.enc_tmp[1] = A(huff_encode_tmp_bytes(N));
   d.enc_tmp[2] = A(huff_encode_tmp_bytes(N));
@@ -237,7 +251,15 @@ int job_alloc(cpsz_b200_ctx* ctx, Job2D& j) {
   d.bits[1] = (uint32_t*)A(j.codes_bits_cap);
   d.bits[2] = (uint32_t*)A(j.codes_bits_cap);
   d.blob = (uint8_t*)A(j.blob_cap);
-  if (!d.blob) return set_error(CPSZ_ERR_NOMEM, "workspace layout overflow");
+  d.stage = (uint8_t*)A(stage_bytes(j));
+  if (!d.stage) return set_error(CPSZ_ERR_NOMEM, "workspace layout overflow");
+  if (j.dev_out && j.dev_cap >= j.blob_cap + 8) {
+    j.blob_base = j.dev_out;
+    j.blob_room = j.dev_cap;
+  } else {
+    j.blob_base = d.blob;
+    j.blob_room = align_up(j.blob_cap, 256);
+  }
   if (j.log_form) {
     d.logs[0] = (float*)A(4 * N);
     d.logs[1] = (float*)A(4 * N);
@@ -332,38 +354,58 @@ int job_layout(const Job2D& j, BlobLayout& L) {
   return CPSZ_OK;
 }
 
-int job_assemble(cpsz_b200_ctx* ctx, Job2D& j) {
+// The small pieces of a blob in one launch: CTA (x, y) copies bytes
+// [x * 4096, (x + 1) * 4096) of piece y from the staged bytes (byte stores:
+// the bytes around a piece belong to other sections, some written before it).
+constexpr int PIECE_CHUNK = 4096;
+__global__ void __launch_bounds__(256) pieces_kernel(const uint8_t* __restrict__ small,
+                                                     const unsigned long long* __restrict__ desc,
+                                                     uint8_t* __restrict__ blob) {
+  const unsigned long long dst = desc[3 * blockIdx.y], src = desc[3 * blockIdx.y + 1], n = desc[3 * blockIdx.y + 2];
+  const unsigned long long c0 = (unsigned long long)blockIdx.x * PIECE_CHUNK;
+  const unsigned long long c1 = n < c0 + PIECE_CHUNK ? n : c0 + PIECE_CHUNK;
+  for (unsigned long long i = c0 + threadIdx.x; i < c1; i += 256) blob[dst + i] = small[src + i];
+}
+
+// Bytes job_assemble uploads: the small pieces, then their descriptors.
+size_t assemble_upload_bytes(const BlobLayout& L) { return align_up(L.small.size(), 8) + 24 * L.pieces.size(); }
+
+// The sections of a device blob that the packers do not write: the staged
+// small pieces (header, trees, stream sizes, field headers, indicators), the
+// unpredictable values and the sign maps.  h_up: page-locked staging of
+// assemble_upload_bytes(L), which must stay untouched until the pass ends.
+int job_assemble(cpsz_b200_ctx* ctx, Job2D& j, const BlobLayout& L, uint8_t* h_up) {
   cudaStream_t st = ctx->stream;
-  BlobLayout L;
-  CPSZ_TRY(job_layout(j, L));
-  const size_t total = L.total;
-  if (total > j.blob_cap) return set_error(CPSZ_ERR_UNSUPPORTED, "blob larger than its bound");
-  const std::vector<uint8_t>& small = L.small;
-  const std::vector<BlobLayout::Piece>& pieces = L.pieces;
-  const size_t* bit_dst = L.bit_dst;
-  const size_t* unpred_dst = L.unpred_dst;
-  uint8_t* blob = j.d.blob;
-  uint8_t* d_small = blob + align_up(total, 256);
-  if (align_up(total, 256) + small.size() > j.blob_cap) {
-    for (const BlobLayout::Piece& p : pieces)
-      CPSZ_CUDA_TRY(cudaMemcpyAsync(blob + p.dst, small.data() + p.src, p.n, cudaMemcpyHostToDevice, st));
-  } else {
-    // pageable source: the runtime stages it before returning, so `small` may go
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(d_small, small.data(), small.size(), cudaMemcpyHostToDevice, st));
-    for (const BlobLayout::Piece& p : pieces)
-      CPSZ_CUDA_TRY(cudaMemcpyAsync(blob + p.dst, d_small + p.src, p.n, cudaMemcpyDeviceToDevice, st));
+  uint8_t* blob = j.blob_base;
+  // pieces and their descriptors go up in one copy
+  const size_t up_size = assemble_upload_bytes(L);
+  memcpy(h_up, L.small.data(), L.small.size());
+  unsigned long long* desc = (unsigned long long*)(h_up + align_up(L.small.size(), 8));
+  for (size_t i = 0; i < L.pieces.size(); i++) {
+    desc[3 * i] = L.pieces[i].dst;
+    desc[3 * i + 1] = L.pieces[i].src;
+    desc[3 * i + 2] = L.pieces[i].n;
   }
-  for (int k = 0; k < 3; k++)
-    if (j.bits_bytes[k])
-      CPSZ_CUDA_TRY(cudaMemcpyAsync(blob + bit_dst[k], j.d.bits[k], j.bits_bytes[k], cudaMemcpyDeviceToDevice, st));
+  if (up_size > stage_bytes(j)) return set_error(CPSZ_ERR_INVALID, "internal: blob pieces exceed their bound");
+  uint8_t* d_up = j.d.stage;
+  CPSZ_CUDA_TRY(cudaMemcpyAsync(d_up, h_up, up_size, cudaMemcpyHostToDevice, st));
+  if (!L.pieces.empty()) {
+    size_t longest = 0;
+    for (const BlobLayout::Piece& pc : L.pieces) longest = std::max(longest, pc.n);
+    const dim3 grid((unsigned)std::max<size_t>(1, (longest + PIECE_CHUNK - 1) / PIECE_CHUNK), (unsigned)L.pieces.size());
+    pieces_kernel<<<grid, 256, 0, st>>>(
+        d_up, (const unsigned long long*)(d_up + align_up(L.small.size(), 8)), blob);
+    count_launch(ctx);
+    CPSZ_TRY(check_launch("pieces_kernel"));
+  }
   for (int f = 0; f < 2; f++)
     if (j.n_unpred[f])
       CPSZ_CUDA_TRY(
-          cudaMemcpyAsync(blob + unpred_dst[f], j.d.unpred[f], 4 * j.n_unpred[f], cudaMemcpyDeviceToDevice, st));
+          cudaMemcpyAsync(blob + L.unpred_dst[f], j.d.unpred[f], 4 * j.n_unpred[f], cudaMemcpyDeviceToDevice, st));
   for (int f = 0; f < 2 && L.sign_bytes; f++)
     CPSZ_CUDA_TRY(cudaMemcpyAsync(blob + L.sign_dst + f * L.sign_bytes, j.d_signs[f], L.sign_bytes,
                                   cudaMemcpyDeviceToDevice, st));
-  j.size = total;
+  j.size = L.total;
   return CPSZ_OK;
 }
 
@@ -390,6 +432,7 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     jobs[k].h_hist_ids = (unsigned long long*)base;
     jobs[k].h_hist_codes = jobs[k].h_hist_ids + 256;
     jobs[k].h_nunpred = (unsigned int*)(jobs[k].h_hist_codes + 2 * 65536);
+    jobs[k].h_ids_ent = (HuffEntry*)(base + (256 + 2 * 65536) * 8 + 64);
   }
 
   // Derived bounds (eb2d) signal per 128-row group, so for one field the
@@ -666,7 +709,6 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   // once everything is done; no blob is assembled in device memory.
   Job2D* hj = (nj == 1 && jobs[0].host_out) ? &jobs[0] : nullptr;
   const bool h_async = hj && host_kind(hj->host_out) == HOST_PINNED;
-  BlobLayout hl;
   // Page-locked output: each section's copy runs on the aux stream behind its
   // producer, so the next producer does not wait for it.  The main stream
   // joins aux before the pass ends; on an early return the guard drains aux, so
@@ -683,10 +725,29 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     aux_drain.s = ctx->aux;
     return d2h(ctx, dst, src, n, ctx->aux);
   };
+  // Bit packing of stream k (0: ids, 1-2: codes of U / V).  A device blob gets
+  // the bits in place, at byte `at` (the sections around it are written later
+  // byte by byte, and the packer ORs only zero bits into their bytes); host
+  // output packs into a buffer of the stream's own that is copied out.
+  auto pack = [&](Job2D& j, int k, size_t at, HuffEntry* h_stage) -> int {
+    uint8_t* dst = j.host_out ? (uint8_t*)j.d.bits[k] : j.blob_base + at;
+    const size_t room = j.host_out ? (k ? j.codes_bits_cap : j.ids_bits_cap) : j.blob_room - at;
+    const size_t mis = (uintptr_t)dst & 3;
+    CPSZ_CUDA_TRY(cudaMemsetAsync(dst, 0, j.bits_bytes[k], ctx->stream));
+    CPSZ_TRY(huff_upload(ctx, j.cb[k], h_stage, j.d.enc_ent[k], j.d.enc_code[k], j.d.enc_len[k]));
+    const HuffEncTable tab{j.d.enc_code[k], j.d.enc_len[k], k ? 65536 : 256};
+    uint32_t* w = (uint32_t*)(dst - mis);
+    if (k == 0)
+      return launch_huff_encode_u8(ctx, j.d.ids, j.log_form ? j.N : 2 * j.N, true, tab, w, room + mis, nullptr,
+                                   j.d.enc_tmp[0], (int)(8 * mis));
+    return launch_huff_encode_u16(ctx, j.d.cblocks[k - 1], j.N, tab, w, room + mis, nullptr, j.d.enc_tmp[k],
+                                  (int)(8 * mis));
+  };
 
-  // host: the id trees (their histograms arrived while the wavefront ran) and
-  // their bit packing, which the GPU runs right after stage 3 while the host
-  // builds the code trees
+  // host: the id trees (their histograms arrive with the bounds), and their
+  // bit packing on the aux stream as soon as the bounds are done: it runs
+  // beside the wavefront's tail, which leaves most SMs idle, and the main
+  // stream joins aux before the blob is finished
   auto tree_failure = [&]() {
     int fl = 0;
     CPSZ_TRY(read_flag(ctx, &fl));
@@ -694,31 +755,29 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     return set_error(CPSZ_ERR_UNSUPPORTED, "Huffman tree construction failed (code longer than 64 bits)");
   };
   CPSZ_CUDA_TRY(cudaEventSynchronize(ctx->ev[0]));
-  parallel_for(nj, [&](int k) { jobs[k].tree_ok[0] = huff_build(jobs[k].h_hist_ids, 256, 2048, &jobs[k].cb[0]); });
+  host_parallel_for(nj, [&](int k) { jobs[k].tree_ok[0] = huff_build(jobs[k].h_hist_ids, 256, 2048, &jobs[k].cb[0]); });
+  CPSZ_CUDA_TRY(cudaStreamWaitEvent(ctx->aux, ctx->ev[0], 0));
+  aux_drain.s = ctx->aux;
   for (Job2D& j : jobs) {
     if (!j.tree_ok[0]) return tree_failure();
     j.sec_bytes[0] = huff_section_bytes(j.cb[0]);
     j.bits_bytes[0] = (j.cb[0].total_bits + 7) / 8;
     if (j.bits_bytes[0] + 8 > j.ids_bits_cap) return set_error(CPSZ_ERR_UNSUPPORTED, "Huffman stream larger than its bound");
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.enc_code[0], j.cb[0].code.data(), 256 * 8, cudaMemcpyHostToDevice, st));
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.enc_len[0], j.cb[0].len.data(), 256, cudaMemcpyHostToDevice, st));
-    CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.bits[0], 0, align_up(j.bits_bytes[0], 4) + 8, st));
-    CPSZ_TRY(launch_huff_encode_u8(ctx, j.d.ids, j.log_form ? j.N : 2 * j.N, true,
-                                   HuffEncTable{j.d.enc_code[0], j.d.enc_len[0], 256},
-                                   j.d.bits[0], j.ids_bits_cap, nullptr, j.d.enc_tmp[0]));
+    OnStream on_aux(ctx, ctx->aux);
+    CPSZ_TRY(pack(j, 0, ids_bits_at(j), j.h_ids_ent));
   }
   if (h_async) {
     const size_t at = ids_bits_at(*hj);
     if (at + hj->bits_bytes[0] > hj->host_cap)
       return set_error(CPSZ_ERR_INVALID, "output capacity %zu too small for the blob", hj->host_cap);
-    CPSZ_TRY(d2h_beside(hj->host_out + at, hj->d.bits[0], hj->bits_bytes[0]));
+    CPSZ_TRY(d2h(ctx, hj->host_out + at, hj->d.bits[0], hj->bits_bytes[0], ctx->aux));
   }
   // code trees, each as soon as its histogram is on the host
   auto code_trees = [&]() {
-    parallel_for(2 * nj, [&](int q) {
+    host_parallel_for(2 * nj, [&](int q) {
       Job2D& j = jobs[q / 2];
       const int f = q % 2;
-      j.tree_ok[1 + f] = cudaEventSynchronize(ctx->job_ev[q]) == cudaSuccess &&
+      j.tree_ok[1 + f] = cudaSetDevice(ctx->device) == cudaSuccess && cudaEventSynchronize(ctx->job_ev[q]) == cudaSuccess &&
                          huff_build(j.h_hist_codes + (size_t)f * 65536, 65536, 131072, &j.cb[1 + f]);
     });
   };
@@ -745,7 +804,8 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     }
   }
 
-  // ---- stage 4: bit packing of the codes ----
+  // ---- stage 4: blob layout (every section size is known once the
+  // unpredictable counts are on the host) and bit packing of the codes ----
   mark(ctx, "huffman_encode");
   for (Job2D& j : jobs) {
     if (!j.tree_ok[1] || !j.tree_ok[2]) return tree_failure();
@@ -756,14 +816,35 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
         return set_error(CPSZ_ERR_UNSUPPORTED, "Huffman stream larger than its bound");
     }
   }
+  CPSZ_CUDA_TRY(cudaEventSynchronize(ctx->ev[5]));
+  std::vector<BlobLayout> lay(nj);
+  for (int q = 0; q < nj; q++) {
+    Job2D& j = jobs[q];
+    j.n_unpred[0] = j.h_nunpred[0];
+    j.n_unpred[1] = j.h_nunpred[1];
+    CPSZ_TRY(job_layout(j, lay[q]));
+    if (j.host_out) {
+      if (lay[q].total > j.host_cap)
+        return set_error(CPSZ_ERR_INVALID, "output capacity %zu < blob size %zu", j.host_cap, lay[q].total);
+    } else if (lay[q].total > j.blob_cap) {
+      return set_error(CPSZ_ERR_UNSUPPORTED, "blob larger than its bound");
+    }
+  }
+  // page-locked staging of the pass's remaining uploads: code entries, and
+  // the device blobs' small pieces (no copy from it is in flight here)
+  size_t up_bytes = 0;
+  for (int q = 0; q < nj; q++)
+    up_bytes += (jobs[q].cb[1].entries.size() + jobs[q].cb[2].entries.size()) * sizeof(HuffEntry) +
+                (jobs[q].host_out ? 0 : assemble_upload_bytes(lay[q]));
+  CPSZ_TRY(upload_reserve(ctx, up_bytes));
+  uint8_t* up_at = (uint8_t*)ctx->up_pinned;
+  auto up_take = [&](size_t n) {
+    uint8_t* p = up_at;
+    up_at += align_up(n, 16);
+    return p;
+  };
   if (hj) {
-    // every section size is known: lay the blob out in the caller's memory
-    CPSZ_CUDA_TRY(cudaEventSynchronize(ctx->ev[5]));
-    hj->n_unpred[0] = hj->h_nunpred[0];
-    hj->n_unpred[1] = hj->h_nunpred[1];
-    CPSZ_TRY(job_layout(*hj, hl));
-    if (hl.total > hj->host_cap)
-      return set_error(CPSZ_ERR_INVALID, "output capacity %zu < blob size %zu", hj->host_cap, hl.total);
+    const BlobLayout& hl = lay[0];
     for (const BlobLayout::Piece& pc : hl.pieces) memcpy(hj->host_out + pc.dst, hl.small.data() + pc.src, pc.n);
     if (h_async)
       for (int f = 0; f < 2; f++) {
@@ -772,34 +853,25 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
           CPSZ_TRY(d2h_beside(hj->host_out + hl.sign_dst + f * hl.sign_bytes, hj->d_signs[f], hl.sign_bytes));
       }
   }
-  for (Job2D& j : jobs) {
+  for (int q = 0; q < nj; q++) {
+    Job2D& j = jobs[q];
     for (int k = 1; k < 3; k++) {
-      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.enc_code[k], j.cb[k].code.data(), 65536 * 8, cudaMemcpyHostToDevice, st));
-      CPSZ_CUDA_TRY(cudaMemcpyAsync(j.d.enc_len[k], j.cb[k].len.data(), 65536, cudaMemcpyHostToDevice, st));
-      CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.bits[k], 0, align_up(j.bits_bytes[k], 4) + 8, st));
-      CPSZ_TRY(launch_huff_encode_u16(ctx, j.d.cblocks[k - 1], j.N,
-                                      HuffEncTable{j.d.enc_code[k], j.d.enc_len[k], 65536}, j.d.bits[k],
-                                      j.codes_bits_cap, nullptr, j.d.enc_tmp[k]));
-      if (h_async) CPSZ_TRY(d2h_beside(j.host_out + hl.bit_dst[k], j.d.bits[k], j.bits_bytes[k]));
+      CPSZ_TRY(pack(j, k, lay[q].bit_dst[k], (HuffEntry*)up_take(j.cb[k].entries.size() * sizeof(HuffEntry))));
+      if (h_async) CPSZ_TRY(d2h_beside(j.host_out + lay[q].bit_dst[k], j.d.bits[k], j.bits_bytes[k]));
     }
   }
-  if (aux_drain.s) {  // the section copies join the main stream
+  if (aux_drain.s) {  // the aux stream's work (id packing, section copies) joins the main stream
     CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[7], ctx->aux));
     CPSZ_CUDA_TRY(cudaStreamWaitEvent(st, ctx->ev[7], 0));
   }
-  // ---- stage 5: blob assembly in device memory, enqueued behind the encoders
-  // (the unpredictable counts it needs are on the host since stage 3), or, for
-  // host output, the sections not yet copied ----
-  CPSZ_CUDA_TRY(cudaEventSynchronize(ctx->ev[5]));
-  for (Job2D& j : jobs) {
-    j.n_unpred[0] = j.h_nunpred[0];
-    j.n_unpred[1] = j.h_nunpred[1];
-  }
+  // ---- stage 5: the rest of a device blob (header, trees, unpredictable
+  // values, sign maps), enqueued behind the packers, or, for host output
+  // without page-locked memory, the sections not yet copied ----
   mark(ctx, "blob_assembly");
   int assembled = CPSZ_OK;
   if (!hj)
-    for (Job2D& j : jobs)
-      if ((assembled = job_assemble(ctx, j)) != CPSZ_OK) break;
+    for (int q = 0; q < nj; q++)
+      if ((assembled = job_assemble(ctx, jobs[q], lay[q], up_take(assemble_upload_bytes(lay[q])))) != CPSZ_OK) break;
   {
     int flag = 0;
     CPSZ_TRY(read_flag(ctx, &flag));  // synchronizes the stream; a kernel's error outranks the assembly's
@@ -807,6 +879,7 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   }
   if (assembled != CPSZ_OK) return assembled;
   if (hj) {
+    const BlobLayout& hl = lay[0];
     if (!h_async) {
       CPSZ_TRY(d2h(ctx, hj->host_out + hl.bit_dst[0], hj->d.bits[0], hj->bits_bytes[0], st));
       for (int f = 0; f < 2; f++) {
@@ -865,12 +938,17 @@ int compress_2d(cpsz_b200_ctx* ctx, const float* U_in, const float* V_in, size_t
   CPSZ_TRY(job_init(jobs[0], U_in, V_in, r1s, r2s, max_pwr_eb));
   jobs[0].log_form = log_form;
   jobs[0].eb_ext = eb_ext;
-  jobs[0].host_out = host_out;
-  jobs[0].host_cap = host_cap;
+  if (host_out && host_kind(host_out) == HOST_DEVICE) {
+    jobs[0].dev_out = host_out;
+    jobs[0].dev_cap = host_cap;
+  } else {
+    jobs[0].host_out = host_out;
+    jobs[0].host_cap = host_cap;
+  }
   CPSZ_TRY(arena_reserve(ctx, pass_bytes(jobs)));
   CPSZ_TRY(pinned_reserve(ctx, PINNED_BASE + JOB_PINNED));
   CPSZ_TRY(run_pass(ctx, jobs, tap));
-  out->d_blob = host_out ? nullptr : jobs[0].d.blob;
+  out->d_blob = jobs[0].host_out ? nullptr : jobs[0].blob_base;
   out->size = jobs[0].size;
   out->n_unpred[0] = jobs[0].n_unpred[0];
   out->n_unpred[1] = jobs[0].n_unpred[1];
@@ -905,7 +983,7 @@ int compress_2d_batch(cpsz_b200_ctx* ctx, int n, const float* const* U, const fl
       const Job2D& j = jobs[q];
       if (at + j.size > out_cap)
         return set_error(CPSZ_ERR_INVALID, "output capacity %zu < %zu bytes of blobs", out_cap, at + j.size);
-      CPSZ_TRY(d2h(ctx, out + at, j.d.blob, j.size, ctx->stream));
+      CPSZ_TRY(d2h(ctx, out + at, j.blob_base, j.size, ctx->stream));
       at += j.size;
       offsets[k0 + q + 1] = at;
     }

@@ -90,6 +90,8 @@ int compress_3d(cpsz_b200_ctx* ctx, const float* U_in, const float* V_in, const 
   add(QUANT_TAB_MAX * 8);
   add(256 * 9);
   add(65536 * 9);
+  add(256 * sizeof(HuffEntry));
+  add(std::min<size_t>(65536, 3 * N + 1) * sizeof(HuffEntry));
   add(huff_encode_tmp_bytes(N));
   add(huff_encode_tmp_bytes(3 * N));
   const size_t ids_bits_cap = (N * 8 + 7) / 8 + 64;
@@ -134,6 +136,8 @@ int compress_3d(cpsz_b200_ctx* ctx, const float* U_in, const float* V_in, const 
   double* thr_tab = (double*)A(QUANT_TAB_MAX * 8);
   unsigned long long* enc_code[2] = {(unsigned long long*)A(256 * 8), (unsigned long long*)A(65536 * 8)};
   uint8_t* enc_len[2] = {(uint8_t*)A(256), (uint8_t*)A(65536)};
+  HuffEntry* enc_ent[2] = {(HuffEntry*)A(256 * sizeof(HuffEntry)),
+                           (HuffEntry*)A(std::min<size_t>(65536, 3 * N + 1) * sizeof(HuffEntry))};
   void* enc_tmp[2] = {A(huff_encode_tmp_bytes(N)), A(huff_encode_tmp_bytes(3 * N))};
   uint32_t* bits[2] = {(uint32_t*)A(ids_bits_cap), (uint32_t*)A(codes_bits_cap)};
   (void)A(64);
@@ -183,9 +187,7 @@ int compress_3d(cpsz_b200_ctx* ctx, const float* U_in, const float* V_in, const 
   if (bits_bytes[0] + 8 > ids_bits_cap || bits_bytes[1] + 8 > codes_bits_cap)
     return set_error(CPSZ_ERR_UNSUPPORTED, "Huffman stream larger than its bound");
   for (int k = 0; k < 2; k++) {
-    const size_t bins = k ? 65536 : 256;
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(enc_code[k], cb[k].code.data(), bins * 8, cudaMemcpyHostToDevice, st));
-    CPSZ_CUDA_TRY(cudaMemcpyAsync(enc_len[k], cb[k].len.data(), bins, cudaMemcpyHostToDevice, st));
+    CPSZ_TRY(huff_upload(ctx, cb[k], nullptr, enc_ent[k], enc_code[k], enc_len[k]));
     CPSZ_CUDA_TRY(cudaMemsetAsync(bits[k], 0, align_up(bits_bytes[k], 4) + 8, st));
   }
   CPSZ_TRY(launch_huff_encode_u8(ctx, ids, N, false, HuffEncTable{enc_code[0], enc_len[0], 256}, bits[0],

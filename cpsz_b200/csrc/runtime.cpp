@@ -229,6 +229,22 @@ int pinned_reserve(cpsz_b200_ctx* ctx, size_t bytes) {
   return CPSZ_OK;
 }
 
+int upload_reserve(cpsz_b200_ctx* ctx, size_t bytes) {
+  if (ctx->up_cap >= bytes) return CPSZ_OK;
+  if (ctx->up_pinned) cudaFreeHost(ctx->up_pinned);
+  ctx->up_pinned = nullptr;
+  ctx->up_cap = 0;
+  bytes = align_up(bytes, 1 << 20);
+  cudaError_t e = cudaMallocHost(&ctx->up_pinned, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    ctx->up_pinned = nullptr;
+    return set_error(CPSZ_ERR_NOMEM, "pinned upload staging of %zu bytes: %s", bytes, cudaGetErrorString(e));
+  }
+  ctx->up_cap = bytes;
+  return CPSZ_OK;
+}
+
 void reset_marks(cpsz_b200_ctx* ctx) { ctx->nmarks = 0; }
 
 void mark(cpsz_b200_ctx* ctx, const char* name) {
@@ -305,6 +321,7 @@ int cpsz_b200_ctx_destroy(cpsz_b200_ctx* c) {
   for (auto& g : c->pass_graphs) cudaGraphExecDestroy(g.exec);
   if (c->arena.base) cudaFree(c->arena.base);
   if (c->pinned) cudaFreeHost(c->pinned);
+  if (c->up_pinned) cudaFreeHost(c->up_pinned);
   if (c->stage) cudaFreeHost(c->stage);
   if (c->d_flag) cudaFree(c->d_flag);
   if (c->libm_mem) cudaFree(c->libm_mem);

@@ -100,6 +100,11 @@ struct cpsz_b200_ctx {
   cudaEvent_t stage_ev[kStageSlots] = {};
   void* pinned = nullptr;
   size_t pinned_cap = 0;
+  // pinned staging of a pass's small uploads made once the pass's trees are
+  // known (codebook entries, blob pieces): page-locked, so the copies are
+  // asynchronous and never wait on the streams' earlier work
+  void* up_pinned = nullptr;
+  size_t up_cap = 0;
   uint64_t launches = 0;
   int num_sms = 0;
   int* d_flag = nullptr;  // device error / timeout flag (persistent)
@@ -134,6 +139,9 @@ int arena_reserve(cpsz_b200_ctx* ctx, size_t bytes);
 void* arena_alloc(cpsz_b200_ctx* ctx, size_t bytes);
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 int pinned_reserve(cpsz_b200_ctx* ctx, size_t bytes);
+// Grows ctx->up_pinned to at least `bytes` (its old contents are dropped:
+// call it only when no copy from it is in flight).
+int upload_reserve(cpsz_b200_ctx* ctx, size_t bytes);
 
 // Pointer kind: true if `p` is device (or managed) memory usable by kernels.
 bool is_device_ptr(const void* p);

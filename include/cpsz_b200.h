@@ -260,13 +260,13 @@ int cpsz_b200_huffman_encode_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t
  * encode -- an in-situ hook inside a simulation that reserved the GPU's memory
  * for its own pool, a plugin handed only preallocated buffers, a loop where a
  * possibly synchronising cudaMalloc is not allowed.  This entry point has no
- * counterpart in the reference.  It calls no allocator: its scratch (per-CTA
- * bit counts and their scan) is a fixed ~260 KB array inside the library that
- * every GPU loading it keeps until process exit, which limits n to 67,108,864
- * symbols per call (larger n is rejected with CPSZ_ERR_INVALID).
+ * counterpart in the reference.  It calls no allocator: its scratch (a tile
+ * ticket and per-tile look-back states) is a fixed ~64 KB array inside the
+ * library that every GPU loading it keeps until process exit, which limits n
+ * to 67,108,864 symbols per call (larger n is rejected with CPSZ_ERR_INVALID).
  * All pointers are device memory: sym (n symbols), code/len (codebook from
  * cpsz_b200_huffman_codebook: every length must be at most 64 bits, which that
- * function guarantees -- the packer's shared-memory buffer is sized for it),
+ * function guarantees -- the packer appends codes of at most 64 bits),
  * out (out_cap bytes, 4-byte aligned, out_cap a multiple of 4, zeroed by the
  * call), total_bits (one uint64, receives the bit count).  The work is
  * enqueued on `stream` (a cudaStream_t; NULL = legacy default stream) and the
