@@ -370,8 +370,13 @@ __device__ __forceinline__ void hist_add(unsigned int* sh, unsigned long long* h
   }
 }
 
-__global__ void __launch_bounds__(HIST_NT) hist_u16_kernel(const uint16_t* __restrict__ s, size_t n,
-                                                           unsigned long long* __restrict__ hist) {
+// Stream blockIdx.y (s0 / s1, n symbols each) into its histogram (h0 / h1).
+__global__ void __launch_bounds__(HIST_NT) hist_u16_kernel(const uint16_t* __restrict__ s0,
+                                                           const uint16_t* __restrict__ s1, size_t n,
+                                                           unsigned long long* __restrict__ h0,
+                                                           unsigned long long* __restrict__ h1) {
+  const uint16_t* __restrict__ s = blockIdx.y ? s1 : s0;
+  unsigned long long* __restrict__ hist = blockIdx.y ? h1 : h0;
   __shared__ unsigned int sh[HIST_W + 1];  // window + symbol 0
   for (int k = threadIdx.x; k <= HIST_W; k += HIST_NT) sh[k] = 0;
   __syncthreads();
@@ -667,11 +672,16 @@ int launch_huff_encode_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, Hu
 }
 
 int launch_hist_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, unsigned long long* hist) {
+  return launch_hist_u16_pair(ctx, sym, nullptr, n, hist, nullptr);
+}
+int launch_hist_u16_pair(cpsz_b200_ctx* ctx, const uint16_t* a, const uint16_t* b, size_t n, unsigned long long* ha,
+                         unsigned long long* hb) {
   if (n == 0) return CPSZ_OK;
-  int grid = ctx->num_sms * 2;
+  const int k = b ? 2 : 1;
+  int grid = ctx->num_sms * 2 / k;
   size_t need = (n + HIST_NT - 1) / HIST_NT;
   if ((size_t)grid > need) grid = (int)need;
-  hist_u16_kernel<<<grid, HIST_NT, 0, ctx->stream>>>(sym, n, hist);
+  hist_u16_kernel<<<dim3(grid, k), HIST_NT, 0, ctx->stream>>>(a, b, n, ha, hb);
   count_launch(ctx);
   return check_launch("hist_u16_kernel");
 }

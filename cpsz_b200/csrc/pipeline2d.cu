@@ -461,9 +461,11 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
                      : 0;
   for (int k = 0; k < nj; k++) {
     Job2D& j = jobs[k];
-    for (int f = 0; f < 2; f++)
+    for (int f = 0; f < 2; f++) {
       CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.gbnd + ((size_t)f * j.ngroups + g0) * j.r2, 0,
                                     (size_t)(j.ngroups - g0) * j.r2 * 8, st));
+      CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.hist_codes[f], 0, 65536 * 8, st));  // stage 3's histograms
+    }
     if (overlap) CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.band, 0, ((size_t)j.ngroups + 1) * 8, st));
     for (int f = 0; f < 2; f++) {
       WaveField& F = hf[2 * k + f];
@@ -626,9 +628,8 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     // them while the GPU converts to block order and gathers unpredictables) ----
     for (int k = 0; k < nj; k++) {
       Job2D& j = jobs[k];
+      CPSZ_TRY(launch_hist_u16_pair(ctx, j.d.craster[0], j.d.craster[1], j.N, j.d.hist_codes[0], j.d.hist_codes[1]));
       for (int f = 0; f < 2; f++) {
-        CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.hist_codes[f], 0, 65536 * 8, st));
-        CPSZ_TRY(launch_hist_u16(ctx, j.d.craster[f], j.N, j.d.hist_codes[f]));
         CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_hist_codes + (size_t)f * 65536, j.d.hist_codes[f], 65536 * 8,
                                       cudaMemcpyDeviceToHost, st));
         CPSZ_CUDA_TRY(record(ctx->job_ev[2 * k + f]));
@@ -795,7 +796,10 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       CPSZ_CUDA_TRY(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), st));
       for (WaveField& F : hf) F.band_done = nullptr;
       CPSZ_CUDA_TRY(cudaMemcpyAsync(d_fields, hf.data(), hf.size() * sizeof(WaveField), cudaMemcpyHostToDevice, st));
-      for (Job2D& j : jobs) CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.gbnd, 0, 2 * (size_t)j.ngroups * j.r2 * 8, st));
+      for (Job2D& j : jobs) {
+        CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.gbnd, 0, 2 * (size_t)j.ngroups * j.r2 * 8, st));
+        for (int f = 0; f < 2; f++) CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.hist_codes[f], 0, 65536 * 8, st));
+      }
       CPSZ_CUDA_TRY(cudaMemsetAsync(queue, 0, 64, st));
       CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points));
       CPSZ_TRY(stage_3());
