@@ -47,6 +47,9 @@ WORKLOADS = {
     "2d_2400x3600_eb0.1": ("2d", (2400, 3600), 0.1, "cfg0"),
     # profiling-size case of the same kernels (cfg0 generator at 4096^2, 134 MB > L2)
     "2d_4096x4096_eb0.1": ("2d", (4096, 4096), 0.1, "cfg0like"),
+    # profiling-size case with the 8192^2 field's flow density and width (cfg1
+    # generator at 4096^2: 500 flows, sigma 60; critical points as sparse as there)
+    "2d_4096x4096_cfg1like_eb0.1": ("2d", (4096, 4096), 0.1, "cfg1like"),
     "3d_384x384x384_eb0.05": ("3d", (384, 384, 384), 0.05, "cfg2"),
     # profiling-size case of the 3D kernels (cfg2 generator at 256^3, 201 MB > L2)
     "3d_256x256x256_eb0.05": ("3d", (256, 256, 256), 0.05, "cfg2"),
@@ -135,6 +138,11 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(self.rows)}
 
 
+def CFG1LIKE_FLOWS(r1: int, r2: int) -> int:
+    """Flows of a field with the 8192^2 workload's density (2000 per 8192^2)."""
+    return max(1, round(2000 / (8192 * 8192) * r1 * r2))
+
+
 def make_fields(workload: str, seed_offset: int = 0):
     from cpsz_b200 import workloads as W
 
@@ -145,6 +153,8 @@ def make_fields(workload: str, seed_offset: int = 0):
         return W.cfg0(0 + seed_offset), eb
     if gen == "cfg0like":
         return W.cfg0_like(5 + seed_offset, *shape), eb
+    if gen == "cfg1like":
+        return W.field_2d(1 + seed_offset, *shape, CFG1LIKE_FLOWS(*shape), 60.0), eb
     if gen == "cfg0like_heldout":
         return W.cfg0_like(123457 + seed_offset, *shape), eb
     if gen == "cfg2":
@@ -168,6 +178,8 @@ def oracle_fields(workload: str, seed_offset: int = 0):
     kind, shape, eb, gen = WORKLOADS[workload]
     if gen == "cfg1":
         return O.field_2d(1 + seed_offset, 8192, 8192, 2000, 60.0), eb
+    if gen == "cfg1like":
+        return O.field_2d(1 + seed_offset, *shape, CFG1LIKE_FLOWS(*shape), 60.0), eb
     if gen == "cfg0":
         return O.field_2d(0 + seed_offset, 2400, 3600, 200, 40.0), eb
     if gen in ("cfg0like", "cfg0like_heldout"):

@@ -40,6 +40,7 @@ DEFAULT_OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning_b
 # wavefront run side by side, so either one's shape moves both stages.
 SWEEP = {
     "wave2d.overlap": ("2d", "eb2d+wave2d_compress", [0, 1], 0),
+    "eb2d.skew": ("2d", "eb2d+wave2d_compress", [0, 1, 2, 4, 8], 0),
     "eb2d.tile": ("2d", "eb2d+wave2d_compress", [0, 1, 2, 3, 4, 5], 0),
     "wave2d.ctas_per_sm": ("2d", "wave2d_compress", [0, 1, 2, 3, 4], 0),
     "h2d.chunks": ("2d_host", "e2e", [1, 2, 4, 8, 16, 24, 32], 1 << 22),

@@ -23,6 +23,8 @@
 // roughly in order): measured faster than a persistent grid that takes tiles
 // with a stride or from a counter (3.75 against 4.27 ms at 8192^2 alone, and
 // the wavefront beside it keeps pace only with the per-tile grid).
+#include <algorithm>
+
 #include "eb_math.cuh"
 #include "kernels.h"
 #include "tuning.h"
@@ -38,10 +40,12 @@ __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const f
                                                   unsigned long long* __restrict__ hist, int* __restrict__ flag,
                                                   float2* __restrict__ pair_u, float2* __restrict__ pair_v,
                                                   double* __restrict__ eb_out, int row_begin, int row_end,
-                                                  unsigned long long* __restrict__ band_done, int log_ids) {
+                                                  const int2* __restrict__ unit_order, int unit_ncb,
+                                                  unsigned long long* __restrict__ unit_done, int log_ids) {
   constexpr int CX = TX + 1;  // cells per tile row
   constexpr int CY = TY + 1;
   static_assert(WAVE_GROUP_ROWS % TY == 0, "a tile's rows must lie in one wavefront group");
+  static_assert(UNIT_COLS % TX == 0, "a tile's columns must lie in one unit");
   __shared__ float su[TY + 2][TX + 3];
   __shared__ float sv[TY + 2][TX + 3];
   // compression (FAST): the float bound of an ordinary triangle, or -1 when
@@ -52,7 +56,19 @@ __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const f
   __shared__ unsigned int shist[256];
 
   const int tid = threadIdx.x;
-  const int i0 = row_begin + blockIdx.y * TY, j0 = blockIdx.x * TX;
+  int i0, j0;
+  if (unit_order) {
+    // tile t of unit blockIdx.x / tiles-per-unit, row-major inside the unit
+    constexpr int TPR = UNIT_COLS / TX;  // tiles per unit row
+    const int2 u = unit_order[blockIdx.x / (TPR * (WAVE_GROUP_ROWS / TY))];
+    const int t = blockIdx.x % (TPR * (WAVE_GROUP_ROWS / TY));
+    i0 = u.x * WAVE_GROUP_ROWS + (t / TPR) * TY;
+    j0 = u.y * UNIT_COLS + (t % TPR) * TX;
+    if (i0 >= row_end || j0 >= r2) return;  // beyond the field's last rows / columns (uniform)
+  } else {
+    i0 = row_begin + blockIdx.y * TY;
+    j0 = blockIdx.x * TX;
+  }
   for (int k = tid; k < 256; k += NT) shist[k] = 0;
   for (int k = tid; k < thr_n; k += NT) tab[k] = thr_tab[k];
   // vertex halo: rows i0-1 .. i0+TY, cols j0-1 .. j0+TX
@@ -205,17 +221,27 @@ __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const f
   __syncthreads();
   for (int k = tid; k < 256; k += NT)
     if (shist[k]) atomicAdd(&hist[k], (unsigned long long)shist[k]);
-  if (band_done) {
+  if (unit_done) {
     // every thread's outputs are visible device-wide before the tile counts;
-    // band_done[-1] counts finished tiles (the wavefront's sign of progress)
+    // unit_done[-1] counts finished tiles (the wavefront's sign of progress)
     __threadfence();
     __syncthreads();
     if (tid == 0) {
       const int rows = min(TY, row_end - i0), cols = min(TX, r2 - j0);
-      atomicAdd(&band_done[i0 / WAVE_GROUP_ROWS], (unsigned long long)rows * cols);
-      atomicAdd(&band_done[-1], 1ull);
+      atomicAdd(&unit_done[(i0 / WAVE_GROUP_ROWS) * unit_ncb + j0 / UNIT_COLS], (unsigned long long)rows * cols);
+      atomicAdd(&unit_done[-1], 1ull);
     }
   }
+}
+
+void unit_order(int g0, int g1, int ncb, int skew, std::vector<int2>& out) {
+  out.clear();
+  for (int g = g0; g < g1; g++)
+    for (int b = 0; b < ncb; b++) out.push_back(make_int2(g, b));
+  std::stable_sort(out.begin(), out.end(), [&](const int2& a, const int2& c) {
+    const long long ka = (long long)a.y * skew + a.x, kc = (long long)c.y * skew + c.x;
+    return ka < kc;
+  });
 }
 
 int preload_eb2d() {
@@ -240,17 +266,25 @@ int preload_eb2d() {
 int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, double max_pwr_eb,
                 const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
                 float2* pair_u, float2* pair_v, double* eb_out, int row_begin, int row_end,
-                unsigned long long* band_done, bool log_ids) {
+                const Eb2dUnits* units, bool log_ids) {
   if (row_end < 0) row_end = r1;
   if (log_ids && (pair_u || pair_v || ids_v))
     return set_error(CPSZ_ERR_INVALID, "eb2d: the log-domain ids have no wavefront pairs and one stream");
   if (row_end <= row_begin) return CPSZ_OK;
-  if (band_done && row_begin % WAVE_GROUP_ROWS)
+  if (units && row_begin % WAVE_GROUP_ROWS)
     return set_error(CPSZ_ERR_INVALID, "eb2d band start %d is not a multiple of %d", row_begin, WAVE_GROUP_ROWS);
   auto go = [&](auto kernel, int tx, int ty, int nt) {
+    if (units) {
+      const long long tiles = (long long)units->n * (UNIT_COLS / tx) * (WAVE_GROUP_ROWS / ty);
+      kernel<<<(unsigned)tiles, nt, 0, ctx->stream>>>(U, V, r1, r2, max_pwr_eb, d_thr_tab, thr_n, ids_u, ids_v, hist,
+                                                      ctx->d_flag, pair_u, pair_v, eb_out, row_begin, row_end,
+                                                      units->order, units->ncb, units->done, log_ids ? 1 : 0);
+      return;
+    }
     dim3 grid((r2 + tx - 1) / tx, (row_end - row_begin + ty - 1) / ty);
     kernel<<<grid, nt, 0, ctx->stream>>>(U, V, r1, r2, max_pwr_eb, d_thr_tab, thr_n, ids_u, ids_v, hist, ctx->d_flag,
-                                         pair_u, pair_v, eb_out, row_begin, row_end, band_done, log_ids ? 1 : 0);
+                                         pair_u, pair_v, eb_out, row_begin, row_end, nullptr, 0, nullptr,
+                                         log_ids ? 1 : 0);
   };
   // filtered bounds unless the caller wants the bounds themselves (or an
   // unusual max_pwr_eb takes the reference's NaN paths)

@@ -3,6 +3,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 #include "libm.h"
 #include "runtime.h"
@@ -24,20 +25,35 @@ constexpr int FLAG_RAW_RANGE = 8;     // an unpredictable-value index fell outsi
 constexpr int FLAG_OUT_CAPACITY = 16; // an output stream did not fit its buffer
 
 // ---- 2D error bounds ---------------------------------------------------------
+// The bound kernel beside the wavefront runs unit by unit: a unit is a
+// (WAVE_GROUP_ROWS-row group, UNIT_COLS-column block) of vertices, and the
+// units go in `order` (host-made by unit_order), so that the wavefront, which
+// waits per unit, meets its inputs along its own diagonal.  Every tile adds
+// the vertices it finished to its unit's counter after its outputs are
+// visible device-wide; done[-1] counts finished tiles, the waiting
+// wavefront's sign that the kernel is running.
+constexpr int UNIT_COLS = 256;
+struct Eb2dUnits {
+  const int2* order = nullptr;         // device: the launch's units, (group, column block)
+  int n = 0;                           // units in order
+  int ncb = 0;                         // column blocks per group: ceil(r2 / UNIT_COLS)
+  unsigned long long* done = nullptr;  // device: one counter per unit (group * ncb + block), zeroed
+};
+// The units of groups [g0, g1) in production order: unit (g, b) before
+// (g', b') when b * skew + g is smaller (ties: lower group first); skew 0 is
+// row order.
+void unit_order(int g0, int g1, int ncb, int skew, std::vector<int2>& out);
+
 // Rows [row_begin, row_end) of the vertex outputs (row_end < 0: all rows); the
-// kernel reads rows row_begin - 1 .. row_end of U and V.  With `band_done`
-// (one counter per WAVE_GROUP_ROWS-row group, zeroed beforehand), every tile
-// adds the number of vertices it finished to its group's counter after its
-// outputs are visible device-wide (row_begin must then be a multiple of
-// WAVE_GROUP_ROWS), so a concurrently running wavefront can start on a group
-// as soon as its counter reaches rows x r2; band_done[-1] counts finished
-// tiles, the waiting wavefront's sign that the kernel is running.
+// kernel reads rows row_begin - 1 .. row_end of U and V.  With `units`
+// (row_begin a multiple of WAVE_GROUP_ROWS; the order holds exactly the
+// units of the rows' groups), the tiles run in unit order and count.
 // log_ids: the offline_log form -- one id per vertex, of the vertex bound
 // itself against quant_table_2d_log() (ids_v, pair_u and pair_v null).
 int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, double max_pwr_eb,
                 const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
                 float2* pair_u, float2* pair_v, double* eb_out = nullptr, int row_begin = 0, int row_end = -1,
-                unsigned long long* band_done = nullptr, bool log_ids = false);
+                const Eb2dUnits* units = nullptr, bool log_ids = false);
 
 // Loads every eb2d instantiation (required before a consumer that waits on
 // eb2d is launched: a lazily loaded first launch could wait for it).
@@ -69,13 +85,15 @@ struct WaveField {
   // optional diagnostics: per (group, warp) 4 counters {start clock, end clock,
   // spins waiting for the row above, spins waiting for ring credit}
   long long* trace;
-  // optional: per-group counters of input points written by a concurrently
-  // running producer (launch_eb2d's band_done, band_done[-1] its finished
-  // tiles); an item starts once its group's counter reaches rows x r2 +
-  // band_extra.  The wait gives up (FLAG_TIMEOUT) once the producer has shown
+  // optional: per-unit counters of input points written by a concurrently
+  // running producer (launch_eb2d's units.done, unit_done[-1] its finished
+  // tiles, unit_ncb column blocks per group); a window of the recurrence
+  // starts once the counters of the units it reads reach their vertex counts
+  // + band_extra.  A wait gives up (FLAG_TIMEOUT) once the producer has shown
   // no progress for band_wait_ns (0: the default).  band_extra is 0 except in
   // the test that makes the wait run out on purpose.
-  const unsigned long long* band_done;
+  const unsigned long long* unit_done;
+  int unit_ncb;
   long long band_wait_ns;
   unsigned long long band_extra;
 };
@@ -89,7 +107,7 @@ constexpr int WAVE_GROUP_ROWS = WAVE_WARPS * 32;
 // (all fields of the launch together) keys the launch-shape table.  The launch
 // goes to `stream` (default: the context's stream).  Modes:
 //   WAVE_ALONE   the only wavefront launch on the queue: the tuned CTAs per SM;
-//   WAVE_BESIDE  runs beside its producer (fields with band_done): one CTA per
+//   WAVE_BESIDE  runs beside its producer (fields with unit_done): one CTA per
 //                SM, which leaves every SM room for the producer's CTAs, so
 //                the producer always progresses while wavefront CTAs wait;
 //   WAVE_JOIN    launched once the producer is done, while a WAVE_BESIDE launch

@@ -62,7 +62,8 @@ struct DevBuf {
   uint16_t* cblocks[2];
   unsigned long long* hist_codes[2];
   unsigned long long* gbnd;
-  unsigned long long* band;  // per-group counters of finished eb2d vertices
+  unsigned long long* units;  // eb2d progress word, then per-unit counters of finished vertices
+  int2* uorder;               // eb2d's unit order (every band's units, band after band)
   void* strip[2];            // strip-pass look-back words and counters
   float* unpred[2];
   unsigned long long* enc_code[3];
@@ -80,7 +81,7 @@ struct DevBuf {
 struct Job2D {
   const float* U_in = nullptr;
   const float* V_in = nullptr;
-  int r1 = 0, r2 = 0, ngroups = 0;
+  int r1 = 0, r2 = 0, ngroups = 0, ncb = 0;
   size_t N = 0, nseg = 0, nblocks = 0;
   double eb = 0;
   const double* eb_ext = nullptr;  // given per-vertex bounds (device), else derived
@@ -156,6 +157,7 @@ int job_init(Job2D& j, const float* U, const float* V, size_t r1s, size_t r2s, d
   j.N = r1s * r2s;
   j.eb = eb;
   j.ngroups = (j.r1 + WAVE_GROUP_ROWS - 1) / WAVE_GROUP_ROWS;
+  j.ncb = (j.r2 + UNIT_COLS - 1) / UNIT_COLS;
   const int nby = (j.r2 - 1) / BS + 1, nbx = (j.r1 - 1) / BS + 1;
   j.nseg = (size_t)j.r1 * nby;
   j.nblocks = (size_t)nbx * nby;
@@ -189,7 +191,8 @@ size_t job_bytes(const Job2D& j) {
   add(4 * N);                           // codes blocks
   add(2 * 65536 * 8);                   // hist codes
   add(2 * (size_t)j.ngroups * j.r2 * 8);  // boundary rows (tagged words)
-  add(((size_t)j.ngroups + 1) * 8);       // eb2d progress word + group counters
+  add(((size_t)j.ngroups * j.ncb + 1) * 8);       // eb2d progress word + unit counters
+  add((size_t)j.ngroups * j.ncb * sizeof(int2));  // eb2d unit order
   add(2 * strip_scratch_bytes(j.r1, j.r2));
   add(2 * 4 * N);  // unpred
   add(256 * 9);
@@ -230,7 +233,8 @@ int job_alloc(cpsz_b200_ctx* ctx, Job2D& j) {
     d.hist_codes[f] = (unsigned long long*)A(65536 * 8);
   }
   d.gbnd = (unsigned long long*)A(2 * (size_t)j.ngroups * j.r2 * 8);
-  d.band = (unsigned long long*)A(((size_t)j.ngroups + 1) * 8);
+  d.units = (unsigned long long*)A(((size_t)j.ngroups * j.ncb + 1) * 8);
+  d.uorder = (int2*)A((size_t)j.ngroups * j.ncb * sizeof(int2));
   for (int f = 0; f < 2; f++) {
     d.strip[f] = A(strip_scratch_bytes(j.r1, j.r2));
     d.unpred[f] = (float*)A(4 * N);
@@ -444,6 +448,12 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   // wavefront after the bounds with every CTA slot.
   const bool overlap =
       nj == 1 && jobs[0].eb_ext == nullptr && !log_form && tune_get(TUNE_WAVE2D_OVERLAP, jobs[0].N) != 0;
+  // Host input is uploaded and bounded in bands of band_rows(j) rows (a
+  // multiple of WAVE_GROUP_ROWS), band c right after its upload.
+  auto band_rows = [&](const Job2D& j) -> int {
+    const int K = (!j.dev_in && j.N >= ((size_t)1 << 22) && !j.eb_ext) ? tune_get(TUNE_H2D_CHUNKS, j.N) : 1;
+    return (int)align_up((size_t)(j.r1 + K - 1) / K, WAVE_GROUP_ROWS);
+  };
 
   // ---- setup: flags, tables, wavefront descriptors ----
   reset_marks(ctx);
@@ -466,7 +476,24 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
                                     (size_t)(j.ngroups - g0) * j.r2 * 8, st));
       CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.hist_codes[f], 0, 65536 * 8, st));  // stage 3's histograms
     }
-    if (overlap) CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.band, 0, ((size_t)j.ngroups + 1) * 8, st));
+    if (overlap) {
+      // eb2d's unit counters and its unit order, band by band (units along
+      // diagonals of slope eb2d.skew column blocks per group)
+      CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.units, 0, ((size_t)j.ngroups * j.ncb + 1) * 8, st));
+      const int R = band_rows(j), skew = tune_get(TUNE_EB2D_SKEW, j.N);
+      std::vector<int2> order, part;
+      for (int r0 = 0; r0 < j.r1; r0 += R) {
+        unit_order(r0 / WAVE_GROUP_ROWS, (std::min(j.r1, r0 + R) + WAVE_GROUP_ROWS - 1) / WAVE_GROUP_ROWS, j.ncb, skew,
+                   part);
+        order.insert(order.end(), part.begin(), part.end());
+      }
+      // through the page-locked upload staging (no copy from it is in flight
+      // yet; the pass's later uploads reuse it after this copy has run)
+      CPSZ_TRY(upload_reserve(ctx, order.size() * sizeof(int2)));
+      memcpy(ctx->up_pinned, order.data(), order.size() * sizeof(int2));
+      CPSZ_CUDA_TRY(
+          cudaMemcpyAsync(j.d.uorder, ctx->up_pinned, order.size() * sizeof(int2), cudaMemcpyHostToDevice, st));
+    }
     for (int f = 0; f < 2; f++) {
       WaveField& F = hf[2 * k + f];
       F.pair = j.d.pairs[f];
@@ -481,7 +508,8 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       F.out_pitch = j.r2;
       F.r1 = j.r1;
       F.r2 = j.r2;
-      F.band_done = overlap ? j.d.band + 1 : nullptr;
+      F.unit_done = overlap ? j.d.units + 1 : nullptr;
+      F.unit_ncb = j.ncb;
       F.band_wait_ns = ctx->band_wait_ns;
       F.band_extra = ctx->band_unreachable ? 1 : 0;
       r1v[2 * k + f] = j.r1;
@@ -547,7 +575,16 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       CPSZ_CUDA_TRY(cudaStreamWaitEvent(ctx->aux, ctx->ev[2], 0));
     }
     for (Job2D& j : jobs) {
-      unsigned long long* band = overlap ? j.d.band + 1 : nullptr;  // [-1]: tiles finished
+      // beside the wavefront, eb2d runs unit by unit in the order made in the
+      // setup; band_units(g0, g1) is the slice for the rows of groups [g0, g1)
+      auto band_units = [&](int g0, int g1) {
+        Eb2dUnits u;
+        u.order = j.d.uorder + (size_t)g0 * j.ncb;
+        u.n = (g1 - g0) * j.ncb;
+        u.ncb = j.ncb;
+        u.done = j.d.units + 1;  // [-1]: tiles finished
+        return u;
+      };
       if (j.log_form) {
         // offline_log: the fields whole, one id per vertex, then the logs,
         // wavefront pairs and sign maps
@@ -566,9 +603,11 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
         else if (j.eb_ext)
           CPSZ_TRY(launch_quant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
                                   j.d.hist_ids, j.d.pairs[0], j.d.pairs[1]));
-        else
+        else {
+          const Eb2dUnits u = band_units(0, j.ngroups);
           CPSZ_TRY(launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
-                               j.d.hist_ids, j.d.pairs[0], j.d.pairs[1], nullptr, 0, -1, band));
+                               j.d.hist_ids, j.d.pairs[0], j.d.pairs[1], nullptr, 0, -1, overlap ? &u : nullptr));
+        }
       } else {
         // Host input: row chunks go up on the second stream and the bound kernel
         // runs band by band as soon as a band's rows and the row below it are
@@ -577,8 +616,7 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
         // and the next band's first row (which chunk c + 1 writes again, with
         // the same bytes), so band c waits for chunk c alone and only the last
         // band's bounds follow the end of the transfer.
-        const int K = (j.N >= ((size_t)1 << 22) && !j.eb_ext) ? tune_get(TUNE_H2D_CHUNKS, j.N) : 1;
-        const int R = (int)align_up((size_t)(j.r1 + K - 1) / K, WAVE_GROUP_ROWS);
+        const int R = band_rows(j);
         const int nch = (j.r1 + R - 1) / R;
         // band c is enqueued right after chunk c's copy call (a copy from
         // pageable memory returns only once the host has staged it, so
@@ -589,8 +627,11 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
           if (j.eb_ext)
             return launch_quant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
                                   j.d.hist_ids, j.d.pairs[0], j.d.pairs[1]);
+          const Eb2dUnits u = band_units(c * R / WAVE_GROUP_ROWS, (std::min(j.r1, (c + 1) * R) + WAVE_GROUP_ROWS - 1) /
+                                                                     WAVE_GROUP_ROWS);
           return launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N, j.d.hist_ids,
-                             j.d.pairs[0], j.d.pairs[1], nullptr, c * R, std::min(j.r1, (c + 1) * R), band);
+                             j.d.pairs[0], j.d.pairs[1], nullptr, c * R, std::min(j.r1, (c + 1) * R),
+                             overlap ? &u : nullptr);
         };
         for (int c = 0; c < nch; c++) {
           const size_t off = (size_t)c * R * j.r2;
@@ -794,7 +835,7 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     if (snap & FLAG_TIMEOUT) {
       if (snap != FLAG_TIMEOUT) return flag_error(snap);
       CPSZ_CUDA_TRY(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), st));
-      for (WaveField& F : hf) F.band_done = nullptr;
+      for (WaveField& F : hf) F.unit_done = nullptr;
       CPSZ_CUDA_TRY(cudaMemcpyAsync(d_fields, hf.data(), hf.size() * sizeof(WaveField), cudaMemcpyHostToDevice, st));
       for (Job2D& j : jobs) {
         CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.gbnd, 0, 2 * (size_t)j.ngroups * j.r2 * 8, st));

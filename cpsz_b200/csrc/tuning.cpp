@@ -29,6 +29,7 @@ const TuneInfo kInfo[TUNE_COUNT] = {
     {"eb3d.min_chunk", 8, 1, 256},
     {"h2d.chunks", 8, 1, 32},
     {"wave2d.overlap", 1, 0, 1},
+    {"eb2d.skew", 1, 0, 64},
 };
 
 struct Entry {

@@ -30,6 +30,8 @@ enum TuneParam {
   TUNE_WAVE2D_OVERLAP,      // 1: the wavefront runs beside eb2d (0: after it; tools
                             // that serialize kernels need 0, also set by
                             // the environment variable CPSZ_B200_OVERLAP=0)
+  TUNE_EB2D_SKEW,           // beside the wavefront: eb2d's unit order, column
+                            // blocks per group of lag (0: row order)
   TUNE_COUNT
 };
 

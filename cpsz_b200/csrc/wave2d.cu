@@ -43,11 +43,14 @@
 //    queue (atomic counter).  An item's predecessor (same field, previous
 //    group) was dequeued earlier by a running CTA, so every wait ends;
 //  * compression runs beside its producer: the bound kernel (eb2d) counts the
-//    points it has finished per group, and an item starts when its group's
-//    count is complete (one thread polls with ld.acquire.gpu, every thread
-//    then acquires before its first load).  Such a launch keeps to one CTA per
-//    SM, so each SM keeps room for the producer's CTAs and the producer
-//    cannot be starved by waiting consumers.  The wait ends with FLAG_TIMEOUT
+//    points it has finished per unit (a 128-row group x 256-column block) and
+//    produces the units along diagonals that follow the wavefront's own skew,
+//    so a group's recurrence sweeps along as its inputs appear instead of
+//    waiting for the whole group; a helper warp stages a window once the
+//    units it reads are complete (lane 0 polls with ld.acquire.gpu, every
+//    lane then acquires before its loads).  Such a launch keeps to one CTA
+//    per SM, so each SM keeps room for the producer's CTAs and the producer
+//    cannot be starved by waiting consumers.  A wait ends with FLAG_TIMEOUT
 //    when the producer has finished no tile for a while (it is not running
 //    beside it), and the host then runs the wavefront again after it.
 //
@@ -171,15 +174,61 @@ __device__ __forceinline__ void tile_drain(const WaveField& F, const WarpTiles& 
   }
 }
 
+// Compression beside the producer: before window k is staged, wait until the
+// producer has finished the units of this group that it reads (columns up to
+// 32k + 31).  Lane 0 polls; every lane then acquires.  `ready` is the first
+// column block not yet known finished.  A wait gives up (FLAG_TIMEOUT) once
+// the producer has finished no tile for the limit, and ends at once when an
+// earlier wait gave up.
+__device__ __forceinline__ void wait_units(const WaveField& F, int group, int k, int lane, int& ready, int* flag) {
+  const int cb_hi = min(32 * k + 31, F.r2 - 1) / UNIT_COLS;
+  if (cb_hi < ready) return;
+  const unsigned long long* row = F.unit_done + (size_t)group * F.unit_ncb;
+  if (lane == 0) {
+    const unsigned long long rows = (unsigned long long)min(WAVE_GROUP_ROWS, F.r1 - group * WAVE_GROUP_ROWS);
+    const long long limit = F.band_wait_ns > 0 ? F.band_wait_ns : BAND_WAIT_NS;
+    for (int cb = ready; cb <= cb_hi; cb++) {
+      const unsigned long long target =
+          rows * (unsigned long long)min(UNIT_COLS, F.r2 - cb * UNIT_COLS) + F.band_extra;
+      if (ld_acquire(row + cb) >= target) continue;
+      // progress: the producer's count of finished tiles (unit_done[-1])
+      const unsigned long long* tiles = F.unit_done - 1;
+      unsigned long long seen = ld_acquire(tiles);
+      long long t_seen = globaltimer_ns();
+      while (ld_acquire(row + cb) < target) {
+        if (*(volatile int*)flag & FLAG_TIMEOUT) break;
+        const unsigned long long now_tiles = ld_acquire(tiles);
+        const long long now = globaltimer_ns();
+        if (now_tiles != seen) {
+          seen = now_tiles;
+          t_seen = now;
+        } else if (now - t_seen > limit) {
+          atomicOr(flag, FLAG_TIMEOUT);
+          break;
+        }
+        __nanosleep(500);
+      }
+    }
+  }
+  __syncwarp();
+  (void)ld_acquire(row + cb_hi);
+  ready = cb_hi + 1;
+}
+
 template <bool DECOMP>
-__device__ __forceinline__ void run_helper(const WaveField& F, int group, int strip, int lane, WarpTiles& T) {
+__device__ __forceinline__ void run_helper(const WaveField& F, int group, int strip, int lane, WarpTiles& T,
+                                           int* flag) {
   const long long row0 = (long long)group * WAVE_GROUP_ROWS + strip * 32;
   const int nrows = min(32, F.r1 - (int)row0);
   const int nwin = (F.r2 + 31 + 31) / 32;  // windows that contain any step
+  const bool waits = !DECOMP && F.unit_done;
+  int ready = 0;
+  if (waits) wait_units(F, group, 0, lane, ready, flag);
   tile_fill<DECOMP>(F, T, row0, nrows, lane, 0, 0);
   cp_wait_all();
   for (int k = 0; k < nwin; k++) {
     pair_sync(strip);  // the compute warp starts window k (tiles buf = k & 1)
+    if (waits && k + 1 < nwin) wait_units(F, group, k + 1, lane, ready, flag);
     if (k + 1 < nwin) tile_fill<DECOMP>(F, T, row0, nrows, lane, k + 1, (k + 1) & 1);
     if (k >= 1) tile_drain<DECOMP>(F, T, row0, nrows, lane, k - 1, (k - 1) & 1);
     cp_wait_all();
@@ -381,44 +430,12 @@ __device__ __forceinline__ void wave2d_body(const WaveField* __restrict__ fields
     if (it >= n_items) break;
     const WaveItem item = items[it];
     const WaveField F = fields[item.field];
-    if (F.band_done) {
-      // the producer (eb2d) runs concurrently: wait until every input point of
-      // this group is written; one thread polls, then every thread acquires
-      const unsigned long long* cnt = F.band_done + item.group;
-      const unsigned long long target =
-          (unsigned long long)min(WAVE_GROUP_ROWS, F.r1 - item.group * WAVE_GROUP_ROWS) * (unsigned long long)F.r2 +
-          F.band_extra;
-      const long long limit = F.band_wait_ns > 0 ? F.band_wait_ns : BAND_WAIT_NS;
-      if (threadIdx.x == 0 && ld_acquire(cnt) < target) {
-        // progress: the producer's count of finished tiles (band_done[-1])
-        const unsigned long long* tiles = F.band_done - 1;
-        unsigned long long seen = ld_acquire(tiles);
-        long long t_seen = globaltimer_ns();
-        while (ld_acquire(cnt) < target) {
-          // a wait that already gave up (this launch or the producer failed)
-          // ends every later wait at once
-          if (*(volatile int*)flag & FLAG_TIMEOUT) break;
-          const unsigned long long now_tiles = ld_acquire(tiles);
-          const long long now = globaltimer_ns();
-          if (now_tiles != seen) {
-            seen = now_tiles;
-            t_seen = now;
-          } else if (now - t_seen > limit) {
-            atomicOr(flag, FLAG_TIMEOUT);
-            break;
-          }
-          __nanosleep(256);
-        }
-      }
-      __syncthreads();
-      (void)ld_acquire(cnt);
-    }
     if (item.group * WAVE_GROUP_ROWS + strip * 32 < F.r1) {
       if (warp < WAVE_WARPS) {
         if (!DECOMP && F.out) run_strip<DECOMP, true>(F, item.group, strip, lane, sh, tiles[strip], flag);
         else run_strip<DECOMP, false>(F, item.group, strip, lane, sh, tiles[strip], flag);
       }
-      else run_helper<DECOMP>(F, item.group, strip, lane, tiles[strip]);
+      else run_helper<DECOMP>(F, item.group, strip, lane, tiles[strip], flag);
     }
     __syncthreads();
   }

@@ -23,7 +23,7 @@ def _restore_table():
 def test_parameters_and_defaults():
     p = cpsz_b200.tuning_params()
     assert set(p) == {"eb2d.tile", "wave2d.ctas_per_sm", "eb3d.fill", "eb3d.min_chunk", "h2d.chunks",
-                      "wave2d.overlap"}
+                      "wave2d.overlap", "eb2d.skew"}
     for name, (d, lo, hi) in p.items():
         assert lo <= d <= hi
     cpsz_b200.tuning_clear()
