@@ -458,6 +458,29 @@ def run_product(args, rank, world, device):
         e2e_size = comp(*hptr, *shape, eb, h_out, ctx=ctx)
     e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
     blob = h_out[:e2e_size].tobytes()
+    # ---- end to end with the lossless stage on the GPU: pinned host fields
+    # in, the blob built in device memory, a Zstandard frame of it written on
+    # the GPU (the reference's sz_lossless_decompress reads it) and read back
+    # into pinned host memory ----
+    lossless_gpu = None
+    if kind == "2d":
+        h_frame = torch.empty(e2e_size + e2e_size // 64 + (1 << 20), dtype=torch.uint8).pin_memory().numpy()
+
+        def step_lossless():
+            n = comp(*hptr, *shape, eb, d_out, ctx=ctx)
+            return cpsz_b200.lossless_compress_gpu(d_out[:n], out=h_frame, ctx=ctx)
+
+        for _ in range(2):
+            fsize = step_lossless()
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            fsize = step_lossless()
+        ll_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+        frame = h_frame[:fsize].tobytes()
+        lossless_gpu = {"e2e": round(raw_bytes / (ll_ms / 1e3) / 1e9, 3), "unit": "GB/s", "ms_per_step": round(ll_ms, 4),
+                        "frame_bytes": fsize, "ratio": round(raw_bytes / fsize, 4),
+                        "frame_decodes_to_blob": cpsz_b200.sz_lossless_decompress(frame, len(blob)) == blob}
     # ---- decompression (host blob in, host fields out) ----
     decompress = (cpsz_b200.sz_decompress_cp_preserve_2d_offline if kind == "2d"
                   else cpsz_b200.sz_decompress_cp_preserve_3d_online_log)
@@ -495,7 +518,8 @@ def run_product(args, rank, world, device):
                 "algorithmic_bytes": alg[dom]}
     return {
         "value": value, "ms": ms, "e2e_ms": e2e_ms, "dec_ms": dec_ms, "blob": len(blob), "size_dev": size,
-        "lossless": len(lossless), "raw": raw_bytes, "stages": stages, "roofline": roof, "launches": launches,
+        "lossless": len(lossless), "lossless_gpu": lossless_gpu, "raw": raw_bytes, "stages": stages, "roofline": roof,
+        "launches": launches,
         "clocks": clk.summary(), "fields": fields, "eb": eb, "blob_bytes": blob, "check": check,
     }
 
@@ -805,6 +829,8 @@ def main():
         "decompress_GBps_e2e": round(raw / (r["dec_ms"] / 1e3) / 1e9, 3),
         "e2e": {"value": round(raw / (r["e2e_ms"] / 1e3) / 1e9, 3), "unit": "GB/s", "h2d_bytes_per_step": raw,
                 "d2h_bytes_per_step": r["blob"]},
+        # the same, with the lossless stage on the GPU (frame read back instead of the blob)
+        "e2e_with_lossless_gpu": r["lossless_gpu"],
         "roofline": r["roofline"], "stages_ms": {k: round(v, 4) for k, v in r["stages"].items()},
         "cpu_baseline": cpu, "parity": parity, **r["check"], "clocks": r["clocks"], "gpu_launches": r["launches"],
     }

@@ -3,11 +3,17 @@
 // The reference applies ZSTD_compress(level 3) to every blob on the host
 // (src/sz_lossless.cpp:11-26); here the same kind of frame is written on the
 // GPU (format: zstd_format.h), readable by any Zstandard decoder and so by the
-// reference's sz_lossless_decompress.  The input is cut into 32 KB blocks that
-// are encoded independently, one warp each:
+// reference's sz_lossless_decompress.  The input is cut into 8 KB blocks that
+// are encoded independently, one warp each (16 warps an SM):
+//   0. the warp stages its block in shared memory with 16-byte loads, so the
+//      match loop below (a dependent chain: one step per match on the
+//      Huffman bit streams of a blob, a match every few bytes) waits on
+//      shared memory, not on global loads (32 KB blocks read from global
+//      memory: 9.6 ms for a 89 MB blob; staged, with four warps an SM for
+//      lack of shared memory: 17.7 ms);
 //   1. greedy matching: the warp looks at 32 consecutive positions at a time,
 //      each lane hashing the 4 bytes at its position into the warp's table of
-//      last positions (shared memory, 4096 16-bit entries) and checking the
+//      last positions (shared memory, 2048 16-bit entries) and checking the
 //      candidate; the first matching lane starts a match, which the warp
 //      extends 32 bytes per step; positions before it enter the table.  With
 //      no match the window advances 32 positions;
@@ -17,8 +23,7 @@
 //      an all-equal block becomes an RLE block, a block that does not shrink
 //      a raw block.
 // Block sizes are scanned and a gather kernel places the blocks after the
-// frame header.  Matches stay inside their block (measured on 2D blobs: 32 KB
-// blocks lose 0.5 % of the size against 128 KB blocks with the same matcher).
+// frame header.  Matches stay inside their block.
 #include <cstring>
 
 #include "kernels.h"
@@ -28,9 +33,9 @@ namespace cpsz {
 
 namespace {
 
-constexpr int ZBLK = 32 * 1024;
-constexpr int ZHT_BITS = 12;
-constexpr int ZWARPS = 4;  // blocks per CTA
+constexpr int ZBLK = 8 * 1024;
+constexpr int ZHT_BITS = 11;
+constexpr int ZWARPS = 8;  // blocks per CTA
 constexpr int ZMAXSEQ = ZBLK / zstd::kMinMatch + 1;
 constexpr int ZOUT = ZBLK + 16;  // per-block output slot: a raw block and its header fit
 constexpr unsigned FULLMASK = 0xffffffffu;
@@ -42,23 +47,45 @@ __device__ __forceinline__ uint32_t load4(const uint8_t* p) {
 }
 __device__ __forceinline__ uint32_t zhash(uint32_t v) { return (v * 2654435761u) >> (32 - ZHT_BITS); }
 
-// One warp per block: matches, then the encoded block (header included) into
-// its slot of `slots`; sizes[b] = the encoded block's bytes.
+// Shared memory of one warp: its block's bytes and its hash table of
+// block-local positions + 1 (0 = empty).
+struct ZWarpSmem {
+  uint8_t data[ZBLK];
+  uint16_t ht[1 << ZHT_BITS];
+};
+constexpr size_t ZSMEM = sizeof(ZWarpSmem) * ZWARPS;
+
+// One warp per block: the block staged in shared memory (16-byte loads), so
+// the match loop's byte reads are shared-memory reads; matches, then the
+// encoded block (header included) into its slot of `slots`; sizes[b] = the
+// encoded block's bytes.
 __global__ void __launch_bounds__(32 * ZWARPS) zstd_block_kernel(const uint8_t* __restrict__ src, size_t n,
                                                                  long long nblocks, zstd::Seq* __restrict__ seq_all,
                                                                  uint8_t* __restrict__ slots,
                                                                  unsigned int* __restrict__ sizes) {
-  // block-local position + 1 (at most 32768), 0 = empty
-  __shared__ uint16_t ht_all[ZWARPS][1 << ZHT_BITS];
+  extern __shared__ __align__(16) uint8_t zsm[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long b = (long long)blockIdx.x * ZWARPS + warp;
   if (b >= nblocks) return;  // warp-uniform; only __syncwarp below
+  ZWarpSmem& W = reinterpret_cast<ZWarpSmem*>(zsm)[warp];
   const size_t s0 = (size_t)b * ZBLK;
   const int len = (int)((n - s0) < (size_t)ZBLK ? (n - s0) : (size_t)ZBLK);
-  const uint8_t* blk = src + s0;
+  {
+    const uint8_t* g = src + s0;
+    int k0 = 0;
+    if (((uintptr_t)g & 15) == 0) {
+      const int nv = len >> 4;
+      for (int q = lane; q < nv; q += 32)
+        reinterpret_cast<uint4*>(W.data)[q] = __ldcs(reinterpret_cast<const uint4*>(g) + q);
+      k0 = nv << 4;
+    }
+    for (int i = k0 + lane; i < len; i += 32) W.data[i] = g[i];
+    __syncwarp();
+  }
+  const uint8_t* blk = W.data;
   uint8_t* out = slots + (size_t)b * ZOUT;
   const bool last = b == nblocks - 1;
-  uint16_t* ht = ht_all[warp];
+  uint16_t* ht = W.ht;
 
   // ---- RLE block: every byte equal ----
   {
@@ -177,6 +204,7 @@ __global__ void __launch_bounds__(256) zstd_gather_kernel(const uint8_t* __restr
 }
 
 bool g_tables_ready[64] = {};
+bool g_smem_set[64] = {};
 
 }  // namespace
 
@@ -226,7 +254,12 @@ int launch_zstd_frame(cpsz_b200_ctx* ctx, const uint8_t* d_in, size_t n, uint8_t
   }
   if (n > ((size_t)1 << 32) - 4 * (size_t)nb - 64)
     return set_error(CPSZ_ERR_UNSUPPORTED, "lossless stage input of %zu bytes exceeds 4 GB", n);
-  zstd_block_kernel<<<(unsigned)((nb + ZWARPS - 1) / ZWARPS), 32 * ZWARPS, 0, st>>>(d_in, n, nb, seqs, slots, sizes);
+  if (!g_smem_set[ctx->device & 63]) {
+    CPSZ_CUDA_TRY(cudaFuncSetAttribute(zstd_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZSMEM));
+    g_smem_set[ctx->device & 63] = true;
+  }
+  zstd_block_kernel<<<(unsigned)((nb + ZWARPS - 1) / ZWARPS), 32 * ZWARPS, ZSMEM, st>>>(d_in, n, nb, seqs, slots,
+                                                                                         sizes);
   count_launch(ctx);
   CPSZ_TRY(check_launch("zstd_block_kernel"));
   CPSZ_TRY(launch_scan_u32(ctx, sizes, off, (size_t)nb, scan_tmp));

@@ -212,13 +212,28 @@ ZHD void fse_encode(BitWriter& w, FseState& s, int sym) {
 }
 ZHD void fse_flush(BitWriter& w, const FseState& s) { bw_add(w, s.value, s.t->table_log); }
 
+// The encoder's constant tables: the three predefined FSE tables and the
+// sequence codes as lookups (device code reads them from constant memory; a
+// length beyond the lookup takes the format's highbit rule).
 struct Tables {
   FseCTable ll, ml, of;
+  uint8_t ll_code[64];   // literals length -> code (>= 64: highbit + 19)
+  uint8_t ml_code[128];  // match length - 3 -> code (>= 128: highbit + 36)
+  uint8_t ll_bits[36], ml_bits[53];
 };
 inline void build_tables(Tables* t) {
   fse_build(kLLNorm, 35, kLLLog, &t->ll);
   fse_build(kMLNorm, 52, kMLLog, &t->ml);
   fse_build(kOFNorm, 28, kOFLog, &t->of);
+  for (uint32_t v = 0; v < 64; v++) t->ll_code[v] = (uint8_t)ll_code(v);
+  for (uint32_t v = 0; v < 128; v++) t->ml_code[v] = (uint8_t)ml_code(v + 3);
+  for (int c = 0; c < 36; c++) t->ll_bits[c] = (uint8_t)ll_bits(c);
+  for (int c = 0; c < 53; c++) t->ml_bits[c] = (uint8_t)ml_bits(c);
+}
+ZHD int ll_code_t(const Tables& T, uint32_t ll) { return ll < 64 ? T.ll_code[ll] : highbit32(ll) + 19; }
+ZHD int ml_code_t(const Tables& T, uint32_t ml) {
+  const uint32_t b = ml - 3;
+  return b < 128 ? T.ml_code[b] : highbit32(b) + 36;
 }
 
 // One sequence: `lit` literals, then a match of `ml` (>= 3) bytes at distance `off`.
@@ -246,9 +261,9 @@ ZHD size_t write_sequences(const Tables& T, const Seq* seq, int nseq, uint8_t* o
   out[p++] = 0;  // predefined modes for literal lengths, offsets, match lengths
   BitWriter w;
   bw_init(w, out + p, cap - p);
-  auto codes = [](const Seq& q, int& llc, int& mlc, int& ofc, uint32_t& ofv) {
-    llc = ll_code(q.lit);
-    mlc = ml_code(q.ml);
+  auto codes = [&T](const Seq& q, int& llc, int& mlc, int& ofc, uint32_t& ofv) {
+    llc = ll_code_t(T, q.lit);
+    mlc = ml_code_t(T, q.ml);
     ofv = q.off + 3;  // a real offset, never a repeat code
     ofc = highbit32(ofv);
   };
@@ -259,16 +274,16 @@ ZHD size_t write_sequences(const Tables& T, const Seq* seq, int nseq, uint8_t* o
   fse_init(sml, &T.ml, mlc);
   fse_init(sof, &T.of, ofc);
   fse_init(sll, &T.ll, llc);
-  bw_add(w, seq[nseq - 1].lit, ll_bits(llc));
-  bw_add(w, seq[nseq - 1].ml - 3, ml_bits(mlc));
+  bw_add(w, seq[nseq - 1].lit, T.ll_bits[llc]);
+  bw_add(w, seq[nseq - 1].ml - 3, T.ml_bits[mlc]);
   bw_add(w, ofv, ofc);
   for (int n = nseq - 2; n >= 0; n--) {
     codes(seq[n], llc, mlc, ofc, ofv);
     fse_encode(w, sof, ofc);
     fse_encode(w, sml, mlc);
     fse_encode(w, sll, llc);
-    bw_add(w, seq[n].lit, ll_bits(llc));
-    bw_add(w, seq[n].ml - 3, ml_bits(mlc));
+    bw_add(w, seq[n].lit, T.ll_bits[llc]);
+    bw_add(w, seq[n].ml - 3, T.ml_bits[mlc]);
     bw_add(w, ofv, ofc);
   }
   fse_flush(w, sml);
