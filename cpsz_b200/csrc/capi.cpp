@@ -206,7 +206,8 @@ int cpsz_b200_debug_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, siz
   cudaMemcpy(dV, V, 4 * N, cudaMemcpyHostToDevice);
   cudaMemcpy(dtab, qt.t, QUANT_TAB_MAX * 8, cudaMemcpyHostToDevice);
   cudaMemset(dh, 0, 256 * 8);
-  int rc = launch_eb2d(ctx, dU, dV, (int)r1, (int)r2, max_pwr_eb, dtab, qt.n, dids, dids + N, dh, nullptr, nullptr, deb);
+  int rc = launch_eb2d(ctx, dU, dV, (int)r1, (int)r2, max_pwr_eb, dtab, qt.n, dids, dids + N, dh, nullptr, nullptr, deb,
+                       0, -1, nullptr, false, qt.float_pow4);
   cudaStreamSynchronize(ctx->stream);
   if (rc == CPSZ_OK) {
     if (eb_out) cudaMemcpy(eb_out, deb, 8 * N, cudaMemcpyDeviceToHost);

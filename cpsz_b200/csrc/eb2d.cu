@@ -41,7 +41,8 @@ __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const f
                                                   float2* __restrict__ pair_u, float2* __restrict__ pair_v,
                                                   double* __restrict__ eb_out, int row_begin, int row_end,
                                                   const int2* __restrict__ unit_order, int unit_ncb,
-                                                  unsigned long long* __restrict__ unit_done, int log_ids) {
+                                                  unsigned long long* __restrict__ unit_done, int log_ids,
+                                                  int pow4_ids) {
   constexpr int CX = TX + 1;  // cells per tile row
   constexpr int CY = TY + 1;
   static_assert(WAVE_GROUP_ROWS % TY == 0, "a tile's rows must lie in one wavefront group");
@@ -112,6 +113,7 @@ __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const f
   }
   __syncthreads();
   const double thr = tab[0];
+  const float eb_dn = __double2float_rd(max_pwr_eb), eb_up = __double2float_ru(max_pwr_eb);
   // id of a quantized bound e (-1 for precision 0), before the range check
   auto quant = [&](double e) -> int {
     if (e <= thr) return -1;
@@ -172,22 +174,46 @@ __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const f
         take(0, a + 1, b + 1);
         take(1, a + 1, b + 1);
       }
-      const double m = (double)mf;
-      const double lo = fmin(max_pwr_eb, fmin(m * (1.0 - dev::FFILT_REL) - dev::FFILT_ABS, md));
-      const double hi = fmin(max_pwr_eb, fmin(m * (1.0 + dev::FFILT_REL) + dev::FFILT_ABS, md));
-      code[0] = quant(s0 * lo);
-      code[1] = log_ids ? -1 : quant(s1 * lo);
-      // the upper end has the same id iff it stays below the next threshold
-      auto stays = [&](int c, double e) { return c < 0 ? e <= thr : (c + 1 >= thr_n || e < tab[c + 1]); };
-      if (nan || !stays(code[0], s0 * hi) || (!log_ids && !stays(code[1], s1 * hi))) {
-        // the enclosure straddles a threshold (or a bound is NaN): exact bounds
-        eb = vertex_eb([&](int kind, int ca, int cb) {
-          const int a1 = ca + (kind == 0), b1 = cb + (kind == 1);
-          return dev::tri_eb_exact(su[ca][cb], su[a1][b1], su[ca + 1][cb + 1], sv[ca][cb], sv[a1][b1],
-                                   sv[ca + 1][cb + 1], kind);
-        });
-        code[0] = quant(s0 * eb);
-        code[1] = log_ids ? -1 : quant(s1 * eb);
+      // The float route: the same enclosure rounded outwards in float, each
+      // component's |x| * bound with directed products, and the id of a float
+      // read off its exponent (exact for this table: quant_table_2d's
+      // float_pow4).  Ends with different ids, an id past the table's range
+      // or an overflow take the double route below.
+      bool decided = false;
+      if (pow4_ids && !nan) {
+        float lo_f = fminf(__fmaf_rd(mf, 1.0f - dev::FFILT_REL, -dev::FFILT_ABS), eb_dn);
+        float hi_f = fminf(__fmaf_ru(mf, 1.0f + dev::FFILT_REL, dev::FFILT_ABS), eb_up);
+        if (md < INFINITY) {
+          lo_f = fminf(lo_f, __double2float_rd(md));
+          hi_f = fminf(hi_f, __double2float_ru(md));
+        }
+        const float su = fabsf(uu), sv = fabsf(vv);
+        const int c0 = dev::pow4_id(__fmul_rd(su, lo_f)), c0h = dev::pow4_id(__fmul_ru(su, hi_f));
+        const int c1 = dev::pow4_id(__fmul_rd(sv, lo_f)), c1h = dev::pow4_id(__fmul_ru(sv, hi_f));
+        if (c0 == c0h && c1 == c1h && c0h <= ID_MAX_2D && c1h <= ID_MAX_2D) {
+          code[0] = c0;
+          code[1] = c1;
+          decided = true;
+        }
+      }
+      if (!decided) {
+        const double m = (double)mf;
+        const double lo = fmin(max_pwr_eb, fmin(m * (1.0 - dev::FFILT_REL) - dev::FFILT_ABS, md));
+        const double hi = fmin(max_pwr_eb, fmin(m * (1.0 + dev::FFILT_REL) + dev::FFILT_ABS, md));
+        // the upper end has the same id iff it stays below the next threshold
+        auto stays = [&](int c, double e) { return c < 0 ? e <= thr : (c + 1 >= thr_n || e < tab[c + 1]); };
+        code[0] = quant(s0 * lo);
+        code[1] = log_ids ? -1 : quant(s1 * lo);
+        if (nan || !stays(code[0], s0 * hi) || (!log_ids && !stays(code[1], s1 * hi))) {
+          // the enclosure straddles a threshold (or a bound is NaN): exact bounds
+          eb = vertex_eb([&](int kind, int ca, int cb) {
+            const int a1 = ca + (kind == 0), b1 = cb + (kind == 1);
+            return dev::tri_eb_exact(su[ca][cb], su[a1][b1], su[ca + 1][cb + 1], sv[ca][cb], sv[a1][b1],
+                                     sv[ca + 1][cb + 1], kind);
+          });
+          code[0] = quant(s0 * eb);
+          code[1] = log_ids ? -1 : quant(s1 * eb);
+        }
       }
     } else {
       eb = vertex_eb([&](int kind, int ca, int cb) { return tri[kind][ca][cb]; });
@@ -266,7 +292,7 @@ int preload_eb2d() {
 int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, double max_pwr_eb,
                 const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
                 float2* pair_u, float2* pair_v, double* eb_out, int row_begin, int row_end,
-                const Eb2dUnits* units, bool log_ids) {
+                const Eb2dUnits* units, bool log_ids, bool pow4_ids) {
   if (row_end < 0) row_end = r1;
   if (log_ids && (pair_u || pair_v || ids_v))
     return set_error(CPSZ_ERR_INVALID, "eb2d: the log-domain ids have no wavefront pairs and one stream");
@@ -278,13 +304,14 @@ int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int 
       const long long tiles = (long long)units->n * (UNIT_COLS / tx) * (WAVE_GROUP_ROWS / ty);
       kernel<<<(unsigned)tiles, nt, 0, ctx->stream>>>(U, V, r1, r2, max_pwr_eb, d_thr_tab, thr_n, ids_u, ids_v, hist,
                                                       ctx->d_flag, pair_u, pair_v, eb_out, row_begin, row_end,
-                                                      units->order, units->ncb, units->done, log_ids ? 1 : 0);
+                                                      units->order, units->ncb, units->done, log_ids ? 1 : 0,
+                                                      pow4_ids && !log_ids ? 1 : 0);
       return;
     }
     dim3 grid((r2 + tx - 1) / tx, (row_end - row_begin + ty - 1) / ty);
     kernel<<<grid, nt, 0, ctx->stream>>>(U, V, r1, r2, max_pwr_eb, d_thr_tab, thr_n, ids_u, ids_v, hist, ctx->d_flag,
                                          pair_u, pair_v, eb_out, row_begin, row_end, nullptr, 0, nullptr,
-                                         log_ids ? 1 : 0);
+                                         log_ids ? 1 : 0, pow4_ids && !log_ids ? 1 : 0);
   };
   // filtered bounds unless the caller wants the bounds themselves (or an
   // unusual max_pwr_eb takes the reference's NaN paths)

@@ -548,6 +548,16 @@ static __device__ __forceinline__ double tet_eb(float u0, float u1, float u2, fl
 
 // Quantized-id lookup against host-computed thresholds t[1..n): the id is the
 // number of thresholds <= e.  `guess` starts near the answer; the loops fix it.
+// The 2D id of a float x under thresholds t[k] in (the float below 2^(2k-52),
+// 2^(2k-52)]: -1 up to thr = 2^-52, else #{k >= 1 : x >= 2^(2k-52)} =
+// (exponent(x) + 52) / 2 rounded down.  Floats from FLT_MAX's binade up (inf
+// and nan: 90) give ids past the 2D range of 0..88.
+__device__ __forceinline__ int pow4_id(float x) {
+  if (x <= 2.220446049250313e-16f) return -1;
+  const int e = (int)((__float_as_uint(x) >> 23) & 0xff) - 127;
+  return (e + 52) >> 1;
+}
+
 __device__ __forceinline__ int count_thresholds(const double* t, int n, double e, int guess) {
   int g = guess < 0 ? 0 : (guess > n - 1 ? n - 1 : guess);
   while (g + 1 < n && e >= t[g + 1]) g++;

@@ -50,10 +50,12 @@ void unit_order(int g0, int g1, int ncb, int skew, std::vector<int2>& out);
 // units of the rows' groups), the tiles run in unit order and count.
 // log_ids: the offline_log form -- one id per vertex, of the vertex bound
 // itself against quant_table_2d_log() (ids_v, pair_u and pair_v null).
+// pow4_ids: the table is quant_table_2d() with float_pow4 (the filtered path
+// then decides most ids in float).
 int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int r2, double max_pwr_eb,
                 const double* d_thr_tab, int thr_n, uint8_t* ids_u, uint8_t* ids_v, unsigned long long* hist,
                 float2* pair_u, float2* pair_v, double* eb_out = nullptr, int row_begin = 0, int row_end = -1,
-                const Eb2dUnits* units = nullptr, bool log_ids = false);
+                const Eb2dUnits* units = nullptr, bool log_ids = false, bool pow4_ids = false);
 
 // Loads every eb2d instantiation (required before a consumer that waits on
 // eb2d is launched: a lazily loaded first launch could wait for it).

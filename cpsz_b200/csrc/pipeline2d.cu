@@ -606,7 +606,8 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
         else {
           const Eb2dUnits u = band_units(0, j.ngroups);
           CPSZ_TRY(launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
-                               j.d.hist_ids, j.d.pairs[0], j.d.pairs[1], nullptr, 0, -1, overlap ? &u : nullptr));
+                               j.d.hist_ids, j.d.pairs[0], j.d.pairs[1], nullptr, 0, -1, overlap ? &u : nullptr,
+                               false, qt.float_pow4));
         }
       } else {
         // Host input: row chunks go up on the second stream and the bound kernel
@@ -631,7 +632,7 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
                                                                      WAVE_GROUP_ROWS);
           return launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N, j.d.hist_ids,
                              j.d.pairs[0], j.d.pairs[1], nullptr, c * R, std::min(j.r1, (c + 1) * R),
-                             overlap ? &u : nullptr);
+                             overlap ? &u : nullptr, false, qt.float_pow4);
         };
         for (int c = 0; c < nch; c++) {
           const size_t off = (size_t)c * R * j.r2;

@@ -120,6 +120,12 @@ const QuantTable& quant_table_2d() {
     // e ranges over |U| * eb; the upper end keeps e / thr finite (ids beyond
     // the table's 255 are rejected by the kernel anyway).
     build_table(T, id_2d, DBL_EPSILON, 1e280);
+    bool ok = T.n > 1;
+    for (int k = 0; k < T.n && ok; k++) {
+      const double p = ldexp(1.0, 2 * k - 52);
+      ok = T.t[k] <= p && T.t[k] > (double)nextafterf((float)p, 0.f);
+    }
+    T.float_pow4 = ok;
   });
   return T;
 }

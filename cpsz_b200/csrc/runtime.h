@@ -51,6 +51,10 @@ struct QuantTable {
   int base = 0;         // 4 (2D) or 2 (3D)
   int n = 0;            // thresholds t[1..n) valid; t[0] = thr (id >= 0 region starts above thr)
   double t[kMax] = {};  // t[k] = smallest e with id(e) >= k
+  // 2D table only: every t[k] (k >= 0) lies in (the float below 2^(2k-52),
+  // 2^(2k-52)], so a float x has id >= k exactly when x >= 2^(2k-52): the
+  // float id of x > thr is (exponent(x) + 52) >> 1 (eb2d's float vertex path)
+  bool float_pow4 = false;
 };
 // 2D: base 4, thr = DBL_EPSILON, applied to e = |U| * eb.
 const QuantTable& quant_table_2d();
