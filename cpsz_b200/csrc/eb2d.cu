@@ -49,9 +49,10 @@ __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const f
   static_assert(UNIT_COLS % TX == 0, "a tile's columns must lie in one unit");
   __shared__ float su[TY + 2][TX + 3];
   __shared__ float sv[TY + 2][TX + 3];
-  // compression (FAST): the float bound of an ordinary triangle, or -1 when
-  // the triangle took the exact path and its bound is in tri; exact mode: tri
-  __shared__ float trf[FAST ? 2 : 1][FAST ? CY : 1][FAST ? CX : 1];
+  // compression (FAST): the float bound of an ordinary triangle, or +inf when
+  // the triangle took the exact path (its bound is in tri) or does not exist;
+  // exact mode: tri alone
+  __shared__ float trf[2][CY][CX];
   __shared__ double tri[2][CY][CX];
   __shared__ double tab[QUANT_TAB_MAX];
   __shared__ unsigned int shist[256];
@@ -86,32 +87,59 @@ __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const f
     sv[a][b] = v;
   }
   __syncthreads();
-  // triangles of cells (ci, cj) = (i0-1+a, j0-1+b), a in [0, CY), b in [0, CX);
-  // one triangle per thread and round (2 * 561 triangles over 256 threads at 32x16)
-  for (int k = tid; k < 2 * CY * CX; k += NT) {
-    const int kind = k >= CY * CX;
-    const int c = k - kind * CY * CX;
-    const int a = c / CX, b = c % CX;
-    const int ci = i0 - 1 + a, cj = j0 - 1 + b;
-    double e = 0;
-    float t = 0.f;
-    if (ci >= 0 && ci < r1 - 1 && cj >= 0 && cj < r2 - 1) {
-      // upper: offsets {0, r2, r2+1} -> (a,b), (a+1,b), (a+1,b+1);
-      // lower: offsets {0, 1, r2+1} -> (a,b), (a,b+1), (a+1,b+1).
-      // One call site of the exact bound keeps a single copy of its code in
-      // the instruction cache.
-      const int a1 = a + (kind == 0), b1 = b + (kind == 1);
-      const float x0 = su[a][b], x1 = su[a1][b1], x2 = su[a + 1][b + 1];
-      const float y0 = sv[a][b], y1 = sv[a1][b1], y2 = sv[a + 1][b + 1];
-      if (!FAST || !dev::tri_eb_float(x0, x1, x2, y0, y1, y2, t)) {
-        e = dev::tri_eb_exact(x0, x1, x2, y0, y1, y2, kind);
-        t = -1.f;
+  // cells (ci, cj) = (i0-1+a, j0-1+b), a in [0, CY), b in [0, CX).
+  // Compression (FAST): both triangles of a cell per thread and round
+  // (1089 cells over 256 threads at 32x32), the float bound in trf, or +inf
+  // there and the exact bound in tri for a triangle that takes the exact
+  // path; a cell outside the field holds +inf in both (it has no triangles,
+  // and +inf leaves every vertex minimum unchanged).  Exact mode: one
+  // triangle per thread and round, every exact bound in tri.  The exact
+  // bound is a call (tri_eb_exact is not inlined), so its code is in the
+  // instruction cache once.
+  bool any_exact = false;
+  if (FAST) {
+    for (int c = tid; c < CY * CX; c += NT) {
+      const int a = c / CX, b = c - (c / CX) * CX;
+      const int ci = i0 - 1 + a, cj = j0 - 1 + b;
+      const bool in = ci >= 0 && ci < r1 - 1 && cj >= 0 && cj < r2 - 1;
+      float t[2] = {INFINITY, INFINITY};
+      bool ok[2] = {false, false};
+      if (in)
+        dev::cell_eb_float(su[a][b], su[a + 1][b], su[a][b + 1], su[a + 1][b + 1], sv[a][b], sv[a + 1][b],
+                           sv[a][b + 1], sv[a + 1][b + 1], t[0], t[1], ok[0], ok[1]);
+#pragma unroll
+      for (int kind = 0; kind < 2; kind++) {
+        if (!ok[kind]) {
+          double e = INFINITY;
+          if (in) {
+            // upper: (a,b), (a+1,b), (a+1,b+1); lower: (a,b), (a,b+1), (a+1,b+1)
+            const int a1 = a + (kind == 0), b1 = b + (kind == 1);
+            e = dev::tri_eb_exact(su[a][b], su[a1][b1], su[a + 1][b + 1], sv[a][b], sv[a1][b1], sv[a + 1][b + 1],
+                                  kind);
+            t[kind] = INFINITY;
+            any_exact = true;
+          }
+          tri[kind][a][b] = e;
+        }
+        trf[kind][a][b] = t[kind];
       }
     }
-    if (FAST) trf[FAST ? kind : 0][FAST ? a : 0][FAST ? b : 0] = t;
-    tri[kind][a][b] = e;
+  } else {
+    for (int k = tid; k < 2 * CY * CX; k += NT) {
+      const int kind = k >= CY * CX;
+      const int c = k - kind * CY * CX;
+      const int a = c / CX, b = c % CX;
+      const int ci = i0 - 1 + a, cj = j0 - 1 + b;
+      double e = 0;
+      if (ci >= 0 && ci < r1 - 1 && cj >= 0 && cj < r2 - 1) {
+        const int a1 = a + (kind == 0), b1 = b + (kind == 1);
+        e = dev::tri_eb_exact(su[a][b], su[a1][b1], su[a + 1][b + 1], sv[a][b], sv[a1][b1], sv[a + 1][b + 1], kind);
+      }
+      tri[kind][a][b] = e;
+    }
   }
-  __syncthreads();
+  // whether any triangle of the tile took the exact path (uniform over the CTA)
+  const bool tile_exact = __syncthreads_or(any_exact);
   const double thr = tab[0];
   const float eb_dn = __double2float_rd(max_pwr_eb), eb_up = __double2float_ru(max_pwr_eb);
   // id of a quantized bound e (-1 for precision 0), before the range check
@@ -150,27 +178,25 @@ __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const f
     if (FAST) {
       // enclosure of the vertex bound: the float bounds of its ordinary
       // triangles (min mf, each within FFILT_REL and FFILT_ABS of the
-      // reference's value) and the exact ones (min md)
-      float mf = INFINITY;
+      // reference's value) and the exact ones (min md).  The six incident
+      // triangles are read unconditionally: a missing one (a cell outside the
+      // field) holds +inf.
+      const float mf = fminf(fminf(fminf(trf[0][a][b], trf[1][a][b]), fminf(trf[0][a][b + 1], trf[1][a + 1][b])),
+                             fminf(trf[0][a + 1][b + 1], trf[1][a + 1][b + 1]));
       double md = INFINITY;
       bool nan = false;
-      auto take = [&](int kind, int ca, int cb) {
-        const float t = trf[FAST ? kind : 0][FAST ? ca : 0][FAST ? cb : 0];
-        if (t >= 0.f) {
-          mf = fminf(mf, t);
-        } else {
-          const double e = tri[kind][ca][cb];
-          nan |= isnan(e);
-          md = fmin(md, e);
-        }
-      };
-      if (up && left) {
+      if (tile_exact) {
+        auto take = [&](int kind, int ca, int cb) {
+          if (trf[kind][ca][cb] == INFINITY) {
+            const double e = tri[kind][ca][cb];
+            nan |= isnan(e);
+            md = fmin(md, e);
+          }
+        };
         take(0, a, b);
         take(1, a, b);
-      }
-      if (up && right) take(0, a, b + 1);
-      if (down && left) take(1, a + 1, b);
-      if (down && right) {
+        take(0, a, b + 1);
+        take(1, a + 1, b);
         take(0, a + 1, b + 1);
         take(1, a + 1, b + 1);
       }

@@ -246,12 +246,6 @@ constexpr float FFILT_ABS = 9.09494702e-13f;           // 2^-40
 struct Frac {
   float n, d;  // the value n / d, d > 0
 };
-// a + b = s + e exactly (Knuth's two-sum; no assumption on magnitudes)
-__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
-  s = a + b;
-  const float bb = s - a;
-  e = (a - (s - bb)) + (b - bb);
-}
 // keep_sign2 as a fraction: numerator |D| (D = P - N, accurate), P and N for the denominator
 __device__ __forceinline__ Frac ks2_frac(float D, float P, float N, bool& bad) {
   if (P == 0.f || N == 0.f) return Frac{1.f, 1.f};
@@ -259,54 +253,208 @@ __device__ __forceinline__ Frac ks2_frac(float D, float P, float N, bool& bad) {
   bad |= !(pn >= 1.2924697e-33f);  // 2^-110
   return Frac{fabsf(D), (P + N) + 2.f * sqrt_approx(pn)};
 }
-__device__ __forceinline__ Frac frac_min(Frac a, Frac b) { return (a.n * b.d <= b.n * a.d) ? a : b; }
-__device__ __forceinline__ Frac frac_max(Frac a, Frac b) { return (a.n * b.d >= b.n * a.d) ? a : b; }
 __device__ __forceinline__ float pos_part(float t) { return t > 0.f ? t : 0.f; }
 __device__ __forceinline__ float neg_part(float t) { return t < 0.f ? -t : 0.f; }
 // two-term bound (max_eb_to_keep_sign_2d_offline_2) of (a, b) with a + b = D
 __device__ __forceinline__ Frac off2_frac(float D, float a, float b, bool& bad) {
   return ks2_frac(D, pos_part(a) + pos_part(b), neg_part(a) + neg_part(b), bad);
 }
-// four-term bound (_4) of (a, b, c, d) with a + b + c + d = D
-__device__ __forceinline__ Frac off4_frac(float D, float a, float b, float c, float d, bool& bad) {
-  const float P = ((pos_part(a) + pos_part(b)) + pos_part(c)) + pos_part(d);
-  const float N = ((neg_part(a) + neg_part(b)) + neg_part(c)) + neg_part(d);
-  return ks2_frac(D, P, N, bad);
+
+// ---- both triangles of a cell at once --------------------------------------------
+// Cell (a, b) of the grid holds the "upper" triangle {(a,b), (a+1,b), (a+1,b+1)}
+// and the "lower" one {(a,b), (a,b+1), (a+1,b+1)}: vertices 0 and 2 are
+// shared, so p02, p20, x1 and the two-term bound of x1 are the same for both.
+// cell_eb_float runs the filter above for the two triangles together, the
+// upper one in the low word and the lower one in the high word of packed
+// f32x2 operands: add / sub / mul.rn.f32x2 round each word exactly as the
+// scalar instruction does, so every quantity is the one-triangle filter's
+// (the two-sum error of a difference a - c is formed as (a - (s - bb)) -
+// (c + bb), the scalar two_sum(a, -c)'s value up to the sign of a zero, which
+// no later decision sees: a sum that is exactly zero fails its |.| > T test
+// either way).  One instruction issue covers both words; comparisons and
+// selects act on each word.
+typedef unsigned long long f32x2;  // low word .x (upper triangle), high word .y (lower)
+__device__ __forceinline__ f32x2 pk2(float x, float y) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(x), "f"(y));
+  return r;
+}
+__device__ __forceinline__ void unpk2(f32x2 r, float& x, float& y) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(x), "=f"(y) : "l"(r));
+}
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+  f32x2 c;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(c) : "l"(a), "l"(b));
+  return c;
+}
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+  f32x2 c;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(c) : "l"(a), "l"(b));
+  return c;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+  f32x2 c;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(c) : "l"(a), "l"(b));
+  return c;
+}
+// a + b = s + e exactly, word by word
+__device__ __forceinline__ void two_sum2(f32x2 a, f32x2 b, f32x2& s, f32x2& e) {
+  s = add2(a, b);
+  const f32x2 bb = sub2(s, a);
+  e = add2(sub2(a, sub2(s, bb)), sub2(b, bb));
+}
+// a - c = s + e exactly, word by word
+__device__ __forceinline__ void two_diff2(f32x2 a, f32x2 c, f32x2& s, f32x2& e) {
+  s = sub2(a, c);
+  const f32x2 bb = sub2(s, a);
+  e = sub2(sub2(a, sub2(s, bb)), add2(c, bb));
+}
+struct Frac2 {
+  f32x2 n, d;  // word by word the value n / d (d > 0); n may carry D's sign: the value is |n| / d
+};
+// ks2_frac of both words: D, P, N per word
+__device__ __forceinline__ Frac2 ks2_frac2(f32x2 D, f32x2 P, f32x2 N, bool& bad_x, bool& bad_y) {
+  const f32x2 pn = mul2(P, N);
+  float P0, P1, N0, N1, q0, q1, D0, D1;
+  unpk2(P, P0, P1);
+  unpk2(N, N0, N1);
+  unpk2(pn, q0, q1);
+  unpk2(D, D0, D1);
+  const bool one0 = P0 == 0.f || N0 == 0.f, one1 = P1 == 0.f || N1 == 0.f;
+  bad_x |= !one0 && !(q0 >= 1.2924697e-33f);  // 2^-110
+  bad_y |= !one1 && !(q1 >= 1.2924697e-33f);
+  const f32x2 sq = pk2(sqrt_approx(q0), sqrt_approx(q1));
+  const f32x2 d = add2(add2(P, N), add2(sq, sq));  // (P + N) + 2 sqrt(P N)
+  float d0, d1;
+  unpk2(d, d0, d1);
+  return Frac2{pk2(one0 ? 1.f : D0, one1 ? 1.f : D1), pk2(one0 ? 1.f : d0, one1 ? 1.f : d1)};
+}
+__device__ __forceinline__ f32x2 pos2(f32x2 t) {
+  float a, b;
+  unpk2(t, a, b);
+  return pk2(pos_part(a), pos_part(b));
+}
+__device__ __forceinline__ f32x2 neg2(f32x2 t) {
+  float a, b;
+  unpk2(t, a, b);
+  return pk2(neg_part(a), neg_part(b));
+}
+// two-term bound of (a, -c), a - c = D
+__device__ __forceinline__ Frac2 off2_frac2(f32x2 D, f32x2 a, f32x2 c, bool& bad_x, bool& bad_y) {
+  return ks2_frac2(D, add2(pos2(a), neg2(c)), add2(neg2(a), pos2(c)), bad_x, bad_y);
+}
+// four-term bound of (a, -b, c, -d), a - b + c - d = D
+__device__ __forceinline__ Frac2 off4_frac2(f32x2 D, f32x2 a, f32x2 b, f32x2 c, f32x2 d, bool& bad_x,
+                                            bool& bad_y) {
+  const f32x2 P = add2(add2(add2(pos2(a), neg2(b)), pos2(c)), neg2(d));
+  const f32x2 N = add2(add2(add2(neg2(a), pos2(b)), neg2(c)), pos2(d));
+  return ks2_frac2(D, P, N, bad_x, bad_y);
+}
+// word by word: take b where pick (else a)
+__device__ __forceinline__ Frac2 frac_pick2(Frac2 a, Frac2 b, bool pick0, bool pick1) {
+  float an0, an1, ad0, ad1, bn0, bn1, bd0, bd1;
+  unpk2(a.n, an0, an1);
+  unpk2(a.d, ad0, ad1);
+  unpk2(b.n, bn0, bn1);
+  unpk2(b.d, bd0, bd1);
+  return Frac2{pk2(pick0 ? bn0 : an0, pick1 ? bn1 : an1), pk2(pick0 ? bd0 : ad0, pick1 ? bd1 : ad1)};
+}
+// |a.n| * b.d against |b.n| * a.d, word by word (d > 0, so |n| * d = |n * d|)
+__device__ __forceinline__ void frac_cmp2(Frac2 a, Frac2 b, float& l0, float& l1, float& r0, float& r1) {
+  unpk2(mul2(a.n, b.d), l0, l1);
+  unpk2(mul2(b.n, a.d), r0, r1);
+  l0 = fabsf(l0);
+  l1 = fabsf(l1);
+  r0 = fabsf(r0);
+  r1 = fabsf(r1);
+}
+__device__ __forceinline__ Frac2 frac_min2(Frac2 a, Frac2 b) {
+  float l0, l1, r0, r1;
+  frac_cmp2(a, b, l0, l1, r0, r1);
+  return frac_pick2(a, b, !(l0 <= r0), !(l1 <= r1));
+}
+// e = frac_max(e, a) in the words where take is set
+__device__ __forceinline__ Frac2 frac_max2_if(Frac2 e, Frac2 a, bool take0, bool take1) {
+  float l0, l1, r0, r1;
+  frac_cmp2(e, a, l0, l1, r0, r1);
+  return frac_pick2(e, a, take0 && !(l0 >= r0), take1 && !(l1 >= r1));
 }
 
-// The float bound of an ordinary triangle (true), or false: take the exact path.
-__device__ __forceinline__ bool tri_eb_float(float u0, float u1, float u2, float v0, float v1, float v2, float& t) {
-  const float p01 = u0 * v1, p10 = u1 * v0, p02 = u0 * v2, p20 = u2 * v0, p12 = u1 * v2, p21 = u2 * v1;
-  const float S = ((((fabsf(p01) + fabsf(p10)) + fabsf(p12)) + fabsf(p21)) + fabsf(p20)) + fabsf(p02);
-  float x1, e1, x2, e2, x3, e3;
-  two_sum(p20, -p02, x1, e1);
-  two_sum(p12, -p21, x2, e2);
-  two_sum(p01, -p10, x3, e3);
-  float h1, g1, h2, g2, h3, g3, hd, gd;
-  two_sum(x2, x3, h1, g1);
-  two_sum(x1, x3, h2, g2);
-  two_sum(x1, x2, h3, g3);
-  two_sum(h1, x1, hd, gd);
-  const float s1 = h1 + (g1 + (e2 + e3));
-  const float s2 = h2 + (g2 + (e1 + e3));
-  const float s3 = h3 + (g3 + (e1 + e2));
-  const float det = hd + (gd + (g1 + ((e1 + e2) + e3)));
-  const float T = S * 5.68434189e-14f;  // 2^-44
-  bool bad = !(S >= 8.67361738e-19f && S <= 1.09951163e12f);  // [2^-60, 2^40], false for NaN
-  bad |= !(fabsf(s1) > T && fabsf(s2) > T && fabsf(s3) > T && fabsf(det) > T);
-  bad |= x1 == 0.f || x2 == 0.f || x3 == 0.f;
-  const bool f1 = (s1 > 0.f) == (x1 > 0.f), f2 = (s2 > 0.f) == (x2 > 0.f), f3 = (s3 > 0.f) == (x3 > 0.f);
-  bad |= f1 && f2 && f3;  // a critical point: exact path
-  // max over failing flags of min(off2, off4), all three evaluated (no divergence)
-  Frac e = Frac{0.f, 1.f};
-  const Frac a1 = frac_min(off2_frac(x1, p20, -p02, bad), off4_frac(s1, p01, -p10, p12, -p21, bad));
-  const Frac a2 = frac_min(off2_frac(x2, p12, -p21, bad), off4_frac(s2, p01, -p10, p20, -p02, bad));
-  const Frac a3 = frac_min(off2_frac(x3, p01, -p10, bad), off4_frac(s3, p12, -p21, p20, -p02, bad));
-  if (!f1) e = frac_max(e, a1);
-  if (!f2) e = frac_max(e, a2);
-  if (!f3) e = frac_max(e, a3);
-  t = div_approx(e.n, e.d);
-  return !bad;
+// The float bounds of the cell's upper (t_up) and lower (t_lo) triangles, with
+// ok_* false for a triangle that takes the exact path.  Vertices: U00 = (a,b),
+// U10 = (a+1,b), U01 = (a,b+1), U11 = (a+1,b+1); the upper triangle is
+// (U00, U10, U11), the lower (U00, U01, U11) -- tri_eb's (u0, u1, u2).
+__device__ __forceinline__ void cell_eb_float(float U00, float U10, float U01, float U11, float V00, float V10,
+                                              float V01, float V11, float& t_up, float& t_lo, bool& ok_up,
+                                              bool& ok_lo) {
+  const f32x2 u0 = pk2(U00, U00), u1 = pk2(U10, U01), u2 = pk2(U11, U11);
+  const f32x2 v0 = pk2(V00, V00), v1 = pk2(V10, V01), v2 = pk2(V11, V11);
+  const f32x2 p01 = mul2(u0, v1), p10 = mul2(u1, v0), p02 = mul2(u0, v2), p20 = mul2(u2, v0), p12 = mul2(u1, v2),
+              p21 = mul2(u2, v1);
+  f32x2 x1, e1, x2, e2, x3, e3;
+  two_diff2(p20, p02, x1, e1);
+  two_diff2(p12, p21, x2, e2);
+  two_diff2(p01, p10, x3, e3);
+  f32x2 h1, g1, h2, g2, h3, g3, hd, gd;
+  two_sum2(x2, x3, h1, g1);
+  two_sum2(x1, x3, h2, g2);
+  two_sum2(x1, x2, h3, g3);
+  two_sum2(h1, x1, hd, gd);
+  const f32x2 e12 = add2(e1, e2);
+  const f32x2 s1 = add2(h1, add2(g1, add2(e2, e3)));
+  const f32x2 s2 = add2(h2, add2(g2, add2(e1, e3)));
+  const f32x2 s3 = add2(h3, add2(g3, e12));
+  const f32x2 det = add2(hd, add2(gd, add2(g1, add2(e12, e3))));
+  float P01[2], P10[2], P02[2], P20[2], P12[2], P21[2], X1[2], X2[2], X3[2], S1[2], S2[2], S3[2], DT[2];
+  unpk2(p01, P01[0], P01[1]);
+  unpk2(p10, P10[0], P10[1]);
+  unpk2(p02, P02[0], P02[1]);
+  unpk2(p20, P20[0], P20[1]);
+  unpk2(p12, P12[0], P12[1]);
+  unpk2(p21, P21[0], P21[1]);
+  unpk2(x1, X1[0], X1[1]);
+  unpk2(x2, X2[0], X2[1]);
+  unpk2(x3, X3[0], X3[1]);
+  unpk2(s1, S1[0], S1[1]);
+  unpk2(s2, S2[0], S2[1]);
+  unpk2(s3, S3[0], S3[1]);
+  unpk2(det, DT[0], DT[1]);
+  bool bad[2], f1[2], f2[2], f3[2];
+#pragma unroll
+  for (int w = 0; w < 2; w++) {
+    // the shared values are bitwise the same in both words: word 0's serve both
+    const float S = ((((fabsf(P01[w]) + fabsf(P10[w])) + fabsf(P12[w])) + fabsf(P21[w])) + fabsf(P20[0])) +
+                    fabsf(P02[0]);
+    const float T = S * 5.68434189e-14f;  // 2^-44
+    bool b = !(S >= 8.67361738e-19f && S <= 1.09951163e12f);  // [2^-60, 2^40], false for NaN
+    b |= !(fabsf(S1[w]) > T && fabsf(S2[w]) > T && fabsf(S3[w]) > T && fabsf(DT[w]) > T);
+    b |= X1[0] == 0.f || X2[w] == 0.f || X3[w] == 0.f;
+    f1[w] = (S1[w] > 0.f) == (X1[0] > 0.f);
+    f2[w] = (S2[w] > 0.f) == (X2[w] > 0.f);
+    f3[w] = (S3[w] > 0.f) == (X3[w] > 0.f);
+    bad[w] = b || (f1[w] && f2[w] && f3[w]);  // a critical point: exact path
+  }
+  // max over failing flags of min(off2, off4), all three evaluated (no
+  // divergence); off2 of x1 is the same for both triangles
+  bool bad1 = false;
+  const Frac t1 = off2_frac(X1[0], P20[0], -P02[0], bad1);
+  bad[0] |= bad1;
+  bad[1] |= bad1;
+  const Frac2 a1 = frac_min2(Frac2{pk2(t1.n, t1.n), pk2(t1.d, t1.d)},
+                             off4_frac2(s1, p01, p10, p12, p21, bad[0], bad[1]));
+  const Frac2 a2 = frac_min2(off2_frac2(x2, p12, p21, bad[0], bad[1]), off4_frac2(s2, p01, p10, p20, p02, bad[0], bad[1]));
+  const Frac2 a3 = frac_min2(off2_frac2(x3, p01, p10, bad[0], bad[1]), off4_frac2(s3, p12, p21, p20, p02, bad[0], bad[1]));
+  Frac2 e{pk2(0.f, 0.f), pk2(1.f, 1.f)};
+  e = frac_max2_if(e, a1, !f1[0], !f1[1]);
+  e = frac_max2_if(e, a2, !f2[0], !f2[1]);
+  e = frac_max2_if(e, a3, !f3[0], !f3[1]);
+  float n0, n1, d0, d1;
+  unpk2(e.n, n0, n1);
+  unpk2(e.d, d0, d1);
+  t_up = div_approx(fabsf(n0), d0);
+  t_lo = div_approx(fabsf(n1), d1);
+  ok_up = !bad[0];
+  ok_lo = !bad[1];
 }
 
 // ---- 3D (src/sz_compress_cp_preserve_3d.cpp:266-358) --------------------------

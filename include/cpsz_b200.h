@@ -363,7 +363,7 @@ int cpsz_b200_batch_layout(uint64_t base_seed, int n_fields, int lo, int hi, siz
  * src/sz_lossless.cpp:11-26) on the GPU: `in` (n bytes, host or device) becomes
  * a standard Zstandard frame at `out` (host or device, out_cap bytes; at most
  * cpsz_b200_lossless_bound(n)), which ZSTD_decompress -- and so the
- * reference's sz_lossless_decompress -- reads back.  32 KB blocks encoded
+ * reference's sz_lossless_decompress -- reads back.  8 KB blocks encoded
  * independently (greedy matches within the block, raw literals, sequences
  * with the predefined FSE tables); the frame is larger than ZSTD level 3's. */
 size_t cpsz_b200_lossless_bound(size_t n);
