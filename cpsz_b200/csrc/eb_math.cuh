@@ -243,22 +243,8 @@ __device__ __forceinline__ float div_approx(float a, float b) {
 constexpr float FFILT_REL = 1.0f / 65536.0f;           // 2^-16
 constexpr float FFILT_ABS = 9.09494702e-13f;           // 2^-40
 
-struct Frac {
-  float n, d;  // the value n / d, d > 0
-};
-// keep_sign2 as a fraction: numerator |D| (D = P - N, accurate), P and N for the denominator
-__device__ __forceinline__ Frac ks2_frac(float D, float P, float N, bool& bad) {
-  if (P == 0.f || N == 0.f) return Frac{1.f, 1.f};
-  const float pn = P * N;
-  bad |= !(pn >= 1.2924697e-33f);  // 2^-110
-  return Frac{fabsf(D), (P + N) + 2.f * sqrt_approx(pn)};
-}
 __device__ __forceinline__ float pos_part(float t) { return t > 0.f ? t : 0.f; }
 __device__ __forceinline__ float neg_part(float t) { return t < 0.f ? -t : 0.f; }
-// two-term bound (max_eb_to_keep_sign_2d_offline_2) of (a, b) with a + b = D
-__device__ __forceinline__ Frac off2_frac(float D, float a, float b, bool& bad) {
-  return ks2_frac(D, pos_part(a) + pos_part(b), neg_part(a) + neg_part(b), bad);
-}
 
 // ---- both triangles of a cell at once --------------------------------------------
 // Cell (a, b) of the grid holds the "upper" triangle {(a,b), (a+1,b), (a+1,b+1)}
@@ -312,8 +298,8 @@ __device__ __forceinline__ void two_diff2(f32x2 a, f32x2 c, f32x2& s, f32x2& e) 
 struct Frac2 {
   f32x2 n, d;  // word by word the value n / d (d > 0); n may carry D's sign: the value is |n| / d
 };
-// ks2_frac of both words: D, P, N per word
-__device__ __forceinline__ Frac2 ks2_frac2(f32x2 D, f32x2 P, f32x2 N, bool& bad_x, bool& bad_y) {
+// ks2_frac of both words: D, P, N and PpN (P + N) per word
+__device__ __forceinline__ Frac2 ks2_frac2(f32x2 D, f32x2 P, f32x2 N, f32x2 PpN, bool& bad_x, bool& bad_y) {
   const f32x2 pn = mul2(P, N);
   float P0, P1, N0, N1, q0, q1, D0, D1;
   unpk2(P, P0, P1);
@@ -324,7 +310,7 @@ __device__ __forceinline__ Frac2 ks2_frac2(f32x2 D, f32x2 P, f32x2 N, bool& bad_
   bad_x |= !one0 && !(q0 >= 1.2924697e-33f);  // 2^-110
   bad_y |= !one1 && !(q1 >= 1.2924697e-33f);
   const f32x2 sq = pk2(sqrt_approx(q0), sqrt_approx(q1));
-  const f32x2 d = add2(add2(P, N), add2(sq, sq));  // (P + N) + 2 sqrt(P N)
+  const f32x2 d = add2(PpN, add2(sq, sq));  // (P + N) + 2 sqrt(P N)
   float d0, d1;
   unpk2(d, d0, d1);
   return Frac2{pk2(one0 ? 1.f : D0, one1 ? 1.f : D1), pk2(one0 ? 1.f : d0, one1 ? 1.f : d1)};
@@ -338,17 +324,6 @@ __device__ __forceinline__ f32x2 neg2(f32x2 t) {
   float a, b;
   unpk2(t, a, b);
   return pk2(neg_part(a), neg_part(b));
-}
-// two-term bound of (a, -c), a - c = D
-__device__ __forceinline__ Frac2 off2_frac2(f32x2 D, f32x2 a, f32x2 c, bool& bad_x, bool& bad_y) {
-  return ks2_frac2(D, add2(pos2(a), neg2(c)), add2(neg2(a), pos2(c)), bad_x, bad_y);
-}
-// four-term bound of (a, -b, c, -d), a - b + c - d = D
-__device__ __forceinline__ Frac2 off4_frac2(f32x2 D, f32x2 a, f32x2 b, f32x2 c, f32x2 d, bool& bad_x,
-                                            bool& bad_y) {
-  const f32x2 P = add2(add2(add2(pos2(a), neg2(b)), pos2(c)), neg2(d));
-  const f32x2 N = add2(add2(add2(neg2(a), pos2(b)), neg2(c)), pos2(d));
-  return ks2_frac2(D, P, N, bad_x, bad_y);
 }
 // word by word: take b where pick (else a)
 __device__ __forceinline__ Frac2 frac_pick2(Frac2 a, Frac2 b, bool pick0, bool pick1) {
@@ -384,6 +359,14 @@ __device__ __forceinline__ Frac2 frac_max2_if(Frac2 e, Frac2 a, bool take0, bool
 // ok_* false for a triangle that takes the exact path.  Vertices: U00 = (a,b),
 // U10 = (a+1,b), U01 = (a,b+1), U11 = (a+1,b+1); the upper triangle is
 // (U00, U10, U11), the lower (U00, U01, U11) -- tri_eb's (u0, u1, u2).
+//
+// Sums of parts.  Every bound's P and N are sums of the positive / negated
+// negative parts of two or four of the terms (p20, -p02), (p12, -p21),
+// (p01, -p10), whose pairs give P_k = pos(a) + neg(c), N_k = neg(a) + pos(c)
+// for edge k = (a, -c): the two-term bound of x_k uses P_k, N_k, the
+// four-term bound of s_k = x_i + x_j uses P_i + P_j, N_i + N_j, and
+// S = (PN_1 + PN_2) + PN_3 with PN_k = P_k + N_k = |a| + |c|.  Summed in
+// pairs, each is within 2u of its exact value (the filter allows 3u).
 __device__ __forceinline__ void cell_eb_float(float U00, float U10, float U01, float U11, float V00, float V10,
                                               float V01, float V11, float& t_up, float& t_lo, bool& ok_up,
                                               bool& ok_lo) {
@@ -405,13 +388,12 @@ __device__ __forceinline__ void cell_eb_float(float U00, float U10, float U01, f
   const f32x2 s2 = add2(h2, add2(g2, add2(e1, e3)));
   const f32x2 s3 = add2(h3, add2(g3, e12));
   const f32x2 det = add2(hd, add2(gd, add2(g1, add2(e12, e3))));
-  float P01[2], P10[2], P02[2], P20[2], P12[2], P21[2], X1[2], X2[2], X3[2], S1[2], S2[2], S3[2], DT[2];
-  unpk2(p01, P01[0], P01[1]);
-  unpk2(p10, P10[0], P10[1]);
-  unpk2(p02, P02[0], P02[1]);
-  unpk2(p20, P20[0], P20[1]);
-  unpk2(p12, P12[0], P12[1]);
-  unpk2(p21, P21[0], P21[1]);
+  const f32x2 P1 = add2(pos2(p20), neg2(p02)), N1 = add2(neg2(p20), pos2(p02));
+  const f32x2 P2 = add2(pos2(p12), neg2(p21)), N2 = add2(neg2(p12), pos2(p21));
+  const f32x2 P3 = add2(pos2(p01), neg2(p10)), N3 = add2(neg2(p01), pos2(p10));
+  const f32x2 PN1 = add2(P1, N1), PN2 = add2(P2, N2), PN3 = add2(P3, N3);
+  float S[2], X1[2], X2[2], X3[2], S1[2], S2[2], S3[2], DT[2];
+  unpk2(add2(add2(PN1, PN2), PN3), S[0], S[1]);
   unpk2(x1, X1[0], X1[1]);
   unpk2(x2, X2[0], X2[1]);
   unpk2(x3, X3[0], X3[1]);
@@ -422,11 +404,9 @@ __device__ __forceinline__ void cell_eb_float(float U00, float U10, float U01, f
   bool bad[2], f1[2], f2[2], f3[2];
 #pragma unroll
   for (int w = 0; w < 2; w++) {
-    // the shared values are bitwise the same in both words: word 0's serve both
-    const float S = ((((fabsf(P01[w]) + fabsf(P10[w])) + fabsf(P12[w])) + fabsf(P21[w])) + fabsf(P20[0])) +
-                    fabsf(P02[0]);
-    const float T = S * 5.68434189e-14f;  // 2^-44
-    bool b = !(S >= 8.67361738e-19f && S <= 1.09951163e12f);  // [2^-60, 2^40], false for NaN
+    // x1 is bitwise the same in both words: word 0's serves both
+    const float T = S[w] * 5.68434189e-14f;  // 2^-44
+    bool b = !(S[w] >= 8.67361738e-19f && S[w] <= 1.09951163e12f);  // [2^-60, 2^40], false for NaN
     b |= !(fabsf(S1[w]) > T && fabsf(S2[w]) > T && fabsf(S3[w]) > T && fabsf(DT[w]) > T);
     b |= X1[0] == 0.f || X2[w] == 0.f || X3[w] == 0.f;
     f1[w] = (S1[w] > 0.f) == (X1[0] > 0.f);
@@ -434,16 +414,28 @@ __device__ __forceinline__ void cell_eb_float(float U00, float U10, float U01, f
     f3[w] = (S3[w] > 0.f) == (X3[w] > 0.f);
     bad[w] = b || (f1[w] && f2[w] && f3[w]);  // a critical point: exact path
   }
-  // max over failing flags of min(off2, off4), all three evaluated (no
-  // divergence); off2 of x1 is the same for both triangles
-  bool bad1 = false;
-  const Frac t1 = off2_frac(X1[0], P20[0], -P02[0], bad1);
-  bad[0] |= bad1;
-  bad[1] |= bad1;
-  const Frac2 a1 = frac_min2(Frac2{pk2(t1.n, t1.n), pk2(t1.d, t1.d)},
-                             off4_frac2(s1, p01, p10, p12, p21, bad[0], bad[1]));
-  const Frac2 a2 = frac_min2(off2_frac2(x2, p12, p21, bad[0], bad[1]), off4_frac2(s2, p01, p10, p20, p02, bad[0], bad[1]));
-  const Frac2 a3 = frac_min2(off2_frac2(x3, p01, p10, bad[0], bad[1]), off4_frac2(s3, p12, p21, p20, p02, bad[0], bad[1]));
+  // max over failing flags of min(two-term, four-term bound), all three
+  // evaluated (no divergence); the two-term bound of x1 is the same for both
+  // triangles and is evaluated once
+  Frac2 t1;
+  {
+    float P10w, N10w, PN10w, unused;
+    unpk2(P1, P10w, unused);
+    unpk2(N1, N10w, unused);
+    unpk2(PN1, PN10w, unused);
+    bool one = P10w == 0.f || N10w == 0.f;
+    const float q = P10w * N10w;
+    const bool b1 = !one && !(q >= 1.2924697e-33f);  // 2^-110
+    bad[0] |= b1;
+    bad[1] |= b1;
+    const float n = one ? 1.f : X1[0], d = one ? 1.f : PN10w + 2.f * sqrt_approx(q);
+    t1 = Frac2{pk2(n, n), pk2(d, d)};
+  }
+  const Frac2 a1 = frac_min2(t1, ks2_frac2(s1, add2(P2, P3), add2(N2, N3), add2(PN2, PN3), bad[0], bad[1]));
+  const Frac2 a2 = frac_min2(ks2_frac2(x2, P2, N2, PN2, bad[0], bad[1]),
+                             ks2_frac2(s2, add2(P1, P3), add2(N1, N3), add2(PN1, PN3), bad[0], bad[1]));
+  const Frac2 a3 = frac_min2(ks2_frac2(x3, P3, N3, PN3, bad[0], bad[1]),
+                             ks2_frac2(s3, add2(P1, P2), add2(N1, N2), add2(PN1, PN2), bad[0], bad[1]));
   Frac2 e{pk2(0.f, 0.f), pk2(1.f, 1.f)};
   e = frac_max2_if(e, a1, !f1[0], !f1[1]);
   e = frac_max2_if(e, a2, !f2[0], !f2[1]);
