@@ -3,7 +3,8 @@
     python -m cpsz_b200.autotune [--out cpsz_b200/tuning_b200.json] [--quick]
 
 For each size bucket and each output-invariant launch parameter, the sweep
-compresses a seeded synthetic field with every candidate value (the other
+compresses a seeded synthetic field (2D: the flow density and width of the
+8192^2 headline field, scaled to the side) with every candidate value (the other
 parameters at their current best), times the stage that the parameter shapes
 with the context's CUDA-event stage marks, and keeps the fastest value.  Every
 candidate's blob must equal the default's byte for byte, or the sweep stops:
@@ -64,7 +65,9 @@ class Case:
 
         self.kind, self.side, self.ctx = kind, side, ctx
         if kind == "2d":
-            self.host = workloads.cfg0_like(seed, side, side)
+            # the 8192^2 headline field's flow density and width at every side
+            n_flows = max(1, round(2000 * (side / 8192) ** 2))
+            self.host = workloads.field_2d(seed, side, side, n_flows, 60.0)
             self.shape = (side, side)
             self.eb = 0.1
         else:
