@@ -198,9 +198,9 @@ __device__ __forceinline__ float sqrt_approx(float x) {
   asm("sqrt.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
-__device__ __forceinline__ float div_approx(float a, float b) {
+__device__ __forceinline__ float rcp_approx(float x) {
   float y;
-  asm("div.approx.f32 %0, %1, %2;" : "=f"(y) : "f"(a), "f"(b));
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
 // ---- float-filtered 2D bound ------------------------------------------------------
@@ -231,13 +231,14 @@ __device__ __forceinline__ float div_approx(float a, float b) {
 //    accurate values above: x_k for the two-term bounds, s_k for the
 //    four-term ones (p01 - p10 + p12 - p21 = x3 + x2, and so on).  The
 //    denominator d = P + N + 2 sqrt(P N) comes from float sums of the terms
-//    (3u relative each) and sqrt.approx: within 2^-20 relative.  The
-//    triangle's bound is the max over failing flags of the min of two such
-//    fractions, compared by cross-multiplication (a choice can only go wrong
-//    between values within 2^-22 of each other), with one div.approx
-//    (2 ulp) at the end.  The result t is within 2^-18 t of the real value,
-//    and the reference's double value within 2^-50 r + 2^-52 of it; the
-//    enclosure uses 2^-16 relative and 2^-40 absolute.
+//    (3u relative each) and sqrt.approx: within 2^-20 relative.  Each value
+//    is |D| times rcp.approx(d) (at most 9.9e-8 relative on these operands,
+//    measured with the other premises) rounded once: within 2^-19.6 of the
+//    real one.  The triangle's bound is the max over failing flags of the
+//    min of two such values, both exact, so it too is within 2^-19.6 of the
+//    real value's; the result t is within 2^-18 t of the real value, and the
+//    reference's double value within 2^-50 r + 2^-52 of it; the enclosure
+//    uses 2^-16 relative and 2^-40 absolute.
 //  * range.  Exact path when S is not finite, S > 2^40 or S < 2^-60, or a
 //    product P N is below 2^-110 and not 0 (sqrt of a subnormal product).
 constexpr float FFILT_REL = 1.0f / 65536.0f;           // 2^-16
@@ -295,25 +296,23 @@ __device__ __forceinline__ void two_diff2(f32x2 a, f32x2 c, f32x2& s, f32x2& e) 
   const f32x2 bb = sub2(s, a);
   e = sub2(sub2(a, sub2(s, bb)), add2(c, bb));
 }
-struct Frac2 {
-  f32x2 n, d;  // word by word the value n / d (d > 0); n may carry D's sign: the value is |n| / d
-};
-// ks2_frac of both words: D, P, N and PpN (P + N) per word
-__device__ __forceinline__ Frac2 ks2_frac2(f32x2 D, f32x2 P, f32x2 N, f32x2 PpN, bool& bad_x, bool& bad_y) {
+// keep_sign2 of both words: 1 where P or N is 0, else +-|D| / d with
+// d = (P + N) + 2 sqrt(P N) (PpN = P + N) as D * rcp.approx(d); the sign is
+// D's (callers take |.|)
+__device__ __forceinline__ f32x2 ks2_val2(f32x2 D, f32x2 P, f32x2 N, f32x2 PpN, bool& bad_x, bool& bad_y) {
   const f32x2 pn = mul2(P, N);
-  float P0, P1, N0, N1, q0, q1, D0, D1;
+  float P0, P1, N0, N1, q0, q1;
   unpk2(P, P0, P1);
   unpk2(N, N0, N1);
   unpk2(pn, q0, q1);
-  unpk2(D, D0, D1);
   const bool one0 = P0 == 0.f || N0 == 0.f, one1 = P1 == 0.f || N1 == 0.f;
   bad_x |= !one0 && !(q0 >= 1.2924697e-33f);  // 2^-110
   bad_y |= !one1 && !(q1 >= 1.2924697e-33f);
   const f32x2 sq = pk2(sqrt_approx(q0), sqrt_approx(q1));
-  const f32x2 d = add2(PpN, add2(sq, sq));  // (P + N) + 2 sqrt(P N)
-  float d0, d1;
-  unpk2(d, d0, d1);
-  return Frac2{pk2(one0 ? 1.f : D0, one1 ? 1.f : D1), pk2(one0 ? 1.f : d0, one1 ? 1.f : d1)};
+  float d0, d1, v0, v1;
+  unpk2(add2(PpN, add2(sq, sq)), d0, d1);
+  unpk2(mul2(D, pk2(rcp_approx(d0), rcp_approx(d1))), v0, v1);
+  return pk2(one0 ? 1.f : v0, one1 ? 1.f : v1);
 }
 __device__ __forceinline__ f32x2 pos2(f32x2 t) {
   float a, b;
@@ -325,36 +324,6 @@ __device__ __forceinline__ f32x2 neg2(f32x2 t) {
   unpk2(t, a, b);
   return pk2(neg_part(a), neg_part(b));
 }
-// word by word: take b where pick (else a)
-__device__ __forceinline__ Frac2 frac_pick2(Frac2 a, Frac2 b, bool pick0, bool pick1) {
-  float an0, an1, ad0, ad1, bn0, bn1, bd0, bd1;
-  unpk2(a.n, an0, an1);
-  unpk2(a.d, ad0, ad1);
-  unpk2(b.n, bn0, bn1);
-  unpk2(b.d, bd0, bd1);
-  return Frac2{pk2(pick0 ? bn0 : an0, pick1 ? bn1 : an1), pk2(pick0 ? bd0 : ad0, pick1 ? bd1 : ad1)};
-}
-// |a.n| * b.d against |b.n| * a.d, word by word (d > 0, so |n| * d = |n * d|)
-__device__ __forceinline__ void frac_cmp2(Frac2 a, Frac2 b, float& l0, float& l1, float& r0, float& r1) {
-  unpk2(mul2(a.n, b.d), l0, l1);
-  unpk2(mul2(b.n, a.d), r0, r1);
-  l0 = fabsf(l0);
-  l1 = fabsf(l1);
-  r0 = fabsf(r0);
-  r1 = fabsf(r1);
-}
-__device__ __forceinline__ Frac2 frac_min2(Frac2 a, Frac2 b) {
-  float l0, l1, r0, r1;
-  frac_cmp2(a, b, l0, l1, r0, r1);
-  return frac_pick2(a, b, !(l0 <= r0), !(l1 <= r1));
-}
-// e = frac_max(e, a) in the words where take is set
-__device__ __forceinline__ Frac2 frac_max2_if(Frac2 e, Frac2 a, bool take0, bool take1) {
-  float l0, l1, r0, r1;
-  frac_cmp2(e, a, l0, l1, r0, r1);
-  return frac_pick2(e, a, take0 && !(l0 >= r0), take1 && !(l1 >= r1));
-}
-
 // The float bounds of the cell's upper (t_up) and lower (t_lo) triangles, with
 // ok_* false for a triangle that takes the exact path.  Vertices: U00 = (a,b),
 // U10 = (a+1,b), U01 = (a,b+1), U11 = (a+1,b+1); the upper triangle is
@@ -417,34 +386,36 @@ __device__ __forceinline__ void cell_eb_float(float U00, float U10, float U01, f
   // max over failing flags of min(two-term, four-term bound), all three
   // evaluated (no divergence); the two-term bound of x1 is the same for both
   // triangles and is evaluated once
-  Frac2 t1;
+  float k1;
   {
-    float P10w, N10w, PN10w, unused;
-    unpk2(P1, P10w, unused);
-    unpk2(N1, N10w, unused);
-    unpk2(PN1, PN10w, unused);
-    bool one = P10w == 0.f || N10w == 0.f;
-    const float q = P10w * N10w;
+    float P1w, N1w, PN1w, unused;
+    unpk2(P1, P1w, unused);
+    unpk2(N1, N1w, unused);
+    unpk2(PN1, PN1w, unused);
+    const bool one = P1w == 0.f || N1w == 0.f;
+    const float q = P1w * N1w;
     const bool b1 = !one && !(q >= 1.2924697e-33f);  // 2^-110
     bad[0] |= b1;
     bad[1] |= b1;
-    const float n = one ? 1.f : X1[0], d = one ? 1.f : PN10w + 2.f * sqrt_approx(q);
-    t1 = Frac2{pk2(n, n), pk2(d, d)};
+    k1 = one ? 1.f : X1[0] * rcp_approx(PN1w + 2.f * sqrt_approx(q));
   }
-  const Frac2 a1 = frac_min2(t1, ks2_frac2(s1, add2(P2, P3), add2(N2, N3), add2(PN2, PN3), bad[0], bad[1]));
-  const Frac2 a2 = frac_min2(ks2_frac2(x2, P2, N2, PN2, bad[0], bad[1]),
-                             ks2_frac2(s2, add2(P1, P3), add2(N1, N3), add2(PN1, PN3), bad[0], bad[1]));
-  const Frac2 a3 = frac_min2(ks2_frac2(x3, P3, N3, PN3, bad[0], bad[1]),
-                             ks2_frac2(s3, add2(P1, P2), add2(N1, N2), add2(PN1, PN2), bad[0], bad[1]));
-  Frac2 e{pk2(0.f, 0.f), pk2(1.f, 1.f)};
-  e = frac_max2_if(e, a1, !f1[0], !f1[1]);
-  e = frac_max2_if(e, a2, !f2[0], !f2[1]);
-  e = frac_max2_if(e, a3, !f3[0], !f3[1]);
-  float n0, n1, d0, d1;
-  unpk2(e.n, n0, n1);
-  unpk2(e.d, d0, d1);
-  t_up = div_approx(fabsf(n0), d0);
-  t_lo = div_approx(fabsf(n1), d1);
+  float a1[2], a2[2], a3[2], b2[2], b3[2];
+  unpk2(ks2_val2(s1, add2(P2, P3), add2(N2, N3), add2(PN2, PN3), bad[0], bad[1]), a1[0], a1[1]);
+  unpk2(ks2_val2(x2, P2, N2, PN2, bad[0], bad[1]), a2[0], a2[1]);
+  unpk2(ks2_val2(s2, add2(P1, P3), add2(N1, N3), add2(PN1, PN3), bad[0], bad[1]), b2[0], b2[1]);
+  unpk2(ks2_val2(x3, P3, N3, PN3, bad[0], bad[1]), a3[0], a3[1]);
+  unpk2(ks2_val2(s3, add2(P1, P2), add2(N1, N2), add2(PN1, PN2), bad[0], bad[1]), b3[0], b3[1]);
+  float t[2];
+#pragma unroll
+  for (int w = 0; w < 2; w++) {
+    float e = 0.f;
+    if (!f1[w]) e = fmaxf(e, fminf(fabsf(k1), fabsf(a1[w])));
+    if (!f2[w]) e = fmaxf(e, fminf(fabsf(a2[w]), fabsf(b2[w])));
+    if (!f3[w]) e = fmaxf(e, fminf(fabsf(a3[w]), fabsf(b3[w])));
+    t[w] = e;
+  }
+  t_up = t[0];
+  t_lo = t[1];
   ok_up = !bad[0];
   ok_lo = !bad[1];
 }
@@ -537,11 +508,6 @@ __device__ __forceinline__ float lg2_approx(float x) {
 __device__ __forceinline__ float ex2_approx(float x) {
   float y;
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-__device__ __forceinline__ float rcp_approx(float x) {
-  float y;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
 // Enclosure [lo, hi] of keep_sign_3d(P, N) for finite P, N >= 0 ([-1, 2]
