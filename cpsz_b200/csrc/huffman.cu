@@ -370,20 +370,10 @@ __device__ __forceinline__ void hist_add(unsigned int* sh, unsigned long long* h
   }
 }
 
-// Stream blockIdx.y (s0 / s1, n symbols each) into its histogram (h0 / h1).
-__global__ void __launch_bounds__(HIST_NT) hist_u16_kernel(const uint16_t* __restrict__ s0,
-                                                           const uint16_t* __restrict__ s1, size_t n,
-                                                           unsigned long long* __restrict__ h0,
-                                                           unsigned long long* __restrict__ h1) {
-  const uint16_t* __restrict__ s = blockIdx.y ? s1 : s0;
-  unsigned long long* __restrict__ hist = blockIdx.y ? h1 : h0;
-  __shared__ unsigned int sh[HIST_W + 1];  // window + symbol 0
-  for (int k = threadIdx.x; k <= HIST_W; k += HIST_NT) sh[k] = 0;
-  __syncthreads();
-  unsigned c_lo = 0, c_mid = 0, c_hi = 0;
-  const size_t stride = (size_t)gridDim.x * HIST_NT;
-  const size_t t0 = (size_t)blockIdx.x * HIST_NT + threadIdx.x;
-  // elements before the first 16-byte boundary, the vector body, the tail
+// Symbols t0, t0 + stride, ... of s[0, n) into the shared window / registers:
+// the elements before the first 16-byte boundary, the vector body, the tail.
+__device__ __forceinline__ void hist_span(unsigned* sh, unsigned long long* hist, const uint16_t* s, size_t n,
+                                          size_t t0, size_t stride, unsigned& c_lo, unsigned& c_mid, unsigned& c_hi) {
   const size_t head = ((16 - ((uintptr_t)s & 15)) & 15) / 2;
   const size_t h = head < n ? head : n;
   if (t0 < h) hist_add(sh, hist, s[t0], c_lo, c_mid, c_hi);
@@ -399,6 +389,10 @@ __global__ void __launch_bounds__(HIST_NT) hist_u16_kernel(const uint16_t* __res
     }
   }
   for (size_t i = h + nv * 8 + t0; i < n; i += stride) hist_add(sh, hist, s[i], c_lo, c_mid, c_hi);
+}
+// The register counts and the shared window into the global histogram.
+__device__ __forceinline__ void hist_flush(unsigned* sh, unsigned long long* hist, unsigned c_lo, unsigned c_mid,
+                                           unsigned c_hi) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     c_lo += __shfl_down_sync(0xffffffffu, c_lo, o);
@@ -414,6 +408,92 @@ __global__ void __launch_bounds__(HIST_NT) hist_u16_kernel(const uint16_t* __res
   for (int k = threadIdx.x; k < HIST_W; k += HIST_NT)
     if (sh[k]) atomicAdd(&hist[HIST_LO + k], (unsigned long long)sh[k]);
   if (threadIdx.x == 0 && sh[HIST_W]) atomicAdd(&hist[0], (unsigned long long)sh[HIST_W]);
+}
+
+// Stream blockIdx.y (s0 / s1, n symbols each) into its histogram (h0 / h1).
+__global__ void __launch_bounds__(HIST_NT) hist_u16_kernel(const uint16_t* __restrict__ s0,
+                                                           const uint16_t* __restrict__ s1, size_t n,
+                                                           unsigned long long* __restrict__ h0,
+                                                           unsigned long long* __restrict__ h1) {
+  const uint16_t* __restrict__ s = blockIdx.y ? s1 : s0;
+  unsigned long long* __restrict__ hist = blockIdx.y ? h1 : h0;
+  __shared__ unsigned int sh[HIST_W + 1];  // window + symbol 0
+  for (int k = threadIdx.x; k <= HIST_W; k += HIST_NT) sh[k] = 0;
+  __syncthreads();
+  unsigned c_lo = 0, c_mid = 0, c_hi = 0;
+  hist_span(sh, hist, s, n, (size_t)blockIdx.x * HIST_NT + threadIdx.x, (size_t)gridDim.x * HIST_NT, c_lo, c_mid,
+            c_hi);
+  hist_flush(sh, hist, c_lo, c_mid, c_hi);
+}
+
+// ---- histogram follower ----------------------------------------------------------
+// Counts a field's code histograms while its wavefront is still running:
+// blockIdx.y is the component; the CTAs take slices of FOLLOW_ROWS rows in
+// row order from the component's ticket, wait for the slice's row group to
+// be flagged done by the wavefront (thread 0 polls with acquire loads, the
+// CTA then acquires), and count the slice.  The wavefront finishes its
+// groups in row order, so most of the field is counted during the
+// wavefront's tail and only the last group's slices remain once it ends.
+// A wait that outlasts FOLLOW_WAIT_NS (the wavefront is not running: a tool
+// serialises kernels) sets *gave_up and every CTA stops; the host counts
+// the histograms again.
+constexpr int FOLLOW_ROWS = 8;
+constexpr long long FOLLOW_WAIT_NS = 100000000ll;  // 100 ms
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ long long follow_clock_ns() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__global__ void __launch_bounds__(HIST_NT) hist_follow_kernel(const uint16_t* __restrict__ c0,
+                                                              const uint16_t* __restrict__ c1,
+                                                              const unsigned* __restrict__ d0,
+                                                              const unsigned* __restrict__ d1, int r1, int r2,
+                                                              unsigned long long* __restrict__ h0,
+                                                              unsigned long long* __restrict__ h1,
+                                                              unsigned* __restrict__ tickets, int* gave_up) {
+  const uint16_t* __restrict__ codes = blockIdx.y ? c1 : c0;
+  const unsigned* __restrict__ done = blockIdx.y ? d1 : d0;
+  unsigned long long* __restrict__ hist = blockIdx.y ? h1 : h0;
+  __shared__ unsigned int sh[HIST_W + 1];
+  __shared__ int s_slice;
+  for (int k = threadIdx.x; k <= HIST_W; k += HIST_NT) sh[k] = 0;
+  unsigned c_lo = 0, c_mid = 0, c_hi = 0;
+  const int nslices = (r1 + FOLLOW_ROWS - 1) / FOLLOW_ROWS;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      int sl = (int)atomicAdd(tickets + blockIdx.y, 1u);
+      if (sl < nslices) {
+        const unsigned* flag = done + (sl * FOLLOW_ROWS) / WAVE_GROUP_ROWS;
+        if (!ld_acquire_u32(flag)) {
+          const long long t0 = follow_clock_ns();
+          while (!ld_acquire_u32(flag)) {
+            if (*(volatile int*)gave_up || follow_clock_ns() - t0 > FOLLOW_WAIT_NS) {
+              atomicOr(gave_up, 1);
+              sl = nslices;
+              break;
+            }
+            __nanosleep(1000);
+          }
+        }
+      }
+      s_slice = sl;
+    }
+    __syncthreads();
+    const int sl = s_slice;
+    if (sl >= nslices) break;
+    (void)ld_acquire_u32(done + (sl * FOLLOW_ROWS) / WAVE_GROUP_ROWS);
+    const int row0 = sl * FOLLOW_ROWS, rows = min(FOLLOW_ROWS, r1 - row0);
+    hist_span(sh, hist, codes + (size_t)row0 * r2, (size_t)rows * r2, threadIdx.x, HIST_NT, c_lo, c_mid, c_hi);
+    __syncthreads();  // s_slice is rewritten only after every thread has read it
+  }
+  hist_flush(sh, hist, c_lo, c_mid, c_hi);
 }
 
 // ---- decoder ---------------------------------------------------------------------
@@ -684,6 +764,17 @@ int launch_hist_u16_pair(cpsz_b200_ctx* ctx, const uint16_t* a, const uint16_t* 
   hist_u16_kernel<<<dim3(grid, k), HIST_NT, 0, ctx->stream>>>(a, b, n, ha, hb);
   count_launch(ctx);
   return check_launch("hist_u16_kernel");
+}
+
+int launch_hist_follow(cpsz_b200_ctx* ctx, const uint16_t* const codes[2], const unsigned* const group_done[2], int r1,
+                       int r2, unsigned long long* const hist[2], unsigned* tickets, int* gave_up, cudaStream_t stream) {
+  if (r1 <= 0 || r2 <= 0) return CPSZ_OK;
+  const int nslices = (r1 + FOLLOW_ROWS - 1) / FOLLOW_ROWS;
+  const int grid = std::min(nslices, ctx->num_sms);
+  hist_follow_kernel<<<dim3(grid, 2), HIST_NT, 0, stream>>>(codes[0], codes[1], group_done[0], group_done[1], r1, r2,
+                                                            hist[0], hist[1], tickets, gave_up);
+  count_launch(ctx);
+  return check_launch("hist_follow_kernel");
 }
 
 size_t huff_decode_tmp_bytes(size_t nbits) {

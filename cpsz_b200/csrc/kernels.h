@@ -98,6 +98,9 @@ struct WaveField {
   int unit_ncb;
   long long band_wait_ns;
   unsigned long long band_extra;
+  // optional (compression): per row group, set to 1 once the group's codes
+  // are stored (the histogram follower's signal); zeroed before the launch
+  unsigned* group_done;
 };
 struct WaveItem {
   int field;
@@ -197,6 +200,14 @@ int launch_hist_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, unsigned 
 // Two streams of n symbols each in one launch.
 int launch_hist_u16_pair(cpsz_b200_ctx* ctx, const uint16_t* a, const uint16_t* b, size_t n, unsigned long long* ha,
                          unsigned long long* hb);
+// The two code histograms of one field (r1 x r2 raster codes, pitch r2)
+// while its wavefront runs: row groups are counted as their group_done flags
+// (WaveField::group_done) appear.  tickets: 2 words, zeroed.  A wait that
+// outlasts its bound sets *gave_up (zeroed by the caller) and leaves the
+// histograms incomplete; the caller then counts them with
+// launch_hist_u16_pair.  Enqueued on `stream`.
+int launch_hist_follow(cpsz_b200_ctx* ctx, const uint16_t* const codes[2], const unsigned* const group_done[2], int r1,
+                       int r2, unsigned long long* const hist[2], unsigned* tickets, int* gave_up, cudaStream_t stream);
 
 // Decoder table: first-level lookup of HUFF_LUT_BITS bits; entries
 //   leaf:  (sym << 8) | len            (len in 1..HUFF_LUT_BITS)

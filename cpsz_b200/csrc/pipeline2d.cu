@@ -62,6 +62,7 @@ struct DevBuf {
   uint16_t* cblocks[2];
   unsigned long long* hist_codes[2];
   unsigned long long* gbnd;
+  unsigned* gdone;            // per component and row group: the wavefront is done with it; then 2 tickets, gave_up
   unsigned long long* units;  // eb2d progress word, then per-unit counters of finished vertices
   int2* uorder;               // eb2d's unit order (every band's units, band after band)
   void* strip[2];            // strip-pass look-back words and counters
@@ -124,6 +125,8 @@ int read_flag(cpsz_b200_ctx* ctx, int* out) {
 // Pinned word receiving the device flag right after the wavefront of a pass
 // whose wavefront ran beside the bound kernel.
 int* wave_flag_snapshot(cpsz_b200_ctx* ctx) { return (int*)((char*)ctx->pinned + 2048); }
+// Pinned word receiving the histogram follower's gave-up flag.
+int* follow_flag_snapshot(cpsz_b200_ctx* ctx) { return (int*)((char*)ctx->pinned + 2056); }
 
 int flag_error(int flag) {
   if (flag & FLAG_TIMEOUT) return set_error(CPSZ_ERR_TIMEOUT, "a bounded device-side wait gave up");
@@ -233,6 +236,7 @@ int job_alloc(cpsz_b200_ctx* ctx, Job2D& j) {
     d.hist_codes[f] = (unsigned long long*)A(65536 * 8);
   }
   d.gbnd = (unsigned long long*)A(2 * (size_t)j.ngroups * j.r2 * 8);
+  d.gdone = (unsigned*)A((2 * (size_t)j.ngroups + 4) * 4);
   d.units = (unsigned long long*)A(((size_t)j.ngroups * j.ncb + 1) * 8);
   d.uorder = (int2*)A((size_t)j.ngroups * j.ncb * sizeof(int2));
   for (int f = 0; f < 2; f++) {
@@ -469,8 +473,13 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   const int g0 = (nj == 1 && tap && tap->recon_only && tap->requant && jobs[0].eb_ext)
                      ? std::min(std::max(tap->first_group, 0), jobs[0].ngroups)
                      : 0;
+  // One field beside its bounds: the code histograms are counted while the
+  // wavefront's tail runs (hist_follow on the second stream), as its row
+  // groups finish, instead of after it.
+  const bool follow = overlap && nj == 1 && !tap;
   for (int k = 0; k < nj; k++) {
     Job2D& j = jobs[k];
+    if (follow) CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.gdone, 0, (2 * (size_t)j.ngroups + 4) * 4, st));
     for (int f = 0; f < 2; f++) {
       CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.gbnd + ((size_t)f * j.ngroups + g0) * j.r2, 0,
                                     (size_t)(j.ngroups - g0) * j.r2 * 8, st));
@@ -512,6 +521,7 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       F.unit_ncb = j.ncb;
       F.band_wait_ns = ctx->band_wait_ns;
       F.band_extra = ctx->band_unreachable ? 1 : 0;
+      F.group_done = follow ? j.d.gdone + (size_t)f * j.ngroups : nullptr;
       r1v[2 * k + f] = j.r1;
     }
   }
@@ -532,7 +542,7 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     ~HiDrain() {
       if (s) cudaStreamSynchronize(s);
     }
-  } hi_drain;
+  } hi_drain, follow_drain;
   if (overlap) {
     // The wavefront (high-priority stream, one CTA per SM) is launched before
     // its producer eb2d (stage 1), whose CTAs then fill the rest of every SM:
@@ -646,6 +656,25 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_hist_ids, j.d.hist_ids, 256 * 8, cudaMemcpyDeviceToHost, st));
     }
     CPSZ_CUDA_TRY(record(ctx->ev[0]));
+    if (follow) {
+      // the code histograms, counted on the second stream as the wavefront
+      // finishes its row groups; the flag and the histograms come back there
+      Job2D& j = jobs[0];
+      follow_drain.s = ctx->aux;
+      CPSZ_CUDA_TRY(cudaStreamWaitEvent(ctx->aux, ctx->ev[0], 0));
+      const uint16_t* codes[2] = {j.d.craster[0], j.d.craster[1]};
+      const unsigned* gd[2] = {j.d.gdone, j.d.gdone + j.ngroups};
+      unsigned long long* hc[2] = {j.d.hist_codes[0], j.d.hist_codes[1]};
+      unsigned* tix = j.d.gdone + 2 * (size_t)j.ngroups;
+      CPSZ_TRY(launch_hist_follow(ctx, codes, gd, j.r1, j.r2, hc, tix, (int*)(tix + 2), ctx->aux));
+      CPSZ_CUDA_TRY(
+          cudaMemcpyAsync(follow_flag_snapshot(ctx), tix + 2, sizeof(int), cudaMemcpyDeviceToHost, ctx->aux));
+      for (int f = 0; f < 2; f++) {
+        CPSZ_CUDA_TRY(cudaMemcpyAsync(j.h_hist_codes + (size_t)f * 65536, j.d.hist_codes[f], 65536 * 8,
+                                      cudaMemcpyDeviceToHost, ctx->aux));
+        CPSZ_CUDA_TRY(cudaEventRecord(ctx->job_ev[f], ctx->aux));
+      }
+    }
     if (tap && tap->ids)
       CPSZ_CUDA_TRY(cudaMemcpyAsync(tap->ids, jobs[0].d.ids, 2 * jobs[0].N, cudaMemcpyDeviceToDevice, st));
 
@@ -658,16 +687,13 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       // the flag as the wavefront left it, read by the host once the code
       // histograms (enqueued after it) have arrived
       CPSZ_CUDA_TRY(cudaMemcpyAsync(wave_flag_snapshot(ctx), ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+      CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[1], st));
     } else {
       CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points));
     }
     return CPSZ_OK;
   };
-  auto stage_3 = [&]() -> int {
-    mark(ctx, "blocks+hist+unpred");
-
-    // ---- stage 3: code histograms first (the host builds the code trees from
-    // them while the GPU converts to block order and gathers unpredictables) ----
+  auto count_codes = [&]() -> int {
     for (int k = 0; k < nj; k++) {
       Job2D& j = jobs[k];
       CPSZ_TRY(launch_hist_u16_pair(ctx, j.d.craster[0], j.d.craster[1], j.N, j.d.hist_codes[0], j.d.hist_codes[1]));
@@ -677,6 +703,16 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
         CPSZ_CUDA_TRY(record(ctx->job_ev[2 * k + f]));
       }
     }
+    return CPSZ_OK;
+  };
+  bool hist_in_stage3 = !follow;
+  auto stage_3 = [&]() -> int {
+    mark(ctx, "blocks+hist+unpred");
+
+    // ---- stage 3: code histograms first (the host builds the code trees from
+    // them while the GPU converts to block order and gathers unpredictables);
+    // a single field beside its bounds has them from the follower ----
+    if (hist_in_stage3) CPSZ_TRY(count_codes());
     for (int k = 0; k < nj; k++) {
       Job2D& j = jobs[k];
       const float* x[2] = {j.log_form ? j.d.logs[0] : j.d.U, j.log_form ? j.d.logs[1] : j.d.V};
@@ -824,6 +860,15 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
                          huff_build(j.h_hist_codes + (size_t)f * 65536, 65536, 131072, &j.cb[1 + f]);
     });
   };
+  if (follow) {
+    // the follower's histograms; one that gave up (its wavefront was not
+    // running beside it) leaves them to be counted here
+    CPSZ_CUDA_TRY(cudaEventSynchronize(ctx->job_ev[1]));
+    if (*(volatile int*)follow_flag_snapshot(ctx)) {
+      for (int f = 0; f < 2; f++) CPSZ_CUDA_TRY(cudaMemsetAsync(jobs[0].d.hist_codes[f], 0, 65536 * 8, st));
+      CPSZ_TRY(count_codes());
+    }
+  }
   code_trees();
   if (overlap) {
     // The histograms are on the host, so is the flag snapshot taken before
@@ -832,11 +877,15 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
     // incomplete inputs; the bounds are complete now, so the wavefront and
     // everything after it runs again, after the bounds, and the pass goes on.
     // The id stream's packing, already enqueued, depends on the bounds only.
+    CPSZ_CUDA_TRY(cudaEventSynchronize(ctx->ev[1]));
     const int snap = *(volatile int*)wave_flag_snapshot(ctx);
     if (snap & FLAG_TIMEOUT) {
       if (snap != FLAG_TIMEOUT) return flag_error(snap);
       CPSZ_CUDA_TRY(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), st));
-      for (WaveField& F : hf) F.unit_done = nullptr;
+      for (WaveField& F : hf) {
+        F.unit_done = nullptr;
+        F.group_done = nullptr;
+      }
       CPSZ_CUDA_TRY(cudaMemcpyAsync(d_fields, hf.data(), hf.size() * sizeof(WaveField), cudaMemcpyHostToDevice, st));
       for (Job2D& j : jobs) {
         CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.gbnd, 0, 2 * (size_t)j.ngroups * j.r2 * 8, st));
@@ -844,6 +893,7 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       }
       CPSZ_CUDA_TRY(cudaMemsetAsync(queue, 0, 64, st));
       CPSZ_TRY(launch_wave2d(ctx, false, d_fields, d_items, n_items, queue, pass_points));
+      hist_in_stage3 = true;
       CPSZ_TRY(stage_3());
       code_trees();
       ctx->wave_reruns++;

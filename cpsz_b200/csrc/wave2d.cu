@@ -437,6 +437,12 @@ __device__ __forceinline__ void wave2d_body(const WaveField* __restrict__ fields
       }
       else run_helper<DECOMP>(F, item.group, strip, lane, tiles[strip], flag);
     }
+    if (!DECOMP && F.group_done) {
+      // every thread's code stores are visible device-wide before the flag
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) *(volatile unsigned*)(F.group_done + item.group) = 1u;
+    }
     __syncthreads();
   }
 }

@@ -164,6 +164,28 @@ def test_gpu_wavefront_wait_that_gives_up_reruns(oracle):
         c.close()
 
 
+def test_gpu_histogram_follower_that_gives_up_recounts(oracle):
+    """A field compressed beside its bounds has its code histograms counted
+    while the wavefront finishes its row groups.  With the wavefront held back
+    past the follower's 100 ms wait (its own wait for the bounds made to run
+    out after 300 ms), the follower gives up, the pass counts the histograms
+    after the wavefront, runs the wavefront again and returns the oracle's blob."""
+    import time
+
+    c = cpsz_b200.Context(0)
+    try:
+        c.debug_band_wait(300_000_000, unreachable=True)
+        U, V = W.cfg0_like(9, 1000, 1100)
+        n0 = c.wave_reruns
+        t0 = time.perf_counter()
+        a = cpsz_b200.sz_compress_cp_preserve_2d_offline(U, V, max_pwr_eb=0.1, ctx=c)
+        assert time.perf_counter() - t0 > 0.25
+        assert c.wave_reruns == n0 + 1
+        assert_blob_equal_2d(a, oracle.compress_2d(U, V, 0.1))
+    finally:
+        c.close()
+
+
 def test_gpu_serialised_launches_still_compress(tmp_path):
     """With every launch serialised (CUDA_LAUNCH_BLOCKING=1, as under tools that
     run kernels one at a time) the wavefront waits for bounds that no kernel
