@@ -93,12 +93,18 @@ class Heap {
   int end_ = 1;
 };
 
+// Per node of a built tree: its code (right-aligned), pre-order number and depth.
+struct NodeInfo {
+  unsigned long long code;
+  uint32_t pre, depth;
+};
+
 // Per-thread scratch reused by every build on the thread.
 struct Scratch {
-  std::vector<uint32_t> leaf_sym, L, R, C, size, pre;
-  std::vector<uint8_t> T, leaf_len;
-  std::vector<int> kids, depth;
-  std::vector<unsigned long long> heap, leaf_freq, leaf_code, ncode;
+  std::vector<uint32_t> leaf_sym, size;
+  std::vector<int> kids;
+  std::vector<unsigned long long> heap, leaf_freq;
+  std::vector<NodeInfo> info;
 };
 Scratch& scratch() {
   static thread_local Scratch s;
@@ -109,12 +115,6 @@ size_t tree_size_for(size_t nodes) {
   if (nodes <= 256) return 1 + 3 * nodes + 4 * nodes;
   if (nodes <= 65536) return 1 + 4 * nodes + nodes + 4 * nodes;
   return 1 + 12 * nodes + nodes;
-}
-
-template <class T>
-void put(std::vector<uint8_t>& v, size_t& at, T x) {
-  memcpy(v.data() + at, &x, sizeof(T));
-  at += sizeof(T);
 }
 
 }  // namespace
@@ -172,77 +172,63 @@ bool huff_build(const unsigned long long* hist, size_t bins, size_t state_num, H
   // created after both its children, so subtree sizes follow in creation
   // order, and pre-order numbers, depths and codes in reverse creation order
   // (pre(left) = pre(node) + 1, pre(right) = pre(node) + 1 + size(left)).
-  // Each pass reads the merge list sequentially; no load depends on the last.
-  std::vector<uint32_t>&L = sc.L, &R = sc.R, &C = sc.C;
-  std::vector<uint8_t>& T = sc.T;
-  std::vector<unsigned long long>& leaf_code = sc.leaf_code;
-  std::vector<uint8_t>& leaf_len = sc.leaf_len;
-  std::vector<uint32_t>&size = sc.size, &pre = sc.pre;
-  std::vector<unsigned long long>& ncode = sc.ncode;
-  std::vector<int>& depth = sc.depth;
-  L.assign(nn, 0);
-  R.assign(nn, 0);
-  C.assign(nn, 0);
-  T.assign(nn, 0);
+  // L, R, C and t go straight into the serialized tree (zeros where the
+  // reference leaves them 0: leaves' L/R, merged nodes' C/t).
+  std::vector<uint32_t>& size = sc.size;
+  std::vector<NodeInfo>& info = sc.info;
   size.resize(nn);
-  pre.resize(nn);
-  ncode.resize(nn);
-  depth.resize(nn);
-  leaf_code.resize(distinct);
-  leaf_len.resize(distinct);
+  info.resize(nn);
   const size_t nm = nn - distinct;
   for (size_t d = 0; d < distinct; d++) size[d] = 1;
   for (size_t m = 0; m < nm; m++) size[distinct + m] = size[kids[2 * m]] + size[kids[2 * m + 1]] + 1;
-  pre[root] = 0;
-  depth[root] = 0;
-  ncode[root] = 0;
-  int deepest = 0;
-  for (size_t m = nm; m-- > 0;) {
-    const size_t node = distinct + m;
-    const int l = kids[2 * m], r = kids[2 * m + 1];
-    const uint32_t p = pre[node];
-    const int dc = depth[node] + 1;
-    pre[l] = p + 1;
-    pre[r] = p + 1 + size[l];
-    depth[l] = depth[r] = dc;
-    ncode[l] = ncode[node] << 1;
-    ncode[r] = (ncode[node] << 1) | 1ull;
-    L[p] = p + 1;
-    R[p] = p + 1 + size[l];
-    deepest = dc > deepest ? dc : deepest;
+  const size_t tsz = tree_size_for(node_count);
+  out->tree_bytes.assign(8 + 4 + tsz, 0);
+  uint8_t* tb = out->tree_bytes.data();
+  {
+    const unsigned long long nc = node_count;
+    const uint32_t ts = (uint32_t)tsz;
+    memcpy(tb, &nc, 8);
+    memcpy(tb + 8, &ts, 4);  // then sysEndianType 0
   }
+  const int wdt = node_count <= 256 ? 1 : (node_count <= 65536 ? 2 : 4);
+  uint8_t* Lb = tb + 13;
+  uint8_t* Rb = Lb + (size_t)wdt * node_count;
+  uint8_t* Cb = Rb + (size_t)wdt * node_count;
+  uint8_t* Tb = Cb + 4 * node_count;
+  info[root] = NodeInfo{0ull, 0u, 0u};
+  int deepest = 0;
+  auto walk = [&](auto tag) {
+    using Wd = decltype(tag);
+    Wd* Lw = reinterpret_cast<Wd*>(Lb);
+    Wd* Rw = reinterpret_cast<Wd*>(Rb);
+    for (size_t m = nm; m-- > 0;) {
+      const NodeInfo nd = info[distinct + m];
+      const int l = kids[2 * m], r = kids[2 * m + 1];
+      const uint32_t dc = nd.depth + 1, pl = nd.pre + 1, pr = nd.pre + 1 + size[l];
+      info[l] = NodeInfo{nd.code << 1, pl, dc};
+      info[r] = NodeInfo{(nd.code << 1) | 1ull, pr, dc};
+      Wd vl = (Wd)pl, vr = (Wd)pr;
+      memcpy(Lw + nd.pre, &vl, sizeof(Wd));
+      memcpy(Rw + nd.pre, &vr, sizeof(Wd));
+      deepest = (int)dc > deepest ? (int)dc : deepest;
+    }
+  };
+  if (wdt == 1) walk(uint8_t{});
+  else if (wdt == 2) walk(uint16_t{});
+  else walk(uint32_t{});
   if (deepest > 64) {
     set_error(CPSZ_ERR_UNSUPPORTED, "Huffman code longer than 64 bits");
     return false;
   }
-  for (size_t d = 0; d < distinct; d++) {
-    const uint32_t i = pre[d];
-    C[i] = leaf_sym[d];
-    T[i] = 1;
-    leaf_code[d] = ncode[d];
-    leaf_len[d] = (uint8_t)depth[d];
-    out->total_bits += leaf_freq[d] * (unsigned long long)depth[d];
-  }
   out->max_len = deepest;
   out->entries.resize(distinct);
-  for (size_t d = 0; d < distinct; d++) out->entries[d] = HuffEntry{leaf_code[d], leaf_sym[d], leaf_len[d]};
-  const size_t tsz = tree_size_for(node_count);
-  out->tree_bytes.assign(8 + 4 + tsz, 0);
-  size_t at = 0;
-  put<unsigned long long>(out->tree_bytes, at, (unsigned long long)node_count);
-  put<uint32_t>(out->tree_bytes, at, (uint32_t)tsz);
-  put<uint8_t>(out->tree_bytes, at, 0);  // sysEndianType
-  const int wdt = node_count <= 256 ? 1 : (node_count <= 65536 ? 2 : 4);
-  for (int side = 0; side < 2; side++) {
-    const std::vector<uint32_t>& A = side ? R : L;
-    for (size_t i = 0; i < node_count; i++) {
-      if (wdt == 1) put<uint8_t>(out->tree_bytes, at, (uint8_t)A[i]);
-      else if (wdt == 2) put<uint16_t>(out->tree_bytes, at, (uint16_t)A[i]);
-      else put<uint32_t>(out->tree_bytes, at, A[i]);
-    }
+  for (size_t d = 0; d < distinct; d++) {
+    const NodeInfo nd = info[d];
+    memcpy(Cb + 4 * (size_t)nd.pre, &leaf_sym[d], 4);
+    Tb[nd.pre] = 1;
+    out->entries[d] = HuffEntry{nd.code, leaf_sym[d], nd.depth};
+    out->total_bits += leaf_freq[d] * (unsigned long long)nd.depth;
   }
-  for (size_t i = 0; i < node_count; i++) put<uint32_t>(out->tree_bytes, at, C[i]);
-  for (size_t i = 0; i < node_count; i++) put<uint8_t>(out->tree_bytes, at, T[i]);
   return true;
 }
 
