@@ -354,6 +354,7 @@ constexpr int HIST_W = 8192;
 // one quantum): those three are counted in registers and reduced once per
 // warp, so the shared-memory atomics see only the spread-out remainder (no
 // 32-way same-address conflicts).  Reads are 16-byte vectors where aligned.
+template <bool SKIP0 = false>
 __device__ __forceinline__ void hist_add(unsigned int* sh, unsigned long long* hist, unsigned v, unsigned& c_lo,
                                          unsigned& c_mid, unsigned& c_hi) {
   const unsigned d = v - 32767u;
@@ -362,7 +363,7 @@ __device__ __forceinline__ void hist_add(unsigned int* sh, unsigned long long* h
     c_mid += d == 1u;
     c_hi += d == 2u;
   } else if (v == 0u) {
-    atomicAdd(&sh[HIST_W], 1u);
+    if (!SKIP0) atomicAdd(&sh[HIST_W], 1u);
   } else if (v - (unsigned)HIST_LO < (unsigned)HIST_W) {
     atomicAdd(&sh[v - HIST_LO], 1u);
   } else {
@@ -372,11 +373,12 @@ __device__ __forceinline__ void hist_add(unsigned int* sh, unsigned long long* h
 
 // Symbols t0, t0 + stride, ... of s[0, n) into the shared window / registers:
 // the elements before the first 16-byte boundary, the vector body, the tail.
+template <bool SKIP0 = false>
 __device__ __forceinline__ void hist_span(unsigned* sh, unsigned long long* hist, const uint16_t* s, size_t n,
                                           size_t t0, size_t stride, unsigned& c_lo, unsigned& c_mid, unsigned& c_hi) {
   const size_t head = ((16 - ((uintptr_t)s & 15)) & 15) / 2;
   const size_t h = head < n ? head : n;
-  if (t0 < h) hist_add(sh, hist, s[t0], c_lo, c_mid, c_hi);
+  if (t0 < h) hist_add<SKIP0>(sh, hist, s[t0], c_lo, c_mid, c_hi);
   const size_t nv = (n - h) / 8;
   const uint4* sv = reinterpret_cast<const uint4*>(s + h);
   for (size_t i = t0; i < nv; i += stride) {
@@ -384,11 +386,11 @@ __device__ __forceinline__ void hist_span(unsigned* sh, unsigned long long* hist
     const unsigned ws[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-      hist_add(sh, hist, ws[q] & 0xffffu, c_lo, c_mid, c_hi);
-      hist_add(sh, hist, ws[q] >> 16, c_lo, c_mid, c_hi);
+      hist_add<SKIP0>(sh, hist, ws[q] & 0xffffu, c_lo, c_mid, c_hi);
+      hist_add<SKIP0>(sh, hist, ws[q] >> 16, c_lo, c_mid, c_hi);
     }
   }
-  for (size_t i = h + nv * 8 + t0; i < n; i += stride) hist_add(sh, hist, s[i], c_lo, c_mid, c_hi);
+  for (size_t i = h + nv * 8 + t0; i < n; i += stride) hist_add<SKIP0>(sh, hist, s[i], c_lo, c_mid, c_hi);
 }
 // The register counts and the shared window into the global histogram.
 __device__ __forceinline__ void hist_flush(unsigned* sh, unsigned long long* hist, unsigned c_lo, unsigned c_mid,
@@ -410,7 +412,9 @@ __device__ __forceinline__ void hist_flush(unsigned* sh, unsigned long long* his
   if (threadIdx.x == 0 && sh[HIST_W]) atomicAdd(&hist[0], (unsigned long long)sh[HIST_W]);
 }
 
-// Stream blockIdx.y (s0 / s1, n symbols each) into its histogram (h0 / h1).
+// Stream blockIdx.y (s0 / s1, n symbols each) into its histogram (h0 / h1);
+// SKIP0: symbol 0 is not counted.
+template <bool SKIP0>
 __global__ void __launch_bounds__(HIST_NT) hist_u16_kernel(const uint16_t* __restrict__ s0,
                                                            const uint16_t* __restrict__ s1, size_t n,
                                                            unsigned long long* __restrict__ h0,
@@ -421,8 +425,8 @@ __global__ void __launch_bounds__(HIST_NT) hist_u16_kernel(const uint16_t* __res
   for (int k = threadIdx.x; k <= HIST_W; k += HIST_NT) sh[k] = 0;
   __syncthreads();
   unsigned c_lo = 0, c_mid = 0, c_hi = 0;
-  hist_span(sh, hist, s, n, (size_t)blockIdx.x * HIST_NT + threadIdx.x, (size_t)gridDim.x * HIST_NT, c_lo, c_mid,
-            c_hi);
+  hist_span<SKIP0>(sh, hist, s, n, (size_t)blockIdx.x * HIST_NT + threadIdx.x, (size_t)gridDim.x * HIST_NT, c_lo,
+                   c_mid, c_hi);
   hist_flush(sh, hist, c_lo, c_mid, c_hi);
 }
 
@@ -761,7 +765,16 @@ int launch_hist_u16_pair(cpsz_b200_ctx* ctx, const uint16_t* a, const uint16_t* 
   int grid = ctx->num_sms * 2 / k;
   size_t need = (n + HIST_NT - 1) / HIST_NT;
   if ((size_t)grid > need) grid = (int)need;
-  hist_u16_kernel<<<dim3(grid, k), HIST_NT, 0, ctx->stream>>>(a, b, n, ha, hb);
+  hist_u16_kernel<false><<<dim3(grid, k), HIST_NT, 0, ctx->stream>>>(a, b, n, ha, hb);
+  count_launch(ctx);
+  return check_launch("hist_u16_kernel");
+}
+int launch_hist_u16_nonzero(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, unsigned long long* hist) {
+  if (n == 0) return CPSZ_OK;
+  int grid = ctx->num_sms * 2;
+  size_t need = (n + HIST_NT - 1) / HIST_NT;
+  if ((size_t)grid > need) grid = (int)need;
+  hist_u16_kernel<true><<<dim3(grid, 1), HIST_NT, 0, ctx->stream>>>(sym, nullptr, n, hist, nullptr);
   count_launch(ctx);
   return check_launch("hist_u16_kernel");
 }

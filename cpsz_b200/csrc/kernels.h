@@ -197,6 +197,8 @@ int launch_huff_encode_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, Hu
                            int bit0 = 0);
 // Histograms (global, 64-bit bins).
 int launch_hist_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, unsigned long long* hist);
+// The same without symbol 0 (its bin stays as it was).
+int launch_hist_u16_nonzero(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t n, unsigned long long* hist);
 // Two streams of n symbols each in one launch.
 int launch_hist_u16_pair(cpsz_b200_ctx* ctx, const uint16_t* a, const uint16_t* b, size_t n, unsigned long long* ha,
                          unsigned long long* hb);

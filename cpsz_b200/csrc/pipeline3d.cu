@@ -158,28 +158,36 @@ int compress_3d(cpsz_b200_ctx* ctx, const float* U_in, const float* V_in, const 
   CPSZ_TRY(launch_wave3d(ctx, false, pairs, rec, codes, nullptr, 0, &lt, nullptr, nullptr, nullptr, r1, r2, r3,
                           wave_sync));
   mark(ctx, "compact+hist");
-  CPSZ_TRY(launch_chunk_count_3d(ctx, true, codes, N, chunk_cnt));
-  CPSZ_TRY(launch_scan_u32(ctx, chunk_cnt, chunk_off, nchunks, scan_tmp));
-  CPSZ_TRY(launch_compact3d(ctx, codes, ids, dU, dV, dW, N, chunk_off, codes_out, unpred, hist_ids));
+  // The code histogram straight from the raster codes, so the host builds
+  // the code tree while the GPU compacts: a predictable point's three codes
+  // are never 0 (|q| <= 32767 around 32768), an unpredictable point's are,
+  // and so is every fourth lane, so the count without symbol 0 is the
+  // compacted codes' histogram.
   unsigned* h_npred = (unsigned*)ctx->pinned + 4;  // the flag word lives at offset 0
   unsigned long long* h_hist_ids = (unsigned long long*)ctx->pinned + 8;
   unsigned long long* h_hist_codes = h_hist_ids + 256;
+  CPSZ_TRY(launch_hist_u16_nonzero(ctx, reinterpret_cast<const uint16_t*>(codes), 4 * N, hist_codes));
+  CPSZ_CUDA_TRY(cudaMemcpyAsync(h_hist_codes, hist_codes, 65536 * 8, cudaMemcpyDeviceToHost, st));
+  CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[1], st));
+  CPSZ_TRY(launch_chunk_count_3d(ctx, true, codes, N, chunk_cnt));
+  CPSZ_TRY(launch_scan_u32(ctx, chunk_cnt, chunk_off, nchunks, scan_tmp));
+  CPSZ_TRY(launch_compact3d(ctx, codes, ids, dU, dV, dW, N, chunk_off, codes_out, unpred, hist_ids));
   CPSZ_CUDA_TRY(cudaMemcpyAsync(h_npred, chunk_off + nchunks, 4, cudaMemcpyDeviceToHost, st));
   CPSZ_CUDA_TRY(cudaMemcpyAsync(h_hist_ids, hist_ids, 256 * 8, cudaMemcpyDeviceToHost, st));
+  mark(ctx, "host_trees");
+  HuffCodebook cb[2];
+  CPSZ_CUDA_TRY(cudaEventSynchronize(ctx->ev[1]));
+  bool any_code = false;
+  for (size_t s = 1; s < 65536 && !any_code; s++) any_code = h_hist_codes[s] != 0;
+  if (!any_code) h_hist_codes[0] = 1;  // no predictable point: one-leaf tree of symbol 0, no bits
+  if (!huff_build(h_hist_codes, 65536, 131072, &cb[1])) return CPSZ_ERR_INVALID;
   CPSZ_CUDA_TRY(cudaStreamSynchronize(st));
   int flag = 0;
   CPSZ_TRY(read_flag3(ctx, &flag));
   if (flag) return flag_error3(flag);
   const size_t n_pred = *h_npred;
   const size_t n_codes = 3 * n_pred, n_unpred = 3 * (N - n_pred);
-  if (n_codes) CPSZ_TRY(launch_hist_u16(ctx, codes_out, n_codes, hist_codes));
-  CPSZ_CUDA_TRY(cudaMemcpyAsync(h_hist_codes, hist_codes, 65536 * 8, cudaMemcpyDeviceToHost, st));
-  mark(ctx, "host_trees");
-  HuffCodebook cb[2];
   if (!huff_build(h_hist_ids, 256, 512, &cb[0])) return CPSZ_ERR_INVALID;
-  CPSZ_CUDA_TRY(cudaStreamSynchronize(st));
-  if (n_codes == 0) h_hist_codes[0] = 1;  // one-leaf tree of symbol 0, no bits
-  if (!huff_build(h_hist_codes, 65536, 131072, &cb[1])) return CPSZ_ERR_INVALID;
 
   mark(ctx, "huffman_encode");
   const size_t sec_bytes[2] = {huff_section_bytes(cb[0]), huff_section_bytes(cb[1])};
