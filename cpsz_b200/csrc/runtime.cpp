@@ -191,10 +191,22 @@ cpsz_b200_ctx* resolve_ctx(cpsz_b200_ctx* ctx, int* rc) {
   return g_default_ctx[dev];
 }
 
+// Cached pass graphs hold the workspace's and the page-locked staging's
+// addresses (kernel arguments, memset and copy nodes); once either is
+// reallocated they are destroyed, even if the new allocation happens to
+// return the same address (the copy nodes refer to the old allocation).
+static void drop_pass_graphs(cpsz_b200_ctx* ctx) {
+  if (ctx->pass_graphs.empty()) return;
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& g : ctx->pass_graphs) cudaGraphExecDestroy(g.exec);
+  ctx->pass_graphs.clear();
+}
+
 int arena_reserve(cpsz_b200_ctx* ctx, size_t bytes) {
   bytes = align_up(bytes + 4096, 1 << 20);
   ctx->arena.used = 0;
   if (ctx->arena.cap >= bytes) return CPSZ_OK;
+  drop_pass_graphs(ctx);
   if (ctx->arena.base) {
     cudaStreamSynchronize(ctx->stream);
     cudaFree(ctx->arena.base);
@@ -219,6 +231,7 @@ void* arena_alloc(cpsz_b200_ctx* ctx, size_t bytes) {
 
 int pinned_reserve(cpsz_b200_ctx* ctx, size_t bytes) {
   if (ctx->pinned_cap >= bytes) return CPSZ_OK;
+  drop_pass_graphs(ctx);
   if (ctx->pinned) {
     cudaStreamSynchronize(ctx->stream);
     cudaFreeHost(ctx->pinned);
