@@ -481,10 +481,11 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   const int g0 = (nj == 1 && tap && tap->recon_only && tap->requant && jobs[0].eb_ext)
                      ? std::min(std::max(tap->first_group, 0), jobs[0].ngroups)
                      : 0;
-  // One field beside its bounds: the code histograms are counted while the
-  // wavefront's tail runs (hist_follow on the second stream), as its row
-  // groups finish, instead of after it.
-  const bool follow = overlap && nj == 1 && !tap;
+  // One large field beside its bounds: the code histograms are counted while
+  // the wavefront's tail runs (hist_follow on the second stream), as its row
+  // groups finish, instead of after it (below 2^22 points the histograms take
+  // a few microseconds and the follower's own launch and waits cost more).
+  const bool follow = overlap && nj == 1 && !tap && jobs[0].N >= ((size_t)1 << 22);
   for (int k = 0; k < nj; k++) {
     Job2D& j = jobs[k];
     if (follow) CPSZ_CUDA_TRY(cudaMemsetAsync(j.d.gdone, 0, (2 * (size_t)j.ngroups + 4) * 4, st));

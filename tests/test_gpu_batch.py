@@ -156,3 +156,34 @@ def test_sharded_batch_over_nccl_one_rank(oracle, tmp_path):
     fields, ebs = _batch(6, 6, 8, 300)
     for k, ((U, V), eb) in enumerate(zip(fields, ebs)):
         assert_blob_equal_2d(data[int(offs[k]):int(offs[k + 1])], oracle.compress_2d(U, V, eb))
+
+
+def test_batch_graphs_dropped_when_workspace_grows():
+    """Cached pass graphs hold workspace and staging addresses: a call that
+    grows either (a larger batch) drops them, so the first batch is captured
+    again afterwards instead of replayed from a graph whose copy nodes refer
+    to freed memory (a same-address reallocation once crashed the replay)."""
+    torch = pytest.importorskip("torch")
+    c = cpsz_b200.Context(0)
+    try:
+        small, ebs_s = _batch(6, 7, 40, 120)
+        big, ebs_b = _batch(30, 8, 200, 500)
+        dev_s = [(torch.from_numpy(U).cuda(), torch.from_numpy(V).cuda()) for U, V in small]
+        dev_b = [(torch.from_numpy(U).cuda(), torch.from_numpy(V).cuda()) for U, V in big]
+        out = torch.zeros(128 << 20, dtype=torch.uint8, device="cuda")
+
+        def run(dev, e):
+            offs = cpsz_b200.compress_2d_batch(dev, e, out=out, ctx=c)
+            host = out[:int(offs[-1])].cpu().numpy().tobytes()
+            return [host[int(offs[k]):int(offs[k + 1])] for k in range(len(dev))]
+
+        first = run(dev_s, ebs_s)
+        c0, _ = c.graph_stats
+        assert run(dev_s, ebs_s) == first
+        assert c.graph_stats[0] == c0  # replayed
+        run(dev_b, ebs_b)  # grows the workspace and the staging
+        c1, _ = c.graph_stats
+        assert run(dev_s, ebs_s) == first
+        assert c.graph_stats[0] == c1 + 1  # captured again, not replayed
+    finally:
+        c.close()
