@@ -298,8 +298,12 @@ int job_alloc(cpsz_b200_ctx* ctx, Job2D& j) {
 // staged in `small`; the bit streams and unpredictable floats go to bit_dst /
 // unpred_dst.
 struct BlobLayout {
+  // bytes [dst, dst + n) of the blob: from small[src] (ext null), from ext
+  // (host memory that outlives the pass: a code tree), or zeros (zero)
   struct Piece {
     size_t dst, src, n;
+    const uint8_t* ext;
+    bool zero;
   };
   size_t total = 0, bit_dst[3] = {0, 0, 0}, unpred_dst[2] = {0, 0}, sign_dst = 0, sign_bytes = 0;
   std::vector<uint8_t> small;
@@ -318,9 +322,15 @@ int job_layout(const Job2D& j, BlobLayout& L) {
   L.total = total;
   L.sign_bytes = sign_bytes;
   std::vector<uint8_t>& small = L.small;
+  small.reserve(BLOB_HDR + j.cb[0].tree_bytes.size() + 3 * 8 + 2 * FIELD_HDR);
   auto stage = [&](size_t dst, const void* p, size_t n) {
-    L.pieces.push_back(BlobLayout::Piece{dst, small.size(), n});
+    L.pieces.push_back(BlobLayout::Piece{dst, small.size(), n, nullptr, false});
     small.insert(small.end(), (const uint8_t*)p, (const uint8_t*)p + n);
+  };
+  // the code trees and the zero indicator bytes are referenced, not copied:
+  // the layout precedes the code packing, their bytes go up after it
+  auto refer = [&](size_t dst, const uint8_t* p, size_t n) {
+    L.pieces.push_back(BlobLayout::Piece{dst, 0, n, p, p == nullptr});
   };
   {
     uint8_t hdr[BLOB_HDR];
@@ -337,7 +347,8 @@ int job_layout(const Job2D& j, BlobLayout& L) {
   size_t* bit_dst = L.bit_dst;
   size_t* unpred_dst = L.unpred_dst;
   auto stage_huff = [&](int k) {
-    stage(at, j.cb[k].tree_bytes.data(), j.cb[k].tree_bytes.size());
+    if (k == 0) stage(at, j.cb[k].tree_bytes.data(), j.cb[k].tree_bytes.size());
+    else refer(at, j.cb[k].tree_bytes.data(), j.cb[k].tree_bytes.size());
     at += j.cb[k].tree_bytes.size();
     unsigned long long nb = j.bits_bytes[k];
     stage(at, &nb, 8);
@@ -348,7 +359,6 @@ int job_layout(const Job2D& j, BlobLayout& L) {
   stage_huff(0);
   L.sign_dst = at;  // offline_log: sign maps of U and V (copied from the device)
   at += 2 * sign_bytes;
-  std::vector<uint8_t> zeros(ind_bytes, 0);
   for (int f = 0; f < 2; f++) {
     uint8_t fh[FIELD_HDR];
     memset(fh, 0, sizeof(fh));
@@ -362,7 +372,7 @@ int job_layout(const Job2D& j, BlobLayout& L) {
     at += FIELD_HDR;
     unpred_dst[f] = at;
     at += 4 * j.n_unpred[f];
-    stage(at, zeros.data(), ind_bytes);
+    refer(at, nullptr, ind_bytes);
     at += ind_bytes;
     stage_huff(1 + f);
   }
@@ -380,11 +390,22 @@ __global__ void __launch_bounds__(256) pieces_kernel(const uint8_t* __restrict__
   const unsigned long long dst = desc[3 * blockIdx.y], src = desc[3 * blockIdx.y + 1], n = desc[3 * blockIdx.y + 2];
   const unsigned long long c0 = (unsigned long long)blockIdx.x * PIECE_CHUNK;
   const unsigned long long c1 = n < c0 + PIECE_CHUNK ? n : c0 + PIECE_CHUNK;
+  if (src == ~0ull) {  // a run of zeros
+    for (unsigned long long i = c0 + threadIdx.x; i < c1; i += 256) blob[dst + i] = 0;
+    return;
+  }
   for (unsigned long long i = c0 + threadIdx.x; i < c1; i += 256) blob[dst + i] = small[src + i];
 }
 
-// Bytes job_assemble uploads: the small pieces, then their descriptors.
-size_t assemble_upload_bytes(const BlobLayout& L) { return align_up(L.small.size(), 8) + 24 * L.pieces.size(); }
+// Bytes job_assemble uploads: the small pieces and the referenced ones, then
+// their descriptors.
+size_t assemble_payload_bytes(const BlobLayout& L) {
+  size_t n = L.small.size();
+  for (const BlobLayout::Piece& pc : L.pieces)
+    if (pc.ext) n += pc.n;
+  return align_up(n, 8);
+}
+size_t assemble_upload_bytes(const BlobLayout& L) { return assemble_payload_bytes(L) + 24 * L.pieces.size(); }
 
 // The sections of a device blob that the packers do not write: the staged
 // small pieces (header, trees, stream sizes, field headers, indicators), the
@@ -394,13 +415,21 @@ int job_assemble(cpsz_b200_ctx* ctx, Job2D& j, const BlobLayout& L, uint8_t* h_u
   cudaStream_t st = ctx->stream;
   uint8_t* blob = j.blob_base;
   // pieces and their descriptors go up in one copy
-  const size_t up_size = assemble_upload_bytes(L);
+  const size_t up_size = assemble_upload_bytes(L), payload = assemble_payload_bytes(L);
   memcpy(h_up, L.small.data(), L.small.size());
-  unsigned long long* desc = (unsigned long long*)(h_up + align_up(L.small.size(), 8));
+  size_t ext_at = L.small.size();
+  unsigned long long* desc = (unsigned long long*)(h_up + payload);
   for (size_t i = 0; i < L.pieces.size(); i++) {
-    desc[3 * i] = L.pieces[i].dst;
-    desc[3 * i + 1] = L.pieces[i].src;
-    desc[3 * i + 2] = L.pieces[i].n;
+    const BlobLayout::Piece& pc = L.pieces[i];
+    size_t src = pc.src;
+    if (pc.ext) {
+      memcpy(h_up + ext_at, pc.ext, pc.n);
+      src = ext_at;
+      ext_at += pc.n;
+    }
+    desc[3 * i] = pc.dst;
+    desc[3 * i + 1] = pc.zero ? ~0ull : src;
+    desc[3 * i + 2] = pc.n;
   }
   if (up_size > stage_bytes(j)) return set_error(CPSZ_ERR_INVALID, "internal: blob pieces exceed their bound");
   uint8_t* d_up = j.d.stage;
@@ -409,8 +438,7 @@ int job_assemble(cpsz_b200_ctx* ctx, Job2D& j, const BlobLayout& L, uint8_t* h_u
     size_t longest = 0;
     for (const BlobLayout::Piece& pc : L.pieces) longest = std::max(longest, pc.n);
     const dim3 grid((unsigned)std::max<size_t>(1, (longest + PIECE_CHUNK - 1) / PIECE_CHUNK), (unsigned)L.pieces.size());
-    pieces_kernel<<<grid, 256, 0, st>>>(
-        d_up, (const unsigned long long*)(d_up + align_up(L.small.size(), 8)), blob);
+    pieces_kernel<<<grid, 256, 0, st>>>(d_up, (const unsigned long long*)(d_up + payload), blob);
     count_launch(ctx);
     CPSZ_TRY(check_launch("pieces_kernel"));
   }
@@ -953,7 +981,10 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   };
   if (hj) {
     const BlobLayout& hl = lay[0];
-    for (const BlobLayout::Piece& pc : hl.pieces) memcpy(hj->host_out + pc.dst, hl.small.data() + pc.src, pc.n);
+    for (const BlobLayout::Piece& pc : hl.pieces) {
+      if (pc.zero) memset(hj->host_out + pc.dst, 0, pc.n);
+      else memcpy(hj->host_out + pc.dst, pc.ext ? pc.ext : hl.small.data() + pc.src, pc.n);
+    }
     if (h_async)
       for (int f = 0; f < 2; f++) {
         CPSZ_TRY(d2h_beside(hj->host_out + hl.unpred_dst[f], hj->d.unpred[f], 4 * hj->n_unpred[f]));
