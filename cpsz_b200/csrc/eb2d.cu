@@ -33,7 +33,7 @@ namespace cpsz {
 
 // 64 registers a thread at most (2048 threads an SM): with the wavefront
 // beside it, three 256-thread CTAs of this kernel still fit on an SM.
-template <int TX, int TY, int NT, bool FAST>
+template <int TX, int TY, int NT, bool FAST, bool BATCH = false>
 __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const float* __restrict__ U, const float* __restrict__ V, int r1,
                                                   int r2, double max_pwr_eb, const double* __restrict__ thr_tab,
                                                   int thr_n, uint8_t* __restrict__ ids_u, uint8_t* __restrict__ ids_v,
@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const f
                                                   double* __restrict__ eb_out, int row_begin, int row_end,
                                                   const int2* __restrict__ unit_order, int unit_ncb,
                                                   unsigned long long* __restrict__ unit_done, int log_ids,
-                                                  int pow4_ids) {
+                                                  int pow4_ids, const Eb2dJob* __restrict__ bjobs, int bn) {
   constexpr int CX = TX + 1;  // cells per tile row
   constexpr int CY = TY + 1;
   static_assert(WAVE_GROUP_ROWS % TY == 0, "a tile's rows must lie in one wavefront group");
@@ -59,7 +59,37 @@ __global__ void __launch_bounds__(NT, 2048 / 64 / (NT / 32)) eb2d_kernel(const f
 
   const int tid = threadIdx.x;
   int i0, j0;
-  if (unit_order) {
+  if constexpr (BATCH) {
+    __shared__ int s_job;
+    // a batched launch: the CTA's field (the last one whose tiles start at or
+    // before it) takes the place of the single field's arguments
+    if (tid == 0) {
+      int lo = 0, hi = bn - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (bjobs[mid].tile0 <= (int)blockIdx.x) lo = mid;
+        else hi = mid - 1;
+      }
+      s_job = lo;
+    }
+    __syncthreads();
+    const Eb2dJob& d = bjobs[s_job];
+    U = d.U;
+    V = d.V;
+    r1 = d.r1;
+    r2 = d.r2;
+    max_pwr_eb = d.max_pwr_eb;
+    ids_u = d.ids_u;
+    ids_v = d.ids_v;
+    hist = d.hist;
+    pair_u = d.pair_u;
+    pair_v = d.pair_v;
+    row_begin = 0;
+    row_end = d.r1;
+    const int t = (int)blockIdx.x - d.tile0;
+    i0 = (t / d.tiles_x) * TY;
+    j0 = (t % d.tiles_x) * TX;
+  } else if (unit_order) {
     // tile t of unit blockIdx.x / tiles-per-unit, row-major inside the unit
     constexpr int TPR = UNIT_COLS / TX;  // tiles per unit row
     const int2 u = unit_order[blockIdx.x / (TPR * (WAVE_GROUP_ROWS / TY))];
@@ -331,13 +361,13 @@ int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int 
       kernel<<<(unsigned)tiles, nt, 0, ctx->stream>>>(U, V, r1, r2, max_pwr_eb, d_thr_tab, thr_n, ids_u, ids_v, hist,
                                                       ctx->d_flag, pair_u, pair_v, eb_out, row_begin, row_end,
                                                       units->order, units->ncb, units->done, log_ids ? 1 : 0,
-                                                      pow4_ids && !log_ids ? 1 : 0);
+                                                      pow4_ids && !log_ids ? 1 : 0, nullptr, 0);
       return;
     }
     dim3 grid((r2 + tx - 1) / tx, (row_end - row_begin + ty - 1) / ty);
     kernel<<<grid, nt, 0, ctx->stream>>>(U, V, r1, r2, max_pwr_eb, d_thr_tab, thr_n, ids_u, ids_v, hist, ctx->d_flag,
                                          pair_u, pair_v, eb_out, row_begin, row_end, nullptr, 0, nullptr,
-                                         log_ids ? 1 : 0, pow4_ids && !log_ids ? 1 : 0);
+                                         log_ids ? 1 : 0, pow4_ids && !log_ids ? 1 : 0, nullptr, 0);
   };
   // filtered bounds unless the caller wants the bounds themselves (or an
   // unusual max_pwr_eb takes the reference's NaN paths)
@@ -358,6 +388,33 @@ int launch_eb2d(cpsz_b200_ctx* ctx, const float* U, const float* V, int r1, int 
   }
   count_launch(ctx);
   return check_launch("eb2d_kernel");
+}
+
+void eb2d_tile_shape(int shape, int* tx, int* ty) {
+  static const int shapes[6][2] = {{32, 16}, {32, 8}, {64, 8}, {32, 32}, {64, 16}, {32, 16}};
+  const int s = shape >= 0 && shape < 6 ? shape : 0;
+  *tx = shapes[s][0];
+  *ty = shapes[s][1];
+}
+
+int launch_eb2d_batch(cpsz_b200_ctx* ctx, const Eb2dJob* jobs, int n, int tiles, int shape, const double* d_thr_tab,
+                      int thr_n, bool pow4_ids) {
+  if (n <= 0 || tiles <= 0) return CPSZ_OK;
+  auto go = [&](auto kernel, int nt) {
+    kernel<<<(unsigned)tiles, nt, 0, ctx->stream>>>(nullptr, nullptr, 0, 0, 0.0, d_thr_tab, thr_n, nullptr, nullptr,
+                                                    nullptr, ctx->d_flag, nullptr, nullptr, nullptr, 0, 0, nullptr, 0,
+                                                    nullptr, 0, pow4_ids ? 1 : 0, jobs, n);
+  };
+  switch (shape) {
+    case 1: go(eb2d_kernel<32, 8, 128, true, true>, 128); break;
+    case 2: go(eb2d_kernel<64, 8, 256, true, true>, 256); break;
+    case 3: go(eb2d_kernel<32, 32, 256, true, true>, 256); break;
+    case 4: go(eb2d_kernel<64, 16, 256, true, true>, 256); break;
+    case 5: go(eb2d_kernel<32, 16, 128, true, true>, 128); break;
+    default: go(eb2d_kernel<32, 16, 256, true, true>, 256); break;
+  }
+  count_launch(ctx);
+  return check_launch("eb2d_kernel (batched)");
 }
 
 }  // namespace cpsz

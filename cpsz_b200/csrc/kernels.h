@@ -39,6 +39,28 @@ struct Eb2dUnits {
   int ncb = 0;                         // column blocks per group: ceil(r2 / UNIT_COLS)
   unsigned long long* done = nullptr;  // device: one counter per unit (group * ncb + block), zeroed
 };
+// One field of a batched bound-kernel launch (launch_eb2d_batch): its
+// inputs and outputs as launch_eb2d takes them, and its tiles' place in the
+// launch (tiles tile0 .. tile0 + tiles of the grid, tiles_x per tile row).
+struct Eb2dJob {
+  const float* U;
+  const float* V;
+  uint8_t* ids_u;
+  uint8_t* ids_v;
+  unsigned long long* hist;
+  float2* pair_u;
+  float2* pair_v;
+  double max_pwr_eb;
+  int r1, r2;
+  int tile0, tiles_x;
+};
+// Tile shape (TX, TY) of the batched launch for a launch-shape table value.
+void eb2d_tile_shape(int shape, int* tx, int* ty);
+// The filtered bounds of several fields in one launch: jobs (device, n,
+// ascending tile0, every max_pwr_eb in [0, 1e300]) with their tiles laid
+// out for `shape` (eb2d_tile_shape); tiles = the launch's tile count.
+int launch_eb2d_batch(cpsz_b200_ctx* ctx, const Eb2dJob* jobs, int n, int tiles, int shape, const double* d_thr_tab,
+                      int thr_n, bool pow4_ids);
 // The units of groups [g0, g1) in production order: unit (g, b) before
 // (g', b') when b * skew + g is smaller (ties: lower group first); skew 0 is
 // row order.

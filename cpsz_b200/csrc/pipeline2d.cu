@@ -469,7 +469,8 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   int total_groups = 0;
   for (const Job2D& j : jobs) total_groups += j.ngroups;
   WaveItem* d_items = (WaveItem*)arena_alloc(ctx, 2 * (size_t)total_groups * sizeof(WaveItem));
-  if (!d_items) return set_error(CPSZ_ERR_NOMEM, "workspace layout overflow");
+  Eb2dJob* d_ebjobs = (Eb2dJob*)arena_alloc(ctx, nj * sizeof(Eb2dJob));
+  if (!d_items || !d_ebjobs) return set_error(CPSZ_ERR_NOMEM, "workspace layout overflow");
   for (Job2D& j : jobs) CPSZ_TRY(job_alloc(ctx, j));
   for (int k = 0; k < nj; k++) {
     uint8_t* base = (uint8_t*)ctx->pinned + PINNED_BASE + (size_t)k * JOB_PINNED;
@@ -570,6 +571,51 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
   CPSZ_CUDA_TRY(cudaMemcpyAsync(d_fields, hf.data(), hf.size() * sizeof(WaveField), cudaMemcpyHostToDevice, st));
   CPSZ_CUDA_TRY(cudaMemcpyAsync(d_items, items.data(), n_items * sizeof(WaveItem), cudaMemcpyHostToDevice, st));
   CPSZ_CUDA_TRY(cudaMemsetAsync(queue, 0, 64, st));
+  // A batch of device-resident fields derives its bounds in one bound-kernel
+  // launch: every field's tiles in one grid (largest field first, so the
+  // small fields' tiles fill the launch's tail), each CTA finding its field in
+  // a descriptor table, instead of a launch per field that leaves the SMs
+  // idle while a small field's few tiles run.
+  bool eb_batched = nj > 1;
+  for (const Job2D& j : jobs)
+    eb_batched = eb_batched && j.dev_in && !j.eb_ext && !j.log_form && j.eb >= 0 && j.eb <= 1e300;
+  int eb_shape = 0, eb_tiles = 0;
+  if (eb_batched) {
+    size_t largest = 0;
+    for (const Job2D& j : jobs) largest = std::max(largest, j.N);
+    eb_shape = tune_get(TUNE_EB2D_TILE, largest);
+    int tx, ty;
+    eb2d_tile_shape(eb_shape, &tx, &ty);
+    std::vector<int> by_size(nj);
+    for (int k = 0; k < nj; k++) by_size[k] = k;
+    std::stable_sort(by_size.begin(), by_size.end(), [&](int a, int b) { return jobs[a].N > jobs[b].N; });
+    std::vector<Eb2dJob> ebj;
+    for (int k : by_size) {
+      const Job2D& j = jobs[k];
+      Eb2dJob e;
+      e.U = j.d.U;
+      e.V = j.d.V;
+      e.ids_u = j.d.ids;
+      e.ids_v = j.d.ids + j.N;
+      e.hist = j.d.hist_ids;
+      e.pair_u = j.d.pairs[0];
+      e.pair_v = j.d.pairs[1];
+      e.max_pwr_eb = j.eb;
+      e.r1 = j.r1;
+      e.r2 = j.r2;
+      e.tiles_x = (j.r2 + tx - 1) / tx;
+      e.tile0 = eb_tiles;
+      const size_t t = (size_t)e.tiles_x * ((j.r1 + ty - 1) / ty);
+      if (eb_tiles + t > (size_t)INT32_MAX) {
+        eb_batched = false;  // beyond one grid's tile count: a launch per field
+        break;
+      }
+      eb_tiles += (int)t;
+      ebj.push_back(e);
+    }
+    if (eb_batched)
+      CPSZ_CUDA_TRY(cudaMemcpyAsync(d_ebjobs, ebj.data(), nj * sizeof(Eb2dJob), cudaMemcpyHostToDevice, st));
+  }
   size_t pass_points = 0;
   for (const Job2D& j : jobs) pass_points += j.N;
   // a wavefront launched beside its producer must be finished before this
@@ -621,6 +667,8 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
       CPSZ_CUDA_TRY(cudaEventRecord(ctx->ev[2], st));
       CPSZ_CUDA_TRY(cudaStreamWaitEvent(ctx->aux, ctx->ev[2], 0));
     }
+    if (eb_batched)
+      CPSZ_TRY(launch_eb2d_batch(ctx, d_ebjobs, nj, eb_tiles, eb_shape, thr_tab, qt.n, qt.float_pow4));
     for (Job2D& j : jobs) {
       // beside the wavefront, eb2d runs unit by unit in the order made in the
       // setup; band_units(g0, g1) is the slice for the rows of groups [g0, g1)
@@ -650,7 +698,7 @@ int run_pass(cpsz_b200_ctx* ctx, std::vector<Job2D>& jobs, const StageTap* tap) 
         else if (j.eb_ext)
           CPSZ_TRY(launch_quant2d(ctx, j.d.U, j.d.V, j.N, j.eb_ext, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
                                   j.d.hist_ids, j.d.pairs[0], j.d.pairs[1]));
-        else {
+        else if (!eb_batched) {
           const Eb2dUnits u = band_units(0, j.ngroups);
           CPSZ_TRY(launch_eb2d(ctx, j.d.U, j.d.V, j.r1, j.r2, j.eb, thr_tab, qt.n, j.d.ids, j.d.ids + j.N,
                                j.d.hist_ids, j.d.pairs[0], j.d.pairs[1], nullptr, 0, -1, overlap ? &u : nullptr,
@@ -1060,7 +1108,8 @@ size_t pass_bytes(const std::vector<Job2D>& jobs) {
     total_groups += j.ngroups;
   }
   bytes += align_up(QUANT_TAB_MAX * 8, 256) + 256 + 512 + align_up(2 * jobs.size() * sizeof(WaveField), 256) + 256 +
-           align_up(2 * (size_t)total_groups * sizeof(WaveItem), 256) + 256;
+           align_up(2 * (size_t)total_groups * sizeof(WaveItem), 256) + 256 + align_up(jobs.size() * sizeof(Eb2dJob), 256) +
+           256;
   return bytes;
 }
 

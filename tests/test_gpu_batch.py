@@ -46,6 +46,32 @@ def test_batch_several_passes_and_device_io(ctx):
         assert np.all(np.isfinite(du)) and np.all(np.isfinite(dv))
 
 
+@pytest.mark.parametrize("shape", range(6))
+def test_batch_one_bound_launch_every_tile_shape(ctx, shape):
+    """A batch of device fields derives all its fields' bounds in one launch
+    (each CTA finds its field in a per-pass table, largest field first): for
+    every launch shape, with ragged fields (single rows, single columns, a
+    single point, sizes that are no multiple of a tile), every blob equals
+    the single-field compressor's."""
+    torch = pytest.importorskip("torch")
+    fields, ebs = _batch(9, 10 + shape, 1, 300)
+    for k, (r1, r2) in enumerate([(1, 1), (1, 97), (83, 1), (33, 65), (17, 129)]):
+        fields.append(W.cfg0_like(500 + 10 * shape + k, r1, r2))
+        ebs.append(0.1 if k % 2 else 0.01)
+    dev = [(torch.from_numpy(U).cuda(), torch.from_numpy(V).cuda()) for U, V in fields]
+    out = torch.zeros(32 << 20, dtype=torch.uint8, device="cuda")
+    try:
+        cpsz_b200.tuning_set("eb2d.tile", shape, min_points=0)
+        offs = cpsz_b200.compress_2d_batch(dev, ebs, out=out, ctx=ctx)
+        host = out[:int(offs[-1])].cpu().numpy().tobytes()
+        for k, ((U, V), eb) in enumerate(zip(fields, ebs)):
+            assert host[int(offs[k]):int(offs[k + 1])] == cpsz_b200.sz_compress_cp_preserve_2d_offline(
+                U, V, max_pwr_eb=eb, ctx=ctx), k
+    finally:
+        cpsz_b200.tuning_clear()
+        cpsz_b200.tuning_load()
+
+
 def test_batch_rejects_small_output(ctx):
     fields, ebs = _batch(3, 3, 50, 60)
     with pytest.raises(cpsz_b200.CpszError):
