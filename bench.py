@@ -18,7 +18,9 @@ Prints ONE JSON line (rank 0):
   ratio    raw bytes / ZSTD(level 3)'d blob bytes (the reference's definition),
            plus the pre-ZSTD ratio and decompress GB/s;
   roofline the dominant kernel's algorithmic bytes / its CUDA-event duration
-           vs the measured HBM copy bandwidth;
+           vs the measured HBM copy bandwidth; for the 2D bound kernel, which
+           is bound by instruction issue, also its warp instructions a second
+           vs 4 a cycle per SM (roofline.issue);
   cpu_baseline the reference's own CPU implementation on a bounded sample.
 Multi-GPU: a single field does not shard (its Lorenzo stage is one serial
 recurrence), so N GPUs run N independent replicas ("replicas only"); value is
@@ -516,12 +518,40 @@ def run_product(args, rank, world, device):
         roof = {"bound": "hbm", "kernel": dom, "achieved": round(ach, 2), "peak": peak, "unit": "GB/s",
                 "frac": round(ach / peak, 4), "traffic": round(tr * n) if tr else None, "peak_source": peak_kind,
                 "algorithmic_bytes": alg[dom]}
+        issue = issue_roofline(dom, n, stages[dom], clk.summary().get("sm_mhz"))
+        if issue:
+            roof["issue"] = issue
     return {
         "value": value, "ms": ms, "e2e_ms": e2e_ms, "dec_ms": dec_ms, "blob": len(blob), "size_dev": size,
         "lossless": len(lossless), "lossless_gpu": lossless_gpu, "raw": raw_bytes, "stages": stages, "roofline": roof,
         "launches": launches,
         "clocks": clk.summary(), "fields": fields, "eb": eb, "blob_bytes": blob, "check": check,
     }
+
+
+# Warp instructions per point of a kernel that is bound by instruction issue
+# rather than by HBM, from one ncu capture of it on the 4096^2 case
+# (smsp__inst_executed.sum: 404,377,736 for 16.8 M vertices).
+INSTR_PER_POINT = {"eb2d": 404377736 / 4096 ** 2}
+B200_SMS = 148
+ISSUE_PER_SM_CYCLE = 4  # one warp instruction a cycle on each of an SM's four schedulers
+
+
+def issue_roofline(kernel, points, ms, sm_mhz):
+    """The issue roofline of `kernel` over a launch of `points` points that
+    took `ms`: its warp instructions (scaled from the captured case by the
+    points) a second against 4 a cycle on each of the 148 SMs at the SM clock
+    sampled during the run; None when the kernel has no captured count or no
+    clock was sampled."""
+    per = INSTR_PER_POINT.get(kernel)
+    if per is None or not sm_mhz or not ms or ms <= 0:
+        return None
+    instr = per * points
+    achieved = instr / (ms / 1e3) / 1e9
+    peak = B200_SMS * ISSUE_PER_SM_CYCLE * float(sm_mhz) * 1e6 / 1e9
+    return {"achieved": round(achieved, 2), "peak": round(peak, 2), "unit": "G warp instructions/s",
+            "frac": round(achieved / peak, 4), "instructions": round(instr),
+            "min_ms": round(instr / (peak * 1e9) * 1e3, 4)}
 
 
 def cp_and_bound_check(kind, fields, decoded, eb, ctx):
