@@ -198,6 +198,13 @@ size_t cpo_huffman_encode(size_t state_num, const int* sym, size_t n, unsigned c
   size_t node_count = 0;
   for (size_t i = 0; i < state_num; i++)
     if (freq[i]) node_count++;
+  if (node_count == 0) { /* every symbol at or above state_num: unsupported */
+    free(cb.code);
+    free(cb.len);
+    free_tree(&h);
+    free(freq);
+    return 0;
+  }
   node_count = node_count * 2 - 1;
   /* tree serialization */
   unsigned int* L = (unsigned int*)calloc(node_count, sizeof(unsigned int));
