@@ -500,6 +500,21 @@ def run_product(args, rank, world, device):
 
     stages = {k: statistics.mean(v) for k, v in stage_acc.items()}
     n = int(np.prod(shape))
+    roof = product_roofline(kind, n, stages, clk.summary().get("sm_mhz"))
+    return {
+        "value": value, "ms": ms, "e2e_ms": e2e_ms, "dec_ms": dec_ms, "blob": len(blob), "size_dev": size,
+        "lossless": len(lossless), "lossless_gpu": lossless_gpu, "raw": raw_bytes, "stages": stages, "roofline": roof,
+        "launches": launches,
+        "clocks": clk.summary(), "fields": fields, "eb": eb, "blob_bytes": blob, "check": check,
+    }
+
+
+def product_roofline(kind, n, stages, sm_mhz):
+    """The roofline of the step's dominant kernel (the stage with the longest
+    CUDA-event time among those with algorithmic bytes) for a field of `n`
+    points: its algorithmic bytes over the stage time against the measured
+    copy bandwidth, its DRAM traffic, and for a kernel bound by instruction
+    issue its issue roofline.  None when no such stage was timed."""
     comps = 2 if kind == "2d" else 3
     # algorithmic bytes per launch of each stage's dominant kernel
     alg = {"eb2d": 4 * comps * n + comps * n,  # read fields, write one id byte per component
@@ -510,23 +525,18 @@ def run_product(args, rank, world, device):
     # launch by its points
     traffic_per_point = {"eb2d": (134.725632e6 + 254.642176e6) / 4096 ** 2}
     dom = max((k for k in stages if k in alg and alg[k]), key=lambda k: stages[k], default=None)
+    if not dom:
+        return None
     peak, peak_kind = measured_peaks()
-    roof = None
-    if dom:
-        ach = alg[dom] / (stages[dom] / 1e3) / 1e9
-        tr = traffic_per_point.get(dom)
-        roof = {"bound": "hbm", "kernel": dom, "achieved": round(ach, 2), "peak": peak, "unit": "GB/s",
-                "frac": round(ach / peak, 4), "traffic": round(tr * n) if tr else None, "peak_source": peak_kind,
-                "algorithmic_bytes": alg[dom]}
-        issue = issue_roofline(dom, n, stages[dom], clk.summary().get("sm_mhz"))
-        if issue:
-            roof["issue"] = issue
-    return {
-        "value": value, "ms": ms, "e2e_ms": e2e_ms, "dec_ms": dec_ms, "blob": len(blob), "size_dev": size,
-        "lossless": len(lossless), "lossless_gpu": lossless_gpu, "raw": raw_bytes, "stages": stages, "roofline": roof,
-        "launches": launches,
-        "clocks": clk.summary(), "fields": fields, "eb": eb, "blob_bytes": blob, "check": check,
-    }
+    ach = alg[dom] / (stages[dom] / 1e3) / 1e9
+    tr = traffic_per_point.get(dom)
+    roof = {"bound": "hbm", "kernel": dom, "achieved": round(ach, 2), "peak": peak, "unit": "GB/s",
+            "frac": round(ach / peak, 4), "traffic": round(tr * n) if tr else None, "peak_source": peak_kind,
+            "algorithmic_bytes": alg[dom]}
+    issue = issue_roofline(dom, n, stages[dom], sm_mhz)
+    if issue:
+        roof["issue"] = issue
+    return roof
 
 
 # Warp instructions per point of a kernel that is bound by instruction issue
