@@ -23,6 +23,43 @@ def test_2d_blob_and_decode_identical(oracle, reference, r1, r2, eb, seed):
         assert_bits_equal(x, y)
 
 
+def _edge_field(case):
+    g = np.random.default_rng(31)
+    if case == "zeros":
+        return np.zeros((50, 70), np.float32), np.zeros((50, 70), np.float32), 0.1
+    if case == "constant":
+        return np.full((40, 40), 3.5, np.float32), np.full((40, 40), -2.0, np.float32), 0.1
+    if case == "small_integers":  # many degenerate and tied triangles
+        return (g.integers(-3, 4, (60, 50)).astype(np.float32), g.integers(-3, 4, (60, 50)).astype(np.float32), 0.1)
+    if case == "tiny_magnitudes":
+        U, V = W.cfg0_like(22, 80, 90)
+        return U * np.float32(1e-30), V * np.float32(1e-30), 0.1
+    if case == "bound_1":
+        U, V = W.cfg0_like(23, 70, 60)
+        return U, V, 1.0
+    r1, r2 = (int(x) for x in case.split("x"))
+    U, V = W.cfg0_like(25, r1, r2)
+    return U, V, 0.1
+
+
+# Fields whose products overflow float (|x| near 1e30) are left out: the
+# reference's bounds are NaN there and its id histogram is indexed out of range.
+@pytest.mark.parametrize("case", ["zeros", "constant", "small_integers", "tiny_magnitudes", "bound_1", "1x50", "50x1",
+                                  "12x12", "13x25", "2x300"])
+def test_2d_edge_cases_identical(oracle, reference, case):
+    """Constant and all-zero fields, integer-valued fields, magnitudes near the
+    float minimum, the largest relative bound, and shapes of one row, one
+    column, exactly one block and one block plus a ragged edge."""
+    U, V, eb = _edge_field(case)
+    r1, r2 = U.shape
+    a = oracle.compress_2d(U, V, eb)
+    assert ref_2d_in_bounds(a, r1, r2)
+    b = reference.compress_2d(U, V, eb)
+    assert_blob_equal_2d(a, b)
+    for x, y in zip(oracle.decompress_2d(a, r1, r2), reference.decompress_2d(b, r1, r2)):
+        assert_bits_equal(x, y)
+
+
 @pytest.mark.parametrize("r1,r2,eb,seed", [(200, 300, 0.1, 16), (317, 211, 0.01, 17), (64, 900, 0.05, 18)])
 def test_2d_log_blob_and_decode_identical(oracle, reference, r1, r2, eb, seed):
     U, V = W.cfg0_like(seed, r1, r2)
