@@ -50,6 +50,8 @@ def build_reference(ref_dir: str | None = None) -> str | None:
 
 
 def _take_blob(lib, ptr, size) -> bytes:
+    if not ptr:
+        raise ValueError("input outside the compressor's domain (bound ids out of range)")
     out = C.string_at(ptr, size)
     lib.cpo_free(ptr) if hasattr(lib, "cpo_free") else lib.cpsz_ref_free(ptr)
     return out

@@ -321,6 +321,13 @@ unsigned char* cpo_compress_2d_offline(const float* U, const float* V, size_t r1
   unsigned char* ceb = (unsigned char*)calloc(cpo_huffman_encode_bound(2 * 1024, 2 * n), 1);
   size_t ceb_size = cpo_huffman_encode(2 * 1024, ids, 2 * n, ceb);
   free(ids);
+  if (!ceb_size) { /* bound ids out of range (NaN bounds): unsupported */
+    free(ceb);
+    free(eb_u);
+    free(eb_v);
+    *size = 0;
+    return NULL;
+  }
   size_t cu_size = 0, cv_size = 0;
   unsigned char* cu = cpo_compress_2d_with_eb(U, eb_u, r1, r2, &cu_size);
   unsigned char* cv = cpo_compress_2d_with_eb(V, eb_v, r1, r2, &cv_size);
@@ -502,6 +509,15 @@ unsigned char* cpo_compress_2d_offline_log(const float* U, const float* V, size_
   unsigned char* ceb = (unsigned char*)calloc(cpo_huffman_encode_bound(2 * 1024, n), 1);
   size_t ceb_size = cpo_huffman_encode(2 * 1024, ids, n, ceb);
   free(ids);
+  if (!ceb_size) { /* bound ids out of range (NaN bounds): unsupported */
+    free(ceb);
+    free(log_u);
+    free(log_v);
+    free(eb);
+    free(signs);
+    *size = 0;
+    return NULL;
+  }
   size_t cu_size = 0, cv_size = 0;
   unsigned char* cu = cpo_compress_2d_with_eb(log_u, eb, r1, r2, &cu_size);
   free(log_u);

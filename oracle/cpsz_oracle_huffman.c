@@ -149,18 +149,27 @@ size_t cpo_huffman_encode_bound(size_t state_num, size_t n) {
   return 8 + 4 + tree_bytes_size(nodes) + 8 + n * 8 + 16;
 }
 
-static void histogram(const int* sym, size_t n, size_t bins, size_t* freq) {
+/* 0, or -1 when a symbol lies outside [0, bins) (the reference indexes its
+ * histogram out of range there: NaN bounds give such ids). */
+static int histogram(const int* sym, size_t n, size_t bins, size_t* freq) {
   memset(freq, 0, bins * sizeof(size_t));
-  for (size_t i = 0; i < n; i++) freq[sym[i]]++;
+  for (size_t i = 0; i < n; i++) {
+    if (sym[i] < 0 || (size_t)sym[i] >= bins) return -1;
+    freq[sym[i]]++;
+  }
+  return 0;
 }
 
 size_t cpo_huffman_code_lengths(size_t state_num, const int* sym, size_t n, unsigned char* len) {
   size_t bins = 2 * state_num;
   size_t* freq = (size_t*)malloc(bins * sizeof(size_t));
-  histogram(sym, n, bins, freq);
+  memset(len, 0, bins);
+  if (histogram(sym, n, bins, freq) != 0) {
+    free(freq);
+    return 0;
+  }
   HTree h;
   int root = build_tree(&h, freq, bins);
-  memset(len, 0, bins);
   size_t distinct = 0;
   for (size_t i = 0; i < bins; i++) distinct += freq[i] != 0;
   if (root >= 0 && tree_depth(&h, root) <= 64) {
@@ -183,7 +192,10 @@ static void put(unsigned char** p, const void* v, size_t n) {
 size_t cpo_huffman_encode(size_t state_num, const int* sym, size_t n, unsigned char* out) {
   size_t bins = 2 * state_num; /* allNodes */
   size_t* freq = (size_t*)malloc(bins * sizeof(size_t));
-  histogram(sym, n, bins, freq);
+  if (histogram(sym, n, bins, freq) != 0) { /* symbols out of range: unsupported */
+    free(freq);
+    return 0;
+  }
   HTree h;
   int root = build_tree(&h, freq, bins);
   if (root < 0 || tree_depth(&h, root) > 64) { /* empty input / >64-bit codes: unsupported */

@@ -63,3 +63,18 @@ def test_huffman_roundtrip_and_single_symbol(oracle):
         dec, used = oracle.huffman_decode(65536, n, enc)
         assert used == len(enc)
         assert np.array_equal(dec, sym)
+
+
+def test_oracle_rejects_bounds_outside_the_domain(oracle):
+    """Products of field values beyond FLT_MAX make the reference's bounds NaN
+    and its bound ids index its histogram out of range; the restatement
+    refuses such a field instead of reading past its arrays."""
+    from cpsz_b200 import workloads as W
+
+    U, V = W.cfg0_like(21, 80, 90)
+    U, V = U * np.float32(1e30), V * np.float32(1e30)
+    assert np.isnan(oracle.eb_2d(U, V, 0.1)).all()
+    for compress in (oracle.compress_2d, oracle.compress_2d_log):
+        with pytest.raises(ValueError):
+            compress(U, V, 0.1)
+
