@@ -276,7 +276,7 @@ int cpsz_b200_huffman_encode_u16(cpsz_b200_ctx* ctx, const uint16_t* sym, size_t
  * (cudaGetSymbolAddress) in the calling thread's current device and context,
  * so the address stays valid after a device reset and in a context the caller
  * made current; the first call on a device also loads the library's kernels
- * there, so make it before any stream capture.  All calls on a device share
+ * there.  All calls on a device share
  * the one array, which keeps the last call's contents (the call clears what
  * must start at zero), so calls whose GPU work overlaps (concurrent streams,
  * threads) race and must be serialised by the caller. */
